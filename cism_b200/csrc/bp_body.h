@@ -1,0 +1,366 @@
+// bp_body.h -- per-thread arithmetic of the device kernels.
+//
+// Everything here is plain per-node / per-element arithmetic on a DevView,
+// compiled as __host__ __device__ so the exact same code can also be checked
+// against the CPU oracle without a GPU (tests/hostemu).  Block reductions,
+// shuffles and launch logic live in bp_kernels.cu.
+#pragma once
+
+#include <cmath>
+
+#include "bp_common.h"
+
+#if defined(__CUDA_ARCH__)
+#define BP_LD_STREAM(p) __ldcs(p)
+#define BP_LD_RO(p) __ldg(p)
+#define BP_FMA(a, b, c) __fma_rn((a), (b), (c))
+#else
+#define BP_LD_STREAM(p) (*(p))
+#define BP_LD_RO(p) (*(p))
+#define BP_FMA(a, b, c) std::fma((a), (b), (c))
+#endif
+
+namespace bp {
+
+// ---------------------------------------------------------------------
+// Reference-element tables, glissade_velo_higher_init
+// (glissade_velo_higher.F90:270-650).  Node numbering: 1-4 lower face
+// (SW, SE, NE, NW), 5-8 upper face; quadrature points likewise at
+// +-1/sqrt(3), unit weights.
+// ---------------------------------------------------------------------
+struct RefTables {
+  double dxr[8][8], dyr[8][8], dzr[8][8];  // [p][n] d(phi_n)/d(xi) at point p
+  double phi2[4][4];                        // [p][n] bilinear face basis
+  double dxr2[4][4], dyr2[4][4];            // [p][n]
+};
+
+inline void fill_ref_tables(RefTables* t) {
+  const double r = 1.0 / std::sqrt(3.0);
+  const double sx[8] = {-1, 1, 1, -1, -1, 1, 1, -1};
+  const double sy[8] = {-1, -1, 1, 1, -1, -1, 1, 1};
+  const double sz[8] = {-1, -1, -1, -1, 1, 1, 1, 1};
+  for (int p = 0; p < 8; ++p) {
+    const double x = sx[p] * r, y = sy[p] * r, z = sz[p] * r;
+    for (int n = 0; n < 8; ++n) {
+      t->dxr[p][n] = sx[n] * (1.0 + sy[n] * y) * (1.0 + sz[n] * z) / 8.0;
+      t->dyr[p][n] = sy[n] * (1.0 + sx[n] * x) * (1.0 + sz[n] * z) / 8.0;
+      t->dzr[p][n] = sz[n] * (1.0 + sx[n] * x) * (1.0 + sy[n] * y) / 8.0;
+    }
+  }
+  for (int p = 0; p < 4; ++p) {
+    const double x = sx[p] * r, y = sy[p] * r;
+    for (int n = 0; n < 4; ++n) {
+      t->phi2[p][n] = (1.0 + sx[n] * x) * (1.0 + sy[n] * y) / 4.0;
+      t->dxr2[p][n] = sx[n] * (1.0 + sy[n] * y) / 4.0;
+      t->dyr2[p][n] = sy[n] * (1.0 + sx[n] * x) / 4.0;
+    }
+  }
+}
+
+// ishift/jshift/kshift (glissade_velo_higher.F90:453-486): offset of node
+// nc relative to node nr inside one element; nodes 0..3 lower, 4..7 upper.
+BP_HD constexpr int node_di(int n) { return (n == 1 || n == 2 || n == 5 || n == 6) ? 1 : 0; }
+BP_HD constexpr int node_dj(int n) { return (n == 2 || n == 3 || n == 6 || n == 7) ? 1 : 0; }
+BP_HD constexpr int node_up(int n) { return n >= 4 ? 1 : 0; }
+// stencil index (0-based indxA_3d) into which K(nr,nc) is summed; k grows downward
+BP_HD constexpr int elem_m(int nr, int nc) {
+  return (node_di(nc) - node_di(nr) + 1) + 3 * (node_dj(nc) - node_dj(nr) + 1) +
+         9 * (node_up(nr) - node_up(nc) + 1);
+}
+
+// ---------------------------------------------------------------------
+// Pass 1 of assembly: one quadrature point of one element.
+// get_basis_function_derivatives_3d (:6360-6579) and
+// compute_effective_viscosity (:7199-7378).  Writes f = efvs*w*detJ/vol0
+// and J^-1 (row-major) to out[0..9]; returns false for a singular Jacobian.
+// ---------------------------------------------------------------------
+BP_HD bool qp_compute(const RefTables& T, int p, const double* x,
+                      const double* y, const double* z, const double* u,
+                      const double* w, int which_efvs, double efvs_constant,
+                      double flwafact, double* out, double* efvs_qp) {
+  double J00 = 0, J01 = 0, J02 = 0, J10 = 0, J11 = 0, J12 = 0, J20 = 0, J21 = 0, J22 = 0;
+#pragma unroll
+  for (int n = 0; n < 8; ++n) {
+    const double a = T.dxr[p][n], b = T.dyr[p][n], c = T.dzr[p][n];
+    J00 += a * x[n]; J01 += a * y[n]; J02 += a * z[n];
+    J10 += b * x[n]; J11 += b * y[n]; J12 += b * z[n];
+    J20 += c * x[n]; J21 += c * y[n]; J22 += c * z[n];
+  }
+  const double c00 = J11 * J22 - J12 * J21;
+  const double c01 = -(J10 * J22 - J12 * J20);
+  const double c02 = J10 * J21 - J11 * J20;
+  const double c10 = -(J01 * J22 - J02 * J21);
+  const double c11 = J00 * J22 - J02 * J20;
+  const double c12 = -(J00 * J21 - J01 * J20);
+  const double c20 = J01 * J12 - J02 * J11;
+  const double c21 = -(J00 * J12 - J02 * J10);
+  const double c22 = J00 * J11 - J01 * J10;
+  const double det = J00 * c00 + J01 * c01 + J02 * c02;
+  if (!(fabs(det) > 0.0)) return false;
+  // Jinv(row,col) = cofactor(col,row)/detJ
+  const double i00 = c00 / det, i01 = c10 / det, i02 = c20 / det;
+  const double i10 = c01 / det, i11 = c11 / det, i12 = c21 / det;
+  const double i20 = c02 / det, i21 = c12 / det, i22 = c22 / det;
+  double efvs;
+  if (which_efvs == 0) {
+    efvs = efvs_constant;
+  } else if (which_efvs == 1) {
+    const double scyr = 31536000.0;
+    const double effstrain = (500.0 / scyr) / 200.0e3 * scyr;
+    efvs = flwafact * pow(effstrain, (1.0 - 3.0) / 3.0);
+  } else {
+    double ux = 0, uy = 0, uz = 0, vx = 0, vy = 0, vz = 0;
+#pragma unroll
+    for (int n = 0; n < 8; ++n) {
+      const double a = T.dxr[p][n], b = T.dyr[p][n], c = T.dzr[p][n];
+      const double dx = BP_FMA(i02, c, BP_FMA(i01, b, i00 * a));
+      const double dy = BP_FMA(i12, c, BP_FMA(i11, b, i10 * a));
+      const double dz = BP_FMA(i22, c, BP_FMA(i21, b, i20 * a));
+      ux += dx * u[n]; uy += dy * u[n]; uz += dz * u[n];
+      vx += dx * w[n]; vy += dy * w[n]; vz += dz * w[n];
+    }
+    const double smin = 1.0e-8;
+    const double sq = smin * smin + (ux * ux + vy * vy + ux * vy + 0.25 * ((vx + uy) * (vx + uy))) +
+                      0.25 * (uz * uz + vz * vz);
+    const double p2 = ((1.0 - 3.0) / 3.0) / 2.0;
+    efvs = flwafact * pow(sq, p2);
+  }
+  *efvs_qp = efvs;
+  out[0] = efvs * 1.0 * det / kVol0;
+  out[1] = i00; out[2] = i01; out[3] = i02;
+  out[4] = i10; out[5] = i11; out[6] = i12;
+  out[7] = i20; out[8] = i21; out[9] = i22;
+  return true;
+}
+
+// Gather the 8 nodes of element e (cell, layer kk) and run qp_compute.
+BP_HD bool qp_element_point(const DevView& v, const RefTables& T, int e, int p,
+                            double* out, double* efvs_qp) {
+  const int nz = v.nz, nl = nz - 1;
+  const int cell = e / nl, kk = e - cell * nl;
+  const InstParams& ip = v.inst[v.cell_inst[cell]];
+  const int ic = v.cell_ij[cell], jc = v.cell_ij[v.ncells + cell];
+  double x[8], y[8], z[8], u[8], w[8];
+#pragma unroll
+  for (int n = 0; n < 8; ++n) {
+    const int corner = n & 3;              // SW, SE, NE, NW
+    const int lev = n < 4 ? kk + 1 : kk;   // nodes 1-4 lower (k+1), 5-8 upper (k)
+    const int iv = (corner == 1 || corner == 2) ? ic : ic - 1;
+    const int jv = (corner >= 2) ? jc : jc - 1;
+    x[n] = ip.dx * iv;
+    y[n] = ip.dy * jv;
+    const double s = v.cell_s[corner * v.ncells + cell];
+    const double h = v.cell_h[corner * v.ncells + cell];
+    z[n] = s - ip.sigma[lev] * h;
+    const int col = v.cell_cols[corner * v.ncells + cell];
+    if (col >= 0) {
+      const double2 xv = v.x[(size_t)col * nz + lev];
+      u[n] = xv.x; w[n] = xv.y;
+    } else {
+      u[n] = 0.0; w[n] = 0.0;
+    }
+  }
+  return qp_compute(T, p, x, y, z, u, w, ip.which_efvs, ip.efvs_constant,
+                    v.flwafact[e], out, efvs_qp);
+}
+
+// ---------------------------------------------------------------------
+// Pass 2 of assembly: the row of node (col,k) in block B (0 uu, 1 uv,
+// 2 vu, 3 vv), gathered from its incident elements in the reference's
+// element order (j, then i, then k).  compute_element_matrix (:7868-7986)
+// and element_to_global_matrix_3d (:7990-8054).  The element terms use
+// one fixed fma pattern so that K(nr,nc) and K(nc,nr) are bitwise equal
+// and the assembled matrix is exactly symmetric.
+// ---------------------------------------------------------------------
+template <int B>
+BP_HD double block_term(double ar, double br, double cr, double ac, double bc, double cc) {
+  if (B == 0) return BP_FMA(cr, cc, BP_FMA(4.0 * ar, ac, br * bc));
+  if (B == 1) return BP_FMA(2.0 * ar, bc, br * ac);
+  if (B == 2) return BP_FMA(2.0 * br, ac, ar * bc);
+  return BP_FMA(cr, cc, BP_FMA(4.0 * br, bc, ar * ac));
+}
+
+template <int NR, int B>
+BP_HD void row_element(const RefTables& T, const double* qpe, double* acc) {
+  double K[8];
+#pragma unroll
+  for (int nc = 0; nc < 8; ++nc) K[nc] = 0.0;
+  for (int p = 0; p < 8; ++p) {
+    const double* q = qpe + p * 10;
+    const double f = BP_LD_RO(q + 0);
+    const double i00 = BP_LD_RO(q + 1), i01 = BP_LD_RO(q + 2), i02 = BP_LD_RO(q + 3);
+    const double i10 = BP_LD_RO(q + 4), i11 = BP_LD_RO(q + 5), i12 = BP_LD_RO(q + 6);
+    const double i20 = BP_LD_RO(q + 7), i21 = BP_LD_RO(q + 8), i22 = BP_LD_RO(q + 9);
+    double ax[8], ay[8], az[8];
+#pragma unroll
+    for (int n = 0; n < 8; ++n) {
+      const double a = T.dxr[p][n], b = T.dyr[p][n], c = T.dzr[p][n];
+      ax[n] = BP_FMA(i02, c, BP_FMA(i01, b, i00 * a));
+      ay[n] = BP_FMA(i12, c, BP_FMA(i11, b, i10 * a));
+      az[n] = BP_FMA(i22, c, BP_FMA(i21, b, i20 * a));
+    }
+#pragma unroll
+    for (int nc = 0; nc < 8; ++nc)
+      K[nc] = BP_FMA(f, block_term<B>(ax[NR], ay[NR], az[NR], ax[nc], ay[nc], az[nc]), K[nc]);
+  }
+#pragma unroll
+  for (int nc = 0; nc < 8; ++nc) acc[elem_m(NR, nc)] += K[nc];
+}
+
+// Element index of (cell, layer) or -1.
+BP_HD int elem_of(int cell, int kk, int nz) { return cell < 0 ? -1 : cell * (nz - 1) + kk; }
+
+template <int B>
+BP_HD void row_assemble(const DevView& v, const RefTables& T, int col, int k,
+                        double* acc) {
+  const int nz = v.nz, nc = v.ncols;
+#pragma unroll
+  for (int m = 0; m < 27; ++m) acc[m] = 0.0;
+  const int c0 = v.col_cells[0 * nc + col];  // cell (i,j):     vertex is its NE corner
+  const int c1 = v.col_cells[1 * nc + col];  // cell (i+1,j):   NW corner
+  const int c2 = v.col_cells[2 * nc + col];  // cell (i,j+1):   SE corner
+  const int c3 = v.col_cells[3 * nc + col];  // cell (i+1,j+1): SW corner
+  const bool lo = k >= 1, up = k <= nz - 2;  // element above (k-1) / below (k)
+  const double* qp = v.qp;
+  if (c0 >= 0) {
+    if (lo) row_element<2, B>(T, qp + (size_t)elem_of(c0, k - 1, nz) * 80, acc);
+    if (up) row_element<6, B>(T, qp + (size_t)elem_of(c0, k, nz) * 80, acc);
+  }
+  if (c1 >= 0) {
+    if (lo) row_element<3, B>(T, qp + (size_t)elem_of(c1, k - 1, nz) * 80, acc);
+    if (up) row_element<7, B>(T, qp + (size_t)elem_of(c1, k, nz) * 80, acc);
+  }
+  if (c2 >= 0) {
+    if (lo) row_element<1, B>(T, qp + (size_t)elem_of(c2, k - 1, nz) * 80, acc);
+    if (up) row_element<5, B>(T, qp + (size_t)elem_of(c2, k, nz) * 80, acc);
+  }
+  if (c3 >= 0) {
+    if (lo) row_element<0, B>(T, qp + (size_t)elem_of(c3, k - 1, nz) * 80, acc);
+    if (up) row_element<4, B>(T, qp + (size_t)elem_of(c3, k, nz) * 80, acc);
+  }
+}
+
+// basal_sliding_bc (:8125-8381), bed layer only, diagonal blocks only.
+template <int B>
+BP_HD void row_basal(const DevView& v, const RefTables& T, int col, int k,
+                     double* acc) {
+  if (B != 0 && B != 3) return;
+  if (k != v.nz - 1) return;
+  const InstParams& ip = v.inst[v.col_inst[col]];
+  if (ip.which_babc == 6) return;  // HO_BABC_NO_SLIP: no basal term
+  if (ip.which_assemble_beta == 1) {  // HO_ASSEMBLE_BETA_LOCAL
+    acc[13] += ip.dx * ip.dy / kVol0 * v.col_beta[col];
+    return;
+  }
+  // standard: 2x2 face quadrature of beta * phi_r * phi_c on each bed face;
+  // in-plane entries (kA = 0, stencil 9..17) gathered in a side array so
+  // that acc keeps compile-time indices
+  const int nc = v.ncols;
+  const int nr_of_q[4] = {2, 3, 1, 0};  // 2-D node of this vertex in cells q = 0..3
+  double bacc[9];
+  for (int t = 0; t < 9; ++t) bacc[t] = 0.0;
+  for (int qc = 0; qc < 4; ++qc) {
+    const int cell = v.col_cells[qc * nc + col];
+    if (cell < 0) continue;
+    const int nr = nr_of_q[qc];
+    const int ic = v.cell_ij[cell], jc = v.cell_ij[v.ncells + cell];
+    const double xs[4] = {ip.dx * (ic - 1), ip.dx * ic, ip.dx * ic, ip.dx * (ic - 1)};
+    const double ys[4] = {ip.dy * (jc - 1), ip.dy * (jc - 1), ip.dy * jc, ip.dy * jc};
+    double b[4];
+    for (int q = 0; q < 4; ++q) b[q] = v.cell_beta[q * v.ncells + cell];
+    for (int p = 0; p < 4; ++p) {
+      double J11 = 0, J12 = 0, J21 = 0, J22 = 0;
+      for (int n = 0; n < 4; ++n) {
+        J11 += T.dxr2[p][n] * xs[n]; J12 += T.dxr2[p][n] * ys[n];
+        J21 += T.dyr2[p][n] * xs[n]; J22 += T.dyr2[p][n] * ys[n];
+      }
+      const double detJ = J11 * J22 - J12 * J21;
+      double bq = 0.0;
+      for (int n = 0; n < 4; ++n) bq += T.phi2[p][n] * b[n];
+      for (int ncn = 0; ncn < 4; ++ncn) {
+        const double kv = bq * 1.0 * detJ / kVol0 * T.phi2[p][nr] * T.phi2[p][ncn];
+        bacc[(node_di(ncn) - node_di(nr) + 1) + 3 * (node_dj(ncn) - node_dj(nr) + 1)] += kv;
+      }
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < 9; ++t) acc[9 + t] += bacc[t];
+}
+
+// dirichlet_boundary_conditions_3d (:8385-8578) restated row-locally: the
+// row of node (col,k) is replaced when its own component is prescribed,
+// and its entries toward prescribed neighbours are moved to the right-hand
+// side.  Returns the sum moved to b (to be subtracted).
+template <int B>
+BP_HD double row_dirichlet(const DevView& v, int col, int k, double* acc) {
+  const int nz = v.nz, nc = v.ncols;
+  const uint8_t me = v.dmask[(size_t)col * nz + k];
+  const bool ur = me & 1, vr = me & 2;
+  const bool row_presc = (B <= 1) ? ur : vr;
+  double adj = 0.0;
+  if (!row_presc && !v.any_dirichlet) return 0.0;
+#pragma unroll
+  for (int m = 0; m < 27; ++m) {
+    const int iA = m % 3 - 1, jA = (m / 3) % 3 - 1, kA = m / 9 - 1;
+    const bool diag = (m == 13);
+    const int kn = k + kA;
+    const int cn = v.col_nbr[((jA + 1) * 3 + (iA + 1)) * nc + col];
+    const bool inb = (kn >= 0 && kn < nz && cn >= 0);
+    if (row_presc) {
+      if (inb || diag) acc[m] = (diag && (B == 0 || B == 3)) ? 1.0 : 0.0;
+      continue;
+    }
+    if (!inb) continue;
+    const size_t nn = (size_t)cn * nz + kn;
+    const uint8_t pm = v.dmask[nn];
+    if (diag) {
+      // the reference zeroes the u-v coupling at a node whose other
+      // component is prescribed, without moving it to the rhs
+      if (B == 1 && vr) acc[m] = 0.0;
+      if (B == 2 && ur) acc[m] = 0.0;
+      continue;
+    }
+    const bool col_u = (B == 0 || B == 2);  // this block multiplies u of the neighbour
+    const bool pres = col_u ? (pm & 1) : (pm & 2);
+    if (pres) {
+      const double2 xp = v.x[nn];
+      adj += acc[m] * (col_u ? xp.x : xp.y);
+      acc[m] = 0.0;
+    }
+  }
+  return adj;
+}
+
+// ---------------------------------------------------------------------
+// Structured 27-point block matvec, one row pair (u,v) of node (col,k):
+// matvec_multiply_structured_3d (glissade_velo_higher_pcg.F90:2533-2647),
+// same kA/jA/iA summation order.  SRC returns the source vector at a node.
+// ---------------------------------------------------------------------
+template <typename Mat, typename Src>
+BP_HD double2 matvec_row(const DevView& v, const Mat* A, int col, int k, size_t n,
+                         const Src& src) {
+  const int nz = v.nz, nc = v.ncols;
+  const size_t np = (size_t)v.npad;
+  int cn[9];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) cn[q] = v.col_nbr[q * nc + col];
+  double yu = 0.0, yv = 0.0;
+#pragma unroll
+  for (int kA = -1; kA <= 1; ++kA) {
+    const int kn = k + kA;
+    if (kn < 0 || kn >= nz) continue;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+      if (cn[q] < 0) continue;
+      const int m = (kA + 1) * 9 + q;
+      const Mat au = BP_LD_STREAM(A + (size_t)m * np + n);
+      const Mat av = BP_LD_STREAM(A + (size_t)(27 + m) * np + n);
+      const double2 s = src((size_t)cn[q] * nz + kn);
+      yu += (double)au.x * s.x + (double)au.y * s.y;
+      yv += (double)av.x * s.x + (double)av.y * s.y;
+    }
+  }
+  return double2{yu, yv};
+}
+
+}  // namespace bp

@@ -1,0 +1,123 @@
+// bp_common.h -- types shared by the host plan builder and the device kernels.
+//
+// Device data model.  A solve (or a batch of independent solves) is
+// compiled into a set of *columns*: the locally owned, active vertices of
+// each instance (the rows the reference's matvec computes,
+// glissade_velo_higher_pcg.F90:2605-2612).  The halo of the reference's
+// local grid disappears: a periodic image map turns halo vertices into the
+// owned vertices they copy (parallel_slap.F90:2807-2925), so every stencil
+// neighbour is an owned column or absent.  Node n = col * nz + k (k = 0 is
+// the upper surface, k = nz-1 the bed, as in the reference).  Elements are
+// the reference's active cells (i,j in [nhalo+1, n-nhalo+1]) times nz-1
+// layers; their geometry is taken from the halo'd vertex arrays so periodic
+// surface offsets are preserved.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+#if defined(__CUDACC__)
+#define BP_HD __host__ __device__ __forceinline__
+#include <cuda_runtime.h>
+#else
+#define BP_HD inline
+#include <vector_types.h>  // double2 / float2 (plain structs under a host compiler)
+#endif
+
+namespace bp {
+
+constexpr int kNzMax = 64;     // largest supported number of levels
+constexpr int kTile = 256;     // nodes per tile; one CTA of kTile threads per tile
+constexpr double kVol0 = 1.0e9;  // volume scale, glissade_velo_higher.F90:1111
+
+// Per-instance constants (read-only on the device).
+struct InstParams {
+  double dx, dy;
+  double efvs_constant;
+  double pcg_tol;
+  double inner_tol;
+  double sigma[kNzMax];
+  int which_efvs, which_babc, which_assemble_beta, which_resid;
+  int precond, variant, precision;
+  int pcg_maxiters, ncheck, maxiter_nonlinear;
+  int col_begin, col_end;
+  int node_begin, node_end;
+  int tile_begin, tile_end;
+  int cell_begin, cell_end;
+  int elem_begin, elem_end;
+};
+
+// Per-instance solver state (device-resident, written by finalizers).
+struct InstState {
+  double bb, L2_rhs;            // (b,b) and its root
+  double rz, rz_old;            // eta1 / eta0 (standard) ; rho / rho_old (Chron-Gear)
+  double alpha, beta, sigma;    // CG scalars
+  double err;                   // |b-Ax|/|b| at the last check
+  double L2_norm, L2_rel;       // residual before the linear solve
+  double resid_velo;            // Picard criterion value
+  double in_rr0;                // mixed: inner initial (r,r)
+  int pcg_iter, pcg_active, pcg_converged;
+  int picard_iter, picard_active, picard_converged;
+  int status;                   // bp_status
+  int nonzero;                  // any nonzero matrix entry (count_nonzeros_3d)
+  int zero_x;                   // velocity must be zeroed (all-zero matrix)
+  int pcg_iters_total, pcg_iters_last;
+  int refine_active, refine_steps, refine_steps_total;
+  int inner_iter;
+  int pad;
+};
+
+// Global counters polled by the host.
+struct Counters {
+  int pcg_active;
+  int picard_active;
+  int refine_active;
+  int pad;
+};
+
+// Device view of a compiled problem (all pointers are device pointers).
+struct DevView {
+  int nz, ncols, nnodes, npad, ncells, nelem, ninst, ntiles;
+  int any_dirichlet;       // any prescribed node in the problem
+  const InstParams* inst;
+  InstState* st;
+  Counters* cnt;
+  // columns
+  const int* col_inst;     // [ncols]
+  const int* col_nbr;      // [9][ncols], q = (jA+1)*3 + (iA+1); -1 = none
+  const int* col_cells;    // [4][ncols], cells (i,j),(i+1,j),(i,j+1),(i+1,j+1)
+  const int* col_ij;       // [2][ncols], halo'd Fortran vertex indices
+  const double* col_beta;  // [ncols] beta_internal
+  // nodes
+  const double2* load;     // [nnodes] (loadu, loadv)
+  const uint8_t* dmask;    // [nnodes] bit0 u prescribed, bit1 v prescribed
+  // cells
+  const int* cell_inst;    // [ncells]
+  const int* cell_ij;      // [2][ncells] halo'd Fortran cell indices
+  const int* cell_cols;    // [4][ncells] corner columns SW, SE, NE, NW (-1 = none)
+  const double* cell_s;    // [4][ncells] stagusrf at the corners
+  const double* cell_h;    // [4][ncells] stagthck at the corners
+  const double* cell_beta; // [4][ncells] beta_internal at the corners
+  const double* flwafact;  // [ncells*(nz-1)]
+  // tiles
+  const int* tile_start;   // [ntiles]
+  const int* tile_inst;    // [ntiles]
+  // assembly / matrix
+  double* qp;              // [nelem*8*10]: f, Jinv(3x3) per quadrature point
+  double* efvs;            // [nelem]
+  double2* A;              // [2][27][npad]: (uu,uv) rows then (vu,vv) rows
+  float2* A32;             // [2][27][npad]: equilibrated FP32 copy (mixed)
+  double* badj;            // [4][npad] Dirichlet column moves per block
+  // vectors (per node, (u,v) pairs)
+  double2 *x, *b, *r, *d0, *d1, *q, *Az, *Dinv, *usav;
+  double2 *scale;          // mixed: 1/sqrt(diag)
+  float2 *y32, *r32, *p32a, *p32b, *q32;
+  // reductions
+  double* partials;        // [2][ntiles]
+  unsigned* tile_counter;  // [ninst]
+};
+
+// indxA_3d (glissade_velo_higher.F90:599-619), 0-based: iA fastest.
+BP_HD int stencil_index(int iA, int jA, int kA) { return (iA + 1) + 3 * (jA + 1) + 9 * (kA + 1); }
+
+}  // namespace bp

@@ -1,0 +1,32 @@
+// bp_kernels.h -- host-callable launchers of the device kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "bp_common.h"
+
+namespace bp {
+
+enum MvMode { MV_INIT = 0, MV_STD_A = 1, MV_CG_FIRST = 2, MV_CG1 = 3, MV_CHECK = 4 };
+
+cudaError_t upload_ref_tables();
+// Upper bound on the grid of tile kernels (0 = one CTA per tile).
+void set_grid_cap(int cap);
+
+void launch_picard_begin(const DevView& v, cudaStream_t s);
+void launch_save_usav(const DevView& v, cudaStream_t s);
+void launch_assemble(const DevView& v, cudaStream_t s);
+void launch_mv(int mode, const DevView& v, cudaStream_t s);
+void launch_std_update(bool check, const DevView& v, cudaStream_t s);
+void launch_cg_first_update(const DevView& v, cudaStream_t s);
+void launch_cg_update(bool check, const DevView& v, cudaStream_t s);
+void launch_picard_check(const DevView& v, cudaStream_t s);
+void launch_mixed_setup(const DevView& v, cudaStream_t s);
+void launch_refine_resid(const DevView& v, cudaStream_t s);
+void launch_inner(const DevView& v, cudaStream_t s);
+void launch_refine_update(const DevView& v, cudaStream_t s);
+void launch_matvec_plain(const DevView& v, const double2* x, double2* y, cudaStream_t s);
+void launch_dinv(const DevView& v, int precond, cudaStream_t s);
+void launch_bb(const DevView& v, cudaStream_t s);
+
+}  // namespace bp

@@ -1,0 +1,371 @@
+// bp_plan.cpp -- compile reference-layout inputs into the compact device form.
+#include "bp_plan.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+namespace bp {
+
+namespace {
+
+inline size_t vtx(int i, int j, int nx) { return (size_t)(j - 1) * (nx - 1) + (i - 1); }
+inline size_t cel(int i, int j, int nx) { return (size_t)(j - 1) * nx + (i - 1); }
+
+int round_up(int a, int b) { return (a + b - 1) / b * b; }
+
+// Column ids of the owned active vertices of one instance.
+struct ColumnMap {
+  int nx, ny, periodic;
+  std::vector<int> id;  // (nx-1)*(ny-1), -1 where not an owned active vertex
+  int lookup(int i, int j) const {
+    int ii = vertex_image(i, nx, periodic), jj = vertex_image(j, ny, periodic);
+    if (ii < 0 || jj < 0) return -1;
+    return id[vtx(ii, jj, nx)];
+  }
+};
+
+void add_columns(int nx, int ny, int nz, int periodic, const int* active_vertex,
+                 int inst_index, HostPlan* p, ColumnMap* cm,
+                 std::vector<std::pair<int, int>>* cols_ij) {
+  OwnedRange R = owned_range(nx, ny, periodic);
+  cm->nx = nx; cm->ny = ny; cm->periodic = periodic;
+  cm->id.assign((size_t)(nx - 1) * (ny - 1), -1);
+  for (int j = R.jlo; j <= R.jhi; ++j)
+    for (int i = R.ilo; i <= R.ihi; ++i)
+      if (active_vertex[vtx(i, j, nx)]) {
+        cm->id[vtx(i, j, nx)] = p->ncols + (int)cols_ij->size();
+        cols_ij->push_back({i, j});
+      }
+  (void)nz;
+  (void)inst_index;
+}
+
+void add_tiles(HostPlan* p, int b, int node_begin, int node_end) {
+  p->inst[b].tile_begin = (int)p->tile_start.size();
+  for (int s = node_begin; s < node_end; s += kTile) {
+    p->tile_start.push_back(s);
+    p->tile_inst.push_back(b);
+  }
+  p->inst[b].tile_end = (int)p->tile_start.size();
+}
+
+}  // namespace
+
+OwnedRange owned_range(int nx, int ny, int periodic) {
+  OwnedRange r;
+  r.ilo = periodic ? 3 : 2;
+  r.jlo = periodic ? 3 : 2;
+  r.ihi = nx - 2;
+  r.jhi = ny - 2;
+  return r;
+}
+
+int vertex_image(int i, int n, int periodic) {
+  const int V = n - 1;
+  if (periodic) {
+    const int P = n - 4;  // owned vertices per row
+    if (i < 1 || i > V) return -1;
+    int t = ((i - 3) % P + P) % P;
+    return t + 3;
+  }
+  return (i >= 2 && i <= n - 2) ? i : -1;
+}
+
+bool build_column_plan(int nx, int ny, int nz, int periodic,
+                       const int* active_vertex, HostPlan* p,
+                       std::string* err) {
+  if (nx < 6 || ny < 6 || nz < 2 || nz > kNzMax) {
+    *err = "grid too small or nz out of range";
+    return false;
+  }
+  *p = HostPlan();
+  p->nz = nz;
+  p->ninst = 1;
+  p->inst.resize(1);
+  std::memset(&p->inst[0], 0, sizeof(InstParams));
+  p->nx = {nx}; p->ny = {ny}; p->periodic = {periodic};
+  ColumnMap cm;
+  std::vector<std::pair<int, int>> cols;
+  add_columns(nx, ny, nz, periodic, active_vertex, 0, p, &cm, &cols);
+  const int nc = (int)cols.size();
+  p->ncols = nc;
+  p->nnodes = nc * nz;
+  p->npad = round_up(std::max(p->nnodes, 1), 64);
+  p->col_inst.assign(nc, 0);
+  p->col_ij.resize(2 * (size_t)nc);
+  p->col_nbr.resize(9 * (size_t)nc);
+  p->col_cells.assign(4 * (size_t)nc, -1);
+  p->col_beta.assign(nc, 0.0);
+  for (int c = 0; c < nc; ++c) {
+    int i = cols[c].first, j = cols[c].second;
+    p->col_ij[c] = i;
+    p->col_ij[nc + c] = j;
+    for (int jA = -1; jA <= 1; ++jA)
+      for (int iA = -1; iA <= 1; ++iA)
+        p->col_nbr[(size_t)((jA + 1) * 3 + (iA + 1)) * nc + c] = cm.lookup(i + iA, j + jA);
+  }
+  InstParams& ip = p->inst[0];
+  ip.col_begin = 0; ip.col_end = nc;
+  ip.node_begin = 0; ip.node_end = nc * nz;
+  add_tiles(p, 0, 0, nc * nz);
+  p->ntiles = (int)p->tile_start.size();
+  p->load.assign(p->nnodes, double2{0.0, 0.0});
+  p->dmask.assign(p->nnodes, 0);
+  return true;
+}
+
+bool build_plan(const bp_inputs* in, int n, HostPlan* p, std::string* err) {
+  if (n < 1 || !in) { *err = "no instances"; return false; }
+  *p = HostPlan();
+  const int nz = in[0].nz;
+  if (nz < 2 || nz > kNzMax) { *err = "nz out of range (2..64)"; return false; }
+  p->nz = nz;
+  p->ninst = n;
+  p->inst.resize(n);
+  std::vector<std::vector<std::pair<int, int>>> cols(n);
+  std::vector<ColumnMap> cms(n);
+  std::vector<std::vector<std::pair<int, int>>> cells(n);
+  // pass 1: columns and cells of every instance
+  for (int b = 0; b < n; ++b) {
+    const bp_inputs& I = in[b];
+    if (I.nz != nz) { *err = "all instances of a batch must share nz"; return false; }
+    if (I.nhalo != 2) { *err = "nhalo must be 2"; return false; }
+    if (I.nx < 6 || I.ny < 6) { *err = "grid too small"; return false; }
+    if (I.pcg_variant != in[0].pcg_variant || I.pcg_ncheck != in[0].pcg_ncheck ||
+        I.precision != in[0].precision) {
+      *err = "all instances of a batch must share pcg_variant, pcg_ncheck and precision";
+      return false;
+    }
+    if (!I.stagusrf || !I.stagthck || !I.flwafact || !I.active_cell || !I.active_vertex ||
+        !I.loadu || !I.loadv || !I.umask_dirichlet || !I.vmask_dirichlet || !I.sigma ||
+        !I.beta_internal) {
+      *err = "missing input array";
+      return false;
+    }
+    p->nx.push_back(I.nx); p->ny.push_back(I.ny); p->periodic.push_back(I.periodic);
+    add_columns(I.nx, I.ny, nz, I.periodic, I.active_vertex, b, p, &cms[b], &cols[b]);
+    p->ncols += (int)cols[b].size();
+  }
+  // global columns
+  const int NC = p->ncols;
+  p->nnodes = NC * nz;
+  p->npad = round_up(std::max(p->nnodes, 1), 64);
+  p->col_inst.resize(NC);
+  p->col_ij.resize(2 * (size_t)NC);
+  p->col_nbr.resize(9 * (size_t)NC);
+  p->col_cells.assign(4 * (size_t)NC, -1);
+  p->col_beta.resize(NC);
+  p->load.resize(p->nnodes);
+  p->dmask.resize(p->nnodes);
+  // cells: count first (cell ids must be global)
+  std::vector<std::vector<int>> cellid(n);
+  for (int b = 0; b < n; ++b) {
+    const bp_inputs& I = in[b];
+    const int nx = I.nx, ny = I.ny, nh = I.nhalo;
+    cellid[b].assign((size_t)nx * ny, -1);
+    for (int j = nh + 1; j <= ny - nh + 1; ++j)
+      for (int i = nh + 1; i <= nx - nh + 1; ++i)
+        if (I.active_cell[cel(i, j, nx)]) {
+          cellid[b][cel(i, j, nx)] = p->ncells + (int)cells[b].size();
+          cells[b].push_back({i, j});
+        }
+    p->ncells += (int)cells[b].size();
+  }
+  const int NCELL = p->ncells;
+  p->nelem = NCELL * (nz - 1);
+  p->cell_inst.resize(NCELL);
+  p->cell_ij.resize(2 * (size_t)NCELL);
+  p->cell_cols.resize(4 * (size_t)NCELL);
+  p->cell_s.resize(4 * (size_t)NCELL);
+  p->cell_h.resize(4 * (size_t)NCELL);
+  p->cell_beta.resize(4 * (size_t)NCELL);
+  p->flwafact.resize((size_t)NCELL * (nz - 1));
+  int col_base = 0, cell_base = 0;
+  for (int b = 0; b < n; ++b) {
+    const bp_inputs& I = in[b];
+    const int nx = I.nx, ny = I.ny;
+    InstParams& ip = p->inst[b];
+    std::memset(&ip, 0, sizeof(ip));
+    ip.dx = I.dx; ip.dy = I.dy;
+    ip.efvs_constant = I.efvs_constant;
+    ip.pcg_tol = I.pcg_tol;
+    ip.inner_tol = I.inner_tol > 0.0 ? I.inner_tol : 1.0e-4;
+    for (int k = 0; k < nz; ++k) ip.sigma[k] = I.sigma[k];
+    ip.which_efvs = I.which_efvs;
+    ip.which_babc = I.which_babc;
+    ip.which_assemble_beta = I.which_assemble_beta;
+    ip.which_resid = I.which_resid;
+    ip.precond = I.which_precond;
+    ip.variant = I.pcg_variant;
+    ip.precision = I.precision;
+    ip.pcg_maxiters = I.pcg_maxiters;
+    ip.ncheck = I.pcg_ncheck > 0 ? I.pcg_ncheck : 5;
+    ip.maxiter_nonlinear = I.maxiter_nonlinear;
+    const int nc = (int)cols[b].size();
+    ip.col_begin = col_base; ip.col_end = col_base + nc;
+    ip.node_begin = col_base * nz; ip.node_end = (col_base + nc) * nz;
+    const int ncl = (int)cells[b].size();
+    ip.cell_begin = cell_base; ip.cell_end = cell_base + ncl;
+    ip.elem_begin = cell_base * (nz - 1); ip.elem_end = (cell_base + ncl) * (nz - 1);
+    for (int c = 0; c < nc; ++c) {
+      const int g = col_base + c;
+      const int i = cols[b][c].first, j = cols[b][c].second;
+      p->col_inst[g] = b;
+      p->col_ij[g] = i;
+      p->col_ij[NC + g] = j;
+      for (int jA = -1; jA <= 1; ++jA)
+        for (int iA = -1; iA <= 1; ++iA)
+          p->col_nbr[(size_t)((jA + 1) * 3 + (iA + 1)) * NC + g] = cms[b].lookup(i + iA, j + jA);
+      // cells (i,j), (i+1,j), (i,j+1), (i+1,j+1): the reference's element order
+      const int ci[4] = {i, i + 1, i, i + 1}, cj[4] = {j, j, j + 1, j + 1};
+      for (int q = 0; q < 4; ++q) {
+        int id = -1;
+        if (ci[q] >= 1 && ci[q] <= nx && cj[q] >= 1 && cj[q] <= ny)
+          id = cellid[b][cel(ci[q], cj[q], nx)];
+        p->col_cells[(size_t)q * NC + g] = id;
+      }
+      p->col_beta[g] = I.beta_internal[vtx(i, j, nx)];
+      for (int k = 0; k < nz; ++k) {
+        const size_t src = vtx(i, j, nx) * nz + k;
+        p->load[(size_t)g * nz + k] = double2{I.loadu[src], I.loadv[src]};
+        p->dmask[(size_t)g * nz + k] =
+            (uint8_t)((I.umask_dirichlet[src] == 1 ? 1 : 0) | (I.vmask_dirichlet[src] == 1 ? 2 : 0));
+      }
+    }
+    for (int c = 0; c < ncl; ++c) {
+      const int g = cell_base + c;
+      const int ic = cells[b][c].first, jc = cells[b][c].second;
+      p->cell_inst[g] = b;
+      p->cell_ij[g] = ic;
+      p->cell_ij[NCELL + g] = jc;
+      const int vi[4] = {ic - 1, ic, ic, ic - 1}, vj[4] = {jc - 1, jc - 1, jc, jc};
+      for (int q = 0; q < 4; ++q) {
+        const size_t v = vtx(vi[q], vj[q], nx);
+        p->cell_cols[(size_t)q * NCELL + g] = cms[b].lookup(vi[q], vj[q]);
+        p->cell_s[(size_t)q * NCELL + g] = I.stagusrf[v];
+        p->cell_h[(size_t)q * NCELL + g] = I.stagthck[v];
+        p->cell_beta[(size_t)q * NCELL + g] = I.beta_internal[v];
+      }
+      for (int k = 0; k < nz - 1; ++k)
+        p->flwafact[(size_t)g * (nz - 1) + k] = I.flwafact[cel(ic, jc, nx) * (nz - 1) + k];
+    }
+    add_tiles(p, b, ip.node_begin, ip.node_end);
+    col_base += nc;
+    cell_base += ncl;
+  }
+  p->ntiles = (int)p->tile_start.size();
+  return true;
+}
+
+void gather_velocity(const HostPlan& p, int b, const double* uvel,
+                     const double* vvel, double2* x) {
+  const InstParams& ip = p.inst[b];
+  const int nx = p.nx[b], nz = p.nz, NC = p.ncols;
+  for (int g = ip.col_begin; g < ip.col_end; ++g) {
+    const int i = p.col_ij[g], j = p.col_ij[NC + g];
+    for (int k = 0; k < nz; ++k) {
+      const size_t src = vtx(i, j, nx) * nz + k;
+      x[(size_t)g * nz + k] = double2{uvel[src], vvel[src]};
+    }
+  }
+}
+
+void scatter_vector(const HostPlan& p, int b, const double2* x, double* vu,
+                    double* vv) {
+  const InstParams& ip = p.inst[b];
+  const int nx = p.nx[b], nz = p.nz, NC = p.ncols;
+  for (int g = ip.col_begin; g < ip.col_end; ++g) {
+    const int i = p.col_ij[g], j = p.col_ij[NC + g];
+    for (int k = 0; k < nz; ++k) {
+      const size_t dst = vtx(i, j, nx) * nz + k;
+      const double2 v = x[(size_t)g * nz + k];
+      if (vu) vu[dst] = v.x;
+      if (vv) vv[dst] = v.y;
+    }
+  }
+}
+
+void scatter_velocity(const HostPlan& p, int b, const double2* x,
+                      double* uvel, double* vvel) {
+  scatter_vector(p, b, x, uvel, vvel);
+  halo_stag(p.nx[b], p.ny[b], p.nz, p.periodic[b], uvel);
+  halo_stag(p.nx[b], p.ny[b], p.nz, p.periodic[b], vvel);
+}
+
+void scatter_efvs(const HostPlan& p, int b, const double* efvs_elem,
+                  double* efvs) {
+  const InstParams& ip = p.inst[b];
+  const int nx = p.nx[b], ny = p.ny[b], nz = p.nz, NCELL = p.ncells;
+  std::memset(efvs, 0, sizeof(double) * (size_t)(nz - 1) * nx * ny);
+  for (int g = ip.cell_begin; g < ip.cell_end; ++g) {
+    const int ic = p.cell_ij[g], jc = p.cell_ij[NCELL + g];
+    for (int k = 0; k < nz - 1; ++k)
+      efvs[cel(ic, jc, nx) * (nz - 1) + k] = efvs_elem[(size_t)g * (nz - 1) + k];
+  }
+}
+
+void gather_matrix(const HostPlan& p, const double* Auu, const double* Auv,
+                   const double* Avu, const double* Avv, double2* A) {
+  const int nx = p.nx[0], nz = p.nz, NC = p.ncols, np = p.npad;
+  std::memset((void*)A, 0, sizeof(double2) * 2 * 27 * (size_t)np);
+  for (int g = 0; g < NC; ++g) {
+    const int i = p.col_ij[g], j = p.col_ij[NC + g];
+    for (int k = 0; k < nz; ++k) {
+      const size_t n = (size_t)g * nz + k;
+      const size_t base = (vtx(i, j, nx) * nz + k) * 27;
+      for (int m = 0; m < 27; ++m) {
+        A[(size_t)m * np + n] = double2{Auu[base + m], Auv[base + m]};
+        A[(size_t)(27 + m) * np + n] = double2{Avu[base + m], Avv[base + m]};
+      }
+    }
+  }
+}
+
+void scatter_matrix(const HostPlan& p, const double2* A, double* Auu,
+                    double* Auv, double* Avu, double* Avv) {
+  const int nx = p.nx[0], ny = p.ny[0], nz = p.nz, NC = p.ncols, np = p.npad;
+  const size_t tot = (size_t)27 * nz * (nx - 1) * (ny - 1);
+  for (double* a : {Auu, Auv, Avu, Avv})
+    if (a) std::memset(a, 0, sizeof(double) * tot);
+  for (int g = 0; g < NC; ++g) {
+    const int i = p.col_ij[g], j = p.col_ij[NC + g];
+    for (int k = 0; k < nz; ++k) {
+      const size_t n = (size_t)g * nz + k;
+      const size_t base = (vtx(i, j, nx) * nz + k) * 27;
+      for (int m = 0; m < 27; ++m) {
+        const double2 u = A[(size_t)m * np + n], v = A[(size_t)(27 + m) * np + n];
+        if (Auu) Auu[base + m] = u.x;
+        if (Auv) Auv[base + m] = u.y;
+        if (Avu) Avu[base + m] = v.x;
+        if (Avv) Avv[base + m] = v.y;
+      }
+    }
+  }
+}
+
+void halo_stag(int nx, int ny, int nlead, int periodic, double* a) {
+  const int V = nx - 1, W = ny - 1;
+  auto at = [&](int l, int i, int j) -> double& {
+    return a[((size_t)(j - 1) * V + (i - 1)) * nlead + l];
+  };
+  if (!periodic) {
+    for (int j = 1; j <= W; ++j)
+      for (int l = 0; l < nlead; ++l) { at(l, 1, j) = 0.0; at(l, V, j) = 0.0; }
+    for (int i = 1; i <= V; ++i)
+      for (int l = 0; l < nlead; ++l) { at(l, i, 1) = 0.0; at(l, i, W) = 0.0; }
+    return;
+  }
+  for (int j = 3; j <= W - 1; ++j)
+    for (int l = 0; l < nlead; ++l) {
+      const double w = at(l, 3, j), e1 = at(l, V - 2, j), e2 = at(l, V - 1, j);
+      at(l, V, j) = w; at(l, 1, j) = e1; at(l, 2, j) = e2;
+    }
+  for (int i = 1; i <= V; ++i)
+    for (int l = 0; l < nlead; ++l) {
+      const double s = at(l, i, 3), n1 = at(l, i, W - 2), n2 = at(l, i, W - 1);
+      at(l, i, W) = s; at(l, i, 1) = n1; at(l, i, 2) = n2;
+    }
+}
+
+}  // namespace bp

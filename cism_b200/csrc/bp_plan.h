@@ -1,0 +1,68 @@
+// bp_plan.h -- host-side compilation of reference-layout inputs into the
+// compact column/element form used by the device kernels (pure C++, no CUDA).
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "bp_b200.h"
+#include "bp_common.h"
+
+namespace bp {
+
+// Locally owned vertex range of the serial build (parallel_slap.F90:655-673),
+// 1-based Fortran indices into the (nx-1, ny-1) vertex grid.
+struct OwnedRange {
+  int ilo, ihi, jlo, jhi;
+};
+OwnedRange owned_range(int nx, int ny, int periodic);
+
+// Owned image of a halo'd vertex index (1-based) or -1 when the vertex lies
+// outside the global domain (outflow).  Periodic: the staggered halo update
+// copies vertex V-2 -> 1, V-1 -> 2 and 3 -> V (V = n-1 vertices).
+int vertex_image(int i, int n, int periodic);
+
+struct HostPlan {
+  int nz = 0, ninst = 0;
+  int ncols = 0, nnodes = 0, npad = 0, ncells = 0, nelem = 0, ntiles = 0;
+  std::vector<InstParams> inst;
+  std::vector<int> col_inst, col_nbr, col_cells, col_ij;
+  std::vector<double> col_beta;
+  std::vector<double2> load;
+  std::vector<uint8_t> dmask;
+  std::vector<int> cell_inst, cell_ij, cell_cols;
+  std::vector<double> cell_s, cell_h, cell_beta, flwafact;
+  std::vector<int> tile_start, tile_inst;
+  // per-instance grid sizes, for scatters
+  std::vector<int> nx, ny, periodic;
+};
+
+// Columns only (matrix-level entry points): fills columns, neighbours and
+// tiles of one instance; cells are left empty.
+bool build_column_plan(int nx, int ny, int nz, int periodic,
+                       const int* active_vertex, HostPlan* plan,
+                       std::string* err);
+
+// Full plan for n solves.
+bool build_plan(const bp_inputs* in, int n, HostPlan* plan, std::string* err);
+
+// velocity (nz,nx-1,ny-1) of instance b <-> node vector
+void gather_velocity(const HostPlan& p, int b, const double* uvel,
+                     const double* vvel, double2* x);
+void scatter_velocity(const HostPlan& p, int b, const double2* x,
+                      double* uvel, double* vvel);
+// element-averaged viscosity -> efvs (nz-1,nx,ny), zero elsewhere
+void scatter_efvs(const HostPlan& p, int b, const double* efvs_elem,
+                  double* efvs);
+// matrix blocks (27,nz,nx-1,ny-1) -> device layout [2][27][npad] of (u,v) pairs
+void gather_matrix(const HostPlan& p, const double* Auu, const double* Auv,
+                   const double* Avu, const double* Avv, double2* A);
+void scatter_matrix(const HostPlan& p, const double2* A, double* Auu,
+                    double* Auv, double* Avu, double* Avv);
+void scatter_vector(const HostPlan& p, int b, const double2* v, double* vu,
+                    double* vv);
+
+// staggered_parallel_halo for an (nlead, nx-1, ny-1) field.
+void halo_stag(int nx, int ny, int nlead, int periodic, double* a);
+
+}  // namespace bp

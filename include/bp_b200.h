@@ -1,0 +1,193 @@
+/*
+ * bp_b200.h -- C ABI of the B200 Blatter-Pattyn velocity solver.
+ *
+ * Drop-in replacement for the body of CISM's Picard loop in
+ * glissade_velo_higher_solve (libglissade/glissade_velo_higher.F90:2206-3727)
+ * and for its native PCG solvers (libglissade/glissade_velo_higher_pcg.F90),
+ * selected on the Fortran side by a new which_ho_sparse value (5).
+ *
+ * Conventions
+ *  - Every array is in the reference's Fortran column-major layout on the
+ *    local grid with a 2-cell halo (nhalo = 2): cell fields (nx,ny), vertex
+ *    fields (nx-1,ny-1), 3-D velocity fields (nz,nx-1,ny-1), matrix blocks
+ *    (27,nz,nx-1,ny-1) with the stencil index fastest (indxA_3d: iA fastest,
+ *    then jA, then kA; diagonal = 14 in 1-based numbering).
+ *  - Units are the solver's internal ones: m, m/a, Pa a, Pa^-3 a^-1; the
+ *    matrix is scaled by vol0 = 1e9 m^3 as in the reference.
+ *  - Integer masks are 0/1 ints.  Host arrays are owned by the caller and
+ *    only read/written during the call.
+ *  - All entry points return a bp_status code (0 = success).  Codes 3 and 4
+ *    are warnings: the output is valid but not converged, as the reference
+ *    continues after the same conditions (glissade_velo_higher_pcg.F90:542-547,
+ *    glissade_velo_higher.F90:3731-3745).
+ *  - Calls on one context are serialised by the caller (no re-entrancy);
+ *    distinct contexts may be used from distinct threads.
+ */
+#ifndef BP_B200_H
+#define BP_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BP_ABI_VERSION 1
+
+typedef struct bp_ctx bp_ctx;
+
+typedef enum {
+  BP_OK = 0,
+  BP_ERR_NAN = 1,              /* alpha/eta NaN, glissade_velo_higher_pcg.F90:397-399, 460-463 */
+  BP_ERR_SINGULAR_JAC = 2,     /* glissade_velo_higher.F90:6458-6473 */
+  BP_WARN_PCG_NOT_CONVERGED = 3,
+  BP_WARN_PICARD_NOT_CONVERGED = 4,
+  BP_ZERO_MATRIX = 5,          /* all-zero matrix: velocity zeroed, :3191-3220 */
+  BP_ERR_CUDA = 6,
+  BP_ERR_BUDGET = 7,           /* device iteration budget exhausted */
+  BP_ERR_BAD_BETA = 9,         /* glissade_basal_traction.F90:567-579 */
+  BP_ERR_ARGS = 10,
+  BP_ERR_NO_DEVICE = 11
+} bp_status;
+
+typedef enum { BP_FP64 = 0, BP_MIXED = 1 } bp_precision;
+
+/* Boundary inputs of one solve: what the setup part of
+ * glissade_velo_higher_solve (:987-2199) has computed when the Picard loop
+ * starts (:2206).  beta_internal is the calcbeta result (velocity-independent
+ * sliding laws: constant or external beta). */
+typedef struct {
+  int nx, ny, nz, nhalo;        /* local grid incl. halo; nhalo must be 2 */
+  int periodic;                 /* 1: periodic global BC (serial default), 0: outflow */
+  double dx, dy;                /* m */
+  const double *sigma;          /* nz */
+  const double *stagusrf;       /* (nx-1,ny-1) m */
+  const double *stagthck;       /* (nx-1,ny-1) m */
+  const double *beta_internal;  /* (nx-1,ny-1) Pa a/m */
+  const double *flwafact;       /* (nz-1,nx,ny) 0.5*A^(-1/n), :1919-1939 */
+  const int *active_cell;       /* (nx,ny), get_vertex_geometry :4163-4313 */
+  const int *active_vertex;     /* (nx-1,ny-1) */
+  const double *loadu, *loadv;  /* (nz,nx-1,ny-1) load vector, :2024-2111 */
+  const int *umask_dirichlet;   /* (nz,nx-1,ny-1), :1270-1324 */
+  const int *vmask_dirichlet;   /* (nz,nx-1,ny-1) */
+  /* options (values of libglide/glide_types.F90:198-263) */
+  int which_babc;               /* 6 = no-slip (no basal term); else basal term from beta */
+  int which_efvs;               /* 0 constant, 1 flow factor, 2 nonlinear */
+  double efvs_constant;         /* Pa a */
+  int which_assemble_beta;      /* 0 standard (2x2 face quadrature), 1 local */
+  int which_resid;              /* 0..4, :3716-3725 */
+  int pcg_variant;              /* 2 standard PCG, 3 Chronopoulos-Gear */
+  int which_precond;            /* 0 none, 1 diagonal, 2 SIA column */
+  int maxiter_nonlinear;        /* Picard cap, default 100 */
+  int pcg_maxiters;             /* reference: 200 */
+  int pcg_ncheck;               /* reference: 5 */
+  double pcg_tol;               /* reference: 1e-8 */
+  int precision;                /* bp_precision */
+  double inner_tol;             /* BP_MIXED: relative tolerance of each FP32 inner solve */
+} bp_inputs;
+
+typedef struct {
+  int status;
+  int picard_iters;
+  int pcg_iters_total;          /* inner iterations for BP_MIXED */
+  int pcg_iters_last;
+  int refine_steps_total;       /* BP_MIXED outer refinement steps */
+  int converged;                /* Picard converged */
+  double pcg_err_last;          /* |b-Ax|/|b| of the last linear solve */
+  double resid_velo;            /* last Picard velocity criterion */
+  double L2_norm, L2_norm_relative; /* |Ax-b| before the last linear solve */
+  float ms_upload, ms_assemble, ms_pcg, ms_total;
+} bp_stats;
+
+/* Context: one CUDA device, one stream, persistent device buffers. */
+int bp_create(int device, bp_ctx **ctx);
+int bp_destroy(bp_ctx *ctx);
+const char *bp_last_error(const bp_ctx *ctx);
+int bp_abi_version(void);
+
+/* Whole Picard loop of glissade_velo_higher_solve on the device
+ * (replaces :2206-3727 when which_ho_sparse = 5).  uvel/vvel are the
+ * initial guess on input and the solution on output (nz,nx-1,ny-1); efvs
+ * (nz-1,nx,ny) receives the element-averaged viscosity (:5167-5172).  Any
+ * of efvs/stats may be NULL. */
+int bp_solve(bp_ctx *ctx, const bp_inputs *in, double *uvel, double *vvel,
+             double *efvs, bp_stats *stats);
+
+/* n independent solves in one set of launches (uneven grid sizes allowed,
+ * common nz, pcg_variant and pcg_ncheck).  Arrays of n pointers. */
+int bp_batch_solve(bp_ctx *ctx, int n, const bp_inputs *in,
+                   double *const *uvel, double *const *vvel,
+                   double *const *efvs, bp_stats *stats);
+
+/* Linear solve only, on an assembled system (drop-in for the calls of
+ * pcg_solver_standard_3d / pcg_solver_chrongear_3d at
+ * glissade_velo_higher.F90:3329-3356).  variant 2 = standard, 3 =
+ * Chronopoulos-Gear; precond 0/1/2.  xu/xv: initial guess in, solution out. */
+int bp_pcg(bp_ctx *ctx, int nx, int ny, int nz, int periodic,
+           const int *active_vertex, const double *Auu, const double *Auv,
+           const double *Avu, const double *Avv, const double *bu,
+           const double *bv, double *xu, double *xv, int precond, int variant,
+           double tol, int maxiters, int ncheck, int precision,
+           double *err, int *niters);
+
+/* y = A x on owned active rows (matvec_multiply_structured_3d,
+ * glissade_velo_higher_pcg.F90:2533-2647); other rows of y are zero. */
+int bp_matvec(bp_ctx *ctx, int nx, int ny, int nz, int periodic,
+              const int *active_vertex, const double *Auu, const double *Auv,
+              const double *Avu, const double *Avv, const double *xu,
+              const double *xv, double *yu, double *yv);
+
+/* One assembled system at velocity (uvel, vvel): assembly, basal BC and
+ * Dirichlet BC (:3003-3119).  Rows of owned active vertices are filled;
+ * all other rows are zero.  Any output may be NULL. */
+int bp_assemble(bp_ctx *ctx, const bp_inputs *in, const double *uvel,
+                const double *vvel, double *Auu, double *Auv, double *Avu,
+                double *Avv, double *bu, double *bv, double *efvs);
+
+/* ------------------------------------------------------------------
+ * Host-side mirror of the setup part of glissade_velo_higher_solve, for
+ * callers that hold the model fields rather than the boundary inputs.
+ * ------------------------------------------------------------------ */
+typedef struct {
+  int nx, ny, nz, nhalo, periodic;
+  double dx, dy;
+  const double *thck, *usrf, *topg;   /* (nx,ny) halo-filled, m */
+  const double *flwa;                 /* (nz-1,nx,ny) Pa^-3 a^-1 */
+  const double *beta_external;        /* (nx-1,ny-1) Pa a/m */
+  const int *kinbcmask;               /* (nx-1,ny-1) or NULL */
+  double eus, thklim, max_slope, thck_gradient_ramp;
+  double rhoi, rhoo, grav;
+  double beta_const, beta_grounded_min, efvs_constant;
+  int which_babc, which_efvs, which_resid, which_sparse, which_precond;
+  int which_gradient, which_gradient_margin;
+  int which_assemble_beta, which_assemble_taud, which_ground;
+  int maxiter_nonlinear, pcg_maxiters, pcg_ncheck;
+  double pcg_tol;
+  int precision;
+  double inner_tol;
+} bp_model;
+
+/* Caller-allocated outputs of the setup (sizes as in bp_inputs). */
+typedef struct {
+  double *sigma;                   /* nz */
+  double *stagusrf, *stagthck;     /* (nx-1,ny-1) */
+  double *beta_internal;           /* (nx-1,ny-1) */
+  double *flwafact;                /* (nz-1,nx,ny) */
+  int *active_cell;                /* (nx,ny) */
+  int *active_vertex;              /* (nx-1,ny-1) */
+  double *loadu, *loadv;           /* (nz,nx-1,ny-1) */
+  int *umask_dirichlet, *vmask_dirichlet; /* (nz,nx-1,ny-1) */
+} bp_setup_arrays;
+
+/* Masks, staggering, surface gradient, vertex geometry, flow factor, load
+ * vector and calcbeta (:1270-2199, :2502-2517); zeroes uvel/vvel at owned
+ * inactive vertices (:1700-1711).  Fills *in to point at the arrays. */
+int bp_setup(const bp_model *m, bp_setup_arrays *out, double *uvel,
+             double *vvel, bp_inputs *in);
+
+/* bp_setup followed by bp_solve. */
+int bp_velo_higher_solve(bp_ctx *ctx, const bp_model *m, double *uvel,
+                         double *vvel, double *efvs, bp_stats *stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

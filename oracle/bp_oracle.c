@@ -1,0 +1,1366 @@
+/*
+ * bp_oracle.c -- CPU restatement of CISM's Blatter-Pattyn velocity solve.
+ *
+ * TEST INFRASTRUCTURE ONLY: the checker for the B200 solver, never part of
+ * the product path.  Only tests/, __graft_entry__.smoke() and bench.py's
+ * CPU-baseline leg may load this library.
+ *
+ * Each function cites the reference routine it restates (paths relative to
+ * the CISM source tree).  Loop order, constants, units (m, m/a, Pa a) and
+ * the vol0 = 1e9 matrix scaling follow the Fortran, so results agree with
+ * the reference to floating-point roundoff.  Arrays use the reference's
+ * column-major layout with a 2-cell halo; indices below are 1-based.
+ *
+ * Parity pinning: the reference ships no golden vectors and its Fortran
+ * cannot be compiled here (no Fortran compiler).  The oracle is pinned by
+ * the reference's own invariants, the analytic first-order slab solution of
+ * tests/slab/plotSlab.py:143-157 and standard-vs-Chronopoulos-Gear
+ * agreement (tests/test_oracle.py).
+ */
+#include "bp_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define IC(i, j) (((size_t)(j) - 1) * (size_t)nx + ((size_t)(i) - 1))
+#define IV(i, j) (((size_t)(j) - 1) * (size_t)(nx - 1) + ((size_t)(i) - 1))
+#define IX(k, i, j) (IV(i, j) * (size_t)nz + ((size_t)(k) - 1))
+#define IFL(k, i, j) (IC(i, j) * (size_t)(nz - 1) + ((size_t)(k) - 1))
+#define IA(m, k, i, j) (IX(k, i, j) * 27 + ((size_t)(m) - 1))
+
+/* indxA_3d(iA,jA,kA): iA fastest, diagonal = 14
+ * (glissade_velo_higher.F90:599-619). */
+static int indxA(int iA, int jA, int kA) {
+  return 1 + (iA + 1) + 3 * (jA + 1) + 9 * (kA + 1);
+}
+
+/* ---------------------------------------------------------------------
+ * Finite-element tables, glissade_velo_higher_init
+ * (glissade_velo_higher.F90:270-650).
+ * ------------------------------------------------------------------- */
+static double xqp[8], yqp[8], zqp[8], wqp[8];
+static double phi3[8][8], dxr3[8][8], dyr3[8][8], dzr3[8][8]; /* [n][p] */
+static double xqp2[4], yqp2[4], wqp2[4];
+static double phi2[4][4], dxr2[4][4], dyr2[4][4];
+static int ishift[8][8], jshift[8][8], kshift[8][8];
+static int tables_ready = 0;
+
+static void init_tables(void) {
+  if (tables_ready) return;
+  const double r = 1.0 / sqrt(3.0);
+  const double sx[8] = {-1, 1, 1, -1, -1, 1, 1, -1};
+  const double sy[8] = {-1, -1, 1, 1, -1, -1, 1, 1};
+  const double sz[8] = {-1, -1, -1, -1, 1, 1, 1, 1};
+  for (int p = 0; p < 8; ++p) {
+    xqp[p] = sx[p] * r; yqp[p] = sy[p] * r; zqp[p] = sz[p] * r; wqp[p] = 1.0;
+  }
+  for (int p = 0; p < 8; ++p) {
+    double x = xqp[p], y = yqp[p], z = zqp[p];
+    for (int n = 0; n < 8; ++n) {
+      double ax = sx[n], ay = sy[n], az = sz[n];
+      phi3[n][p] = (1.0 + ax * x) * (1.0 + ay * y) * (1.0 + az * z) / 8.0;
+      dxr3[n][p] = ax * (1.0 + ay * y) * (1.0 + az * z) / 8.0;
+      dyr3[n][p] = ay * (1.0 + ax * x) * (1.0 + az * z) / 8.0;
+      dzr3[n][p] = az * (1.0 + ax * x) * (1.0 + ay * y) / 8.0;
+    }
+  }
+  const double s2x[4] = {-1, 1, 1, -1}, s2y[4] = {-1, -1, 1, 1};
+  for (int p = 0; p < 4; ++p) {
+    xqp2[p] = s2x[p] * r; yqp2[p] = s2y[p] * r; wqp2[p] = 1.0;
+  }
+  for (int p = 0; p < 4; ++p)
+    for (int n = 0; n < 4; ++n) {
+      phi2[n][p] = (1.0 + s2x[n] * xqp2[p]) * (1.0 + s2y[n] * yqp2[p]) / 4.0;
+      dxr2[n][p] = s2x[n] * (1.0 + s2y[n] * yqp2[p]) / 4.0;
+      dyr2[n][p] = s2y[n] * (1.0 + s2x[n] * xqp2[p]) / 4.0;
+    }
+  /* ishift/jshift/kshift, glissade_velo_higher.F90:453-486 */
+  const int i1[8] = {0, 1, 1, 0, 0, 1, 1, 0};
+  const int i2[8] = {-1, 0, 0, -1, -1, 0, 0, -1};
+  const int j1[8] = {0, 0, 1, 1, 0, 0, 1, 1};
+  const int j3[8] = {-1, -1, 0, 0, -1, -1, 0, 0};
+  const int k1[8] = {0, 0, 0, 0, -1, -1, -1, -1};
+  const int k5[8] = {1, 1, 1, 1, 0, 0, 0, 0};
+  const int irow[8] = {0, 1, 1, 0, 0, 1, 1, 0}; /* 0 -> i1, 1 -> i2 */
+  const int jrow[8] = {0, 0, 1, 1, 0, 0, 1, 1}; /* 0 -> j1, 1 -> j3 */
+  const int krow[8] = {0, 0, 0, 0, 1, 1, 1, 1}; /* 0 -> k1, 1 -> k5 */
+  for (int n = 0; n < 8; ++n)
+    for (int c = 0; c < 8; ++c) {
+      ishift[n][c] = irow[n] ? i2[c] : i1[c];
+      jshift[n][c] = jrow[n] ? j3[c] : j1[c];
+      kshift[n][c] = krow[n] ? k5[c] : k1[c];
+    }
+  tables_ready = 1;
+}
+
+/* Glide sigma, glide_setup.F90:281-290 and 375-382 (which_sigma = 0). */
+void orc_sigma_glide(int nz, double *sigma, double *stagwbndsigma) {
+  for (int up = 1; up <= nz; ++up) {
+    double level = (double)(up - 1) / (double)(nz - 1);
+    sigma[up - 1] = (1.0 - pow(level + 1.0, -2.0)) / (1.0 - pow(2.0, -2.0));
+  }
+  if (stagwbndsigma) {
+    stagwbndsigma[0] = 0.0;
+    for (int k = 1; k <= nz - 1; ++k)
+      stagwbndsigma[k] = (sigma[k - 1] + sigma[k]) / 2.0;
+    stagwbndsigma[nz] = 1.0;
+  }
+}
+
+/* ---------------------------------------------------------------------
+ * Halo updates: parallel_slap.F90 parallel_halo_real8_2d (:1790-1860) and
+ * staggered_parallel_halo_real8_3d/_4d (:2807-2925).  lhalo = uhalo = 2
+ * for cells; staggered_lhalo = 2, staggered_uhalo = 1.
+ * ------------------------------------------------------------------- */
+void orc_halo_cell_real(int nx, int ny, int periodic, double *a,
+                        double offset_ew, double offset_ns) {
+  if (!periodic) {
+    for (int j = 3; j <= ny - 2; ++j) {
+      a[IC(1, j)] = a[IC(2, j)] = 0.0;
+      a[IC(nx - 1, j)] = a[IC(nx, j)] = 0.0;
+    }
+    for (int i = 1; i <= nx; ++i) {
+      a[IC(i, 1)] = a[IC(i, 2)] = 0.0;
+      a[IC(i, ny - 1)] = a[IC(i, ny)] = 0.0;
+    }
+    return;
+  }
+  for (int j = 3; j <= ny - 2; ++j) {
+    double e1 = a[IC(nx - 3, j)], e2 = a[IC(nx - 2, j)];
+    double w1 = a[IC(3, j)], w2 = a[IC(4, j)];
+    a[IC(1, j)] = e1 + offset_ew; a[IC(2, j)] = e2 + offset_ew;
+    a[IC(nx - 1, j)] = w1 - offset_ew; a[IC(nx, j)] = w2 - offset_ew;
+  }
+  for (int i = 1; i <= nx; ++i) {
+    double n1 = a[IC(i, ny - 3)], n2 = a[IC(i, ny - 2)];
+    double s1 = a[IC(i, 3)], s2 = a[IC(i, 4)];
+    a[IC(i, 1)] = n1 + offset_ns; a[IC(i, 2)] = n2 + offset_ns;
+    a[IC(i, ny - 1)] = s1 - offset_ns; a[IC(i, ny)] = s2 - offset_ns;
+  }
+}
+
+static void halo_cell_int(int nx, int ny, int periodic, int *a) {
+  if (!periodic) {
+    for (int j = 3; j <= ny - 2; ++j) {
+      a[IC(1, j)] = a[IC(2, j)] = 0;
+      a[IC(nx - 1, j)] = a[IC(nx, j)] = 0;
+    }
+    for (int i = 1; i <= nx; ++i) {
+      a[IC(i, 1)] = a[IC(i, 2)] = 0;
+      a[IC(i, ny - 1)] = a[IC(i, ny)] = 0;
+    }
+    return;
+  }
+  for (int j = 3; j <= ny - 2; ++j) {
+    int e1 = a[IC(nx - 3, j)], e2 = a[IC(nx - 2, j)];
+    int w1 = a[IC(3, j)], w2 = a[IC(4, j)];
+    a[IC(1, j)] = e1; a[IC(2, j)] = e2;
+    a[IC(nx - 1, j)] = w1; a[IC(nx, j)] = w2;
+  }
+  for (int i = 1; i <= nx; ++i) {
+    int n1 = a[IC(i, ny - 3)], n2 = a[IC(i, ny - 2)];
+    int s1 = a[IC(i, 3)], s2 = a[IC(i, 4)];
+    a[IC(i, 1)] = n1; a[IC(i, 2)] = n2;
+    a[IC(i, ny - 1)] = s1; a[IC(i, ny)] = s2;
+  }
+}
+
+/* a has leading dimension nlead and trailing (nx-1, ny-1). */
+void orc_halo_stag(int nx, int ny, int nlead, int periodic, double *a) {
+  const int V = nx - 1, W = ny - 1;
+#define AS(l, i, j) a[(((size_t)(j) - 1) * (size_t)V + ((size_t)(i) - 1)) * (size_t)nlead + (size_t)(l)]
+  if (!periodic) {
+    for (int j = 1; j <= W; ++j)
+      for (int l = 0; l < nlead; ++l) { AS(l, 1, j) = 0.0; AS(l, V, j) = 0.0; }
+    for (int i = 1; i <= V; ++i)
+      for (int l = 0; l < nlead; ++l) { AS(l, i, 1) = 0.0; AS(l, i, W) = 0.0; }
+    return;
+  }
+  for (int j = 3; j <= W - 1; ++j)
+    for (int l = 0; l < nlead; ++l) {
+      double wcp = AS(l, 3, j);
+      double e1 = AS(l, V - 2, j), e2 = AS(l, V - 1, j);
+      AS(l, V, j) = wcp;
+      AS(l, 1, j) = e1;
+      AS(l, 2, j) = e2;
+    }
+  for (int i = 1; i <= V; ++i)
+    for (int l = 0; l < nlead; ++l) {
+      double scp = AS(l, i, 3);
+      double n1 = AS(l, i, W - 2), n2 = AS(l, i, W - 1);
+      AS(l, i, W) = scp;
+      AS(l, i, 1) = n1;
+      AS(l, i, 2) = n2;
+    }
+#undef AS
+}
+
+/* Locally owned vertex range, parallel_slap.F90:655-673. */
+static void owned_range(int nx, int ny, int periodic, int *ilo, int *ihi,
+                        int *jlo, int *jhi) {
+  *ilo = periodic ? 3 : 2;
+  *jlo = periodic ? 3 : 2;
+  *ihi = nx - 2;
+  *jhi = ny - 2;
+}
+
+/* ---------------------------------------------------------------------
+ * glissade_get_masks (glissade_masks.F90:55-457) with the default
+ * which_ho_calving_front = NO_SUBGRID, so active_ice_mask = ice_mask and
+ * calving_front_mask = 0.
+ * ------------------------------------------------------------------- */
+void orc_get_masks(int nx, int ny, int periodic, const double *thck,
+                   const double *topg, double eus, double thklim,
+                   double rhoi, double rhoo, int *ice_mask,
+                   int *floating_mask, int *ocean_mask, int *land_mask,
+                   int *active_ice_mask) {
+  for (int j = 1; j <= ny; ++j)
+    for (int i = 1; i <= nx; ++i) {
+      size_t c = IC(i, j);
+      ice_mask[c] = thck[c] > thklim ? 1 : 0;
+      ocean_mask[c] = (topg[c] < eus && ice_mask[c] == 0) ? 1 : 0;
+      floating_mask[c] =
+          (topg[c] - eus < (-rhoi / rhoo) * thck[c] && ice_mask[c] == 1) ? 1 : 0;
+      land_mask[c] = topg[c] >= eus ? 1 : 0;
+      active_ice_mask[c] = ice_mask[c];
+    }
+  halo_cell_int(nx, ny, periodic, ice_mask);
+  halo_cell_int(nx, ny, periodic, floating_mask);
+  halo_cell_int(nx, ny, periodic, active_ice_mask);
+}
+
+/* glissade_stagger (glissade_grid_operators.F90:60-148). */
+void orc_stagger(int nx, int ny, const double *var, double *stagvar,
+                 const int *mask, int stagger_margin) {
+  for (int j = 1; j <= ny - 1; ++j)
+    for (int i = 1; i <= nx - 1; ++i) {
+      size_t v = IV(i, j);
+      stagvar[v] = 0.0;
+      if (stagger_margin == 0) {
+        stagvar[v] = (var[IC(i, j + 1)] + var[IC(i + 1, j + 1)] +
+                      var[IC(i, j)] + var[IC(i + 1, j)]) / 4.0;
+      } else {
+        double sumvar = mask[IC(i, j + 1)] * var[IC(i, j + 1)] +
+                        mask[IC(i + 1, j + 1)] * var[IC(i + 1, j + 1)] +
+                        mask[IC(i, j)] * var[IC(i, j)] +
+                        mask[IC(i + 1, j)] * var[IC(i + 1, j)];
+        double summask = (double)(mask[IC(i, j + 1)] + mask[IC(i + 1, j + 1)] +
+                                  mask[IC(i, j)] + mask[IC(i + 1, j)]);
+        if (summask > 0.0) stagvar[v] = sumvar / summask;
+      }
+    }
+}
+
+/* Fortran MIN/MAX on a NaN operand: the finite operand is returned (IEEE
+ * minNum/maxNum), which fmin/fmax implement. */
+static double edge_ramp(double thck_upper, double thklim, double ramp) {
+  double f = fmin(1.0, (thck_upper - thklim) / ramp);
+  return fmax(f, 0.0);
+}
+
+/* glissade_surface_elevation_gradient (glissade_grid_operators.F90:734-1168),
+ * centered gradient (which_ho_gradient = 0). */
+void orc_surface_gradient(int nx, int ny, int periodic, double dx, double dy,
+                          const int *active_ice_mask, const int *land_mask,
+                          const double *usrf, const double *thck,
+                          double thklim, double thck_gradient_ramp,
+                          int ho_gradient, int ho_gradient_margin,
+                          double max_slope, double *ds_dx, double *ds_dy) {
+  (void)ho_gradient;
+  double *ex = calloc((size_t)nx * ny, sizeof(double));
+  double *ey = calloc((size_t)nx * ny, sizeof(double));
+  if (ho_gradient_margin == ORC_GRADIENT_MARGIN_LAND) {
+    for (int j = 1; j <= ny; ++j)
+      for (int i = 1; i <= nx - 1; ++i)
+        ex[IC(i, j)] = (usrf[IC(i + 1, j)] - usrf[IC(i, j)]) / dx;
+    for (int j = 1; j <= ny - 1; ++j)
+      for (int i = 1; i <= nx; ++i)
+        ey[IC(i, j)] = (usrf[IC(i, j + 1)] - usrf[IC(i, j)]) / dy;
+  } else if (ho_gradient_margin == ORC_GRADIENT_MARGIN_MARINE) {
+    for (int j = 1; j <= ny; ++j)
+      for (int i = 1; i <= nx - 1; ++i)
+        if (active_ice_mask[IC(i, j)] == 1 && active_ice_mask[IC(i + 1, j)] == 1)
+          ex[IC(i, j)] = (usrf[IC(i + 1, j)] - usrf[IC(i, j)]) / dx;
+    for (int j = 1; j <= ny - 1; ++j)
+      for (int i = 1; i <= nx; ++i)
+        if (active_ice_mask[IC(i, j)] == 1 && active_ice_mask[IC(i, j + 1)] == 1)
+          ey[IC(i, j)] = (usrf[IC(i, j + 1)] - usrf[IC(i, j)]) / dy;
+  } else { /* HYBRID */
+    for (int j = 1; j <= ny; ++j)
+      for (int i = 1; i <= nx - 1; ++i) {
+        int iu, il; double sgn;
+        if (usrf[IC(i, j)] > usrf[IC(i + 1, j)]) { iu = i; il = i + 1; sgn = -1.0; }
+        else { iu = i + 1; il = i; sgn = 1.0; }
+        double ef = 1.0;
+        if (land_mask[IC(iu, j)] == 1)
+          ef = edge_ramp(thck[IC(iu, j)], thklim, thck_gradient_ramp);
+        if (active_ice_mask[IC(iu, j)] == 1 && active_ice_mask[IC(il, j)] == 1)
+          ex[IC(i, j)] = ef * sgn * (usrf[IC(iu, j)] - usrf[IC(il, j)]) / dx;
+        else if (active_ice_mask[IC(iu, j)] == 1 && land_mask[IC(il, j)] == 1)
+          ex[IC(i, j)] = ef * sgn * (usrf[IC(iu, j)] - usrf[IC(il, j)]) / dx;
+      }
+    for (int j = 1; j <= ny - 1; ++j)
+      for (int i = 1; i <= nx; ++i) {
+        int ju, jl; double sgn;
+        if (usrf[IC(i, j)] > usrf[IC(i, j + 1)]) { ju = j; jl = j + 1; sgn = -1.0; }
+        else { ju = j + 1; jl = j; sgn = 1.0; }
+        double ef = 1.0;
+        if (land_mask[IC(i, ju)] == 1)
+          ef = edge_ramp(thck[IC(i, ju)], thklim, thck_gradient_ramp);
+        if (active_ice_mask[IC(i, ju)] == 1 && active_ice_mask[IC(i, jl)] == 1)
+          ey[IC(i, j)] = ef * sgn * (usrf[IC(i, ju)] - usrf[IC(i, jl)]) / dy;
+        else if (active_ice_mask[IC(i, ju)] == 1 && land_mask[IC(i, jl)] == 1)
+          ey[IC(i, j)] = ef * sgn * (usrf[IC(i, ju)] - usrf[IC(i, jl)]) / dy;
+      }
+  }
+  for (int j = 1; j <= ny - 1; ++j)
+    for (int i = 1; i <= nx - 1; ++i) {
+      ds_dx[IV(i, j)] = 0.5 * (ex[IC(i, j)] + ex[IC(i, j + 1)]);
+      ds_dy[IV(i, j)] = 0.5 * (ey[IC(i, j)] + ey[IC(i + 1, j)]);
+    }
+  for (int j = 1; j <= ny - 1; ++j)
+    for (int i = 1; i <= nx - 1; ++i) {
+      size_t v = IV(i, j);
+      ds_dx[v] = ds_dx[v] > 0.0 ? fmin(ds_dx[v], max_slope) : fmax(ds_dx[v], -max_slope);
+      ds_dy[v] = ds_dy[v] > 0.0 ? fmin(ds_dy[v], max_slope) : fmax(ds_dy[v], -max_slope);
+    }
+  orc_halo_stag(nx, ny, 1, periodic, ds_dx);
+  orc_halo_stag(nx, ny, 1, periodic, ds_dy);
+  free(ex);
+  free(ey);
+}
+
+/* glissade_grounded_fraction (glissade_grounding_line.F90:55-178).  The
+ * vmask test reads land_mask(i+1,j+1) twice and never land_mask(i+1,j)
+ * (:117); restated verbatim. */
+void orc_grounded_fraction(int nx, int ny, const int *ice_mask,
+                           const int *floating_mask, const int *land_mask,
+                           int whichground, double *f_ground) {
+  for (int j = 1; j <= ny - 1; ++j)
+    for (int i = 1; i <= nx - 1; ++i) {
+      int vm = ice_mask[IC(i, j + 1)] == 1 || ice_mask[IC(i + 1, j + 1)] == 1 ||
+               ice_mask[IC(i, j)] == 1 || ice_mask[IC(i + 1, j)] == 1 ||
+               land_mask[IC(i, j + 1)] == 1 || land_mask[IC(i + 1, j + 1)] == 1 ||
+               land_mask[IC(i, j)] == 1 || land_mask[IC(i + 1, j + 1)] == 1;
+      size_t v = IV(i, j);
+      f_ground[v] = 0.0;
+      if (!vm) continue;
+      if (whichground == ORC_GROUND_ALL) { f_ground[v] = 1.0; continue; }
+#define CG(a, b) ((ice_mask[IC(a, b)] == 1 && floating_mask[IC(a, b)] == 0) || land_mask[IC(a, b)] == 1)
+      if (CG(i, j + 1) || CG(i + 1, j + 1) || CG(i, j) || CG(i + 1, j))
+        f_ground[v] = 1.0;
+#undef CG
+    }
+}
+
+/* ---------------------------------------------------------------------
+ * get_basis_function_derivatives_3d (glissade_velo_higher.F90:6360-6579)
+ * ------------------------------------------------------------------- */
+static int basis_derivs_3d(const double *x, const double *y, const double *z,
+                           int p, double *dx, double *dy, double *dz,
+                           double *detJ) {
+  double J[3][3] = {{0}};
+  for (int n = 0; n < 8; ++n) {
+    J[0][0] = J[0][0] + dxr3[n][p] * x[n];
+    J[0][1] = J[0][1] + dxr3[n][p] * y[n];
+    J[0][2] = J[0][2] + dxr3[n][p] * z[n];
+    J[1][0] = J[1][0] + dyr3[n][p] * x[n];
+    J[1][1] = J[1][1] + dyr3[n][p] * y[n];
+    J[1][2] = J[1][2] + dyr3[n][p] * z[n];
+    J[2][0] = J[2][0] + dzr3[n][p] * x[n];
+    J[2][1] = J[2][1] + dzr3[n][p] * y[n];
+    J[2][2] = J[2][2] + dzr3[n][p] * z[n];
+  }
+  double cf[3][3];
+  cf[0][0] = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+  cf[0][1] = -(J[1][0] * J[2][2] - J[1][2] * J[2][0]);
+  cf[0][2] = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+  cf[1][0] = -(J[0][1] * J[2][2] - J[0][2] * J[2][1]);
+  cf[1][1] = J[0][0] * J[2][2] - J[0][2] * J[2][0];
+  cf[1][2] = -(J[0][0] * J[2][1] - J[0][1] * J[2][0]);
+  cf[2][0] = J[0][1] * J[1][2] - J[0][2] * J[1][1];
+  cf[2][1] = -(J[0][0] * J[1][2] - J[0][2] * J[1][0]);
+  cf[2][2] = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+  double d = J[0][0] * cf[0][0] + J[0][1] * cf[0][1] + J[0][2] * cf[0][2];
+  *detJ = d;
+  if (!(fabs(d) > 0.0)) return ORC_ERR_SINGULAR_JAC;
+  double Ji[3][3];
+  for (int col = 0; col < 3; ++col)
+    for (int row = 0; row < 3; ++row) Ji[row][col] = cf[col][row] / d;
+  for (int n = 0; n < 8; ++n) {
+    dx[n] = Ji[0][0] * dxr3[n][p] + Ji[0][1] * dyr3[n][p] + Ji[0][2] * dzr3[n][p];
+    dy[n] = Ji[1][0] * dxr3[n][p] + Ji[1][1] * dyr3[n][p] + Ji[1][2] * dzr3[n][p];
+    dz[n] = Ji[2][0] * dxr3[n][p] + Ji[2][1] * dyr3[n][p] + Ji[2][2] * dzr3[n][p];
+  }
+  return ORC_OK;
+}
+
+/* get_basis_function_derivatives_2d (:6583-6751), detJ only is used. */
+static int basis_detJ_2d(const double *x, const double *y, int p,
+                         double *detJ) {
+  double J11 = 0, J12 = 0, J21 = 0, J22 = 0;
+  for (int n = 0; n < 4; ++n) {
+    J11 = J11 + dxr2[n][p] * x[n];
+    J12 = J12 + dxr2[n][p] * y[n];
+    J21 = J21 + dyr2[n][p] * x[n];
+    J22 = J22 + dyr2[n][p] * y[n];
+  }
+  *detJ = J11 * J22 - J12 * J21;
+  return fabs(*detJ) > 0.0 ? ORC_OK : ORC_ERR_SINGULAR_JAC;
+}
+
+/* compute_effective_viscosity, BP branch (:7199-7378). */
+static double effective_viscosity(int whichefvs, double efvs_constant,
+                                  const double *dx, const double *dy,
+                                  const double *dz, const double *u,
+                                  const double *v, double flwafact) {
+  const double effstrain_min = 1.0e-8;
+  const double p_effstr = (1.0 - 3.0) / 3.0;
+  const double p2_effstr = p_effstr / 2.0;
+  if (whichefvs == ORC_EFVS_CONSTANT) return efvs_constant;
+  if (whichefvs == ORC_EFVS_FLOWFACT) {
+    const double scyr = 31536000.0;
+    double effstrain = (500.0 / scyr) / 200.0e3 * scyr;
+    return flwafact * pow(effstrain, p_effstr);
+  }
+  double ux = 0, uy = 0, uz = 0, vx = 0, vy = 0, vz = 0;
+  for (int n = 0; n < 8; ++n) {
+    ux = ux + dx[n] * u[n];
+    uy = uy + dy[n] * u[n];
+    uz = uz + dz[n] * u[n];
+    vx = vx + dx[n] * v[n];
+    vy = vy + dy[n] * v[n];
+    vz = vz + dz[n] * v[n];
+  }
+  double sq = effstrain_min * effstrain_min +
+              (ux * ux + vy * vy + ux * vy + 0.25 * ((vx + uy) * (vx + uy))) +
+              0.25 * (uz * uz + vz * vz);
+  return flwafact * pow(sq, p2_effstr);
+}
+
+/* assemble_stiffness_matrix_3d (:4954-5204) with compute_element_matrix
+ * (:7868-7986), check_symmetry_element_matrix (:9468-9529) and
+ * element_to_global_matrix_3d (:7990-8054). */
+int orc_assemble_3d(int nx, int ny, int nz, int nhalo, const double *sigma,
+                    const int *active_cell, const double *xVertex,
+                    const double *yVertex, const double *uvel,
+                    const double *vvel, const double *stagusrf,
+                    const double *stagthck, const double *flwafact,
+                    int whichefvs, double efvs_constant, double *efvs,
+                    double *Auu, double *Auv, double *Avu, double *Avv) {
+  init_tables();
+  const double vol0 = 1.0e9;
+  size_t nA = (size_t)27 * nz * (nx - 1) * (ny - 1);
+  memset(Auu, 0, nA * sizeof(double));
+  memset(Auv, 0, nA * sizeof(double));
+  memset(Avu, 0, nA * sizeof(double));
+  memset(Avv, 0, nA * sizeof(double));
+  memset(efvs, 0, (size_t)(nz - 1) * nx * ny * sizeof(double));
+  for (int j = nhalo + 1; j <= ny - nhalo + 1; ++j)
+    for (int i = nhalo + 1; i <= nx - nhalo + 1; ++i) {
+      if (!active_cell[IC(i, j)]) continue;
+      for (int k = 1; k <= nz - 1; ++k) {
+        double Kuu[8][8] = {{0}}, Kuv[8][8] = {{0}}, Kvu[8][8] = {{0}},
+               Kvv[8][8] = {{0}};
+        double x[8], y[8], z[8], u[8], v[8];
+        for (int n = 0; n < 8; ++n) {
+          int in = i + ishift[6][n], jn = j + jshift[6][n], kn = k + kshift[6][n];
+          x[n] = xVertex[IV(in, jn)];
+          y[n] = yVertex[IV(in, jn)];
+          z[n] = stagusrf[IV(in, jn)] - sigma[kn - 1] * stagthck[IV(in, jn)];
+          u[n] = uvel[IX(kn, in, jn)];
+          v[n] = vvel[IX(kn, in, jn)];
+        }
+        double efvs_qp[8];
+        for (int p = 0; p < 8; ++p) {
+          double ddx[8], ddy[8], ddz[8], detJ;
+          if (basis_derivs_3d(x, y, z, p, ddx, ddy, ddz, &detJ) != ORC_OK)
+            return ORC_ERR_SINGULAR_JAC;
+          efvs_qp[p] = effective_viscosity(whichefvs, efvs_constant, ddx, ddy,
+                                           ddz, u, v, flwafact[IFL(k, i, j)]);
+          double f = efvs_qp[p] * wqp[p] * detJ / vol0;
+          for (int nc = 0; nc < 8; ++nc)
+            for (int nr = 0; nr < 8; ++nr) {
+              Kuu[nr][nc] = Kuu[nr][nc] + f * (4.0 * ddx[nr] * ddx[nc] +
+                                               ddy[nr] * ddy[nc] + ddz[nr] * ddz[nc]);
+              Kuv[nr][nc] = Kuv[nr][nc] + f * (2.0 * ddx[nr] * ddy[nc] + ddy[nr] * ddx[nc]);
+              Kvu[nr][nc] = Kvu[nr][nc] + f * (2.0 * ddy[nr] * ddx[nc] + ddx[nr] * ddy[nc]);
+              Kvv[nr][nc] = Kvv[nr][nc] + f * (4.0 * ddy[nr] * ddy[nc] +
+                                               ddx[nr] * ddx[nc] + ddz[nr] * ddz[nc]);
+            }
+        }
+        double e = 0.0;
+        for (int p = 0; p < 8; ++p) e = e + efvs_qp[p];
+        efvs[IFL(k, i, j)] = e / 8.0;
+        /* check_symmetry_element_matrix: eps10 absolute */
+        for (int a = 0; a < 8; ++a)
+          for (int b = 0; b < 8; ++b) {
+            if (fabs(Kuu[a][b] - Kuu[b][a]) > 1.0e-10) return ORC_ERR_ASYMMETRIC_ELEMENT;
+            if (fabs(Kvv[a][b] - Kvv[b][a]) > 1.0e-10) return ORC_ERR_ASYMMETRIC_ELEMENT;
+            if (fabs(Kuv[a][b] - Kvu[b][a]) > 1.0e-10) return ORC_ERR_ASYMMETRIC_ELEMENT;
+          }
+        for (int nr = 0; nr < 8; ++nr) {
+          int ii = i + ishift[6][nr], jj = j + jshift[6][nr], kk = k + kshift[6][nr];
+          for (int nc = 0; nc < 8; ++nc) {
+            int m = indxA(ishift[nr][nc], jshift[nr][nc], kshift[nr][nc]);
+            size_t a = IA(m, kk, ii, jj);
+            Auu[a] = Auu[a] + Kuu[nr][nc];
+            Auv[a] = Auv[a] + Kuv[nr][nc];
+            Avu[a] = Avu[a] + Kvu[nr][nc];
+            Avv[a] = Avv[a] + Kvv[nr][nc];
+          }
+        }
+      }
+    }
+  return ORC_OK;
+}
+
+/* basal_sliding_bc (:8125-8381) applied to the bed layer (k = nz). */
+static void basal_sliding_bc(int nx, int ny, int nz, int nhalo, double dx,
+                             double dy, const int *active_cell,
+                             const int *active_vertex, const double *beta,
+                             const double *xVertex, const double *yVertex,
+                             int whichassemble_beta, double *Auu,
+                             double *Avv) {
+  const double vol0 = 1.0e9;
+  if (whichassemble_beta == ORC_ASSEMBLE_LOCAL) {
+    int m = indxA(0, 0, 0);
+    for (int j = 1; j <= ny - 1; ++j)
+      for (int i = 1; i <= nx - 1; ++i)
+        if (active_vertex[IV(i, j)]) {
+          Auu[IA(m, nz, i, j)] = Auu[IA(m, nz, i, j)] + dx * dy / vol0 * beta[IV(i, j)];
+          Avv[IA(m, nz, i, j)] = Avv[IA(m, nz, i, j)] + dx * dy / vol0 * beta[IV(i, j)];
+        }
+    return;
+  }
+  for (int j = nhalo + 1; j <= ny - nhalo + 1; ++j)
+    for (int i = nhalo + 1; i <= nx - nhalo + 1; ++i) {
+      if (!active_cell[IC(i, j)]) continue;
+      double x[4] = {xVertex[IV(i - 1, j - 1)], xVertex[IV(i, j - 1)],
+                     xVertex[IV(i, j)], xVertex[IV(i - 1, j)]};
+      double y[4] = {yVertex[IV(i - 1, j - 1)], yVertex[IV(i, j - 1)],
+                     yVertex[IV(i, j)], yVertex[IV(i - 1, j)]};
+      double b[4] = {beta[IV(i - 1, j - 1)], beta[IV(i, j - 1)],
+                     beta[IV(i, j)], beta[IV(i - 1, j)]};
+      for (int p = 0; p < 4; ++p) {
+        double detJ;
+        basis_detJ_2d(x, y, p, &detJ);
+        double bq = 0.0;
+        for (int n = 0; n < 4; ++n) bq = bq + phi2[n][p] * b[n];
+        double K[4][4];
+        for (int nc = 0; nc < 4; ++nc)
+          for (int nr = 0; nr < 4; ++nr)
+            K[nr][nc] = 0.0 + bq * wqp2[p] * detJ / vol0 * phi2[nr][p] * phi2[nc][p];
+        for (int nr = 0; nr < 4; ++nr) {
+          int ii = i + ishift[2][nr], jj = j + jshift[2][nr];
+          for (int nc = 0; nc < 4; ++nc) {
+            int m = indxA(ishift[nr][nc], jshift[nr][nc], 0);
+            Auu[IA(m, nz, ii, jj)] = Auu[IA(m, nz, ii, jj)] + K[nr][nc];
+            Avv[IA(m, nz, ii, jj)] = Avv[IA(m, nz, ii, jj)] + K[nr][nc];
+          }
+        }
+      }
+    }
+}
+
+/* dirichlet_boundary_conditions_3d (:8385-8578). */
+static void dirichlet_bc_3d(int nx, int ny, int nz, int nhalo,
+                            const int *active_vertex, const int *umask,
+                            const int *vmask, const double *uvel,
+                            const double *vvel, double *Auu, double *Auv,
+                            double *Avu, double *Avv, double *bu,
+                            double *bv) {
+  for (int j = nhalo; j <= ny - nhalo + 1; ++j)
+    for (int i = nhalo; i <= nx - nhalo + 1; ++i) {
+      if (!active_vertex[IV(i, j)]) continue;
+      for (int k = 1; k <= nz; ++k) {
+        if (umask[IX(k, i, j)] == 1) {
+          bu[IX(k, i, j)] = uvel[IX(k, i, j)];
+          for (int kA = -1; kA <= 1; ++kA)
+            for (int jA = -1; jA <= 1; ++jA)
+              for (int iA = -1; iA <= 1; ++iA) {
+                if (!(k + kA >= 1 && k + kA <= nz && i + iA >= 1 && i + iA <= nx - 1 &&
+                      j + jA >= 1 && j + jA <= ny - 1)) continue;
+                if (iA == 0 && jA == 0 && kA == 0) {
+                  int m = indxA(0, 0, 0);
+                  Auu[IA(m, k, i, j)] = 1.0;
+                  Auv[IA(m, k, i, j)] = 0.0;
+                  Avu[IA(m, k, i, j)] = 0.0;
+                } else {
+                  int m = indxA(iA, jA, kA);
+                  Auu[IA(m, k, i, j)] = 0.0;
+                  Auv[IA(m, k, i, j)] = 0.0;
+                  int mm = indxA(-iA, -jA, -kA);
+                  size_t nb = IX(k + kA, i + iA, j + jA);
+                  size_t an = IA(mm, k + kA, i + iA, j + jA);
+                  if (umask[nb] != 1) {
+                    bu[nb] = bu[nb] - Auu[an] * uvel[IX(k, i, j)];
+                    Auu[an] = 0.0;
+                  }
+                  if (vmask[nb] != 1) {
+                    bv[nb] = bv[nb] - Avu[an] * uvel[IX(k, i, j)];
+                    Avu[an] = 0.0;
+                  }
+                }
+              }
+        }
+        if (vmask[IX(k, i, j)] == 1) {
+          bv[IX(k, i, j)] = vvel[IX(k, i, j)];
+          for (int kA = -1; kA <= 1; ++kA)
+            for (int jA = -1; jA <= 1; ++jA)
+              for (int iA = -1; iA <= 1; ++iA) {
+                if (!(k + kA >= 1 && k + kA <= nz && i + iA >= 1 && i + iA <= nx - 1 &&
+                      j + jA >= 1 && j + jA <= ny - 1)) continue;
+                if (iA == 0 && jA == 0 && kA == 0) {
+                  int m = indxA(0, 0, 0);
+                  Auv[IA(m, k, i, j)] = 0.0;
+                  Avu[IA(m, k, i, j)] = 0.0;
+                  Avv[IA(m, k, i, j)] = 1.0;
+                } else {
+                  int m = indxA(iA, jA, kA);
+                  Avu[IA(m, k, i, j)] = 0.0;
+                  Avv[IA(m, k, i, j)] = 0.0;
+                  int mm = indxA(-iA, -jA, -kA);
+                  size_t nb = IX(k + kA, i + iA, j + jA);
+                  size_t an = IA(mm, k + kA, i + iA, j + jA);
+                  if (umask[nb] != 1) {
+                    bu[nb] = bu[nb] - Auv[an] * vvel[IX(k, i, j)];
+                    Auv[an] = 0.0;
+                  }
+                  if (vmask[nb] != 1) {
+                    bv[nb] = bv[nb] - Avv[an] * vvel[IX(k, i, j)];
+                    Avv[an] = 0.0;
+                  }
+                }
+              }
+        }
+      }
+    }
+}
+
+/* check_symmetry_assembled_matrix_3d (:9533-9741). */
+static void check_symmetry_assembled_3d(int nx, int ny, int nz, int periodic,
+                                        const int *active_vertex, double *Auu,
+                                        double *Auv, double *Avu,
+                                        double *Avv) {
+  int ilo, ihi, jlo, jhi;
+  owned_range(nx, ny, periodic, &ilo, &ihi, &jlo, &jhi);
+  const double eps08 = 1.0e-8;
+  for (int j = jlo; j <= jhi; ++j)
+    for (int i = ilo; i <= ihi; ++i) {
+      if (!active_vertex[IV(i, j)]) continue;
+      for (int k = 1; k <= nz; ++k) {
+        for (int pass = 0; pass < 2; ++pass) {
+          double *D = pass == 0 ? Auu : Avv;   /* block that owns the diag */
+          double *O1 = pass == 0 ? Auv : Avu;  /* off-diagonal block, row */
+          double *O2 = pass == 0 ? Avu : Auv;  /* its transpose partner */
+          double diag = D[IA(indxA(0, 0, 0), k, i, j)];
+          for (int jA = -1; jA <= 1; ++jA)
+            for (int iA = -1; iA <= 1; ++iA)
+              for (int kA = -1; kA <= 1; ++kA) {
+                if (!(k + kA >= 1 && k + kA <= nz)) continue;
+                int m = indxA(iA, jA, kA), mm = indxA(-iA, -jA, -kA);
+                size_t a1 = IA(m, k, i, j), a2 = IA(mm, k + kA, i + iA, j + jA);
+                double v1 = D[a1], v2 = D[a2];
+                if (v2 != v1 && fabs(v2 - v1) < eps08 * fabs(diag)) {
+                  double avg = 0.5 * (v1 + v2);
+                  D[a1] = avg;
+                  D[a2] = avg;
+                }
+                v1 = O1[a1];
+                v2 = O2[a2];
+                if (v2 != v1 && fabs(v2 - v1) < eps08 * fabs(diag)) {
+                  double avg = 0.5 * (v1 + v2);
+                  O1[a1] = avg;
+                  O2[a2] = avg;
+                }
+              }
+        }
+      }
+    }
+}
+
+/* count_nonzeros_3d (:9355-9410). */
+static long count_nonzeros_3d(int nx, int ny, int nz, int periodic,
+                              const int *active_vertex, const double *Auu,
+                              const double *Auv, const double *Avu,
+                              const double *Avv) {
+  int ilo, ihi, jlo, jhi;
+  owned_range(nx, ny, periodic, &ilo, &ihi, &jlo, &jhi);
+  long nnz = 0;
+  for (int j = jlo; j <= jhi; ++j)
+    for (int i = ilo; i <= ihi; ++i) {
+      if (!active_vertex[IV(i, j)]) continue;
+      for (int k = 1; k <= nz; ++k)
+        for (int m = 1; m <= 27; ++m) {
+          size_t a = IA(m, k, i, j);
+          nnz += (Auu[a] != 0.0) + (Auv[a] != 0.0) + (Avu[a] != 0.0) + (Avv[a] != 0.0);
+        }
+    }
+  return nnz;
+}
+
+/* matvec_multiply_structured_3d (glissade_velo_higher_pcg.F90:2533-2647). */
+void orc_matvec_3d(int nx, int ny, int nz, int periodic,
+                   const int *active_vertex, const double *Auu,
+                   const double *Auv, const double *Avu, const double *Avv,
+                   const double *xu, const double *xv, double *yu,
+                   double *yv) {
+  int ilo, ihi, jlo, jhi;
+  owned_range(nx, ny, periodic, &ilo, &ihi, &jlo, &jhi);
+  size_t nv = (size_t)nz * (nx - 1) * (ny - 1);
+  memset(yu, 0, nv * sizeof(double));
+  memset(yv, 0, nv * sizeof(double));
+  for (int j = jlo; j <= jhi; ++j)
+    for (int i = ilo; i <= ihi; ++i) {
+      if (!active_vertex[IV(i, j)]) continue;
+      for (int k = 1; k <= nz; ++k) {
+        double su = 0.0, sv = 0.0;
+        for (int kA = -1; kA <= 1; ++kA)
+          for (int jA = -1; jA <= 1; ++jA)
+            for (int iA = -1; iA <= 1; ++iA) {
+              if (!(k + kA >= 1 && k + kA <= nz && i + iA >= 1 && i + iA <= nx - 1 &&
+                    j + jA >= 1 && j + jA <= ny - 1)) continue;
+              int m = indxA(iA, jA, kA);
+              size_t a = IA(m, k, i, j), x = IX(k + kA, i + iA, j + jA);
+              su = su + Auu[a] * xu[x] + Auv[a] * xv[x];
+              sv = sv + Avu[a] * xu[x] + Avv[a] * xv[x];
+            }
+        yu[IX(k, i, j)] = su;
+        yv[IX(k, i, j)] = sv;
+      }
+    }
+}
+
+/* global_sum_staggered_3d_real8 (:2333-2375): owned vertices only. */
+static double gsum2(int nx, int ny, int nz, int periodic, const double *a1,
+                    const double *b1, const double *a2, const double *b2) {
+  int ilo, ihi, jlo, jhi;
+  owned_range(nx, ny, periodic, &ilo, &ihi, &jlo, &jhi);
+  double s = 0.0;
+  for (int j = jlo; j <= jhi; ++j)
+    for (int i = ilo; i <= ihi; ++i)
+      for (int k = 1; k <= nz; ++k) {
+        size_t x = IX(k, i, j);
+        double w1 = a1[x] * b1[x];
+        double w2 = a2[x] * b2[x];
+        s = s + w1 + w2;
+      }
+  return s;
+}
+
+/* setup_preconditioner_3d (:2150-2265) + diagonal / SIA application. */
+typedef struct {
+  int precond;
+  double *Adiagu, *Adiagv; /* nz,nx-1,ny-1 */
+  double *Muu, *Mvv;       /* (-1:1,nz,nx-1,ny-1) */
+} precond_t;
+
+static void setup_precond(int nx, int ny, int nz, int precond,
+                          const double *Auu, const double *Avv,
+                          precond_t *pc) {
+  size_t nv = (size_t)nz * (nx - 1) * (ny - 1);
+  pc->precond = precond;
+  pc->Adiagu = calloc(nv, sizeof(double));
+  pc->Adiagv = calloc(nv, sizeof(double));
+  pc->Muu = calloc(3 * nv, sizeof(double));
+  pc->Mvv = calloc(3 * nv, sizeof(double));
+  for (size_t x = 0; x < nv; ++x) {
+    if (precond == ORC_PRECOND_DIAG) {
+      pc->Adiagu[x] = Auu[x * 27 + 13];
+      pc->Adiagv[x] = Avv[x * 27 + 13];
+    } else if (precond == ORC_PRECOND_SIA) {
+      for (int d = 0; d < 3; ++d) {
+        int m = indxA(0, 0, d - 1);
+        pc->Muu[x * 3 + d] = Auu[x * 27 + (m - 1)];
+        pc->Mvv[x * 3 + d] = Avv[x * 27 + (m - 1)];
+      }
+    }
+  }
+}
+
+static void free_precond(precond_t *pc) {
+  free(pc->Adiagu); free(pc->Adiagv); free(pc->Muu); free(pc->Mvv);
+}
+
+/* easy_sia_solver + tridiag_solver (:2759-2904). */
+static void easy_sia_solver(int nx, int ny, int nz, const int *active_vertex,
+                            const double *M, const double *b, double *x) {
+  double *gamma = malloc((size_t)nz * sizeof(double));
+  for (int j = 1; j <= ny - 1; ++j)
+    for (int i = 1; i <= nx - 1; ++i) {
+      if (!active_vertex[IV(i, j)]) continue;
+      const double *Mc = M + IX(1, i, j) * 3;
+      const double *r = b + IX(1, i, j);
+      double *s = x + IX(1, i, j);
+      /* sbdiag(k) = M(-1,k), diag = M(0,k), spdiag = M(1,k); ends zeroed */
+      double beta = Mc[1];
+      s[0] = r[0] / beta;
+      for (int k = 2; k <= nz; ++k) {
+        double spd = (k - 1 == nz) ? 0.0 : Mc[(k - 2) * 3 + 2];
+        double sbd = Mc[(k - 1) * 3 + 0];
+        gamma[k - 1] = spd / beta;
+        beta = Mc[(k - 1) * 3 + 1] - sbd * gamma[k - 1];
+        s[k - 1] = (r[k - 1] - sbd * s[k - 2]) / beta;
+      }
+      for (int k = nz - 1; k >= 1; --k) s[k - 1] = s[k - 1] - gamma[k] * s[k];
+    }
+  free(gamma);
+}
+
+static void apply_precond(int nx, int ny, int nz, const precond_t *pc,
+                          const int *active_vertex, const double *ru,
+                          const double *rv, double *zu, double *zv) {
+  size_t nv = (size_t)nz * (nx - 1) * (ny - 1);
+  if (pc->precond == ORC_PRECOND_NONE) {
+    memcpy(zu, ru, nv * sizeof(double));
+    memcpy(zv, rv, nv * sizeof(double));
+  } else if (pc->precond == ORC_PRECOND_DIAG) {
+    for (size_t x = 0; x < nv; ++x) {
+      zu[x] = pc->Adiagu[x] != 0.0 ? ru[x] / pc->Adiagu[x] : 0.0;
+      zv[x] = pc->Adiagv[x] != 0.0 ? rv[x] / pc->Adiagv[x] : 0.0;
+    }
+  } else {
+    easy_sia_solver(nx, ny, nz, active_vertex, pc->Muu, ru, zu);
+    easy_sia_solver(nx, ny, nz, active_vertex, pc->Mvv, rv, zv);
+  }
+}
+
+/* pcg_solver_standard_3d (glissade_velo_higher_pcg.F90:84-549); maxiters,
+ * tolerance and solve_ncheck are parameters here (hard-coded 200, 1e-8, 5
+ * in the reference, :67-77). */
+int orc_pcg_standard_3d(int nx, int ny, int nz, int periodic,
+                        const int *active_vertex, const double *Auu,
+                        const double *Auv, const double *Avu,
+                        const double *Avv, const double *bu, const double *bv,
+                        double *xu, double *xv, int precond, int maxiters,
+                        double tolerance, int ncheck, double *err,
+                        int *niters) {
+  size_t nv = (size_t)nz * (nx - 1) * (ny - 1);
+  double *ru = calloc(nv, 8), *rv = calloc(nv, 8), *du = calloc(nv, 8),
+         *dv = calloc(nv, 8), *qu = calloc(nv, 8), *qv = calloc(nv, 8),
+         *zu = calloc(nv, 8), *zv = calloc(nv, 8);
+  precond_t pc;
+  setup_precond(nx, ny, nz, precond, Auu, Avv, &pc);
+  orc_halo_stag(nx, ny, nz, periodic, xu);
+  orc_halo_stag(nx, ny, nz, periodic, xv);
+  orc_matvec_3d(nx, ny, nz, periodic, active_vertex, Auu, Auv, Avu, Avv, xu, xv, zu, zv);
+  for (size_t x = 0; x < nv; ++x) { ru[x] = bu[x] - zu[x]; rv[x] = bv[x] - zv[x]; }
+  *niters = maxiters;
+  *err = -1.0;
+  double eta0 = 1.0;
+  memset(du, 0, nv * 8); memset(dv, 0, nv * 8);
+  memset(zu, 0, nv * 8); memset(zv, 0, nv * 8);
+  double L2_rhs = sqrt(gsum2(nx, ny, nz, periodic, bu, bu, bv, bv));
+  int status = ORC_WARN_PCG_NOT_CONVERGED;
+  for (int n = 1; n <= maxiters; ++n) {
+    apply_precond(nx, ny, nz, &pc, active_vertex, ru, rv, zu, zv);
+    double eta1 = gsum2(nx, ny, nz, periodic, ru, zu, rv, zv);
+    if (eta1 != eta1) { status = ORC_ERR_NAN; break; }
+    double beta = eta1 / eta0;
+    for (size_t x = 0; x < nv; ++x) { du[x] = zu[x] + beta * du[x]; dv[x] = zv[x] + beta * dv[x]; }
+    orc_halo_stag(nx, ny, nz, periodic, du);
+    orc_halo_stag(nx, ny, nz, periodic, dv);
+    orc_matvec_3d(nx, ny, nz, periodic, active_vertex, Auu, Auv, Avu, Avv, du, dv, qu, qv);
+    eta0 = eta1;
+    double eta2 = gsum2(nx, ny, nz, periodic, du, qu, dv, qv);
+    double alpha = eta1 / eta2;
+    if (alpha != alpha) { status = ORC_ERR_NAN; break; }
+    for (size_t x = 0; x < nv; ++x) {
+      xu[x] = xu[x] + alpha * du[x]; xv[x] = xv[x] + alpha * dv[x];
+      ru[x] = ru[x] - alpha * qu[x]; rv[x] = rv[x] - alpha * qv[x];
+    }
+    if (n % ncheck == 0) {
+      orc_halo_stag(nx, ny, nz, periodic, xu);
+      orc_halo_stag(nx, ny, nz, periodic, xv);
+      orc_matvec_3d(nx, ny, nz, periodic, active_vertex, Auu, Auv, Avu, Avv, xu, xv, zu, zv);
+      for (size_t x = 0; x < nv; ++x) { ru[x] = bu[x] - zu[x]; rv[x] = bv[x] - zv[x]; }
+      double L2_resid = sqrt(gsum2(nx, ny, nz, periodic, ru, ru, rv, rv));
+      *err = L2_resid / L2_rhs;
+      if (*err < tolerance) { *niters = n; status = ORC_OK; break; }
+    }
+  }
+  free_precond(&pc);
+  free(ru); free(rv); free(du); free(dv); free(qu); free(qv); free(zu); free(zv);
+  return status;
+}
+
+/* pcg_solver_chrongear_3d (glissade_velo_higher_pcg.F90:965-1610). */
+int orc_pcg_chrongear_3d(int nx, int ny, int nz, int periodic,
+                         const int *active_vertex, const double *Auu,
+                         const double *Auv, const double *Avu,
+                         const double *Avv, const double *bu,
+                         const double *bv, double *xu, double *xv,
+                         int precond, int maxiters, double tolerance,
+                         int ncheck, double *err, int *niters) {
+  size_t nv = (size_t)nz * (nx - 1) * (ny - 1);
+  double *ru = calloc(nv, 8), *rv = calloc(nv, 8), *du = calloc(nv, 8),
+         *dv = calloc(nv, 8), *zu = calloc(nv, 8), *zv = calloc(nv, 8),
+         *qu = calloc(nv, 8), *qv = calloc(nv, 8), *Azu = calloc(nv, 8),
+         *Azv = calloc(nv, 8);
+  precond_t pc;
+  setup_precond(nx, ny, nz, precond, Auu, Avv, &pc);
+  *niters = maxiters;
+  *err = -1.0;
+  double bb = gsum2(nx, ny, nz, periodic, bu, bu, bv, bv);
+  double L2_rhs = sqrt(bb);
+  orc_halo_stag(nx, ny, nz, periodic, xu);
+  orc_halo_stag(nx, ny, nz, periodic, xv);
+  orc_matvec_3d(nx, ny, nz, periodic, active_vertex, Auu, Auv, Avu, Avv, xu, xv, zu, zv);
+  for (size_t x = 0; x < nv; ++x) { ru[x] = bu[x] - zu[x]; rv[x] = bv[x] - zv[x]; }
+  orc_halo_stag(nx, ny, nz, periodic, ru);
+  orc_halo_stag(nx, ny, nz, periodic, rv);
+  apply_precond(nx, ny, nz, &pc, active_vertex, ru, rv, zu, zv);
+  memcpy(du, zu, nv * 8); memcpy(dv, zv, nv * 8);
+  orc_matvec_3d(nx, ny, nz, periodic, active_vertex, Auu, Auv, Avu, Avv, du, dv, qu, qv);
+  double rho_old = gsum2(nx, ny, nz, periodic, ru, zu, rv, zv);
+  double sigma = gsum2(nx, ny, nz, periodic, du, qu, dv, qv);
+  orc_halo_stag(nx, ny, nz, periodic, qu);
+  orc_halo_stag(nx, ny, nz, periodic, qv);
+  double alpha = rho_old / sigma;
+  int status = ORC_WARN_PCG_NOT_CONVERGED;
+  if (alpha != alpha) status = ORC_ERR_NAN;
+  else {
+    for (size_t x = 0; x < nv; ++x) {
+      xu[x] = xu[x] + alpha * du[x]; xv[x] = xv[x] + alpha * dv[x];
+      ru[x] = ru[x] - alpha * qu[x]; rv[x] = rv[x] - alpha * qv[x];
+    }
+    for (int n = 2; n <= maxiters; ++n) {
+      apply_precond(nx, ny, nz, &pc, active_vertex, ru, rv, zu, zv);
+      orc_matvec_3d(nx, ny, nz, periodic, active_vertex, Auu, Auv, Avu, Avv, zu, zv, Azu, Azv);
+      double rho = gsum2(nx, ny, nz, periodic, ru, zu, rv, zv);
+      double delta = gsum2(nx, ny, nz, periodic, Azu, zu, Azv, zv);
+      orc_halo_stag(nx, ny, nz, periodic, Azu);
+      orc_halo_stag(nx, ny, nz, periodic, Azv);
+      double beta = rho / rho_old;
+      sigma = delta - beta * rho / alpha;
+      alpha = rho / sigma;
+      rho_old = rho;
+      if (alpha != alpha) { status = ORC_ERR_NAN; break; }
+      for (size_t x = 0; x < nv; ++x) {
+        du[x] = zu[x] + beta * du[x]; dv[x] = zv[x] + beta * dv[x];
+        qu[x] = Azu[x] + beta * qu[x]; qv[x] = Azv[x] + beta * qv[x];
+        xu[x] = xu[x] + alpha * du[x]; xv[x] = xv[x] + alpha * dv[x];
+        ru[x] = ru[x] - alpha * qu[x]; rv[x] = rv[x] - alpha * qv[x];
+      }
+      if (n % ncheck == 0) {
+        orc_matvec_3d(nx, ny, nz, periodic, active_vertex, Auu, Auv, Avu, Avv, xu, xv, zu, zv);
+        for (size_t x = 0; x < nv; ++x) { ru[x] = bu[x] - zu[x]; rv[x] = bv[x] - zv[x]; }
+        double rr = gsum2(nx, ny, nz, periodic, ru, ru, rv, rv);
+        *err = sqrt(rr) / L2_rhs;
+        if (*err < tolerance) { *niters = n; status = ORC_OK; break; }
+        orc_halo_stag(nx, ny, nz, periodic, ru);
+        orc_halo_stag(nx, ny, nz, periodic, rv);
+      }
+    }
+  }
+  free_precond(&pc);
+  free(ru); free(rv); free(du); free(dv); free(zu); free(zv); free(qu);
+  free(qv); free(Azu); free(Azv);
+  return status;
+}
+
+/* compute_residual_vector_3d (:8768-8927). */
+static void residual_vector_3d(int nx, int ny, int nz, int periodic,
+                               const int *active_vertex, const double *Auu,
+                               const double *Auv, const double *Avu,
+                               const double *Avv, const double *bu,
+                               const double *bv, const double *uvel,
+                               const double *vvel, double *L2_norm,
+                               double *L2_rel) {
+  int ilo, ihi, jlo, jhi;
+  owned_range(nx, ny, periodic, &ilo, &ihi, &jlo, &jhi);
+  size_t nv = (size_t)nz * (nx - 1) * (ny - 1);
+  double *resu = calloc(nv, 8), *resv = calloc(nv, 8);
+  orc_matvec_3d(nx, ny, nz, periodic, active_vertex, Auu, Auv, Avu, Avv, uvel, vvel, resu, resv);
+  double L2 = 0.0, L2b = 0.0;
+  for (int j = jlo; j <= jhi; ++j)
+    for (int i = ilo; i <= ihi; ++i) {
+      if (!active_vertex[IV(i, j)]) continue;
+      for (int k = 1; k <= nz; ++k) {
+        size_t x = IX(k, i, j);
+        resu[x] = resu[x] - bu[x];
+        resv[x] = resv[x] - bv[x];
+        L2 = L2 + resu[x] * resu[x] + resv[x] * resv[x];
+      }
+    }
+  *L2_norm = sqrt(L2);
+  for (int j = jlo; j <= jhi; ++j)
+    for (int i = ilo; i <= ihi; ++i) {
+      if (!active_vertex[IV(i, j)]) continue;
+      for (int k = 1; k <= nz; ++k) {
+        size_t x = IX(k, i, j);
+        L2b = L2b + bu[x] * bu[x] + bv[x] * bv[x];
+      }
+    }
+  L2b = sqrt(L2b);
+  *L2_rel = L2b > 0.0 ? *L2_norm / L2b : 0.0;
+  free(resu);
+  free(resv);
+}
+
+/* compute_residual_velocity_3d (:9111-9234). */
+static double residual_velocity_3d(int nx, int ny, int nz, int periodic,
+                                   int whichresid, const double *uvel,
+                                   const double *vvel, const double *usav,
+                                   const double *vsav) {
+  int ilo, ihi, jlo, jhi;
+  owned_range(nx, ny, periodic, &ilo, &ihi, &jlo, &jhi);
+  double r = 0.0;
+  long count = 0;
+  int kmax = (whichresid == ORC_RESID_MAXU_NO_UBAS || whichresid == ORC_RESID_MEANU) ? nz - 1 : nz;
+  for (int j = jlo; j <= jhi; ++j)
+    for (int i = ilo; i <= ihi; ++i)
+      for (int k = 1; k <= kmax; ++k) {
+        size_t x = IX(k, i, j);
+        double speed = sqrt(uvel[x] * uvel[x] + vvel[x] * vvel[x]);
+        if (speed != 0.0) {
+          double oldspeed = sqrt(usav[x] * usav[x] + vsav[x] * vsav[x]);
+          double diff = fabs((oldspeed - speed) / speed);
+          if (whichresid == ORC_RESID_MEANU) { r = r + diff; ++count; }
+          else if (diff > r) r = diff;
+        }
+      }
+  if (whichresid == ORC_RESID_MEANU && count > 0) r = r / (double)count;
+  return r;
+}
+
+/* load_vector_gravity (:4317-4532). */
+static void load_vector_gravity(const orc_model *m, const orc_setup *s) {
+  const int nx = m->nx, ny = m->ny, nz = m->nz, nhalo = m->nhalo;
+  const double vol0 = 1.0e9, rhoi = m->rhoi, grav = m->grav;
+  const double dx = m->dx, dy = m->dy;
+  if (m->which_assemble_taud == ORC_ASSEMBLE_LOCAL) {
+    for (int j = 1; j <= ny - 1; ++j)
+      for (int i = 1; i <= nx - 1; ++i) {
+        if (!s->active_vertex[IV(i, j)]) continue;
+        for (int k = 1; k <= nz; ++k) {
+          double dz = s->stagthck[IV(i, j)] * (s->stagwbndsigma[k] - s->stagwbndsigma[k - 1]);
+          s->loadu[IX(k, i, j)] = s->loadu[IX(k, i, j)] - rhoi * grav * dx * dy * dz / vol0 * s->dusrf_dx[IV(i, j)];
+          s->loadv[IX(k, i, j)] = s->loadv[IX(k, i, j)] - rhoi * grav * dx * dy * dz / vol0 * s->dusrf_dy[IV(i, j)];
+        }
+      }
+    return;
+  }
+  for (int j = nhalo + 1; j <= ny - nhalo + 1; ++j)
+    for (int i = nhalo + 1; i <= nx - nhalo + 1; ++i) {
+      if (!s->active_cell[IC(i, j)]) continue;
+      for (int k = 1; k <= nz - 1; ++k) {
+        double x[8], y[8], z[8], dsdx[8], dsdy[8];
+        for (int n = 0; n < 8; ++n) {
+          int in = i + ishift[6][n], jn = j + jshift[6][n], kn = k + kshift[6][n];
+          x[n] = s->xVertex[IV(in, jn)];
+          y[n] = s->yVertex[IV(in, jn)];
+          z[n] = s->stagusrf[IV(in, jn)] - s->sigma[kn - 1] * s->stagthck[IV(in, jn)];
+          dsdx[n] = s->dusrf_dx[IV(in, jn)];
+          dsdy[n] = s->dusrf_dy[IV(in, jn)];
+        }
+        for (int p = 0; p < 8; ++p) {
+          double ddx[8], ddy[8], ddz[8], detJ;
+          basis_derivs_3d(x, y, z, p, ddx, ddy, ddz, &detJ);
+          double sx = 0.0, sy = 0.0;
+          for (int n = 0; n < 8; ++n) { sx = sx + phi3[n][p] * dsdx[n]; sy = sy + phi3[n][p] * dsdy[n]; }
+          for (int n = 0; n < 8; ++n) {
+            int in = i + ishift[6][n], jn = j + jshift[6][n], kn = k + kshift[6][n];
+            s->loadu[IX(kn, in, jn)] = s->loadu[IX(kn, in, jn)] - rhoi * grav * wqp[p] * detJ / vol0 * sx * phi3[n][p];
+            s->loadv[IX(kn, in, jn)] = s->loadv[IX(kn, in, jn)] - rhoi * grav * wqp[p] * detJ / vol0 * sy * phi3[n][p];
+          }
+        }
+      }
+    }
+}
+
+/* lateral_shelf_bc (:4659-4950). face: 0 west, 1 east, 2 south, 3 north. */
+static void lateral_shelf_bc(const orc_model *m, const orc_setup *s, int face,
+                             int iCell, int jCell) {
+  const int nx = m->nx, nz = m->nz;
+  const double vol0 = 1.0e9, rhoi = m->rhoi, rhoo = m->rhoo, grav = m->grav;
+  int iN[4], jN[4], kN[4];
+  double x[4], y[4], sv[4], h[4];
+  if (face == 0) { iN[0] = iCell - 1; jN[0] = jCell; iN[1] = iCell - 1; jN[1] = jCell - 1; }
+  else if (face == 1) { iN[0] = iCell; jN[0] = jCell - 1; iN[1] = iCell; jN[1] = jCell; }
+  else if (face == 2) { iN[0] = iCell - 1; jN[0] = jCell - 1; iN[1] = iCell; jN[1] = jCell - 1; }
+  else { iN[0] = iCell; jN[0] = jCell; iN[1] = iCell - 1; jN[1] = jCell; }
+  const double *coord = (face <= 1) ? s->yVertex : s->xVertex;
+  x[0] = coord[IV(iN[0], jN[0])];
+  x[1] = coord[IV(iN[1], jN[1])];
+  iN[2] = iN[1]; jN[2] = jN[1]; iN[3] = iN[0]; jN[3] = jN[0];
+  x[2] = x[1]; x[3] = x[0];
+  sv[0] = s->stagusrf[IV(iN[0], jN[0])]; sv[1] = s->stagusrf[IV(iN[1], jN[1])];
+  sv[2] = sv[1]; sv[3] = sv[0];
+  h[0] = s->stagthck[IV(iN[0], jN[0])]; h[1] = s->stagthck[IV(iN[1], jN[1])];
+  h[2] = h[1]; h[3] = h[0];
+  for (int k = 1; k <= nz - 1; ++k) {
+    y[0] = sv[0] - s->sigma[k] * h[0];
+    y[1] = sv[1] - s->sigma[k] * h[1];
+    y[2] = sv[2] - s->sigma[k - 1] * h[2];
+    y[3] = sv[3] - s->sigma[k - 1] * h[3];
+    kN[0] = k + 1; kN[1] = k + 1; kN[2] = k; kN[3] = k;
+    for (int p = 0; p < 4; ++p) {
+      double detJ;
+      basis_detJ_2d(x, y, p, &detJ);
+      detJ = fabs(detJ);
+      double hq = 0.0, sq = 0.0;
+      for (int n = 0; n < 4; ++n) { hq = hq + phi2[n][p] * h[n]; sq = sq + phi2[n][p] * sv[n]; }
+      double t = 1.0 - fmin(sq / hq, 1.0);
+      double p_av = 0.5 * rhoi * grav * hq - 0.5 * rhoo * grav * hq * (t * t);
+      for (int n = 0; n < 4; ++n) {
+        size_t xidx = IX(kN[n], iN[n], jN[n]);
+        double f = p_av * wqp2[p] * detJ / vol0 * phi2[n][p];
+        if (face == 0) s->loadu[xidx] = s->loadu[xidx] - f;
+        else if (face == 1) s->loadu[xidx] = s->loadu[xidx] + f;
+        else if (face == 2) s->loadv[xidx] = s->loadv[xidx] - f;
+        else s->loadv[xidx] = s->loadv[xidx] + f;
+      }
+    }
+  }
+}
+
+/* load_vector_lateral_bc (:4536-4655); calving_front_mask = 0. */
+static void load_vector_lateral_bc(const orc_model *m, const orc_setup *s) {
+  const int nx = m->nx, ny = m->ny, nhalo = m->nhalo;
+  for (int j = nhalo + 1; j <= ny - nhalo + 1; ++j)
+    for (int i = nhalo + 1; i <= nx - nhalo + 1; ++i) {
+      if (!s->active_cell[IC(i, j)]) continue;
+      if (s->ocean_mask[IC(i - 1, j)] == 1) lateral_shelf_bc(m, s, 0, i, j);
+      if (s->ocean_mask[IC(i + 1, j)] == 1) lateral_shelf_bc(m, s, 1, i, j);
+      if (s->ocean_mask[IC(i, j - 1)] == 1) lateral_shelf_bc(m, s, 2, i, j);
+      if (s->ocean_mask[IC(i, j + 1)] == 1) lateral_shelf_bc(m, s, 3, i, j);
+    }
+}
+
+/* Setup part of glissade_velo_higher_solve (:1270-2199) plus the masks and
+ * grounded fraction computed by glissade_diagnostic_variable_solve
+ * (glissade.F90:1818-1846). */
+int orc_setup_solve(const orc_model *m, orc_setup *s, double *uvel,
+                    double *vvel) {
+  init_tables();
+  const int nx = m->nx, ny = m->ny, nz = m->nz, nhalo = m->nhalo;
+  if (nhalo != 2 || nx < 6 || ny < 6 || nz < 2) return ORC_ERR_ARGS;
+  size_t nc = (size_t)nx * ny, nvx = (size_t)(nx - 1) * (ny - 1), n3 = nvx * nz;
+  orc_sigma_glide(nz, s->sigma, s->stagwbndsigma);
+  memset(s->umask_dirichlet, 0, n3 * sizeof(int));
+  memset(s->vmask_dirichlet, 0, n3 * sizeof(int));
+  if (m->which_babc == ORC_BABC_NO_SLIP)
+    for (size_t v = 0; v < nvx; ++v) {
+      s->umask_dirichlet[v * nz + (nz - 1)] = 1;
+      s->vmask_dirichlet[v * nz + (nz - 1)] = 1;
+    }
+  if (m->kinbcmask)
+    for (size_t v = 0; v < nvx; ++v)
+      if (m->kinbcmask[v] == 1)
+        for (int k = 0; k < nz; ++k) {
+          s->umask_dirichlet[v * nz + k] = 1;
+          s->vmask_dirichlet[v * nz + k] = 1;
+        }
+  int *active_ice = malloc(nc * sizeof(int));
+  int *ipl = malloc(nc * sizeof(int));
+  orc_get_masks(nx, ny, m->periodic, m->thck, m->topg, m->eus, m->thklim,
+                m->rhoi, m->rhoo, s->ice_mask, s->floating_mask,
+                s->ocean_mask, s->land_mask, active_ice);
+  for (size_t c = 0; c < nc; ++c)
+    ipl[c] = (active_ice[c] == 1 || s->land_mask[c] == 1) ? 1 : 0;
+  orc_stagger(nx, ny, m->thck, s->stagthck, ipl, 1);
+  orc_stagger(nx, ny, m->usrf, s->stagusrf, ipl, 1);
+  orc_surface_gradient(nx, ny, m->periodic, m->dx, m->dy, active_ice,
+                       s->land_mask, m->usrf, m->thck, m->thklim,
+                       m->thck_gradient_ramp, m->which_gradient,
+                       m->which_gradient_margin, m->max_slope, s->dusrf_dx,
+                       s->dusrf_dy);
+  /* get_vertex_geometry (:4163-4313) */
+  for (int j = 1; j <= ny - 1; ++j)
+    for (int i = 1; i <= nx - 1; ++i) {
+      s->xVertex[IV(i, j)] = m->dx * i;
+      s->yVertex[IV(i, j)] = m->dy * j;
+    }
+  memset(s->active_cell, 0, nc * sizeof(int));
+  memset(s->active_vertex, 0, nvx * sizeof(int));
+  for (int j = nhalo + 1; j <= ny - nhalo + 1; ++j)
+    for (int i = nhalo + 1; i <= nx - nhalo + 1; ++i)
+      if (active_ice[IC(i, j)] == 1) s->active_cell[IC(i, j)] = 1;
+  for (int j = nhalo + 1; j <= ny - nhalo + 1; ++j)
+    for (int i = nhalo + 1; i <= nx - nhalo + 1; ++i)
+      if (s->active_cell[IC(i, j)]) {
+        s->active_vertex[IV(i - 1, j - 1)] = 1; s->active_vertex[IV(i, j - 1)] = 1;
+        s->active_vertex[IV(i - 1, j)] = 1; s->active_vertex[IV(i, j)] = 1;
+      }
+  int ilo, ihi, jlo, jhi;
+  owned_range(nx, ny, m->periodic, &ilo, &ihi, &jlo, &jhi);
+  for (int j = jlo; j <= jhi; ++j)
+    for (int i = ilo; i <= ihi; ++i)
+      if (!s->active_vertex[IV(i, j)])
+        for (int k = 1; k <= nz; ++k) { uvel[IX(k, i, j)] = 0.0; vvel[IX(k, i, j)] = 0.0; }
+  /* flwafact (:1919-1939) */
+  memset(s->flwafact, 0, (size_t)(nz - 1) * nc * sizeof(double));
+  for (int j = 1 + nhalo; j <= ny - nhalo + 1; ++j)
+    for (int i = 1 + nhalo; i <= nx - nhalo + 1; ++i)
+      for (int k = 1; k <= nz - 1; ++k)
+        if (m->flwa[IFL(k, i, j)] > 0.0)
+          s->flwafact[IFL(k, i, j)] = 0.5 * pow(m->flwa[IFL(k, i, j)], -1.0 / 3.0);
+  memset(s->loadu, 0, n3 * sizeof(double));
+  memset(s->loadv, 0, n3 * sizeof(double));
+  load_vector_gravity(m, s);
+  load_vector_lateral_bc(m, s);
+  orc_grounded_fraction(nx, ny, s->ice_mask, s->floating_mask, s->land_mask,
+                        m->which_ground, s->f_ground);
+  free(active_ice);
+  free(ipl);
+  return ORC_OK;
+}
+
+/* calcbeta (glissade_basal_traction.F90:67-598), constant and external
+ * laws: beta * f_ground (:540), grounded minimum (:560-566), validity
+ * check (:567-579), halo update. */
+int orc_calcbeta(const orc_model *m, const orc_setup *s,
+                 double *beta_internal) {
+  const int nx = m->nx, ny = m->ny;
+  size_t nvx = (size_t)(nx - 1) * (ny - 1);
+  for (size_t v = 0; v < nvx; ++v) {
+    double b = 0.0;
+    if (m->which_babc == ORC_BABC_BETA_CONSTANT) b = m->beta_const;
+    else if (m->which_babc == ORC_BABC_BETA_EXTERNAL) b = m->beta_external[v];
+    b = b * s->f_ground[v];
+    if (s->f_ground[v] > 0.0 && b < m->beta_grounded_min) b = m->beta_grounded_min;
+    if (!(b >= 0.0)) return ORC_ERR_BAD_BETA;
+    beta_internal[v] = b;
+  }
+  orc_halo_stag(nx, ny, 1, m->periodic, beta_internal);
+  return ORC_OK;
+}
+
+int orc_assemble_system(const orc_model *m, const orc_setup *s,
+                        const double *beta_internal, const double *uvel,
+                        const double *vvel, double *efvs, double *Auu,
+                        double *Auv, double *Avu, double *Avv, double *bu,
+                        double *bv, long *nNonzeros) {
+  const int nx = m->nx, ny = m->ny, nz = m->nz;
+  size_t n3 = (size_t)nz * (nx - 1) * (ny - 1);
+  int st = orc_assemble_3d(nx, ny, nz, m->nhalo, s->sigma, s->active_cell,
+                           s->xVertex, s->yVertex, uvel, vvel, s->stagusrf,
+                           s->stagthck, s->flwafact, m->which_efvs,
+                           m->efvs_constant, efvs, Auu, Auv, Avu, Avv);
+  if (st != ORC_OK) return st;
+  if (m->which_babc != ORC_BABC_NO_SLIP)
+    basal_sliding_bc(nx, ny, nz, m->nhalo, m->dx, m->dy, s->active_cell,
+                     s->active_vertex, beta_internal, s->xVertex, s->yVertex,
+                     m->which_assemble_beta, Auu, Avv);
+  memcpy(bu, s->loadu, n3 * sizeof(double));
+  memcpy(bv, s->loadv, n3 * sizeof(double));
+  dirichlet_bc_3d(nx, ny, nz, m->nhalo, s->active_vertex, s->umask_dirichlet,
+                  s->vmask_dirichlet, uvel, vvel, Auu, Auv, Avu, Avv, bu, bv);
+  orc_halo_stag(nx, ny, 27 * nz, m->periodic, Auu);
+  orc_halo_stag(nx, ny, 27 * nz, m->periodic, Auv);
+  orc_halo_stag(nx, ny, 27 * nz, m->periodic, Avu);
+  orc_halo_stag(nx, ny, 27 * nz, m->periodic, Avv);
+  orc_halo_stag(nx, ny, nz, m->periodic, bu);
+  orc_halo_stag(nx, ny, nz, m->periodic, bv);
+  check_symmetry_assembled_3d(nx, ny, nz, m->periodic, s->active_vertex, Auu,
+                              Auv, Avu, Avv);
+  *nNonzeros = count_nonzeros_3d(nx, ny, nz, m->periodic, s->active_vertex,
+                                 Auu, Auv, Avu, Avv);
+  return ORC_OK;
+}
+
+static void *xalloc(size_t n) { return calloc(n ? n : 1, 1); }
+
+void orc_setup_alloc(const orc_model *m, orc_setup *s) {
+  size_t nx = m->nx, ny = m->ny, nz = m->nz;
+  size_t nc = nx * ny, nvx = (nx - 1) * (ny - 1), n3 = nvx * nz;
+  s->sigma = xalloc(nz * 8); s->stagwbndsigma = xalloc((nz + 1) * 8);
+  s->stagusrf = xalloc(nvx * 8); s->stagthck = xalloc(nvx * 8);
+  s->dusrf_dx = xalloc(nvx * 8); s->dusrf_dy = xalloc(nvx * 8);
+  s->xVertex = xalloc(nvx * 8); s->yVertex = xalloc(nvx * 8);
+  s->f_ground = xalloc(nvx * 8); s->flwafact = xalloc((nz - 1) * nc * 8);
+  s->loadu = xalloc(n3 * 8); s->loadv = xalloc(n3 * 8);
+  s->active_cell = xalloc(nc * 4); s->active_vertex = xalloc(nvx * 4);
+  s->umask_dirichlet = xalloc(n3 * 4); s->vmask_dirichlet = xalloc(n3 * 4);
+  s->ice_mask = xalloc(nc * 4); s->floating_mask = xalloc(nc * 4);
+  s->ocean_mask = xalloc(nc * 4); s->land_mask = xalloc(nc * 4);
+}
+
+void orc_setup_free(orc_setup *s) {
+  free(s->sigma); free(s->stagwbndsigma); free(s->stagusrf); free(s->stagthck);
+  free(s->dusrf_dx); free(s->dusrf_dy); free(s->xVertex); free(s->yVertex);
+  free(s->f_ground); free(s->flwafact); free(s->loadu); free(s->loadv);
+  free(s->active_cell); free(s->active_vertex); free(s->umask_dirichlet);
+  free(s->vmask_dirichlet); free(s->ice_mask); free(s->floating_mask);
+  free(s->ocean_mask); free(s->land_mask);
+}
+
+/* glissade_velo_higher_solve, 3-D Blatter-Pattyn branch with the native
+ * PCG solvers (glissade_velo_higher.F90:654-3986). */
+int orc_velo_higher_solve(const orc_model *m, double *uvel, double *vvel,
+                          double *efvs, double *beta_internal,
+                          orc_stats *stats) {
+  const int nx = m->nx, ny = m->ny, nz = m->nz;
+  size_t n3 = (size_t)nz * (nx - 1) * (ny - 1), nA = n3 * 27;
+  orc_setup s;
+  orc_setup_alloc(m, &s);
+  memset(stats, 0, sizeof(*stats));
+  int st = orc_setup_solve(m, &s, uvel, vvel);
+  if (st != ORC_OK) { orc_setup_free(&s); stats->status = st; return st; }
+  double *Auu = xalloc(nA * 8), *Auv = xalloc(nA * 8), *Avu = xalloc(nA * 8),
+         *Avv = xalloc(nA * 8), *bu = xalloc(n3 * 8), *bv = xalloc(n3 * 8),
+         *usav = xalloc(n3 * 8), *vsav = xalloc(n3 * 8);
+  int counter = 0;
+  double outer_it_criterion = 1.0e10, outer_it_target = 1.0e-12;
+  const double L2_target = 1.0e-4, L2_target_relative = 1.0e-7, resid_target = 1.0e-4;
+  int status = ORC_OK;
+  while (outer_it_criterion >= outer_it_target && counter < m->maxiter_nonlinear) {
+    counter = counter + 1;
+    st = orc_calcbeta(m, &s, beta_internal);
+    if (st != ORC_OK) { status = st; break; }
+    memcpy(usav, uvel, n3 * 8);
+    memcpy(vsav, vvel, n3 * 8);
+    long nnz = 0;
+    st = orc_assemble_system(m, &s, beta_internal, uvel, vvel, efvs, Auu, Auv,
+                             Avu, Avv, bu, bv, &nnz);
+    if (st != ORC_OK) { status = st; break; }
+    if (nnz == 0) {
+      memset(uvel, 0, n3 * 8);
+      memset(vvel, 0, n3 * 8);
+      status = ORC_ZERO_MATRIX;
+      break;
+    }
+    residual_vector_3d(nx, ny, nz, m->periodic, s.active_vertex, Auu, Auv, Avu,
+                       Avv, bu, bv, uvel, vvel, &stats->L2_norm,
+                       &stats->L2_norm_relative);
+    double err = 0.0;
+    int niters = 0;
+    if (m->which_sparse == ORC_SPARSE_PCG_CHRONGEAR)
+      st = orc_pcg_chrongear_3d(nx, ny, nz, m->periodic, s.active_vertex, Auu,
+                                Auv, Avu, Avv, bu, bv, uvel, vvel,
+                                m->which_precond, m->pcg_maxiters, m->pcg_tol,
+                                m->pcg_ncheck, &err, &niters);
+    else
+      st = orc_pcg_standard_3d(nx, ny, nz, m->periodic, s.active_vertex, Auu,
+                               Auv, Avu, Avv, bu, bv, uvel, vvel,
+                               m->which_precond, m->pcg_maxiters, m->pcg_tol,
+                               m->pcg_ncheck, &err, &niters);
+    stats->pcg_iters_total += niters;
+    stats->pcg_iters_last = niters;
+    stats->pcg_err_last = err;
+    if (st == ORC_ERR_NAN) { status = st; break; }
+    orc_halo_stag(nx, ny, nz, m->periodic, uvel);
+    orc_halo_stag(nx, ny, nz, m->periodic, vvel);
+    double resid_velo = residual_velocity_3d(nx, ny, nz, m->periodic,
+                                             m->which_resid, uvel, vvel, usav, vsav);
+    stats->resid_velo = resid_velo;
+    if (m->which_resid == ORC_RESID_L2NORM) {
+      outer_it_criterion = stats->L2_norm; outer_it_target = L2_target;
+    } else if (m->which_resid == ORC_RESID_L2NORM_RELATIVE) {
+      outer_it_criterion = stats->L2_norm_relative; outer_it_target = L2_target_relative;
+    } else {
+      outer_it_criterion = resid_velo; outer_it_target = resid_target;
+    }
+  }
+  stats->picard_iters = counter;
+  stats->converged = (status == ORC_OK && counter < m->maxiter_nonlinear) ? 1 : 0;
+  if (status == ORC_OK && !stats->converged) status = ORC_WARN_PICARD_NOT_CONVERGED;
+  stats->status = status;
+  free(Auu); free(Auv); free(Avu); free(Avv); free(bu); free(bv);
+  free(usav); free(vsav);
+  orc_setup_free(&s);
+  return status;
+}

@@ -1,0 +1,125 @@
+// hostemu.cpp -- TEST ONLY.  Runs the device kernels' per-thread bodies
+// (cism_b200/csrc/bp_body.h) sequentially on the CPU through the same host
+// plan, so the compaction, periodic images and assembly indexing can be
+// checked against the oracle without a GPU.  Not part of the product
+// library and never loaded by it.
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "bp_body.h"
+#include "bp_plan.h"
+
+using namespace bp;
+
+namespace {
+struct Emu {
+  HostPlan p;
+  std::vector<InstParams> inst;
+  std::vector<InstState> st;
+  std::vector<double> qp, efvs, badj;
+  std::vector<double2> A, x, b;
+  DevView v;
+  void bind() {
+    std::memset(&v, 0, sizeof(v));
+    v.nz = p.nz; v.ncols = p.ncols; v.nnodes = p.nnodes; v.npad = p.npad;
+    v.ncells = p.ncells; v.nelem = p.nelem; v.ninst = p.ninst; v.ntiles = p.ntiles;
+    int anyd = 0;
+    for (auto m : p.dmask) anyd |= m != 0;
+    v.any_dirichlet = anyd;
+    v.inst = p.inst.data();
+    st.assign(p.ninst, InstState{});
+    v.st = st.data();
+    v.col_inst = p.col_inst.data(); v.col_nbr = p.col_nbr.data(); v.col_cells = p.col_cells.data();
+    v.col_ij = p.col_ij.data(); v.col_beta = p.col_beta.data(); v.load = p.load.data();
+    v.dmask = p.dmask.data(); v.cell_inst = p.cell_inst.data(); v.cell_ij = p.cell_ij.data();
+    v.cell_cols = p.cell_cols.data(); v.cell_s = p.cell_s.data(); v.cell_h = p.cell_h.data();
+    v.cell_beta = p.cell_beta.data(); v.flwafact = p.flwafact.data();
+    qp.assign((size_t)p.nelem * 80, 0.0); v.qp = qp.data();
+    efvs.assign(std::max(p.nelem, 1), 0.0); v.efvs = efvs.data();
+    badj.assign(4 * (size_t)p.npad, 0.0); v.badj = badj.data();
+    A.assign(2 * 27 * (size_t)p.npad, double2{0, 0}); v.A = A.data();
+    x.assign(p.npad, double2{0, 0}); v.x = x.data();
+    b.assign(p.npad, double2{0, 0}); v.b = b.data();
+  }
+};
+
+template <int B>
+void rows(Emu& E, const RefTables& T) {
+  const DevView& v = E.v;
+  double* Ad = reinterpret_cast<double*>(E.A.data());
+  for (int n = 0; n < v.nnodes; ++n) {
+    const int col = n / v.nz, k = n - col * v.nz;
+    double acc[27];
+    row_assemble<B>(v, T, col, k, acc);
+    row_basal<B>(v, T, col, k, acc);
+    const double adj = row_dirichlet<B>(v, col, k, acc);
+    for (int m = 0; m < 27; ++m)
+      Ad[(((size_t)((B >> 1) * 27 + m)) * v.npad + n) * 2 + (B & 1)] = acc[m];
+    E.badj[(size_t)B * v.npad + n] = adj;
+  }
+}
+}  // namespace
+
+extern "C" int emu_assemble(const bp_inputs* in, const double* uvel, const double* vvel,
+                            double* Auu, double* Auv, double* Avu, double* Avv, double* bu,
+                            double* bv, double* efvs) {
+  Emu E;
+  std::string err;
+  if (!build_plan(in, 1, &E.p, &err)) return 10;
+  E.bind();
+  gather_velocity(E.p, 0, uvel, vvel, E.x.data());
+  RefTables T;
+  fill_ref_tables(&T);
+  for (int e = 0; e < E.p.nelem; ++e) {
+    double s = 0.0;
+    for (int p = 0; p < 8; ++p) {
+      double out[10], eq = 0.0;
+      if (!qp_element_point(E.v, T, e, p, out, &eq)) return 2;
+      std::memcpy(&E.qp[((size_t)e * 8 + p) * 10], out, sizeof(out));
+      s += eq;
+    }
+    E.efvs[e] = s / 8.0;
+  }
+  rows<0>(E, T); rows<1>(E, T); rows<2>(E, T); rows<3>(E, T);
+  const size_t np = E.p.npad;
+  for (int n = 0; n < E.p.nnodes; ++n) {
+    const uint8_t dm = E.p.dmask[n];
+    double u = E.p.load[n].x - E.badj[n] - E.badj[np + n];
+    double w = E.p.load[n].y - E.badj[2 * np + n] - E.badj[3 * np + n];
+    if (dm & 1) u = E.x[n].x;
+    if (dm & 2) w = E.x[n].y;
+    E.b[n] = double2{u, w};
+  }
+  scatter_matrix(E.p, E.A.data(), Auu, Auv, Avu, Avv);
+  const size_t tot = (size_t)in->nz * (in->nx - 1) * (in->ny - 1);
+  std::memset(bu, 0, tot * 8);
+  std::memset(bv, 0, tot * 8);
+  scatter_vector(E.p, 0, E.b.data(), bu, bv);
+  scatter_efvs(E.p, 0, E.efvs.data(), efvs);
+  return 0;
+}
+
+extern "C" int emu_matvec(int nx, int ny, int nz, int periodic, const int* active_vertex,
+                          const double* Auu, const double* Auv, const double* Avu,
+                          const double* Avv, const double* xu, const double* xv, double* yu,
+                          double* yv) {
+  Emu E;
+  std::string err;
+  if (!build_column_plan(nx, ny, nz, periodic, active_vertex, &E.p, &err)) return 10;
+  E.bind();
+  gather_matrix(E.p, Auu, Auv, Avu, Avv, E.A.data());
+  gather_velocity(E.p, 0, xu, xv, E.x.data());
+  std::vector<double2> y(E.p.npad, double2{0, 0});
+  const double2* xs = E.x.data();
+  auto src = [xs](size_t m) { return xs[m]; };
+  for (int n = 0; n < E.p.nnodes; ++n) {
+    const int col = n / nz, k = n - col * nz;
+    y[n] = matvec_row(E.v, E.A.data(), col, k, (size_t)n, src);
+  }
+  const size_t tot = (size_t)nz * (nx - 1) * (ny - 1);
+  std::memset(yu, 0, tot * 8);
+  std::memset(yv, 0, tot * 8);
+  scatter_vector(E.p, 0, y.data(), yu, yv);
+  return 0;
+}
