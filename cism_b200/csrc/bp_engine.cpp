@@ -134,23 +134,31 @@ DevView make_view(bp_ctx* c, const HostPlan& p, bool with_cells, bool mixed) {
   return v;
 }
 
-void init_state(bp_ctx* c, const DevView& v, int ninst, bool picard, bool pcg) {
+void init_state(bp_ctx* c, const DevView& v, const HostPlan& p, bool picard, bool pcg) {
+  const int ninst = p.ninst;
   std::vector<InstState> st(ninst);
-  for (auto& s : st) {
+  int live = 0;
+  for (int b = 0; b < ninst; ++b) {
+    InstState& s = st[b];
     std::memset(&s, 0, sizeof(s));
-    s.picard_active = picard ? 1 : 0;
-    s.pcg_active = pcg ? 1 : 0;
-    s.refine_active = pcg ? 1 : 0;
+    const bool empty = p.inst[b].node_end == p.inst[b].node_begin;
+    // no active vertex at all: count_nonzeros_3d = 0, velocity zero
+    // (glissade_velo_higher.F90:3191-3220)
+    s.status = empty ? BP_ZERO_MATRIX : BP_OK;
+    s.picard_active = (picard && !empty) ? 1 : 0;
+    s.pcg_active = (pcg && !empty) ? 1 : 0;
+    s.refine_active = s.pcg_active;
     s.pcg_iter = 1;
     s.rz = 1.0;
     s.rz_old = 1.0;
     s.err = -1.0;
+    live += empty ? 0 : 1;
   }
   CK(cudaMemcpyAsync(v.st, st.data(), sizeof(InstState) * ninst, cudaMemcpyHostToDevice, c->stream));
   Counters h{};
-  h.picard_active = picard ? ninst : 0;
-  h.pcg_active = pcg ? ninst : 0;
-  h.refine_active = pcg ? ninst : 0;
+  h.picard_active = picard ? live : 0;
+  h.pcg_active = pcg ? live : 0;
+  h.refine_active = pcg ? live : 0;
   CK(cudaMemcpyAsync(v.cnt, &h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
 }
 
@@ -283,7 +291,7 @@ int solve_batch(bp_ctx* c, int n, const bp_inputs* in, double* const* uvel,
   std::vector<double2> x(p.npad, double2{0.0, 0.0});
   for (int b = 0; b < n; ++b) gather_velocity(p, b, uvel[b], vvel[b], x.data());
   CK(cudaMemcpyAsync(v.x, x.data(), sizeof(double2) * p.npad, cudaMemcpyHostToDevice, c->stream));
-  init_state(c, v, n, true, false);
+  init_state(c, v, p, true, false);
   CK(cudaEventRecord(c->t1, c->stream));
   int max_picard = 1;
   for (const auto& ip : p.inst) max_picard = std::max(max_picard, ip.maxiter_nonlinear);
@@ -452,7 +460,7 @@ int bp_pcg(bp_ctx* c, int nx, int ny, int nz, int periodic,
   gather_velocity(p, 0, bu, bv, b.data());
   CK(cudaMemcpyAsync(v.x, x.data(), sizeof(double2) * p.npad, cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(v.b, b.data(), sizeof(double2) * p.npad, cudaMemcpyHostToDevice, c->stream));
-  init_state(c, v, 1, false, true);
+  init_state(c, v, p, false, true);
   launch_dinv(v, precond, c->stream);
   launch_bb(v, c->stream);
   linear_solve(c, v, p);
@@ -516,7 +524,7 @@ int bp_assemble(bp_ctx* c, const bp_inputs* in, const double* uvel,
   std::vector<double2> x(p.npad, double2{0, 0});
   gather_velocity(p, 0, uvel, vvel, x.data());
   CK(cudaMemcpyAsync(v.x, x.data(), sizeof(double2) * p.npad, cudaMemcpyHostToDevice, c->stream));
-  init_state(c, v, 1, true, false);
+  init_state(c, v, p, true, false);
   launch_picard_begin(v, c->stream);
   launch_assemble(v, c->stream);
   std::vector<double2> A(2 * 27 * (size_t)p.npad), b(p.npad);

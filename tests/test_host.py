@@ -1,0 +1,103 @@
+"""CPU tests of the product's host side: the setup mirror (C++), the host
+plan (compaction, periodic images) and the device kernels' per-thread
+bodies (compiled for the CPU by tests/hostemu), all against the oracle, and
+the C-ABI library's exported symbols."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from cism_b200 import configs, solver
+from oracle import oracle
+
+from helpers import oracle_system, owned_active_rows, random_state, rel_l2
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+EMU = os.path.join(ROOT, "tests", "hostemu", "libhostemu.so")
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+
+def _p(a):
+    return a.ctypes.data_as(_ip if a.dtype == np.int32 else _dp)
+
+
+def _models():
+    out = [configs.dome(), configs.slab(n=24), configs.marine(n=40, dx=4000.0),
+           configs.analytic_slab(nz=8)]
+    m = configs.marine(n=32, dx=4000.0)
+    m.which_assemble_beta = 0
+    m.name = "marine_standard_beta"
+    out.append(m)
+    m = configs.dome()
+    m.kinbcmask = np.zeros((m.ny - 1, m.nx - 1), np.int32)
+    m.kinbcmask[15:18, 14:16] = 1
+    m.which_babc = 5
+    m.beta_external[:] = 500.0
+    m.name = "dome_kinematic_bc"
+    out.append(m)
+    m = configs.dome(n=20).copy(periodic=0)
+    m.name = "dome_outflow"
+    out.append(m)
+    return out
+
+
+MODELS = _models()
+
+
+@pytest.mark.parametrize("m", MODELS, ids=lambda m: m.name)
+def test_setup_mirror_bitwise(m):
+    prep, u, v = solver.prepare(m)
+    su = oracle.setup(m)
+    for k, a in prep.arrays.items():
+        assert np.array_equal(a, su[k]), k
+
+
+@pytest.mark.parametrize("m", MODELS, ids=lambda m: m.name)
+def test_kernel_bodies_match_oracle(m):
+    emu = C.CDLL(EMU)
+    prep, _, _ = solver.prepare(m)
+    su, u, v, A, bu, bv, efvs = oracle_system(m, seed=0, scale=10.0)
+    shp = (m.ny - 1, m.nx - 1, m.nz, 27)
+    E = [np.zeros(shp) for _ in range(4)]
+    ebu, ebv = np.zeros(m.vshape3), np.zeros(m.vshape3)
+    eef = np.zeros((m.ny, m.nx, m.nz - 1))
+    rc = emu.emu_assemble(C.byref(prep.inputs), _p(np.ascontiguousarray(u)), _p(np.ascontiguousarray(v)),
+                          *[_p(a) for a in E], _p(ebu), _p(ebv), _p(eef))
+    assert rc == 0
+    rows = owned_active_rows(m, su["active_vertex"])
+    for a, e in zip(A, E):
+        assert np.max(np.abs(a[rows] - e[rows])) <= 1e-13 * np.max(np.abs(a[rows]))
+    assert rel_l2([ebu[rows], ebv[rows]], [bu[rows], bv[rows]]) < 1e-13
+    assert np.max(np.abs(eef - efvs)) <= 1e-13 * np.max(np.abs(efvs))
+    xu, xv = random_state(m, su, seed=9, scale=1.0)
+    yu, yv = oracle.matvec(m, su["active_vertex"], A, xu, xv)
+    eyu, eyv = np.zeros(m.vshape3), np.zeros(m.vshape3)
+    av = np.ascontiguousarray(su["active_vertex"], np.int32)
+    rc = emu.emu_matvec(m.nx, m.ny, m.nz, m.periodic, _p(av), *[_p(np.ascontiguousarray(a)) for a in A],
+                        _p(xu), _p(xv), _p(eyu), _p(eyv))
+    assert rc == 0
+    assert rel_l2([eyu, eyv], [yu, yv]) < 1e-14
+
+
+def test_library_exports_every_declared_symbol():
+    hdr = open(os.path.join(ROOT, "include", "bp_b200.h")).read()
+    names = set(re.findall(r"^\s*(?:int|const char \*)\s*\**\s*(bp_\w+)\s*\(", hdr, re.M))
+    assert {"bp_create", "bp_solve", "bp_pcg", "bp_matvec", "bp_assemble", "bp_batch_solve"} <= names
+    lib = C.CDLL(solver.LIB_PATH)
+    for n in sorted(names):
+        assert hasattr(lib, n), n
+    assert lib.bp_abi_version() == 1
+
+
+def test_context_needs_a_device():
+    """No CPU fallback: without a CUDA device bp_create fails loudly."""
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    with pytest.raises(solver.BPError) as e:
+        solver.Context(0)
+    assert e.value.code == 11
