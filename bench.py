@@ -1,0 +1,433 @@
+#!/usr/bin/env python
+"""Converged Blatter-Pattyn velocity solves per second on B200.
+
+Workload (default): the periodic slab on a sliding bed, 160 x 160 cells,
+dx = 0.5 km, 11 sigma levels, beta = 1000 + 1000 sin(2 pi x/L) sin(2 pi y/L),
+Glen n = 3, A = 1e-16; Picard to 1e-4 max relative speed change, every
+linear solve to a relative residual of 1e-8.  A "step" is one full
+converged solve from a zero initial guess.  Synthetic seeded inputs (no
+dataset is used).
+
+Paths: plain FP64 GPU solve ("fp64") and FP32-inner / FP64-refined solve
+("mixed").  The headline `value` is the fastest path whose final relative
+residual is below 1e-8 and whose velocity is within 1e-6 relative L2 of
+the FP64 solution; every path is reported under "paths".
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun) every rank solves its own replica (the solve does
+not shard across GPUs); value = all ranks' solves / max rank time.
+`--impl reference` times the CPU oracle (a restatement of the reference's
+Fortran, which cannot be compiled here) on the box's host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "converged velocity solves/sec @1e-8 rel resid: learned+mixed vs plain FP64, 1 B200"
+UNIT = "solves/s"
+WORKLOAD_DESC = {
+    "c1": "periodic slab 160x160 cells x 11 levels, dx=0.5 km, sinusoidal beta, Glen n=3 (BP Picard+PCG)",
+    "c0": "parabolic dome 31x31 cells x 10 levels, dx=2 km, no-slip bed (BP Picard+PCG)",
+    "c2": "marine ice sheet 400x400 cells x 11 levels, dx=4 km, grounding line + shelf (BP Picard+CG-PCG)",
+}
+# FP64 Picard/PCG iteration counts of one converged solve of each workload
+# (the same algorithm runs in the oracle; the parity tests check the counts
+# agree).  Used to extrapolate the bounded CPU samples to whole solves.
+ITERATION_COUNTS = os.path.join(ROOT, "profiles", "iteration_counts.json")
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c1", choices=sorted(WORKLOAD_DESC))
+    ap.add_argument("--precision", default="best", choices=["best", "fp64", "mixed"])
+    ap.add_argument("--pcg-maxiters", type=int, default=3000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-run", action="store_true",
+                    help="one untimed solve (for ncu launch lists / captures)")
+    ap.add_argument("--picard-cap", type=int, default=0,
+                    help="with --profile-run: stop after this many Picard iterations")
+    return ap.parse_args()
+
+
+def make_model(name, pcg_maxiters):
+    from cism_b200 import configs
+
+    m = configs.workload(name)
+    # the reference hard-codes maxiters = 200 (glissade_velo_higher_pcg.F90:67-69),
+    # which does not reach 1e-8 on these systems; the metric needs converged solves
+    return m.copy(pcg_maxiters=pcg_maxiters)
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (replicas only)
+# ---------------------------------------------------------------------------
+class Dist:
+    def __init__(self, gpus):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+
+            torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            import torch
+
+            self.pg.barrier(device_ids=[self.local])
+            torch.cuda.synchronize()
+
+    def max(self, x):
+        if not self.pg:
+            return x
+        import torch
+
+        t = torch.tensor([float(x)], device=f"cuda:{self.local}", dtype=torch.float64)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class Clocks:
+    Q = ("uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index=0):
+        self.proc = None
+        self.path = None
+        self.uuid = None
+        try:
+            import torch
+
+            u = torch.cuda.get_device_properties(device_index).uuid
+            self.uuid = "GPU-" + str(u)
+        except Exception:
+            pass
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader",
+                                          "-lms", "200"], stdout=open(self.path, "w"),
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            if self.uuid and f[0] != self.uuid:
+                continue
+            try:
+                rows.append((float(f[1].split()[0]), float(f[2].split()[0]), f[5:9]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for _, _, r in rows for n, v in zip(names, r) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def matvec_traffic(nodes, precision):
+    """DRAM bytes per launch of the dominant kernel from the committed ncu
+    summary (bytes per node, scaled to this workload), or None."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if not os.path.exists(p):
+        return None
+    d = json.load(open(p))
+    k = d.get("fp32_inner" if precision == "mixed" else "fp64_pcg")
+    if not k:
+        return None
+    return k["dram_bytes_per_node"] * nodes
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: bounded sample of the oracle, extrapolated to a whole solve
+# ---------------------------------------------------------------------------
+def cpu_sample(workload, pcg_maxiters, counts, iters=(20, 200)):
+    import numpy as np
+
+    from oracle import oracle  # the checker
+
+    m = make_model(workload, pcg_maxiters)
+    t0 = time.perf_counter()
+    su = oracle.setup(m)
+    t_setup = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    A, bu, bv, _, _ = oracle.assemble_system(m, su, su["uvel"], su["vvel"])
+    t_asm = time.perf_counter() - t0
+    z = np.zeros(m.vshape3)
+    ts = []
+    for it in iters:
+        t0 = time.perf_counter()
+        oracle.pcg(m, su["active_vertex"], A, bu, bv, z, z, precond=m.which_precond,
+                   variant=m.which_sparse if m.which_sparse in (2, 3) else 2, maxiters=it, tol=0.0)
+        ts.append(time.perf_counter() - t0)
+    t_iter = (ts[1] - ts[0]) / (iters[1] - iters[0])
+    t_pcg_fixed = ts[0] - iters[0] * t_iter  # preconditioner setup + initial residual
+    P, I = counts["picard_iters"], counts["pcg_iters_total"]
+    t_solve = t_setup + P * (t_asm + t_pcg_fixed) + I * t_iter
+    sample = (f"oracle port (C, 1 thread): setup + one assembly + {iters[0]} and {iters[1]} PCG "
+              f"iterations of the {workload} system, extrapolated to {P} Picard / {I} PCG iterations "
+              f"per converged solve")
+    return {"solves_per_s": 1.0 / t_solve, "t_setup": t_setup, "t_assembly": t_asm,
+            "t_pcg_iter": t_iter, "t_solve_est": t_solve, "sample": sample,
+            "sample_seconds": t_setup + t_asm + sum(ts)}
+
+
+def load_counts(workload):
+    if os.path.exists(ITERATION_COUNTS):
+        d = json.load(open(ITERATION_COUNTS))
+        if workload in d:
+            return d[workload]
+    return None
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(args, D):
+    import numpy as np
+
+    from cism_b200 import solver
+
+    ctx = solver.Context(D.local)
+    m = make_model(args.workload, args.pcg_maxiters)
+    paths = ["fp64", "mixed"] if args.precision == "best" else [args.precision]
+    res = {}
+    sol = {}
+    for path in paths:
+        prec = solver.MIXED if path == "mixed" else solver.FP64
+        prep, u0, v0 = solver.prepare(m, precision=prec, inner_tol=1e-4)
+        prob = ctx.problem([prep])
+        prob.set_guess([u0], [v0])
+        for _ in range(args.warmup):
+            prob.run()
+        D.barrier()
+        clocks = Clocks(D.local)
+        clocks.start()
+        ctx.timer_start()
+        sts = [prob.run()[0] for _ in range(args.steps)]
+        ms = ctx.timer_stop()
+        ck = clocks.stop()
+        D.barrier()
+        ms_max = D.max(ms)
+        us, vs, _ = prob.get()
+        sol[path] = (us[0], vs[0])
+        st = sts[-1]
+        # kernel timing pass (CUDA events around every launch, graphs off)
+        prob.timing(True)
+        st_t = prob.run()[0]
+        kt = prob.kernel_times()
+        prob.timing(False)
+        info = prob.info()
+        launches = sum(n for _, n in kt.values())
+        res[path] = {"value": D.world * args.steps / (ms_max / 1000.0), "ms_per_step": ms_max / args.steps,
+                     "status": st["status"], "picard_iters": st["picard_iters"],
+                     "pcg_iters_total": st["pcg_iters_total"], "refine_steps": st["refine_steps_total"],
+                     "final_rel_resid": st["pcg_err_last"], "kernel_times": kt, "info": info,
+                     "launches_per_step": launches, "clocks": ck, "prep": prep, "prob": prob,
+                     "u0": u0, "v0": v0, "timing_status": st_t["status"]}
+    # accuracy of each path against the FP64 solution
+    if "fp64" in sol:
+        uf, vf = sol["fp64"]
+        den = math.sqrt(float(np.sum(uf ** 2 + vf ** 2)))
+        for path, (u, v) in sol.items():
+            res[path]["rel_l2_vs_fp64"] = math.sqrt(float(np.sum((u - uf) ** 2 + (v - vf) ** 2))) / den
+    ok = [p for p in paths if res[p]["status"] == 0 and res[p]["final_rel_resid"] < 1e-8
+          and res[p].get("rel_l2_vs_fp64", 0.0) <= 1e-6]
+    head = max(ok, key=lambda p: res[p]["value"]) if ok else paths[0]
+    H = res[head]
+    # e2e: the C-ABI call with host buffers (plan, H2D, solve, D2H per step)
+    prep = H["prep"]
+    for _ in range(max(1, args.warmup // 2)):
+        ctx.solve_prepared(prep, H["u0"], H["v0"], want_efvs=False)
+    D.barrier()
+    ctx.timer_start()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        _, _, _, st_e = ctx.solve_prepared(prep, H["u0"], H["v0"], want_efvs=False)
+    ms_e = ctx.timer_stop()
+    wall_e = (time.perf_counter() - t0) * 1000.0
+    D.barrier()
+    ms_e = D.max(max(ms_e, wall_e))
+    e2e = {"value": D.world * args.steps / (ms_e / 1000.0), "unit": UNIT,
+           "h2d_bytes_per_step": int(st_e["h2d_bytes"]), "d2h_bytes_per_step": int(st_e["d2h_bytes"]),
+           "call": "bp_solve (C ABI) on host arrays"}
+    # roofline of the dominant kernel
+    cat = "inner_matvec_fp32" if head == "mixed" else "pcg_matvec_fp64"
+    kms, kn = H["kernel_times"][cat]
+    bytes_launch = H["info"]["matvec_bytes_fp32" if head == "mixed" else "matvec_bytes_fp64"]
+    peak, peak_src = measured_peaks()
+    avg_s = (kms / max(kn, 1)) / 1000.0
+    achieved = bytes_launch / avg_s / 1e9 if kn else 0.0
+    traffic = matvec_traffic(H["info"]["nodes"], head)
+    roof = {"bound": "hbm", "kernel": ("k_inner_a (FP32 inner CG matvec)" if head == "mixed"
+                                       else "k_mv<MV_STD_A> (fused d-update + FP64 matvec + (d,q))"),
+            "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)",
+            "traffic": traffic, "algorithmic_bytes_per_launch": bytes_launch,
+            "avg_launch_us": round(avg_s * 1e6, 2), "launches_timed": kn}
+    out = {
+        "metric": METRIC, "value": round(H["value"], 4), "unit": UNIT, "n_gpus": D.world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(H["ms_per_step"], 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64" if head == "fp64" else "f32+f64",
+        "data": "synthetic (seeded geometry generator, no dataset)",
+        "config": {"workload": WORKLOAD_DESC[args.workload], "name": args.workload, "path": head,
+                   "nodes": H["info"]["nodes"], "columns": H["info"]["columns"],
+                   "pcg_maxiters": args.pcg_maxiters, "pcg_tol": 1e-8, "picard_tol": 1e-4,
+                   "l2": "inputs larger than L2 (FP64 matrix %.0f MB > 126 MB)" % (
+                       H["info"]["nodes"] * 864 / 1e6),
+                   "parallelism": f"replicas x{D.world}" if D.world > 1 else "single GPU"},
+        "e2e": e2e,
+        "roofline": roof,
+        "gpu_launches": H["launches_per_step"] * args.steps,
+        "clocks": H["clocks"],
+        "paths": {p: {k: (round(v, 6) if isinstance(v, float) else v) for k, v in r.items()
+                      if k in ("value", "ms_per_step", "status", "picard_iters", "pcg_iters_total",
+                               "refine_steps", "final_rel_resid", "rel_l2_vs_fp64")}
+                  for p, r in res.items()},
+    }
+    if "fp64" in res and head != "fp64":
+        out["speedup_vs_plain_fp64"] = round(H["value"] / res["fp64"]["value"], 3)
+    if D.rank == 0 and D.world == 1 and not args.no_cpu_baseline:
+        counts = {"picard_iters": res.get("fp64", H)["picard_iters"],
+                  "pcg_iters_total": res.get("fp64", H)["pcg_iters_total"]}
+        cs = cpu_sample(args.workload, args.pcg_maxiters, counts)
+        out["cpu_baseline"] = {"value": round(cs["solves_per_s"], 8), "unit": UNIT, "cores": 1,
+                               "kind": "port", "sample": cs["sample"],
+                               "sample_seconds": round(cs["sample_seconds"], 1)}
+    for r in res.values():
+        r["prob"].close()
+    ctx.close()
+    return out
+
+
+# ---------------------------------------------------------------------------
+# reference arm: the oracle (restatement of the reference Fortran) on the
+# host cores, one bounded sample per worker process
+# ---------------------------------------------------------------------------
+def _ref_worker(a):
+    workload, maxit, counts = a
+    sys.path.insert(0, ROOT)
+    return cpu_sample(workload, maxit, counts, iters=(10, 40))
+
+
+def run_reference(args, D):
+    if D.rank != 0:
+        return None
+    import multiprocessing as mp
+
+    counts = load_counts(args.workload)
+    if counts is None:
+        return {"impl": "reference", "unavailable": "no recorded iteration counts for this workload"}
+    ncores = os.cpu_count() or 1
+    workers = max(1, min(ncores, 16))
+    ctx = mp.get_context("spawn")
+    vals = []
+    with ctx.Pool(workers) as pool:
+        for step in range(args.warmup + args.steps):
+            r = pool.map(_ref_worker, [(args.workload, args.pcg_maxiters, counts)] * workers)
+            if step >= args.warmup:
+                vals.append(sum(x["solves_per_s"] for x in r))
+            last = r[0]
+    v = statistics.median(vals)
+    sample = (f"{workers} concurrent oracle processes (1 thread each, {ncores} host cores), each: "
+              + last["sample"])
+    return {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": D.world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 / v if v else None, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD_DESC[args.workload], "name": args.workload},
+            "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": workers, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def profile_run(args):
+    """One solve of the workload through the resident-problem API, untimed."""
+    from cism_b200 import solver
+
+    m = make_model(args.workload, args.pcg_maxiters)
+    if args.picard_cap > 0:
+        m = m.copy(maxiter_nonlinear=args.picard_cap)
+    prec = solver.MIXED if args.precision == "mixed" else solver.FP64
+    ctx = solver.Context(0)
+    prep, u0, v0 = solver.prepare(m, precision=prec)
+    prob = ctx.problem([prep])
+    prob.set_guess([u0], [v0])
+    st = prob.run()[0]
+    print(json.dumps({"profile_run": args.workload, "precision": args.precision,
+                      "status": st["status"], "picard_iters": st["picard_iters"],
+                      "pcg_iters_total": st["pcg_iters_total"]}), flush=True)
+    prob.close()
+    ctx.close()
+
+
+def main():
+    args = parse_args()
+    if args.profile_run:
+        profile_run(args)
+        return
+    D = Dist(args.gpus)
+    try:
+        out = run_reference(args, D) if args.impl == "reference" else run_ours(args, D)
+        if D.rank == 0 and out is not None:
+            print(json.dumps(out), flush=True)
+    finally:
+        D.close()
+
+
+if __name__ == "__main__":
+    main()

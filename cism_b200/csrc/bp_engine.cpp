@@ -1,18 +1,18 @@
-// bp_engine.cpp -- context, device memory, solver drivers and the C ABI.
+// bp_engine.cpp -- context, resident problems, solver drivers and the C ABI.
 //
-// One context = one device + one stream + a growing device arena that is
-// reused across calls (time steps), so repeated solves do not reallocate.
-// The drivers only enqueue work; all scalar decisions (alpha, beta,
-// convergence, Picard stop) are taken on the device.  The host reads two
-// counters per PCG check chunk and one per Picard iteration, one chunk
-// behind the device, to know when to stop enqueuing.
+// A context is one device and one stream.  A problem is a compiled solve (or
+// batch) resident in device memory: its plan arrays, matrix, vectors and the
+// CUDA graphs of its PCG check chunks, reused across runs.  The drivers only
+// enqueue work; every scalar decision (alpha, beta, convergence, Picard
+// stop) is taken on the device.  The host reads a 16-byte counter snapshot
+// once per check chunk, one chunk behind the device, to stop enqueuing.
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <string>
 #include <vector>
@@ -22,22 +22,7 @@
 #include "bp_kernels.h"
 #include "bp_plan.h"
 
-struct bp_ctx {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  std::string err;
-  std::map<std::string, std::pair<void*, size_t>> arena;
-  bp::Counters* h_cnt = nullptr;   // pinned, [2] slots
-  cudaEvent_t ev[2] = {nullptr, nullptr};
-  cudaEvent_t t0 = nullptr, t1 = nullptr, t2 = nullptr, t3 = nullptr;
-  int num_sms = 0;
-  int grid_cap = 0;
-  bool tables_ready = false;
-};
-
 namespace {
-
-using namespace bp;
 
 struct CudaError {
   cudaError_t e;
@@ -50,31 +35,95 @@ struct CudaError {
     if (e_ != cudaSuccess) throw CudaError{e_, #call};     \
   } while (0)
 
-template <typename T>
-T* arena_get(bp_ctx* c, const char* name, size_t count) {
-  size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
-  bytes = (bytes + 255) / 256 * 256;
-  auto it = c->arena.find(name);
-  if (it != c->arena.end() && it->second.second >= bytes) return static_cast<T*>(it->second.first);
-  if (it != c->arena.end()) {
-    CK(cudaStreamSynchronize(c->stream));
-    CK(cudaFree(it->second.first));
-    c->arena.erase(it);
+// Named device allocations that only grow.
+struct Arena {
+  std::map<std::string, std::pair<void*, size_t>> m;
+  template <typename T>
+  T* get(cudaStream_t s, const char* name, size_t count) {
+    size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+    bytes = (bytes + 255) / 256 * 256;
+    auto it = m.find(name);
+    if (it != m.end() && it->second.second >= bytes) return static_cast<T*>(it->second.first);
+    if (it != m.end()) {
+      CK(cudaStreamSynchronize(s));
+      CK(cudaFree(it->second.first));
+      m.erase(it);
+    }
+    void* p = nullptr;
+    CK(cudaMalloc(&p, bytes));
+    m[name] = {p, bytes};
+    return static_cast<T*>(p);
   }
-  void* p = nullptr;
-  CK(cudaMalloc(&p, bytes));
-  c->arena[name] = {p, bytes};
-  return static_cast<T*>(p);
-}
+  void release() {
+    for (auto& kv : m) cudaFree(kv.second.first);
+    m.clear();
+  }
+};
+
+// Event pairs around kernel launches, by category.
+struct Timing {
+  bool on = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pool;
+  std::vector<int> cat;
+  double ms[BP_NUM_KERNEL_CATEGORIES] = {0};
+  int n[BP_NUM_KERNEL_CATEGORIES] = {0};
+  void reset() {
+    cat.clear();
+    for (int i = 0; i < BP_NUM_KERNEL_CATEGORIES; ++i) { ms[i] = 0.0; n[i] = 0; }
+  }
+  void destroy() {
+    for (auto& pr : pool) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
+    pool.clear();
+  }
+};
+
+}  // namespace
+
+struct bp_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  Arena arena;                     // for the one-shot entry points
+  bp::Counters* h_cnt = nullptr;   // pinned, 2 slots
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  cudaEvent_t t0 = nullptr, t1 = nullptr, t2 = nullptr, t3 = nullptr;
+  cudaEvent_t r0 = nullptr, r1 = nullptr;  // bp_timer_start / stop
+  int num_sms = 0;
+};
+
+struct bp_problem {
+  bp_ctx* c = nullptr;
+  Arena own;
+  Arena* arena = nullptr;
+  bp::HostPlan plan;
+  bp::DevView v;
+  bool mixed = false;
+  double2* x0 = nullptr;
+  cudaGraphExec_t chunk_graph = nullptr;
+  cudaGraphExec_t inner_graph = nullptr;
+  bool use_graphs = true;
+  Timing timing;
+  std::vector<bp::InstState> state;
+  float ms_upload = 0, ms_solve = 0;
+  double h2d_bytes = 0, d2h_bytes = 0;
+};
+
+namespace {
+
+using namespace bp;
+
+double g_h2d = 0.0;  // bytes uploaded by the current call (single-threaded per context)
 
 template <typename T>
-void upload(bp_ctx* c, T* dst, const std::vector<T>& src) {
-  if (!src.empty())
-    CK(cudaMemcpyAsync(dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, c->stream));
+void upload(cudaStream_t s, T* dst, const std::vector<T>& src) {
+  if (!src.empty()) {
+    CK(cudaMemcpyAsync(dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+    g_h2d += (double)src.size() * sizeof(T);
+  }
 }
 
-// Device arrays of a plan.  `with_cells` = element data needed.
-DevView make_view(bp_ctx* c, const HostPlan& p, bool with_cells, bool mixed) {
+// Allocate and upload the device arrays of a plan.
+DevView make_view(Arena& a, cudaStream_t s, const HostPlan& p, bool with_cells, bool mixed) {
   DevView v;
   std::memset(&v, 0, sizeof(v));
   v.nz = p.nz; v.ncols = p.ncols; v.nnodes = p.nnodes; v.npad = p.npad;
@@ -83,86 +132,91 @@ DevView make_view(bp_ctx* c, const HostPlan& p, bool with_cells, bool mixed) {
   for (uint8_t m : p.dmask) anyd |= (m != 0);
   v.any_dirichlet = anyd;
   const size_t np = (size_t)p.npad;
-  InstParams* inst = arena_get<InstParams>(c, "inst", p.ninst);
-  upload(c, inst, p.inst);
-  v.inst = inst;
-  v.st = arena_get<InstState>(c, "st", p.ninst);
-  v.cnt = arena_get<Counters>(c, "cnt", 1);
-  int* col_inst = arena_get<int>(c, "col_inst", p.ncols); upload(c, col_inst, p.col_inst); v.col_inst = col_inst;
-  int* col_nbr = arena_get<int>(c, "col_nbr", p.col_nbr.size()); upload(c, col_nbr, p.col_nbr); v.col_nbr = col_nbr;
-  int* col_cells = arena_get<int>(c, "col_cells", p.col_cells.size()); upload(c, col_cells, p.col_cells); v.col_cells = col_cells;
-  int* col_ij = arena_get<int>(c, "col_ij", p.col_ij.size()); upload(c, col_ij, p.col_ij); v.col_ij = col_ij;
-  double* col_beta = arena_get<double>(c, "col_beta", p.col_beta.size()); upload(c, col_beta, p.col_beta); v.col_beta = col_beta;
-  double2* load = arena_get<double2>(c, "load", p.load.size()); upload(c, load, p.load); v.load = load;
-  uint8_t* dmask = arena_get<uint8_t>(c, "dmask", p.dmask.size()); upload(c, dmask, p.dmask); v.dmask = dmask;
+#define UP(T, name, vec, field)                           \
+  {                                                       \
+    T* d_ = a.get<T>(s, name, (vec).size());              \
+    upload(s, d_, vec);                                   \
+    v.field = d_;                                         \
+  }
+  UP(InstParams, "inst", p.inst, inst);
+  v.st = a.get<InstState>(s, "st", p.ninst);
+  v.cnt = a.get<Counters>(s, "cnt", 1);
+  UP(int, "col_inst", p.col_inst, col_inst);
+  UP(int, "col_nbr", p.col_nbr, col_nbr);
+  UP(int, "col_cells", p.col_cells, col_cells);
+  UP(int, "col_ij", p.col_ij, col_ij);
+  UP(double, "col_beta", p.col_beta, col_beta);
+  UP(double2, "load", p.load, load);
+  UP(uint8_t, "dmask", p.dmask, dmask);
   if (with_cells) {
-    int* a = arena_get<int>(c, "cell_inst", p.cell_inst.size()); upload(c, a, p.cell_inst); v.cell_inst = a;
-    a = arena_get<int>(c, "cell_ij", p.cell_ij.size()); upload(c, a, p.cell_ij); v.cell_ij = a;
-    a = arena_get<int>(c, "cell_cols", p.cell_cols.size()); upload(c, a, p.cell_cols); v.cell_cols = a;
-    double* d = arena_get<double>(c, "cell_s", p.cell_s.size()); upload(c, d, p.cell_s); v.cell_s = d;
-    d = arena_get<double>(c, "cell_h", p.cell_h.size()); upload(c, d, p.cell_h); v.cell_h = d;
-    d = arena_get<double>(c, "cell_beta", p.cell_beta.size()); upload(c, d, p.cell_beta); v.cell_beta = d;
-    d = arena_get<double>(c, "flwafact", p.flwafact.size()); upload(c, d, p.flwafact); v.flwafact = d;
-    v.qp = arena_get<double>(c, "qp", (size_t)p.nelem * 80);
-    v.efvs = arena_get<double>(c, "efvs", p.nelem);
-    v.badj = arena_get<double>(c, "badj", 4 * np);
+    UP(int, "cell_inst", p.cell_inst, cell_inst);
+    UP(int, "cell_ij", p.cell_ij, cell_ij);
+    UP(int, "cell_cols", p.cell_cols, cell_cols);
+    UP(double, "cell_s", p.cell_s, cell_s);
+    UP(double, "cell_h", p.cell_h, cell_h);
+    UP(double, "cell_beta", p.cell_beta, cell_beta);
+    UP(double, "flwafact", p.flwafact, flwafact);
+    v.qp = a.get<double>(s, "qp", (size_t)p.nelem * 80);
+    v.efvs = a.get<double>(s, "efvs", p.nelem);
+    v.badj = a.get<double>(s, "badj", 4 * np);
   }
-  int* ts = arena_get<int>(c, "tile_start", p.tile_start.size()); upload(c, ts, p.tile_start); v.tile_start = ts;
-  int* ti = arena_get<int>(c, "tile_inst", p.tile_inst.size()); upload(c, ti, p.tile_inst); v.tile_inst = ti;
-  v.A = arena_get<double2>(c, "A", 2 * 27 * np);
-  v.x = arena_get<double2>(c, "x", np);
-  v.b = arena_get<double2>(c, "b", np);
-  v.r = arena_get<double2>(c, "r", np);
-  v.d0 = arena_get<double2>(c, "d0", np);
-  v.d1 = arena_get<double2>(c, "d1", np);
-  v.q = arena_get<double2>(c, "q", np);
-  v.Az = arena_get<double2>(c, "Az", np);
-  v.Dinv = arena_get<double2>(c, "Dinv", np);
-  v.usav = arena_get<double2>(c, "usav", np);
+  UP(int, "tile_start", p.tile_start, tile_start);
+  UP(int, "tile_inst", p.tile_inst, tile_inst);
+#undef UP
+  v.A = a.get<double2>(s, "A", 2 * 27 * np);
+  v.x = a.get<double2>(s, "x", np);
+  v.b = a.get<double2>(s, "b", np);
+  v.r = a.get<double2>(s, "r", np);
+  v.d0 = a.get<double2>(s, "d0", np);
+  v.d1 = a.get<double2>(s, "d1", np);
+  v.q = a.get<double2>(s, "q", np);
+  v.Az = a.get<double2>(s, "Az", np);
+  v.Dinv = a.get<double2>(s, "Dinv", np);
+  v.usav = a.get<double2>(s, "usav", np);
   if (mixed) {
-    v.A32 = arena_get<float2>(c, "A32", 2 * 27 * np);
-    v.scale = arena_get<double2>(c, "scale", np);
-    v.y32 = arena_get<float2>(c, "y32", np);
-    v.r32 = arena_get<float2>(c, "r32", np);
-    v.p32a = arena_get<float2>(c, "p32a", np);
-    v.p32b = arena_get<float2>(c, "p32b", np);
-    v.q32 = arena_get<float2>(c, "q32", np);
+    v.A32 = a.get<float2>(s, "A32", 2 * 27 * np);
+    v.scale = a.get<double2>(s, "scale", np);
+    v.y32 = a.get<float2>(s, "y32", np);
+    v.r32 = a.get<float2>(s, "r32", np);
+    v.p32a = a.get<float2>(s, "p32a", np);
+    v.p32b = a.get<float2>(s, "p32b", np);
+    v.q32 = a.get<float2>(s, "q32", np);
   }
-  v.partials = arena_get<double>(c, "partials", 2 * (size_t)std::max(p.ntiles, 1));
-  v.tile_counter = arena_get<unsigned>(c, "tile_counter", p.ninst);
-  CK(cudaMemsetAsync(v.tile_counter, 0, sizeof(unsigned) * p.ninst, c->stream));
+  v.partials = a.get<double>(s, "partials", 2 * (size_t)std::max(p.ntiles, 1));
+  v.tile_counter = a.get<unsigned>(s, "tile_counter", p.ninst);
+  CK(cudaMemsetAsync(v.tile_counter, 0, sizeof(unsigned) * p.ninst, s));
   return v;
 }
 
-void init_state(bp_ctx* c, const DevView& v, const HostPlan& p, bool picard, bool pcg) {
+void init_state(cudaStream_t s, const DevView& v, const HostPlan& p, bool picard, bool pcg) {
   const int ninst = p.ninst;
   std::vector<InstState> st(ninst);
   int live = 0;
   for (int b = 0; b < ninst; ++b) {
-    InstState& s = st[b];
-    std::memset(&s, 0, sizeof(s));
+    InstState& x = st[b];
+    std::memset(&x, 0, sizeof(x));
     const bool empty = p.inst[b].node_end == p.inst[b].node_begin;
     // no active vertex at all: count_nonzeros_3d = 0, velocity zero
     // (glissade_velo_higher.F90:3191-3220)
-    s.status = empty ? BP_ZERO_MATRIX : BP_OK;
-    s.picard_active = (picard && !empty) ? 1 : 0;
-    s.pcg_active = (pcg && !empty) ? 1 : 0;
-    s.refine_active = s.pcg_active;
-    s.pcg_iter = 1;
-    s.rz = 1.0;
-    s.rz_old = 1.0;
-    s.err = -1.0;
+    x.status = empty ? BP_ZERO_MATRIX : BP_OK;
+    x.picard_active = (picard && !empty) ? 1 : 0;
+    x.pcg_active = (pcg && !empty) ? 1 : 0;
+    x.refine_active = x.pcg_active;
+    x.pcg_iter = 1;
+    x.rz = 1.0;
+    x.rz_old = 1.0;
+    x.err = -1.0;
     live += empty ? 0 : 1;
   }
-  CK(cudaMemcpyAsync(v.st, st.data(), sizeof(InstState) * ninst, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(v.st, st.data(), sizeof(InstState) * ninst, cudaMemcpyHostToDevice, s));
   Counters h{};
   h.picard_active = picard ? live : 0;
   h.pcg_active = pcg ? live : 0;
   h.refine_active = pcg ? live : 0;
-  CK(cudaMemcpyAsync(v.cnt, &h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(v.cnt, &h, sizeof(h), cudaMemcpyHostToDevice, s));
+  CK(cudaStreamSynchronize(s));  // st/h are host temporaries
 }
 
-// Copy the counters to pinned slot `slot` and record its event.
 void snapshot(bp_ctx* c, const DevView& v, int slot) {
   CK(cudaMemcpyAsync(&c->h_cnt[slot], v.cnt, sizeof(Counters), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaEventRecord(c->ev[slot], c->stream));
@@ -179,95 +233,177 @@ int max_pcg_iters(const HostPlan& p) {
   return m;
 }
 
-// FP64 PCG (standard or Chronopoulos-Gear) for all instances with
-// pcg_active, starting after MV_INIT.  Iterations run in chunks that end
-// at a convergence check; the host polls one chunk behind.
-void run_pcg_fp64(bp_ctx* c, const DevView& v, const HostPlan& p) {
+// Launch with optional event timing.
+template <typename F>
+void L(bp_problem* P, int cat, F&& f) {
+  Timing& T = P->timing;
+  if (!T.on) {
+    f();
+    return;
+  }
+  const size_t i = T.cat.size();
+  if (i >= T.pool.size()) {
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    T.pool.push_back({a, b});
+  }
+  CK(cudaEventRecord(T.pool[i].first, P->c->stream));
+  f();
+  CK(cudaEventRecord(T.pool[i].second, P->c->stream));
+  T.cat.push_back(cat);
+}
+
+void collect_timing(bp_problem* P) {
+  Timing& T = P->timing;
+  if (!T.on) return;
+  CK(cudaStreamSynchronize(P->c->stream));
+  for (size_t i = 0; i < T.cat.size(); ++i) {
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, T.pool[i].first, T.pool[i].second));
+    T.ms[T.cat[i]] += ms;
+    T.n[T.cat[i]] += 1;
+  }
+  T.cat.clear();
+}
+
+enum { C_MV = 0, C_UPD = 1, C_CHECK = 2, C_MV32 = 3, C_UPD32 = 4, C_ASM1 = 5, C_ASM2 = 6, C_RHS = 7, C_OTHER = 8 };
+
+// One PCG iteration n (standard or Chronopoulos-Gear), check included.
+void enqueue_iteration(bp_problem* P, int variant, bool check) {
+  const DevView& v = P->v;
+  cudaStream_t s = P->c->stream;
+  if (variant == 3) {
+    L(P, C_MV, [&] { launch_mv(MV_CG1, v, s); });
+    L(P, C_UPD, [&] { launch_cg_update(check, v, s); });
+  } else {
+    L(P, C_MV, [&] { launch_mv(MV_STD_A, v, s); });
+    L(P, C_UPD, [&] { launch_std_update(check, v, s); });
+  }
+  if (check) L(P, C_CHECK, [&] { launch_mv(MV_CHECK, v, s); });
+}
+
+// A whole check chunk (ncheck iterations, the last one checks), captured
+// once into a CUDA graph and replayed.
+void enqueue_chunk(bp_problem* P, int variant, int ncheck) {
+  cudaStream_t s = P->c->stream;
+  if (P->use_graphs && !P->timing.on) {
+    if (!P->chunk_graph) {
+      cudaGraph_t g;
+      CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      for (int j = 0; j < ncheck; ++j) enqueue_iteration(P, variant, j == ncheck - 1);
+      CK(cudaStreamEndCapture(s, &g));
+      CK(cudaGraphInstantiate(&P->chunk_graph, g, 0));
+      CK(cudaGraphDestroy(g));
+    }
+    CK(cudaGraphLaunch(P->chunk_graph, s));
+    return;
+  }
+  for (int j = 0; j < ncheck; ++j) enqueue_iteration(P, variant, j == ncheck - 1);
+}
+
+// FP64 PCG for all instances with pcg_active, after MV_INIT.
+void run_pcg_fp64(bp_problem* P) {
+  const HostPlan& p = P->plan;
+  const DevView& v = P->v;
+  bp_ctx* c = P->c;
   const int variant = p.inst[0].variant;
   const int ncheck = std::max(1, p.inst[0].ncheck);
   const int maxit = max_pcg_iters(p);
   int n = 1;
   if (variant == 3) {
-    launch_mv(MV_CG_FIRST, v, c->stream);
-    launch_cg_first_update(v, c->stream);
+    L(P, C_MV, [&] { launch_mv(MV_CG_FIRST, v, c->stream); });
+    L(P, C_UPD, [&] { launch_cg_first_update(v, c->stream); });
     n = 2;
   }
   int chunk = 0;
   while (n <= maxit + 1) {
-    // iterations n .. next multiple of ncheck
-    do {
-      const bool check = (n % ncheck) == 0;
-      if (variant == 3) {
-        launch_mv(MV_CG1, v, c->stream);
-        launch_cg_update(check, v, c->stream);
-      } else {
-        launch_mv(MV_STD_A, v, c->stream);
-        launch_std_update(check, v, c->stream);
-      }
-      if (check) launch_mv(MV_CHECK, v, c->stream);
-      ++n;
-    } while ((n - 1) % ncheck != 0 && n <= maxit + 1);
-    snapshot(c, v, chunk & 1);
-    if (chunk >= 1) {
-      const Counters h = wait_snapshot(c, (chunk - 1) & 1);
-      if (h.pcg_active <= 0) break;
+    if ((n - 1) % ncheck == 0) {
+      enqueue_chunk(P, variant, ncheck);
+      n += ncheck;
+    } else {  // head chunk of the Chronopoulos-Gear variant
+      do {
+        enqueue_iteration(P, variant, (n % ncheck) == 0);
+        ++n;
+      } while ((n - 1) % ncheck != 0);
     }
+    snapshot(c, v, chunk & 1);
+    if (chunk >= 1 && wait_snapshot(c, (chunk - 1) & 1).pcg_active <= 0) break;
     ++chunk;
   }
   CK(cudaGetLastError());
 }
 
-// Mixed precision linear solve: FP64 refinement around FP32 inner CG.
-void run_mixed(bp_ctx* c, const DevView& v, const HostPlan& p) {
-  launch_mixed_setup(v, c->stream);
+// Mixed precision: FP64 refinement around FP32 inner CG.
+void run_mixed(bp_problem* P) {
+  const HostPlan& p = P->plan;
+  const DevView& v = P->v;
+  bp_ctx* c = P->c;
+  cudaStream_t s = c->stream;
+  L(P, C_OTHER, [&] { launch_mixed_setup(v, s); });
   const int maxit = max_pcg_iters(p);
+  const int inner_chunk = 8;
   for (int ref = 0; ref < 24; ++ref) {
-    CK(cudaMemsetAsync(&v.cnt->pcg_active, 0, sizeof(int), c->stream));
-    launch_refine_resid(v, c->stream);
+    CK(cudaMemsetAsync(&v.cnt->pcg_active, 0, sizeof(int), s));
+    L(P, C_CHECK, [&] { launch_refine_resid(v, s); });
     snapshot(c, v, 0);
-    const Counters h = wait_snapshot(c, 0);
-    if (h.refine_active <= 0) break;
-    int chunk = 0, it = 0;
-    const int inner_chunk = 8;
-    while (it < maxit) {
-      for (int j = 0; j < inner_chunk; ++j) launch_inner(v, c->stream);
-      it += inner_chunk;
-      snapshot(c, v, chunk & 1);
-      if (chunk >= 1) {
-        const Counters hh = wait_snapshot(c, (chunk - 1) & 1);
-        if (hh.pcg_active <= 0) break;
+    if (wait_snapshot(c, 0).refine_active <= 0) break;
+    int chunk = 0;
+    for (int it = 0; it < maxit; it += inner_chunk) {
+      if (P->use_graphs && !P->timing.on) {
+        if (!P->inner_graph) {
+          cudaGraph_t g;
+          CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+          for (int j = 0; j < inner_chunk; ++j) launch_inner(v, s);
+          CK(cudaStreamEndCapture(s, &g));
+          CK(cudaGraphInstantiate(&P->inner_graph, g, 0));
+          CK(cudaGraphDestroy(g));
+        }
+        CK(cudaGraphLaunch(P->inner_graph, s));
+      } else {
+        for (int j = 0; j < inner_chunk; ++j) {
+          L(P, C_MV32, [&] { launch_inner_a(v, s); });
+          L(P, C_UPD32, [&] { launch_inner_b(v, s); });
+        }
       }
+      snapshot(c, v, chunk & 1);
+      if (chunk >= 1 && wait_snapshot(c, (chunk - 1) & 1).pcg_active <= 0) break;
       ++chunk;
     }
-    launch_refine_update(v, c->stream);
+    L(P, C_OTHER, [&] { launch_refine_update(v, s); });
   }
   CK(cudaGetLastError());
 }
 
-// Linear solve of the currently assembled system for active instances.
-void linear_solve(bp_ctx* c, const DevView& v, const HostPlan& p) {
-  if (p.inst[0].precision == BP_MIXED) {
-    run_mixed(c, v, p);
+void linear_solve(bp_problem* P) {
+  if (P->mixed) {
+    run_mixed(P);
   } else {
-    launch_mv(MV_INIT, v, c->stream);
-    run_pcg_fp64(c, v, p);
+    L(P, C_CHECK, [&] { launch_mv(MV_INIT, P->v, P->c->stream); });
+    run_pcg_fp64(P);
   }
 }
 
-int fill_stats(const InstState& s, bp_stats* st) {
-  if (!st) return s.status;
-  std::memset(st, 0, sizeof(*st));
-  st->status = s.status;
-  st->picard_iters = s.picard_iter;
-  st->pcg_iters_total = s.pcg_iters_total;
-  st->pcg_iters_last = s.pcg_iters_last;
-  st->refine_steps_total = s.refine_steps_total;
-  st->converged = s.picard_converged;
-  st->pcg_err_last = s.err;
-  st->resid_velo = s.resid_velo;
-  st->L2_norm = s.L2_norm;
-  st->L2_norm_relative = s.L2_rel;
-  return s.status;
+// The Picard loop of glissade_velo_higher_solve on the device.
+void run_picard(bp_problem* P) {
+  const HostPlan& p = P->plan;
+  const DevView& v = P->v;
+  bp_ctx* c = P->c;
+  cudaStream_t s = c->stream;
+  int max_picard = 1;
+  for (const auto& ip : p.inst) max_picard = std::max(max_picard, ip.maxiter_nonlinear);
+  for (int it = 0; it < max_picard; ++it) {
+    L(P, C_OTHER, [&] { launch_picard_begin(v, s); });
+    L(P, C_OTHER, [&] { launch_save_usav(v, s); });
+    L(P, C_ASM1, [&] { launch_asm_qp(v, s); });
+    L(P, C_ASM2, [&] { launch_asm_rows(v, s); });
+    L(P, C_RHS, [&] { launch_rhs(v, s); });
+    linear_solve(P);
+    L(P, C_OTHER, [&] { launch_picard_check(v, s); });
+    snapshot(c, v, 0);
+    if (wait_snapshot(c, 0).picard_active <= 0) break;
+  }
+  CK(cudaGetLastError());
 }
 
 int final_status(const InstState& s) {
@@ -277,67 +413,105 @@ int final_status(const InstState& s) {
   return BP_OK;
 }
 
-int solve_batch(bp_ctx* c, int n, const bp_inputs* in, double* const* uvel,
-                double* const* vvel, double* const* efvs, bp_stats* stats) {
-  HostPlan p;
-  std::string err;
-  if (!build_plan(in, n, &p, &err)) {
-    c->err = err;
-    return BP_ERR_ARGS;
+void fill_stats(const bp_problem* P, int b, bp_stats* st) {
+  const InstState& s = P->state[b];
+  std::memset(st, 0, sizeof(*st));
+  st->status = final_status(s);
+  st->picard_iters = s.picard_iter;
+  st->pcg_iters_total = s.pcg_iters_total;
+  st->pcg_iters_last = s.pcg_iters_last;
+  st->refine_steps_total = s.refine_steps_total;
+  st->converged = s.picard_converged;
+  st->pcg_err_last = s.err;
+  st->resid_velo = s.resid_velo;
+  st->L2_norm = s.L2_norm;
+  st->L2_norm_relative = s.L2_rel;
+  st->ms_upload = P->ms_upload;
+  st->h2d_bytes = P->h2d_bytes / std::max(1, P->plan.ninst);
+  st->d2h_bytes = P->d2h_bytes / std::max(1, P->plan.ninst);
+  st->ms_pcg = P->ms_solve;
+  st->ms_total = P->ms_upload + P->ms_solve;
+  if (P->timing.on)
+    st->ms_assemble = (float)(P->timing.ms[C_ASM1] + P->timing.ms[C_ASM2] + P->timing.ms[C_RHS]);
+}
+
+int worst_status(const bp_problem* P) {
+  int worst = BP_OK;
+  for (const auto& s0 : P->state) {
+    const int s = final_status(s0);
+    const bool warn = s == BP_WARN_PCG_NOT_CONVERGED || s == BP_WARN_PICARD_NOT_CONVERGED || s == BP_ZERO_MATRIX;
+    if (s == BP_OK) continue;
+    if (worst == BP_OK || !warn) worst = s;
   }
-  const bool mixed = p.inst[0].precision == BP_MIXED;
+  return worst;
+}
+
+bp_problem* problem_new(bp_ctx* c, Arena* arena, int n, const bp_inputs* in, std::string* err) {
+  bp_problem* P = new bp_problem();
+  P->c = c;
+  P->arena = arena ? arena : &P->own;
+  if (!build_plan(in, n, &P->plan, err)) {
+    delete P;
+    return nullptr;
+  }
+  P->mixed = P->plan.inst[0].precision == BP_MIXED;
   CK(cudaEventRecord(c->t0, c->stream));
-  DevView v = make_view(c, p, true, mixed);
-  std::vector<double2> x(p.npad, double2{0.0, 0.0});
-  for (int b = 0; b < n; ++b) gather_velocity(p, b, uvel[b], vvel[b], x.data());
-  CK(cudaMemcpyAsync(v.x, x.data(), sizeof(double2) * p.npad, cudaMemcpyHostToDevice, c->stream));
-  init_state(c, v, p, true, false);
+  g_h2d = 0.0;
+  P->v = make_view(*P->arena, c->stream, P->plan, true, P->mixed);
+  P->h2d_bytes = g_h2d;
+  P->x0 = P->arena->get<double2>(c->stream, "x0", P->plan.npad);
+  CK(cudaMemsetAsync(P->x0, 0, sizeof(double2) * P->plan.npad, c->stream));
+  P->state.resize(n);
+  return P;
+}
+
+void problem_free(bp_problem* P) {
+  if (!P) return;
+  if (P->chunk_graph) cudaGraphExecDestroy(P->chunk_graph);
+  if (P->inner_graph) cudaGraphExecDestroy(P->inner_graph);
+  P->timing.destroy();
+  P->own.release();
+  delete P;
+}
+
+void problem_set_guess(bp_problem* P, double* const* uvel, double* const* vvel) {
+  std::vector<double2> x(P->plan.npad, double2{0.0, 0.0});
+  for (int b = 0; b < P->plan.ninst; ++b) gather_velocity(P->plan, b, uvel[b], vvel[b], x.data());
+  CK(cudaMemcpyAsync(P->x0, x.data(), sizeof(double2) * P->plan.npad, cudaMemcpyHostToDevice, P->c->stream));
+  P->h2d_bytes += sizeof(double2) * (double)P->plan.nnodes;
+  CK(cudaStreamSynchronize(P->c->stream));
+}
+
+void problem_run(bp_problem* P) {
+  bp_ctx* c = P->c;
   CK(cudaEventRecord(c->t1, c->stream));
-  int max_picard = 1;
-  for (const auto& ip : p.inst) max_picard = std::max(max_picard, ip.maxiter_nonlinear);
-  for (int it = 0; it < max_picard; ++it) {
-    launch_picard_begin(v, c->stream);
-    launch_save_usav(v, c->stream);
-    launch_assemble(v, c->stream);
-    linear_solve(c, v, p);
-    launch_picard_check(v, c->stream);
-    snapshot(c, v, 0);
-    const Counters h = wait_snapshot(c, 0);
-    if (h.picard_active <= 0) break;
-  }
+  CK(cudaMemcpyAsync(P->v.x, P->x0, sizeof(double2) * P->plan.npad, cudaMemcpyDeviceToDevice, c->stream));
+  init_state(c->stream, P->v, P->plan, true, false);
+  run_picard(P);
   CK(cudaEventRecord(c->t2, c->stream));
-  CK(cudaMemcpyAsync(x.data(), v.x, sizeof(double2) * p.npad, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(P->state.data(), P->v.st, sizeof(InstState) * P->plan.ninst,
+                     cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  collect_timing(P);
+  cudaEventElapsedTime(&P->ms_solve, c->t1, c->t2);
+}
+
+void problem_get(bp_problem* P, double* const* uvel, double* const* vvel, double* const* efvs) {
+  const HostPlan& p = P->plan;
+  std::vector<double2> x(p.npad);
+  CK(cudaMemcpyAsync(x.data(), P->v.x, sizeof(double2) * p.npad, cudaMemcpyDeviceToHost, P->c->stream));
   std::vector<double> ef;
   if (efvs) {
     ef.resize(std::max(p.nelem, 1));
     if (p.nelem > 0)
-      CK(cudaMemcpyAsync(ef.data(), v.efvs, sizeof(double) * p.nelem, cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaMemcpyAsync(ef.data(), P->v.efvs, sizeof(double) * p.nelem, cudaMemcpyDeviceToHost, P->c->stream));
   }
-  std::vector<InstState> st(n);
-  CK(cudaMemcpyAsync(st.data(), v.st, sizeof(InstState) * n, cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaEventRecord(c->t3, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
-  CK(cudaGetLastError());
-  float ms_up = 0, ms_solve = 0, ms_tot = 0;
-  cudaEventElapsedTime(&ms_up, c->t0, c->t1);
-  cudaEventElapsedTime(&ms_solve, c->t1, c->t2);
-  cudaEventElapsedTime(&ms_tot, c->t0, c->t3);
-  int worst = BP_OK;
-  for (int b = 0; b < n; ++b) {
-    scatter_velocity(p, b, x.data(), uvel[b], vvel[b]);
+  CK(cudaStreamSynchronize(P->c->stream));
+  P->d2h_bytes = sizeof(double2) * (double)p.nnodes + (efvs ? sizeof(double) * (double)p.nelem : 0.0);
+  for (int b = 0; b < p.ninst; ++b) {
+    if (uvel && vvel) scatter_velocity(p, b, x.data(), uvel[b], vvel[b]);
     if (efvs && efvs[b]) scatter_efvs(p, b, ef.data(), efvs[b]);
-    if (stats) {
-      fill_stats(st[b], &stats[b]);
-      stats[b].status = final_status(st[b]);
-      stats[b].ms_upload = ms_up;
-      stats[b].ms_pcg = ms_solve;
-      stats[b].ms_total = ms_tot;
-    }
-    const int s = final_status(st[b]);
-    if (s != BP_OK && (worst == BP_OK || (s != BP_WARN_PCG_NOT_CONVERGED && s != BP_WARN_PICARD_NOT_CONVERGED)))
-      worst = s;
   }
-  return worst;
 }
 
 }  // namespace
@@ -366,9 +540,10 @@ int bp_create(int device, bp_ctx** out) {
     CK(cudaEventCreate(&c->t1));
     CK(cudaEventCreate(&c->t2));
     CK(cudaEventCreate(&c->t3));
+    CK(cudaEventCreate(&c->r0));
+    CK(cudaEventCreate(&c->r1));
     CK(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device));
     CK(bp::upload_ref_tables());
-    c->tables_ready = true;
   } catch (const CudaError& e) {
     std::fprintf(stderr, "bp_create: %s failed: %s\n", e.what, cudaGetErrorString(e.e));
     bp_destroy(c);
@@ -382,11 +557,11 @@ int bp_destroy(bp_ctx* c) {
   if (!c) return BP_OK;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
-  for (auto& kv : c->arena) cudaFree(kv.second.first);
+  c->arena.release();
   if (c->h_cnt) cudaFreeHost(c->h_cnt);
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);
-  for (cudaEvent_t e : {c->t0, c->t1, c->t2, c->t3})
+  for (cudaEvent_t e : {c->t0, c->t1, c->t2, c->t3, c->r0, c->r1})
     if (e) cudaEventDestroy(e);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -395,23 +570,151 @@ int bp_destroy(bp_ctx* c) {
 
 const char* bp_last_error(const bp_ctx* c) { return c ? c->err.c_str() : "no context"; }
 
-#define GUARD_BEGIN                 \
-  if (!c) return BP_ERR_ARGS;       \
-  c->err.clear();                   \
+#define GUARD_BEGIN(ctx)            \
+  bp_ctx* c_ = (ctx);               \
+  if (!c_) return BP_ERR_ARGS;      \
+  c_->err.clear();                  \
   try {                             \
-    CK(cudaSetDevice(c->device));
-#define GUARD_END                                                     \
-  }                                                                   \
-  catch (const CudaError& e) {                                        \
-    c->err = std::string(e.what) + ": " + cudaGetErrorString(e.e);    \
-    return BP_ERR_CUDA;                                               \
+    CK(cudaSetDevice(c_->device));
+#define GUARD_END                                                      \
+  }                                                                    \
+  catch (const CudaError& e) {                                         \
+    c_->err = std::string(e.what) + ": " + cudaGetErrorString(e.e);    \
+    return BP_ERR_CUDA;                                                \
+  }                                                                    \
+  return BP_ERR_CUDA;
+
+int bp_problem_create(bp_ctx* c, int n, const bp_inputs* in, bp_problem** out) {
+  GUARD_BEGIN(c)
+  if (!out || n < 1 || !in) return BP_ERR_ARGS;
+  *out = nullptr;
+  std::string err;
+  bp_problem* P = problem_new(c, nullptr, n, in, &err);
+  if (!P) {
+    c->err = err;
+    return BP_ERR_ARGS;
   }
+  CK(cudaEventRecord(c->t3, c->stream));
+  CK(cudaEventSynchronize(c->t3));
+  cudaEventElapsedTime(&P->ms_upload, c->t0, c->t3);
+  *out = P;
+  return BP_OK;
+  GUARD_END
+}
+
+int bp_problem_set_guess(bp_problem* P, double* const* uvel, double* const* vvel) {
+  if (!P) return BP_ERR_ARGS;
+  GUARD_BEGIN(P->c)
+  if (!uvel || !vvel) return BP_ERR_ARGS;
+  problem_set_guess(P, uvel, vvel);
+  return BP_OK;
+  GUARD_END
+}
+
+int bp_problem_run(bp_problem* P, bp_stats* stats) {
+  if (!P) return BP_ERR_ARGS;
+  GUARD_BEGIN(P->c)
+  problem_run(P);
+  if (stats)
+    for (int b = 0; b < P->plan.ninst; ++b) fill_stats(P, b, &stats[b]);
+  return worst_status(P);
+  GUARD_END
+}
+
+int bp_problem_get(bp_problem* P, double* const* uvel, double* const* vvel, double* const* efvs) {
+  if (!P) return BP_ERR_ARGS;
+  GUARD_BEGIN(P->c)
+  problem_get(P, uvel, vvel, efvs);
+  return BP_OK;
+  GUARD_END
+}
+
+int bp_problem_destroy(bp_problem* P) {
+  if (!P) return BP_OK;
+  cudaSetDevice(P->c->device);
+  cudaStreamSynchronize(P->c->stream);
+  problem_free(P);
+  return BP_OK;
+}
+
+int bp_timer_start(bp_ctx* c) {
+  GUARD_BEGIN(c)
+  CK(cudaEventRecord(c->r0, c->stream));
+  return BP_OK;
+  GUARD_END
+}
+
+int bp_timer_stop(bp_ctx* c, float* ms) {
+  GUARD_BEGIN(c)
+  CK(cudaEventRecord(c->r1, c->stream));
+  CK(cudaEventSynchronize(c->r1));
+  float t = 0.f;
+  CK(cudaEventElapsedTime(&t, c->r0, c->r1));
+  if (ms) *ms = t;
+  return BP_OK;
+  GUARD_END
+}
+
+int bp_problem_timing(bp_problem* P, int enable) {
+  if (!P) return BP_ERR_ARGS;
+  P->timing.on = enable != 0;
+  P->timing.reset();
+  return BP_OK;
+}
+
+int bp_problem_kernel_times(bp_problem* P, double* ms, int* launches) {
+  if (!P) return BP_ERR_ARGS;
+  for (int i = 0; i < BP_NUM_KERNEL_CATEGORIES; ++i) {
+    if (ms) ms[i] = P->timing.ms[i];
+    if (launches) launches[i] = P->timing.n[i];
+  }
+  return BP_OK;
+}
+
+int bp_problem_info(bp_problem* P, long* nodes, long* cols, long* elems, double* mvb64,
+                    double* mvb32) {
+  if (!P) return BP_ERR_ARGS;
+  const double N = (double)P->plan.nnodes;
+  if (nodes) *nodes = P->plan.nnodes;
+  if (cols) *cols = P->plan.ncols;
+  if (elems) *elems = P->plan.nelem;
+  // algorithmic bytes of one fused PCG matvec launch per node:
+  // standard: 108 FP64 coefficients + r, D^-1, d_old read + d, q written
+  // Chronopoulos-Gear: 108 coefficients + r, D^-1 read + Az written
+  const bool cg = P->plan.inst[0].variant == 3;
+  if (mvb64) *mvb64 = N * (108.0 * 8.0 + (cg ? 3.0 : 5.0) * 16.0);
+  // FP32 inner: 108 FP32 coefficients + r, p_old read + p, q written (8 B each)
+  if (mvb32) *mvb32 = N * (108.0 * 4.0 + 4.0 * 8.0);
+  return BP_OK;
+}
 
 int bp_batch_solve(bp_ctx* c, int n, const bp_inputs* in, double* const* uvel,
                    double* const* vvel, double* const* efvs, bp_stats* stats) {
-  GUARD_BEGIN
+  GUARD_BEGIN(c)
   if (n < 1 || !in || !uvel || !vvel) return BP_ERR_ARGS;
-  return solve_batch(c, n, in, uvel, vvel, efvs, stats);
+  std::string err;
+  bp_problem* P = problem_new(c, &c->arena, n, in, &err);
+  if (!P) {
+    c->err = err;
+    return BP_ERR_ARGS;
+  }
+  int rc = BP_OK;
+  try {
+    problem_set_guess(P, uvel, vvel);
+    CK(cudaEventRecord(c->t3, c->stream));
+    CK(cudaEventSynchronize(c->t3));
+    cudaEventElapsedTime(&P->ms_upload, c->t0, c->t3);
+    problem_run(P);
+    problem_get(P, uvel, vvel, efvs);
+    if (stats)
+      for (int b = 0; b < n; ++b) fill_stats(P, b, &stats[b]);
+    rc = worst_status(P);
+  } catch (...) {
+    problem_free(P);
+    throw;
+  }
+  problem_free(P);
+  return rc;
   GUARD_END
 }
 
@@ -429,20 +732,22 @@ int bp_pcg(bp_ctx* c, int nx, int ny, int nz, int periodic,
            const double* bv, double* xu, double* xv, int precond, int variant,
            double tol, int maxiters, int ncheck, int precision, double* err,
            int* niters) {
-  GUARD_BEGIN
+  GUARD_BEGIN(c)
   if (!active_vertex || !Auu || !Auv || !Avu || !Avv || !bu || !bv || !xu || !xv)
     return BP_ERR_ARGS;
   if (precond != 0 && precond != 1) {
     c->err = "bp_pcg: precond must be 0 or 1";
     return BP_ERR_ARGS;
   }
-  HostPlan p;
+  bp_problem P;
+  P.c = c;
+  P.arena = &c->arena;
   std::string e;
-  if (!build_column_plan(nx, ny, nz, periodic, active_vertex, &p, &e)) {
+  if (!build_column_plan(nx, ny, nz, periodic, active_vertex, &P.plan, &e)) {
     c->err = e;
     return BP_ERR_ARGS;
   }
-  InstParams& ip = p.inst[0];
+  InstParams& ip = P.plan.inst[0];
   ip.precond = precond;
   ip.variant = variant == 3 ? 3 : 2;
   ip.pcg_tol = tol;
@@ -450,28 +755,30 @@ int bp_pcg(bp_ctx* c, int nx, int ny, int nz, int periodic,
   ip.ncheck = ncheck > 0 ? ncheck : 5;
   ip.precision = precision;
   ip.inner_tol = 1.0e-4;
-  const bool mixed = precision == BP_MIXED;
-  DevView v = make_view(c, p, false, mixed);
-  std::vector<double2> A(2 * 27 * (size_t)p.npad);
-  gather_matrix(p, Auu, Auv, Avu, Avv, A.data());
+  P.mixed = precision == BP_MIXED;
+  P.use_graphs = false;
+  P.v = make_view(*P.arena, c->stream, P.plan, false, P.mixed);
+  const DevView& v = P.v;
+  std::vector<double2> A(2 * 27 * (size_t)P.plan.npad);
+  gather_matrix(P.plan, Auu, Auv, Avu, Avv, A.data());
   CK(cudaMemcpyAsync(v.A, A.data(), sizeof(double2) * A.size(), cudaMemcpyHostToDevice, c->stream));
-  std::vector<double2> x(p.npad, double2{0, 0}), b(p.npad, double2{0, 0});
-  gather_velocity(p, 0, xu, xv, x.data());
-  gather_velocity(p, 0, bu, bv, b.data());
-  CK(cudaMemcpyAsync(v.x, x.data(), sizeof(double2) * p.npad, cudaMemcpyHostToDevice, c->stream));
-  CK(cudaMemcpyAsync(v.b, b.data(), sizeof(double2) * p.npad, cudaMemcpyHostToDevice, c->stream));
-  init_state(c, v, p, false, true);
+  std::vector<double2> x(P.plan.npad, double2{0, 0}), b(P.plan.npad, double2{0, 0});
+  gather_velocity(P.plan, 0, xu, xv, x.data());
+  gather_velocity(P.plan, 0, bu, bv, b.data());
+  CK(cudaMemcpyAsync(v.x, x.data(), sizeof(double2) * P.plan.npad, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(v.b, b.data(), sizeof(double2) * P.plan.npad, cudaMemcpyHostToDevice, c->stream));
+  init_state(c->stream, v, P.plan, false, true);
   launch_dinv(v, precond, c->stream);
   launch_bb(v, c->stream);
-  linear_solve(c, v, p);
-  CK(cudaMemcpyAsync(x.data(), v.x, sizeof(double2) * p.npad, cudaMemcpyDeviceToHost, c->stream));
+  linear_solve(&P);
+  CK(cudaMemcpyAsync(x.data(), v.x, sizeof(double2) * P.plan.npad, cudaMemcpyDeviceToHost, c->stream));
   InstState st;
   CK(cudaMemcpyAsync(&st, v.st, sizeof(st), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   CK(cudaGetLastError());
-  scatter_velocity(p, 0, x.data(), xu, xv);
+  scatter_velocity(P.plan, 0, x.data(), xu, xv);
   if (err) *err = st.err;
-  if (niters) *niters = mixed ? st.pcg_iters_total : st.pcg_iters_last;
+  if (niters) *niters = P.mixed ? st.pcg_iters_total : st.pcg_iters_last;
   if (st.status != BP_OK) return st.status;
   return st.pcg_converged ? BP_OK : BP_WARN_PCG_NOT_CONVERGED;
   GUARD_END
@@ -481,7 +788,7 @@ int bp_matvec(bp_ctx* c, int nx, int ny, int nz, int periodic,
               const int* active_vertex, const double* Auu, const double* Auv,
               const double* Avu, const double* Avv, const double* xu,
               const double* xv, double* yu, double* yv) {
-  GUARD_BEGIN
+  GUARD_BEGIN(c)
   if (!active_vertex || !Auu || !Auv || !Avu || !Avv || !xu || !xv || !yu || !yv)
     return BP_ERR_ARGS;
   HostPlan p;
@@ -490,7 +797,7 @@ int bp_matvec(bp_ctx* c, int nx, int ny, int nz, int periodic,
     c->err = e;
     return BP_ERR_ARGS;
   }
-  DevView v = make_view(c, p, false, false);
+  DevView v = make_view(c->arena, c->stream, p, false, false);
   std::vector<double2> A(2 * 27 * (size_t)p.npad);
   gather_matrix(p, Auu, Auv, Avu, Avv, A.data());
   CK(cudaMemcpyAsync(v.A, A.data(), sizeof(double2) * A.size(), cudaMemcpyHostToDevice, c->stream));
@@ -512,7 +819,7 @@ int bp_matvec(bp_ctx* c, int nx, int ny, int nz, int periodic,
 int bp_assemble(bp_ctx* c, const bp_inputs* in, const double* uvel,
                 const double* vvel, double* Auu, double* Auv, double* Avu,
                 double* Avv, double* bu, double* bv, double* efvs) {
-  GUARD_BEGIN
+  GUARD_BEGIN(c)
   if (!in || !uvel || !vvel) return BP_ERR_ARGS;
   HostPlan p;
   std::string e;
@@ -520,13 +827,15 @@ int bp_assemble(bp_ctx* c, const bp_inputs* in, const double* uvel,
     c->err = e;
     return BP_ERR_ARGS;
   }
-  DevView v = make_view(c, p, true, false);
+  DevView v = make_view(c->arena, c->stream, p, true, false);
   std::vector<double2> x(p.npad, double2{0, 0});
   gather_velocity(p, 0, uvel, vvel, x.data());
   CK(cudaMemcpyAsync(v.x, x.data(), sizeof(double2) * p.npad, cudaMemcpyHostToDevice, c->stream));
-  init_state(c, v, p, true, false);
+  init_state(c->stream, v, p, true, false);
   launch_picard_begin(v, c->stream);
-  launch_assemble(v, c->stream);
+  launch_asm_qp(v, c->stream);
+  launch_asm_rows(v, c->stream);
+  launch_rhs(v, c->stream);
   std::vector<double2> A(2 * 27 * (size_t)p.npad), b(p.npad);
   std::vector<double> ef(std::max(p.nelem, 1));
   CK(cudaMemcpyAsync(A.data(), v.A, sizeof(double2) * A.size(), cudaMemcpyDeviceToHost, c->stream));
@@ -543,7 +852,7 @@ int bp_assemble(bp_ctx* c, const bp_inputs* in, const double* uvel,
   if (bv) std::memset(bv, 0, sizeof(double) * tot);
   scatter_vector(p, 0, b.data(), bu, bv);
   if (efvs) scatter_efvs(p, 0, ef.data(), efvs);
-  return st.status == BP_ZERO_MATRIX ? BP_ZERO_MATRIX : st.status;
+  return st.status;
   GUARD_END
 }
 

@@ -833,14 +833,21 @@ cudaError_t upload_ref_tables() {
 
 void launch_picard_begin(const DevView& v, cudaStream_t s) { k_picard_begin<<<1, 256, 0, s>>>(v); }
 void launch_save_usav(const DevView& v, cudaStream_t s) { k_save_usav<<<tile_grid(v), kTile, 0, s>>>(v); }
-void launch_assemble(const DevView& v, cudaStream_t s) {
+void launch_asm_qp(const DevView& v, cudaStream_t s) {
   if (v.nelem > 0) {
     const long threads = (long)v.nelem * 8;
     k_asm_qp<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(v);
   }
+}
+void launch_asm_rows(const DevView& v, cudaStream_t s) {
   dim3 g(tile_grid(v), 4);
   k_asm_rows<<<g, kTile, 0, s>>>(v);
-  k_rhs<<<tile_grid(v), kTile, 0, s>>>(v);
+}
+void launch_rhs(const DevView& v, cudaStream_t s) { k_rhs<<<tile_grid(v), kTile, 0, s>>>(v); }
+void launch_assemble(const DevView& v, cudaStream_t s) {
+  launch_asm_qp(v, s);
+  launch_asm_rows(v, s);
+  launch_rhs(v, s);
 }
 void launch_mv(int mode, const DevView& v, cudaStream_t s) {
   const int g = tile_grid(v);
@@ -873,9 +880,11 @@ void launch_mixed_setup(const DevView& v, cudaStream_t s) {
 void launch_refine_resid(const DevView& v, cudaStream_t s) {
   k_refine_resid<<<tile_grid(v), kTile, 0, s>>>(v);
 }
+void launch_inner_a(const DevView& v, cudaStream_t s) { k_inner_a<<<tile_grid(v), kTile, 0, s>>>(v); }
+void launch_inner_b(const DevView& v, cudaStream_t s) { k_inner_b<<<tile_grid(v), kTile, 0, s>>>(v); }
 void launch_inner(const DevView& v, cudaStream_t s) {
-  k_inner_a<<<tile_grid(v), kTile, 0, s>>>(v);
-  k_inner_b<<<tile_grid(v), kTile, 0, s>>>(v);
+  launch_inner_a(v, s);
+  launch_inner_b(v, s);
 }
 void launch_refine_update(const DevView& v, cudaStream_t s) {
   k_refine_update<<<tile_grid(v), kTile, 0, s>>>(v);

@@ -16,6 +16,9 @@ void set_grid_cap(int cap);
 void launch_picard_begin(const DevView& v, cudaStream_t s);
 void launch_save_usav(const DevView& v, cudaStream_t s);
 void launch_assemble(const DevView& v, cudaStream_t s);
+void launch_asm_qp(const DevView& v, cudaStream_t s);
+void launch_asm_rows(const DevView& v, cudaStream_t s);
+void launch_rhs(const DevView& v, cudaStream_t s);
 void launch_mv(int mode, const DevView& v, cudaStream_t s);
 void launch_std_update(bool check, const DevView& v, cudaStream_t s);
 void launch_cg_first_update(const DevView& v, cudaStream_t s);
@@ -24,6 +27,8 @@ void launch_picard_check(const DevView& v, cudaStream_t s);
 void launch_mixed_setup(const DevView& v, cudaStream_t s);
 void launch_refine_resid(const DevView& v, cudaStream_t s);
 void launch_inner(const DevView& v, cudaStream_t s);
+void launch_inner_a(const DevView& v, cudaStream_t s);
+void launch_inner_b(const DevView& v, cudaStream_t s);
 void launch_refine_update(const DevView& v, cudaStream_t s);
 void launch_matvec_plain(const DevView& v, const double2* x, double2* y, cudaStream_t s);
 void launch_dinv(const DevView& v, int precond, cudaStream_t s);

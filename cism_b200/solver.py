@@ -64,7 +64,8 @@ class Stats(C.Structure):
         ("pcg_iters_last", C.c_int), ("refine_steps_total", C.c_int), ("converged", C.c_int),
         ("pcg_err_last", C.c_double), ("resid_velo", C.c_double), ("L2_norm", C.c_double),
         ("L2_norm_relative", C.c_double), ("ms_upload", C.c_float), ("ms_assemble", C.c_float),
-        ("ms_pcg", C.c_float), ("ms_total", C.c_float),
+        ("ms_pcg", C.c_float), ("ms_total", C.c_float), ("h2d_bytes", C.c_double),
+        ("d2h_bytes", C.c_double),
     ]
 
     def as_dict(self):
@@ -119,6 +120,16 @@ def lib():
         L.bp_assemble.argtypes = [C.c_void_p, C.POINTER(Inputs)] + [_dp] * 9
         L.bp_setup.argtypes = [C.POINTER(Model), C.POINTER(SetupArrays), _dp, _dp, C.POINTER(Inputs)]
         L.bp_velo_higher_solve.argtypes = [C.c_void_p, C.POINTER(Model), _dp, _dp, _dp, C.POINTER(Stats)]
+        L.bp_problem_create.argtypes = [C.c_void_p, C.c_int, C.POINTER(Inputs), C.POINTER(C.c_void_p)]
+        L.bp_problem_set_guess.argtypes = [C.c_void_p, C.POINTER(_dp), C.POINTER(_dp)]
+        L.bp_problem_run.argtypes = [C.c_void_p, C.POINTER(Stats)]
+        L.bp_problem_get.argtypes = [C.c_void_p, C.POINTER(_dp), C.POINTER(_dp), C.POINTER(_dp)]
+        L.bp_problem_destroy.argtypes = [C.c_void_p]
+        L.bp_problem_timing.argtypes = [C.c_void_p, C.c_int]
+        L.bp_problem_kernel_times.argtypes = [C.c_void_p, _dp, _ip]
+        L.bp_problem_info.argtypes = [C.c_void_p] + [C.POINTER(C.c_long)] * 3 + [_dp, _dp]
+        L.bp_timer_start.argtypes = [C.c_void_p]
+        L.bp_timer_stop.argtypes = [C.c_void_p, C.POINTER(C.c_float)]
         _lib = L
     return _lib
 
@@ -264,6 +275,17 @@ class Context:
         self._check(rc)
         return us, vs, es, [s.as_dict() for s in st]
 
+    def problem(self, preps: Sequence[Prepared]) -> "Problem":
+        return Problem(self, preps)
+
+    def timer_start(self):
+        lib().bp_timer_start(self.h)
+
+    def timer_stop(self) -> float:
+        ms = C.c_float()
+        lib().bp_timer_stop(self.h, C.byref(ms))
+        return ms.value
+
     # -- matrix-level entry points -------------------------------------------
     def pcg_solve(self, m: configs.BPModel, active_vertex, A, bu, bv, xu, xv, precond=1,
                   variant=2, tol=1e-8, maxiters=200, ncheck=5, precision=FP64):
@@ -302,6 +324,75 @@ class Context:
                                _p(bu), _p(bv), _p(efvs))
         self._check(rc, allow=(0, 5))
         return A, bu, bv, efvs
+
+
+KERNEL_CATEGORIES = ("pcg_matvec_fp64", "pcg_update_fp64", "residual_check_fp64", "inner_matvec_fp32",
+                     "inner_update_fp32", "assembly_qp", "assembly_rows", "rhs", "other")
+
+
+class Problem:
+    """A compiled solve (or batch) resident in device memory (bp_problem)."""
+
+    def __init__(self, ctx: "Context", preps: Sequence[Prepared]):
+        self.ctx = ctx
+        self.preps = list(preps)
+        self.n = len(self.preps)
+        self._arr = (Inputs * self.n)(*[p.inputs for p in self.preps])
+        h = C.c_void_p()
+        rc = lib().bp_problem_create(ctx.h, self.n, self._arr, C.byref(h))
+        ctx._check(rc, allow=(0,))
+        self.h = h
+
+    def set_guess(self, uvels, vvels):
+        us = [_f64(u) for u in uvels]
+        vs = [_f64(v) for v in vvels]
+        rc = lib().bp_problem_set_guess(self.h, (_dp * self.n)(*[_p(a) for a in us]),
+                                        (_dp * self.n)(*[_p(a) for a in vs]))
+        self.ctx._check(rc, allow=(0,))
+
+    def run(self):
+        st = (Stats * self.n)()
+        rc = lib().bp_problem_run(self.h, st)
+        self.ctx._check(rc)
+        return [s.as_dict() for s in st]
+
+    def get(self, want_efvs=False):
+        us = [np.zeros(p.model.vshape3) for p in self.preps]
+        vs = [np.zeros(p.model.vshape3) for p in self.preps]
+        es = [np.zeros((p.model.ny, p.model.nx, p.model.nz - 1)) for p in self.preps] if want_efvs else None
+        rc = lib().bp_problem_get(self.h, (_dp * self.n)(*[_p(a) for a in us]),
+                                  (_dp * self.n)(*[_p(a) for a in vs]),
+                                  (_dp * self.n)(*[_p(a) for a in es]) if es else C.cast(None, C.POINTER(_dp)))
+        self.ctx._check(rc, allow=(0,))
+        return us, vs, es
+
+    def timing(self, enable: bool):
+        lib().bp_problem_timing(self.h, 1 if enable else 0)
+
+    def kernel_times(self):
+        ms = (C.c_double * len(KERNEL_CATEGORIES))()
+        n = (C.c_int * len(KERNEL_CATEGORIES))()
+        lib().bp_problem_kernel_times(self.h, ms, n)
+        return {k: (ms[i], n[i]) for i, k in enumerate(KERNEL_CATEGORIES)}
+
+    def info(self):
+        nodes, cols, elems = C.c_long(), C.c_long(), C.c_long()
+        b64, b32 = C.c_double(), C.c_double()
+        lib().bp_problem_info(self.h, C.byref(nodes), C.byref(cols), C.byref(elems), C.byref(b64),
+                              C.byref(b32))
+        return {"nodes": nodes.value, "columns": cols.value, "elements": elems.value,
+                "matvec_bytes_fp64": b64.value, "matvec_bytes_fp32": b32.value}
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().bp_problem_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 _default_ctx: Optional[Context] = None

@@ -95,6 +95,7 @@ typedef struct {
   double resid_velo;            /* last Picard velocity criterion */
   double L2_norm, L2_norm_relative; /* |Ax-b| before the last linear solve */
   float ms_upload, ms_assemble, ms_pcg, ms_total;
+  double h2d_bytes, d2h_bytes;  /* host<->device bytes moved by this call */
 } bp_stats;
 
 /* Context: one CUDA device, one stream, persistent device buffers. */
@@ -141,6 +142,43 @@ int bp_matvec(bp_ctx *ctx, int nx, int ny, int nz, int periodic,
 int bp_assemble(bp_ctx *ctx, const bp_inputs *in, const double *uvel,
                 const double *vvel, double *Auu, double *Auv, double *Avu,
                 double *Avv, double *bu, double *bv, double *efvs);
+
+/* ------------------------------------------------------------------
+ * Resident problems: the compiled inputs of one solve (or a batch) kept
+ * in device memory across runs, e.g. for repeated solves on one geometry.
+ * The reference has no counterpart (it recomputes everything per call);
+ * bp_solve is bp_problem_create + set_guess + run + get + destroy.
+ * ------------------------------------------------------------------ */
+typedef struct bp_problem bp_problem;
+
+int bp_problem_create(bp_ctx *ctx, int n, const bp_inputs *in, bp_problem **out);
+/* Upload an initial guess (n arrays (nz,nx-1,ny-1)); it is kept on the
+ * device and restored at the start of every bp_problem_run. */
+int bp_problem_set_guess(bp_problem *p, double *const *uvel, double *const *vvel);
+/* Run the Picard solve from the stored guess entirely on device data;
+ * stats (array of n, may be NULL) are filled at the end. */
+int bp_problem_run(bp_problem *p, bp_stats *stats);
+/* Copy the solution (and efvs if non-NULL) back to the host. */
+int bp_problem_get(bp_problem *p, double *const *uvel, double *const *vvel,
+                   double *const *efvs);
+int bp_problem_destroy(bp_problem *p);
+
+/* Kernel timing with CUDA events on the solver's stream, per category, for
+ * the runs made while enabled (CUDA graphs are bypassed while enabled).
+ * Categories: 0 FP64 PCG matvec, 1 FP64 PCG vector update, 2 FP64
+ * residual check, 3 FP32 inner matvec, 4 FP32 inner update, 5 assembly
+ * pass 1, 6 assembly pass 2, 7 right-hand side, 8 other. */
+#define BP_NUM_KERNEL_CATEGORIES 9
+int bp_problem_timing(bp_problem *p, int enable);
+/* Device-side wall clock of a region of work on the context's stream:
+ * CUDA events recorded at start and stop (ms). */
+int bp_timer_start(bp_ctx *ctx);
+int bp_timer_stop(bp_ctx *ctx, float *ms);
+int bp_problem_kernel_times(bp_problem *p, double *ms, int *launches);
+/* Node count and, per FP64 matvec launch, the algorithmic bytes moved. */
+int bp_problem_info(bp_problem *p, long *nodes, long *active_columns,
+                    long *elements, double *matvec_bytes_fp64,
+                    double *matvec_bytes_fp32);
 
 /* ------------------------------------------------------------------
  * Host-side mirror of the setup part of glissade_velo_higher_solve, for
