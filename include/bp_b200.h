@@ -143,6 +143,26 @@ int bp_assemble(bp_ctx *ctx, const bp_inputs *in, const double *uvel,
                 const double *vvel, double *Auu, double *Auv, double *Avu,
                 double *Avv, double *bu, double *bv, double *efvs);
 
+/* Residual resid = A x - b on owned active rows, with |A x - b|, |b| and
+ * their ratio in norms[0..2] -- without allocating any device memory.
+ * No counterpart in the reference: it is for callers that own all device
+ * memory themselves (a fixed pool, or code that must not hit the implicit
+ * device synchronisation of cudaMalloc/cudaFree inside a time step).
+ * Every pointer is a DEVICE pointer in the reference layout above (halo
+ * included, x halo-consistent); stream is a cudaStream_t (NULL = default).
+ * Work is enqueued on the stream and not waited for.  The reduction scratch
+ * is a fixed file-scope device array shared by all calls: at most
+ * nz*(nx-1)*(ny-1) = 16,777,216 rows (larger: BP_ERR_ARGS); calls that
+ * overlap on the GPU race on it and must be serialised; the first call on
+ * a device looks up the array's address and should precede any stream
+ * capture. */
+int bp_residual_noalloc(int nx, int ny, int nz, int periodic,
+                        const int *active_vertex, const double *Auu,
+                        const double *Auv, const double *Avu, const double *Avv,
+                        const double *xu, const double *xv, const double *bu,
+                        const double *bv, double *resid_u, double *resid_v,
+                        double *norms, void *stream);
+
 /* ------------------------------------------------------------------
  * Resident problems: the compiled inputs of one solve (or a batch) kept
  * in device memory across runs, e.g. for repeated solves on one geometry.
