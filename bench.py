@@ -57,11 +57,15 @@ def parse_args():
     ap.add_argument("--workload", default="c1", choices=sorted(WORKLOAD_DESC))
     ap.add_argument("--precision", default="best", choices=["best", "fp64", "mixed"])
     ap.add_argument("--pcg-maxiters", type=int, default=3000)
+    ap.add_argument("--mixed-switch", type=float, default=1e-6,
+                    help="mixed path: true residual below which the Krylov matvec uses FP64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-run", action="store_true",
                     help="one untimed solve (for ncu launch lists / captures)")
     ap.add_argument("--picard-cap", type=int, default=0,
                     help="with --profile-run: stop after this many Picard iterations")
+    ap.add_argument("--kernel-sweep", action="store_true",
+                    help="time matvec storage / occupancy / grid variants on the workload")
     return ap.parse_args()
 
 
@@ -250,7 +254,7 @@ def run_ours(args, D):
     sol = {}
     for path in paths:
         prec = solver.MIXED if path == "mixed" else solver.FP64
-        prep, u0, v0 = solver.prepare(m, precision=prec, inner_tol=1e-4)
+        prep, u0, v0 = solver.prepare(m, precision=prec, inner_tol=args.mixed_switch)
         prob = ctx.problem([prep])
         prob.set_guess([u0], [v0])
         for _ in range(args.warmup):
@@ -271,8 +275,10 @@ def run_ours(args, D):
         prob.timing(True)
         st_t = prob.run()[0]
         kt = prob.kernel_times()
+        n64, n32, minb, grid = prob.mv_nodes()
         prob.timing(False)
         info = prob.info()
+        info.update({"mv_nodes_fp64": n64, "mv_nodes_fp32": n32, "tuned_minb": minb, "tuned_grid": grid})
         launches = sum(n for _, n in kt.values())
         res[path] = {"value": D.world * args.steps / (ms_max / 1000.0), "ms_per_step": ms_max / args.steps,
                      "status": st["status"], "picard_iters": st["picard_iters"],
@@ -306,20 +312,28 @@ def run_ours(args, D):
     e2e = {"value": D.world * args.steps / (ms_e / 1000.0), "unit": UNIT,
            "h2d_bytes_per_step": int(st_e["h2d_bytes"]), "d2h_bytes_per_step": int(st_e["d2h_bytes"]),
            "call": "bp_solve (C ABI) on host arrays"}
-    # roofline of the dominant kernel
-    cat = "inner_matvec_fp32" if head == "mixed" else "pcg_matvec_fp64"
-    kms, kn = H["kernel_times"][cat]
-    bytes_launch = H["info"]["matvec_bytes_fp32" if head == "mixed" else "matvec_bytes_fp64"]
+    # roofline of the dominant kernel: the Krylov matvec (FP32 matrix until
+    # the true residual reaches the switch tolerance on the mixed path)
+    kms, kn = H["kernel_times"]["pcg_matvec_fp64"]
+    info = H["info"]
+    N = info["nodes"]
+    b64 = info["matvec_bytes_fp64"] / N
+    b32 = info["matvec_bytes_fp32"] / N
+    total_bytes = info["mv_nodes_fp64"] * b64 + info["mv_nodes_fp32"] * b32
+    bytes_launch = total_bytes / max(kn, 1)
     peak, peak_src = measured_peaks()
     avg_s = (kms / max(kn, 1)) / 1000.0
-    achieved = bytes_launch / avg_s / 1e9 if kn else 0.0
-    traffic = matvec_traffic(H["info"]["nodes"], head)
-    roof = {"bound": "hbm", "kernel": ("k_inner_a (FP32 inner CG matvec)" if head == "mixed"
-                                       else "k_mv<MV_STD_A> (fused d-update + FP64 matvec + (d,q))"),
+    achieved = total_bytes / (kms / 1000.0) / 1e9 if kn else 0.0
+    traffic = matvec_traffic(N, head)
+    roof = {"bound": "hbm",
+            "kernel": ("k_std_mv<ST_SYM32> (Krylov q = A d, FP32 symmetric matrix, FP64 at the end)"
+                       if head == "mixed" else "k_std_mv<ST_SYM> (Krylov q = A d, FP64 symmetric matrix)"),
             "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)",
-            "traffic": traffic, "algorithmic_bytes_per_launch": bytes_launch,
-            "avg_launch_us": round(avg_s * 1e6, 2), "launches_timed": kn}
+            "traffic": traffic, "algorithmic_bytes_per_launch": round(bytes_launch),
+            "avg_launch_us": round(avg_s * 1e6, 2), "launches_timed": kn,
+            "fp32_share": round(info["mv_nodes_fp32"] / max(1.0, info["mv_nodes_fp32"] + info["mv_nodes_fp64"]), 3),
+            "autotuned": {"min_ctas_per_sm": info["tuned_minb"], "grid": info["tuned_grid"]}}
     out = {
         "metric": METRIC, "value": round(H["value"], 4), "unit": UNIT, "n_gpus": D.world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(H["ms_per_step"], 3),
@@ -337,7 +351,9 @@ def run_ours(args, D):
         "clocks": H["clocks"],
         "paths": {p: {k: (round(v, 6) if isinstance(v, float) else v) for k, v in r.items()
                       if k in ("value", "ms_per_step", "status", "picard_iters", "pcg_iters_total",
-                               "refine_steps", "final_rel_resid", "rel_l2_vs_fp64")}
+                               "refine_steps")}
+                  | {"final_rel_resid": float("%.3e" % r["final_rel_resid"]),
+                     "rel_l2_vs_fp64": float("%.3e" % r.get("rel_l2_vs_fp64", 0.0))}
                   for p, r in res.items()},
     }
     if "fp64" in res and head != "fp64":
@@ -415,10 +431,47 @@ def profile_run(args):
     ctx.close()
 
 
+def kernel_sweep(args):
+    """Matvec variants on the workload's assembled matrix (one Picard iteration)."""
+    from cism_b200 import solver
+
+    ctx = solver.Context(0)
+    peak, _ = measured_peaks()
+    out = []
+    for storage in ("sym", "full"):
+        os.environ["BP_MATRIX_STORAGE"] = storage
+        m = make_model(args.workload, args.pcg_maxiters).copy(maxiter_nonlinear=1)
+        prep, u0, v0 = solver.prepare(m)
+        prob = ctx.problem([prep])
+        prob.set_guess([u0], [v0])
+        prob.run()
+        N = prob.info()["nodes"]
+        sms = 148
+        for store in ((1, 2) if storage == "sym" else (0,)):
+            coef = 56 if store else 108
+            wb = 4 if store == 2 else 8
+            nbytes = N * (coef * wb + 32)
+            for minb in (0, 4, 6, 8):
+                for grid in (0, 4 * sms, 8 * sms):
+                    ms = prob.tune_mv(store, minb, grid, reps=50)
+                    if ms is None:
+                        continue
+                    out.append({"store": ["full64", "sym64", "sym32"][store], "minb": minb, "grid": grid,
+                                "us": round(ms * 1e3, 2), "GBps": round(nbytes / (ms / 1e3) / 1e9, 1),
+                                "frac": round(nbytes / (ms / 1e3) / 1e9 / peak, 3)})
+                    print(json.dumps(out[-1]), flush=True)
+        prob.close()
+    os.environ.pop("BP_MATRIX_STORAGE", None)
+    ctx.close()
+
+
 def main():
     args = parse_args()
     if args.profile_run:
         profile_run(args)
+        return
+    if args.kernel_sweep:
+        kernel_sweep(args)
         return
     D = Dist(args.gpus)
     try:

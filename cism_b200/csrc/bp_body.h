@@ -363,4 +363,90 @@ BP_HD double2 matvec_row(const DevView& v, const Mat* A, int col, int k, size_t 
   return double2{yu, yv};
 }
 
+// ---------------------------------------------------------------------
+// Symmetric storage.  Only stencil offsets m = 13..26 (the diagonal and the
+// neighbours that come after the node in (kA, jA, iA) order) are stored per
+// node; the entry toward an earlier neighbour P is the transpose of P's
+// stored entry toward this node: Auu_m(R) = Auu_{26-m}(P),
+// Auv_m(R) = Avu_{26-m}(P), Avu_m(R) = Auv_{26-m}(P), Avv_m(R) = Avv_{26-m}(P).
+// Same kA/jA/iA summation order as the full-storage product.
+// ---------------------------------------------------------------------
+BP_HD double diag_u(const DevView& v, size_t n) {
+  return v.sym ? v.A[n].x : v.A[(size_t)13 * v.npad + n].x;
+}
+BP_HD double diag_v(const DevView& v, size_t n) {
+  return v.sym ? v.A[(size_t)14 * v.npad + n].y : v.A[(size_t)(27 + 13) * v.npad + n].y;
+}
+
+template <typename Src>
+BP_HD double2 matvec_row_sym(const DevView& v, const double2* A, int col, int k, size_t n,
+                             const Src& src) {
+  const int nz = v.nz, nc = v.ncols;
+  const size_t np = (size_t)v.npad;
+  int cn[9];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) cn[q] = v.col_nbr[q * nc + col];
+  double yu = 0.0, yv = 0.0;
+#pragma unroll
+  for (int kA = -1; kA <= 1; ++kA) {
+    const int kn = k + kA;
+    const bool kin = kn >= 0 && kn < nz;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+      const int m = (kA + 1) * 9 + q;
+      const bool ok = kin && cn[q] >= 0;
+      const size_t p = ok ? (size_t)cn[q] * nz + kn : n;  // in-bounds stand-in when absent
+      double2 s = src(p);
+      if (!ok) s = double2{0.0, 0.0};
+      if (m >= 13) {
+        const double2 a0 = BP_LD_RO(A + (size_t)(m - 13) * np + n);
+        const double2 a1 = BP_LD_RO(A + (size_t)(14 + m - 13) * np + n);
+        yu += a0.x * s.x + a0.y * s.y;
+        yv += a1.x * s.x + a1.y * s.y;
+      } else {
+        const double2 b0 = BP_LD_RO(A + (size_t)(13 - m) * np + p);
+        const double2 b1 = BP_LD_RO(A + (size_t)(14 + 13 - m) * np + p);
+        yu += b0.x * s.x + b1.x * s.y;
+        yv += b0.y * s.x + b1.y * s.y;
+      }
+    }
+  }
+  return double2{yu, yv};
+}
+
+// FP32 symmetric storage, (uu, uv, vu, vv) packed per offset; FP64 sums.
+template <typename Src>
+BP_HD double2 matvec_row_sym32(const DevView& v, const float4* A, int col, int k, size_t n,
+                               const Src& src) {
+  const int nz = v.nz, nc = v.ncols;
+  const size_t np = (size_t)v.npad;
+  int cn[9];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) cn[q] = v.col_nbr[q * nc + col];
+  double yu = 0.0, yv = 0.0;
+#pragma unroll
+  for (int kA = -1; kA <= 1; ++kA) {
+    const int kn = k + kA;
+    const bool kin = kn >= 0 && kn < nz;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+      const int m = (kA + 1) * 9 + q;
+      const bool ok = kin && cn[q] >= 0;
+      const size_t p = ok ? (size_t)cn[q] * nz + kn : n;
+      double2 s = src(p);
+      if (!ok) s = double2{0.0, 0.0};
+      if (m >= 13) {
+        const float4 a = BP_LD_RO(A + (size_t)(m - 13) * np + n);
+        yu += (double)a.x * s.x + (double)a.y * s.y;
+        yv += (double)a.z * s.x + (double)a.w * s.y;
+      } else {
+        const float4 b = BP_LD_RO(A + (size_t)(13 - m) * np + p);
+        yu += (double)b.x * s.x + (double)b.z * s.y;
+        yv += (double)b.y * s.x + (double)b.w * s.y;
+      }
+    }
+  }
+  return double2{yu, yv};
+}
+
 }  // namespace bp

@@ -64,7 +64,7 @@ struct InstState {
   int pcg_iters_total, pcg_iters_last;
   int refine_active, refine_steps, refine_steps_total;
   int inner_iter;
-  int pad;
+  int krylov_fp64;              // mixed: Krylov matvecs switched to the FP64 matrix
 };
 
 // Global counters polled by the host.
@@ -79,6 +79,10 @@ struct Counters {
 struct DevView {
   int nz, ncols, nnodes, npad, ncells, nelem, ninst, ntiles;
   int any_dirichlet;       // any prescribed node in the problem
+  int sym;                 // matrix stored as its 14 upper stencil offsets (exactly symmetric)
+  int minb;                // Krylov matvec variant: resident CTAs per SM it is built for (0 or 4)
+  int grid_cap;            // CTAs of the tile kernels (0 = one per tile)
+  unsigned long long* mv_nodes;  // [2] nodes through FP64 / FP32 Krylov matvecs (timing runs), or null
   const InstParams* inst;
   InstState* st;
   Counters* cnt;
@@ -105,13 +109,15 @@ struct DevView {
   // assembly / matrix
   double* qp;              // [nelem*8*10]: f, Jinv(3x3) per quadrature point
   double* efvs;            // [nelem]
-  double2* A;              // [2][27][npad]: (uu,uv) rows then (vu,vv) rows
-  float2* A32;             // [2][27][npad]: equilibrated FP32 copy (mixed)
+  // FP64 matrix, (u,v) pairs: h = 0 the u-row (Auu, Auv), h = 1 the v-row
+  // (Avu, Avv).  Full storage [2][27][npad]; symmetric storage [2][14][npad]
+  // holds stencil offsets m = 13..26 (diagonal first), the lower half being
+  // read from the neighbour's row.
+  double2* A;
+  float4* A32;             // mixed: [14][npad] (uu, uv, vu, vv) of offsets 13..26 in FP32
   double* badj;            // [4][npad] Dirichlet column moves per block
   // vectors (per node, (u,v) pairs)
-  double2 *x, *b, *r, *d0, *d1, *q, *Az, *Dinv, *usav;
-  double2 *scale;          // mixed: 1/sqrt(diag)
-  float2 *y32, *r32, *p32a, *p32b, *q32;
+  double2 *x, *b, *r, *z, *d0, *q, *Az, *Dinv, *usav;
   // reductions
   double* partials;        // [2][ntiles]
   unsigned* tile_counter;  // [ninst]

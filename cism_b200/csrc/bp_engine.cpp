@@ -11,9 +11,11 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <functional>
 #include <map>
+#include <tuple>
 #include <string>
 #include <vector>
 
@@ -89,6 +91,8 @@ struct bp_ctx {
   cudaEvent_t t0 = nullptr, t1 = nullptr, t2 = nullptr, t3 = nullptr;
   cudaEvent_t r0 = nullptr, r1 = nullptr;  // bp_timer_start / stop
   int num_sms = 0;
+  // autotuner results: (node bucket, nz, storage, precision) -> (minb, grid)
+  std::map<std::tuple<int, int, int, int>, std::pair<int, int>> tuned;
 };
 
 struct bp_problem {
@@ -103,6 +107,9 @@ struct bp_problem {
   cudaGraphExec_t inner_graph = nullptr;
   bool use_graphs = true;
   Timing timing;
+  bool tuned = false;
+  unsigned long long* mv_nodes_dev = nullptr;
+  unsigned long long mv_nodes[2] = {0, 0};
   std::vector<bp::InstState> state;
   float ms_upload = 0, ms_solve = 0;
   double h2d_bytes = 0, d2h_bytes = 0;
@@ -131,6 +138,10 @@ DevView make_view(Arena& a, cudaStream_t s, const HostPlan& p, bool with_cells, 
   int anyd = 0;
   for (uint8_t m : p.dmask) anyd |= (m != 0);
   v.any_dirichlet = anyd;
+  // systems assembled on the device are exactly symmetric: store half
+  // (BP_MATRIX_STORAGE=full keeps whole rows, for the kernel sweep)
+  const char* st_env = std::getenv("BP_MATRIX_STORAGE");
+  v.sym = (with_cells && !(st_env && std::string(st_env) == "full")) ? 1 : 0;
   const size_t np = (size_t)p.npad;
 #define UP(T, name, vec, field)                           \
   {                                                       \
@@ -163,25 +174,17 @@ DevView make_view(Arena& a, cudaStream_t s, const HostPlan& p, bool with_cells, 
   UP(int, "tile_start", p.tile_start, tile_start);
   UP(int, "tile_inst", p.tile_inst, tile_inst);
 #undef UP
-  v.A = a.get<double2>(s, "A", 2 * 27 * np);
+  v.A = a.get<double2>(s, "A", (v.sym ? 2 * 14 : 2 * 27) * np);
   v.x = a.get<double2>(s, "x", np);
   v.b = a.get<double2>(s, "b", np);
   v.r = a.get<double2>(s, "r", np);
   v.d0 = a.get<double2>(s, "d0", np);
-  v.d1 = a.get<double2>(s, "d1", np);
+  v.z = a.get<double2>(s, "z", np);
   v.q = a.get<double2>(s, "q", np);
   v.Az = a.get<double2>(s, "Az", np);
   v.Dinv = a.get<double2>(s, "Dinv", np);
   v.usav = a.get<double2>(s, "usav", np);
-  if (mixed) {
-    v.A32 = a.get<float2>(s, "A32", 2 * 27 * np);
-    v.scale = a.get<double2>(s, "scale", np);
-    v.y32 = a.get<float2>(s, "y32", np);
-    v.r32 = a.get<float2>(s, "r32", np);
-    v.p32a = a.get<float2>(s, "p32a", np);
-    v.p32b = a.get<float2>(s, "p32b", np);
-    v.q32 = a.get<float2>(s, "q32", np);
-  }
+  if (mixed && v.sym) v.A32 = a.get<float4>(s, "A32", 14 * np);
   v.partials = a.get<double>(s, "partials", 2 * (size_t)std::max(p.ntiles, 1));
   v.tile_counter = a.get<unsigned>(s, "tile_counter", p.ninst);
   CK(cudaMemsetAsync(v.tile_counter, 0, sizeof(unsigned) * p.ninst, s));
@@ -276,11 +279,13 @@ void enqueue_iteration(bp_problem* P, int variant, bool check) {
   if (variant == 3) {
     L(P, C_MV, [&] { launch_mv(MV_CG1, v, s); });
     L(P, C_UPD, [&] { launch_cg_update(check, v, s); });
+    if (check) L(P, C_CHECK, [&] { launch_mv(MV_CHECK, v, s); });
   } else {
     L(P, C_MV, [&] { launch_mv(MV_STD_A, v, s); });
     L(P, C_UPD, [&] { launch_std_update(check, v, s); });
+    if (check) L(P, C_CHECK, [&] { launch_mv(MV_CHECK, v, s); });
+    L(P, C_UPD, [&] { launch_std_dir(v, s); });
   }
-  if (check) L(P, C_CHECK, [&] { launch_mv(MV_CHECK, v, s); });
 }
 
 // A whole check chunk (ncheck iterations, the last one checks), captured
@@ -315,6 +320,8 @@ void run_pcg_fp64(bp_problem* P) {
     L(P, C_MV, [&] { launch_mv(MV_CG_FIRST, v, c->stream); });
     L(P, C_UPD, [&] { launch_cg_first_update(v, c->stream); });
     n = 2;
+  } else {
+    L(P, C_UPD, [&] { launch_std_dir(v, c->stream); });  // d = z
   }
   int chunk = 0;
   while (n <= maxit + 1) {
@@ -334,54 +341,52 @@ void run_pcg_fp64(bp_problem* P) {
   CK(cudaGetLastError());
 }
 
-// Mixed precision: FP64 refinement around FP32 inner CG.
-void run_mixed(bp_problem* P) {
-  const HostPlan& p = P->plan;
-  const DevView& v = P->v;
-  bp_ctx* c = P->c;
-  cudaStream_t s = c->stream;
-  L(P, C_OTHER, [&] { launch_mixed_setup(v, s); });
-  const int maxit = max_pcg_iters(p);
-  const int inner_chunk = 8;
-  for (int ref = 0; ref < 24; ++ref) {
-    CK(cudaMemsetAsync(&v.cnt->pcg_active, 0, sizeof(int), s));
-    L(P, C_CHECK, [&] { launch_refine_resid(v, s); });
-    snapshot(c, v, 0);
-    if (wait_snapshot(c, 0).refine_active <= 0) break;
-    int chunk = 0;
-    for (int it = 0; it < maxit; it += inner_chunk) {
-      if (P->use_graphs && !P->timing.on) {
-        if (!P->inner_graph) {
-          cudaGraph_t g;
-          CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-          for (int j = 0; j < inner_chunk; ++j) launch_inner(v, s);
-          CK(cudaStreamEndCapture(s, &g));
-          CK(cudaGraphInstantiate(&P->inner_graph, g, 0));
-          CK(cudaGraphDestroy(g));
-        }
-        CK(cudaGraphLaunch(P->inner_graph, s));
-      } else {
-        for (int j = 0; j < inner_chunk; ++j) {
-          L(P, C_MV32, [&] { launch_inner_a(v, s); });
-          L(P, C_UPD32, [&] { launch_inner_b(v, s); });
-        }
-      }
-      snapshot(c, v, chunk & 1);
-      if (chunk >= 1 && wait_snapshot(c, (chunk - 1) & 1).pcg_active <= 0) break;
-      ++chunk;
-    }
-    L(P, C_OTHER, [&] { launch_refine_update(v, s); });
-  }
-  CK(cudaGetLastError());
+// Linear solve of the assembled systems of all active instances.  With
+// an FP32 matrix copy (mixed precision) the same kernels run the Krylov
+// matvecs on it while every true residual stays FP64.
+void linear_solve(bp_problem* P) {
+  if (P->v.A32) L(P, C_OTHER, [&] { launch_make_a32(P->v, P->c->stream); });
+  L(P, C_CHECK, [&] { launch_mv(MV_INIT, P->v, P->c->stream); });
+  run_pcg_fp64(P);
 }
 
-void linear_solve(bp_problem* P) {
-  if (P->mixed) {
-    run_mixed(P);
-  } else {
-    L(P, C_CHECK, [&] { launch_mv(MV_INIT, P->v, P->c->stream); });
-    run_pcg_fp64(P);
+// Autotuner: after the first assembly of a problem, time the Krylov matvec
+// in each (occupancy target, grid) variant on the problem's own matrix and
+// keep the fastest for every tile kernel; results are cached per context
+// by (size bucket, nz, storage, precision).
+void autotune(bp_problem* P) {
+  bp_ctx* c = P->c;
+  DevView& v = P->v;
+  P->tuned = true;
+  const auto key = std::make_tuple(P->plan.nnodes >> 14, P->plan.nz, v.sym, v.A32 ? 1 : 0);
+  auto it = c->tuned.find(key);
+  if (it != c->tuned.end()) {
+    v.minb = it->second.first;
+    v.grid_cap = it->second.second;
+    return;
   }
+  const int store = v.sym ? (v.A32 ? 2 : 1) : 0;
+  if (v.A32) launch_make_a32(v, c->stream);
+  const int grids[2] = {0, 4 * c->num_sms};
+  const int minbs[2] = {0, 4};
+  float best = 1e30f;
+  int bm = 0, bg = 0;
+  for (int mb : minbs)
+    for (int g : grids) {
+      if (g > 0 && g >= P->plan.ntiles) continue;  // same as one CTA per tile
+      launch_tune_mv(store, mb, g, v, c->stream);
+      CK(cudaEventRecord(c->r0, c->stream));
+      for (int i = 0; i < 5; ++i) launch_tune_mv(store, mb, g, v, c->stream);
+      CK(cudaEventRecord(c->r1, c->stream));
+      CK(cudaEventSynchronize(c->r1));
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, c->r0, c->r1));
+      if (ms < best) { best = ms; bm = mb; bg = g; }
+    }
+  CK(cudaGetLastError());
+  v.minb = bm;
+  v.grid_cap = bg;
+  c->tuned[key] = {bm, bg};
 }
 
 // The Picard loop of glissade_velo_higher_solve on the device.
@@ -398,6 +403,7 @@ void run_picard(bp_problem* P) {
     L(P, C_ASM1, [&] { launch_asm_qp(v, s); });
     L(P, C_ASM2, [&] { launch_asm_rows(v, s); });
     L(P, C_RHS, [&] { launch_rhs(v, s); });
+    if (!P->tuned) autotune(P);
     linear_solve(P);
     L(P, C_OTHER, [&] { launch_picard_check(v, s); });
     snapshot(c, v, 0);
@@ -484,6 +490,13 @@ void problem_set_guess(bp_problem* P, double* const* uvel, double* const* vvel) 
 
 void problem_run(bp_problem* P) {
   bp_ctx* c = P->c;
+  if (P->timing.on) {
+    if (!P->mv_nodes_dev) P->mv_nodes_dev = P->arena->get<unsigned long long>(c->stream, "mv_nodes", 2);
+    CK(cudaMemsetAsync(P->mv_nodes_dev, 0, 2 * sizeof(unsigned long long), c->stream));
+    P->v.mv_nodes = P->mv_nodes_dev;
+  } else {
+    P->v.mv_nodes = nullptr;
+  }
   CK(cudaEventRecord(c->t1, c->stream));
   CK(cudaMemcpyAsync(P->v.x, P->x0, sizeof(double2) * P->plan.npad, cudaMemcpyDeviceToDevice, c->stream));
   init_state(c->stream, P->v, P->plan, true, false);
@@ -493,6 +506,10 @@ void problem_run(bp_problem* P) {
                      cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   collect_timing(P);
+  if (P->v.mv_nodes) {
+    CK(cudaMemcpy(P->mv_nodes, P->mv_nodes_dev, sizeof(P->mv_nodes), cudaMemcpyDeviceToHost));
+    P->v.mv_nodes = nullptr;
+  }
   cudaEventElapsedTime(&P->ms_solve, c->t1, c->t2);
 }
 
@@ -671,6 +688,37 @@ int bp_problem_kernel_times(bp_problem* P, double* ms, int* launches) {
   return BP_OK;
 }
 
+int bp_problem_tune_mv(bp_problem* P, int store, int minb, int grid, int reps, float* ms) {
+  if (!P) return BP_ERR_ARGS;
+  GUARD_BEGIN(P->c)
+  bp_ctx* c = P->c;
+  if (store == 2 && P->v.sym && !P->v.A32) {
+    P->v.A32 = P->arena->get<float4>(c->stream, "A32", 14 * (size_t)P->plan.npad);
+    launch_make_a32(P->v, c->stream);
+  }
+  if (launch_tune_mv(store, minb, grid, P->v, c->stream) != 0) return BP_ERR_ARGS;  // warm
+  CK(cudaEventRecord(c->r0, c->stream));
+  for (int i = 0; i < reps; ++i) launch_tune_mv(store, minb, grid, P->v, c->stream);
+  CK(cudaEventRecord(c->r1, c->stream));
+  CK(cudaEventSynchronize(c->r1));
+  CK(cudaGetLastError());
+  float t = 0.f;
+  CK(cudaEventElapsedTime(&t, c->r0, c->r1));
+  if (ms) *ms = t / std::max(1, reps);
+  if (store == 2 && !P->mixed) P->v.A32 = nullptr;  // keep the FP64 path unchanged
+  return BP_OK;
+  GUARD_END
+}
+
+int bp_problem_mv_nodes(bp_problem* P, double* fp64_nodes, double* fp32_nodes, int* minb, int* grid) {
+  if (!P) return BP_ERR_ARGS;
+  if (fp64_nodes) *fp64_nodes = (double)P->mv_nodes[0];
+  if (fp32_nodes) *fp32_nodes = (double)P->mv_nodes[1];
+  if (minb) *minb = P->v.minb;
+  if (grid) *grid = P->v.grid_cap;
+  return BP_OK;
+}
+
 int bp_problem_info(bp_problem* P, long* nodes, long* cols, long* elems, double* mvb64,
                     double* mvb32) {
   if (!P) return BP_ERR_ARGS;
@@ -681,10 +729,16 @@ int bp_problem_info(bp_problem* P, long* nodes, long* cols, long* elems, double*
   // algorithmic bytes of one fused PCG matvec launch per node:
   // standard: 108 FP64 coefficients + r, D^-1, d_old read + d, q written
   // Chronopoulos-Gear: 108 coefficients + r, D^-1 read + Az written
+  // coefficients read per node: symmetric storage streams the 14 upper
+  // stencil offsets (the lower half is re-read from neighbours, from L2)
+  // vectors of the Krylov matvec kernel: source read + result written
+  // (+ the vectors of its fused dots: d for the standard PCG, r and z for
+  // Chronopoulos-Gear)
   const bool cg = P->plan.inst[0].variant == 3;
-  if (mvb64) *mvb64 = N * (108.0 * 8.0 + (cg ? 3.0 : 5.0) * 16.0);
-  // FP32 inner: 108 FP32 coefficients + r, p_old read + p, q written (8 B each)
-  if (mvb32) *mvb32 = N * (108.0 * 4.0 + 4.0 * 8.0);
+  const double vec = (cg ? 3.0 : 2.0) * 16.0;
+  const double coef = P->v.sym ? 14.0 * 4.0 : 27.0 * 4.0;
+  if (mvb64) *mvb64 = N * (coef * 8.0 + vec);
+  if (mvb32) *mvb32 = N * (coef * 4.0 + vec);
   return BP_OK;
 }
 
@@ -739,6 +793,10 @@ int bp_pcg(bp_ctx* c, int nx, int ny, int nz, int periodic,
     c->err = "bp_pcg: precond must be 0 or 1";
     return BP_ERR_ARGS;
   }
+  if (precision != BP_FP64) {
+    c->err = "bp_pcg: an external matrix is solved in FP64 (precision 0)";
+    return BP_ERR_ARGS;
+  }
   bp_problem P;
   P.c = c;
   P.arena = &c->arena;
@@ -755,7 +813,7 @@ int bp_pcg(bp_ctx* c, int nx, int ny, int nz, int periodic,
   ip.ncheck = ncheck > 0 ? ncheck : 5;
   ip.precision = precision;
   ip.inner_tol = 1.0e-4;
-  P.mixed = precision == BP_MIXED;
+  P.mixed = false;
   P.use_graphs = false;
   P.v = make_view(*P.arena, c->stream, P.plan, false, P.mixed);
   const DevView& v = P.v;
@@ -836,7 +894,7 @@ int bp_assemble(bp_ctx* c, const bp_inputs* in, const double* uvel,
   launch_asm_qp(v, c->stream);
   launch_asm_rows(v, c->stream);
   launch_rhs(v, c->stream);
-  std::vector<double2> A(2 * 27 * (size_t)p.npad), b(p.npad);
+  std::vector<double2> A((v.sym ? 2 * 14 : 2 * 27) * (size_t)p.npad), b(p.npad);
   std::vector<double> ef(std::max(p.nelem, 1));
   CK(cudaMemcpyAsync(A.data(), v.A, sizeof(double2) * A.size(), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaMemcpyAsync(b.data(), v.b, sizeof(double2) * p.npad, cudaMemcpyDeviceToHost, c->stream));
@@ -846,7 +904,8 @@ int bp_assemble(bp_ctx* c, const bp_inputs* in, const double* uvel,
   CK(cudaMemcpyAsync(&st, v.st, sizeof(st), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   CK(cudaGetLastError());
-  scatter_matrix(p, A.data(), Auu, Auv, Avu, Avv);
+  if (v.sym) scatter_matrix_sym(p, A.data(), Auu, Auv, Avu, Avv);
+  else scatter_matrix(p, A.data(), Auu, Auv, Avu, Avv);
   const size_t tot = (size_t)in->nz * (in->nx - 1) * (in->ny - 1);
   if (bu) std::memset(bu, 0, sizeof(double) * tot);
   if (bv) std::memset(bv, 0, sizeof(double) * tot);

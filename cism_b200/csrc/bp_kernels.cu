@@ -150,6 +150,7 @@ __global__ void k_picard_begin(DevView v) {
     S.refine_active = 1;
     S.inner_iter = 0;
     S.pcg_iters_last = 0;
+    S.krylov_fp64 = 0;
     ++mine;
   }
   atomicAdd(&cnt, mine);
@@ -219,7 +220,11 @@ __device__ __forceinline__ bool asm_row(const DevView& v, int n) {
 #pragma unroll
   for (int m = 0; m < 27; ++m) {
     nz |= (acc[m] != 0.0);
-    Ad[(((size_t)(h * 27 + m)) * np + n) * 2 + comp] = acc[m];
+    if (v.sym) {
+      if (m >= 13) Ad[(((size_t)(h * 14 + m - 13)) * np + n) * 2 + comp] = acc[m];
+    } else {
+      Ad[(((size_t)(h * 27 + m)) * np + n) * 2 + comp] = acc[m];
+    }
   }
   v.badj[(size_t)B * np + n] = adj;
   return nz;
@@ -266,7 +271,7 @@ __global__ void __launch_bounds__(kTile) k_rhs(DevView v) {
       v.b[n] = make_double2(bu, bv);
       double2 di = make_double2(1.0, 1.0);
       if (ip.precond == 1) {
-        const double du = v.A[13 * np + n].x, dv = v.A[(27 + 13) * np + n].y;
+        const double du = diag_u(v, n), dv = diag_v(v, n);
         di.x = du != 0.0 ? 1.0 / du : 0.0;
         di.y = dv != 0.0 ? 1.0 / dv : 0.0;
       }
@@ -289,147 +294,131 @@ __global__ void __launch_bounds__(kTile) k_rhs(DevView v) {
 }
 
 // ---------------------------------------------------------------------
-// Fused matvec kernels.  Source vectors are formed on the fly at the
-// node and its neighbours (z = D^-1 r, d = z + beta d_old) so no separate
-// preconditioner or direction-update pass is needed.
+// PCG kernels.  Every Krylov matvec reads one stored source vector (d for
+// the standard PCG, z = D^-1 r for Chronopoulos-Gear, x for residuals), so
+// each matvec is a plain y = A s with its dot products fused in.  Storage
+// variants: full FP64 rows, symmetric FP64, symmetric FP32 (Krylov matvecs
+// of the mixed path; residuals always use the FP64 matrix).
 // ---------------------------------------------------------------------
+enum { ST_FULL = 0, ST_SYM = 1, ST_SYM32 = 2 };
+
 struct SrcX {
   const double2* x;
   __device__ double2 operator()(size_t m) const { return x[m]; }
 };
-struct SrcZ {  // z = D^-1 r
-  const double2 *r, *di;
-  __device__ double2 operator()(size_t m) const {
-    const double2 a = r[m], b = di[m];
-    return make_double2(a.x * b.x, a.y * b.y);
-  }
-};
-struct SrcD {  // d = z + beta d_old
-  const double2 *r, *di, *dold;
-  double beta;
-  bool first;
-  __device__ double2 operator()(size_t m) const {
-    const double2 a = r[m], b = di[m];
-    double2 z = make_double2(a.x * b.x, a.y * b.y);
-    if (!first) {
-      const double2 o = dold[m];
-      z.x = z.x + beta * o.x;
-      z.y = z.y + beta * o.y;
-    }
-    return z;
-  }
-};
 
-template <int MODE>
-__global__ void __launch_bounds__(kTile) k_mv(DevView v) {
+template <int STORE>
+__device__ __forceinline__ double2 mv_row(const DevView& v, int col, int k, size_t n,
+                                          const double2* s) {
+  const SrcX src{s};
+  if (STORE == ST_FULL) return matvec_row(v, v.A, col, k, n, src);
+  if (STORE == ST_SYM) return matvec_row_sym(v, v.A, col, k, n, src);
+  return matvec_row_sym32(v, v.A32, col, k, n, src);
+}
+
+// r = b - A x with the FP64 matrix; z = D^-1 r stored; (r,z) and (r,r).
+// MV_INIT starts a linear solve (also compute_residual_vector_3d's norms);
+// MV_CHECK is the every-ncheck true residual (pcg:478-536, 1542-1597).
+template <int MODE, int STORE, int MINB>
+__global__ void __launch_bounds__(kTile, MINB) k_resid(DevView v) {
+  constexpr int ST64 = STORE == ST_SYM32 ? ST_SYM : STORE;
   for (int t = blockIdx.x; t < v.ntiles; t += gridDim.x) {
     const TileRange R = tile_range(v, t);
-    InstState& S = v.st[R.inst];
-    if (!S.pcg_active) continue;
-    const InstParams& ip = v.inst[R.inst];
+    if (!v.st[R.inst].pcg_active) continue;
     const int n = R.n0 + threadIdx.x;
-    const int it = S.pcg_iter;
     double part[2] = {0.0, 0.0};
     if (n < R.nend) {
       const int col = n / v.nz, k = n - col * v.nz;
-      if (MODE == MV_INIT || MODE == MV_CHECK) {
-        const double2 y = matvec_row(v, v.A, col, k, n, SrcX{v.x});
-        const double2 b = v.b[n], di = v.Dinv[n];
-        const double ru = b.x - y.x, rv = b.y - y.y;
-        v.r[n] = make_double2(ru, rv);
-        part[0] = ru * (ru * di.x) + rv * (rv * di.y);  // (r, z)
-        part[1] = ru * ru + rv * rv;                    // (r, r)
-      } else if (MODE == MV_STD_A) {
-        double2* dold = (it & 1) ? v.d0 : v.d1;
-        double2* dnew = (it & 1) ? v.d1 : v.d0;
-        const SrcD src{v.r, v.Dinv, dold, S.beta, it == 1};
-        const double2 y = matvec_row(v, v.A, col, k, n, src);
-        const double2 d = src((size_t)n);
-        dnew[n] = d;
-        v.q[n] = y;
-        part[0] = d.x * y.x + d.y * y.y;
-      } else if (MODE == MV_CG_FIRST) {
-        const SrcZ src{v.r, v.Dinv};
-        const double2 y = matvec_row(v, v.A, col, k, n, src);
-        const double2 z = src((size_t)n), r = v.r[n];
-        v.d0[n] = z;
-        v.q[n] = y;
-        part[0] = r.x * z.x + r.y * z.y;
-        part[1] = z.x * y.x + z.y * y.y;
-      } else if (MODE == MV_CG1) {
-        const SrcZ src{v.r, v.Dinv};
-        const double2 y = matvec_row(v, v.A, col, k, n, src);
-        const double2 z = src((size_t)n), r = v.r[n];
-        v.Az[n] = y;
-        part[0] = r.x * z.x + r.y * z.y;
-        part[1] = y.x * z.x + y.y * z.y;
-      }
+      const double2 y = mv_row<ST64>(v, col, k, n, v.x);
+      const double2 b = v.b[n], di = v.Dinv[n];
+      const double ru = b.x - y.x, rv = b.y - y.y;
+      const double zu = ru * di.x, zv = rv * di.y;
+      v.r[n] = make_double2(ru, rv);
+      v.z[n] = make_double2(zu, zv);
+      part[0] = ru * zu + rv * zv;
+      part[1] = ru * ru + rv * rv;
     }
     tile_finish<2, false>(v, t, R.inst, part, [&](int inst, const double* s) {
-      InstState& S2 = v.st[inst];
-      const InstParams& ip2 = v.inst[inst];
+      InstState& S = v.st[inst];
+      const InstParams& ip = v.inst[inst];
       if (MODE == MV_INIT) {
-        S2.L2_norm = sqrt(s[1]);
-        S2.L2_rel = S2.L2_rhs > 0.0 ? S2.L2_norm / S2.L2_rhs : 0.0;
-        if (ip2.variant != 3) {  // standard PCG: eta1 of iteration 1
-          if (is_nan(s[0])) { fail(v, S2, BP_ERR_NAN); return; }
-          S2.beta = s[0] / S2.rz;
-          S2.rz = s[0];
-        }
-      } else if (MODE == MV_STD_A) {
-        const double alpha = S2.rz / s[0];
-        if (is_nan(alpha)) { fail(v, S2, BP_ERR_NAN); return; }
-        S2.alpha = alpha;
-      } else if (MODE == MV_CG_FIRST) {
-        S2.rz_old = s[0];
-        S2.sigma = s[1];
-        const double alpha = s[0] / s[1];
-        if (is_nan(alpha)) { fail(v, S2, BP_ERR_NAN); return; }
-        S2.alpha = alpha;
-      } else if (MODE == MV_CG1) {
-        S2.pcg_iter += 1;
-        if (S2.pcg_iter > ip2.pcg_maxiters) {
-          S2.pcg_iter = ip2.pcg_maxiters;
-          pcg_stop(v, S2, false);
-          return;
-        }
-        const double rho = s[0], delta = s[1];
-        const double beta = rho / S2.rz_old;
-        const double sigma = delta - beta * rho / S2.alpha;
-        const double alpha = rho / sigma;
-        S2.rz_old = rho;
-        S2.beta = beta;
-        S2.sigma = sigma;
-        if (is_nan(alpha)) { fail(v, S2, BP_ERR_NAN); return; }
-        S2.alpha = alpha;
-      } else if (MODE == MV_CHECK) {
-        S2.err = sqrt(s[1]) / S2.L2_rhs;
-        if (S2.err < ip2.pcg_tol) { pcg_stop(v, S2, true); return; }
-        if (S2.pcg_iter >= ip2.pcg_maxiters) { pcg_stop(v, S2, false); return; }
-        if (ip2.variant != 3) {
-          if (is_nan(s[0])) { fail(v, S2, BP_ERR_NAN); return; }
-          S2.beta = s[0] / S2.rz;
-          S2.rz = s[0];
-          S2.pcg_iter += 1;
-        }
+        S.L2_norm = sqrt(s[1]);
+        S.L2_rel = S.L2_rhs > 0.0 ? S.L2_norm / S.L2_rhs : 0.0;
+      } else {
+        S.err = sqrt(s[1]) / S.L2_rhs;
+        S.refine_steps_total += 1;
+        if (S.err < ip.pcg_tol) { pcg_stop(v, S, true); return; }
+        if (S.pcg_iter >= ip.pcg_maxiters) { pcg_stop(v, S, false); return; }
+        // mixed: the last decades of the solve use the FP64 matrix
+        if (STORE == ST_SYM32 && S.err < ip.inner_tol) S.krylov_fp64 = 1;
+      }
+      if (ip.variant != 3) {  // standard PCG: eta1 of the next iteration
+        if (is_nan(s[0])) { fail(v, S, BP_ERR_NAN); return; }
+        S.beta = s[0] / S.rz;
+        S.rz = s[0];
+        if (MODE == MV_CHECK) S.pcg_iter += 1;
       }
     });
   }
 }
 
-// Standard PCG update: x += alpha d; r -= alpha q; (r, D^-1 r).
+// Krylov matvec of the mixed path: FP32 matrix until the instance's true
+// residual falls below inner_tol, FP64 after.  In timing runs the nodes
+// through each precision are counted, to turn the measured time into bytes.
+template <int STORE>
+__device__ __forceinline__ double2 krylov_row(const DevView& v, const InstState& S, int col, int k,
+                                              size_t n, const double2* s) {
+  if (STORE == ST_SYM32 && S.krylov_fp64) return mv_row<ST_SYM>(v, col, k, n, s);
+  return mv_row<STORE>(v, col, k, n, s);
+}
+
+template <int STORE>
+__device__ __forceinline__ void count_tile(const DevView& v, const InstState& S, const TileRange& R) {
+  if (v.mv_nodes && threadIdx.x == 0) {
+    const bool f32 = STORE == ST_SYM32 && !S.krylov_fp64;
+    atomicAdd(&v.mv_nodes[f32 ? 1 : 0], (unsigned long long)(R.nend - R.n0));
+  }
+}
+
+// Standard PCG: q = A d; (d, q); alpha = eta1 / (d, q)   (pcg:426-463).
+template <int STORE, int MINB>
+__global__ void __launch_bounds__(kTile, MINB) k_std_mv(DevView v) {
+  for (int t = blockIdx.x; t < v.ntiles; t += gridDim.x) {
+    const TileRange R = tile_range(v, t);
+    const InstState& S0 = v.st[R.inst];
+    if (!S0.pcg_active) continue;
+    count_tile<STORE>(v, S0, R);
+    const int n = R.n0 + threadIdx.x;
+    double part[1] = {0.0};
+    if (n < R.nend) {
+      const int col = n / v.nz, k = n - col * v.nz;
+      const double2 y = krylov_row<STORE>(v, S0, col, k, n, v.d0);
+      const double2 d = v.d0[n];
+      v.q[n] = y;
+      part[0] = d.x * y.x + d.y * y.y;
+    }
+    tile_finish<1, false>(v, t, R.inst, part, [&](int inst, const double* s) {
+      InstState& S = v.st[inst];
+      const double alpha = S.rz / s[0];
+      if (is_nan(alpha)) { fail(v, S, BP_ERR_NAN); return; }
+      S.alpha = alpha;
+    });
+  }
+}
+
+// x += alpha d; r -= alpha q; z = D^-1 r; (r, z) -> beta  (pcg:347-407, 468-472).
+// On check iterations only x is updated (r is recomputed from b - A x).
 template <bool CHECK>
 __global__ void __launch_bounds__(kTile) k_std_update(DevView v) {
   for (int t = blockIdx.x; t < v.ntiles; t += gridDim.x) {
     const TileRange R = tile_range(v, t);
-    InstState& S = v.st[R.inst];
+    const InstState& S = v.st[R.inst];
     if (!S.pcg_active) continue;
     const int n = R.n0 + threadIdx.x;
-    const int it = S.pcg_iter;
     const double alpha = S.alpha;
     double part[1] = {0.0};
     if (n < R.nend) {
-      const double2 d = ((it & 1) ? v.d1 : v.d0)[n];
+      const double2 d = v.d0[n];
       double2 x = v.x[n];
       x.x = x.x + alpha * d.x;
       x.y = x.y + alpha * d.y;
@@ -439,8 +428,10 @@ __global__ void __launch_bounds__(kTile) k_std_update(DevView v) {
         double2 r = v.r[n];
         r.x = r.x - alpha * q.x;
         r.y = r.y - alpha * q.y;
+        const double zu = r.x * di.x, zv = r.y * di.y;
         v.r[n] = r;
-        part[0] = r.x * (r.x * di.x) + r.y * (r.y * di.y);
+        v.z[n] = make_double2(zu, zv);
+        part[0] = r.x * zu + r.y * zv;
       }
     }
     if (!CHECK) {
@@ -456,7 +447,81 @@ __global__ void __launch_bounds__(kTile) k_std_update(DevView v) {
   }
 }
 
-// Chronopoulos-Gear first-pass update: x += alpha d; r -= alpha q.
+// d = z + beta d; d = z at the first iteration (pcg:403-407).
+__global__ void __launch_bounds__(kTile) k_std_dir(DevView v) {
+  for (int t = blockIdx.x; t < v.ntiles; t += gridDim.x) {
+    const TileRange R = tile_range(v, t);
+    const InstState& S = v.st[R.inst];
+    if (!S.pcg_active) continue;
+    const int n = R.n0 + threadIdx.x;
+    if (n >= R.nend) continue;
+    const double2 z = v.z[n];
+    if (S.pcg_iter == 1) {
+      v.d0[n] = z;
+    } else {
+      const double beta = S.beta;
+      const double2 d = v.d0[n];
+      v.d0[n] = make_double2(z.x + beta * d.x, z.y + beta * d.y);
+    }
+  }
+}
+
+// Chronopoulos-Gear matvec Az = A z with (r,z), (Az,z) and the scalar
+// recurrences (pcg:1461-1512).  FIRST: the first pass (pcg:1304-1405),
+// which also sets d = z, q = A d.
+template <bool FIRST, int STORE, int MINB>
+__global__ void __launch_bounds__(kTile, MINB) k_cg_mv(DevView v) {
+  for (int t = blockIdx.x; t < v.ntiles; t += gridDim.x) {
+    const TileRange R = tile_range(v, t);
+    const InstState& S0 = v.st[R.inst];
+    if (!S0.pcg_active) continue;
+    count_tile<STORE>(v, S0, R);
+    const int n = R.n0 + threadIdx.x;
+    double part[2] = {0.0, 0.0};
+    if (n < R.nend) {
+      const int col = n / v.nz, k = n - col * v.nz;
+      const double2 y = krylov_row<STORE>(v, S0, col, k, n, v.z);
+      const double2 z = v.z[n], r = v.r[n];
+      if (FIRST) {
+        v.d0[n] = z;
+        v.q[n] = y;
+      } else {
+        v.Az[n] = y;
+      }
+      part[0] = r.x * z.x + r.y * z.y;
+      part[1] = y.x * z.x + y.y * z.y;
+    }
+    tile_finish<2, false>(v, t, R.inst, part, [&](int inst, const double* s) {
+      InstState& S = v.st[inst];
+      if (FIRST) {
+        S.rz_old = s[0];
+        S.sigma = s[1];
+        const double alpha = s[0] / s[1];
+        if (is_nan(alpha)) { fail(v, S, BP_ERR_NAN); return; }
+        S.alpha = alpha;
+        return;
+      }
+      const InstParams& ip = v.inst[inst];
+      S.pcg_iter += 1;
+      if (S.pcg_iter > ip.pcg_maxiters) {
+        S.pcg_iter = ip.pcg_maxiters;
+        pcg_stop(v, S, false);
+        return;
+      }
+      const double rho = s[0], delta = s[1];
+      const double beta = rho / S.rz_old;
+      const double sigma = delta - beta * rho / S.alpha;
+      const double alpha = rho / sigma;
+      S.rz_old = rho;
+      S.beta = beta;
+      S.sigma = sigma;
+      if (is_nan(alpha)) { fail(v, S, BP_ERR_NAN); return; }
+      S.alpha = alpha;
+    });
+  }
+}
+
+// Chronopoulos-Gear first-pass update: x += alpha d; r -= alpha q; z = D^-1 r.
 __global__ void __launch_bounds__(kTile) k_cg_first_update(DevView v) {
   for (int t = blockIdx.x; t < v.ntiles; t += gridDim.x) {
     const TileRange R = tile_range(v, t);
@@ -465,17 +530,19 @@ __global__ void __launch_bounds__(kTile) k_cg_first_update(DevView v) {
     const int n = R.n0 + threadIdx.x;
     if (n >= R.nend) continue;
     const double alpha = S.alpha;
-    const double2 d = v.d0[n], q = v.q[n];
+    const double2 d = v.d0[n], q = v.q[n], di = v.Dinv[n];
     double2 x = v.x[n], r = v.r[n];
     x.x = x.x + alpha * d.x; x.y = x.y + alpha * d.y;
     r.x = r.x - alpha * q.x; r.y = r.y - alpha * q.y;
     v.x[n] = x;
     v.r[n] = r;
+    v.z[n] = make_double2(r.x * di.x, r.y * di.y);
   }
 }
 
-// Chronopoulos-Gear loop update: d = z + beta d; q = Az + beta q;
-// x += alpha d; r -= alpha q (glissade_velo_higher_pcg.F90:1519-1534).
+// Chronopoulos-Gear loop update (pcg:1519-1534): d = z + beta d;
+// q = Az + beta q; x += alpha d; r -= alpha q; z = D^-1 r for the next
+// iteration (skipped on check iterations, where r and z come from b - A x).
 template <bool CHECK>
 __global__ void __launch_bounds__(kTile) k_cg_update(DevView v) {
   for (int t = blockIdx.x; t < v.ntiles; t += gridDim.x) {
@@ -485,16 +552,20 @@ __global__ void __launch_bounds__(kTile) k_cg_update(DevView v) {
     const int n = R.n0 + threadIdx.x;
     if (n >= R.nend) continue;
     const double alpha = S.alpha, beta = S.beta;
-    const double2 r = v.r[n], di = v.Dinv[n], az = v.Az[n];
+    const double2 z = v.z[n], az = v.Az[n];
     double2 d = v.d0[n], q = v.q[n], x = v.x[n];
-    const double zu = r.x * di.x, zv = r.y * di.y;
-    d.x = zu + beta * d.x; d.y = zv + beta * d.y;
+    d.x = z.x + beta * d.x; d.y = z.y + beta * d.y;
     q.x = az.x + beta * q.x; q.y = az.y + beta * q.y;
     x.x = x.x + alpha * d.x; x.y = x.y + alpha * d.y;
     v.d0[n] = d;
     v.q[n] = q;
     v.x[n] = x;
-    if (!CHECK) v.r[n] = make_double2(r.x - alpha * q.x, r.y - alpha * q.y);
+    if (!CHECK) {
+      const double2 r = v.r[n], di = v.Dinv[n];
+      const double ru = r.x - alpha * q.x, rv = r.y - alpha * q.y;
+      v.r[n] = make_double2(ru, rv);
+      v.z[n] = make_double2(ru * di.x, rv * di.y);
+    }
   }
 }
 
@@ -549,221 +620,22 @@ __global__ void __launch_bounds__(kTile) k_picard_check(DevView v) {
 }
 
 // ---------------------------------------------------------------------
-// Mixed precision: FP32 equilibrated matrix, FP32 inner CG with FP64
-// reductions, FP64 iterative refinement.
+// Mixed precision: FP32 copy of the symmetric matrix for the Krylov
+// iteration; the every-ncheck true residual r = b - A x stays FP64, so the
+// iteration is a reliable-update PCG that converges to the FP64 solution.
 // ---------------------------------------------------------------------
-__global__ void __launch_bounds__(kTile) k_scale(DevView v) {
-  for (int t = blockIdx.x; t < v.ntiles; t += gridDim.x) {
-    const TileRange R = tile_range(v, t);
-    if (!v.st[R.inst].pcg_active) continue;
-    const int n = R.n0 + threadIdx.x;
-    if (n >= R.nend) continue;
-    const size_t np = (size_t)v.npad;
-    const double du = v.A[13 * np + n].x, dv = v.A[(27 + 13) * np + n].y;
-    v.scale[n] = make_double2(du > 0.0 ? 1.0 / sqrt(du) : 0.0, dv > 0.0 ? 1.0 / sqrt(dv) : 0.0);
-  }
-}
-
 __global__ void __launch_bounds__(kTile) k_make_a32(DevView v) {
   for (int t = blockIdx.x; t < v.ntiles; t += gridDim.x) {
     const TileRange R = tile_range(v, t);
     if (!v.st[R.inst].pcg_active) continue;
     const int n = R.n0 + threadIdx.x;
     if (n >= R.nend) continue;
-    const int nz = v.nz, nc = v.ncols;
-    const int col = n / nz, k = n - col * nz;
     const size_t np = (size_t)v.npad;
-    const double2 sn = v.scale[n];
 #pragma unroll
-    for (int kA = -1; kA <= 1; ++kA)
-#pragma unroll
-      for (int q = 0; q < 9; ++q) {
-        const int m = (kA + 1) * 9 + q;
-        const int cn = v.col_nbr[q * nc + col];
-        const int kn = k + kA;
-        double2 sm = make_double2(0.0, 0.0);
-        if (cn >= 0 && kn >= 0 && kn < nz) sm = v.scale[(size_t)cn * nz + kn];
-        const double2 au = v.A[(size_t)m * np + n], av = v.A[(size_t)(27 + m) * np + n];
-        v.A32[(size_t)m * np + n] =
-            make_float2((float)(sn.x * au.x * sm.x), (float)(sn.x * au.y * sm.y));
-        v.A32[(size_t)(27 + m) * np + n] =
-            make_float2((float)(sn.y * av.x * sm.x), (float)(sn.y * av.y * sm.y));
-      }
-  }
-}
-
-// Outer residual r = b - A x (FP64); start of an inner solve.
-__global__ void __launch_bounds__(kTile) k_refine_resid(DevView v) {
-  for (int t = blockIdx.x; t < v.ntiles; t += gridDim.x) {
-    const TileRange R = tile_range(v, t);
-    InstState& S = v.st[R.inst];
-    if (!S.refine_active) continue;
-    const int n = R.n0 + threadIdx.x;
-    double part[2] = {0.0, 0.0};
-    if (n < R.nend) {
-      const int col = n / v.nz, k = n - col * v.nz;
-      const double2 y = matvec_row(v, v.A, col, k, n, SrcX{v.x});
-      const double2 b = v.b[n], s = v.scale[n];
-      const double ru = b.x - y.x, rv = b.y - y.y;
-      const float su = (float)(s.x * ru), sv = (float)(s.y * rv);
-      v.r32[n] = make_float2(su, sv);
-      v.y32[n] = make_float2(0.f, 0.f);
-      part[0] = ru * ru + rv * rv;
-      part[1] = (double)su * su + (double)sv * sv;
+    for (int mm = 0; mm < 14; ++mm) {
+      const double2 a = v.A[(size_t)mm * np + n], b = v.A[(size_t)(14 + mm) * np + n];
+      v.A32[(size_t)mm * np + n] = make_float4((float)a.x, (float)a.y, (float)b.x, (float)b.y);
     }
-    tile_finish<2, false>(v, t, R.inst, part, [&](int inst, const double* s) {
-      InstState& S2 = v.st[inst];
-      const InstParams& ip2 = v.inst[inst];
-      S2.err = S2.L2_rhs > 0.0 ? sqrt(s[0]) / S2.L2_rhs : 0.0;
-      if (S2.refine_steps == 0) {
-        S2.L2_norm = sqrt(s[0]);
-        S2.L2_rel = S2.err;
-      }
-      const bool conv = !(S2.err >= ip2.pcg_tol);
-      if (conv || S2.refine_steps >= 20 || S2.pcg_iters_last >= ip2.pcg_maxiters || is_nan(s[0])) {
-        S2.refine_active = 0;
-        S2.pcg_active = 0;
-        S2.pcg_converged = conv ? 1 : 0;
-        S2.refine_steps_total += S2.refine_steps;
-        S2.pcg_iters_total += S2.pcg_iters_last;
-        atomicSub(&v.cnt->refine_active, 1);
-        if (is_nan(s[0])) fail(v, S2, BP_ERR_NAN);
-        return;
-      }
-      S2.refine_steps += 1;
-      S2.in_rr0 = s[1];
-      S2.rz = s[1];
-      S2.beta = 0.0;
-      S2.inner_iter = 1;
-      S2.pcg_active = 1;
-      atomicAdd(&v.cnt->pcg_active, 1);
-    });
-  }
-}
-
-struct SrcP32 {  // p = r + beta p_old, FP32 storage
-  const float2 *r, *pold;
-  float beta;
-  bool first;
-  __device__ float2 operator()(size_t m) const {
-    const float2 a = r[m];
-    if (first) return a;
-    const float2 o = pold[m];
-    return make_float2(a.x + beta * o.x, a.y + beta * o.y);
-  }
-};
-
-template <typename Src>
-__device__ __forceinline__ float2 matvec_row32(const DevView& v, int col, int k, size_t n,
-                                               const Src& src) {
-  const int nz = v.nz, nc = v.ncols;
-  const size_t np = (size_t)v.npad;
-  int cn[9];
-#pragma unroll
-  for (int q = 0; q < 9; ++q) cn[q] = v.col_nbr[q * nc + col];
-  float yu = 0.f, yv = 0.f;
-#pragma unroll
-  for (int kA = -1; kA <= 1; ++kA) {
-    const int kn = k + kA;
-    if (kn < 0 || kn >= nz) continue;
-#pragma unroll
-    for (int q = 0; q < 9; ++q) {
-      if (cn[q] < 0) continue;
-      const int m = (kA + 1) * 9 + q;
-      const float2 au = __ldcs(v.A32 + (size_t)m * np + n);
-      const float2 av = __ldcs(v.A32 + (size_t)(27 + m) * np + n);
-      const float2 s = src((size_t)cn[q] * nz + kn);
-      yu = fmaf(au.x, s.x, fmaf(au.y, s.y, yu));
-      yv = fmaf(av.x, s.x, fmaf(av.y, s.y, yv));
-    }
-  }
-  return make_float2(yu, yv);
-}
-
-// Inner CG, part A: p = r + beta p_old; q = A32 p; (p, q).
-__global__ void __launch_bounds__(kTile) k_inner_a(DevView v) {
-  for (int t = blockIdx.x; t < v.ntiles; t += gridDim.x) {
-    const TileRange R = tile_range(v, t);
-    InstState& S = v.st[R.inst];
-    if (!S.pcg_active) continue;
-    const int n = R.n0 + threadIdx.x;
-    const int it = S.inner_iter;
-    double part[1] = {0.0};
-    if (n < R.nend) {
-      const int col = n / v.nz, k = n - col * v.nz;
-      float2* pold = (it & 1) ? v.p32a : v.p32b;
-      float2* pnew = (it & 1) ? v.p32b : v.p32a;
-      const SrcP32 src{v.r32, pold, (float)S.beta, it == 1};
-      const float2 y = matvec_row32(v, col, k, n, src);
-      const float2 p = src((size_t)n);
-      pnew[n] = p;
-      v.q32[n] = y;
-      part[0] = (double)p.x * y.x + (double)p.y * y.y;
-    }
-    tile_finish<1, false>(v, t, R.inst, part, [&](int inst, const double* s) {
-      InstState& S2 = v.st[inst];
-      const double alpha = S2.rz / s[0];
-      if (is_nan(alpha) || !(s[0] > 0.0)) {  // breakdown: end this inner solve
-        S2.alpha = 0.0;
-        S2.pcg_active = 0;
-        atomicSub(&v.cnt->pcg_active, 1);
-        return;
-      }
-      S2.alpha = alpha;
-    });
-  }
-}
-
-// Inner CG, part B: y += alpha p; r -= alpha q; (r, r); inner stop test.
-__global__ void __launch_bounds__(kTile) k_inner_b(DevView v) {
-  for (int t = blockIdx.x; t < v.ntiles; t += gridDim.x) {
-    const TileRange R = tile_range(v, t);
-    InstState& S = v.st[R.inst];
-    if (!S.pcg_active) continue;
-    const int n = R.n0 + threadIdx.x;
-    const int it = S.inner_iter;
-    const float alpha = (float)S.alpha;
-    double part[1] = {0.0};
-    if (n < R.nend) {
-      const float2 p = ((it & 1) ? v.p32b : v.p32a)[n];
-      const float2 q = v.q32[n];
-      float2 y = v.y32[n], r = v.r32[n];
-      y.x = fmaf(alpha, p.x, y.x); y.y = fmaf(alpha, p.y, y.y);
-      r.x = fmaf(-alpha, q.x, r.x); r.y = fmaf(-alpha, q.y, r.y);
-      v.y32[n] = y;
-      v.r32[n] = r;
-      part[0] = (double)r.x * r.x + (double)r.y * r.y;
-    }
-    tile_finish<1, false>(v, t, R.inst, part, [&](int inst, const double* s) {
-      InstState& S2 = v.st[inst];
-      const InstParams& ip2 = v.inst[inst];
-      S2.pcg_iters_last += 1;
-      const double tol = ip2.inner_tol;
-      if (!(s[0] > tol * tol * S2.in_rr0) || S2.pcg_iters_last >= ip2.pcg_maxiters) {
-        S2.pcg_active = 0;
-        atomicSub(&v.cnt->pcg_active, 1);
-        return;
-      }
-      S2.beta = s[0] / S2.rz;
-      S2.rz = s[0];
-      S2.inner_iter += 1;
-    });
-  }
-}
-
-// x += S y after an inner solve.
-__global__ void __launch_bounds__(kTile) k_refine_update(DevView v) {
-  for (int t = blockIdx.x; t < v.ntiles; t += gridDim.x) {
-    const TileRange R = tile_range(v, t);
-    if (!v.st[R.inst].refine_active) continue;
-    const int n = R.n0 + threadIdx.x;
-    if (n >= R.nend) continue;
-    const float2 y = v.y32[n];
-    const double2 s = v.scale[n];
-    double2 x = v.x[n];
-    x.x += s.x * (double)y.x;
-    x.y += s.y * (double)y.y;
-    v.x[n] = x;
   }
 }
 
@@ -774,7 +646,20 @@ __global__ void __launch_bounds__(kTile) k_matvec_plain(DevView v, const double2
     const int n = R.n0 + threadIdx.x;
     if (n >= R.nend) continue;
     const int col = n / v.nz, k = n - col * v.nz;
-    y[n] = matvec_row(v, v.A, col, k, n, SrcX{x});
+    y[n] = v.sym ? matvec_row_sym(v, v.A, col, k, n, SrcX{x}) : matvec_row(v, v.A, col, k, n, SrcX{x});
+  }
+}
+
+// y = A x for the autotuner and the kernel sweep: one storage variant and
+// one occupancy target (MINB = minimum resident CTAs per SM, 0 = free).
+template <int STORE, int MINB>
+__global__ void __launch_bounds__(kTile, MINB) k_tune_mv(DevView v) {
+  for (int t = blockIdx.x; t < v.ntiles; t += gridDim.x) {
+    const TileRange R = tile_range(v, t);
+    const int n = R.n0 + threadIdx.x;
+    if (n >= R.nend) continue;
+    const int col = n / v.nz, k = n - col * v.nz;
+    v.Az[n] = mv_row<STORE>(v, col, k, n, v.x);
   }
 }
 
@@ -786,8 +671,9 @@ __global__ void __launch_bounds__(kTile) k_dinv(DevView v, int precond) {
     if (n >= R.nend) continue;
     const size_t np = (size_t)v.npad;
     double2 di = make_double2(1.0, 1.0);
+    (void)np;
     if (precond == 1) {
-      const double du = v.A[13 * np + n].x, dv = v.A[(27 + 13) * np + n].y;
+      const double du = diag_u(v, n), dv = diag_v(v, n);
       di.x = du != 0.0 ? 1.0 / du : 0.0;
       di.y = dv != 0.0 ? 1.0 / dv : 0.0;
     }
@@ -815,13 +701,9 @@ __global__ void __launch_bounds__(kTile) k_bb(DevView v) {
 // ---------------------------------------------------------------------
 // host-side launchers
 // ---------------------------------------------------------------------
-static int g_grid_cap = 0;
-
-void set_grid_cap(int cap) { g_grid_cap = cap; }
-
 static inline int tile_grid(const DevView& v) {
   int g = v.ntiles > 0 ? v.ntiles : 1;
-  if (g_grid_cap > 0 && g > g_grid_cap) g = g_grid_cap;
+  if (v.grid_cap > 0 && g > v.grid_cap) g = v.grid_cap;
   return g;
 }
 
@@ -849,20 +731,32 @@ void launch_assemble(const DevView& v, cudaStream_t s) {
   launch_asm_rows(v, s);
   launch_rhs(v, s);
 }
+template <int STORE, int MINB>
+static void launch_mv_store(int mode, const DevView& v, cudaStream_t s, int g) {
+  switch (mode) {
+    case MV_INIT: k_resid<MV_INIT, STORE, MINB><<<g, kTile, 0, s>>>(v); break;
+    case MV_CHECK: k_resid<MV_CHECK, STORE, MINB><<<g, kTile, 0, s>>>(v); break;
+    case MV_STD_A: k_std_mv<STORE, MINB><<<g, kTile, 0, s>>>(v); break;
+    case MV_CG_FIRST: k_cg_mv<true, STORE, MINB><<<g, kTile, 0, s>>>(v); break;
+    default: k_cg_mv<false, STORE, MINB><<<g, kTile, 0, s>>>(v); break;
+  }
+}
+template <int STORE>
+static void launch_mv_minb(int mode, const DevView& v, cudaStream_t s, int g) {
+  if (v.minb == 4) launch_mv_store<STORE, 4>(mode, v, s, g);
+  else launch_mv_store<STORE, 0>(mode, v, s, g);
+}
 void launch_mv(int mode, const DevView& v, cudaStream_t s) {
   const int g = tile_grid(v);
-  switch (mode) {
-    case MV_INIT: k_mv<MV_INIT><<<g, kTile, 0, s>>>(v); break;
-    case MV_STD_A: k_mv<MV_STD_A><<<g, kTile, 0, s>>>(v); break;
-    case MV_CG_FIRST: k_mv<MV_CG_FIRST><<<g, kTile, 0, s>>>(v); break;
-    case MV_CG1: k_mv<MV_CG1><<<g, kTile, 0, s>>>(v); break;
-    default: k_mv<MV_CHECK><<<g, kTile, 0, s>>>(v); break;
-  }
+  if (!v.sym) launch_mv_minb<ST_FULL>(mode, v, s, g);
+  else if (v.A32) launch_mv_minb<ST_SYM32>(mode, v, s, g);
+  else launch_mv_minb<ST_SYM>(mode, v, s, g);
 }
 void launch_std_update(bool check, const DevView& v, cudaStream_t s) {
   if (check) k_std_update<true><<<tile_grid(v), kTile, 0, s>>>(v);
   else k_std_update<false><<<tile_grid(v), kTile, 0, s>>>(v);
 }
+void launch_std_dir(const DevView& v, cudaStream_t s) { k_std_dir<<<tile_grid(v), kTile, 0, s>>>(v); }
 void launch_cg_first_update(const DevView& v, cudaStream_t s) {
   k_cg_first_update<<<tile_grid(v), kTile, 0, s>>>(v);
 }
@@ -873,22 +767,7 @@ void launch_cg_update(bool check, const DevView& v, cudaStream_t s) {
 void launch_picard_check(const DevView& v, cudaStream_t s) {
   k_picard_check<<<tile_grid(v), kTile, 0, s>>>(v);
 }
-void launch_mixed_setup(const DevView& v, cudaStream_t s) {
-  k_scale<<<tile_grid(v), kTile, 0, s>>>(v);
-  k_make_a32<<<tile_grid(v), kTile, 0, s>>>(v);
-}
-void launch_refine_resid(const DevView& v, cudaStream_t s) {
-  k_refine_resid<<<tile_grid(v), kTile, 0, s>>>(v);
-}
-void launch_inner_a(const DevView& v, cudaStream_t s) { k_inner_a<<<tile_grid(v), kTile, 0, s>>>(v); }
-void launch_inner_b(const DevView& v, cudaStream_t s) { k_inner_b<<<tile_grid(v), kTile, 0, s>>>(v); }
-void launch_inner(const DevView& v, cudaStream_t s) {
-  launch_inner_a(v, s);
-  launch_inner_b(v, s);
-}
-void launch_refine_update(const DevView& v, cudaStream_t s) {
-  k_refine_update<<<tile_grid(v), kTile, 0, s>>>(v);
-}
+void launch_make_a32(const DevView& v, cudaStream_t s) { k_make_a32<<<tile_grid(v), kTile, 0, s>>>(v); }
 void launch_matvec_plain(const DevView& v, const double2* x, double2* y, cudaStream_t s) {
   k_matvec_plain<<<tile_grid(v), kTile, 0, s>>>(v, x, y);
 }
@@ -896,5 +775,23 @@ void launch_dinv(const DevView& v, int precond, cudaStream_t s) {
   k_dinv<<<tile_grid(v), kTile, 0, s>>>(v, precond);
 }
 void launch_bb(const DevView& v, cudaStream_t s) { k_bb<<<tile_grid(v), kTile, 0, s>>>(v); }
+int launch_tune_mv(int store, int minb, int grid, const DevView& v, cudaStream_t s) {
+  const int g = grid > 0 ? grid : tile_grid(v);
+#define TUNE(ST, MB) k_tune_mv<ST, MB><<<g, kTile, 0, s>>>(v)
+  if (store == ST_FULL && !v.sym) {
+    if (minb == 8) TUNE(ST_FULL, 8); else if (minb == 6) TUNE(ST_FULL, 6);
+    else if (minb == 4) TUNE(ST_FULL, 4); else TUNE(ST_FULL, 0);
+  } else if (store == ST_SYM && v.sym) {
+    if (minb == 8) TUNE(ST_SYM, 8); else if (minb == 6) TUNE(ST_SYM, 6);
+    else if (minb == 4) TUNE(ST_SYM, 4); else TUNE(ST_SYM, 0);
+  } else if (store == ST_SYM32 && v.sym && v.A32) {
+    if (minb == 8) TUNE(ST_SYM32, 8); else if (minb == 6) TUNE(ST_SYM32, 6);
+    else if (minb == 4) TUNE(ST_SYM32, 4); else TUNE(ST_SYM32, 0);
+  } else {
+    return -1;
+  }
+#undef TUNE
+  return 0;
+}
 
 }  // namespace bp

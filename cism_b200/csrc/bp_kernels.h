@@ -10,8 +10,6 @@ namespace bp {
 enum MvMode { MV_INIT = 0, MV_STD_A = 1, MV_CG_FIRST = 2, MV_CG1 = 3, MV_CHECK = 4 };
 
 cudaError_t upload_ref_tables();
-// Upper bound on the grid of tile kernels (0 = one CTA per tile).
-void set_grid_cap(int cap);
 
 void launch_picard_begin(const DevView& v, cudaStream_t s);
 void launch_save_usav(const DevView& v, cudaStream_t s);
@@ -21,17 +19,16 @@ void launch_asm_rows(const DevView& v, cudaStream_t s);
 void launch_rhs(const DevView& v, cudaStream_t s);
 void launch_mv(int mode, const DevView& v, cudaStream_t s);
 void launch_std_update(bool check, const DevView& v, cudaStream_t s);
+void launch_std_dir(const DevView& v, cudaStream_t s);
 void launch_cg_first_update(const DevView& v, cudaStream_t s);
 void launch_cg_update(bool check, const DevView& v, cudaStream_t s);
 void launch_picard_check(const DevView& v, cudaStream_t s);
-void launch_mixed_setup(const DevView& v, cudaStream_t s);
-void launch_refine_resid(const DevView& v, cudaStream_t s);
-void launch_inner(const DevView& v, cudaStream_t s);
-void launch_inner_a(const DevView& v, cudaStream_t s);
-void launch_inner_b(const DevView& v, cudaStream_t s);
-void launch_refine_update(const DevView& v, cudaStream_t s);
+void launch_make_a32(const DevView& v, cudaStream_t s);
 void launch_matvec_plain(const DevView& v, const double2* x, double2* y, cudaStream_t s);
 void launch_dinv(const DevView& v, int precond, cudaStream_t s);
 void launch_bb(const DevView& v, cudaStream_t s);
+// store: 0 full FP64, 1 symmetric FP64, 2 symmetric FP32; minb: 0, 6 or 8
+// resident CTAs per SM; grid: CTAs (0 = one per tile).  -1 if unavailable.
+int launch_tune_mv(int store, int minb, int grid, const DevView& v, cudaStream_t s);
 
 }  // namespace bp

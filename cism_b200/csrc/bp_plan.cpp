@@ -190,7 +190,7 @@ bool build_plan(const bp_inputs* in, int n, HostPlan* p, std::string* err) {
     ip.dx = I.dx; ip.dy = I.dy;
     ip.efvs_constant = I.efvs_constant;
     ip.pcg_tol = I.pcg_tol;
-    ip.inner_tol = I.inner_tol > 0.0 ? I.inner_tol : 1.0e-4;
+    ip.inner_tol = I.inner_tol > 0.0 ? I.inner_tol : 1.0e-6;
     for (int k = 0; k < nz; ++k) ip.sigma[k] = I.sigma[k];
     ip.which_efvs = I.which_efvs;
     ip.which_babc = I.which_babc;
@@ -339,6 +339,57 @@ void scatter_matrix(const HostPlan& p, const double2* A, double* Auu,
         if (Auv) Auv[base + m] = u.y;
         if (Avu) Avu[base + m] = v.x;
         if (Avv) Avv[base + m] = v.y;
+      }
+    }
+  }
+}
+
+void scatter_matrix_sym(const HostPlan& p, const double2* A, double* Auu,
+                        double* Auv, double* Avu, double* Avv) {
+  const int nx = p.nx[0], ny = p.ny[0], nz = p.nz, NC = p.ncols, np = p.npad;
+  const size_t tot = (size_t)27 * nz * (nx - 1) * (ny - 1);
+  for (double* a : {Auu, Auv, Avu, Avv})
+    if (a) std::memset(a, 0, sizeof(double) * tot);
+  for (int g = 0; g < NC; ++g) {
+    const int i = p.col_ij[g], j = p.col_ij[NC + g];
+    for (int k = 0; k < nz; ++k) {
+      const size_t n = (size_t)g * nz + k;
+      const size_t base = (vtx(i, j, nx) * nz + k) * 27;
+      for (int m = 0; m < 27; ++m) {
+        double uu, uv, vu, vv;
+        if (m >= 13) {
+          const double2 a0 = A[(size_t)(m - 13) * np + n], a1 = A[(size_t)(14 + m - 13) * np + n];
+          uu = a0.x; uv = a0.y; vu = a1.x; vv = a1.y;
+        } else {
+          const int iA = m % 3 - 1, jA = (m / 3) % 3 - 1, kA = m / 9 - 1;
+          const int cn = p.col_nbr[(size_t)((jA + 1) * 3 + (iA + 1)) * NC + g];
+          const int kn = k + kA;
+          if (cn < 0 || kn < 0 || kn >= nz) continue;
+          const size_t pn = (size_t)cn * nz + kn;
+          const double2 b0 = A[(size_t)(13 - m) * np + pn], b1 = A[(size_t)(14 + 13 - m) * np + pn];
+          uu = b0.x; uv = b1.x; vu = b0.y; vv = b1.y;
+        }
+        if (Auu) Auu[base + m] = uu;
+        if (Auv) Auv[base + m] = uv;
+        if (Avu) Avu[base + m] = vu;
+        if (Avv) Avv[base + m] = vv;
+      }
+    }
+  }
+}
+
+void gather_matrix_sym(const HostPlan& p, const double* Auu, const double* Auv,
+                       const double* Avu, const double* Avv, double2* A) {
+  const int nx = p.nx[0], nz = p.nz, NC = p.ncols, np = p.npad;
+  std::memset((void*)A, 0, sizeof(double2) * 2 * 14 * (size_t)np);
+  for (int g = 0; g < NC; ++g) {
+    const int i = p.col_ij[g], j = p.col_ij[NC + g];
+    for (int k = 0; k < nz; ++k) {
+      const size_t n = (size_t)g * nz + k;
+      const size_t base = (vtx(i, j, nx) * nz + k) * 27;
+      for (int m = 13; m < 27; ++m) {
+        A[(size_t)(m - 13) * np + n] = double2{Auu[base + m], Auv[base + m]};
+        A[(size_t)(14 + m - 13) * np + n] = double2{Avu[base + m], Avv[base + m]};
       }
     }
   }

@@ -59,6 +59,12 @@ void gather_matrix(const HostPlan& p, const double* Auu, const double* Auv,
                    const double* Avu, const double* Avv, double2* A);
 void scatter_matrix(const HostPlan& p, const double2* A, double* Auu,
                     double* Auv, double* Avu, double* Avv);
+// symmetric storage [2][14][npad] -> full rows (lower half from neighbours)
+void scatter_matrix_sym(const HostPlan& p, const double2* A, double* Auu,
+                        double* Auv, double* Avu, double* Avv);
+// full rows -> symmetric storage (upper offsets only)
+void gather_matrix_sym(const HostPlan& p, const double* Auu, const double* Auv,
+                       const double* Avu, const double* Avv, double2* A);
 void scatter_vector(const HostPlan& p, int b, const double2* v, double* vu,
                     double* vv);
 

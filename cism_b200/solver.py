@@ -128,6 +128,9 @@ def lib():
         L.bp_problem_timing.argtypes = [C.c_void_p, C.c_int]
         L.bp_problem_kernel_times.argtypes = [C.c_void_p, _dp, _ip]
         L.bp_problem_info.argtypes = [C.c_void_p] + [C.POINTER(C.c_long)] * 3 + [_dp, _dp]
+        L.bp_problem_tune_mv.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
+                                         C.POINTER(C.c_float)]
+        L.bp_problem_mv_nodes.argtypes = [C.c_void_p, _dp, _dp, _ip, _ip]
         L.bp_timer_start.argtypes = [C.c_void_p]
         L.bp_timer_stop.argtypes = [C.c_void_p, C.POINTER(C.c_float)]
         _lib = L
@@ -156,7 +159,7 @@ class Prepared:
         self._keep = keep
 
 
-def make_model_struct(m: configs.BPModel, precision: int = FP64, inner_tol: float = 1e-4):
+def make_model_struct(m: configs.BPModel, precision: int = FP64, inner_tol: float = 1e-6):
     keep = []
 
     def f(a):
@@ -187,7 +190,7 @@ def make_model_struct(m: configs.BPModel, precision: int = FP64, inner_tol: floa
 
 
 def prepare(m: configs.BPModel, uvel=None, vvel=None, precision: int = FP64,
-            inner_tol: float = 1e-4) -> tuple:
+            inner_tol: float = 1e-6) -> tuple:
     """Host setup (bp_setup): returns (Prepared, uvel, vvel)."""
     nx, ny, nz = m.nx, m.ny, m.nz
     arrays = {
@@ -256,7 +259,7 @@ class Context:
         return u, v, efvs, st.as_dict()
 
     def velo_higher_solve(self, m: configs.BPModel, uvel=None, vvel=None, precision: int = FP64,
-                          inner_tol: float = 1e-4):
+                          inner_tol: float = 1e-6):
         """glissade_velo_higher_solve: host setup + device Picard loop."""
         prep, u, v = prepare(m, uvel, vvel, precision, inner_tol)
         return self.solve_prepared(prep, u, v)
@@ -366,6 +369,12 @@ class Problem:
         self.ctx._check(rc, allow=(0,))
         return us, vs, es
 
+    def tune_mv(self, store: int, minb: int = 0, grid: int = 0, reps: int = 50):
+        """Mean ms of a plain y = A x launch (store 0 full, 1 sym FP64, 2 sym FP32)."""
+        ms = C.c_float()
+        rc = lib().bp_problem_tune_mv(self.h, store, minb, grid, reps, C.byref(ms))
+        return ms.value if rc == 0 else None
+
     def timing(self, enable: bool):
         lib().bp_problem_timing(self.h, 1 if enable else 0)
 
@@ -374,6 +383,14 @@ class Problem:
         n = (C.c_int * len(KERNEL_CATEGORIES))()
         lib().bp_problem_kernel_times(self.h, ms, n)
         return {k: (ms[i], n[i]) for i, k in enumerate(KERNEL_CATEGORIES)}
+
+    def mv_nodes(self):
+        """(FP64 nodes, FP32 nodes) of the last timing run's Krylov matvecs and
+        the autotuner's (minb, grid)."""
+        a, b = C.c_double(), C.c_double()
+        mb, g = C.c_int(), C.c_int()
+        lib().bp_problem_mv_nodes(self.h, C.byref(a), C.byref(b), C.byref(mb), C.byref(g))
+        return a.value, b.value, mb.value, g.value
 
     def info(self):
         nodes, cols, elems = C.c_long(), C.c_long(), C.c_long()
@@ -406,5 +423,5 @@ def default_context() -> Context:
 
 
 def velo_higher_solve(m: configs.BPModel, uvel=None, vvel=None, precision: int = FP64,
-                      inner_tol: float = 1e-4):
+                      inner_tol: float = 1e-6):
     return default_context().velo_higher_solve(m, uvel, vvel, precision, inner_tol)

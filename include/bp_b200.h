@@ -81,7 +81,9 @@ typedef struct {
   int pcg_ncheck;               /* reference: 5 */
   double pcg_tol;               /* reference: 1e-8 */
   int precision;                /* bp_precision */
-  double inner_tol;             /* BP_MIXED: relative tolerance of each FP32 inner solve */
+  double inner_tol;             /* BP_MIXED: true relative residual below which the Krylov
+                                   matvecs switch from the FP32 to the FP64 matrix
+                                   (<= 0: 1e-6) */
 } bp_inputs;
 
 typedef struct {
@@ -195,6 +197,16 @@ int bp_problem_timing(bp_problem *p, int enable);
 int bp_timer_start(bp_ctx *ctx);
 int bp_timer_stop(bp_ctx *ctx, float *ms);
 int bp_problem_kernel_times(bp_problem *p, double *ms, int *launches);
+/* Time reps launches of a plain y = A x kernel on the problem's current
+ * matrix (run the problem once first): store 0 full FP64 rows, 1 symmetric
+ * FP64, 2 symmetric FP32; minb = resident CTAs per SM the kernel is
+ * compiled for (0, 6, 8); grid = CTAs (0 = one per tile).  ms = mean per
+ * launch.  BP_ERR_ARGS if the variant does not match the storage. */
+int bp_problem_tune_mv(bp_problem *p, int store, int minb, int grid, int reps, float *ms);
+/* Nodes that went through FP64 and FP32 Krylov matvecs during the last
+ * timing run, and the autotuner's choice (resident CTAs per SM, grid). */
+int bp_problem_mv_nodes(bp_problem *p, double *fp64_nodes, double *fp32_nodes,
+                        int *minb, int *grid);
 /* Node count and, per FP64 matvec launch, the algorithmic bytes moved. */
 int bp_problem_info(bp_problem *p, long *nodes, long *active_columns,
                     long *elements, double *matvec_bytes_fp64,

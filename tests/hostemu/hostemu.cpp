@@ -100,6 +100,42 @@ extern "C" int emu_assemble(const bp_inputs* in, const double* uvel, const doubl
   return 0;
 }
 
+// Symmetric storage (14 upper offsets; fp32 = 1 for the packed FP32 copy).
+extern "C" int emu_matvec_sym(int nx, int ny, int nz, int periodic, const int* active_vertex,
+                              const double* Auu, const double* Auv, const double* Avu,
+                              const double* Avv, const double* xu, const double* xv, double* yu,
+                              double* yv, int fp32) {
+  Emu E;
+  std::string err;
+  if (!build_column_plan(nx, ny, nz, periodic, active_vertex, &E.p, &err)) return 10;
+  E.bind();
+  E.v.sym = 1;
+  std::vector<double2> As(2 * 14 * (size_t)E.p.npad);
+  gather_matrix_sym(E.p, Auu, Auv, Avu, Avv, As.data());
+  std::vector<float4> A32(14 * (size_t)E.p.npad);
+  for (size_t mm = 0; mm < 14; ++mm)
+    for (int n = 0; n < E.p.npad; ++n) {
+      const double2 a = As[mm * E.p.npad + n], b = As[(14 + mm) * E.p.npad + n];
+      A32[mm * E.p.npad + n] = float4{(float)a.x, (float)a.y, (float)b.x, (float)b.y};
+    }
+  E.v.A = As.data();
+  E.v.A32 = A32.data();
+  gather_velocity(E.p, 0, xu, xv, E.x.data());
+  std::vector<double2> y(E.p.npad, double2{0, 0});
+  const double2* xs = E.x.data();
+  auto src = [xs](size_t m) { return xs[m]; };
+  for (int n = 0; n < E.p.nnodes; ++n) {
+    const int col = n / nz, k = n - col * nz;
+    y[n] = fp32 ? matvec_row_sym32(E.v, A32.data(), col, k, (size_t)n, src)
+                : matvec_row_sym(E.v, As.data(), col, k, (size_t)n, src);
+  }
+  const size_t tot = (size_t)nz * (nx - 1) * (ny - 1);
+  std::memset(yu, 0, tot * 8);
+  std::memset(yv, 0, tot * 8);
+  scatter_vector(E.p, 0, y.data(), yu, yv);
+  return 0;
+}
+
 extern "C" int emu_matvec(int nx, int ny, int nz, int periodic, const int* active_vertex,
                           const double* Auu, const double* Auv, const double* Avu,
                           const double* Avv, const double* xu, const double* xv, double* yu,

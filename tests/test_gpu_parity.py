@@ -107,7 +107,7 @@ def test_picard_matches_oracle(ctx, name):
 def test_mixed_precision_close_to_fp64(ctx):
     m = configs.slab(n=32).copy(pcg_maxiters=2000)
     u64, v64, _, st64 = ctx.velo_higher_solve(m)
-    u32, v32, _, st32 = ctx.velo_higher_solve(m, precision=solver.MIXED, inner_tol=1e-4)
+    u32, v32, _, st32 = ctx.velo_higher_solve(m, precision=solver.MIXED)
     assert st32["status"] == 0, st32
     assert st32["pcg_err_last"] < 1e-8
     assert rel_l2([u32, v32], [u64, v64]) < 1e-6

@@ -82,6 +82,24 @@ def test_kernel_bodies_match_oracle(m):
     assert rel_l2([eyu, eyv], [yu, yv]) < 1e-14
 
 
+@pytest.mark.parametrize("m", MODELS[:4], ids=lambda m: m.name)
+def test_symmetric_storage_matvec_bodies(m):
+    """The device's half-storage matvec (lower stencil half read from the
+    neighbours' rows), FP64 and FP32, against the oracle's full-row matvec."""
+    emu = C.CDLL(EMU)
+    su, u, v, A, bu, bv, efvs = oracle_system(m, seed=2, scale=10.0)
+    xu, xv = random_state(m, su, seed=3, scale=1.0)
+    yu, yv = oracle.matvec(m, su["active_vertex"], A, xu, xv)
+    av = np.ascontiguousarray(su["active_vertex"], np.int32)
+    for fp32, tol in ((0, 1e-13), (1, 1e-6)):
+        eyu, eyv = np.zeros(m.vshape3), np.zeros(m.vshape3)
+        rc = emu.emu_matvec_sym(m.nx, m.ny, m.nz, m.periodic, _p(av),
+                                *[_p(np.ascontiguousarray(a)) for a in A], _p(xu), _p(xv),
+                                _p(eyu), _p(eyv), fp32)
+        assert rc == 0
+        assert rel_l2([eyu, eyv], [yu, yv]) < tol, fp32
+
+
 def test_library_exports_every_declared_symbol():
     hdr = open(os.path.join(ROOT, "include", "bp_b200.h")).read()
     names = set(re.findall(r"^\s*(?:int|const char \*)\s*\**\s*(bp_\w+)\s*\(", hdr, re.M))
