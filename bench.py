@@ -57,8 +57,8 @@ def parse_args():
     ap.add_argument("--workload", default="c1", choices=sorted(WORKLOAD_DESC))
     ap.add_argument("--precision", default="best", choices=["best", "fp64", "mixed"])
     ap.add_argument("--pcg-maxiters", type=int, default=3000)
-    ap.add_argument("--mixed-switch", type=float, default=1e-6,
-                    help="mixed path: true residual below which the Krylov matvec uses FP64")
+    ap.add_argument("--refine-eta", type=float, default=1e-4,
+                    help="mixed path: residual reduction of one FP32 refinement cycle")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-run", action="store_true",
                     help="one untimed solve (for ncu launch lists / captures)")
@@ -254,7 +254,7 @@ def run_ours(args, D):
     sol = {}
     for path in paths:
         prec = solver.MIXED if path == "mixed" else solver.FP64
-        prep, u0, v0 = solver.prepare(m, precision=prec, inner_tol=args.mixed_switch)
+        prep, u0, v0 = solver.prepare(m, precision=prec, inner_tol=args.refine_eta)
         prob = ctx.problem([prep])
         prob.set_guess([u0], [v0])
         for _ in range(args.warmup):

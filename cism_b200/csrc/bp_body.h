@@ -414,7 +414,53 @@ BP_HD double2 matvec_row_sym(const DevView& v, const double2* A, int col, int k,
   return double2{yu, yv};
 }
 
-// FP32 symmetric storage, (uu, uv, vu, vv) packed per offset; FP64 sums.
+// FP32 copy of row n of the symmetric matrix for the mixed-precision
+// Krylov matvecs.  Rounding each entry to FP32 perturbs the row sums, and
+// with them the operator on smooth fields (the translation modes are
+// nearly in its null space), by about eps32 times the unpreconditioned
+// condition number, which stalls the Krylov iteration.  The FP64 diagonal
+// block therefore takes up the rounding of every off-diagonal entry of its
+// row (all 27 offsets, the lower ones read from the neighbours' stored
+// blocks as the matvec reads them), so that the FP32 operator keeps the
+// FP64 row sums exactly.
+BP_HD double rd_err32(double a) { return a - (double)(float)a; }
+
+BP_HD void make_a32_row(const DevView& v, int col, int k, size_t n) {
+  const size_t np = (size_t)v.npad;
+  const int nz = v.nz, nc = v.ncols;
+  for (int mm = 0; mm < 14; ++mm) {
+    const double2 a = v.A[(size_t)mm * np + n], b = v.A[(size_t)(14 + mm) * np + n];
+    v.A32[(size_t)mm * np + n] = float4{(float)a.x, (float)a.y, (float)b.x, (float)b.y};
+  }
+  int cn[9];
+  for (int q = 0; q < 9; ++q) cn[q] = v.col_nbr[q * nc + col];
+  double euu = 0.0, euv = 0.0, evu = 0.0, evv = 0.0;
+  for (int m = 0; m < 27; ++m) {
+    if (m == 13) continue;
+    const int kn = k + m / 9 - 1, q = m % 9;
+    if (kn < 0 || kn >= nz || cn[q] < 0) continue;
+    if (m > 13) {
+      const double2 a = v.A[(size_t)(m - 13) * np + n], b = v.A[(size_t)(m + 1) * np + n];
+      euu += rd_err32(a.x);
+      euv += rd_err32(a.y);
+      evu += rd_err32(b.x);
+      evv += rd_err32(b.y);
+    } else {
+      const size_t p = (size_t)cn[q] * nz + kn;
+      const double2 b0 = v.A[(size_t)(13 - m) * np + p], b1 = v.A[(size_t)(27 - m) * np + p];
+      euu += rd_err32(b0.x);
+      euv += rd_err32(b1.x);
+      evu += rd_err32(b0.y);
+      evv += rd_err32(b1.y);
+    }
+  }
+  const double2 d0 = v.A[n], d1 = v.A[(size_t)14 * np + n];
+  v.A32d[n] = double2{d0.x + euu, d0.y + euv};
+  v.A32d[np + n] = double2{d1.x + evu, d1.y + evv};
+}
+
+// FP32 symmetric storage, (uu, uv, vu, vv) packed per offset, with the
+// row-sum compensated diagonal block in FP64; FP64 sums.
 template <typename Src>
 BP_HD double2 matvec_row_sym32(const DevView& v, const float4* A, int col, int k, size_t n,
                                const Src& src) {
@@ -435,7 +481,11 @@ BP_HD double2 matvec_row_sym32(const DevView& v, const float4* A, int col, int k
       const size_t p = ok ? (size_t)cn[q] * nz + kn : n;
       double2 s = src(p);
       if (!ok) s = double2{0.0, 0.0};
-      if (m >= 13) {
+      if (m == 13) {
+        const double2 a0 = BP_LD_RO(v.A32d + n), a1 = BP_LD_RO(v.A32d + np + n);
+        yu += a0.x * s.x + a0.y * s.y;
+        yv += a1.x * s.x + a1.y * s.y;
+      } else if (m > 13) {
         const float4 a = BP_LD_RO(A + (size_t)(m - 13) * np + n);
         yu += (double)a.x * s.x + (double)a.y * s.y;
         yv += (double)a.z * s.x + (double)a.w * s.y;

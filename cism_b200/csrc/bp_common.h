@@ -55,7 +55,7 @@ struct InstState {
   double err;                   // |b-Ax|/|b| at the last check
   double L2_norm, L2_rel;       // residual before the linear solve
   double resid_velo;            // Picard criterion value
-  double in_rr0;                // mixed: inner initial (r,r)
+  double r_true;                // mixed: |b - A x| at the last refinement
   int pcg_iter, pcg_active, pcg_converged;
   int picard_iter, picard_active, picard_converged;
   int status;                   // bp_status
@@ -65,6 +65,9 @@ struct InstState {
   int refine_active, refine_steps, refine_steps_total;
   int inner_iter;
   int krylov_fp64;              // mixed: Krylov matvecs switched to the FP64 matrix
+  int need_true;                // mixed: the next check computes the FP64 residual
+  int restart;                  // mixed, Chronopoulos-Gear: next pass restarts (beta = 0)
+  int last_true_iter;           // mixed: pcg_iter of the last refinement
 };
 
 // Global counters polled by the host.
@@ -114,12 +117,17 @@ struct DevView {
   // holds stencil offsets m = 13..26 (diagonal first), the lower half being
   // read from the neighbour's row.
   double2* A;
-  float4* A32;             // mixed: [14][npad] (uu, uv, vu, vv) of offsets 13..26 in FP32
+  // mixed: [14][npad] (uu, uv, vu, vv) of offsets 13..26 in FP32 (entry 0,
+  // the diagonal block, unused by the matvec) and the diagonal block in
+  // FP64 [2][npad], carrying the rounding of its row's off-diagonal
+  // entries so that the row sums are those of the FP64 matrix
+  float4* A32;
+  double2* A32d;
   double* badj;            // [4][npad] Dirichlet column moves per block
   // vectors (per node, (u,v) pairs)
   double2 *x, *b, *r, *z, *d0, *q, *Az, *Dinv, *usav;
   // reductions
-  double* partials;        // [2][ntiles]
+  double* partials;        // [3][ntiles]
   unsigned* tile_counter;  // [ninst]
 };
 

@@ -184,8 +184,11 @@ DevView make_view(Arena& a, cudaStream_t s, const HostPlan& p, bool with_cells, 
   v.Az = a.get<double2>(s, "Az", np);
   v.Dinv = a.get<double2>(s, "Dinv", np);
   v.usav = a.get<double2>(s, "usav", np);
-  if (mixed && v.sym) v.A32 = a.get<float4>(s, "A32", 14 * np);
-  v.partials = a.get<double>(s, "partials", 2 * (size_t)std::max(p.ntiles, 1));
+  if (mixed && v.sym) {
+    v.A32 = a.get<float4>(s, "A32", 14 * np);
+    v.A32d = a.get<double2>(s, "A32d", 2 * np);
+  }
+  v.partials = a.get<double>(s, "partials", 3 * (size_t)std::max(p.ntiles, 1));
   v.tile_counter = a.get<unsigned>(s, "tile_counter", p.ninst);
   CK(cudaMemsetAsync(v.tile_counter, 0, sizeof(unsigned) * p.ninst, s));
   return v;
@@ -276,14 +279,19 @@ enum { C_MV = 0, C_UPD = 1, C_CHECK = 2, C_MV32 = 3, C_UPD32 = 4, C_ASM1 = 5, C_
 void enqueue_iteration(bp_problem* P, int variant, bool check) {
   const DevView& v = P->v;
   cudaStream_t s = P->c->stream;
+  // mixed precision: the recurrence runs on through check iterations and
+  // the check is the conditional refinement step
+  const bool refine = v.A32 != nullptr;
+  const bool upd_check = check && !refine;
+  const int check_mode = refine ? MV_REFINE : MV_CHECK;
   if (variant == 3) {
     L(P, C_MV, [&] { launch_mv(MV_CG1, v, s); });
-    L(P, C_UPD, [&] { launch_cg_update(check, v, s); });
-    if (check) L(P, C_CHECK, [&] { launch_mv(MV_CHECK, v, s); });
+    L(P, C_UPD, [&] { launch_cg_update(upd_check, v, s); });
+    if (check) L(P, C_CHECK, [&] { launch_mv(check_mode, v, s); });
   } else {
     L(P, C_MV, [&] { launch_mv(MV_STD_A, v, s); });
-    L(P, C_UPD, [&] { launch_std_update(check, v, s); });
-    if (check) L(P, C_CHECK, [&] { launch_mv(MV_CHECK, v, s); });
+    L(P, C_UPD, [&] { launch_std_update(upd_check, v, s); });
+    if (check) L(P, C_CHECK, [&] { launch_mv(check_mode, v, s); });
     L(P, C_UPD, [&] { launch_std_dir(v, s); });
   }
 }
@@ -350,14 +358,25 @@ void linear_solve(bp_problem* P) {
   run_pcg_fp64(P);
 }
 
-// Autotuner: after the first assembly of a problem, time the Krylov matvec
-// in each (occupancy target, grid) variant on the problem's own matrix and
-// keep the fastest for every tile kernel; results are cached per context
-// by (size bucket, nz, storage, precision).
+// Autotuner: after the first assembly of a problem, time the residual
+// matvec r = b - A x (the Krylov matvec's structure: same row gather, fused
+// dot products and scalar tail; idempotent before the linear solve, which
+// recomputes it) in each (occupancy target, grid) variant on the problem's
+// own matrix and keep the fastest for every tile kernel; results are cached
+// per context by (size bucket, nz, storage, precision).
 void autotune(bp_problem* P) {
   bp_ctx* c = P->c;
   DevView& v = P->v;
   P->tuned = true;
+  // BP_MV_CONFIG="minb,grid" fixes the choice (for sweeps)
+  if (const char* e = std::getenv("BP_MV_CONFIG")) {
+    int mb = 0, g = 0;
+    if (std::sscanf(e, "%d,%d", &mb, &g) == 2) {
+      v.minb = mb;
+      v.grid_cap = g;
+      return;
+    }
+  }
   const auto key = std::make_tuple(P->plan.nnodes >> 14, P->plan.nz, v.sym, v.A32 ? 1 : 0);
   auto it = c->tuned.find(key);
   if (it != c->tuned.end()) {
@@ -365,8 +384,6 @@ void autotune(bp_problem* P) {
     v.grid_cap = it->second.second;
     return;
   }
-  const int store = v.sym ? (v.A32 ? 2 : 1) : 0;
-  if (v.A32) launch_make_a32(v, c->stream);
   const int grids[2] = {0, 4 * c->num_sms};
   const int minbs[2] = {0, 4};
   float best = 1e30f;
@@ -374,9 +391,11 @@ void autotune(bp_problem* P) {
   for (int mb : minbs)
     for (int g : grids) {
       if (g > 0 && g >= P->plan.ntiles) continue;  // same as one CTA per tile
-      launch_tune_mv(store, mb, g, v, c->stream);
+      v.minb = mb;
+      v.grid_cap = g;
+      launch_mv(MV_INIT, v, c->stream);
       CK(cudaEventRecord(c->r0, c->stream));
-      for (int i = 0; i < 5; ++i) launch_tune_mv(store, mb, g, v, c->stream);
+      for (int i = 0; i < 5; ++i) launch_mv(MV_INIT, v, c->stream);
       CK(cudaEventRecord(c->r1, c->stream));
       CK(cudaEventSynchronize(c->r1));
       float ms = 0.f;
@@ -694,6 +713,7 @@ int bp_problem_tune_mv(bp_problem* P, int store, int minb, int grid, int reps, f
   bp_ctx* c = P->c;
   if (store == 2 && P->v.sym && !P->v.A32) {
     P->v.A32 = P->arena->get<float4>(c->stream, "A32", 14 * (size_t)P->plan.npad);
+    P->v.A32d = P->arena->get<double2>(c->stream, "A32d", 2 * (size_t)P->plan.npad);
     launch_make_a32(P->v, c->stream);
   }
   if (launch_tune_mv(store, minb, grid, P->v, c->stream) != 0) return BP_ERR_ARGS;  // warm
@@ -705,7 +725,10 @@ int bp_problem_tune_mv(bp_problem* P, int store, int minb, int grid, int reps, f
   float t = 0.f;
   CK(cudaEventElapsedTime(&t, c->r0, c->r1));
   if (ms) *ms = t / std::max(1, reps);
-  if (store == 2 && !P->mixed) P->v.A32 = nullptr;  // keep the FP64 path unchanged
+  if (store == 2 && !P->mixed) {  // keep the FP64 path unchanged
+    P->v.A32 = nullptr;
+    P->v.A32d = nullptr;
+  }
   return BP_OK;
   GUARD_END
 }

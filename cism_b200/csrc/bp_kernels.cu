@@ -151,6 +151,10 @@ __global__ void k_picard_begin(DevView v) {
     S.inner_iter = 0;
     S.pcg_iters_last = 0;
     S.krylov_fp64 = 0;
+    S.need_true = 0;
+    S.restart = 0;
+    S.last_true_iter = 0;
+    S.r_true = 0.0;
     ++mine;
   }
   atomicAdd(&cnt, mine);
@@ -316,15 +320,34 @@ __device__ __forceinline__ double2 mv_row(const DevView& v, int col, int k, size
   return matvec_row_sym32(v, v.A32, col, k, n, src);
 }
 
+// Mixed precision (iterative refinement): the Krylov iteration runs on the
+// FP32 matrix with FP64 vectors and reductions; the FP64 residual b - A x
+// replaces the recurrence residual only once the latter has fallen by
+// inner_tol since the last replacement (or below the final tolerance, or
+// after 500 iterations), and each replacement restarts the Krylov process,
+// so every cycle is a clean conjugate-gradient solve of A32 e = r.  Called
+// after iteration pcg_iter; replacements follow iterations that are
+// multiples of ncheck.
+__device__ __forceinline__ void refine_request(const InstParams& ip, InstState& S, double rr) {
+  if (S.pcg_iter % ip.ncheck != 0) return;
+  const double rn = sqrt(rr);
+  if (rn < ip.inner_tol * S.r_true || rn < 0.5 * ip.pcg_tol * S.L2_rhs ||
+      S.pcg_iter - S.last_true_iter >= 500)
+    S.need_true = 1;
+}
+
 // r = b - A x with the FP64 matrix; z = D^-1 r stored; (r,z) and (r,r).
 // MV_INIT starts a linear solve (also compute_residual_vector_3d's norms);
-// MV_CHECK is the every-ncheck true residual (pcg:478-536, 1542-1597).
+// MV_CHECK is the every-ncheck true residual (pcg:478-536, 1542-1597);
+// MV_REFINE the mixed-precision refinement step, for instances that
+// requested it.
 template <int MODE, int STORE, int MINB>
 __global__ void __launch_bounds__(kTile, MINB) k_resid(DevView v) {
   constexpr int ST64 = STORE == ST_SYM32 ? ST_SYM : STORE;
   for (int t = blockIdx.x; t < v.ntiles; t += gridDim.x) {
     const TileRange R = tile_range(v, t);
-    if (!v.st[R.inst].pcg_active) continue;
+    const InstState& S0 = v.st[R.inst];
+    if (!S0.pcg_active || (MODE == MV_REFINE && !S0.need_true)) continue;
     const int n = R.n0 + threadIdx.x;
     double part[2] = {0.0, 0.0};
     if (n < R.nend) {
@@ -341,29 +364,42 @@ __global__ void __launch_bounds__(kTile, MINB) k_resid(DevView v) {
     tile_finish<2, false>(v, t, R.inst, part, [&](int inst, const double* s) {
       InstState& S = v.st[inst];
       const InstParams& ip = v.inst[inst];
+      const double rt = sqrt(s[1]);
       if (MODE == MV_INIT) {
-        S.L2_norm = sqrt(s[1]);
+        S.L2_norm = rt;
         S.L2_rel = S.L2_rhs > 0.0 ? S.L2_norm / S.L2_rhs : 0.0;
+        S.r_true = rt;
+        S.last_true_iter = S.pcg_iter;
       } else {
-        S.err = sqrt(s[1]) / S.L2_rhs;
+        S.err = rt / S.L2_rhs;
         S.refine_steps_total += 1;
+        if (MODE == MV_REFINE) {
+          S.need_true = 0;
+          S.last_true_iter = S.pcg_iter;
+        }
         if (S.err < ip.pcg_tol) { pcg_stop(v, S, true); return; }
         if (S.pcg_iter >= ip.pcg_maxiters) { pcg_stop(v, S, false); return; }
-        // mixed: the last decades of the solve use the FP64 matrix
-        if (STORE == ST_SYM32 && S.err < ip.inner_tol) S.krylov_fp64 = 1;
+        if (MODE == MV_REFINE) {
+          // a cycle that did not halve the residual: the FP32 operator is
+          // too coarse for this system, finish with the FP64 matrix
+          if (rt > 0.5 * S.r_true) S.krylov_fp64 = 1;
+          S.r_true = rt;
+        }
       }
       if (ip.variant != 3) {  // standard PCG: eta1 of the next iteration
         if (is_nan(s[0])) { fail(v, S, BP_ERR_NAN); return; }
-        S.beta = s[0] / S.rz;
+        S.beta = MODE == MV_REFINE ? 0.0 : s[0] / S.rz;  // refinement restarts: d = z
         S.rz = s[0];
         if (MODE == MV_CHECK) S.pcg_iter += 1;
+      } else if (MODE == MV_REFINE) {
+        S.restart = 1;
       }
     });
   }
 }
 
-// Krylov matvec of the mixed path: FP32 matrix until the instance's true
-// residual falls below inner_tol, FP64 after.  In timing runs the nodes
+// Krylov matvec of the mixed path: FP32 matrix unless the instance's
+// refinement stalled (krylov_fp64), FP64 then.  In timing runs the nodes
 // through each precision are counted, to turn the measured time into bytes.
 template <int STORE>
 __device__ __forceinline__ double2 krylov_row(const DevView& v, const InstState& S, int col, int k,
@@ -416,7 +452,7 @@ __global__ void __launch_bounds__(kTile) k_std_update(DevView v) {
     if (!S.pcg_active) continue;
     const int n = R.n0 + threadIdx.x;
     const double alpha = S.alpha;
-    double part[1] = {0.0};
+    double part[2] = {0.0, 0.0};
     if (n < R.nend) {
       const double2 d = v.d0[n];
       double2 x = v.x[n];
@@ -432,15 +468,18 @@ __global__ void __launch_bounds__(kTile) k_std_update(DevView v) {
         v.r[n] = r;
         v.z[n] = make_double2(zu, zv);
         part[0] = r.x * zu + r.y * zv;
+        part[1] = r.x * r.x + r.y * r.y;
       }
     }
     if (!CHECK) {
-      tile_finish<1, false>(v, t, R.inst, part, [&](int inst, const double* s) {
+      tile_finish<2, false>(v, t, R.inst, part, [&](int inst, const double* s) {
         InstState& S2 = v.st[inst];
-        if (S2.pcg_iter >= v.inst[inst].pcg_maxiters) { pcg_stop(v, S2, false); return; }
+        const InstParams& ip = v.inst[inst];
+        if (S2.pcg_iter >= ip.pcg_maxiters) { pcg_stop(v, S2, false); return; }
         if (is_nan(s[0])) { fail(v, S2, BP_ERR_NAN); return; }
         S2.beta = s[0] / S2.rz;
         S2.rz = s[0];
+        if (v.A32) refine_request(ip, S2, s[1]);
         S2.pcg_iter += 1;
       });
     }
@@ -477,7 +516,7 @@ __global__ void __launch_bounds__(kTile, MINB) k_cg_mv(DevView v) {
     if (!S0.pcg_active) continue;
     count_tile<STORE>(v, S0, R);
     const int n = R.n0 + threadIdx.x;
-    double part[2] = {0.0, 0.0};
+    double part[3] = {0.0, 0.0, 0.0};
     if (n < R.nend) {
       const int col = n / v.nz, k = n - col * v.nz;
       const double2 y = krylov_row<STORE>(v, S0, col, k, n, v.z);
@@ -490,8 +529,9 @@ __global__ void __launch_bounds__(kTile, MINB) k_cg_mv(DevView v) {
       }
       part[0] = r.x * z.x + r.y * z.y;
       part[1] = y.x * z.x + y.y * z.y;
+      part[2] = r.x * r.x + r.y * r.y;
     }
-    tile_finish<2, false>(v, t, R.inst, part, [&](int inst, const double* s) {
+    tile_finish<3, false>(v, t, R.inst, part, [&](int inst, const double* s) {
       InstState& S = v.st[inst];
       if (FIRST) {
         S.rz_old = s[0];
@@ -509,14 +549,22 @@ __global__ void __launch_bounds__(kTile, MINB) k_cg_mv(DevView v) {
         return;
       }
       const double rho = s[0], delta = s[1];
-      const double beta = rho / S.rz_old;
-      const double sigma = delta - beta * rho / S.alpha;
+      double beta, sigma;
+      if (S.restart) {  // after a refinement: d = z, q = A z (the first pass)
+        beta = 0.0;
+        sigma = delta;
+        S.restart = 0;
+      } else {
+        beta = rho / S.rz_old;
+        sigma = delta - beta * rho / S.alpha;
+      }
       const double alpha = rho / sigma;
       S.rz_old = rho;
       S.beta = beta;
       S.sigma = sigma;
       if (is_nan(alpha)) { fail(v, S, BP_ERR_NAN); return; }
       S.alpha = alpha;
+      if (v.A32) refine_request(ip, S, s[2]);
     });
   }
 }
@@ -551,6 +599,7 @@ __global__ void __launch_bounds__(kTile) k_cg_update(DevView v) {
     if (!S.pcg_active) continue;
     const int n = R.n0 + threadIdx.x;
     if (n >= R.nend) continue;
+    const bool keep_r = !CHECK && !S.need_true;  // a refinement recomputes r and z
     const double alpha = S.alpha, beta = S.beta;
     const double2 z = v.z[n], az = v.Az[n];
     double2 d = v.d0[n], q = v.q[n], x = v.x[n];
@@ -560,7 +609,7 @@ __global__ void __launch_bounds__(kTile) k_cg_update(DevView v) {
     v.d0[n] = d;
     v.q[n] = q;
     v.x[n] = x;
-    if (!CHECK) {
+    if (keep_r) {
       const double2 r = v.r[n], di = v.Dinv[n];
       const double ru = r.x - alpha * q.x, rv = r.y - alpha * q.y;
       v.r[n] = make_double2(ru, rv);
@@ -624,18 +673,16 @@ __global__ void __launch_bounds__(kTile) k_picard_check(DevView v) {
 // iteration; the every-ncheck true residual r = b - A x stays FP64, so the
 // iteration is a reliable-update PCG that converges to the FP64 solution.
 // ---------------------------------------------------------------------
+// FP32 copy of the symmetric matrix with the row-sum compensated FP64
+// diagonal block (make_a32_row).
 __global__ void __launch_bounds__(kTile) k_make_a32(DevView v) {
   for (int t = blockIdx.x; t < v.ntiles; t += gridDim.x) {
     const TileRange R = tile_range(v, t);
     if (!v.st[R.inst].pcg_active) continue;
     const int n = R.n0 + threadIdx.x;
     if (n >= R.nend) continue;
-    const size_t np = (size_t)v.npad;
-#pragma unroll
-    for (int mm = 0; mm < 14; ++mm) {
-      const double2 a = v.A[(size_t)mm * np + n], b = v.A[(size_t)(14 + mm) * np + n];
-      v.A32[(size_t)mm * np + n] = make_float4((float)a.x, (float)a.y, (float)b.x, (float)b.y);
-    }
+    const int col = n / v.nz, k = n - col * v.nz;
+    make_a32_row(v, col, k, (size_t)n);
   }
 }
 
@@ -736,6 +783,7 @@ static void launch_mv_store(int mode, const DevView& v, cudaStream_t s, int g) {
   switch (mode) {
     case MV_INIT: k_resid<MV_INIT, STORE, MINB><<<g, kTile, 0, s>>>(v); break;
     case MV_CHECK: k_resid<MV_CHECK, STORE, MINB><<<g, kTile, 0, s>>>(v); break;
+    case MV_REFINE: k_resid<MV_REFINE, STORE, MINB><<<g, kTile, 0, s>>>(v); break;
     case MV_STD_A: k_std_mv<STORE, MINB><<<g, kTile, 0, s>>>(v); break;
     case MV_CG_FIRST: k_cg_mv<true, STORE, MINB><<<g, kTile, 0, s>>>(v); break;
     default: k_cg_mv<false, STORE, MINB><<<g, kTile, 0, s>>>(v); break;

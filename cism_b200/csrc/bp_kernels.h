@@ -7,7 +7,7 @@
 
 namespace bp {
 
-enum MvMode { MV_INIT = 0, MV_STD_A = 1, MV_CG_FIRST = 2, MV_CG1 = 3, MV_CHECK = 4 };
+enum MvMode { MV_INIT = 0, MV_STD_A = 1, MV_CG_FIRST = 2, MV_CG1 = 3, MV_CHECK = 4, MV_REFINE = 5 };
 
 cudaError_t upload_ref_tables();
 

@@ -190,7 +190,7 @@ bool build_plan(const bp_inputs* in, int n, HostPlan* p, std::string* err) {
     ip.dx = I.dx; ip.dy = I.dy;
     ip.efvs_constant = I.efvs_constant;
     ip.pcg_tol = I.pcg_tol;
-    ip.inner_tol = I.inner_tol > 0.0 ? I.inner_tol : 1.0e-6;
+    ip.inner_tol = I.inner_tol > 0.0 ? I.inner_tol : 1.0e-4;
     for (int k = 0; k < nz; ++k) ip.sigma[k] = I.sigma[k];
     ip.which_efvs = I.which_efvs;
     ip.which_babc = I.which_babc;

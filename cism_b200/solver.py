@@ -159,7 +159,7 @@ class Prepared:
         self._keep = keep
 
 
-def make_model_struct(m: configs.BPModel, precision: int = FP64, inner_tol: float = 1e-6):
+def make_model_struct(m: configs.BPModel, precision: int = FP64, inner_tol: float = 1e-4):
     keep = []
 
     def f(a):
@@ -190,7 +190,7 @@ def make_model_struct(m: configs.BPModel, precision: int = FP64, inner_tol: floa
 
 
 def prepare(m: configs.BPModel, uvel=None, vvel=None, precision: int = FP64,
-            inner_tol: float = 1e-6) -> tuple:
+            inner_tol: float = 1e-4) -> tuple:
     """Host setup (bp_setup): returns (Prepared, uvel, vvel)."""
     nx, ny, nz = m.nx, m.ny, m.nz
     arrays = {
@@ -259,7 +259,7 @@ class Context:
         return u, v, efvs, st.as_dict()
 
     def velo_higher_solve(self, m: configs.BPModel, uvel=None, vvel=None, precision: int = FP64,
-                          inner_tol: float = 1e-6):
+                          inner_tol: float = 1e-4):
         """glissade_velo_higher_solve: host setup + device Picard loop."""
         prep, u, v = prepare(m, uvel, vvel, precision, inner_tol)
         return self.solve_prepared(prep, u, v)
@@ -423,5 +423,5 @@ def default_context() -> Context:
 
 
 def velo_higher_solve(m: configs.BPModel, uvel=None, vvel=None, precision: int = FP64,
-                      inner_tol: float = 1e-6):
+                      inner_tol: float = 1e-4):
     return default_context().velo_higher_solve(m, uvel, vvel, precision, inner_tol)

@@ -81,9 +81,9 @@ typedef struct {
   int pcg_ncheck;               /* reference: 5 */
   double pcg_tol;               /* reference: 1e-8 */
   int precision;                /* bp_precision */
-  double inner_tol;             /* BP_MIXED: true relative residual below which the Krylov
-                                   matvecs switch from the FP32 to the FP64 matrix
-                                   (<= 0: 1e-6) */
+  double inner_tol;             /* BP_MIXED: residual reduction of one refinement cycle
+                                   (FP32-matrix Krylov solve between two FP64
+                                   residuals; <= 0: 1e-4) */
 } bp_inputs;
 
 typedef struct {

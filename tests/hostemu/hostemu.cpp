@@ -113,13 +113,11 @@ extern "C" int emu_matvec_sym(int nx, int ny, int nz, int periodic, const int* a
   std::vector<double2> As(2 * 14 * (size_t)E.p.npad);
   gather_matrix_sym(E.p, Auu, Auv, Avu, Avv, As.data());
   std::vector<float4> A32(14 * (size_t)E.p.npad);
-  for (size_t mm = 0; mm < 14; ++mm)
-    for (int n = 0; n < E.p.npad; ++n) {
-      const double2 a = As[mm * E.p.npad + n], b = As[(14 + mm) * E.p.npad + n];
-      A32[mm * E.p.npad + n] = float4{(float)a.x, (float)a.y, (float)b.x, (float)b.y};
-    }
+  std::vector<double2> A32d(2 * (size_t)E.p.npad);
   E.v.A = As.data();
   E.v.A32 = A32.data();
+  E.v.A32d = A32d.data();
+  for (int n = 0; n < E.p.nnodes; ++n) make_a32_row(E.v, n / nz, n % nz, (size_t)n);
   gather_velocity(E.p, 0, xu, xv, E.x.data());
   std::vector<double2> y(E.p.npad, double2{0, 0});
   const double2* xs = E.x.data();

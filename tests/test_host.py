@@ -119,3 +119,28 @@ def test_context_needs_a_device():
     with pytest.raises(solver.BPError) as e:
         solver.Context(0)
     assert e.value.code == 11
+
+
+@pytest.mark.parametrize("m", MODELS[:4], ids=lambda m: m.name)
+def test_fp32_copy_keeps_row_sums(m):
+    """The FP32 matrix of the mixed path carries the rounding of each row in
+    its FP64 diagonal block: on the translation fields (u = 1, v = 0 and
+    u = 0, v = 1) it gives the FP64 product to summation rounding, where an
+    entry-wise FP32 copy is off by about eps32 times the row's entries."""
+    emu = C.CDLL(EMU)
+    su, u, v, A, bu, bv, efvs = oracle_system(m, seed=4, scale=10.0)
+    av = np.ascontiguousarray(su["active_vertex"], np.int32)
+    one = configs.halo_fill_stag(np.ones(m.vshape3) * av[..., None], m.periodic)
+    zero = np.zeros(m.vshape3)
+    scale = max(np.abs(a).max() for a in A)
+    for xu, xv in ((one, zero), (zero, one)):
+        out = []
+        for fp32 in (0, 1):
+            eyu, eyv = np.zeros(m.vshape3), np.zeros(m.vshape3)
+            rc = emu.emu_matvec_sym(m.nx, m.ny, m.nz, m.periodic, _p(av),
+                                    *[_p(np.ascontiguousarray(a)) for a in A], _p(xu), _p(xv),
+                                    _p(eyu), _p(eyv), fp32)
+            assert rc == 0
+            out.append((eyu, eyv))
+        diff = max(np.abs(out[0][0] - out[1][0]).max(), np.abs(out[0][1] - out[1][1]).max())
+        assert diff <= 1e-13 * scale
