@@ -55,7 +55,8 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c1", choices=sorted(WORKLOAD_DESC))
-    ap.add_argument("--precision", default="best", choices=["best", "fp64", "mixed"])
+    ap.add_argument("--precision", default="best",
+                    choices=["best", "fp64", "mixed", "sia_fp64", "learned_fp64", "learned_mixed"])
     ap.add_argument("--pcg-maxiters", type=int, default=3000)
     ap.add_argument("--refine-eta", type=float, default=1e-4,
                     help="mixed path: residual reduction of one FP32 refinement cycle")
@@ -242,6 +243,21 @@ def load_counts(workload):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
+def _net_launches():
+    mod = sys.modules.get("cism_b200.net")
+    return mod.LAUNCHES if mod is not None else 0
+
+
+def load_guess_net(m):
+    """The trained U-Net for the workload's domain family, if shipped."""
+    path = os.path.join(ROOT, "cism_b200", "weights", "unet_slab.npz")
+    if not (m.periodic and os.path.exists(path)):
+        return None
+    from cism_b200 import net
+
+    return net.UNet.load(path)
+
+
 def run_ours(args, D):
     import numpy as np
 
@@ -249,25 +265,53 @@ def run_ours(args, D):
 
     ctx = solver.Context(D.local)
     m = make_model(args.workload, args.pcg_maxiters)
-    paths = ["fp64", "mixed"] if args.precision == "best" else [args.precision]
+    net_model = load_guess_net(m)
+    if args.precision == "best":
+        paths = ["fp64", "mixed", "sia_fp64"]
+        if net_model is not None:
+            paths += ["learned_fp64", "learned_mixed"]
+    else:
+        paths = [args.precision]
     res = {}
     sol = {}
     for path in paths:
-        prec = solver.MIXED if path == "mixed" else solver.FP64
+        prec = solver.MIXED if path.endswith("mixed") else solver.FP64
         prep, u0, v0 = solver.prepare(m, precision=prec, inner_tol=args.refine_eta)
         prob = ctx.problem([prep])
-        prob.set_guess([u0], [v0])
+        start = path.split("_")[0] if "_" in path else "zero"
+
+        def make_guess():
+            # the guess is part of every timed step (network inference included)
+            if start == "learned":
+                from cism_b200 import guess
+                return guess.learned_guesses(net_model, [m])[0]
+            if start == "sia":
+                from cism_b200 import guess
+                return guess.sia_guess(m)
+            return u0, v0
+
+        def step():
+            gu, gv = make_guess()
+            prob.set_guess([gu], [gv])
+            return prob.run()[0]
+
         for _ in range(args.warmup):
-            prob.run()
+            step()
         D.barrier()
         clocks = Clocks(D.local)
         clocks.start()
         ctx.timer_start()
-        sts = [prob.run()[0] for _ in range(args.steps)]
+        t0 = time.perf_counter()
+        net_l0 = _net_launches()
+        sts = [step() for _ in range(args.steps)]
+        wall = (time.perf_counter() - t0) * 1000.0
+        net_launches = (_net_launches() - net_l0) // max(1, args.steps)
         ms = ctx.timer_stop()
         ck = clocks.stop()
         D.barrier()
-        ms_max = D.max(ms)
+        # device time of the solver stream; with a guess computed on the host
+        # or by the network on another stream, the wall time of the steps
+        ms_max = D.max(ms if start == "zero" else max(ms, wall))
         us, vs, _ = prob.get()
         sol[path] = (us[0], vs[0])
         st = sts[-1]
@@ -279,8 +323,9 @@ def run_ours(args, D):
         prob.timing(False)
         info = prob.info()
         info.update({"mv_nodes_fp64": n64, "mv_nodes_fp32": n32, "tuned_minb": minb, "tuned_grid": grid})
-        launches = sum(n for _, n in kt.values())
+        launches = sum(n for _, n in kt.values()) + net_launches
         res[path] = {"value": D.world * args.steps / (ms_max / 1000.0), "ms_per_step": ms_max / args.steps,
+                     "make_guess": make_guess,
                      "status": st["status"], "picard_iters": st["picard_iters"],
                      "pcg_iters_total": st["pcg_iters_total"], "refine_steps": st["refine_steps_total"],
                      "final_rel_resid": st["pcg_err_last"], "kernel_times": kt, "info": info,
@@ -292,26 +337,33 @@ def run_ours(args, D):
         den = math.sqrt(float(np.sum(uf ** 2 + vf ** 2)))
         for path, (u, v) in sol.items():
             res[path]["rel_l2_vs_fp64"] = math.sqrt(float(np.sum((u - uf) ** 2 + (v - vf) ** 2))) / den
+    # accepted: the reference's convergence criteria met (Picard max speed
+    # change < 1e-4, last linear solve < 1e-8) and, from the same start, the
+    # FP64 answer within 1e-6; from another start the Picard iteration stops
+    # at a different point of the same tolerance, so there within 1e-3
     ok = [p for p in paths if res[p]["status"] == 0 and res[p]["final_rel_resid"] < 1e-8
-          and res[p].get("rel_l2_vs_fp64", 0.0) <= 1e-6]
+          and res[p].get("rel_l2_vs_fp64", 0.0) <= (1e-6 if p in ("fp64", "mixed") else 1e-3)]
     head = max(ok, key=lambda p: res[p]["value"]) if ok else paths[0]
     H = res[head]
     # e2e: the C-ABI call with host buffers (plan, H2D, solve, D2H per step)
     prep = H["prep"]
     for _ in range(max(1, args.warmup // 2)):
-        ctx.solve_prepared(prep, H["u0"], H["v0"], want_efvs=False)
+        gu, gv = H["make_guess"]()
+        ctx.solve_prepared(prep, gu, gv, want_efvs=False)
     D.barrier()
     ctx.timer_start()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        _, _, _, st_e = ctx.solve_prepared(prep, H["u0"], H["v0"], want_efvs=False)
+        gu, gv = H["make_guess"]()
+        _, _, _, st_e = ctx.solve_prepared(prep, gu, gv, want_efvs=False)
     ms_e = ctx.timer_stop()
     wall_e = (time.perf_counter() - t0) * 1000.0
     D.barrier()
     ms_e = D.max(max(ms_e, wall_e))
     e2e = {"value": D.world * args.steps / (ms_e / 1000.0), "unit": UNIT,
            "h2d_bytes_per_step": int(st_e["h2d_bytes"]), "d2h_bytes_per_step": int(st_e["d2h_bytes"]),
-           "call": "bp_solve (C ABI) on host arrays"}
+           "call": "guess (host fields -> network on the GPU -> host) + bp_solve (C ABI) on host arrays"
+                   if head.startswith("learned") else "bp_solve (C ABI) on host arrays"}
     # roofline of the dominant kernel: the Krylov matvec (FP32 matrix until
     # the true residual reaches the switch tolerance on the mixed path)
     kms, kn = H["kernel_times"]["pcg_matvec_fp64"]
@@ -326,8 +378,9 @@ def run_ours(args, D):
     achieved = total_bytes / (kms / 1000.0) / 1e9 if kn else 0.0
     traffic = matvec_traffic(N, head)
     roof = {"bound": "hbm",
-            "kernel": ("k_std_mv<ST_SYM32> (Krylov q = A d, FP32 symmetric matrix, FP64 at the end)"
-                       if head == "mixed" else "k_std_mv<ST_SYM> (Krylov q = A d, FP64 symmetric matrix)"),
+            "kernel": ("k_std_mv<ST_SYM32> (Krylov q = A d, FP32 symmetric matrix, row-sum compensated FP64 "
+                       "diagonal)" if head.endswith("mixed") else
+                       "k_std_mv<ST_SYM> (Krylov q = A d, FP64 symmetric matrix)"),
             "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)",
             "traffic": traffic, "algorithmic_bytes_per_launch": round(bytes_launch),
@@ -337,7 +390,8 @@ def run_ours(args, D):
     out = {
         "metric": METRIC, "value": round(H["value"], 4), "unit": UNIT, "n_gpus": D.world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(H["ms_per_step"], 3),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64" if head == "fp64" else "f32+f64",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": ("f32+f64" if head.endswith("mixed") else "f64") + ("+bf16" if head.startswith("learned") else ""),
         "data": "synthetic (seeded geometry generator, no dataset)",
         "config": {"workload": WORKLOAD_DESC[args.workload], "name": args.workload, "path": head,
                    "nodes": H["info"]["nodes"], "columns": H["info"]["columns"],
@@ -353,6 +407,7 @@ def run_ours(args, D):
                       if k in ("value", "ms_per_step", "status", "picard_iters", "pcg_iters_total",
                                "refine_steps")}
                   | {"final_rel_resid": float("%.3e" % r["final_rel_resid"]),
+                     "start": "zero" if p in ("fp64", "mixed") else p.split("_")[0],
                      "rel_l2_vs_fp64": float("%.3e" % r.get("rel_l2_vs_fp64", 0.0))}
                   for p, r in res.items()},
     }

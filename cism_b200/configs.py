@@ -384,6 +384,31 @@ def _sliding_dome(gx: int, gy: int, dx: float, nz: int, rng: np.random.Generator
                    which_precond=PRECOND_DIAG, which_resid=RESID_MAXU, name=f"dome{gx}x{gy}")
 
 
+def random_slab(rng: np.random.Generator, n: int = 96, dx: float = 500.0, nz: int = 11) -> BPModel:
+    """A member of the periodic-slab family of the learned guess's training
+    and held-out sets: the slab above with a random slope (0.05-0.2 deg),
+    thickness (700-1300 m), rate factor (0.5-2 x 1e-16) and basal friction
+    beta = beta0 (1 + a sin(2 pi kx x / L + px) sin(2 pi ky y / L + py))
+    exp(s g - s^2 / 2), g a periodic unit Gaussian field (correlation 2-8
+    km), beta0 500-2000 Pa a/m, a 0-1, kx, ky in {1, 2}, s 0-0.4."""
+    theta = rng.uniform(0.05, 0.2)
+    H = rng.uniform(700.0, 1300.0)
+    flwa = 1.0e-16 * np.exp(rng.uniform(np.log(0.5), np.log(2.0)))
+    m = slab(n=n, dx=dx, nz=nz, theta_deg=theta, thickness=H, flwa=flwa)
+    L = n * dx
+    xv = (np.arange(n) + 1) * dx
+    XV, YV = np.meshgrid(xv, xv)
+    kx, ky = rng.integers(1, 3, size=2)
+    px, py = rng.uniform(0.0, 2 * np.pi, size=2)
+    beta0 = rng.uniform(500.0, 2000.0)
+    amp = rng.uniform(0.0, 1.0)
+    sig = rng.uniform(0.0, 0.4)
+    g = gaussian_random_field(rng, (n, n), dx, rng.uniform(2.0e3, 8.0e3))
+    beta_v = beta0 * (1.0 + amp * np.sin(2 * np.pi * kx * XV / L + px) * np.sin(2 * np.pi * ky * YV / L + py))
+    beta_v = beta_v * np.exp(sig * g - 0.5 * sig * sig)
+    return m.copy(beta_external=_vertex_from_owned(beta_v), name=f"rslab{n}")
+
+
 def workload(name: str) -> BPModel:
     """The named synthetic workloads."""
     if name == "c0":

@@ -1,0 +1,497 @@
+// net_kernels.cu -- BF16 kernels of the learned initial guess: a 2-D
+// U-Net over the vertex grid, trained and run on the device.
+//
+// Activations are NHWC ([pixel][channel]) in BF16; every contraction is a
+// tensor-core GEMM (mma.sync m16n8k16, BF16 operands, FP32 accumulation)
+// over K-contiguous operands:
+//   forward  Y[P][Cout]  = col(X)[P][K] . W[Cout][K]^T            (K = 9 Cin)
+//   dgrad    dcol[P][K]  = dY[P][Cout] . WT[K][Cout]^T, then col2im
+//   wgrad    dW[Cout][K] = dYT[Cout][P] . colT[K][P]^T
+// with k = tap * Cin + c, tap = (dy + 1) * 3 + (dx + 1).  Borders are
+// periodic (the doubly periodic domains) or zero.  Reductions (bias
+// gradients, the loss) run in a fixed order, so a training run is
+// deterministic.  Every entry point is extern "C" with plain device
+// pointers and the CUDA stream to launch on.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace {
+
+typedef __nv_bfloat16 bf16;
+
+// ---------------------------------------------------------------------
+// GEMM: C[m][n] = sum_k A[m][k] B[n][k] (+ bias[n]) (+ C[m][n] if accum).
+// Tiles 64 x 64 x 32, 4 warps of 32 x 32, cp.async double buffering.
+// K, lda, ldb multiples of 8 (16-byte rows of the 8-element chunks).
+// ---------------------------------------------------------------------
+constexpr int BM = 64, BN = 64, BK = 32, PAD = 8;
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  const int n = valid ? 16 : 0;  // src-size 0: the 16 bytes are zero-filled
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(s), "l"(gmem), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+__device__ __forceinline__ void mma_bf16(float (&c)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+__global__ void __launch_bounds__(128) k_gemm_tn(const bf16* __restrict__ A, const bf16* __restrict__ B,
+                                                 float* __restrict__ C, const float* __restrict__ bias,
+                                                 int M, int N, int K, int lda, int ldb, int ldc,
+                                                 int accum) {
+  __shared__ __align__(16) bf16 As[2][BM][BK + PAD];
+  __shared__ __align__(16) bf16 Bs[2][BN][BK + PAD];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int g = lane >> 2, t4 = lane & 3;
+  const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+  float acc[2][4][4];
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.f;
+
+  auto load = [&](int buf, int k0) {
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {  // 64 rows x 4 chunks = 256 chunks per operand
+      const int id = tid + c * 128;
+      const int r = id >> 2, ch = (id & 3) * 8;
+      const int k = k0 + ch;
+      const bool va = (m0 + r) < M && k < K;
+      const bool vb = (n0 + r) < N && k < K;
+      cp_async16(&As[buf][r][ch], va ? (const void*)(A + (size_t)(m0 + r) * lda + k) : (const void*)A, va);
+      cp_async16(&Bs[buf][r][ch], vb ? (const void*)(B + (size_t)(n0 + r) * ldb + k) : (const void*)B, vb);
+    }
+  };
+
+  const int nk = (K + BK - 1) / BK;
+  load(0, 0);
+  cp_async_commit();
+  for (int kt = 0; kt < nk; ++kt) {
+    const int buf = kt & 1;
+    if (kt + 1 < nk) {
+      load(buf ^ 1, (kt + 1) * BK);
+      cp_async_commit();
+      cp_async_wait1();
+    } else {
+      cp_async_wait0();
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < BK; kk += 16) {
+      uint32_t af[2][4], bfr[4][2];
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const int r = wm + i * 16 + g;
+        af[i][0] = *reinterpret_cast<const uint32_t*>(&As[buf][r][kk + 2 * t4]);
+        af[i][1] = *reinterpret_cast<const uint32_t*>(&As[buf][r + 8][kk + 2 * t4]);
+        af[i][2] = *reinterpret_cast<const uint32_t*>(&As[buf][r][kk + 2 * t4 + 8]);
+        af[i][3] = *reinterpret_cast<const uint32_t*>(&As[buf][r + 8][kk + 2 * t4 + 8]);
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int nn = wn + j * 8 + g;
+        bfr[j][0] = *reinterpret_cast<const uint32_t*>(&Bs[buf][nn][kk + 2 * t4]);
+        bfr[j][1] = *reinterpret_cast<const uint32_t*>(&Bs[buf][nn][kk + 2 * t4 + 8]);
+      }
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) mma_bf16(acc[i][j], af[i], bfr[j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int m = m0 + wm + i * 16 + g + (q >> 1) * 8;
+        const int n = n0 + wn + j * 8 + 2 * t4 + (q & 1);
+        if (m < M && n < N) {
+          float x = acc[i][j][q];
+          if (bias) x += bias[n];
+          float* dst = C + (size_t)m * ldc + n;
+          *dst = accum ? *dst + x : x;
+        }
+      }
+}
+
+// ---------------------------------------------------------------------
+// im2col / col2im over [B][H][W][C] with 3 x 3 taps; periodic != 0 wraps.
+// ---------------------------------------------------------------------
+__device__ __forceinline__ bool tap_pixel(int b, int y, int x, int dy, int dx, int H, int W, int periodic,
+                                          long long* p) {
+  int yy = y + dy, xx = x + dx;
+  if (periodic) {
+    yy = (yy + H) % H;
+    xx = (xx + W) % W;
+  } else if (yy < 0 || yy >= H || xx < 0 || xx >= W) {
+    return false;
+  }
+  *p = ((long long)b * H + yy) * W + xx;
+  return true;
+}
+
+__global__ void k_im2col(const bf16* __restrict__ X, bf16* __restrict__ col, int B, int H, int W, int C,
+                         int Kp, int periodic) {
+  const long long total = (long long)B * H * W * Kp;
+  for (long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x; id < total;
+       id += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(id % Kp);
+    const long long p = id / Kp;
+    bf16 val = __float2bfloat16(0.f);
+    if (k < 9 * C) {
+      const int tap = k / C, c = k - tap * C;
+      const int x = (int)(p % W), y = (int)((p / W) % H), b = (int)(p / ((long long)W * H));
+      long long q;
+      if (tap_pixel(b, y, x, tap / 3 - 1, tap % 3 - 1, H, W, periodic, &q)) val = X[q * C + c];
+    }
+    col[id] = val;
+  }
+}
+
+// dX[p][c] = sum over taps of dcol[q][tap * C + c], q the pixel whose tap
+// lands on p (gather in tap order).
+__global__ void k_col2im(const float* __restrict__ dcol, float* __restrict__ dX, int B, int H, int W, int C,
+                         int Kp, int periodic) {
+  const long long total = (long long)B * H * W * C;
+  for (long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x; id < total;
+       id += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(id % C);
+    const long long p = id / C;
+    const int x = (int)(p % W), y = (int)((p / W) % H), b = (int)(p / ((long long)W * H));
+    float s = 0.f;
+    for (int tap = 0; tap < 9; ++tap) {
+      long long q;
+      if (tap_pixel(b, y, x, -(tap / 3 - 1), -(tap % 3 - 1), H, W, periodic, &q))
+        s += dcol[q * Kp + tap * C + c];
+    }
+    dX[id] = s;
+  }
+}
+
+// [R][Cc] -> [Cc][R] (BF16), 32 x 32 tiles through shared memory.
+__global__ void k_transpose(const bf16* __restrict__ in, bf16* __restrict__ out, int R, int Cc) {
+  __shared__ bf16 tile[32][33];
+  const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+  for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+    const int r = r0 + i, c = c0 + threadIdx.x;
+    if (r < R && c < Cc) tile[i][threadIdx.x] = in[(size_t)r * Cc + c];
+  }
+  __syncthreads();
+  for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+    const int c = c0 + i, r = r0 + threadIdx.x;
+    if (r < R && c < Cc) out[(size_t)c * R + r] = tile[threadIdx.x][i];
+  }
+}
+
+// ---------------------------------------------------------------------
+// pointwise
+// ---------------------------------------------------------------------
+__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.f + erff(x * 0.70710678118654752f)); }
+__device__ __forceinline__ float gelu_grad(float x) {
+  const float cdf = 0.5f * (1.f + erff(x * 0.70710678118654752f));
+  const float pdf = 0.39894228040143268f * expf(-0.5f * x * x);
+  return cdf + x * pdf;
+}
+
+#define GRID_LOOP(id, total) \
+  for (long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x; id < (total); id += (long long)gridDim.x * blockDim.x)
+
+// Y = act(Z) in BF16 into a channel slice [p][c0 .. c0 + C) of rows of ldy.
+__global__ void k_act(const float* __restrict__ Z, bf16* __restrict__ Y, long long P, int C, int ldy, int c0,
+                      int act) {
+  GRID_LOOP(id, P * C) {
+    const long long p = id / C;
+    const int c = (int)(id % C);
+    const float z = Z[id];
+    Y[p * ldy + c0 + c] = __float2bfloat16(act ? gelu(z) : z);
+  }
+}
+
+// dZ = dY * act'(Z), dY read from a channel slice of rows of ldd (FP32).
+__global__ void k_act_grad(const float* __restrict__ Z, const float* __restrict__ dY, float* __restrict__ dZ,
+                           long long P, int C, int ldd, int c0, int act) {
+  GRID_LOOP(id, P * C) {
+    const long long p = id / C;
+    const int c = (int)(id % C);
+    const float d = dY[p * ldd + c0 + c];
+    dZ[id] = act ? d * gelu_grad(Z[id]) : d;
+  }
+}
+
+__global__ void k_f32_to_bf16(const float* __restrict__ x, bf16* __restrict__ y, long long n) {
+  GRID_LOOP(id, n) y[id] = __float2bfloat16(x[id]);
+}
+
+// Column sums db[c] = sum_p dZ[p][c] (fixed order: one thread per column
+// strides the rows, then a fixed-shape tree within the block).
+__global__ void k_colsum(const float* __restrict__ dZ, float* __restrict__ db, long long P, int C) {
+  __shared__ float sm[256];
+  const int c = blockIdx.x;
+  float s = 0.f;
+  for (long long p = threadIdx.x; p < P; p += blockDim.x) s += dZ[p * C + c];
+  sm[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) sm[threadIdx.x] += sm[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) db[c] = sm[0];
+}
+
+// 2 x 2 average pooling, [B][H][W][C] -> [B][H/2][W/2][C] (BF16).
+__global__ void k_pool(const bf16* __restrict__ X, bf16* __restrict__ Y, int B, int H, int W, int C) {
+  const int h = H / 2, w = W / 2;
+  GRID_LOOP(id, (long long)B * h * w * C) {
+    const int c = (int)(id % C);
+    const long long p = id / C;
+    const int x = (int)(p % w), y = (int)((p / w) % h), b = (int)(p / ((long long)w * h));
+    const long long q = ((long long)b * H + 2 * y) * W + 2 * x;
+    const float s = __bfloat162float(X[q * C + c]) + __bfloat162float(X[(q + 1) * C + c]) +
+                    __bfloat162float(X[(q + W) * C + c]) + __bfloat162float(X[(q + W + 1) * C + c]);
+    Y[id] = __float2bfloat16(0.25f * s);
+  }
+}
+
+// gradient of the pooling: dX[fine] += dY[coarse] / 4 (FP32, channel slice
+// of the coarse rows)
+__global__ void k_pool_grad(const float* __restrict__ dY, float* __restrict__ dX, int B, int H, int W, int C,
+                            int ldy, int c0) {
+  GRID_LOOP(id, (long long)B * H * W * C) {
+    const int c = (int)(id % C);
+    const long long p = id / C;
+    const int x = (int)(p % W), y = (int)((p / W) % H), b = (int)(p / ((long long)W * H));
+    const long long q = ((long long)b * (H / 2) + y / 2) * (W / 2) + x / 2;
+    dX[id] += 0.25f * dY[q * ldy + c0 + c];
+  }
+}
+
+// nearest 2x upsampling of [B][h][w][C] into a channel slice of the fine
+// rows (ldy)
+__global__ void k_up(const bf16* __restrict__ X, bf16* __restrict__ Y, int B, int h, int w, int C, int ldy,
+                     int c0) {
+  const int H = 2 * h, W = 2 * w;
+  GRID_LOOP(id, (long long)B * H * W * C) {
+    const int c = (int)(id % C);
+    const long long p = id / C;
+    const int x = (int)(p % W), y = (int)((p / W) % H), b = (int)(p / ((long long)W * H));
+    const long long q = ((long long)b * h + y / 2) * w + x / 2;
+    Y[p * ldy + c0 + c] = X[q * C + c];
+  }
+}
+
+// gradient of the upsampling: dX[coarse] = sum of its 4 fine pixels (fixed order)
+__global__ void k_up_grad(const float* __restrict__ dY, float* __restrict__ dX, int B, int h, int w, int C,
+                          int ldy, int c0) {
+  const int W = 2 * w;
+  GRID_LOOP(id, (long long)B * h * w * C) {
+    const int c = (int)(id % C);
+    const long long p = id / C;
+    const int x = (int)(p % w), y = (int)((p / w) % h), b = (int)(p / ((long long)w * h));
+    const long long q = ((long long)b * 2 * h + 2 * y) * W + 2 * x;
+    dX[id] = dY[q * ldy + c0 + c] + dY[(q + 1) * ldy + c0 + c] + dY[(q + W) * ldy + c0 + c] +
+             dY[(q + W + 1) * ldy + c0 + c];
+  }
+}
+
+// copy a BF16 [P][C] block into a channel slice of rows of ldy
+__global__ void k_copy_slice(const bf16* __restrict__ X, bf16* __restrict__ Y, long long P, int C, int ldy,
+                             int c0) {
+  GRID_LOOP(id, P * C) {
+    const long long p = id / C;
+    const int c = (int)(id % C);
+    Y[p * ldy + c0 + c] = X[id];
+  }
+}
+
+// dX += a channel slice of dY (FP32)
+__global__ void k_add_slice(const float* __restrict__ dY, float* __restrict__ dX, long long P, int C, int ldy,
+                            int c0) {
+  GRID_LOOP(id, P * C) {
+    const long long p = id / C;
+    const int c = (int)(id % C);
+    dX[id] += dY[p * ldy + c0 + c];
+  }
+}
+
+// Masked mean squared error over [P][C] (mask per pixel): per-block
+// partial sums in a fixed order; gradient 2 (y - t) mask / count.
+__global__ void k_mse(const float* __restrict__ Y, const float* __restrict__ T, const float* __restrict__ mask,
+                      float* __restrict__ dY, float* __restrict__ partial, long long P, int C, float inv_count) {
+  __shared__ float sm[256];
+  float s = 0.f;
+  for (long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x; id < P * C;
+       id += (long long)gridDim.x * blockDim.x) {
+    const float m = mask[id / C];
+    const float e = (Y[id] - T[id]) * m;
+    dY[id] = 2.f * e * inv_count;
+    s += e * e;
+  }
+  sm[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) sm[threadIdx.x] += sm[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[blockIdx.x] = sm[0] * inv_count;
+}
+
+// Adam on FP32 master weights; the BF16 GEMM copy W[Cout][Kp] (k < K real,
+// the padding stays zero) is refreshed in the same pass.
+__global__ void k_adam(float* __restrict__ w, const float* __restrict__ grad, float* __restrict__ m1,
+                       float* __restrict__ m2, bf16* __restrict__ wb, long long n, int K, int Kp, float lr,
+                       float b1, float b2, float eps, float c1, float c2) {
+  GRID_LOOP(id, n) {
+    const float gr = grad[id];
+    const float a = b1 * m1[id] + (1.f - b1) * gr;
+    const float b = b2 * m2[id] + (1.f - b2) * gr * gr;
+    m1[id] = a;
+    m2[id] = b;
+    const float x = w[id] - lr * (a * c1) / (sqrtf(b * c2) + eps);
+    w[id] = x;
+    if (wb) {
+      const long long r = id / K;
+      const int k = (int)(id % K);
+      wb[r * Kp + k] = __float2bfloat16(x);
+    }
+  }
+}
+
+// gradient of a padded BF16 GEMM weight [Cout][Kp] back to [Cout][K]
+__global__ void k_unpad(const float* __restrict__ src, float* __restrict__ dst, long long rows, int K, int Kp) {
+  GRID_LOOP(id, rows * K) {
+    const long long r = id / K;
+    const int k = (int)(id % K);
+    dst[id] = src[r * Kp + k];
+  }
+}
+
+inline unsigned grid_for(long long n) {
+  long long g = (n + 255) / 256;
+  if (g > 65535LL * 16) g = 65535LL * 16;
+  return (unsigned)(g < 1 ? 1 : g);
+}
+
+}  // namespace
+
+extern "C" {
+
+// Returns 0, or 10 for arguments the kernel does not take.
+int bpnet_gemm_tn(const void* A, const void* B, float* C, const float* bias, int M, int N, int K, int lda,
+                  int ldb, int ldc, int accum, void* stream) {
+  if (M <= 0 || N <= 0 || K <= 0 || (K % 8) || (lda % 8) || (ldb % 8)) return 10;
+  dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
+  k_gemm_tn<<<grid, 128, 0, (cudaStream_t)stream>>>((const bf16*)A, (const bf16*)B, C, bias, M, N, K, lda,
+                                                     ldb, ldc, accum);
+  return cudaGetLastError() == cudaSuccess ? 0 : 6;
+}
+
+int bpnet_im2col(const void* X, void* col, int B, int H, int W, int C, int Kp, int periodic, void* stream) {
+  const long long n = (long long)B * H * W * Kp;
+  k_im2col<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>((const bf16*)X, (bf16*)col, B, H, W, C, Kp, periodic);
+  return cudaGetLastError() == cudaSuccess ? 0 : 6;
+}
+
+int bpnet_col2im(const float* dcol, float* dX, int B, int H, int W, int C, int Kp, int periodic, void* stream) {
+  const long long n = (long long)B * H * W * C;
+  k_col2im<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(dcol, dX, B, H, W, C, Kp, periodic);
+  return cudaGetLastError() == cudaSuccess ? 0 : 6;
+}
+
+int bpnet_transpose(const void* in, void* out, int R, int Cc, void* stream) {
+  dim3 grid((Cc + 31) / 32, (R + 31) / 32), block(32, 8);
+  k_transpose<<<grid, block, 0, (cudaStream_t)stream>>>((const bf16*)in, (bf16*)out, R, Cc);
+  return cudaGetLastError() == cudaSuccess ? 0 : 6;
+}
+
+int bpnet_act(const float* Z, void* Y, long long P, int C, int ldy, int c0, int act, void* stream) {
+  k_act<<<grid_for(P * C), 256, 0, (cudaStream_t)stream>>>(Z, (bf16*)Y, P, C, ldy, c0, act);
+  return cudaGetLastError() == cudaSuccess ? 0 : 6;
+}
+
+int bpnet_act_grad(const float* Z, const float* dY, float* dZ, long long P, int C, int ldd, int c0, int act,
+                   void* stream) {
+  k_act_grad<<<grid_for(P * C), 256, 0, (cudaStream_t)stream>>>(Z, dY, dZ, P, C, ldd, c0, act);
+  return cudaGetLastError() == cudaSuccess ? 0 : 6;
+}
+
+int bpnet_to_bf16(const float* x, void* y, long long n, void* stream) {
+  k_f32_to_bf16<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(x, (bf16*)y, n);
+  return cudaGetLastError() == cudaSuccess ? 0 : 6;
+}
+
+int bpnet_colsum(const float* dZ, float* db, long long P, int C, void* stream) {
+  k_colsum<<<C, 256, 0, (cudaStream_t)stream>>>(dZ, db, P, C);
+  return cudaGetLastError() == cudaSuccess ? 0 : 6;
+}
+
+int bpnet_pool(const void* X, void* Y, int B, int H, int W, int C, void* stream) {
+  if ((H % 2) || (W % 2)) return 10;
+  const long long n = (long long)B * (H / 2) * (W / 2) * C;
+  k_pool<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>((const bf16*)X, (bf16*)Y, B, H, W, C);
+  return cudaGetLastError() == cudaSuccess ? 0 : 6;
+}
+
+int bpnet_pool_grad(const float* dY, float* dX, int B, int H, int W, int C, int ldy, int c0, void* stream) {
+  const long long n = (long long)B * H * W * C;
+  k_pool_grad<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(dY, dX, B, H, W, C, ldy, c0);
+  return cudaGetLastError() == cudaSuccess ? 0 : 6;
+}
+
+int bpnet_up(const void* X, void* Y, int B, int h, int w, int C, int ldy, int c0, void* stream) {
+  const long long n = (long long)B * 4 * h * w * C;
+  k_up<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>((const bf16*)X, (bf16*)Y, B, h, w, C, ldy, c0);
+  return cudaGetLastError() == cudaSuccess ? 0 : 6;
+}
+
+int bpnet_up_grad(const float* dY, float* dX, int B, int h, int w, int C, int ldy, int c0, void* stream) {
+  const long long n = (long long)B * h * w * C;
+  k_up_grad<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(dY, dX, B, h, w, C, ldy, c0);
+  return cudaGetLastError() == cudaSuccess ? 0 : 6;
+}
+
+int bpnet_copy_slice(const void* X, void* Y, long long P, int C, int ldy, int c0, void* stream) {
+  k_copy_slice<<<grid_for(P * C), 256, 0, (cudaStream_t)stream>>>((const bf16*)X, (bf16*)Y, P, C, ldy, c0);
+  return cudaGetLastError() == cudaSuccess ? 0 : 6;
+}
+
+int bpnet_add_slice(const float* dY, float* dX, long long P, int C, int ldy, int c0, void* stream) {
+  k_add_slice<<<grid_for(P * C), 256, 0, (cudaStream_t)stream>>>(dY, dX, P, C, ldy, c0);
+  return cudaGetLastError() == cudaSuccess ? 0 : 6;
+}
+
+// partial must hold 256 floats; the loss is the sum of them (host side).
+int bpnet_mse(const float* Y, const float* T, const float* mask, float* dY, float* partial, long long P, int C,
+              float inv_count, void* stream) {
+  k_mse<<<256, 256, 0, (cudaStream_t)stream>>>(Y, T, mask, dY, partial, P, C, inv_count);
+  return cudaGetLastError() == cudaSuccess ? 0 : 6;
+}
+
+int bpnet_adam(float* w, const float* grad, float* m1, float* m2, void* wb, long long n, int K, int Kp,
+               float lr, float b1, float b2, float eps, float c1, float c2, void* stream) {
+  k_adam<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(w, grad, m1, m2, (bf16*)wb, n, K, Kp, lr, b1, b2, eps,
+                                                        c1, c2);
+  return cudaGetLastError() == cudaSuccess ? 0 : 6;
+}
+
+int bpnet_unpad(const float* src, float* dst, long long rows, int K, int Kp, void* stream) {
+  k_unpad<<<grid_for(rows * K), 256, 0, (cudaStream_t)stream>>>(src, dst, rows, K, Kp);
+  return cudaGetLastError() == cudaSuccess ? 0 : 6;
+}
+
+}  // extern "C"
