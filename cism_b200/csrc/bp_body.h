@@ -414,6 +414,55 @@ BP_HD double2 matvec_row_sym(const DevView& v, const double2* A, int col, int k,
   return double2{yu, yv};
 }
 
+// SIA column preconditioner (which_ho_precond = 2): z = M^-1 r with M the
+// vertical tridiagonal of the uu and vv blocks, offsets m = 4, 13, 22
+// (setup_preconditioner_3d, glissade_velo_higher_pcg.F90:2242-2252).
+// Coefficients of node n (level k) in row h (0 u, 1 v); half storage reads
+// the entry toward k-1 from the row below's entry toward k+1 (the uu and vv
+// blocks are their own transposes).
+BP_HD void sia_coefs(const DevView& v, size_t n, int k, int h, double* sub, double* dg, double* sup) {
+  const size_t np = (size_t)v.npad;
+  if (v.sym) {
+    const double2 d = v.A[(size_t)(h * 14) * np + n];
+    *dg = h ? d.y : d.x;
+    if (k < v.nz - 1) {
+      const double2 u = v.A[(size_t)(h * 14 + 9) * np + n];
+      *sup = h ? u.y : u.x;
+    } else {
+      *sup = 0.0;
+    }
+    if (k > 0) {
+      const double2 l = v.A[(size_t)(h * 14 + 9) * np + n - 1];
+      *sub = h ? l.y : l.x;
+    } else {
+      *sub = 0.0;
+    }
+  } else {
+    const double2 d = v.A[(size_t)(h * 27 + 13) * np + n];
+    *dg = h ? d.y : d.x;
+    const double2 u = v.A[(size_t)(h * 27 + 22) * np + n];
+    *sup = k < v.nz - 1 ? (h ? u.y : u.x) : 0.0;
+    const double2 l = v.A[(size_t)(h * 27 + 4) * np + n];
+    *sub = k > 0 ? (h ? l.y : l.x) : 0.0;
+  }
+}
+
+// easy_sia_solver / tridiag_solver (pcg:2759-2904) for one column of nz
+// levels: the Thomas algorithm in the reference's order.  s holds r on
+// entry and z on exit (stride apart); sup is overwritten with the
+// elimination factors gamma.
+BP_HD void sia_column(int nz, const double* sub, const double* dg, double* sup, double* s, int stride) {
+  double beta = dg[0];
+  s[0] = s[0] / beta;
+  for (int k = 1; k < nz; ++k) {
+    const double gam = sup[k - 1] / beta;
+    sup[k - 1] = gam;
+    beta = dg[k] - sub[k] * gam;
+    s[k * stride] = (s[k * stride] - sub[k] * s[(k - 1) * stride]) / beta;
+  }
+  for (int k = nz - 2; k >= 0; --k) s[k * stride] = s[k * stride] - sup[k] * s[(k + 1) * stride];
+}
+
 // FP32 copy of row n of the symmetric matrix for the mixed-precision
 // Krylov matvecs.  Rounding each entry to FP32 perturbs the row sums, and
 // with them the operator on smooth fields (the translation modes are

@@ -107,7 +107,8 @@ struct DevView {
   const double* cell_beta; // [4][ncells] beta_internal at the corners
   const double* flwafact;  // [ncells*(nz-1)]
   // tiles
-  const int* tile_start;   // [ntiles]
+  const int* tile_start;   // [ntiles] first node (tiles hold whole columns)
+  const int* tile_end;     // [ntiles] one past the last node
   const int* tile_inst;    // [ntiles]
   // assembly / matrix
   double* qp;              // [nelem*8*10]: f, Jinv(3x3) per quadrature point

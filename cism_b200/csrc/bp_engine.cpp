@@ -172,6 +172,7 @@ DevView make_view(Arena& a, cudaStream_t s, const HostPlan& p, bool with_cells, 
     v.badj = a.get<double>(s, "badj", 4 * np);
   }
   UP(int, "tile_start", p.tile_start, tile_start);
+  UP(int, "tile_end", p.tile_end, tile_end);
   UP(int, "tile_inst", p.tile_inst, tile_inst);
 #undef UP
   v.A = a.get<double2>(s, "A", (v.sym ? 2 * 14 : 2 * 27) * np);
@@ -812,8 +813,8 @@ int bp_pcg(bp_ctx* c, int nx, int ny, int nz, int periodic,
   GUARD_BEGIN(c)
   if (!active_vertex || !Auu || !Auv || !Avu || !Avv || !bu || !bv || !xu || !xv)
     return BP_ERR_ARGS;
-  if (precond != 0 && precond != 1) {
-    c->err = "bp_pcg: precond must be 0 or 1";
+  if (precond < 0 || precond > 2) {
+    c->err = "bp_pcg: precond must be 0, 1 or 2";
     return BP_ERR_ARGS;
   }
   if (precision != BP_FP64) {

@@ -121,7 +121,7 @@ __device__ __forceinline__ TileRange tile_range(const DevView& v, int t) {
   TileRange r;
   r.inst = v.tile_inst[t];
   r.n0 = v.tile_start[t];
-  r.nend = min(r.n0 + kTile, v.inst[r.inst].node_end);
+  r.nend = v.tile_end[t];
   return r;
 }
 
@@ -298,6 +298,49 @@ __global__ void __launch_bounds__(kTile) k_rhs(DevView v) {
 }
 
 // ---------------------------------------------------------------------
+// SIA column preconditioner on a tile of whole columns: every thread puts
+// its node's r and tridiagonal coefficients into shared memory, one thread
+// per (column, component) runs the Thomas solve, every thread takes back
+// its z.  Called by all threads of the CTA (uniform per tile).
+// ---------------------------------------------------------------------
+struct SiaTile {
+  double s[2 * kTile];
+  double sub[2][kTile], dg[2][kTile], sup[2][kTile];
+};
+
+__device__ __forceinline__ double2 sia_tile(const DevView& v, const TileRange& R, double2 r) {
+  __shared__ SiaTile T;
+  const int i = threadIdx.x, len = R.nend - R.n0, nz = v.nz;
+  if (i < len) {
+    const size_t n = (size_t)R.n0 + i;
+    const int k = i % nz;  // tiles start on a column boundary
+    T.s[2 * i] = r.x;
+    T.s[2 * i + 1] = r.y;
+    sia_coefs(v, n, k, 0, &T.sub[0][i], &T.dg[0][i], &T.sup[0][i]);
+    sia_coefs(v, n, k, 1, &T.sub[1][i], &T.dg[1][i], &T.sup[1][i]);
+  }
+  __syncthreads();
+  if (i < 2 * (len / nz)) {
+    const int c = i >> 1, h = i & 1, b = c * nz;
+    sia_column(nz, &T.sub[h][b], &T.dg[h][b], &T.sup[h][b], &T.s[2 * b + h], 2);
+  }
+  __syncthreads();
+  const double2 z = i < len ? make_double2(T.s[2 * i], T.s[2 * i + 1]) : make_double2(0.0, 0.0);
+  __syncthreads();  // T is reused by the CTA's next tile
+  return z;
+}
+
+// z = M^-1 r for the instance's preconditioner (diagonal or none: D^-1
+// from k_rhs / k_dinv; SIA: column solves).  Called by all threads.
+__device__ __forceinline__ double2 precondition(const DevView& v, const TileRange& R, bool mine, size_t n,
+                                                double2 r) {
+  if (v.inst[R.inst].precond == 2) return sia_tile(v, R, r);
+  if (!mine) return make_double2(0.0, 0.0);
+  const double2 di = v.Dinv[n];
+  return make_double2(r.x * di.x, r.y * di.y);
+}
+
+// ---------------------------------------------------------------------
 // PCG kernels.  Every Krylov matvec reads one stored source vector (d for
 // the standard PCG, z = D^-1 r for Chronopoulos-Gear, x for residuals), so
 // each matvec is a plain y = A s with its dot products fused in.  Storage
@@ -349,17 +392,21 @@ __global__ void __launch_bounds__(kTile, MINB) k_resid(DevView v) {
     const InstState& S0 = v.st[R.inst];
     if (!S0.pcg_active || (MODE == MV_REFINE && !S0.need_true)) continue;
     const int n = R.n0 + threadIdx.x;
+    const bool mine = n < R.nend;
     double part[2] = {0.0, 0.0};
-    if (n < R.nend) {
+    double2 r = make_double2(0.0, 0.0);
+    if (mine) {
       const int col = n / v.nz, k = n - col * v.nz;
       const double2 y = mv_row<ST64>(v, col, k, n, v.x);
-      const double2 b = v.b[n], di = v.Dinv[n];
-      const double ru = b.x - y.x, rv = b.y - y.y;
-      const double zu = ru * di.x, zv = rv * di.y;
-      v.r[n] = make_double2(ru, rv);
-      v.z[n] = make_double2(zu, zv);
-      part[0] = ru * zu + rv * zv;
-      part[1] = ru * ru + rv * rv;
+      const double2 b = v.b[n];
+      r = make_double2(b.x - y.x, b.y - y.y);
+    }
+    const double2 z = precondition(v, R, mine, n, r);
+    if (mine) {
+      v.r[n] = r;
+      v.z[n] = z;
+      part[0] = r.x * z.x + r.y * z.y;
+      part[1] = r.x * r.x + r.y * r.y;
     }
     tile_finish<2, false>(v, t, R.inst, part, [&](int inst, const double* s) {
       InstState& S = v.st[inst];
@@ -452,22 +499,28 @@ __global__ void __launch_bounds__(kTile) k_std_update(DevView v) {
     if (!S.pcg_active) continue;
     const int n = R.n0 + threadIdx.x;
     const double alpha = S.alpha;
+    const bool mine = n < R.nend;
     double part[2] = {0.0, 0.0};
-    if (n < R.nend) {
+    double2 r = make_double2(0.0, 0.0);
+    if (mine) {
       const double2 d = v.d0[n];
       double2 x = v.x[n];
       x.x = x.x + alpha * d.x;
       x.y = x.y + alpha * d.y;
       v.x[n] = x;
       if (!CHECK) {
-        const double2 q = v.q[n], di = v.Dinv[n];
-        double2 r = v.r[n];
+        const double2 q = v.q[n];
+        r = v.r[n];
         r.x = r.x - alpha * q.x;
         r.y = r.y - alpha * q.y;
-        const double zu = r.x * di.x, zv = r.y * di.y;
         v.r[n] = r;
-        v.z[n] = make_double2(zu, zv);
-        part[0] = r.x * zu + r.y * zv;
+      }
+    }
+    if (!CHECK) {
+      const double2 z = precondition(v, R, mine, n, r);
+      if (mine) {
+        v.z[n] = z;
+        part[0] = r.x * z.x + r.y * z.y;
         part[1] = r.x * r.x + r.y * r.y;
       }
     }
@@ -576,15 +629,20 @@ __global__ void __launch_bounds__(kTile) k_cg_first_update(DevView v) {
     const InstState& S = v.st[R.inst];
     if (!S.pcg_active) continue;
     const int n = R.n0 + threadIdx.x;
-    if (n >= R.nend) continue;
+    const bool mine = n < R.nend;
     const double alpha = S.alpha;
-    const double2 d = v.d0[n], q = v.q[n], di = v.Dinv[n];
-    double2 x = v.x[n], r = v.r[n];
-    x.x = x.x + alpha * d.x; x.y = x.y + alpha * d.y;
-    r.x = r.x - alpha * q.x; r.y = r.y - alpha * q.y;
-    v.x[n] = x;
-    v.r[n] = r;
-    v.z[n] = make_double2(r.x * di.x, r.y * di.y);
+    double2 r = make_double2(0.0, 0.0);
+    if (mine) {
+      const double2 d = v.d0[n], q = v.q[n];
+      double2 x = v.x[n];
+      r = v.r[n];
+      x.x = x.x + alpha * d.x; x.y = x.y + alpha * d.y;
+      r.x = r.x - alpha * q.x; r.y = r.y - alpha * q.y;
+      v.x[n] = x;
+      v.r[n] = r;
+    }
+    const double2 z = precondition(v, R, mine, n, r);
+    if (mine) v.z[n] = z;
   }
 }
 
@@ -598,22 +656,29 @@ __global__ void __launch_bounds__(kTile) k_cg_update(DevView v) {
     const InstState& S = v.st[R.inst];
     if (!S.pcg_active) continue;
     const int n = R.n0 + threadIdx.x;
-    if (n >= R.nend) continue;
+    const bool mine = n < R.nend;
     const bool keep_r = !CHECK && !S.need_true;  // a refinement recomputes r and z
     const double alpha = S.alpha, beta = S.beta;
-    const double2 z = v.z[n], az = v.Az[n];
-    double2 d = v.d0[n], q = v.q[n], x = v.x[n];
-    d.x = z.x + beta * d.x; d.y = z.y + beta * d.y;
-    q.x = az.x + beta * q.x; q.y = az.y + beta * q.y;
-    x.x = x.x + alpha * d.x; x.y = x.y + alpha * d.y;
-    v.d0[n] = d;
-    v.q[n] = q;
-    v.x[n] = x;
+    double2 r = make_double2(0.0, 0.0);
+    if (mine) {
+      const double2 z = v.z[n], az = v.Az[n];
+      double2 d = v.d0[n], q = v.q[n], x = v.x[n];
+      d.x = z.x + beta * d.x; d.y = z.y + beta * d.y;
+      q.x = az.x + beta * q.x; q.y = az.y + beta * q.y;
+      x.x = x.x + alpha * d.x; x.y = x.y + alpha * d.y;
+      v.d0[n] = d;
+      v.q[n] = q;
+      v.x[n] = x;
+      if (keep_r) {
+        r = v.r[n];
+        r.x = r.x - alpha * q.x;
+        r.y = r.y - alpha * q.y;
+        v.r[n] = r;
+      }
+    }
     if (keep_r) {
-      const double2 r = v.r[n], di = v.Dinv[n];
-      const double ru = r.x - alpha * q.x, rv = r.y - alpha * q.y;
-      v.r[n] = make_double2(ru, rv);
-      v.z[n] = make_double2(ru * di.x, rv * di.y);
+      const double2 z = precondition(v, R, mine, n, r);
+      if (mine) v.z[n] = z;
     }
   }
 }

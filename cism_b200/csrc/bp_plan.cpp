@@ -41,10 +41,14 @@ void add_columns(int nx, int ny, int nz, int periodic, const int* active_vertex,
   (void)inst_index;
 }
 
+// Tiles hold whole columns (as many as fit in kTile nodes), so a CTA can
+// run the column solves of the SIA preconditioner on its own tile.
 void add_tiles(HostPlan* p, int b, int node_begin, int node_end) {
+  const int step = std::max(1, kTile / std::max(1, p->nz)) * std::max(1, p->nz);
   p->inst[b].tile_begin = (int)p->tile_start.size();
-  for (int s = node_begin; s < node_end; s += kTile) {
+  for (int s = node_begin; s < node_end; s += step) {
     p->tile_start.push_back(s);
+    p->tile_end.push_back(std::min(s + step, node_end));
     p->tile_inst.push_back(b);
   }
   p->inst[b].tile_end = (int)p->tile_start.size();

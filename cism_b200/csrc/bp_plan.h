@@ -32,7 +32,7 @@ struct HostPlan {
   std::vector<uint8_t> dmask;
   std::vector<int> cell_inst, cell_ij, cell_cols;
   std::vector<double> cell_s, cell_h, cell_beta, flwafact;
-  std::vector<int> tile_start, tile_inst;
+  std::vector<int> tile_start, tile_end, tile_inst;
   // per-instance grid sizes, for scatters
   std::vector<int> nx, ny, periodic;
 };

@@ -157,3 +157,43 @@ extern "C" int emu_matvec(int nx, int ny, int nz, int periodic, const int* activ
   scatter_vector(E.p, 0, y.data(), yu, yv);
   return 0;
 }
+
+// SIA column preconditioner z = M^-1 r (sym = 1: half storage as solves use;
+// 0: full rows as bp_pcg uses), the column loop of the device tile routine.
+extern "C" int emu_sia_apply(int nx, int ny, int nz, int periodic, const int* active_vertex,
+                             const double* Auu, const double* Auv, const double* Avu,
+                             const double* Avv, const double* ru, const double* rv, double* zu,
+                             double* zv, int sym) {
+  Emu E;
+  std::string err;
+  if (!build_column_plan(nx, ny, nz, periodic, active_vertex, &E.p, &err)) return 10;
+  E.bind();
+  std::vector<double2> As;
+  if (sym) {
+    As.assign(2 * 14 * (size_t)E.p.npad, double2{0, 0});
+    gather_matrix_sym(E.p, Auu, Auv, Avu, Avv, As.data());
+    E.v.sym = 1;
+    E.v.A = As.data();
+  } else {
+    gather_matrix(E.p, Auu, Auv, Avu, Avv, E.A.data());
+  }
+  gather_velocity(E.p, 0, ru, rv, E.x.data());
+  std::vector<double> s(2 * (size_t)nz), sub(nz), dg(nz), sup(nz);
+  std::vector<double2> z(E.p.npad, double2{0, 0});
+  for (int c = 0; c < E.p.ncols; ++c) {
+    for (int h = 0; h < 2; ++h) {
+      for (int k = 0; k < nz; ++k) {
+        const size_t n = (size_t)c * nz + k;
+        sia_coefs(E.v, n, k, h, &sub[k], &dg[k], &sup[k]);
+        s[k] = h ? E.x[n].y : E.x[n].x;
+      }
+      sia_column(nz, sub.data(), dg.data(), sup.data(), s.data(), 1);
+      for (int k = 0; k < nz; ++k) (h ? z[(size_t)c * nz + k].y : z[(size_t)c * nz + k].x) = s[k];
+    }
+  }
+  const size_t tot = (size_t)nz * (nx - 1) * (ny - 1);
+  std::memset(zu, 0, tot * 8);
+  std::memset(zv, 0, tot * 8);
+  scatter_vector(E.p, 0, z.data(), zu, zv);
+  return 0;
+}

@@ -93,6 +93,45 @@ def test_pcg_same_system(ctx, name, variant):
         assert gn == 2000 and gerr >= 1e-8 and oerr >= 1e-8
 
 
+@pytest.mark.parametrize("variant", [2, 3])
+@pytest.mark.parametrize("name", ["dome31x31x10", "slab24x24x11"])
+def test_pcg_sia_preconditioner_same_system(ctx, name, variant):
+    """The SIA column preconditioner (the reference's default,
+    which_ho_precond = 2) on the same assembled system: a fixed iteration
+    count to 1e-10, and the reference tolerance in about the oracle's
+    iteration count (a check apart).  Compared on the owned vertices: the
+    reference's Chronopoulos-Gear multiplies z without a halo update and its
+    SIA solve skips inactive halo vertices, so its halo values of x are not
+    periodic copies (the device's are)."""
+    m = MODELS[name]
+    su, A, bu, bv = _converged_system(m)
+    rows = owned_active_rows(m, su["active_vertex"])
+    z = np.zeros(m.vshape3)
+    gu, gv, _, gn, _ = ctx.pcg_solve(m, su["active_vertex"], A, bu, bv, z, z, precond=2,
+                                     variant=variant, tol=0.0, maxiters=30, ncheck=5)
+    ou, ov, _, on, _ = oracle.pcg(m, su["active_vertex"], A, bu, bv, z, z, precond=2,
+                                 variant=variant, maxiters=30, tol=0.0, ncheck=5)
+    assert gn == on
+    assert rel_l2([gu[rows], gv[rows]], [ou[rows], ov[rows]]) < 1e-10
+    gu, gv, gerr, gn, _ = ctx.pcg_solve(m, su["active_vertex"], A, bu, bv, z, z, precond=2,
+                                        variant=variant, tol=1e-8, maxiters=2000, ncheck=5)
+    ou, ov, oerr, on, _ = oracle.pcg(m, su["active_vertex"], A, bu, bv, z, z, precond=2,
+                                    variant=variant, maxiters=2000, tol=1e-8, ncheck=5)
+    assert abs(gn - on) <= 5 and gerr < 1e-8 and oerr < 1e-8
+    assert rel_l2([gu[rows], gv[rows]], [ou[rows], ov[rows]]) < 1e-6
+
+
+@pytest.mark.parametrize("precision", [solver.FP64, solver.MIXED])
+@pytest.mark.parametrize("name", ["dome31x31x10", "slab24x24x11"])
+def test_picard_sia_preconditioner_matches_oracle(ctx, name, precision):
+    m = MODELS[name].copy(pcg_maxiters=2000, which_precond=configs.PRECOND_SIA)
+    u, v, _, st = ctx.velo_higher_solve(m, precision=precision)
+    uo, vo, _, _, sto = oracle.velo_higher_solve(m)
+    assert st["status"] == 0, st
+    assert st["picard_iters"] == sto["picard_iters"]
+    assert rel_l2([u, v], [uo, vo]) < (1e-8 if precision == solver.FP64 else 1e-6)
+
+
 @pytest.mark.parametrize("name", list(MODELS))
 def test_picard_matches_oracle(ctx, name):
     m = MODELS[name].copy(pcg_maxiters=2000)

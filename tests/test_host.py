@@ -144,3 +144,38 @@ def test_fp32_copy_keeps_row_sums(m):
             out.append((eyu, eyv))
         diff = max(np.abs(out[0][0] - out[1][0]).max(), np.abs(out[0][1] - out[1][1]).max())
         assert diff <= 1e-13 * scale
+
+
+@pytest.mark.parametrize("m", MODELS[:4], ids=lambda m: m.name)
+def test_sia_preconditioner_bodies(m):
+    """The device's SIA column preconditioner (coefficients from half or full
+    storage, Thomas solve) against a banded solve of each owned column's
+    vertical uu and vv tridiagonals (offsets 4, 13, 22) of the oracle's
+    matrix."""
+    from scipy.linalg import solve_banded
+
+    emu = C.CDLL(EMU)
+    su, u, v, A, bu, bv, efvs = oracle_system(m, seed=6, scale=10.0)
+    ru, rv = random_state(m, su, seed=7, scale=1.0)
+    av = np.ascontiguousarray(su["active_vertex"], np.int32)
+    js, is_ = m.owned_vertex_slices()
+    ref = []
+    for Ab, r in ((A[0], ru), (A[3], rv)):
+        z = np.zeros(m.vshape3)
+        for j in range(js.start, js.stop):
+            for i in range(is_.start, is_.stop):
+                if not av[j, i]:
+                    continue
+                ab = np.zeros((3, m.nz))
+                ab[0, 1:] = Ab[j, i, :-1, 22]
+                ab[1, :] = Ab[j, i, :, 13]
+                ab[2, :-1] = Ab[j, i, 1:, 4]
+                z[j, i] = solve_banded((1, 1), ab, r[j, i])
+        ref.append(z)
+    rows = owned_active_rows(m, su["active_vertex"])
+    for sym in (1, 0):
+        zu, zv = np.zeros(m.vshape3), np.zeros(m.vshape3)
+        rc = emu.emu_sia_apply(m.nx, m.ny, m.nz, m.periodic, _p(av), *[_p(np.ascontiguousarray(a)) for a in A],
+                               _p(ru), _p(rv), _p(zu), _p(zv), sym)
+        assert rc == 0
+        assert rel_l2([zu[rows], zv[rows]], [ref[0][rows], ref[1][rows]]) < 1e-12, sym

@@ -175,3 +175,30 @@ def test_bindings_match_the_c_declarations():
     assert decl
     for name, n in decl.items():
         assert len(getattr(L, name).argtypes) == n, name
+
+
+@pytest.mark.gpu
+def test_shipped_network_reduces_iterations_on_held_out_slab(ctx):
+    """The trained weights shipped in cism_b200/weights: on a slab drawn from
+    the family with a seed outside the training seeds, the learned start
+    needs fewer Picard and PCG iterations than the zero start, and both meet
+    the same convergence criteria (Picard max speed change 1e-4, PCG 1e-8),
+    so the answers agree to the Picard tolerance's scale."""
+    import os
+
+    from cism_b200 import configs, guess, net as netmod, solver
+
+    path = os.path.join(os.path.dirname(netmod.__file__), "weights", "unet_slab.npz")
+    model = netmod.UNet.load(path)
+    m = configs.random_slab(np.random.default_rng(424242), n=96).copy(pcg_maxiters=3000)
+    u0, v0, _, st0 = ctx.velo_higher_solve(m)
+    gu, gv = guess.learned_guesses(model, [m])[0]
+    prep, _, _ = solver.prepare(m)
+    u1, v1, _, st1 = ctx.solve_prepared(prep, gu, gv)
+    assert st0["status"] == 0 and st1["status"] == 0
+    js, is_ = m.owned_vertex_slices()
+    guess_err = rel_l2([gu[js, is_], gv[js, is_]], [u0[js, is_], v0[js, is_]])
+    assert guess_err < 0.2
+    assert st1["picard_iters"] < st0["picard_iters"]
+    assert st1["pcg_iters_total"] < 0.8 * st0["pcg_iters_total"]
+    assert rel_l2([u1, v1], [u0, v0]) < 1e-3
