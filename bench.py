@@ -61,6 +61,8 @@ def parse_args():
     ap.add_argument("--refine-eta", type=float, default=1e-4,
                     help="mixed path: residual reduction of one FP32 refinement cycle")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-eval", type=int, default=0,
+                    help="measure B: N held-out slabs, plain one at a time vs learned+mixed batched")
     ap.add_argument("--profile-run", action="store_true",
                     help="one untimed solve (for ncu launch lists / captures)")
     ap.add_argument("--picard-cap", type=int, default=0,
@@ -252,13 +254,16 @@ def path_spec(path, m):
     """(start, precision, model) of a bench path: 'fp64' | 'mixed' with an
     optional start prefix ('sia_', 'learned_') and suffix '_colpc' for the
     SIA column preconditioner (the reference's default which_ho_precond = 2)
-    in place of the workload's configured diagonal one."""
+    in place of the workload's configured diagonal one; '_cg' for the
+    Chronopoulos-Gear PCG variant."""
     from cism_b200 import configs, solver
 
     parts = path.split("_")
     start = parts[0] if parts[0] in ("sia", "learned") else "zero"
     prec = solver.MIXED if "mixed" in parts else solver.FP64
     mp = m.copy(which_precond=configs.PRECOND_SIA) if "colpc" in parts else m
+    if "cg" in parts:  # the single-reduction Chronopoulos-Gear recurrence
+        mp = mp.copy(which_sparse=configs.SPARSE_PCG_CHRONGEAR)
     return start, prec, mp
 
 
@@ -283,7 +288,8 @@ def run_ours(args, D):
     if args.precision == "best":
         paths = ["fp64", "mixed", "sia_fp64", "fp64_colpc"]
         if net_model is not None:
-            paths += ["learned_fp64", "learned_mixed", "learned_mixed_colpc"]
+            paths += ["learned_fp64", "learned_mixed", "learned_fp64_colpc", "learned_mixed_colpc",
+                      "learned_mixed_colpc_cg"]
     else:
         paths = [args.precision]
     res = {}
@@ -327,6 +333,13 @@ def run_ours(args, D):
         ms_max = D.max(ms if start == "zero" else max(ms, wall))
         us, vs, _ = prob.get()
         sol[path] = (us[0], vs[0])
+        guess_err = None
+        if start != "zero":  # the guess against this path's converged answer, owned vertices
+            gu, gv = make_guess()
+            js, is_ = mp.owned_vertex_slices()
+            du, dv = (gu - us[0])[js, is_], (gv - vs[0])[js, is_]
+            guess_err = math.sqrt(float(np.sum(du ** 2 + dv ** 2)) /
+                                  float(np.sum(us[0][js, is_] ** 2 + vs[0][js, is_] ** 2)))
         st = sts[-1]
         # kernel timing pass (CUDA events around every launch, graphs off)
         prob.timing(True)
@@ -338,7 +351,7 @@ def run_ours(args, D):
         info.update({"mv_nodes_fp64": n64, "mv_nodes_fp32": n32, "tuned_minb": minb, "tuned_grid": grid})
         launches = sum(n for _, n in kt.values()) + net_launches
         res[path] = {"value": D.world * args.steps / (ms_max / 1000.0), "ms_per_step": ms_max / args.steps,
-                     "make_guess": make_guess,
+                     "make_guess": make_guess, "guess_rel_err": guess_err,
                      "status": st["status"], "picard_iters": st["picard_iters"],
                      "pcg_iters_total": st["pcg_iters_total"], "refine_steps": st["refine_steps_total"],
                      "final_rel_resid": st["pcg_err_last"], "kernel_times": kt, "info": info,
@@ -393,9 +406,9 @@ def run_ours(args, D):
     achieved = total_bytes / (kms / 1000.0) / 1e9 if kn else 0.0
     traffic = matvec_traffic(N, head)
     roof = {"bound": "hbm",
-            "kernel": ("k_std_mv<ST_SYM32> (Krylov q = A d, FP32 symmetric matrix, row-sum compensated FP64 "
-                       "diagonal)" if "mixed" in head.split("_") else
-                       "k_std_mv<ST_SYM> (Krylov q = A d, FP64 symmetric matrix)"),
+            "kernel": (("k_cg_mv" if "cg" in head.split("_") else "k_std_mv") +
+                       ("<ST_SYM32> (Krylov matvec, FP32 symmetric matrix, row-sum compensated FP64 diagonal)"
+                        if "mixed" in head.split("_") else "<ST_SYM> (Krylov matvec, FP64 symmetric matrix)")),
             "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)",
             "traffic": traffic, "algorithmic_bytes_per_launch": round(bytes_launch),
@@ -424,7 +437,10 @@ def run_ours(args, D):
                   | {"final_rel_resid": float("%.3e" % r["final_rel_resid"]),
                      "start": path_spec(p, m)[0],
                      "preconditioner": "sia_column" if "colpc" in p else "diagonal",
-                     "rel_l2_vs_fp64": float("%.3e" % r.get("rel_l2_vs_fp64", 0.0))}
+                     "pcg": "chronopoulos_gear" if "cg" in p.split("_") else "standard",
+                     "rel_l2_vs_fp64": float("%.3e" % r.get("rel_l2_vs_fp64", 0.0)),
+                     "guess_rel_err": (float("%.3e" % r["guess_rel_err"]) if r.get("guess_rel_err") is not None
+                                       else None)}
                   for p, r in res.items()},
     }
     if "fp64" in res and head != "fp64":
@@ -508,6 +524,72 @@ def profile_run(args):
     ctx.close()
 
 
+def batch_eval(args):
+    """B: N held-out members of the c1 family (160 x 160 periodic slabs,
+    seeded outside the training seeds) solved (a) one at a time by the
+    plain FP64 path (zero start, diagonal preconditioner, standard PCG) and
+    (b) all in one resident problem by the learned + mixed path (column
+    preconditioner, Chronopoulos-Gear), the network's inference for the
+    whole batch included.  Each pass timed once after a warm-up pass (max of
+    device and wall time); prints one JSON line."""
+    import numpy as np
+
+    from cism_b200 import configs, guess, solver
+
+    n = args.batch_eval
+    rng = np.random.default_rng(90210)
+    models = [configs.random_slab(rng, n=160).copy(pcg_maxiters=args.pcg_maxiters) for _ in range(n)]
+    ctx = solver.Context(0)
+    net_model = load_guess_net(models[0])
+    plain = []
+    for m in models:
+        prep, u0, v0 = solver.prepare(m)
+        prob = ctx.problem([prep])
+        prob.set_guess([u0], [v0])
+        prob.run()  # warm-up (autotune, graphs)
+        plain.append(prob)
+    t0 = time.perf_counter()
+    ctx.timer_start()
+    sts_a = [p.run()[0] for p in plain]
+    ms_a = max(ctx.timer_stop(), (time.perf_counter() - t0) * 1000.0)
+    sols_a = [p.get()[:2] for p in plain]
+    for p in plain:
+        p.close()
+    mb = [m.copy(which_precond=configs.PRECOND_SIA, which_sparse=configs.SPARSE_PCG_CHRONGEAR) for m in models]
+    preps = [solver.prepare(m, precision=solver.MIXED, inner_tol=args.refine_eta)[0] for m in mb]
+    prob = ctx.problem(preps)
+    gs = guess.learned_guesses(net_model, mb)
+    prob.set_guess([g[0] for g in gs], [g[1] for g in gs])
+    prob.run()  # warm-up
+    t0 = time.perf_counter()
+    ctx.timer_start()
+    gs = guess.learned_guesses(net_model, mb)
+    prob.set_guess([g[0] for g in gs], [g[1] for g in gs])
+    sts_b = prob.run()
+    ms_b = max(ctx.timer_stop(), (time.perf_counter() - t0) * 1000.0)
+    us, vs, _ = prob.get()
+    prob.close()
+    err = []
+    for (ua, va), u, v in zip(sols_a, us, vs):
+        a = np.concatenate([ua[0].ravel(), va[0].ravel()])
+        b = np.concatenate([u.ravel(), v.ravel()])
+        err.append(float(np.linalg.norm(a - b) / np.linalg.norm(a)))
+
+    def summary(sts, ms):
+        return {"solves_per_s": n / (ms / 1000.0), "ms": ms,
+                "pcg_iters_mean": float(np.mean([s["pcg_iters_total"] for s in sts])),
+                "picard_mean": float(np.mean([s["picard_iters"] for s in sts]))}
+
+    out = {"batch_eval": n, "domains": "160x160x11 periodic slabs (c1 family, held-out seeds)",
+           "plain_fp64_sequential": summary(sts_a, ms_a),
+           "learned_mixed_colpc_cg_batched": summary(sts_b, ms_b),
+           "status": sorted({int(s["status"]) for s in sts_a + sts_b}),
+           "max_rel_l2_vs_plain": max(err)}
+    out["speedup"] = out["learned_mixed_colpc_cg_batched"]["solves_per_s"] / out["plain_fp64_sequential"]["solves_per_s"]
+    print(json.dumps(out), flush=True)
+    ctx.close()
+
+
 def kernel_sweep(args):
     """Matvec variants on the workload's assembled matrix (one Picard iteration)."""
     from cism_b200 import solver
@@ -546,6 +628,9 @@ def main():
     args = parse_args()
     if args.profile_run:
         profile_run(args)
+        return
+    if args.batch_eval > 0:
+        batch_eval(args)
         return
     if args.kernel_sweep:
         kernel_sweep(args)
