@@ -13,6 +13,8 @@
 #include "bp_b200.h"
 #include "bp_kernels.h"
 
+#include <cstdlib>
+
 namespace bp {
 
 __constant__ RefTables c_T;
@@ -116,6 +118,14 @@ __device__ __forceinline__ bool is_nan(double x) { return x != x; }
 struct TileRange {
   int inst, n0, nend;
 };
+
+// Programmatic dependent launch: the PCG kernels are launched so that the
+// next one may be scheduled while its predecessor drains; each calls
+// pdl_wait() (which returns once the predecessor grid has completed and its
+// writes are visible) before it reads anything, in every CTA, so a grid
+// also completes only after its predecessor.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_launch_next() { asm volatile("griddepcontrol.launch_dependents;"); }
 
 __device__ __forceinline__ TileRange tile_range(const DevView& v, int t) {
   TileRange r;
@@ -386,6 +396,8 @@ __device__ __forceinline__ void refine_request(const InstParams& ip, InstState& 
 // requested it.
 template <int MODE, int STORE, int MINB>
 __global__ void __launch_bounds__(kTile, MINB) k_resid(DevView v) {
+  pdl_wait();
+  pdl_launch_next();
   constexpr int ST64 = STORE == ST_SYM32 ? ST_SYM : STORE;
   for (int t = blockIdx.x; t < v.ntiles; t += gridDim.x) {
     const TileRange R = tile_range(v, t);
@@ -466,6 +478,8 @@ __device__ __forceinline__ void count_tile(const DevView& v, const InstState& S,
 // Standard PCG: q = A d; (d, q); alpha = eta1 / (d, q)   (pcg:426-463).
 template <int STORE, int MINB>
 __global__ void __launch_bounds__(kTile, MINB) k_std_mv(DevView v) {
+  pdl_wait();
+  pdl_launch_next();
   for (int t = blockIdx.x; t < v.ntiles; t += gridDim.x) {
     const TileRange R = tile_range(v, t);
     const InstState& S0 = v.st[R.inst];
@@ -493,6 +507,8 @@ __global__ void __launch_bounds__(kTile, MINB) k_std_mv(DevView v) {
 // On check iterations only x is updated (r is recomputed from b - A x).
 template <bool CHECK>
 __global__ void __launch_bounds__(kTile) k_std_update(DevView v) {
+  pdl_wait();
+  pdl_launch_next();
   for (int t = blockIdx.x; t < v.ntiles; t += gridDim.x) {
     const TileRange R = tile_range(v, t);
     const InstState& S = v.st[R.inst];
@@ -541,6 +557,8 @@ __global__ void __launch_bounds__(kTile) k_std_update(DevView v) {
 
 // d = z + beta d; d = z at the first iteration (pcg:403-407).
 __global__ void __launch_bounds__(kTile) k_std_dir(DevView v) {
+  pdl_wait();
+  pdl_launch_next();
   for (int t = blockIdx.x; t < v.ntiles; t += gridDim.x) {
     const TileRange R = tile_range(v, t);
     const InstState& S = v.st[R.inst];
@@ -563,6 +581,8 @@ __global__ void __launch_bounds__(kTile) k_std_dir(DevView v) {
 // which also sets d = z, q = A d.
 template <bool FIRST, int STORE, int MINB>
 __global__ void __launch_bounds__(kTile, MINB) k_cg_mv(DevView v) {
+  pdl_wait();
+  pdl_launch_next();
   for (int t = blockIdx.x; t < v.ntiles; t += gridDim.x) {
     const TileRange R = tile_range(v, t);
     const InstState& S0 = v.st[R.inst];
@@ -624,6 +644,8 @@ __global__ void __launch_bounds__(kTile, MINB) k_cg_mv(DevView v) {
 
 // Chronopoulos-Gear first-pass update: x += alpha d; r -= alpha q; z = D^-1 r.
 __global__ void __launch_bounds__(kTile) k_cg_first_update(DevView v) {
+  pdl_wait();
+  pdl_launch_next();
   for (int t = blockIdx.x; t < v.ntiles; t += gridDim.x) {
     const TileRange R = tile_range(v, t);
     const InstState& S = v.st[R.inst];
@@ -651,6 +673,8 @@ __global__ void __launch_bounds__(kTile) k_cg_first_update(DevView v) {
 // iteration (skipped on check iterations, where r and z come from b - A x).
 template <bool CHECK>
 __global__ void __launch_bounds__(kTile) k_cg_update(DevView v) {
+  pdl_wait();
+  pdl_launch_next();
   for (int t = blockIdx.x; t < v.ntiles; t += gridDim.x) {
     const TileRange R = tile_range(v, t);
     const InstState& S = v.st[R.inst];
@@ -843,15 +867,36 @@ void launch_assemble(const DevView& v, cudaStream_t s) {
   launch_asm_rows(v, s);
   launch_rhs(v, s);
 }
+// PCG kernels are launched as programmatic dependents of their stream
+// predecessor (BP_PDL=0 turns this off).
+static const bool g_pdl = [] {
+  const char* e = std::getenv("BP_PDL");
+  return !(e && e[0] == '0');
+}();
+
+static void launch_pcg(void (*kernel)(DevView), int g, cudaStream_t s, const DevView& v) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(g);
+  cfg.blockDim = dim3(kTile);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = g_pdl ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, kernel, v);
+}
+
 template <int STORE, int MINB>
 static void launch_mv_store(int mode, const DevView& v, cudaStream_t s, int g) {
   switch (mode) {
-    case MV_INIT: k_resid<MV_INIT, STORE, MINB><<<g, kTile, 0, s>>>(v); break;
-    case MV_CHECK: k_resid<MV_CHECK, STORE, MINB><<<g, kTile, 0, s>>>(v); break;
-    case MV_REFINE: k_resid<MV_REFINE, STORE, MINB><<<g, kTile, 0, s>>>(v); break;
-    case MV_STD_A: k_std_mv<STORE, MINB><<<g, kTile, 0, s>>>(v); break;
-    case MV_CG_FIRST: k_cg_mv<true, STORE, MINB><<<g, kTile, 0, s>>>(v); break;
-    default: k_cg_mv<false, STORE, MINB><<<g, kTile, 0, s>>>(v); break;
+    case MV_INIT: launch_pcg(k_resid<MV_INIT, STORE, MINB>, g, s, v); break;
+    case MV_CHECK: launch_pcg(k_resid<MV_CHECK, STORE, MINB>, g, s, v); break;
+    case MV_REFINE: launch_pcg(k_resid<MV_REFINE, STORE, MINB>, g, s, v); break;
+    case MV_STD_A: launch_pcg(k_std_mv<STORE, MINB>, g, s, v); break;
+    case MV_CG_FIRST: launch_pcg(k_cg_mv<true, STORE, MINB>, g, s, v); break;
+    default: launch_pcg(k_cg_mv<false, STORE, MINB>, g, s, v); break;
   }
 }
 template <int STORE>
@@ -866,16 +911,14 @@ void launch_mv(int mode, const DevView& v, cudaStream_t s) {
   else launch_mv_minb<ST_SYM>(mode, v, s, g);
 }
 void launch_std_update(bool check, const DevView& v, cudaStream_t s) {
-  if (check) k_std_update<true><<<tile_grid(v), kTile, 0, s>>>(v);
-  else k_std_update<false><<<tile_grid(v), kTile, 0, s>>>(v);
+  launch_pcg(check ? k_std_update<true> : k_std_update<false>, tile_grid(v), s, v);
 }
-void launch_std_dir(const DevView& v, cudaStream_t s) { k_std_dir<<<tile_grid(v), kTile, 0, s>>>(v); }
+void launch_std_dir(const DevView& v, cudaStream_t s) { launch_pcg(k_std_dir, tile_grid(v), s, v); }
 void launch_cg_first_update(const DevView& v, cudaStream_t s) {
-  k_cg_first_update<<<tile_grid(v), kTile, 0, s>>>(v);
+  launch_pcg(k_cg_first_update, tile_grid(v), s, v);
 }
 void launch_cg_update(bool check, const DevView& v, cudaStream_t s) {
-  if (check) k_cg_update<true><<<tile_grid(v), kTile, 0, s>>>(v);
-  else k_cg_update<false><<<tile_grid(v), kTile, 0, s>>>(v);
+  launch_pcg(check ? k_cg_update<true> : k_cg_update<false>, tile_grid(v), s, v);
 }
 void launch_picard_check(const DevView& v, cudaStream_t s) {
   k_picard_check<<<tile_grid(v), kTile, 0, s>>>(v);

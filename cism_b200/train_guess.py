@@ -50,7 +50,9 @@ def solve_models(ctx, models: List[configs.BPModel], precision=solver.FP64, gues
 def make_set(ctx, count: int, n: int, seed: int, batch: int):
     rng = np.random.default_rng(seed)
     models = [configs.random_slab(rng, n=n) for _ in range(count)]
-    models = [m.copy(pcg_maxiters=3000) for m in models]
+    # targets from the column-preconditioned solver (the same answers to the
+    # solver's tolerances, in a third of the iterations)
+    models = [m.copy(pcg_maxiters=3000, which_precond=configs.PRECOND_SIA) for m in models]
     us, vs, sts, _ = solve_models(ctx, models, batch=batch)
     ok = [i for i, s in enumerate(sts) if s["status"] == 0]
     feats = np.stack([net.features(models[i]) for i in ok])
@@ -97,8 +99,7 @@ def train(model: net.UNet, groups, epochs: int, lr: float, batch: int, seed: int
 def evaluate(ctx, model: net.UNet, models, refs) -> Dict:
     """Held-out domains: guess error and iterations/time from each start."""
     out = {}
-    starts = {"zero": [guess.zero_guess(m) for m in models], "sia": [guess.sia_guess(m) for m in models],
-              "learned": guess.learned_guesses(model, models)}
+    starts = {"zero": [guess.zero_guess(m) for m in models], "learned": guess.learned_guesses(model, models)}
     for name, gs in starts.items():
         errs = []
         for (gu, gv), (u, v), m in zip(gs, refs, models):
@@ -106,8 +107,11 @@ def evaluate(ctx, model: net.UNet, models, refs) -> Dict:
             num = np.linalg.norm(np.concatenate([(gu - u)[js, is_].ravel(), (gv - v)[js, is_].ravel()]))
             den = np.linalg.norm(np.concatenate([u[js, is_].ravel(), v[js, is_].ravel()]))
             errs.append(num / den)
-        for prec_name, prec in (("fp64", solver.FP64), ("mixed", solver.MIXED)):
-            us, vs, sts, ms = solve_models(ctx, models, precision=prec, guesses=gs, batch=len(models))
+        for prec_name, prec, extra in (("fp64_colpc", solver.FP64, {}),
+                                       ("mixed_colpc_cg", solver.MIXED,
+                                        {"which_sparse": configs.SPARSE_PCG_CHRONGEAR})):
+            ms_ = [m.copy(**extra) for m in models]
+            us, vs, sts, ms = solve_models(ctx, ms_, precision=prec, guesses=gs, batch=len(models))
             sol_err = [float(np.linalg.norm(np.concatenate([(a - u).ravel(), (b - v).ravel()])) /
                              np.linalg.norm(np.concatenate([u.ravel(), v.ravel()])))
                        for a, b, (u, v) in zip(us, vs, refs)]
@@ -125,10 +129,10 @@ def evaluate(ctx, model: net.UNet, models, refs) -> Dict:
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=os.path.join(os.path.dirname(__file__), "weights", "unet_slab.npz"))
-    ap.add_argument("--train96", type=int, default=256)
-    ap.add_argument("--train160", type=int, default=32)
+    ap.add_argument("--train96", type=int, default=640)
+    ap.add_argument("--train160", type=int, default=128)
     ap.add_argument("--heldout", type=int, default=8)
-    ap.add_argument("--epochs", type=int, default=120)
+    ap.add_argument("--epochs", type=int, default=200)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--batch", type=int, default=8)
     ap.add_argument("--seed", type=int, default=11)
