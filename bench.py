@@ -85,34 +85,44 @@ def make_model(name, pcg_maxiters):
 # distributed plumbing (replicas only)
 # ---------------------------------------------------------------------------
 class Dist:
-    def __init__(self, gpus):
+    """One process per GPU (replicas): NCCL with a GPU, gloo without (the
+    CPU tests); only a barrier and the max over ranks of the timed region."""
+
+    def __init__(self, gpus, backend=None):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
         self.pg = None
+        self.cuda = False
         if self.world > 1:
             import datetime
 
             import torch
             import torch.distributed as dist
 
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+            self.cuda = backend != "gloo" and torch.cuda.is_available()
+            if self.cuda:
+                torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl" if self.cuda else "gloo", timeout=datetime.timedelta(seconds=120))
             self.pg = dist
 
     def barrier(self):
         if self.pg:
-            import torch
+            if self.cuda:
+                import torch
 
-            self.pg.barrier(device_ids=[self.local])
-            torch.cuda.synchronize()
+                self.pg.barrier(device_ids=[self.local])
+                torch.cuda.synchronize()
+            else:
+                self.pg.barrier()
 
     def max(self, x):
         if not self.pg:
             return x
         import torch
 
-        t = torch.tensor([float(x)], device=f"cuda:{self.local}", dtype=torch.float64)
+        dev = f"cuda:{self.local}" if self.cuda else "cpu"
+        t = torch.tensor([float(x)], device=dev, dtype=torch.float64)
         self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
         return float(t.item())
 
