@@ -61,6 +61,7 @@ def parse_args():
     ap.add_argument("--refine-eta", type=float, default=1e-4,
                     help="mixed path: residual reduction of one FP32 refinement cycle")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-family", default="slab", choices=["slab", "c3"])
     ap.add_argument("--batch-eval", type=int, default=0,
                     help="measure B: N held-out slabs, plain one at a time vs learned+mixed batched")
     ap.add_argument("--profile-run", action="store_true",
@@ -600,6 +601,66 @@ def batch_eval(args):
     ctx.close()
 
 
+def batch_eval_c3(args):
+    """B on the ensemble configuration: N domes and slabs of 32-192 cells
+    per side (dx 2 km, 11 levels, log-normal beta perturbations), zero
+    start, solved (a) one at a time by the plain FP64 path, (b) all in one
+    resident problem by the same FP64 solver, (c) all in one problem by the
+    mixed solver with the column preconditioner and Chronopoulos-Gear.
+    Prints one JSON line."""
+    import numpy as np
+
+    from cism_b200 import configs, solver
+
+    n = args.batch_eval
+    models = [m.copy(pcg_maxiters=args.pcg_maxiters) for m in configs.ensemble(count=n)]
+    ctx = solver.Context(0)
+    sols_a, sts_a = [], []
+    t0 = time.perf_counter()
+    for m in models:
+        prep, u0, v0 = solver.prepare(m)
+        prob = ctx.problem([prep])
+        prob.set_guess([u0], [v0])
+        sts_a.append(prob.run()[0])
+        sols_a.append(prob.get()[:2])
+        prob.close()
+    ms_a = (time.perf_counter() - t0) * 1000.0
+
+    def batched(ms_, prec):
+        preps = [solver.prepare(m, precision=prec, inner_tol=args.refine_eta) for m in ms_]
+        prob = ctx.problem([p_[0] for p_ in preps])
+        prob.set_guess([p_[1] for p_ in preps], [p_[2] for p_ in preps])
+        t1 = time.perf_counter()
+        ctx.timer_start()
+        sts = prob.run()
+        ms = max(ctx.timer_stop(), (time.perf_counter() - t1) * 1000.0)
+        us, vs, _ = prob.get()
+        prob.close()
+        err = max(float(np.linalg.norm(np.concatenate([(u - ua[0]).ravel(), (v - va[0]).ravel()])) /
+                        max(np.linalg.norm(np.concatenate([ua[0].ravel(), va[0].ravel()])), 1e-300))
+                  for (ua, va), u, v in zip(sols_a, us, vs))
+        return sts, ms, err
+
+    sts_b, ms_b, err_b = batched(models, solver.FP64)
+    mc = [m.copy(which_precond=configs.PRECOND_SIA, which_sparse=configs.SPARSE_PCG_CHRONGEAR) for m in models]
+    sts_c, ms_c, err_c = batched(mc, solver.MIXED)
+
+    def summary(sts, ms):
+        return {"solves_per_s": n / (ms / 1000.0), "ms": ms,
+                "pcg_iters_mean": float(np.mean([s["pcg_iters_total"] for s in sts])),
+                "picard_mean": float(np.mean([s["picard_iters"] for s in sts])),
+                "status": sorted({int(s["status"]) for s in sts})}
+
+    out = {"batch_eval_c3": n, "domains": "ensemble: domes and slabs, 32-192 cells per side, dx 2 km, 11 levels",
+           "plain_fp64_sequential": summary(sts_a, ms_a),
+           "plain_fp64_batched": summary(sts_b, ms_b) | {"max_rel_l2_vs_sequential": err_b},
+           "mixed_colpc_cg_batched": summary(sts_c, ms_c) | {"max_rel_l2_vs_sequential": err_c}}
+    out["speedup_batched_fp64"] = ms_a / ms_b
+    out["speedup_batched_mixed_colpc_cg"] = ms_a / ms_c
+    print(json.dumps(out), flush=True)
+    ctx.close()
+
+
 def kernel_sweep(args):
     """Matvec variants on the workload's assembled matrix (one Picard iteration)."""
     from cism_b200 import solver
@@ -640,7 +701,7 @@ def main():
         profile_run(args)
         return
     if args.batch_eval > 0:
-        batch_eval(args)
+        (batch_eval_c3 if args.batch_family == "c3" else batch_eval)(args)
         return
     if args.kernel_sweep:
         kernel_sweep(args)
