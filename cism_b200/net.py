@@ -5,7 +5,7 @@ surface-slope components, log basal friction and the ice mask -- to the
 (u, v) velocity on every sigma level (2 x nz channels, padded to a multiple
 of 8).  Its guess replaces the zero or shallow-ice start of the Picard loop;
 the unchanged solver then drives the solve to the same tolerance, so the
-plain method remains both the fallback and the judge of the network.
+plain method remains both the fallback and the measure of the network's error.
 
 Architecture (four resolution levels, 32/64/96/128 channels, 3 x 3 convs,
 GELU, 2 x 2 average pooling, nearest upsampling, skip concatenation, a 1 x 1
