@@ -83,8 +83,11 @@ struct DevView {
   int nz, ncols, nnodes, npad, ncells, nelem, ninst, ntiles;
   int any_dirichlet;       // any prescribed node in the problem
   int sym;                 // matrix stored as its 14 upper stencil offsets (exactly symmetric)
-  int minb;                // Krylov matvec variant: resident CTAs per SM it is built for (0 or 4)
+  int minb;                // residual kernels: resident CTAs per SM they are built for (0 or 4)
   int grid_cap;            // CTAs of the tile kernels (0 = one per tile)
+  int minb_k;              // Krylov matvecs (k_std_mv, k_cg_mv): the same, 0, 4 or 6
+  int grid_k;              // CTAs of the Krylov matvecs (0 = one per tile)
+  int dry;                 // autotuner pass: Krylov matvecs run every tile, leave the state alone
   unsigned long long* mv_nodes;  // [2] nodes through FP64 / FP32 Krylov matvecs (timing runs), or null
   const InstParams* inst;
   InstState* st;

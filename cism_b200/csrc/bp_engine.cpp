@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -91,8 +92,9 @@ struct bp_ctx {
   cudaEvent_t t0 = nullptr, t1 = nullptr, t2 = nullptr, t3 = nullptr;
   cudaEvent_t r0 = nullptr, r1 = nullptr;  // bp_timer_start / stop
   int num_sms = 0;
-  // autotuner results: (node bucket, nz, storage, precision) -> (minb, grid)
-  std::map<std::tuple<int, int, int, int>, std::pair<int, int>> tuned;
+  // autotuner results: (node bucket, nz, storage, precision, PCG variant)
+  // -> (minb, grid) of the residual kernels, (minb_k, grid_k) of the Krylov matvecs
+  std::map<std::tuple<int, int, int, int, int>, std::array<int, 4>> tuned;
 };
 
 struct bp_problem {
@@ -359,54 +361,96 @@ void linear_solve(bp_problem* P) {
   run_pcg_fp64(P);
 }
 
-// Autotuner: after the first assembly of a problem, time the residual
-// matvec r = b - A x (the Krylov matvec's structure: same row gather, fused
-// dot products and scalar tail; idempotent before the linear solve, which
-// recomputes it) in each (occupancy target, grid) variant on the problem's
-// own matrix and keep the fastest for every tile kernel; results are cached
-// per context by (size bucket, nz, storage, precision).
+// Autotuner: after the first assembly of a problem, time candidate launch
+// shapes on the problem's own matrix and keep the fastest; results are
+// cached per context by (size bucket, nz, storage, precision, PCG variant).
+// Candidates time one warm-up and five timed launches.
+//  * Residual kernels and the grid of the other tile kernels: the residual
+//    matvec r = b - A x (k_resid<MV_INIT>, idempotent before the linear
+//    solve, which recomputes it) for occupancy target 0 or 4 CTAs per SM
+//    and grid one CTA per tile or 4 x SMs.
+//  * Krylov matvecs, the solve's dominant kernel: the instance's own
+//    kernel (k_cg_mv or k_std_mv on the FP32 or FP64 matrix) in a dry pass
+//    (every tile, instance state untouched) for occupancy target 0, 4 or 6
+//    and grid one CTA per tile or one wave of resident CTAs.  Its register
+//    allocation, and so its occupancy, differs from the residual kernel's.
+// BP_MV_CONFIG="minb,grid[,minb_k,grid_k]" fixes the choice (for sweeps);
+// BP_TUNE_LOG=1 prints every candidate's time to stderr.
+static float time_launches(bp_ctx* c, const std::function<void()>& launch) {
+  launch();
+  CK(cudaEventRecord(c->r0, c->stream));
+  for (int i = 0; i < 5; ++i) launch();
+  CK(cudaEventRecord(c->r1, c->stream));
+  CK(cudaEventSynchronize(c->r1));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, c->r0, c->r1));
+  return ms / 5.f;
+}
+
 void autotune(bp_problem* P) {
   bp_ctx* c = P->c;
   DevView& v = P->v;
   P->tuned = true;
-  // BP_MV_CONFIG="minb,grid" fixes the choice (for sweeps)
   if (const char* e = std::getenv("BP_MV_CONFIG")) {
-    int mb = 0, g = 0;
-    if (std::sscanf(e, "%d,%d", &mb, &g) == 2) {
-      v.minb = mb;
-      v.grid_cap = g;
+    int a[4] = {0, 0, 0, 0};
+    const int n = std::sscanf(e, "%d,%d,%d,%d", &a[0], &a[1], &a[2], &a[3]);
+    if (n == 2 || n == 4) {
+      v.minb = a[0];
+      v.grid_cap = a[1];
+      v.minb_k = n == 4 ? a[2] : a[0];
+      v.grid_k = n == 4 ? a[3] : a[1];
       return;
     }
   }
-  const auto key = std::make_tuple(P->plan.nnodes >> 14, P->plan.nz, v.sym, v.A32 ? 1 : 0);
+  const int variant = P->plan.inst.empty() ? 0 : P->plan.inst[0].variant;
+  const auto key = std::make_tuple(P->plan.nnodes >> 14, P->plan.nz, v.sym, v.A32 ? 1 : 0, variant);
   auto it = c->tuned.find(key);
   if (it != c->tuned.end()) {
-    v.minb = it->second.first;
-    v.grid_cap = it->second.second;
+    v.minb = it->second[0];
+    v.grid_cap = it->second[1];
+    v.minb_k = it->second[2];
+    v.grid_k = it->second[3];
     return;
   }
-  const int grids[2] = {0, 4 * c->num_sms};
-  const int minbs[2] = {0, 4};
+  const bool log = std::getenv("BP_TUNE_LOG") != nullptr;
   float best = 1e30f;
   int bm = 0, bg = 0;
-  for (int mb : minbs)
-    for (int g : grids) {
+  for (int mb : {0, 4})
+    for (int g : {0, 4 * c->num_sms}) {
       if (g > 0 && g >= P->plan.ntiles) continue;  // same as one CTA per tile
       v.minb = mb;
       v.grid_cap = g;
-      launch_mv(MV_INIT, v, c->stream);
-      CK(cudaEventRecord(c->r0, c->stream));
-      for (int i = 0; i < 5; ++i) launch_mv(MV_INIT, v, c->stream);
-      CK(cudaEventRecord(c->r1, c->stream));
-      CK(cudaEventSynchronize(c->r1));
-      float ms = 0.f;
-      CK(cudaEventElapsedTime(&ms, c->r0, c->r1));
+      const float ms = time_launches(c, [&] { launch_mv(MV_INIT, v, c->stream); });
+      if (log) std::fprintf(stderr, "autotune resid minb %d grid %d: %.2f us\n", mb, g, ms * 1e3f);
       if (ms < best) { best = ms; bm = mb; bg = g; }
     }
-  CK(cudaGetLastError());
   v.minb = bm;
   v.grid_cap = bg;
-  c->tuned[key] = {bm, bg};
+  // the Krylov matvec on this storage (the FP32 copy is built here first:
+  // the linear solve rebuilds it, so the dry pass reads a real matrix)
+  if (v.A32) launch_make_a32(v, c->stream);
+  const int mode = variant == 3 ? MV_CG1 : MV_STD_A;
+  best = 1e30f;
+  int km = 0, kg = 0;
+  v.dry = 1;
+  for (int mb : {0, 4, 6}) {
+    const int res = krylov_resident_ctas(v, mode, mb);
+    if (res <= 0) continue;
+    for (int g : {0, res * c->num_sms}) {
+      if (g > 0 && g >= P->plan.ntiles) continue;
+      v.minb_k = mb;
+      v.grid_k = g;
+      const float ms = time_launches(c, [&] { launch_mv(mode, v, c->stream); });
+      if (log)
+        std::fprintf(stderr, "autotune krylov minb %d (%d CTAs/SM) grid %d: %.2f us\n", mb, res, g, ms * 1e3f);
+      if (ms < best) { best = ms; km = mb; kg = g; }
+    }
+  }
+  v.dry = 0;
+  CK(cudaGetLastError());
+  v.minb_k = km;
+  v.grid_k = kg;
+  c->tuned[key] = {bm, bg, km, kg};
 }
 
 // The Picard loop of glissade_velo_higher_solve on the device.
@@ -738,8 +782,8 @@ int bp_problem_mv_nodes(bp_problem* P, double* fp64_nodes, double* fp32_nodes, i
   if (!P) return BP_ERR_ARGS;
   if (fp64_nodes) *fp64_nodes = (double)P->mv_nodes[0];
   if (fp32_nodes) *fp32_nodes = (double)P->mv_nodes[1];
-  if (minb) *minb = P->v.minb;
-  if (grid) *grid = P->v.grid_cap;
+  if (minb) *minb = P->v.minb_k;
+  if (grid) *grid = P->v.grid_k;
   return BP_OK;
 }
 

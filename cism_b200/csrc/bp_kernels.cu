@@ -469,13 +469,15 @@ __device__ __forceinline__ double2 krylov_row(const DevView& v, const InstState&
 
 template <int STORE>
 __device__ __forceinline__ void count_tile(const DevView& v, const InstState& S, const TileRange& R) {
-  if (v.mv_nodes && threadIdx.x == 0) {
+  if (v.mv_nodes && !v.dry && threadIdx.x == 0) {
     const bool f32 = STORE == ST_SYM32 && !S.krylov_fp64;
     atomicAdd(&v.mv_nodes[f32 ? 1 : 0], (unsigned long long)(R.nend - R.n0));
   }
 }
 
 // Standard PCG: q = A d; (d, q); alpha = eta1 / (d, q)   (pcg:426-463).
+// In the autotuner's dry pass (v.dry) the Krylov matvecs run on every tile
+// and skip the scalar tail, so timing them changes no instance state.
 template <int STORE, int MINB>
 __global__ void __launch_bounds__(kTile, MINB) k_std_mv(DevView v) {
   pdl_wait();
@@ -483,7 +485,7 @@ __global__ void __launch_bounds__(kTile, MINB) k_std_mv(DevView v) {
   for (int t = blockIdx.x; t < v.ntiles; t += gridDim.x) {
     const TileRange R = tile_range(v, t);
     const InstState& S0 = v.st[R.inst];
-    if (!S0.pcg_active) continue;
+    if (!S0.pcg_active && !v.dry) continue;
     count_tile<STORE>(v, S0, R);
     const int n = R.n0 + threadIdx.x;
     double part[1] = {0.0};
@@ -495,6 +497,7 @@ __global__ void __launch_bounds__(kTile, MINB) k_std_mv(DevView v) {
       part[0] = d.x * y.x + d.y * y.y;
     }
     tile_finish<1, false>(v, t, R.inst, part, [&](int inst, const double* s) {
+      if (v.dry) return;
       InstState& S = v.st[inst];
       const double alpha = S.rz / s[0];
       if (is_nan(alpha)) { fail(v, S, BP_ERR_NAN); return; }
@@ -586,7 +589,7 @@ __global__ void __launch_bounds__(kTile, MINB) k_cg_mv(DevView v) {
   for (int t = blockIdx.x; t < v.ntiles; t += gridDim.x) {
     const TileRange R = tile_range(v, t);
     const InstState& S0 = v.st[R.inst];
-    if (!S0.pcg_active) continue;
+    if (!S0.pcg_active && !v.dry) continue;
     count_tile<STORE>(v, S0, R);
     const int n = R.n0 + threadIdx.x;
     double part[3] = {0.0, 0.0, 0.0};
@@ -605,6 +608,7 @@ __global__ void __launch_bounds__(kTile, MINB) k_cg_mv(DevView v) {
       part[2] = r.x * r.x + r.y * r.y;
     }
     tile_finish<3, false>(v, t, R.inst, part, [&](int inst, const double* s) {
+      if (v.dry) return;
       InstState& S = v.st[inst];
       if (FIRST) {
         S.rz_old = s[0];
@@ -888,27 +892,61 @@ static void launch_pcg(void (*kernel)(DevView), int g, cudaStream_t s, const Dev
   cudaLaunchKernelEx(&cfg, kernel, v);
 }
 
+using TileKernel = void (*)(DevView);
+
 template <int STORE, int MINB>
-static void launch_mv_store(int mode, const DevView& v, cudaStream_t s, int g) {
+static void launch_resid_store(int mode, const DevView& v, cudaStream_t s, int g) {
   switch (mode) {
     case MV_INIT: launch_pcg(k_resid<MV_INIT, STORE, MINB>, g, s, v); break;
     case MV_CHECK: launch_pcg(k_resid<MV_CHECK, STORE, MINB>, g, s, v); break;
-    case MV_REFINE: launch_pcg(k_resid<MV_REFINE, STORE, MINB>, g, s, v); break;
-    case MV_STD_A: launch_pcg(k_std_mv<STORE, MINB>, g, s, v); break;
-    case MV_CG_FIRST: launch_pcg(k_cg_mv<true, STORE, MINB>, g, s, v); break;
-    default: launch_pcg(k_cg_mv<false, STORE, MINB>, g, s, v); break;
+    default: launch_pcg(k_resid<MV_REFINE, STORE, MINB>, g, s, v); break;
+  }
+}
+template <int STORE, int MINB>
+static TileKernel krylov_kernel(int mode) {
+  switch (mode) {
+    case MV_STD_A: return k_std_mv<STORE, MINB>;
+    case MV_CG_FIRST: return k_cg_mv<true, STORE, MINB>;
+    default: return k_cg_mv<false, STORE, MINB>;
   }
 }
 template <int STORE>
-static void launch_mv_minb(int mode, const DevView& v, cudaStream_t s, int g) {
-  if (v.minb == 4) launch_mv_store<STORE, 4>(mode, v, s, g);
-  else launch_mv_store<STORE, 0>(mode, v, s, g);
+static TileKernel krylov_kernel_st(int mode, int minb) {
+  if (minb == 6) return krylov_kernel<STORE, 6>(mode);
+  if (minb == 4) return krylov_kernel<STORE, 4>(mode);
+  return krylov_kernel<STORE, 0>(mode);
+}
+static TileKernel krylov_kernel_for(const DevView& v, int mode, int minb) {
+  if (!v.sym) return krylov_kernel_st<ST_FULL>(mode, minb);
+  if (v.A32) return krylov_kernel_st<ST_SYM32>(mode, minb);
+  return krylov_kernel_st<ST_SYM>(mode, minb);
+}
+static inline bool is_krylov(int mode) {
+  return mode == MV_STD_A || mode == MV_CG_FIRST || mode == MV_CG1;
+}
+template <int STORE>
+static void launch_resid_minb(int mode, const DevView& v, cudaStream_t s, int g) {
+  if (v.minb == 4) launch_resid_store<STORE, 4>(mode, v, s, g);
+  else launch_resid_store<STORE, 0>(mode, v, s, g);
 }
 void launch_mv(int mode, const DevView& v, cudaStream_t s) {
+  if (is_krylov(mode)) {
+    int g = v.ntiles > 0 ? v.ntiles : 1;
+    if (v.grid_k > 0 && g > v.grid_k) g = v.grid_k;
+    launch_pcg(krylov_kernel_for(v, mode, v.minb_k), g, s, v);
+    return;
+  }
   const int g = tile_grid(v);
-  if (!v.sym) launch_mv_minb<ST_FULL>(mode, v, s, g);
-  else if (v.A32) launch_mv_minb<ST_SYM32>(mode, v, s, g);
-  else launch_mv_minb<ST_SYM>(mode, v, s, g);
+  if (!v.sym) launch_resid_minb<ST_FULL>(mode, v, s, g);
+  else if (v.A32) launch_resid_minb<ST_SYM32>(mode, v, s, g);
+  else launch_resid_minb<ST_SYM>(mode, v, s, g);
+}
+int krylov_resident_ctas(const DevView& v, int mode, int minb) {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, krylov_kernel_for(v, mode, minb), kTile, 0) !=
+      cudaSuccess)
+    return 0;
+  return n;
 }
 void launch_std_update(bool check, const DevView& v, cudaStream_t s) {
   launch_pcg(check ? k_std_update<true> : k_std_update<false>, tile_grid(v), s, v);

@@ -17,7 +17,12 @@ void launch_assemble(const DevView& v, cudaStream_t s);
 void launch_asm_qp(const DevView& v, cudaStream_t s);
 void launch_asm_rows(const DevView& v, cudaStream_t s);
 void launch_rhs(const DevView& v, cudaStream_t s);
+// Residual modes (MV_INIT, MV_CHECK, MV_REFINE) run with (minb, grid_cap),
+// the Krylov matvecs (MV_STD_A, MV_CG_FIRST, MV_CG1) with (minb_k, grid_k).
 void launch_mv(int mode, const DevView& v, cudaStream_t s);
+// CTAs of the Krylov matvec of this mode, storage and occupancy target
+// (0, 4, 6) that fit on one SM at once (0 on error).
+int krylov_resident_ctas(const DevView& v, int mode, int minb);
 void launch_std_update(bool check, const DevView& v, cudaStream_t s);
 void launch_std_dir(const DevView& v, cudaStream_t s);
 void launch_cg_first_update(const DevView& v, cudaStream_t s);

@@ -204,7 +204,8 @@ int bp_problem_kernel_times(bp_problem *p, double *ms, int *launches);
  * launch.  BP_ERR_ARGS if the variant does not match the storage. */
 int bp_problem_tune_mv(bp_problem *p, int store, int minb, int grid, int reps, float *ms);
 /* Nodes that went through FP64 and FP32 Krylov matvecs during the last
- * timing run, and the autotuner's choice (resident CTAs per SM, grid). */
+ * timing run, and the autotuner's choice for those matvecs (occupancy
+ * target in resident CTAs per SM, grid; 0 = none / one CTA per tile). */
 int bp_problem_mv_nodes(bp_problem *p, double *fp64_nodes, double *fp32_nodes,
                         int *minb, int *grid);
 /* Node count and, per FP64 matvec launch, the algorithmic bytes moved. */
