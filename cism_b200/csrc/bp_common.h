@@ -126,7 +126,12 @@ struct DevView {
   // FP64 [2][npad], carrying the rounding of its row's off-diagonal
   // entries so that the row sums are those of the FP64 matrix
   float4* A32;
-  double2* A32d;
+  double2* A32d;           // allocated right after A32 (one block of [16][npad] 16-byte elements)
+  // L2 access-policy window carried by the PCG kernels' launches (host-side
+  // launch setting; l2_bytes 0 = none)
+  const void* l2_base;
+  size_t l2_bytes;
+  float l2_hit;
   double* badj;            // [4][npad] Dirichlet column moves per block
   // vectors (per node, (u,v) pairs)
   double2 *x, *b, *r, *z, *d0, *q, *Az, *Dinv, *usav;

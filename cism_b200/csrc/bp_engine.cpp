@@ -92,6 +92,7 @@ struct bp_ctx {
   cudaEvent_t t0 = nullptr, t1 = nullptr, t2 = nullptr, t3 = nullptr;
   cudaEvent_t r0 = nullptr, r1 = nullptr;  // bp_timer_start / stop
   int num_sms = 0;
+  int l2_max_persist = 0, l2_max_window = 0;  // bytes (0 = no persisting L2)
   // autotuner results: (node bucket, nz, storage, precision, PCG variant)
   // -> (minb, grid) of the residual kernels, (minb_k, grid_k) of the Krylov matvecs
   std::map<std::tuple<int, int, int, int, int>, std::array<int, 4>> tuned;
@@ -188,8 +189,9 @@ DevView make_view(Arena& a, cudaStream_t s, const HostPlan& p, bool with_cells, 
   v.Dinv = a.get<double2>(s, "Dinv", np);
   v.usav = a.get<double2>(s, "usav", np);
   if (mixed && v.sym) {
-    v.A32 = a.get<float4>(s, "A32", 14 * np);
-    v.A32d = a.get<double2>(s, "A32d", 2 * np);
+    float4* blk = a.get<float4>(s, "A32", 16 * np);  // A32 then A32d: one L2 window
+    v.A32 = blk;
+    v.A32d = reinterpret_cast<double2*>(blk + 14 * np);
   }
   v.partials = a.get<double>(s, "partials", 3 * (size_t)std::max(p.ntiles, 1));
   v.tile_counter = a.get<unsigned>(s, "tile_counter", p.ninst);
@@ -454,7 +456,55 @@ void autotune(bp_problem* P) {
 }
 
 // The Picard loop of glissade_velo_higher_solve on the device.
+// Keeps the FP32 Krylov matrix of the mixed path (A32 with its FP64
+// diagonal, one block) in L2 across the PCG iterations of a run.  Every
+// matvec re-reads the whole block, and the update kernels stream about as
+// many bytes of vectors in between, which would evict it.  The PCG
+// kernels' launches carry an access-policy window that marks the block
+// persisting, and for the run L2 is set aside for persisting lines up to
+// the block's size (cudaLimitPersistingL2CacheSize, a limit of this
+// process's CUDA context; at the end of the run the persisting lines are
+// demoted and the previous limit restored).  Only when the block fits one
+// window; BP_L2_PIN=0 turns it off.  These are cache hints: a failing call
+// leaves the run as it is without them.
+struct L2Pin {
+  bp_problem* P;
+  size_t old_limit = 0;
+  bool set = false;
+  explicit L2Pin(bp_problem* p) : P(p) {
+    DevView& v = P->v;
+    bp_ctx* c = P->c;
+    v.l2_bytes = 0;
+    const char* e = std::getenv("BP_L2_PIN");
+    if (!v.A32 || (e && e[0] == '0') || c->l2_max_persist <= 0 || c->l2_max_window <= 0) return;
+    // offsets 14..26 and the FP64 diagonal (entry 0 of A32 is not read)
+    const size_t bytes = 15 * sizeof(float4) * (size_t)v.npad;
+    if (bytes > (size_t)c->l2_max_window) return;
+    const size_t aside = std::min(bytes, (size_t)c->l2_max_persist);
+    if (cudaDeviceGetLimit(&old_limit, cudaLimitPersistingL2CacheSize) != cudaSuccess ||
+        cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, aside) != cudaSuccess) {
+      cudaGetLastError();
+      return;
+    }
+    set = true;
+    v.l2_base = v.A32 + v.npad;
+    v.l2_bytes = bytes;
+    v.l2_hit = (float)std::min(1.0, (double)aside / (double)bytes);
+    if (std::getenv("BP_TUNE_LOG"))
+      std::fprintf(stderr, "l2 pin: block %.1f MB, set aside %.1f MB (max %.1f MB, window max %.1f MB), hit %.3f\n",
+                   bytes / 1e6, aside / 1e6, c->l2_max_persist / 1e6, c->l2_max_window / 1e6, v.l2_hit);
+  }
+  ~L2Pin() {
+    if (!set) return;
+    cudaStreamSynchronize(P->c->stream);
+    cudaCtxResetPersistingL2Cache();
+    cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, old_limit);
+    cudaGetLastError();
+  }
+};
+
 void run_picard(bp_problem* P) {
+  const L2Pin pin(P);
   const HostPlan& p = P->plan;
   const DevView& v = P->v;
   bp_ctx* c = P->c;
@@ -624,6 +674,11 @@ int bp_create(int device, bp_ctx** out) {
     CK(cudaEventCreate(&c->r0));
     CK(cudaEventCreate(&c->r1));
     CK(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device));
+    if (cudaDeviceGetAttribute(&c->l2_max_persist, cudaDevAttrMaxPersistingL2CacheSize, device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&c->l2_max_window, cudaDevAttrMaxAccessPolicyWindowSize, device) != cudaSuccess) {
+      c->l2_max_persist = c->l2_max_window = 0;
+      cudaGetLastError();
+    }
     CK(bp::upload_ref_tables());
   } catch (const CudaError& e) {
     std::fprintf(stderr, "bp_create: %s failed: %s\n", e.what, cudaGetErrorString(e.e));
@@ -757,8 +812,9 @@ int bp_problem_tune_mv(bp_problem* P, int store, int minb, int grid, int reps, f
   GUARD_BEGIN(P->c)
   bp_ctx* c = P->c;
   if (store == 2 && P->v.sym && !P->v.A32) {
-    P->v.A32 = P->arena->get<float4>(c->stream, "A32", 14 * (size_t)P->plan.npad);
-    P->v.A32d = P->arena->get<double2>(c->stream, "A32d", 2 * (size_t)P->plan.npad);
+    float4* blk = P->arena->get<float4>(c->stream, "A32", 16 * (size_t)P->plan.npad);
+    P->v.A32 = blk;
+    P->v.A32d = reinterpret_cast<double2*>(blk + 14 * (size_t)P->plan.npad);
     launch_make_a32(P->v, c->stream);
   }
   if (launch_tune_mv(store, minb, grid, P->v, c->stream) != 0) return BP_ERR_ARGS;  // warm

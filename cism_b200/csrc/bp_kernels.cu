@@ -872,7 +872,8 @@ void launch_assemble(const DevView& v, cudaStream_t s) {
   launch_rhs(v, s);
 }
 // PCG kernels are launched as programmatic dependents of their stream
-// predecessor (BP_PDL=0 turns this off).
+// predecessor (BP_PDL=0 turns this off), and with the problem's L2
+// access-policy window when it has one.
 static const bool g_pdl = [] {
   const char* e = std::getenv("BP_PDL");
   return !(e && e[0] == '0');
@@ -884,11 +885,24 @@ static void launch_pcg(void (*kernel)(DevView), int g, cudaStream_t s, const Dev
   cfg.blockDim = dim3(kTile);
   cfg.dynamicSmemBytes = 0;
   cfg.stream = s;
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchAttribute at[2];
+  unsigned na = 0;
+  if (g_pdl) {
+    at[na].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[na].val.programmaticStreamSerializationAllowed = 1;
+    ++na;
+  }
+  if (v.l2_bytes > 0) {
+    at[na].id = cudaLaunchAttributeAccessPolicyWindow;
+    at[na].val.accessPolicyWindow.base_ptr = const_cast<void*>(v.l2_base);
+    at[na].val.accessPolicyWindow.num_bytes = v.l2_bytes;
+    at[na].val.accessPolicyWindow.hitRatio = v.l2_hit;
+    at[na].val.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+    at[na].val.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+    ++na;
+  }
   cfg.attrs = at;
-  cfg.numAttrs = g_pdl ? 1 : 0;
+  cfg.numAttrs = na;
   cudaLaunchKernelEx(&cfg, kernel, v);
 }
 
