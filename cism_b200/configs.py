@@ -34,6 +34,37 @@ SPARSE_PCG_STANDARD, SPARSE_PCG_CHRONGEAR = 2, 3
 SPARSE_B200 = 5
 PRECOND_NONE, PRECOND_DIAG, PRECOND_SIA = 0, 1, 2
 ASSEMBLE_STANDARD, ASSEMBLE_LOCAL = 0, 1
+# velocity-dependent sliding laws (glide_types.F90:211-225)
+(BABC_YIELD_PICARD, BABC_PSEUDO_PLASTIC, BABC_POWERLAW, BABC_COULOMB_FRICTION,
+ BABC_COULOMB_POWERLAW_SCHOOF, BABC_COULOMB_POWERLAW_TSAI, BABC_POWERLAW_EFFECPRESS) = 2, 3, 9, 10, 11, 12, 13
+SLIDING_LAWS = (2, 3, 9, 10, 11, 12, 13)
+
+
+@dataclasses.dataclass
+class SlidingLaw:
+    """A velocity-dependent sliding law of calcbeta
+    (libglissade/glissade_basal_traction.F90:67-598), evaluated from the
+    basal velocity at every Picard iteration.  ``law`` is the which_ho_babc
+    value; the parameters default to libglide/glide_types.F90:1300-1370.
+    Vertex fields have shape (ny-1, nx-1)."""
+
+    law: int
+    effecpress_stag: Optional[np.ndarray] = None      # N, Pa (laws 3, 10-13)
+    c_space_factor_stag: Optional[np.ndarray] = None  # law 10 (None: 1)
+    yield_stress: Optional[np.ndarray] = None          # mintauf * tau0, Pa (law 2)
+    beta_powerlaw_umax: float = 0.0
+    powerlaw_c: float = 1.0e4
+    powerlaw_m: float = 3.0
+    coulomb_c: float = 0.42
+    coulomb_bump_max_slope: float = 0.5
+    coulomb_bump_wavelength: float = 2.0
+    friction_powerlaw_k: float = 8.4e-9
+    pseudo_plastic_q: float = 0.5
+    pseudo_plastic_u0: float = 100.0
+    pseudo_plastic_phimin: float = 5.0
+    pseudo_plastic_phimax: float = 40.0
+    pseudo_plastic_bedmin: float = -700.0
+    pseudo_plastic_bedmax: float = 700.0
 
 
 @dataclasses.dataclass
@@ -76,6 +107,7 @@ class BPModel:
     pcg_maxiters: int = 200
     pcg_tol: float = 1.0e-8
     pcg_ncheck: int = 5
+    sliding: Optional[SlidingLaw] = None  # velocity-dependent law (which_babc = sliding.law)
     name: str = ""
 
     @property
@@ -382,6 +414,33 @@ def _sliding_dome(gx: int, gy: int, dx: float, nz: int, rng: np.random.Generator
                    flwa=np.full((ny, nx, nz - 1), 1.0e-16), beta_external=np.zeros((ny - 1, nx - 1)),
                    thklim=1.0, which_babc=BABC_BETA_EXTERNAL, which_sparse=SPARSE_PCG_STANDARD,
                    which_precond=PRECOND_DIAG, which_resid=RESID_MAXU, name=f"dome{gx}x{gy}")
+
+
+def with_sliding(m: BPModel, law: int, seed: int = 0, n_scale: float = 0.8, **params) -> BPModel:
+    """``m`` with a velocity-dependent sliding law (which_babc = law).
+
+    Synthetic basal fields on the (ny-1, nx-1) vertex grid: effective
+    pressure N = n_scale * rho_i g H (H averaged over the four cells of the
+    vertex) times a seeded smooth factor in [0.7, 1.3]; for law 2 a yield
+    stress of 40 kPa times such a factor; for law 10 a C_space factor in
+    [0.8, 1.2].  ``params`` override SlidingLaw's defaults.
+    """
+    rng = np.random.default_rng(seed)
+    ny, nx = m.thck.shape
+    hv = 0.25 * (m.thck[:-1, :-1] + m.thck[:-1, 1:] + m.thck[1:, :-1] + m.thck[1:, 1:])
+    jj, ii = np.meshgrid(np.arange(ny - 1), np.arange(nx - 1), indexing="ij")
+
+    def factor(amp):
+        ph = rng.uniform(0.0, 2.0 * np.pi, 2)
+        return 1.0 + amp * np.sin(2.0 * np.pi * ii / max(nx - 5, 1) + ph[0]) * \
+            np.cos(2.0 * np.pi * jj / max(ny - 5, 1) + ph[1])
+
+    sl = SlidingLaw(law=law, effecpress_stag=n_scale * m.rhoi * m.grav * hv * factor(0.3), **params)
+    if law == BABC_YIELD_PICARD:
+        sl.yield_stress = 4.0e4 * factor(0.3)
+    if law == BABC_COULOMB_FRICTION:
+        sl.c_space_factor_stag = factor(0.2)
+    return m.copy(which_babc=law, sliding=sl, name=f"{m.name}_law{law}")
 
 
 def random_slab(rng: np.random.Generator, n: int = 96, dx: float = 500.0, nz: int = 11) -> BPModel:

@@ -240,6 +240,58 @@ BP_HD void row_assemble(const DevView& v, const RefTables& T, int col, int k,
   }
 }
 
+// calcbeta (glissade_basal_traction.F90:67-598) at one vertex for the
+// velocity-dependent laws, from the basal velocity (u, v) in m/a: the
+// speed with its 0.01 m/a floor (:181) and optional cap (:187-189), the law
+// (:207-264 pseudo-plastic, :266-277 yield stress, :357-363 power law,
+// :365-382 power law with N, :384-424 Coulomb friction, :426-470
+// Coulomb/power law after Schoof, :472-509 after Tsai), the grounded
+// fraction (:540) and the grounded minimum (:560-566).  fg = f_ground; c1,
+// c2 = the vertex's products formed before the speed enters (see
+// SlideParams); the operations keep the reference's order.
+BP_HD double slide_beta(const SlideParams& sp, double fg, double c1, double c2, double u,
+                        double v) {
+  const double smallnum = 1.0e-2;
+  const double s0 = sqrt(u * u + v * v + smallnum * smallnum);
+  double speed = s0;
+  if (sp.umax > 0.0 && sp.umax < speed) speed = sp.umax;
+  double beta = 0.0;
+  switch (sp.law) {
+    case 2:  // tau_y / |u|, from the uncapped speed
+      beta = c1 / s0;
+      break;
+    case 3:  // tan(phi) N / (u0^q speed^(1-q))
+      beta = c1 / (sp.k * pow(speed, sp.e1));
+      break;
+    case 9:  // C speed^(1/m - 1)
+      beta = sp.c * pow(speed, sp.e2);
+      break;
+    case 10:  // c Cs N speed^(1/n - 1) (speed + N^n lambda)^(-1/n), at most 1e8
+      beta = c1 * pow(speed, sp.e1) * pow(speed + c2, sp.e2);
+      if (beta > 1.0e8) beta = 1.0e8;
+      break;
+    case 11: {  // C c N / (C^m speed + (c N)^m)^(1/m) speed^(1/m - 1), at most 1e8
+      const double den = pow(sp.k * speed + c2, sp.e1);
+      beta = (c1 / den) * pow(speed, sp.e2);
+      if (beta > 1.0e8) beta = 1.0e8;
+      break;
+    }
+    case 12: {  // min(c N, C speed^(1/m)) / speed
+      const double tp = sp.c * pow(speed, sp.e1);
+      beta = (c1 <= tp ? c1 : tp) / speed;
+      break;
+    }
+    case 13:  // k^(-1/p) N^(q/p) speed^(1/p - 1)
+      beta = c1 * pow(speed, sp.e1);
+      break;
+    default:
+      break;
+  }
+  beta = beta * fg;
+  if (fg > 0.0 && beta < sp.bmin) beta = sp.bmin;
+  return beta;
+}
+
 // basal_sliding_bc (:8125-8381), bed layer only, diagonal blocks only.
 template <int B>
 BP_HD void row_basal(const DevView& v, const RefTables& T, int col, int k,

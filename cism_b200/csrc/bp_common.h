@@ -30,6 +30,21 @@ constexpr int kNzMax = 64;     // largest supported number of levels
 constexpr int kTile = 256;     // nodes per tile; one CTA of kTile threads per tile
 constexpr double kVol0 = 1.0e9;  // volume scale, glissade_velo_higher.F90:1111
 
+// Velocity-dependent sliding law of an instance (calcbeta,
+// glissade_basal_traction.F90:67-598), law = which_ho_babc; 0 = none
+// (beta fixed over the Picard loop).  The exponents and the products of
+// constants the law evaluates before the speed enters are formed on the
+// host; per-column products live in DevView::col_slide.
+struct SlideParams {
+  int law;
+  double umax;   // beta_powerlaw_umax (<= 0: no cap)
+  double bmin;   // beta_grounded_min
+  double c;      // powerlaw_c (laws 9, 12)
+  double e1;     // law 3: 1 - q; 10: 1/gn - 1; 11, 12: 1/m; 13: 1/p - 1
+  double e2;     // law 9, 11: 1/m - 1; 10: -1/gn
+  double k;      // law 3: u0^q; 11: powerlaw_c^m
+};
+
 // Per-instance constants (read-only on the device).
 struct InstParams {
   double dx, dy;
@@ -45,6 +60,7 @@ struct InstParams {
   int tile_begin, tile_end;
   int cell_begin, cell_end;
   int elem_begin, elem_end;
+  SlideParams slide;
 };
 
 // Per-instance solver state (device-resident, written by finalizers).
@@ -97,7 +113,8 @@ struct DevView {
   const int* col_nbr;      // [9][ncols], q = (jA+1)*3 + (iA+1); -1 = none
   const int* col_cells;    // [4][ncols], cells (i,j),(i+1,j),(i,j+1),(i+1,j+1)
   const int* col_ij;       // [2][ncols], halo'd Fortran vertex indices
-  const double* col_beta;  // [ncols] beta_internal
+  double* col_beta;        // [ncols] beta_internal (recomputed each Picard iteration with a sliding law)
+  const double* col_slide; // [3][ncols] sliding law: f_ground and two per-vertex products, or null
   // nodes
   const double2* load;     // [nnodes] (loadu, loadv)
   const uint8_t* dmask;    // [nnodes] bit0 u prescribed, bit1 v prescribed
@@ -107,7 +124,7 @@ struct DevView {
   const int* cell_cols;    // [4][ncells] corner columns SW, SE, NE, NW (-1 = none)
   const double* cell_s;    // [4][ncells] stagusrf at the corners
   const double* cell_h;    // [4][ncells] stagthck at the corners
-  const double* cell_beta; // [4][ncells] beta_internal at the corners
+  double* cell_beta;       // [4][ncells] beta_internal at the corners (sliding law: 0 where no column)
   const double* flwafact;  // [ncells*(nz-1)]
   // tiles
   const int* tile_start;   // [ntiles] first node (tiles hold whole columns)

@@ -160,6 +160,7 @@ DevView make_view(Arena& a, cudaStream_t s, const HostPlan& p, bool with_cells, 
   UP(int, "col_cells", p.col_cells, col_cells);
   UP(int, "col_ij", p.col_ij, col_ij);
   UP(double, "col_beta", p.col_beta, col_beta);
+  if (p.any_sliding) UP(double, "col_slide", p.col_slide, col_slide);
   UP(double2, "load", p.load, load);
   UP(uint8_t, "dmask", p.dmask, dmask);
   if (with_cells) {
@@ -514,6 +515,7 @@ void run_picard(bp_problem* P) {
   for (int it = 0; it < max_picard; ++it) {
     L(P, C_OTHER, [&] { launch_picard_begin(v, s); });
     L(P, C_OTHER, [&] { launch_save_usav(v, s); });
+    if (p.any_sliding) L(P, C_OTHER, [&] { launch_slide_beta(v, s); });
     L(P, C_ASM1, [&] { launch_asm_qp(v, s); });
     L(P, C_ASM2, [&] { launch_asm_rows(v, s); });
     L(P, C_RHS, [&] { launch_rhs(v, s); });
@@ -1015,6 +1017,7 @@ int bp_assemble(bp_ctx* c, const bp_inputs* in, const double* uvel,
   CK(cudaMemcpyAsync(v.x, x.data(), sizeof(double2) * p.npad, cudaMemcpyHostToDevice, c->stream));
   init_state(c->stream, v, p, true, false);
   launch_picard_begin(v, c->stream);
+  if (p.any_sliding) launch_slide_beta(v, c->stream);
   launch_asm_qp(v, c->stream);
   launch_asm_rows(v, c->stream);
   launch_rhs(v, c->stream);

@@ -175,6 +175,42 @@ __global__ void k_picard_begin(DevView v) {
   }
 }
 
+// calcbeta with a velocity-dependent law at the start of a Picard iteration
+// (glissade_velo_higher.F90:2502-2517): beta of every column of an active
+// instance from its basal velocity x(nz-1).  An invalid beta (negative or
+// NaN, glissade_basal_traction.F90:570-582) marks the instance; k_rhs ends
+// it with BP_ERR_BAD_BETA before its linear solve.
+__global__ void __launch_bounds__(kTile) k_slide_beta(DevView v) {
+  for (int col = blockIdx.x * blockDim.x + threadIdx.x; col < v.ncols; col += gridDim.x * blockDim.x) {
+    const int inst = v.col_inst[col];
+    const InstParams& ip = v.inst[inst];
+    InstState& S = v.st[inst];
+    if (!S.picard_active || ip.slide.law == 0) continue;
+    const size_t nc = (size_t)v.ncols;
+    const double2 ub = v.x[(size_t)col * v.nz + v.nz - 1];
+    const double beta = slide_beta(ip.slide, v.col_slide[col], v.col_slide[nc + col],
+                                   v.col_slide[2 * nc + col], ub.x, ub.y);
+    if (!(beta >= 0.0) && (S.status == BP_OK || S.status == BP_WARN_PCG_NOT_CONVERGED))
+      S.status = BP_ERR_BAD_BETA;
+    v.col_beta[col] = beta;
+  }
+}
+
+// Corner betas of the bed faces for the standard basal assembly
+// (basal_sliding_bc :8234-8363) after k_slide_beta: the corner's column,
+// or 0 where the corner has no column (a vertex outside an outflow domain,
+// zeroed by the staggered halo update).
+__global__ void __launch_bounds__(kTile) k_cell_beta(DevView v) {
+  for (int cell = blockIdx.x * blockDim.x + threadIdx.x; cell < v.ncells; cell += gridDim.x * blockDim.x) {
+    const int inst = v.cell_inst[cell];
+    if (!v.st[inst].picard_active || v.inst[inst].slide.law == 0) continue;
+    for (int q = 0; q < 4; ++q) {
+      const int col = v.cell_cols[(size_t)q * v.ncells + cell];
+      v.cell_beta[(size_t)q * v.ncells + cell] = col >= 0 ? v.col_beta[col] : 0.0;
+    }
+  }
+}
+
 __global__ void __launch_bounds__(kTile) k_save_usav(DevView v) {
   for (int t = blockIdx.x; t < v.ntiles; t += gridDim.x) {
     const TileRange R = tile_range(v, t);
@@ -296,8 +332,8 @@ __global__ void __launch_bounds__(kTile) k_rhs(DevView v) {
       InstState& S = v.st[inst];
       S.bb = s[0];
       S.L2_rhs = sqrt(s[0]);
-      if (S.status == BP_ERR_SINGULAR_JAC) {
-        fail(v, S, BP_ERR_SINGULAR_JAC);
+      if (S.status == BP_ERR_SINGULAR_JAC || S.status == BP_ERR_BAD_BETA) {
+        fail(v, S, S.status);
       } else if (!S.nonzero) {
         S.status = BP_ZERO_MATRIX;
         S.zero_x = 1;
@@ -855,6 +891,10 @@ cudaError_t upload_ref_tables() {
 
 void launch_picard_begin(const DevView& v, cudaStream_t s) { k_picard_begin<<<1, 256, 0, s>>>(v); }
 void launch_save_usav(const DevView& v, cudaStream_t s) { k_save_usav<<<tile_grid(v), kTile, 0, s>>>(v); }
+void launch_slide_beta(const DevView& v, cudaStream_t s) {
+  if (v.ncols > 0) k_slide_beta<<<(v.ncols + kTile - 1) / kTile, kTile, 0, s>>>(v);
+  if (v.ncells > 0) k_cell_beta<<<(v.ncells + kTile - 1) / kTile, kTile, 0, s>>>(v);
+}
 void launch_asm_qp(const DevView& v, cudaStream_t s) {
   if (v.nelem > 0) {
     const long threads = (long)v.nelem * 8;

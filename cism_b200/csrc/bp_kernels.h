@@ -13,6 +13,9 @@ cudaError_t upload_ref_tables();
 
 void launch_picard_begin(const DevView& v, cudaStream_t s);
 void launch_save_usav(const DevView& v, cudaStream_t s);
+// beta of the velocity-dependent sliding laws from the current velocity
+// (and the corner betas of the standard basal assembly)
+void launch_slide_beta(const DevView& v, cudaStream_t s);
 void launch_assemble(const DevView& v, cudaStream_t s);
 void launch_asm_qp(const DevView& v, cudaStream_t s);
 void launch_asm_rows(const DevView& v, cudaStream_t s);

@@ -119,6 +119,108 @@ bool build_column_plan(int nx, int ny, int nz, int periodic,
   return true;
 }
 
+// calcbeta's velocity-dependent laws (glissade_basal_traction.F90:67-598):
+// the factors that do not depend on the speed, in the reference's order of
+// evaluation.  gn = 3 is an integer in the reference (glimmer_physcon.F90:75),
+// so N**gn is a product and 1/gn a real division; the law with effective
+// pressure fixes p = 3, q = 1 (:378-379); pi is glimmer_physcon's literal.
+bool slide_params(const bp_sliding& L, SlideParams* sp, std::string* err) {
+  std::memset(sp, 0, sizeof(*sp));
+  const bool needN = L.law == 3 || (L.law >= 10 && L.law <= 13);
+  if (L.law != 2 && L.law != 3 && !(L.law >= 9 && L.law <= 13)) {
+    *err = "sliding law must be 2, 3 or 9-13 (velocity-dependent which_ho_babc)";
+    return false;
+  }
+  if (!L.f_ground || (needN && !L.effecpress_stag) || (L.law == 2 && !L.yield_stress) ||
+      (L.law == 3 && !L.topg) || (L.law == 10 && !L.flwa_basal_stag)) {
+    *err = "sliding law: missing input field";
+    return false;
+  }
+  if ((L.law >= 9 && L.law <= 12 && L.law != 10 && !(L.powerlaw_m > 0.0)) ||
+      (L.law == 10 && !(L.coulomb_bump_max_slope > 0.0))) {
+    *err = "sliding law: powerlaw_m and coulomb_bump_max_slope must be > 0";
+    return false;
+  }
+  sp->law = L.law;
+  sp->umax = L.beta_powerlaw_umax;
+  sp->bmin = L.beta_grounded_min;
+  const double m = L.powerlaw_m;
+  switch (L.law) {
+    case 3:
+      sp->k = std::pow(L.pseudo_plastic_u0, L.pseudo_plastic_q);
+      sp->e1 = 1.0 - L.pseudo_plastic_q;
+      break;
+    case 9:
+      sp->c = L.powerlaw_c;
+      sp->e2 = 1.0 / m - 1.0;
+      break;
+    case 10:
+      sp->e1 = 1.0 / 3 - 1.0;
+      sp->e2 = -1.0 / 3;
+      break;
+    case 11:
+      sp->k = std::pow(L.powerlaw_c, m);
+      sp->e1 = 1.0 / m;
+      sp->e2 = 1.0 / m - 1.0;
+      break;
+    case 12:
+      sp->c = L.powerlaw_c;
+      sp->e1 = 1.0 / m;
+      break;
+    case 13:
+      sp->e1 = 1.0 / 3.0 - 1.0;
+      break;
+    default:
+      break;
+  }
+  return true;
+}
+
+void slide_vertex(const bp_sliding& L, int i, int j, int nx, double* c1, double* c2) {
+  const size_t v = vtx(i, j, nx);
+  const double N = L.effecpress_stag ? L.effecpress_stag[v] : 0.0;
+  *c1 = 0.0;
+  *c2 = 0.0;
+  switch (L.law) {
+    case 2:
+      *c1 = L.yield_stress[v];
+      break;
+    case 3: {  // :225-247, phi from topg(ew,ns) read at the vertex's indices
+      const double pi = 3.14159265358979;
+      const double bed = L.topg[cel(i, j, nx)] - L.eus;
+      double phi;
+      if (bed <= L.pseudo_plastic_bedmin) phi = L.pseudo_plastic_phimin;
+      else if (bed >= L.pseudo_plastic_bedmax) phi = L.pseudo_plastic_phimax;
+      else
+        phi = L.pseudo_plastic_phimin + ((bed - L.pseudo_plastic_bedmin) /
+                                         (L.pseudo_plastic_bedmax - L.pseudo_plastic_bedmin)) *
+                                            (L.pseudo_plastic_phimax - L.pseudo_plastic_phimin);
+      const double tanphi = std::tan(phi * pi / 180.0);
+      *c1 = tanphi * N;
+      break;
+    }
+    case 10: {  // :400-418
+      const double cs = L.c_space_factor_stag ? L.c_space_factor_stag[v] : 1.0;
+      const double big_lambda = (L.coulomb_bump_wavelength / L.coulomb_bump_max_slope) * L.flwa_basal_stag[v];
+      *c1 = L.coulomb_c * cs * N;
+      *c2 = N * N * N * big_lambda;
+      break;
+    }
+    case 11:  // :446-451
+      *c1 = L.powerlaw_c * L.coulomb_c * N;
+      *c2 = std::pow(L.coulomb_c * N, L.powerlaw_m);
+      break;
+    case 12:  // :490
+      *c1 = L.coulomb_c * N;
+      break;
+    case 13:  // :380-382
+      *c1 = std::pow(L.friction_powerlaw_k, -1.0 / 3.0) * std::pow(N, 1.0 / 3.0);
+      break;
+    default:
+      break;
+  }
+}
+
 bool build_plan(const bp_inputs* in, int n, HostPlan* p, std::string* err) {
   if (n < 1 || !in) { *err = "no instances"; return false; }
   *p = HostPlan();
@@ -143,9 +245,18 @@ bool build_plan(const bp_inputs* in, int n, HostPlan* p, std::string* err) {
     }
     if (!I.stagusrf || !I.stagthck || !I.flwafact || !I.active_cell || !I.active_vertex ||
         !I.loadu || !I.loadv || !I.umask_dirichlet || !I.vmask_dirichlet || !I.sigma ||
-        !I.beta_internal) {
+        (!I.beta_internal && !I.sliding)) {
       *err = "missing input array";
       return false;
+    }
+    if (I.sliding) {
+      SlideParams sp;
+      if (!slide_params(*I.sliding, &sp, err)) return false;
+      if (I.which_babc != I.sliding->law) {
+        *err = "which_babc must equal the sliding law";
+        return false;
+      }
+      p->any_sliding = true;
     }
     p->nx.push_back(I.nx); p->ny.push_back(I.ny); p->periodic.push_back(I.periodic);
     add_columns(I.nx, I.ny, nz, I.periodic, I.active_vertex, b, p, &cms[b], &cols[b]);
@@ -160,6 +271,7 @@ bool build_plan(const bp_inputs* in, int n, HostPlan* p, std::string* err) {
   p->col_nbr.resize(9 * (size_t)NC);
   p->col_cells.assign(4 * (size_t)NC, -1);
   p->col_beta.resize(NC);
+  if (p->any_sliding) p->col_slide.assign(3 * (size_t)NC, 0.0);
   p->load.resize(p->nnodes);
   p->dmask.resize(p->nnodes);
   // cells: count first (cell ids must be global)
@@ -206,6 +318,7 @@ bool build_plan(const bp_inputs* in, int n, HostPlan* p, std::string* err) {
     ip.pcg_maxiters = I.pcg_maxiters;
     ip.ncheck = I.pcg_ncheck > 0 ? I.pcg_ncheck : 5;
     ip.maxiter_nonlinear = I.maxiter_nonlinear;
+    if (I.sliding) slide_params(*I.sliding, &ip.slide, err);
     const int nc = (int)cols[b].size();
     ip.col_begin = col_base; ip.col_end = col_base + nc;
     ip.node_begin = col_base * nz; ip.node_end = (col_base + nc) * nz;
@@ -229,7 +342,13 @@ bool build_plan(const bp_inputs* in, int n, HostPlan* p, std::string* err) {
           id = cellid[b][cel(ci[q], cj[q], nx)];
         p->col_cells[(size_t)q * NC + g] = id;
       }
-      p->col_beta[g] = I.beta_internal[vtx(i, j, nx)];
+      if (I.sliding) {  // recomputed on the device at every Picard iteration
+        p->col_beta[g] = 0.0;
+        p->col_slide[g] = I.sliding->f_ground[vtx(i, j, nx)];
+        slide_vertex(*I.sliding, i, j, nx, &p->col_slide[(size_t)NC + g], &p->col_slide[2 * (size_t)NC + g]);
+      } else {
+        p->col_beta[g] = I.beta_internal[vtx(i, j, nx)];
+      }
       for (int k = 0; k < nz; ++k) {
         const size_t src = vtx(i, j, nx) * nz + k;
         p->load[(size_t)g * nz + k] = double2{I.loadu[src], I.loadv[src]};
@@ -249,7 +368,7 @@ bool build_plan(const bp_inputs* in, int n, HostPlan* p, std::string* err) {
         p->cell_cols[(size_t)q * NCELL + g] = cms[b].lookup(vi[q], vj[q]);
         p->cell_s[(size_t)q * NCELL + g] = I.stagusrf[v];
         p->cell_h[(size_t)q * NCELL + g] = I.stagthck[v];
-        p->cell_beta[(size_t)q * NCELL + g] = I.beta_internal[v];
+        p->cell_beta[(size_t)q * NCELL + g] = I.sliding ? 0.0 : I.beta_internal[v];
       }
       for (int k = 0; k < nz - 1; ++k)
         p->flwafact[(size_t)g * (nz - 1) + k] = I.flwafact[cel(ic, jc, nx) * (nz - 1) + k];

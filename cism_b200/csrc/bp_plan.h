@@ -28,6 +28,8 @@ struct HostPlan {
   std::vector<InstParams> inst;
   std::vector<int> col_inst, col_nbr, col_cells, col_ij;
   std::vector<double> col_beta;
+  std::vector<double> col_slide;  // [3][ncols] (f_ground, c1, c2) when any instance has a sliding law
+  bool any_sliding = false;
   std::vector<double2> load;
   std::vector<uint8_t> dmask;
   std::vector<int> cell_inst, cell_ij, cell_cols;
@@ -42,6 +44,14 @@ struct HostPlan {
 bool build_column_plan(int nx, int ny, int nz, int periodic,
                        const int* active_vertex, HostPlan* plan,
                        std::string* err);
+
+// Checks a velocity-dependent sliding law and forms its per-instance
+// constants (SlideParams); false with *err when the law or a field it
+// needs is missing.
+bool slide_params(const bp_sliding& L, SlideParams* sp, std::string* err);
+// The two per-vertex products of the law at vertex (i,j) (1-based) of an
+// instance with nx cells in x (SlideParams).
+void slide_vertex(const bp_sliding& L, int i, int j, int nx, double* c1, double* c2);
 
 // Full plan for n solves.
 bool build_plan(const bp_inputs* in, int n, HostPlan* plan, std::string* err);

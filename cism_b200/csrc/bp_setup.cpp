@@ -53,6 +53,9 @@ extern "C" int bp_setup(const bp_model* m, bp_setup_arrays* o, double* uvel,
   const int nx = m->nx, ny = m->ny, nz = m->nz;
   if (m->nhalo != 2 || nx < 6 || ny < 6 || nz < 2 || nz > bp::kNzMax) return BP_ERR_ARGS;
   if (!m->thck || !m->usrf || !m->topg || !m->flwa) return BP_ERR_ARGS;
+  if (m->sliding && (m->sliding->law != m->which_babc || !o->f_ground ||
+                     (m->sliding->law == 10 && !o->flwa_basal_stag)))
+    return BP_ERR_ARGS;
   const Cells C{nx, ny};
   const Verts V{nx, ny};
   const size_t ncell = (size_t)nx * ny, nvert = (size_t)(nx - 1) * (ny - 1), n3 = nvert * nz;
@@ -261,8 +264,37 @@ extern "C" int bp_setup(const bp_model* m, bp_setup_arrays* o, double* uvel,
       if (fg > 0.0 && b < m->beta_grounded_min) b = m->beta_grounded_min;
       if (!(b >= 0.0)) return BP_ERR_BAD_BETA;
       o->beta_internal[V(i, j)] = b;
+      if (m->sliding) o->f_ground[V(i, j)] = fg;
     }
   bp::halo_stag(nx, ny, 1, m->periodic, o->beta_internal);
+
+  // velocity-dependent sliding law: the solve evaluates it every Picard
+  // iteration from f_ground and, for Coulomb friction, the basal layer's
+  // flow factor staggered over cells with thck > 0
+  // (glissade_basal_traction.F90:393-398, glissade_stagger margin 1)
+  if (m->sliding) {
+    if (m->sliding->law == 10) {
+      for (int j = 1; j <= ny - 1; ++j)
+        for (int i = 1; i <= nx - 1; ++i) {
+          const size_t cc[4] = {C(i, j + 1), C(i + 1, j + 1), C(i, j), C(i + 1, j)};
+          double sumvar = 0.0;
+          int summask = 0;
+          for (int q = 0; q < 4; ++q) {
+            const int w = m->thck[cc[q]] > 0.0 ? 1 : 0;
+            const double term = (double)w * m->flwa[cc[q] * (nz - 1) + (nz - 2)];
+            sumvar = q == 0 ? term : sumvar + term;
+            summask += w;
+          }
+          o->flwa_basal_stag[V(i, j)] = summask > 0 ? sumvar / (double)summask : 0.0;
+        }
+    }
+    o->sliding = *m->sliding;
+    o->sliding.f_ground = o->f_ground;
+    o->sliding.topg = m->topg;
+    o->sliding.eus = m->eus;
+    o->sliding.beta_grounded_min = m->beta_grounded_min;
+    if (m->sliding->law == 10) o->sliding.flwa_basal_stag = o->flwa_basal_stag;
+  }
 
   if (in) {
     std::memset(in, 0, sizeof(*in));
@@ -281,6 +313,7 @@ extern "C" int bp_setup(const bp_model* m, bp_setup_arrays* o, double* uvel,
     in->maxiter_nonlinear = m->maxiter_nonlinear;
     in->pcg_maxiters = m->pcg_maxiters; in->pcg_ncheck = m->pcg_ncheck; in->pcg_tol = m->pcg_tol;
     in->precision = m->precision; in->inner_tol = m->inner_tol;
+    in->sliding = m->sliding ? &o->sliding : nullptr;
   }
   return BP_OK;
 }
@@ -293,8 +326,16 @@ extern "C" int bp_velo_higher_solve(bp_ctx* ctx, const bp_model* m, double* uvel
   std::vector<double> sigma(m->nz), su(nvert), sh(nvert), beta(nvert),
       fl((size_t)(m->nz - 1) * ncell), lu(n3), lv(n3);
   std::vector<int> ac(ncell), av(nvert), um(n3), vm(n3);
-  bp_setup_arrays o{sigma.data(), su.data(), sh.data(), beta.data(), fl.data(), ac.data(),
-                    av.data(), lu.data(), lv.data(), um.data(), vm.data()};
+  std::vector<double> fg(m->sliding ? nvert : 0), fbs(m->sliding ? nvert : 0);
+  bp_setup_arrays o{};
+  o.sigma = sigma.data(); o.stagusrf = su.data(); o.stagthck = sh.data();
+  o.beta_internal = beta.data(); o.flwafact = fl.data(); o.active_cell = ac.data();
+  o.active_vertex = av.data(); o.loadu = lu.data(); o.loadv = lv.data();
+  o.umask_dirichlet = um.data(); o.vmask_dirichlet = vm.data();
+  if (m->sliding) {
+    o.f_ground = fg.data();
+    o.flwa_basal_stag = fbs.data();
+  }
   bp_inputs in;
   const int rc = bp_setup(m, &o, uvel, vvel, &in);
   if (rc != BP_OK) return rc;

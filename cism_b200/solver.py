@@ -43,6 +43,21 @@ class BPError(RuntimeError):
         self.code = code
 
 
+class Sliding(C.Structure):
+    """bp_sliding: a velocity-dependent sliding law."""
+    _fields_ = [
+        ("law", C.c_int), ("f_ground", _dp), ("effecpress_stag", _dp), ("c_space_factor_stag", _dp),
+        ("flwa_basal_stag", _dp), ("yield_stress", _dp), ("topg", _dp), ("eus", C.c_double),
+        ("beta_grounded_min", C.c_double), ("beta_powerlaw_umax", C.c_double),
+        ("powerlaw_c", C.c_double), ("powerlaw_m", C.c_double), ("coulomb_c", C.c_double),
+        ("coulomb_bump_max_slope", C.c_double), ("coulomb_bump_wavelength", C.c_double),
+        ("friction_powerlaw_k", C.c_double), ("pseudo_plastic_q", C.c_double),
+        ("pseudo_plastic_u0", C.c_double), ("pseudo_plastic_phimin", C.c_double),
+        ("pseudo_plastic_phimax", C.c_double), ("pseudo_plastic_bedmin", C.c_double),
+        ("pseudo_plastic_bedmax", C.c_double),
+    ]
+
+
 class Inputs(C.Structure):
     _fields_ = [
         ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("nhalo", C.c_int),
@@ -54,7 +69,7 @@ class Inputs(C.Structure):
         ("which_assemble_beta", C.c_int), ("which_resid", C.c_int), ("pcg_variant", C.c_int),
         ("which_precond", C.c_int), ("maxiter_nonlinear", C.c_int), ("pcg_maxiters", C.c_int),
         ("pcg_ncheck", C.c_int), ("pcg_tol", C.c_double), ("precision", C.c_int),
-        ("inner_tol", C.c_double),
+        ("inner_tol", C.c_double), ("sliding", C.POINTER(Sliding)),
     ]
 
 
@@ -88,13 +103,18 @@ class Model(C.Structure):
         ("which_assemble_taud", C.c_int), ("which_ground", C.c_int),
         ("maxiter_nonlinear", C.c_int), ("pcg_maxiters", C.c_int), ("pcg_ncheck", C.c_int),
         ("pcg_tol", C.c_double), ("precision", C.c_int), ("inner_tol", C.c_double),
+        ("sliding", C.POINTER(Sliding)),
     ]
 
 
 class SetupArrays(C.Structure):
     _fields_ = [("sigma", _dp), ("stagusrf", _dp), ("stagthck", _dp), ("beta_internal", _dp),
                 ("flwafact", _dp), ("active_cell", _ip), ("active_vertex", _ip),
-                ("loadu", _dp), ("loadv", _dp), ("umask_dirichlet", _ip), ("vmask_dirichlet", _ip)]
+                ("loadu", _dp), ("loadv", _dp), ("umask_dirichlet", _ip), ("vmask_dirichlet", _ip),
+                ("f_ground", _dp), ("flwa_basal_stag", _dp), ("sliding", Sliding)]
+
+
+SETUP_ARRAYS = [k for k, _ in SetupArrays._fields_[:11]]
 
 
 _lib = None
@@ -186,7 +206,32 @@ def make_model_struct(m: configs.BPModel, precision: int = FP64, inner_tol: floa
         setattr(s, name, getattr(m, name))
     s.precision = precision
     s.inner_tol = inner_tol
+    s.sliding = C.cast(None, C.POINTER(Sliding))
+    if m.sliding is not None:
+        if m.which_babc != m.sliding.law:
+            raise ValueError("which_babc must equal sliding.law")
+        sl = sliding_struct(m.sliding, f)
+        keep.append(sl)
+        s.sliding = C.pointer(sl)
     return s, keep
+
+
+def sliding_struct(law: "configs.SlidingLaw", f) -> Sliding:
+    """bp_sliding of a model's sliding law (vertex fields through f; the
+    setup fills f_ground, flwa_basal_stag, topg and eus)."""
+    sl = Sliding()
+    sl.law = law.law
+    null = C.cast(None, _dp)
+    for name in ("effecpress_stag", "c_space_factor_stag", "yield_stress"):
+        a = getattr(law, name)
+        setattr(sl, name, f(a) if a is not None else null)
+    sl.f_ground = sl.flwa_basal_stag = sl.topg = null
+    for name in ("beta_powerlaw_umax", "powerlaw_c", "powerlaw_m", "coulomb_c",
+                 "coulomb_bump_max_slope", "coulomb_bump_wavelength", "friction_powerlaw_k",
+                 "pseudo_plastic_q", "pseudo_plastic_u0", "pseudo_plastic_phimin",
+                 "pseudo_plastic_phimax", "pseudo_plastic_bedmin", "pseudo_plastic_bedmax"):
+        setattr(sl, name, getattr(law, name))
+    return sl
 
 
 def prepare(m: configs.BPModel, uvel=None, vvel=None, precision: int = FP64,
@@ -202,7 +247,11 @@ def prepare(m: configs.BPModel, uvel=None, vvel=None, precision: int = FP64,
         "umask_dirichlet": np.zeros((ny - 1, nx - 1, nz), np.int32),
         "vmask_dirichlet": np.zeros((ny - 1, nx - 1, nz), np.int32),
     }
-    sa = SetupArrays(*[_p(arrays[k]) for k, _ in SetupArrays._fields_])
+    sa = SetupArrays(*[_p(arrays[k]) for k in SETUP_ARRAYS])
+    if m.sliding is not None:
+        arrays["f_ground"] = np.zeros((ny - 1, nx - 1))
+        arrays["flwa_basal_stag"] = np.zeros((ny - 1, nx - 1))
+        sa.f_ground, sa.flwa_basal_stag = _p(arrays["f_ground"]), _p(arrays["flwa_basal_stag"])
     ms, keep = make_model_struct(m, precision, inner_tol)
     u = np.zeros(m.vshape3) if uvel is None else np.array(uvel, np.float64, copy=True)
     v = np.zeros(m.vshape3) if vvel is None else np.array(vvel, np.float64, copy=True)

@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define BP_ABI_VERSION 1
+#define BP_ABI_VERSION 2
 
 typedef struct bp_ctx bp_ctx;
 
@@ -50,10 +50,51 @@ typedef enum {
 
 typedef enum { BP_FP64 = 0, BP_MIXED = 1 } bp_precision;
 
+/* Velocity-dependent sliding law: calcbeta
+ * (libglissade/glissade_basal_traction.F90:67-598) evaluated on the device
+ * at the start of every Picard iteration from the basal velocity
+ * (uvel, vvel)(nz,:,:), where the reference calls it
+ * (glissade_velo_higher.F90:2502-2517).  law is the which_ho_babc value
+ * (libglide/glide_types.F90:211-225):
+ *    2 yield stress (Picard)   beta = tau_y / |u|                  (:266-277)
+ *    3 pseudo-plastic          beta = tan(phi) N / (u0^q s^(1-q))  (:207-264)
+ *    9 power law               beta = C s^(1/m - 1)                (:357-363)
+ *   10 Coulomb friction (Schoof 2005)                               (:384-424)
+ *   11 Coulomb / power law (Schoof, MISMIP+)                        (:426-470)
+ *   12 Coulomb / power law (Tsai et al. 2015)                       (:472-509)
+ *   13 power law with effective pressure (p = 3, q = 1)            (:365-382)
+ * s = sqrt(u^2 + v^2 + 0.01^2) m/a (:181), capped at beta_powerlaw_umax
+ * when that is > 0 (:187-189); law 2 uses the uncapped sqrt(u^2 + v^2 + 0.01^2).  phi of law 3
+ * varies linearly with topg - eus between bedmin and bedmax; law 10 uses
+ * the basal-layer flow factor staggered over ice cells.  beta is then
+ * multiplied by f_ground, raised to beta_grounded_min where f_ground > 0
+ * (:538-566), and must be >= 0 (else BP_ERR_BAD_BETA, :570-582).  Vertex
+ * fields are (nx-1,ny-1); a field the law does not read may be NULL. */
+typedef struct {
+  int law;
+  const double *f_ground;            /* grounded fraction, :55-178 of glissade_grounding_line.F90 */
+  const double *effecpress_stag;     /* N, Pa (laws 3, 10-13) */
+  const double *c_space_factor_stag; /* law 10 (NULL: 1) */
+  const double *flwa_basal_stag;     /* Pa^-3 a^-1 (law 10) */
+  const double *yield_stress;        /* tau_y = mintauf * tau0, Pa (law 2) */
+  const double *topg;                /* (nx,ny) m, read at the vertex's (i,j) as the reference does (law 3) */
+  double eus;                        /* m (law 3) */
+  double beta_grounded_min;          /* Pa a/m */
+  double beta_powerlaw_umax;         /* m/a, 0 = no cap */
+  double powerlaw_c, powerlaw_m;
+  double coulomb_c, coulomb_bump_max_slope, coulomb_bump_wavelength;
+  double friction_powerlaw_k;        /* law 13 */
+  double pseudo_plastic_q, pseudo_plastic_u0;
+  double pseudo_plastic_phimin, pseudo_plastic_phimax;   /* degrees */
+  double pseudo_plastic_bedmin, pseudo_plastic_bedmax;   /* m */
+} bp_sliding;
+
 /* Boundary inputs of one solve: what the setup part of
  * glissade_velo_higher_solve (:987-2199) has computed when the Picard loop
- * starts (:2206).  beta_internal is the calcbeta result (velocity-independent
- * sliding laws: constant or external beta). */
+ * starts (:2206).  beta_internal is the calcbeta result for the
+ * velocity-independent laws (constant or external beta); with a
+ * velocity-dependent law (sliding != NULL) beta is recomputed on the device
+ * every Picard iteration and beta_internal is not read. */
 typedef struct {
   int nx, ny, nz, nhalo;        /* local grid incl. halo; nhalo must be 2 */
   int periodic;                 /* 1: periodic global BC (serial default), 0: outflow */
@@ -84,6 +125,7 @@ typedef struct {
   double inner_tol;             /* BP_MIXED: residual reduction of one refinement cycle
                                    (FP32-matrix Krylov solve between two FP64
                                    residuals; <= 0: 1e-4) */
+  const bp_sliding *sliding;    /* NULL: beta_internal, fixed over the Picard loop */
 } bp_inputs;
 
 typedef struct {
@@ -234,6 +276,10 @@ typedef struct {
   double pcg_tol;
   int precision;
   double inner_tol;
+  /* velocity-dependent sliding law (which_babc = sliding->law), or NULL;
+   * bp_setup computes its f_ground and flwa_basal_stag and takes topg, eus
+   * and beta_grounded_min from this struct's fields above */
+  const bp_sliding *sliding;
 } bp_model;
 
 /* Caller-allocated outputs of the setup (sizes as in bp_inputs). */
@@ -246,6 +292,10 @@ typedef struct {
   int *active_vertex;              /* (nx-1,ny-1) */
   double *loadu, *loadv;           /* (nz,nx-1,ny-1) */
   int *umask_dirichlet, *vmask_dirichlet; /* (nz,nx-1,ny-1) */
+  /* with a sliding law only: outputs f_ground and, for law 10,
+   * flwa_basal_stag ((nx-1,ny-1) each), and the law handed to the solve */
+  double *f_ground, *flwa_basal_stag;
+  bp_sliding sliding;
 } bp_setup_arrays;
 
 /* Masks, staggering, surface gradient, vertex geometry, flow factor, load

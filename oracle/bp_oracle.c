@@ -1209,22 +1209,112 @@ int orc_setup_solve(const orc_model *m, orc_setup *s, double *uvel,
   return ORC_OK;
 }
 
-/* calcbeta (glissade_basal_traction.F90:67-598), constant and external
- * laws: beta * f_ground (:540), grounded minimum (:560-566), validity
- * check (:567-579), halo update. */
-int orc_calcbeta(const orc_model *m, const orc_setup *s,
-                 double *beta_internal) {
-  const int nx = m->nx, ny = m->ny;
-  size_t nvx = (size_t)(nx - 1) * (ny - 1);
-  for (size_t v = 0; v < nvx; ++v) {
-    double b = 0.0;
-    if (m->which_babc == ORC_BABC_BETA_CONSTANT) b = m->beta_const;
-    else if (m->which_babc == ORC_BABC_BETA_EXTERNAL) b = m->beta_external[v];
-    b = b * s->f_ground[v];
-    if (s->f_ground[v] > 0.0 && b < m->beta_grounded_min) b = m->beta_grounded_min;
-    if (!(b >= 0.0)) return ORC_ERR_BAD_BETA;
-    beta_internal[v] = b;
+/* calcbeta (glissade_basal_traction.F90:67-598) as called at the start of
+ * each Picard iteration (glissade_velo_higher.F90:2502-2517) with ubas,
+ * vbas = uvel(nz,:,:), vvel(nz,:,:) (:2241-2242): the speed with its
+ * 0.01 m/a floor (:181) and optional cap (:187-189); the law; beta *
+ * f_ground (:540); the grounded minimum (:560-566); the validity check
+ * (:570-582); the halo update.  gn = 3 is an integer in the reference
+ * (glimmer_physcon.F90:75): N**gn is a product, 1/gn a real division. */
+int orc_calcbeta(const orc_model *m, const orc_setup *s, const double *uvel,
+                 const double *vvel, double *beta_internal) {
+  const int nx = m->nx, ny = m->ny, nz = m->nz;
+  const orc_basal_physics *bp = m->basal;
+  const double smallnum = 1.0e-2, pi = 3.14159265358979;
+  double *flwa_basal_stag = NULL;
+  if (m->which_babc == ORC_BABC_COULOMB_FRICTION) {
+    /* basal-layer flwa staggered over cells with thck > 0 (:393-398) */
+    int *imask = calloc((size_t)nx * ny, sizeof(int));
+    double *flwa_basal = calloc((size_t)nx * ny, sizeof(double));
+    flwa_basal_stag = calloc((size_t)(nx - 1) * (ny - 1), sizeof(double));
+    for (int j = 1; j <= ny; ++j)
+      for (int i = 1; i <= nx; ++i) {
+        imask[IC(i, j)] = m->thck[IC(i, j)] > 0.0 ? 1 : 0;
+        flwa_basal[IC(i, j)] = m->flwa[IFL(nz - 1, i, j)];
+      }
+    orc_stagger(nx, ny, flwa_basal, flwa_basal_stag, imask, 1);
+    free(imask);
+    free(flwa_basal);
   }
+  int status = ORC_OK;
+  for (int j = 1; j <= ny - 1; ++j)
+    for (int i = 1; i <= nx - 1; ++i) {
+      const size_t v = IV(i, j);
+      const double ub = uvel[IX(nz, i, j)], vb = vvel[IX(nz, i, j)];
+      double speed = sqrt(ub * ub + vb * vb + smallnum * smallnum);
+      double b = 0.0;
+      if (bp && bp->beta_powerlaw_umax > 0.0 && bp->beta_powerlaw_umax < speed)
+        speed = bp->beta_powerlaw_umax;
+      switch (m->which_babc) {
+        case ORC_BABC_BETA_CONSTANT:
+          b = m->beta_const;
+          break;
+        case ORC_BABC_BETA_EXTERNAL:
+          b = m->beta_external[v];
+          break;
+        case ORC_BABC_PSEUDO_PLASTIC: { /* :207-264 */
+          const double bed = m->topg[IC(i, j)] - m->eus;
+          double phi;
+          if (bed <= bp->pseudo_plastic_bedmin) phi = bp->pseudo_plastic_phimin;
+          else if (bed >= bp->pseudo_plastic_bedmax) phi = bp->pseudo_plastic_phimax;
+          else phi = bp->pseudo_plastic_phimin +
+                     ((bed - bp->pseudo_plastic_bedmin) /
+                      (bp->pseudo_plastic_bedmax - bp->pseudo_plastic_bedmin)) *
+                         (bp->pseudo_plastic_phimax - bp->pseudo_plastic_phimin);
+          const double tanphi = tan(phi * pi / 180.0);
+          const double tau_c = tanphi * bp->effecpress_stag[v];
+          b = tau_c / (pow(bp->pseudo_plastic_u0, bp->pseudo_plastic_q) *
+                       pow(speed, 1.0 - bp->pseudo_plastic_q));
+          break;
+        }
+        case ORC_BABC_YIELD_PICARD: /* :266-277 */
+          b = bp->mintauf_tau0[v] / sqrt(ub * ub + vb * vb + smallnum * smallnum);
+          break;
+        case ORC_BABC_POWERLAW: /* :357-363 */
+          b = bp->powerlaw_c * pow(speed, 1.0 / bp->powerlaw_m - 1.0);
+          break;
+        case ORC_BABC_POWERLAW_EFFECPRESS: { /* :365-382, p = 3, q = 1 */
+          const double p = 3.0, q = 1.0;
+          b = pow(bp->friction_powerlaw_k, -1.0 / p) * pow(bp->effecpress_stag[v], q / p) *
+              pow(speed, 1.0 / p - 1.0);
+          break;
+        }
+        case ORC_BABC_COULOMB_FRICTION: { /* :384-424 */
+          const double N = bp->effecpress_stag[v];
+          const double cs = bp->c_space_factor_stag ? bp->c_space_factor_stag[v] : 1.0;
+          const double big_lambda = (bp->coulomb_bump_wavelength / bp->coulomb_bump_max_slope) *
+                                    flwa_basal_stag[v];
+          b = bp->coulomb_c * cs * N * pow(speed, 1.0 / 3 - 1.0) *
+              pow(speed + N * N * N * big_lambda, -1.0 / 3);
+          if (b > 1.0e8) b = 1.0e8;
+          break;
+        }
+        case ORC_BABC_COULOMB_POWERLAW_SCHOOF: { /* :426-470 */
+          const double N = bp->effecpress_stag[v], mm = bp->powerlaw_m;
+          const double numerator = bp->powerlaw_c * bp->coulomb_c * N;
+          const double denominator = pow(pow(bp->powerlaw_c, mm) * speed + pow(bp->coulomb_c * N, mm),
+                                         1.0 / mm);
+          b = (numerator / denominator) * pow(speed, 1.0 / mm - 1.0);
+          if (b > 1.0e8) b = 1.0e8;
+          break;
+        }
+        case ORC_BABC_COULOMB_POWERLAW_TSAI: { /* :472-509 */
+          const double taub_powerlaw = bp->powerlaw_c * pow(speed, 1.0 / bp->powerlaw_m);
+          const double taub_coulomb = bp->coulomb_c * bp->effecpress_stag[v];
+          b = (taub_coulomb <= taub_powerlaw) ? taub_coulomb / speed : taub_powerlaw / speed;
+          break;
+        }
+        default:
+          b = 0.0;
+          break;
+      }
+      b = b * s->f_ground[v];
+      if (s->f_ground[v] > 0.0 && b < m->beta_grounded_min) b = m->beta_grounded_min;
+      if (!(b >= 0.0)) status = ORC_ERR_BAD_BETA;
+      beta_internal[v] = b;
+    }
+  free(flwa_basal_stag);
+  if (status != ORC_OK) return status;
   orc_halo_stag(nx, ny, 1, m->periodic, beta_internal);
   return ORC_OK;
 }
@@ -1309,7 +1399,7 @@ int orc_velo_higher_solve(const orc_model *m, double *uvel, double *vvel,
   int status = ORC_OK;
   while (outer_it_criterion >= outer_it_target && counter < m->maxiter_nonlinear) {
     counter = counter + 1;
-    st = orc_calcbeta(m, &s, beta_internal);
+    st = orc_calcbeta(m, &s, uvel, vvel, beta_internal);
     if (st != ORC_OK) { status = st; break; }
     memcpy(usav, uvel, n3 * 8);
     memcpy(vsav, vvel, n3 * 8);

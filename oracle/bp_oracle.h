@@ -49,6 +49,27 @@ enum {
   ORC_ERR_ARGS = 10
 };
 
+/* Velocity-dependent sliding laws of calcbeta (which_ho_babc values,
+ * libglide/glide_types.F90:211-225) and the basal_physics fields they read
+ * (libglide/glide_types.F90:1300-1370). */
+enum {
+  ORC_BABC_YIELD_PICARD = 2, ORC_BABC_PSEUDO_PLASTIC = 3, ORC_BABC_POWERLAW = 9,
+  ORC_BABC_COULOMB_FRICTION = 10, ORC_BABC_COULOMB_POWERLAW_SCHOOF = 11,
+  ORC_BABC_COULOMB_POWERLAW_TSAI = 12, ORC_BABC_POWERLAW_EFFECPRESS = 13
+};
+typedef struct {
+  const double *effecpress_stag;      /* (nx-1,ny-1) Pa */
+  const double *c_space_factor_stag;  /* (nx-1,ny-1) or NULL (= 1) */
+  const double *mintauf_tau0;         /* (nx-1,ny-1) mintauf * tau0, Pa */
+  double beta_powerlaw_umax;
+  double powerlaw_c, powerlaw_m;
+  double coulomb_c, coulomb_bump_max_slope, coulomb_bump_wavelength;
+  double friction_powerlaw_k;
+  double pseudo_plastic_q, pseudo_plastic_u0;
+  double pseudo_plastic_phimin, pseudo_plastic_phimax;
+  double pseudo_plastic_bedmin, pseudo_plastic_bedmax;
+} orc_basal_physics;
+
 /* Model state handed to the solve.  Sizes include the halo. */
 typedef struct {
   int nx, ny, nz, nhalo;       /* nhalo must be 2 */
@@ -68,6 +89,7 @@ typedef struct {
   int pcg_maxiters;            /* reference hard-codes 200 */
   double pcg_tol;              /* reference hard-codes 1e-8 */
   int pcg_ncheck;              /* reference hard-codes 5 */
+  const orc_basal_physics *basal;  /* velocity-dependent laws, else NULL */
 } orc_model;
 
 typedef struct {
@@ -155,9 +177,10 @@ void orc_setup_alloc(const orc_model *m, orc_setup *s);
 void orc_setup_free(orc_setup *s);
 int orc_setup_solve(const orc_model *m, orc_setup *s, double *uvel,
                     double *vvel);
-/* beta_internal from calcbeta (constant/external laws only). */
-int orc_calcbeta(const orc_model *m, const orc_setup *s,
-                 double *beta_internal);
+/* beta_internal from calcbeta at basal velocity (uvel, vvel)(nz,:,:):
+ * constant and external beta, and the velocity-dependent laws 2, 3, 9-13. */
+int orc_calcbeta(const orc_model *m, const orc_setup *s, const double *uvel,
+                 const double *vvel, double *beta_internal);
 /* One assembled system of Picard iteration "counter": A, b after basal BC,
  * Dirichlet BC, halo update and the symmetry repair. */
 int orc_assemble_system(const orc_model *m, const orc_setup *s,

@@ -20,6 +20,15 @@ _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
 
 
+class OrcBasalPhysics(C.Structure):
+    _fields_ = [("effecpress_stag", _dp), ("c_space_factor_stag", _dp), ("mintauf_tau0", _dp)] + \
+        [(n, C.c_double) for n in (
+            "beta_powerlaw_umax", "powerlaw_c", "powerlaw_m", "coulomb_c", "coulomb_bump_max_slope",
+            "coulomb_bump_wavelength", "friction_powerlaw_k", "pseudo_plastic_q", "pseudo_plastic_u0",
+            "pseudo_plastic_phimin", "pseudo_plastic_phimax", "pseudo_plastic_bedmin",
+            "pseudo_plastic_bedmax")]
+
+
 class OrcModel(C.Structure):
     _fields_ = [
         ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("nhalo", C.c_int),
@@ -35,7 +44,7 @@ class OrcModel(C.Structure):
         ("which_gradient_margin", C.c_int), ("which_assemble_beta", C.c_int),
         ("which_assemble_taud", C.c_int), ("which_ground", C.c_int),
         ("maxiter_nonlinear", C.c_int), ("pcg_maxiters", C.c_int), ("pcg_tol", C.c_double),
-        ("pcg_ncheck", C.c_int),
+        ("pcg_ncheck", C.c_int), ("basal", C.POINTER(OrcBasalPhysics)),
     ]
 
 
@@ -116,6 +125,19 @@ def make_model(m, keep: _Keep) -> OrcModel:
         setattr(om, f, getattr(m, f))
     if om.which_sparse not in (2, 3):
         om.which_sparse = 2
+    om.basal = C.cast(None, C.POINTER(OrcBasalPhysics))
+    if m.sliding is not None:
+        sl = m.sliding
+        bp = OrcBasalPhysics()
+        null = C.cast(None, _dp)
+        bp.effecpress_stag = keep.f64(sl.effecpress_stag) if sl.effecpress_stag is not None else null
+        bp.c_space_factor_stag = (keep.f64(sl.c_space_factor_stag) if sl.c_space_factor_stag is not None
+                                  else null)
+        bp.mintauf_tau0 = keep.f64(sl.yield_stress) if sl.yield_stress is not None else null
+        for n, _ in OrcBasalPhysics._fields_[3:]:
+            setattr(bp, n, getattr(sl, n))
+        keep.items.append(bp)
+        om.basal = C.pointer(bp)
     return om
 
 
@@ -159,7 +181,7 @@ def setup(m, uvel=None, vvel=None):
     if rc != 0:
         raise RuntimeError(f"orc_setup_solve failed: {rc}")
     beta = np.zeros((ny - 1, nx - 1))
-    rc = lib().orc_calcbeta(C.byref(om), C.byref(s), _p(beta))
+    rc = lib().orc_calcbeta(C.byref(om), C.byref(s), _p(u), _p(v), _p(beta))
     if rc != 0:
         raise RuntimeError(f"orc_calcbeta failed: {rc}")
     arrs["beta_internal"] = beta

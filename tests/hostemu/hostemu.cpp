@@ -197,3 +197,26 @@ extern "C" int emu_sia_apply(int nx, int ny, int nz, int periodic, const int* ac
   scatter_vector(E.p, 0, z.data(), zu, zv);
   return 0;
 }
+
+// Sliding-law beta of every column from the basal velocity (the per-column
+// body of k_slide_beta), written to beta (nx-1,ny-1) at each column's
+// vertex; other entries are left as they are.  10 if the plan rejects the
+// inputs.
+extern "C" int emu_slide_beta(const bp_inputs* in, const double* uvel, const double* vvel,
+                              double* beta) {
+  Emu E;
+  std::string err;
+  if (!build_plan(in, 1, &E.p, &err)) return 10;
+  E.bind();
+  gather_velocity(E.p, 0, uvel, vvel, E.x.data());
+  const int nz = E.p.nz, NC = E.p.ncols, nx = in->nx;
+  const SlideParams& sp = E.p.inst[0].slide;
+  for (int c = 0; c < NC; ++c) {
+    const double2 ub = E.x[(size_t)c * nz + nz - 1];
+    const double b = slide_beta(sp, E.p.col_slide[c], E.p.col_slide[(size_t)NC + c],
+                                E.p.col_slide[2 * (size_t)NC + c], ub.x, ub.y);
+    const int i = E.p.col_ij[c], j = E.p.col_ij[NC + c];
+    beta[(size_t)(j - 1) * (nx - 1) + (i - 1)] = b;
+  }
+  return 0;
+}
