@@ -262,10 +262,23 @@ def test_batch_mixes_sliding_and_fixed_beta(ctx):
         assert rel_l2([u, v], [ui, vi]) < 1e-12
 
 
-@pytest.mark.gpu
-def test_negative_beta_is_reported(ctx):
-    m = _model(9, "slab", powerlaw_c=-1.0e3)
-    _, _, _, st = ctx.velo_higher_solve(m)
-    _, _, _, _, sto = oracle.velo_higher_solve(m)
+def _nan_beta_model():
+    """A NaN beta (a negative effective pressure under the cube root of the
+    effective-pressure power law); a negative beta cannot reach the check
+    where ice is grounded, since the grounded minimum raises it first
+    (glissade_basal_traction.F90:560-566)."""
+    m = _model(13, "slab")
+    m.sliding.effecpress_stag = -np.abs(m.sliding.effecpress_stag)
+    return m
+
+
+def test_oracle_reports_nan_beta():
+    _, _, _, _, sto = oracle.velo_higher_solve(_nan_beta_model())
     assert sto["status"] == 9
-    assert st["status"] == 9
+
+
+@pytest.mark.gpu
+def test_nan_beta_from_sliding_law_is_reported(ctx):
+    with pytest.raises(solver.BPError) as e:
+        ctx.velo_higher_solve(_nan_beta_model())
+    assert e.value.code == 9
