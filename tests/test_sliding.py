@@ -252,7 +252,10 @@ def test_sliding_law_with_standard_basal_assembly(ctx):
 
 @pytest.mark.gpu
 def test_batch_mixes_sliding_and_fixed_beta(ctx):
-    ms = [_model(11, "slab"), configs.slab(n=20), _model(9, "dome")]
+    """A batch (one nz for all instances) of two laws and a fixed beta
+    equals the single solves."""
+    dome11 = configs.with_sliding(configs.dome(n=21, radius=15e3, nz=11).copy(eus=0.0), 9, seed=9)
+    ms = [_model(11, "slab"), configs.slab(n=20), dome11]
     ms = [m.copy(pcg_maxiters=2000) for m in ms]
     preps = [solver.prepare(m) for m in ms]
     us, vs, _, sts = ctx.batch_solve([p[0] for p in preps], [p[1] for p in preps], [p[2] for p in preps])
