@@ -71,13 +71,13 @@ BP_HD constexpr int elem_m(int nr, int nc) {
 // ---------------------------------------------------------------------
 // Pass 1 of assembly: one quadrature point of one element.
 // get_basis_function_derivatives_3d (:6360-6579) and
-// compute_effective_viscosity (:7199-7378).  Writes f = efvs*w*detJ/vol0
-// and J^-1 (row-major) to out[0..9]; returns false for a singular Jacobian.
+// compute_effective_viscosity (:7199-7378), in three pieces that the
+// post-solve stress diagnostic shares.
 // ---------------------------------------------------------------------
-BP_HD bool qp_compute(const RefTables& T, int p, const double* x,
-                      const double* y, const double* z, const double* u,
-                      const double* w, int which_efvs, double efvs_constant,
-                      double flwafact, double* out, double* efvs_qp) {
+// J^-1 (row-major, Ji[3*row+col]) of the element's map at quadrature point
+// p; false for a singular Jacobian.
+BP_HD bool qp_jacobian_inverse(const RefTables& T, int p, const double* x, const double* y,
+                               const double* z, double* Ji, double* det_out) {
   double J00 = 0, J01 = 0, J02 = 0, J10 = 0, J11 = 0, J12 = 0, J20 = 0, J21 = 0, J22 = 0;
 #pragma unroll
   for (int n = 0; n < 8; ++n) {
@@ -96,51 +96,77 @@ BP_HD bool qp_compute(const RefTables& T, int p, const double* x,
   const double c21 = -(J00 * J12 - J02 * J10);
   const double c22 = J00 * J11 - J01 * J10;
   const double det = J00 * c00 + J01 * c01 + J02 * c02;
+  *det_out = det;
   if (!(fabs(det) > 0.0)) return false;
   // Jinv(row,col) = cofactor(col,row)/detJ
-  const double i00 = c00 / det, i01 = c10 / det, i02 = c20 / det;
-  const double i10 = c01 / det, i11 = c11 / det, i12 = c21 / det;
-  const double i20 = c02 / det, i21 = c12 / det, i22 = c22 / det;
-  double efvs;
-  if (which_efvs == 0) {
-    efvs = efvs_constant;
-  } else if (which_efvs == 1) {
-    const double scyr = 31536000.0;
-    const double effstrain = (500.0 / scyr) / 200.0e3 * scyr;
-    efvs = flwafact * pow(effstrain, (1.0 - 3.0) / 3.0);
-  } else {
-    double ux = 0, uy = 0, uz = 0, vx = 0, vy = 0, vz = 0;
-#pragma unroll
-    for (int n = 0; n < 8; ++n) {
-      const double a = T.dxr[p][n], b = T.dyr[p][n], c = T.dzr[p][n];
-      const double dx = BP_FMA(i02, c, BP_FMA(i01, b, i00 * a));
-      const double dy = BP_FMA(i12, c, BP_FMA(i11, b, i10 * a));
-      const double dz = BP_FMA(i22, c, BP_FMA(i21, b, i20 * a));
-      ux += dx * u[n]; uy += dy * u[n]; uz += dz * u[n];
-      vx += dx * w[n]; vy += dy * w[n]; vz += dz * w[n];
-    }
-    const double smin = 1.0e-8;
-    const double sq = smin * smin + (ux * ux + vy * vy + ux * vy + 0.25 * ((vx + uy) * (vx + uy))) +
-                      0.25 * (uz * uz + vz * vz);
-    const double p2 = ((1.0 - 3.0) / 3.0) / 2.0;
-    efvs = flwafact * pow(sq, p2);
-  }
-  *efvs_qp = efvs;
-  out[0] = efvs * 1.0 * det / kVol0;
-  out[1] = i00; out[2] = i01; out[3] = i02;
-  out[4] = i10; out[5] = i11; out[6] = i12;
-  out[7] = i20; out[8] = i21; out[9] = i22;
+  Ji[0] = c00 / det; Ji[1] = c10 / det; Ji[2] = c20 / det;
+  Ji[3] = c01 / det; Ji[4] = c11 / det; Ji[5] = c21 / det;
+  Ji[6] = c02 / det; Ji[7] = c12 / det; Ji[8] = c22 / det;
   return true;
 }
 
-// Gather the 8 nodes of element e (cell, layer kk) and run qp_compute.
-BP_HD bool qp_element_point(const DevView& v, const RefTables& T, int e, int p,
-                            double* out, double* efvs_qp) {
+// Velocity gradient at quadrature point p: g = (du/dx, du/dy, du/dz,
+// dv/dx, dv/dy, dv/dz), the derivatives of the basis functions formed from
+// J^-1 in one fixed fma pattern.
+BP_HD void qp_velocity_gradient(const RefTables& T, int p, const double* Ji, const double* u,
+                                const double* w, double* g) {
+  double ux = 0, uy = 0, uz = 0, vx = 0, vy = 0, vz = 0;
+#pragma unroll
+  for (int n = 0; n < 8; ++n) {
+    const double a = T.dxr[p][n], b = T.dyr[p][n], c = T.dzr[p][n];
+    const double dx = BP_FMA(Ji[2], c, BP_FMA(Ji[1], b, Ji[0] * a));
+    const double dy = BP_FMA(Ji[5], c, BP_FMA(Ji[4], b, Ji[3] * a));
+    const double dz = BP_FMA(Ji[8], c, BP_FMA(Ji[7], b, Ji[6] * a));
+    ux += dx * u[n]; uy += dy * u[n]; uz += dz * u[n];
+    vx += dx * w[n]; vy += dy * w[n]; vz += dz * w[n];
+  }
+  g[0] = ux; g[1] = uy; g[2] = uz; g[3] = vx; g[4] = vy; g[5] = vz;
+}
+
+// compute_effective_viscosity, 3-D higher-order branch: constant, from the
+// flow factor at a fixed strain rate, or Glen's law (n = 3) with the
+// 1e-8 /a strain-rate floor; g is read only by the last.
+BP_HD double qp_efvs(int which_efvs, double efvs_constant, double flwafact, const double* g) {
+  if (which_efvs == 0) return efvs_constant;
+  if (which_efvs == 1) {
+    const double scyr = 31536000.0;
+    const double effstrain = (500.0 / scyr) / 200.0e3 * scyr;
+    return flwafact * pow(effstrain, (1.0 - 3.0) / 3.0);
+  }
+  const double ux = g[0], uy = g[1], uz = g[2], vx = g[3], vy = g[4], vz = g[5];
+  const double smin = 1.0e-8;
+  const double sq = smin * smin + (ux * ux + vy * vy + ux * vy + 0.25 * ((vx + uy) * (vx + uy))) +
+                    0.25 * (uz * uz + vz * vz);
+  const double p2 = ((1.0 - 3.0) / 3.0) / 2.0;
+  return flwafact * pow(sq, p2);
+}
+
+// Writes f = efvs*w*detJ/vol0 and J^-1 (row-major) to out[0..9]; returns
+// false for a singular Jacobian.
+BP_HD bool qp_compute(const RefTables& T, int p, const double* x,
+                      const double* y, const double* z, const double* u,
+                      const double* w, int which_efvs, double efvs_constant,
+                      double flwafact, double* out, double* efvs_qp) {
+  double Ji[9], det;
+  if (!qp_jacobian_inverse(T, p, x, y, z, Ji, &det)) return false;
+  double g[6] = {0, 0, 0, 0, 0, 0};
+  if (which_efvs == 2) qp_velocity_gradient(T, p, Ji, u, w, g);
+  const double efvs = qp_efvs(which_efvs, efvs_constant, flwafact, g);
+  *efvs_qp = efvs;
+  out[0] = efvs * 1.0 * det / kVol0;
+#pragma unroll
+  for (int i = 0; i < 9; ++i) out[1 + i] = Ji[i];
+  return true;
+}
+
+// The 8 nodes of element e (cell, layer kk): coordinates and velocity
+// (zero at a corner without a column); returns the element's instance.
+BP_HD const InstParams& elem_gather(const DevView& v, int e, double* x, double* y, double* z,
+                                    double* u, double* w) {
   const int nz = v.nz, nl = nz - 1;
   const int cell = e / nl, kk = e - cell * nl;
   const InstParams& ip = v.inst[v.cell_inst[cell]];
   const int ic = v.cell_ij[cell], jc = v.cell_ij[v.ncells + cell];
-  double x[8], y[8], z[8], u[8], w[8];
 #pragma unroll
   for (int n = 0; n < 8; ++n) {
     const int corner = n & 3;              // SW, SE, NE, NW
@@ -160,8 +186,85 @@ BP_HD bool qp_element_point(const DevView& v, const RefTables& T, int e, int p,
       u[n] = 0.0; w[n] = 0.0;
     }
   }
+  return ip;
+}
+
+// Gather the 8 nodes of element e and run qp_compute.
+BP_HD bool qp_element_point(const DevView& v, const RefTables& T, int e, int p,
+                            double* out, double* efvs_qp) {
+  double x[8], y[8], z[8], u[8], w[8];
+  const InstParams& ip = elem_gather(v, e, x, y, z, u, w);
   return qp_compute(T, p, x, y, z, u, w, ip.which_efvs, ip.efvs_constant,
                     v.flwafact[e], out, efvs_qp);
+}
+
+// compute_internal_stress (:6968-7195), 3-D higher-order branch, for
+// element e at the current velocity: the velocity gradient and the
+// effective viscosity at the 8 quadrature points (assembly's arithmetic),
+// tau_xz = efvs du/dz, tau_yz = efvs dv/dz, tau_xx = 2 efvs du/dx,
+// tau_yy = 2 efvs dv/dy, tau_xy = efvs (dv/dx + du/dy), each averaged, and
+// tau_eff from the averages.  tau = {xz, yz, xx, yy, xy, eff}; false for a
+// singular Jacobian.
+BP_HD bool stress_element(const DevView& v, const RefTables& T, int e, double* tau) {
+  double x[8], y[8], z[8], u[8], w[8];
+  const InstParams& ip = elem_gather(v, e, x, y, z, u, w);
+  double txz = 0.0, tyz = 0.0, txx = 0.0, tyy = 0.0, txy = 0.0;
+  for (int p = 0; p < 8; ++p) {
+    double Ji[9], det, g[6];
+    if (!qp_jacobian_inverse(T, p, x, y, z, Ji, &det)) return false;
+    qp_velocity_gradient(T, p, Ji, u, w, g);
+    const double efvs = qp_efvs(ip.which_efvs, ip.efvs_constant, v.flwafact[e], g);
+    txz = txz + efvs * g[2];
+    tyz = tyz + efvs * g[5];
+    txx = txx + 2.0 * efvs * g[0];
+    tyy = tyy + 2.0 * efvs * g[4];
+    txy = txy + efvs * (g[3] + g[1]);
+  }
+  txz = txz / 8; tyz = tyz / 8; txx = txx / 8; tyy = tyy / 8; txy = txy / 8;
+  tau[0] = txz; tau[1] = tyz; tau[2] = txx; tau[3] = tyy; tau[4] = txy;
+  tau[5] = sqrt(txx * txx + tyy * tyy + txx * tyy + txy * txy + txz * txz + tyz * tyz);
+  return true;
+}
+
+// compute_basal_friction_heatflx (:6755-6964): the frictional heat flux
+// beta |u_b|^2 / scyr (W/m^2).  Finite-element method (which = 0), one
+// active cell: the corner values (bed velocity, zero at a corner without a
+// column; corner beta) interpolated to the 4 face quadrature points, the
+// weighted mean of beta |u|^2 (:6853-6887).  Local method (which = 1), one
+// column: beta |u_b|^2 at the vertex (:6900-6909), unstaggered to the cells
+// on the way out.
+BP_HD double bfric_cell(const DevView& v, const RefTables& T, int cell) {
+  const int nz = v.nz;
+  double u[4], w[4], b[4];
+  for (int q = 0; q < 4; ++q) {  // SW, SE, NE, NW = the reference's 2-D node order
+    const int col = v.cell_cols[q * v.ncells + cell];
+    if (col >= 0) {
+      const double2 xb = v.x[(size_t)col * nz + nz - 1];
+      u[q] = xb.x;
+      w[q] = xb.y;
+    } else {
+      u[q] = 0.0;
+      w[q] = 0.0;
+    }
+    b[q] = v.cell_beta[q * v.ncells + cell];
+  }
+  double f = 0.0, sum_w = 0.0;
+  for (int p = 0; p < 4; ++p) {
+    double uq = 0.0, vq = 0.0, bq = 0.0;
+    for (int n = 0; n < 4; ++n) {
+      uq = uq + T.phi2[p][n] * u[n];
+      vq = vq + T.phi2[p][n] * w[n];
+      bq = bq + T.phi2[p][n] * b[n];
+    }
+    f = f + 1.0 * bq * (uq * uq + vq * vq);  // wqp_2d = 1
+    sum_w = sum_w + 1.0;
+  }
+  return f / (sum_w * 31536000.0);
+}
+
+BP_HD double bfric_vertex(const DevView& v, int col) {
+  const double2 xb = v.x[(size_t)col * v.nz + v.nz - 1];
+  return v.col_beta[col] * (xb.x * xb.x + xb.y * xb.y) / 31536000.0;
 }
 
 // ---------------------------------------------------------------------

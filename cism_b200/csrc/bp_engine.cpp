@@ -767,6 +767,44 @@ int bp_problem_get(bp_problem* P, double* const* uvel, double* const* vvel, doub
   GUARD_END
 }
 
+int bp_problem_diagnostics(bp_problem* P, int which_bfric, double* const* tau_xz,
+                           double* const* tau_yz, double* const* tau_xx,
+                           double* const* tau_yy, double* const* tau_xy,
+                           double* const* tau_eff, double* const* bfricflx) {
+  if (!P || (which_bfric != 0 && which_bfric != 1)) return BP_ERR_ARGS;
+  GUARD_BEGIN(P->c)
+  const HostPlan& p = P->plan;
+  bp_ctx* c = P->c;
+  double* const* outs[6] = {tau_xz, tau_yz, tau_xx, tau_yy, tau_xy, tau_eff};
+  bool want_tau = false;
+  for (auto o : outs) want_tau = want_tau || o;
+  if (!p.ncells) return BP_ERR_ARGS;  // matrix-level problems have no elements
+  const size_t ne = (size_t)p.nelem, nb = (size_t)std::max(p.ncells, p.ncols);
+  double* d = P->arena->get<double>(c->stream, "diagnostics", (want_tau ? 6 * ne : 0) + nb);
+  double* d_tau = want_tau ? d : nullptr;
+  double* d_bf = bfricflx ? d + (want_tau ? 6 * ne : 0) : nullptr;
+  launch_diagnostics(P->v, which_bfric, d_tau, d_bf, c->stream);
+  std::vector<double> tau(d_tau ? 6 * ne : 0), bf(d_bf ? nb : 0);
+  if (d_tau) CK(cudaMemcpyAsync(tau.data(), d_tau, sizeof(double) * tau.size(), cudaMemcpyDeviceToHost, c->stream));
+  if (d_bf) CK(cudaMemcpyAsync(bf.data(), d_bf, sizeof(double) * bf.size(), cudaMemcpyDeviceToHost, c->stream));
+  std::vector<InstState> st(p.ninst);
+  CK(cudaMemcpyAsync(st.data(), P->v.st, sizeof(InstState) * p.ninst, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaGetLastError());
+  int rc = BP_OK;
+  for (int b = 0; b < p.ninst; ++b) {
+    if (st[b].status == BP_ERR_SINGULAR_JAC) rc = BP_ERR_SINGULAR_JAC;
+    if (d_tau) {
+      double* o[6];
+      for (int f = 0; f < 6; ++f) o[f] = outs[f] ? outs[f][b] : nullptr;
+      scatter_elements(p, b, tau.data(), 6, o);
+    }
+    if (d_bf) scatter_bfric(p, b, which_bfric, bf.data(), bfricflx[b]);
+  }
+  return rc;
+  GUARD_END
+}
+
 int bp_problem_destroy(bp_problem* P) {
   if (!P) return BP_OK;
   cudaSetDevice(P->c->device);

@@ -815,6 +815,30 @@ __global__ void __launch_bounds__(kTile) k_make_a32(DevView v) {
   }
 }
 
+// Post-solve diagnostics (glissade_velo_higher.F90:3847-3872) at the
+// current velocity: the element stresses of compute_internal_stress into
+// out[6][nelem] (a singular Jacobian marks the instance, as assembly pass 1
+// does) and the basal frictional heat flux of
+// compute_basal_friction_heatflx into bf (per active cell for the
+// finite-element method, per column for the local one).
+__global__ void __launch_bounds__(256) k_internal_stress(DevView v, double* out) {
+  const size_t ne = (size_t)v.nelem;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < v.nelem; e += gridDim.x * blockDim.x) {
+    double tau[6];
+    if (!stress_element(v, c_T, e, tau)) {
+      atomicExch(&v.st[v.cell_inst[e / (v.nz - 1)]].status, BP_ERR_SINGULAR_JAC);
+      for (int q = 0; q < 6; ++q) tau[q] = 0.0;
+    }
+    for (int q = 0; q < 6; ++q) out[(size_t)q * ne + e] = tau[q];
+  }
+}
+
+__global__ void __launch_bounds__(256) k_bfric(DevView v, int which, double* bf) {
+  const int n = which == 0 ? v.ncells : v.ncols;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    bf[i] = which == 0 ? bfric_cell(v, c_T, i) : bfric_vertex(v, i);
+}
+
 // Plain y = A x for bp_matvec.
 __global__ void __launch_bounds__(kTile) k_matvec_plain(DevView v, const double2* x, double2* y) {
   for (int t = blockIdx.x; t < v.ntiles; t += gridDim.x) {
@@ -1023,6 +1047,11 @@ void launch_dinv(const DevView& v, int precond, cudaStream_t s) {
   k_dinv<<<tile_grid(v), kTile, 0, s>>>(v, precond);
 }
 void launch_bb(const DevView& v, cudaStream_t s) { k_bb<<<tile_grid(v), kTile, 0, s>>>(v); }
+void launch_diagnostics(const DevView& v, int which_bfric, double* tau, double* bf, cudaStream_t s) {
+  if (tau && v.nelem > 0) k_internal_stress<<<(v.nelem + 255) / 256, 256, 0, s>>>(v, tau);
+  const int n = which_bfric == 0 ? v.ncells : v.ncols;
+  if (bf && n > 0) k_bfric<<<(n + 255) / 256, 256, 0, s>>>(v, which_bfric, bf);
+}
 int launch_tune_mv(int store, int minb, int grid, const DevView& v, cudaStream_t s) {
   const int g = grid > 0 ? grid : tile_grid(v);
 #define TUNE(ST, MB) k_tune_mv<ST, MB><<<g, kTile, 0, s>>>(v)

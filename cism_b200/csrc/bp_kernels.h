@@ -35,6 +35,9 @@ void launch_make_a32(const DevView& v, cudaStream_t s);
 void launch_matvec_plain(const DevView& v, const double2* x, double2* y, cudaStream_t s);
 void launch_dinv(const DevView& v, int precond, cudaStream_t s);
 void launch_bb(const DevView& v, cudaStream_t s);
+// element stresses into tau[6][nelem] and the basal frictional heat flux
+// into bf ([ncells] for which_bfric 0, [ncols] for 1); either may be null
+void launch_diagnostics(const DevView& v, int which_bfric, double* tau, double* bf, cudaStream_t s);
 // store: 0 full FP64, 1 symmetric FP64, 2 symmetric FP32; minb: 0, 6 or 8
 // resident CTAs per SM; grid: CTAs (0 = one per tile).  -1 if unavailable.
 int launch_tune_mv(int store, int minb, int grid, const DevView& v, cudaStream_t s);

@@ -518,6 +518,61 @@ void gather_matrix_sym(const HostPlan& p, const double* Auu, const double* Auv,
   }
 }
 
+void halo_cells(int nx, int ny, int periodic, double* a) {
+  auto at = [&](int i, int j) -> double& { return a[cel(i, j, nx)]; };
+  if (!periodic) {
+    for (int j = 3; j <= ny - 2; ++j) at(1, j) = at(2, j) = at(nx - 1, j) = at(nx, j) = 0.0;
+    for (int i = 1; i <= nx; ++i) at(i, 1) = at(i, 2) = at(i, ny - 1) = at(i, ny) = 0.0;
+    return;
+  }
+  for (int j = 3; j <= ny - 2; ++j) {
+    const double e1 = at(nx - 3, j), e2 = at(nx - 2, j), w1 = at(3, j), w2 = at(4, j);
+    at(1, j) = e1; at(2, j) = e2; at(nx - 1, j) = w1; at(nx, j) = w2;
+  }
+  for (int i = 1; i <= nx; ++i) {
+    const double n1 = at(i, ny - 3), n2 = at(i, ny - 2), s1 = at(i, 3), s2 = at(i, 4);
+    at(i, 1) = n1; at(i, 2) = n2; at(i, ny - 1) = s1; at(i, ny) = s2;
+  }
+}
+
+void scatter_elements(const HostPlan& p, int b, const double* vals, int nv,
+                      double* const* out) {
+  const InstParams& ip = p.inst[b];
+  const int nx = p.nx[b], ny = p.ny[b], nz = p.nz, NCELL = p.ncells;
+  const size_t ne = (size_t)p.nelem;
+  for (int f = 0; f < nv; ++f) {
+    if (!out[f]) continue;
+    std::memset(out[f], 0, sizeof(double) * (size_t)(nz - 1) * nx * ny);
+    for (int g = ip.cell_begin; g < ip.cell_end; ++g) {
+      const int ic = p.cell_ij[g], jc = p.cell_ij[NCELL + g];
+      for (int k = 0; k < nz - 1; ++k)
+        out[f][cel(ic, jc, nx) * (nz - 1) + k] = vals[(size_t)f * ne + (size_t)g * (nz - 1) + k];
+    }
+  }
+}
+
+void scatter_bfric(const HostPlan& p, int b, int which, const double* vals,
+                   double* bfricflx) {
+  const InstParams& ip = p.inst[b];
+  const int nx = p.nx[b], ny = p.ny[b], NCELL = p.ncells, NC = p.ncols;
+  std::memset(bfricflx, 0, sizeof(double) * (size_t)nx * ny);
+  if (which == 0) {
+    for (int g = ip.cell_begin; g < ip.cell_end; ++g)
+      bfricflx[cel(p.cell_ij[g], p.cell_ij[NCELL + g], nx)] = vals[g];
+  } else {
+    // vertex values at the owned active vertices, halo vertices from their
+    // images; cells next to the halo are overwritten by the halo update
+    std::vector<double> st((size_t)(nx - 1) * (ny - 1), 0.0);
+    for (int g = ip.col_begin; g < ip.col_end; ++g) st[vtx(p.col_ij[g], p.col_ij[NC + g], nx)] = vals[g];
+    halo_stag(nx, ny, 1, p.periodic[b], st.data());
+    for (int j = 2; j <= ny - 1; ++j)
+      for (int i = 2; i <= nx - 1; ++i)
+        bfricflx[cel(i, j, nx)] = (st[vtx(i, j, nx)] + st[vtx(i - 1, j, nx)] + st[vtx(i, j - 1, nx)] +
+                                   st[vtx(i - 1, j - 1, nx)]) / 4.0;
+  }
+  halo_cells(nx, ny, p.periodic[b], bfricflx);
+}
+
 void halo_stag(int nx, int ny, int nlead, int periodic, double* a) {
   const int V = nx - 1, W = ny - 1;
   auto at = [&](int l, int i, int j) -> double& {

@@ -80,5 +80,19 @@ void scatter_vector(const HostPlan& p, int b, const double2* v, double* vu,
 
 // staggered_parallel_halo for an (nlead, nx-1, ny-1) field.
 void halo_stag(int nx, int ny, int nlead, int periodic, double* a);
+// parallel_halo for an (nx, ny) cell field (parallel_slap.F90:1790-1860).
+void halo_cells(int nx, int ny, int periodic, double* a);
+
+// Post-solve diagnostics of instance b to the reference layout: nv element
+// fields vals[v][nelem] -> out[v] (nz-1,nx,ny), zero outside active cells
+// (a null out[v] is skipped); the basal frictional heat flux (nx,ny) from
+// active-cell values (which = 0) or column values unstaggered to the cells
+// with glissade_unstagger margin 0 (which = 1,
+// glissade_grid_operators.F90:152-231), then the cell halo update
+// (glissade_velo_higher.F90:6960).
+void scatter_elements(const HostPlan& p, int b, const double* vals, int nv,
+                      double* const* out);
+void scatter_bfric(const HostPlan& p, int b, int which, const double* vals,
+                   double* bfricflx);
 
 }  // namespace bp

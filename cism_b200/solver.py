@@ -151,6 +151,7 @@ def lib():
         L.bp_problem_tune_mv.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
                                          C.POINTER(C.c_float)]
         L.bp_problem_mv_nodes.argtypes = [C.c_void_p, _dp, _dp, _ip, _ip]
+        L.bp_problem_diagnostics.argtypes = [C.c_void_p, C.c_int] + [C.POINTER(_dp)] * 7
         L.bp_timer_start.argtypes = [C.c_void_p]
         L.bp_timer_stop.argtypes = [C.c_void_p, C.POINTER(C.c_float)]
         _lib = L
@@ -417,6 +418,17 @@ class Problem:
                                   (_dp * self.n)(*[_p(a) for a in es]) if es else C.cast(None, C.POINTER(_dp)))
         self.ctx._check(rc, allow=(0,))
         return us, vs, es
+
+    def diagnostics(self, which_bfric: int = 1):
+        """Post-solve diagnostics at the last run's solution, per instance:
+        the six element stresses (ny, nx, nz-1) and bfricflx (ny, nx)."""
+        names = ("tau_xz", "tau_yz", "tau_xx", "tau_yy", "tau_xy", "tau_eff")
+        out = [{k: np.zeros((p.model.ny, p.model.nx, p.model.nz - 1)) for k in names} |
+               {"bfricflx": np.zeros((p.model.ny, p.model.nx))} for p in self.preps]
+        arrs = [(_dp * self.n)(*[_p(o[k]) for o in out]) for k in names + ("bfricflx",)]
+        rc = lib().bp_problem_diagnostics(self.h, which_bfric, *arrs)
+        self.ctx._check(rc, allow=(0,))
+        return out
 
     def tune_mv(self, store: int, minb: int = 0, grid: int = 0, reps: int = 50):
         """Mean ms of a plain y = A x launch (store 0 full, 1 sym FP64, 2 sym FP32)."""

@@ -516,6 +516,128 @@ int orc_assemble_3d(int nx, int ny, int nz, int nhalo, const double *sigma,
   return ORC_OK;
 }
 
+/* compute_internal_stress (glissade_velo_higher.F90:6968-7195), 3-D
+ * higher-order branch: at every element of an active cell, the strain
+ * rates and the effective viscosity at the 8 quadrature points of the given
+ * velocity, averaged; tau_eff from the averaged components. */
+int orc_internal_stress(int nx, int ny, int nz, int nhalo, const double *sigma,
+                        const int *active_cell, const double *xVertex,
+                        const double *yVertex, const double *stagusrf,
+                        const double *stagthck, const double *flwafact,
+                        int whichefvs, double efvs_constant, const double *uvel,
+                        const double *vvel, double *tau_xz, double *tau_yz,
+                        double *tau_xx, double *tau_yy, double *tau_xy,
+                        double *tau_eff) {
+  init_tables();
+  const size_t ne = (size_t)(nz - 1) * nx * ny;
+  memset(tau_xz, 0, ne * sizeof(double));
+  memset(tau_yz, 0, ne * sizeof(double));
+  memset(tau_xx, 0, ne * sizeof(double));
+  memset(tau_yy, 0, ne * sizeof(double));
+  memset(tau_xy, 0, ne * sizeof(double));
+  memset(tau_eff, 0, ne * sizeof(double));
+  for (int j = nhalo + 1; j <= ny - nhalo + 1; ++j)
+    for (int i = nhalo + 1; i <= nx - nhalo + 1; ++i) {
+      if (!active_cell[IC(i, j)]) continue;
+      for (int k = 1; k <= nz - 1; ++k) {
+        double x[8], y[8], z[8], u[8], v[8];
+        for (int n = 0; n < 8; ++n) {
+          int in = i + ishift[6][n], jn = j + jshift[6][n], kn = k + kshift[6][n];
+          x[n] = xVertex[IV(in, jn)];
+          y[n] = yVertex[IV(in, jn)];
+          z[n] = stagusrf[IV(in, jn)] - sigma[kn - 1] * stagthck[IV(in, jn)];
+          u[n] = uvel[IX(kn, in, jn)];
+          v[n] = vvel[IX(kn, in, jn)];
+        }
+        const size_t e = IFL(k, i, j);
+        for (int p = 0; p < 8; ++p) {
+          double ddx[8], ddy[8], ddz[8], detJ;
+          if (basis_derivs_3d(x, y, z, p, ddx, ddy, ddz, &detJ) != ORC_OK)
+            return ORC_ERR_SINGULAR_JAC;
+          double du_dx = 0.0, du_dy = 0.0, du_dz = 0.0, dv_dx = 0.0, dv_dy = 0.0, dv_dz = 0.0;
+          for (int n = 0; n < 8; ++n) {
+            du_dx = du_dx + ddx[n] * u[n];
+            du_dy = du_dy + ddy[n] * u[n];
+            du_dz = du_dz + ddz[n] * u[n];
+            dv_dx = dv_dx + ddx[n] * v[n];
+            dv_dy = dv_dy + ddy[n] * v[n];
+            dv_dz = dv_dz + ddz[n] * v[n];
+          }
+          const double efvs_qp = effective_viscosity(whichefvs, efvs_constant, ddx, ddy, ddz,
+                                                     u, v, flwafact[e]);
+          tau_xz[e] = tau_xz[e] + efvs_qp * du_dz;
+          tau_yz[e] = tau_yz[e] + efvs_qp * dv_dz;
+          tau_xx[e] = tau_xx[e] + 2.0 * efvs_qp * du_dx;
+          tau_yy[e] = tau_yy[e] + 2.0 * efvs_qp * dv_dy;
+          tau_xy[e] = tau_xy[e] + efvs_qp * (dv_dx + du_dy);
+        }
+        tau_xz[e] = tau_xz[e] / 8;
+        tau_yz[e] = tau_yz[e] / 8;
+        tau_xx[e] = tau_xx[e] / 8;
+        tau_yy[e] = tau_yy[e] / 8;
+        tau_xy[e] = tau_xy[e] / 8;
+        tau_eff[e] = sqrt(tau_xx[e] * tau_xx[e] + tau_yy[e] * tau_yy[e] + tau_xx[e] * tau_yy[e] +
+                          tau_xy[e] * tau_xy[e] + tau_xz[e] * tau_xz[e] + tau_yz[e] * tau_yz[e]);
+      }
+    }
+  return ORC_OK;
+}
+
+/* compute_basal_friction_heatflx (:6755-6964): the frictional heat flux
+ * beta |u_b|^2 / scyr (W/m^2) at cell centres from the basal velocity
+ * (uvel, vvel)(nz,:,:), by the 2x2 face quadrature over active cells
+ * (which = 0) or at active vertices and unstaggered to cells with
+ * glissade_unstagger margin 0 (which = 1, glissade_grid_operators.F90:
+ * 152-231); then the cell halo update. */
+void orc_basal_friction_heatflx(int nx, int ny, int nz, int nhalo, int periodic,
+                                const int *active_cell, const int *active_vertex,
+                                const double *uvel, const double *vvel,
+                                const double *beta, int which, double *bfricflx) {
+  init_tables();
+  const double scyr = 31536000.0;
+  memset(bfricflx, 0, (size_t)nx * ny * sizeof(double));
+  if (which == 0) {
+    for (int j = nhalo + 1; j <= ny - nhalo; ++j)
+      for (int i = nhalo + 1; i <= nx - nhalo; ++i) {
+        if (!active_cell[IC(i, j)]) continue;
+        double u[4], v[4], b[4];
+        for (int n = 0; n < 4; ++n) {
+          const int iv = i + ishift[2][n], jv = j + jshift[2][n];
+          u[n] = uvel[IX(nz, iv, jv)];
+          v[n] = vvel[IX(nz, iv, jv)];
+          b[n] = beta[IV(iv, jv)];
+        }
+        double sum_wqp = 0.0;
+        for (int p = 0; p < 4; ++p) {
+          double u_qp = 0.0, v_qp = 0.0, beta_qp = 0.0;
+          for (int n = 0; n < 4; ++n) {
+            u_qp = u_qp + phi2[n][p] * u[n];
+            v_qp = v_qp + phi2[n][p] * v[n];
+            beta_qp = beta_qp + phi2[n][p] * b[n];
+          }
+          bfricflx[IC(i, j)] = bfricflx[IC(i, j)] + wqp2[p] * beta_qp * (u_qp * u_qp + v_qp * v_qp);
+          sum_wqp = sum_wqp + wqp2[p];
+        }
+        bfricflx[IC(i, j)] = bfricflx[IC(i, j)] / (sum_wqp * scyr);
+      }
+  } else {
+    double *stag = calloc((size_t)(nx - 1) * (ny - 1), sizeof(double));
+    for (int j = 1; j <= ny - 1; ++j)
+      for (int i = 1; i <= nx - 1; ++i) {
+        if (!active_vertex[IV(i, j)]) continue;
+        const double ub = uvel[IX(nz, i, j)], vb = vvel[IX(nz, i, j)];
+        stag[IV(i, j)] = beta[IV(i, j)] * (ub * ub + vb * vb);
+        stag[IV(i, j)] = stag[IV(i, j)] / scyr;
+      }
+    for (int j = 2; j <= ny - 1; ++j)
+      for (int i = 2; i <= nx - 1; ++i)
+        bfricflx[IC(i, j)] = (stag[IV(i, j)] + stag[IV(i - 1, j)] + stag[IV(i, j - 1)] +
+                              stag[IV(i - 1, j - 1)]) / 4.0;
+    free(stag);
+  }
+  orc_halo_cell_real(nx, ny, periodic, bfricflx, 0.0, 0.0);
+}
+
 /* basal_sliding_bc (:8125-8381) applied to the bed layer (k = nz). */
 static void basal_sliding_bc(int nx, int ny, int nz, int nhalo, double dx,
                              double dy, const int *active_cell,

@@ -157,6 +157,20 @@ int orc_pcg_chrongear_3d(int nx, int ny, int nz, int periodic,
                          int precond, int maxiters, double tolerance,
                          int ncheck, double *err, int *niters);
 
+/* Post-solve diagnostics (glissade_velo_higher.F90:3847-3872). */
+int orc_internal_stress(int nx, int ny, int nz, int nhalo, const double *sigma,
+                        const int *active_cell, const double *xVertex,
+                        const double *yVertex, const double *stagusrf,
+                        const double *stagthck, const double *flwafact,
+                        int whichefvs, double efvs_constant, const double *uvel,
+                        const double *vvel, double *tau_xz, double *tau_yz,
+                        double *tau_xx, double *tau_yy, double *tau_xy,
+                        double *tau_eff);
+void orc_basal_friction_heatflx(int nx, int ny, int nz, int nhalo, int periodic,
+                                const int *active_cell, const int *active_vertex,
+                                const double *uvel, const double *vvel,
+                                const double *beta, int which, double *bfricflx);
+
 /* Boundary inputs computed by the setup part of glissade_velo_higher_solve
  * (libglissade/glissade_velo_higher.F90:987-2199).  Caller allocates. */
 typedef struct {

@@ -208,6 +208,37 @@ def assemble_system(m, su, uvel, vvel):
     return A, bu, bv, efvs, nnz.value
 
 
+def internal_stress(m, su, uvel, vvel):
+    """compute_internal_stress at velocity (uvel, vvel): dict of the six
+    stresses, each (ny, nx, nz-1)."""
+    nx, ny, nz = m.nx, m.ny, m.nz
+    names = ("tau_xz", "tau_yz", "tau_xx", "tau_yy", "tau_xy", "tau_eff")
+    outs = {k: np.zeros((ny, nx, nz - 1)) for k in names}
+    fn = lib().orc_internal_stress
+    fn.argtypes = [C.c_int] * 4 + [_dp, _ip, _dp, _dp, _dp, _dp, _dp, C.c_int, C.c_double, _dp, _dp] + [_dp] * 6
+    rc = fn(nx, ny, nz, 2, _p(su["sigma"]), _p(su["active_cell"], _ip), _p(su["xVertex"]), _p(su["yVertex"]),
+            _p(su["stagusrf"]), _p(su["stagthck"]), _p(su["flwafact"]), m.which_efvs, m.efvs_constant,
+            _p(np.ascontiguousarray(uvel, np.float64)), _p(np.ascontiguousarray(vvel, np.float64)),
+            *[_p(outs[k]) for k in names])
+    if rc != 0:
+        raise RuntimeError(f"orc_internal_stress failed: {rc}")
+    return outs
+
+
+def basal_friction_heatflx(m, su, uvel, vvel, beta, which=1):
+    """compute_basal_friction_heatflx from the bed layer of (uvel, vvel):
+    (ny, nx), W/m^2."""
+    nx, ny, nz = m.nx, m.ny, m.nz
+    out = np.zeros((ny, nx))
+    fn = lib().orc_basal_friction_heatflx
+    fn.argtypes = [C.c_int] * 5 + [_ip, _ip, _dp, _dp, _dp, C.c_int, _dp]
+    fn.restype = None
+    fn(nx, ny, nz, 2, m.periodic, _p(su["active_cell"], _ip), _p(su["active_vertex"], _ip),
+       _p(np.ascontiguousarray(uvel, np.float64)), _p(np.ascontiguousarray(vvel, np.float64)),
+       _p(np.ascontiguousarray(beta, np.float64)), which, _p(out))
+    return out
+
+
 def matvec(m, active_vertex, A, xu, xv):
     nx, ny, nz = m.nx, m.ny, m.nz
     yu, yv = np.zeros((ny - 1, nx - 1, nz)), np.zeros((ny - 1, nx - 1, nz))

@@ -220,3 +220,44 @@ extern "C" int emu_slide_beta(const bp_inputs* in, const double* uvel, const dou
   }
   return 0;
 }
+
+// Post-solve diagnostics at velocity (uvel, vvel) through the device's
+// per-element and per-cell/column bodies and the engine's scatters: the six
+// element stresses (nz-1,nx,ny) and bfricflx (nx,ny) by method which.
+// beta (nx-1,ny-1), when given, replaces the plan's betas: each column
+// takes its vertex's value, each cell corner its column's (0 without one).
+extern "C" int emu_diagnostics(const bp_inputs* in, const double* uvel, const double* vvel,
+                               const double* beta, int which, double* tau_xz, double* tau_yz,
+                               double* tau_xx, double* tau_yy, double* tau_xy, double* tau_eff,
+                               double* bfricflx) {
+  Emu E;
+  std::string err;
+  if (!build_plan(in, 1, &E.p, &err)) return 10;
+  const int nx = in->nx, NC = E.p.ncols, NCELL = E.p.ncells;
+  if (beta) {
+    for (int g = 0; g < NC; ++g)
+      E.p.col_beta[g] = beta[(size_t)(E.p.col_ij[NC + g] - 1) * (nx - 1) + (E.p.col_ij[g] - 1)];
+    for (int q = 0; q < 4; ++q)
+      for (int c = 0; c < NCELL; ++c) {
+        const int col = E.p.cell_cols[(size_t)q * NCELL + c];
+        E.p.cell_beta[(size_t)q * NCELL + c] = col >= 0 ? E.p.col_beta[col] : 0.0;
+      }
+  }
+  E.bind();
+  gather_velocity(E.p, 0, uvel, vvel, E.x.data());
+  RefTables T;
+  fill_ref_tables(&T);
+  const size_t ne = (size_t)E.p.nelem;
+  std::vector<double> tau(6 * ne), bf((size_t)std::max(NCELL, NC));
+  for (int e = 0; e < E.p.nelem; ++e) {
+    double t[6];
+    if (!stress_element(E.v, T, e, t)) return 2;
+    for (int q = 0; q < 6; ++q) tau[(size_t)q * ne + e] = t[q];
+  }
+  const int n = which == 0 ? NCELL : NC;
+  for (int i = 0; i < n; ++i) bf[i] = which == 0 ? bfric_cell(E.v, T, i) : bfric_vertex(E.v, i);
+  double* outs[6] = {tau_xz, tau_yz, tau_xx, tau_yy, tau_xy, tau_eff};
+  scatter_elements(E.p, 0, tau.data(), 6, outs);
+  scatter_bfric(E.p, 0, which, bf.data(), bfricflx);
+  return 0;
+}
