@@ -435,21 +435,28 @@ void autotune(bp_problem* P) {
   const int mode = variant == 3 ? MV_CG1 : MV_STD_A;
   best = 1e30f;
   int km = 0, kg = 0;
-  v.dry = 1;
-  for (int mb : {0, 4, 6}) {
-    const int res = krylov_resident_ctas(v, mode, mb);
-    if (res <= 0) continue;
-    for (int g : {0, res * c->num_sms}) {
-      if (g > 0 && g >= P->plan.ntiles) continue;
-      v.minb_k = mb;
-      v.grid_k = g;
-      const float ms = time_launches(c, [&] { launch_mv(mode, v, c->stream); });
-      if (log)
-        std::fprintf(stderr, "autotune krylov minb %d (%d CTAs/SM) grid %d: %.2f us\n", mb, res, g, ms * 1e3f);
-      if (ms < best) { best = ms; km = mb; kg = g; }
+  struct DryPass {  // the dry flag never outlives the timing, not even on an error
+    DevView& v;
+    explicit DryPass(DevView& w) : v(w) { v.dry = 1; }
+    ~DryPass() { v.dry = 0; }
+  };
+  {
+    const DryPass dry(v);
+    for (int mb : {0, 4, 6}) {
+      const int res = krylov_resident_ctas(v, mode, mb);
+      if (res <= 0) continue;
+      for (int g : {0, res * c->num_sms}) {
+        if (g > 0 && g >= P->plan.ntiles) continue;
+        v.minb_k = mb;
+        v.grid_k = g;
+        const float ms = time_launches(c, [&] { launch_mv(mode, v, c->stream); });
+        if (log)
+          std::fprintf(stderr, "autotune krylov minb %d (%d CTAs/SM) grid %d: %.2f us\n", mb, res, g,
+                       ms * 1e3f);
+        if (ms < best) { best = ms; km = mb; kg = g; }
+      }
     }
   }
-  v.dry = 0;
   CK(cudaGetLastError());
   v.minb_k = km;
   v.grid_k = kg;
