@@ -42,8 +42,6 @@ def test_assembly_matches_oracle(ctx, name):
         assert np.abs(a[rows] - g[rows]).max() <= 1e-13 * np.abs(a[rows]).max()
     assert rel_l2([gbu[rows], gbv[rows]], [bu[rows], bv[rows]]) < 1e-13
     assert np.abs(gef - efvs).max() <= 1e-13 * np.abs(efvs).max()
-    # the device matrix is exactly symmetric (the reference's repair is a no-op)
-    from helpers import owned_active_rows as _o  # noqa: F401
 
 
 def _converged_system(m):
