@@ -179,3 +179,26 @@ def test_sia_preconditioner_bodies(m):
                                _p(ru), _p(rv), _p(zu), _p(zv), sym)
         assert rc == 0
         assert rel_l2([zu[rows], zv[rows]], [ref[0][rows], ref[1][rows]]) < 1e-12, sym
+
+
+def test_singular_jacobian_is_reported_by_body_and_oracle():
+    """The reference stops unless |detJ| > 0 (glissade_velo_higher.F90:
+    6458-6473), which a NaN corner thickness fails (a geometrically flat
+    element rarely gives detJ exactly 0 in floating point).  The device body
+    (assembly pass 1) reports it, as the oracle does."""
+    emu = C.CDLL(EMU)
+    m = configs.slab(n=12)
+    prep, u, v = solver.prepare(m)
+    su = oracle.setup(m)
+    j, i = 6, 6  # vertex (7, 7) in 1-based indices, a corner of four active cells
+    for a in (prep.arrays["stagthck"], su["stagthck"]):
+        a[j, i] = np.nan
+    assert prep.arrays["active_vertex"][j, i] == 1
+    shp = (m.ny - 1, m.nx - 1, m.nz, 27)
+    E = [np.zeros(shp) for _ in range(4)]
+    ebu, ebv = np.zeros(m.vshape3), np.zeros(m.vshape3)
+    eef = np.zeros((m.ny, m.nx, m.nz - 1))
+    rc = emu.emu_assemble(C.byref(prep.inputs), _p(u), _p(v), *[_p(a) for a in E], _p(ebu), _p(ebv), _p(eef))
+    assert rc == 2
+    with pytest.raises(RuntimeError, match="failed: 2"):
+        oracle.assemble_system(m, su, u, v)
