@@ -183,7 +183,73 @@ extern "C" int bp_setup(const bp_model* m, bp_setup_arrays* o, double* uvel,
         }
       }
   } else {
-    return BP_ERR_ARGS;  // standard gravity assembly: not offered by this build
+    // standard assembly (:4436-4528): rho g ds/dx integrated against every
+    // basis function over the elements of the active cells, 2x2x2 Gauss
+    // points, with the surface gradient interpolated to each point
+    const double r = 1.0 / std::sqrt(3.0);
+    const double sgx[8] = {-1, 1, 1, -1, -1, 1, 1, -1};
+    const double sgy[8] = {-1, -1, 1, 1, -1, -1, 1, 1};
+    const double sgz[8] = {-1, -1, -1, -1, 1, 1, 1, 1};
+    double phi[8][8], dxi[8][8], deta[8][8], dzeta[8][8];  // [p][n]
+    for (int q = 0; q < 8; ++q) {
+      const double xq = sgx[q] * r, yq = sgy[q] * r, zq = sgz[q] * r;
+      for (int n = 0; n < 8; ++n) {
+        phi[q][n] = (1.0 + sgx[n] * xq) * (1.0 + sgy[n] * yq) * (1.0 + sgz[n] * zq) / 8.0;
+        dxi[q][n] = sgx[n] * (1.0 + sgy[n] * yq) * (1.0 + sgz[n] * zq) / 8.0;
+        deta[q][n] = sgy[n] * (1.0 + sgx[n] * xq) * (1.0 + sgz[n] * zq) / 8.0;
+        dzeta[q][n] = sgz[n] * (1.0 + sgx[n] * xq) * (1.0 + sgy[n] * yq) / 8.0;
+      }
+    }
+    for (int j = 3; j <= ny - 1; ++j)
+      for (int i = 3; i <= nx - 1; ++i) {
+        if (!o->active_cell[C(i, j)]) continue;
+        for (int k = 0; k < nz - 1; ++k) {
+          // nodes SW, SE, NE, NW of the lower face (level k+1), then the upper face (level k)
+          int vi[8], vj[8], lv[8];
+          double x[8], y[8], z[8], gx8[8], gy8[8];
+          for (int n = 0; n < 8; ++n) {
+            const int c = n & 3;
+            vi[n] = (c == 1 || c == 2) ? i : i - 1;
+            vj[n] = c >= 2 ? j : j - 1;
+            lv[n] = n < 4 ? k + 1 : k;
+            const size_t w = V(vi[n], vj[n]);
+            x[n] = m->dx * vi[n];
+            y[n] = m->dy * vj[n];
+            z[n] = o->stagusrf[w] - o->sigma[lv[n]] * o->stagthck[w];
+            gx8[n] = dsdx[w];
+            gy8[n] = dsdy[w];
+          }
+          for (int q = 0; q < 8; ++q) {
+            double J[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+            for (int n = 0; n < 8; ++n) {
+              J[0][0] = J[0][0] + dxi[q][n] * x[n];
+              J[0][1] = J[0][1] + dxi[q][n] * y[n];
+              J[0][2] = J[0][2] + dxi[q][n] * z[n];
+              J[1][0] = J[1][0] + deta[q][n] * x[n];
+              J[1][1] = J[1][1] + deta[q][n] * y[n];
+              J[1][2] = J[1][2] + deta[q][n] * z[n];
+              J[2][0] = J[2][0] + dzeta[q][n] * x[n];
+              J[2][1] = J[2][1] + dzeta[q][n] * y[n];
+              J[2][2] = J[2][2] + dzeta[q][n] * z[n];
+            }
+            // detJ by cofactor expansion along the first row (:6439-6464)
+            const double c0 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+            const double c1 = -(J[1][0] * J[2][2] - J[1][2] * J[2][0]);
+            const double c2 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+            const double detJ = J[0][0] * c0 + J[0][1] * c1 + J[0][2] * c2;
+            double gxq = 0.0, gyq = 0.0;
+            for (int n = 0; n < 8; ++n) {
+              gxq = gxq + phi[q][n] * gx8[n];
+              gyq = gyq + phi[q][n] * gy8[n];
+            }
+            for (int n = 0; n < 8; ++n) {
+              const size_t t = V(vi[n], vj[n]) * nz + lv[n];
+              o->loadu[t] = o->loadu[t] - rg * 1.0 * detJ / vol0 * gxq * phi[q][n];
+              o->loadv[t] = o->loadv[t] - rg * 1.0 * detJ / vol0 * gyq * phi[q][n];
+            }
+          }
+        }
+      }
   }
   const double r3 = 1.0 / std::sqrt(3.0);
   const double qx[4] = {-r3, r3, r3, -r3}, qy[4] = {-r3, -r3, r3, r3};

@@ -41,6 +41,13 @@ def _models():
     m = configs.dome(n=20).copy(periodic=0)
     m.name = "dome_outflow"
     out.append(m)
+    # standard (finite-element) gravity assembly, :4436-4528
+    m = configs.slab(n=24).copy(which_assemble_taud=configs.ASSEMBLE_STANDARD)
+    m.name = "slab_standard_taud"
+    out.append(m)
+    m = configs.marine(n=32, dx=4000.0).copy(which_assemble_taud=configs.ASSEMBLE_STANDARD, periodic=0)
+    m.name = "marine_outflow_standard_taud"
+    out.append(m)
     return out
 
 
