@@ -53,6 +53,15 @@ extern "C" int bp_setup(const bp_model* m, bp_setup_arrays* o, double* uvel,
   const int nx = m->nx, ny = m->ny, nz = m->nz;
   if (m->nhalo != 2 || nx < 6 || ny < 6 || nz < 2 || nz > bp::kNzMax) return BP_ERR_ARGS;
   if (!m->thck || !m->usrf || !m->topg || !m->flwa) return BP_ERR_ARGS;
+  // options this mirror restates: centred surface gradient with the land,
+  // hybrid or marine margin rule; grounded fraction without the
+  // grounding-line parameterisation, or all grounded (a caller with other
+  // options computes bp_inputs itself)
+  if (m->which_gradient != 0 || m->which_gradient_margin < 0 || m->which_gradient_margin > 2 ||
+      (m->which_ground != 0 && m->which_ground != 2) ||
+      (m->which_assemble_taud != 0 && m->which_assemble_taud != 1) ||
+      (m->which_assemble_beta != 0 && m->which_assemble_beta != 1))
+    return BP_ERR_ARGS;
   if (m->sliding && (m->sliding->law != m->which_babc || !o->f_ground ||
                      (m->sliding->law == 10 && !o->flwa_basal_stag)))
     return BP_ERR_ARGS;

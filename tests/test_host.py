@@ -209,3 +209,14 @@ def test_singular_jacobian_is_reported_by_body_and_oracle():
     assert rc == 2
     with pytest.raises(RuntimeError, match="failed: 2"):
         oracle.assemble_system(m, su, u, v)
+
+
+@pytest.mark.parametrize("opt", [dict(which_gradient=1), dict(which_ground=1), dict(which_gradient_margin=3),
+                                 dict(which_assemble_taud=2)])
+def test_setup_rejects_options_it_does_not_restate(opt):
+    """Upstream gradients and the grounding-line parameterisation are not
+    restated by the host mirror: it refuses them instead of computing
+    something else."""
+    with pytest.raises(solver.BPError) as e:
+        solver.prepare(configs.slab(n=12).copy(**opt))
+    assert e.value.code == 10
