@@ -249,6 +249,14 @@ bool build_plan(const bp_inputs* in, int n, HostPlan* p, std::string* err) {
       *err = "missing input array";
       return false;
     }
+    if (I.which_efvs < 0 || I.which_efvs > 2 || I.which_assemble_beta < 0 || I.which_assemble_beta > 1 ||
+        I.which_resid < 0 || I.which_resid > 4 || (I.pcg_variant != 2 && I.pcg_variant != 3) ||
+        I.which_precond < 0 || I.which_precond > 2 || I.precision < 0 || I.precision > 1 ||
+        I.maxiter_nonlinear < 1 || I.pcg_maxiters < 1) {
+      *err = "option out of range (which_efvs 0-2, which_assemble_beta 0-1, which_resid 0-4, "
+             "pcg_variant 2-3, which_precond 0-2, precision 0-1, iteration caps >= 1)";
+      return false;
+    }
     if (I.sliding) {
       SlideParams sp;
       if (!slide_params(*I.sliding, &sp, err)) return false;

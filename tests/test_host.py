@@ -220,3 +220,16 @@ def test_setup_rejects_options_it_does_not_restate(opt):
     with pytest.raises(solver.BPError) as e:
         solver.prepare(configs.slab(n=12).copy(**opt))
     assert e.value.code == 10
+
+
+@pytest.mark.parametrize("field,value", [("which_efvs", 3), ("which_resid", 5), ("pcg_variant", 4),
+                                         ("which_precond", 3), ("precision", 2), ("maxiter_nonlinear", 0)])
+def test_plan_rejects_out_of_range_options(field, value):
+    """The host plan refuses option values the device does not implement
+    (the library returns BP_ERR_ARGS before any device work)."""
+    emu = C.CDLL(EMU)
+    m = configs.slab(n=12)
+    prep, u, v = solver.prepare(m)
+    setattr(prep.inputs, field, value)
+    out = np.zeros((m.ny - 1, m.nx - 1))
+    assert emu.emu_slide_beta(C.byref(prep.inputs), _p(u), _p(v), _p(out)) == 10
