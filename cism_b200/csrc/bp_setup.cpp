@@ -53,11 +53,12 @@ extern "C" int bp_setup(const bp_model* m, bp_setup_arrays* o, double* uvel,
   const int nx = m->nx, ny = m->ny, nz = m->nz;
   if (m->nhalo != 2 || nx < 6 || ny < 6 || nz < 2 || nz > bp::kNzMax) return BP_ERR_ARGS;
   if (!m->thck || !m->usrf || !m->topg || !m->flwa) return BP_ERR_ARGS;
-  // options this mirror restates: centred surface gradient with the land,
-  // hybrid or marine margin rule; grounded fraction without the
+  // options this mirror restates: centred or upstream surface gradient
+  // with the land, hybrid or marine margin rule; grounded fraction without the
   // grounding-line parameterisation, or all grounded (a caller with other
   // options computes bp_inputs itself)
-  if (m->which_gradient != 0 || m->which_gradient_margin < 0 || m->which_gradient_margin > 2 ||
+  if (m->which_gradient < 0 || m->which_gradient > 2 || m->which_gradient_margin < 0 ||
+      m->which_gradient_margin > 2 ||
       (m->which_ground != 0 && m->which_ground != 2) ||
       (m->which_assemble_taud != 0 && m->which_assemble_taud != 1) ||
       (m->which_assemble_beta != 0 && m->which_assemble_beta != 1))
@@ -120,7 +121,9 @@ extern "C" int bp_setup(const bp_model* m, bp_setup_arrays* o, double* uvel,
   stagger(m->thck, o->stagthck);
   stagger(m->usrf, o->stagusrf);
 
-  // surface gradient on vertices, :734-1168 (centered, margin option)
+  // surface gradient on vertices (glissade_surface_elevation_gradient,
+  // glissade_grid_operators.F90:734-1168): edge gradients by the margin
+  // option, then centred, first- or second-order upstream vertex values
   std::vector<double> gx(ncell, 0.0), gy(ncell, 0.0), dsdx(nvert), dsdy(nvert);
   auto edge = [&](int ia, int ja, int ib, int jb, double d) -> double {
     // gradient from cell a to the next cell b along one axis
@@ -139,10 +142,26 @@ extern "C" int bp_setup(const bp_model* m, bp_setup_arrays* o, double* uvel,
     for (int i = 1; i <= nx - 1; ++i) gx[C(i, j)] = edge(i, j, i + 1, j, m->dx);
   for (int j = 1; j <= ny - 1; ++j)
     for (int i = 1; i <= nx; ++i) gy[C(i, j)] = edge(i, j, i, j + 1, m->dy);
+  const double* sf = m->usrf;
   for (int j = 1; j <= ny - 1; ++j)
     for (int i = 1; i <= nx - 1; ++i) {
-      double a = 0.5 * (gx[C(i, j)] + gx[C(i, j + 1)]);
-      double b = 0.5 * (gy[C(i, j)] + gy[C(i + 1, j)]);
+      double a = 0.0, b = 0.0;
+      if (m->which_gradient == 0) {  // centred (:983-1026)
+        a = 0.5 * (gx[C(i, j)] + gx[C(i, j + 1)]);
+        b = 0.5 * (gy[C(i, j)] + gy[C(i + 1, j)]);
+      } else if (m->which_gradient == 1) {  // the edge on the higher side (:1028-1058)
+        a = (sf[C(i, j + 1)] + sf[C(i + 1, j + 1)] > sf[C(i, j)] + sf[C(i + 1, j)]) ? gx[C(i, j + 1)]
+                                                                                    : gx[C(i, j)];
+        b = (sf[C(i + 1, j)] + sf[C(i + 1, j + 1)] > sf[C(i, j)] + sf[C(i, j + 1)]) ? gy[C(i + 1, j)]
+                                                                                    : gy[C(i, j)];
+      } else if (i >= 2 && i <= nx - 2 && j >= 2 && j <= ny - 2) {  // two edges upstream (:1060-1093)
+        const bool north = sf[C(i, j + 1)] + sf[C(i + 1, j + 1)] + sf[C(i, j + 2)] + sf[C(i + 1, j + 2)] >
+                           sf[C(i, j)] + sf[C(i + 1, j)] + sf[C(i, j - 1)] + sf[C(i + 1, j - 1)];
+        a = north ? 1.5 * gx[C(i, j + 1)] - 0.5 * gx[C(i, j + 2)] : 1.5 * gx[C(i, j)] - 0.5 * gx[C(i, j - 1)];
+        const bool east = sf[C(i + 1, j)] + sf[C(i + 1, j + 1)] + sf[C(i + 2, j)] + sf[C(i + 2, j + 1)] >
+                          sf[C(i, j)] + sf[C(i, j + 1)] + sf[C(i - 1, j)] + sf[C(i - 1, j + 1)];
+        b = east ? 1.5 * gy[C(i + 1, j)] - 0.5 * gy[C(i + 2, j)] : 1.5 * gy[C(i, j)] - 0.5 * gy[C(i - 1, j)];
+      }
       a = a > 0.0 ? std::fmin(a, m->max_slope) : std::fmax(a, -m->max_slope);
       b = b > 0.0 ? std::fmin(b, m->max_slope) : std::fmax(b, -m->max_slope);
       dsdx[V(i, j)] = a;

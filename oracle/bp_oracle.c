@@ -267,7 +267,6 @@ void orc_surface_gradient(int nx, int ny, int periodic, double dx, double dy,
                           double thklim, double thck_gradient_ramp,
                           int ho_gradient, int ho_gradient_margin,
                           double max_slope, double *ds_dx, double *ds_dy) {
-  (void)ho_gradient;
   double *ex = calloc((size_t)nx * ny, sizeof(double));
   double *ey = calloc((size_t)nx * ny, sizeof(double));
   if (ho_gradient_margin == ORC_GRADIENT_MARGIN_LAND) {
@@ -314,11 +313,39 @@ void orc_surface_gradient(int nx, int ny, int periodic, double dx, double dy,
           ey[IC(i, j)] = ef * sgn * (usrf[IC(i, ju)] - usrf[IC(i, jl)]) / dy;
       }
   }
-  for (int j = 1; j <= ny - 1; ++j)
-    for (int i = 1; i <= nx - 1; ++i) {
-      ds_dx[IV(i, j)] = 0.5 * (ex[IC(i, j)] + ex[IC(i, j + 1)]);
-      ds_dy[IV(i, j)] = 0.5 * (ey[IC(i, j)] + ey[IC(i + 1, j)]);
-    }
+  memset(ds_dx, 0, (size_t)(nx - 1) * (ny - 1) * sizeof(double));
+  memset(ds_dy, 0, (size_t)(nx - 1) * (ny - 1) * sizeof(double));
+  if (ho_gradient == ORC_GRADIENT_CENTERED) {
+    for (int j = 1; j <= ny - 1; ++j)
+      for (int i = 1; i <= nx - 1; ++i) {
+        ds_dx[IV(i, j)] = 0.5 * (ex[IC(i, j)] + ex[IC(i, j + 1)]);
+        ds_dy[IV(i, j)] = 0.5 * (ey[IC(i, j)] + ey[IC(i + 1, j)]);
+      }
+  } else if (ho_gradient == ORC_GRADIENT_UPSTREAM1) {
+    /* the edge on the higher side of the vertex (glissade_grid_operators.F90:1028-1058) */
+    for (int j = 1; j <= ny - 1; ++j)
+      for (int i = 1; i <= nx - 1; ++i) {
+        double sum1 = usrf[IC(i, j + 1)] + usrf[IC(i + 1, j + 1)];
+        double sum2 = usrf[IC(i, j)] + usrf[IC(i + 1, j)];
+        ds_dx[IV(i, j)] = sum1 > sum2 ? ex[IC(i, j + 1)] : ex[IC(i, j)];
+        sum1 = usrf[IC(i + 1, j)] + usrf[IC(i + 1, j + 1)];
+        sum2 = usrf[IC(i, j)] + usrf[IC(i, j + 1)];
+        ds_dy[IV(i, j)] = sum1 > sum2 ? ey[IC(i + 1, j)] : ey[IC(i, j)];
+      }
+  } else if (ho_gradient == ORC_GRADIENT_UPSTREAM2) {
+    /* second order: two edges on the higher side (:1060-1093) */
+    for (int j = 2; j <= ny - 2; ++j)
+      for (int i = 2; i <= nx - 2; ++i) {
+        double sum1 = usrf[IC(i, j + 1)] + usrf[IC(i + 1, j + 1)] + usrf[IC(i, j + 2)] + usrf[IC(i + 1, j + 2)];
+        double sum2 = usrf[IC(i, j)] + usrf[IC(i + 1, j)] + usrf[IC(i, j - 1)] + usrf[IC(i + 1, j - 1)];
+        ds_dx[IV(i, j)] = sum1 > sum2 ? 1.5 * ex[IC(i, j + 1)] - 0.5 * ex[IC(i, j + 2)]
+                                      : 1.5 * ex[IC(i, j)] - 0.5 * ex[IC(i, j - 1)];
+        sum1 = usrf[IC(i + 1, j)] + usrf[IC(i + 1, j + 1)] + usrf[IC(i + 2, j)] + usrf[IC(i + 2, j + 1)];
+        sum2 = usrf[IC(i, j)] + usrf[IC(i, j + 1)] + usrf[IC(i - 1, j)] + usrf[IC(i - 1, j + 1)];
+        ds_dy[IV(i, j)] = sum1 > sum2 ? 1.5 * ey[IC(i + 1, j)] - 0.5 * ey[IC(i + 2, j)]
+                                      : 1.5 * ey[IC(i, j)] - 0.5 * ey[IC(i - 1, j)];
+      }
+  }
   for (int j = 1; j <= ny - 1; ++j)
     for (int i = 1; i <= nx - 1; ++i) {
       size_t v = IV(i, j);

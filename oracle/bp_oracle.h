@@ -34,7 +34,7 @@ enum {
   ORC_RESID_L2NORM = 3, ORC_RESID_L2NORM_RELATIVE = 4,
   ORC_SPARSE_PCG_STANDARD = 2, ORC_SPARSE_PCG_CHRONGEAR = 3,
   ORC_PRECOND_NONE = 0, ORC_PRECOND_DIAG = 1, ORC_PRECOND_SIA = 2,
-  ORC_GRADIENT_CENTERED = 0,
+  ORC_GRADIENT_CENTERED = 0, ORC_GRADIENT_UPSTREAM1 = 1, ORC_GRADIENT_UPSTREAM2 = 2,
   ORC_GRADIENT_MARGIN_LAND = 0, ORC_GRADIENT_MARGIN_HYBRID = 1,
   ORC_GRADIENT_MARGIN_MARINE = 2,
   ORC_ASSEMBLE_STANDARD = 0, ORC_ASSEMBLE_LOCAL = 1,

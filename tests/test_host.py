@@ -48,6 +48,12 @@ def _models():
     m = configs.marine(n=32, dx=4000.0).copy(which_assemble_taud=configs.ASSEMBLE_STANDARD, periodic=0)
     m.name = "marine_outflow_standard_taud"
     out.append(m)
+    # first- and second-order upstream surface gradients
+    # (glissade_grid_operators.F90:1028-1093)
+    for g in (1, 2):
+        m = configs.marine(n=32, dx=4000.0).copy(which_gradient=g)
+        m.name = f"marine_upstream{g}_gradient"
+        out.append(m)
     return out
 
 
@@ -211,12 +217,13 @@ def test_singular_jacobian_is_reported_by_body_and_oracle():
         oracle.assemble_system(m, su, u, v)
 
 
-@pytest.mark.parametrize("opt", [dict(which_gradient=1), dict(which_ground=1), dict(which_gradient_margin=3),
+@pytest.mark.parametrize("opt", [dict(which_gradient=3), dict(which_ground=1), dict(which_gradient_margin=3),
                                  dict(which_assemble_taud=2)])
 def test_setup_rejects_options_it_does_not_restate(opt):
-    """Upstream gradients and the grounding-line parameterisation are not
-    restated by the host mirror: it refuses them instead of computing
-    something else."""
+    """The grounding-line parameterisation (which the reference does not
+    support either, glissade_grounding_line.F90:73) and unknown option
+    values are refused by the host mirror instead of computing something
+    else."""
     with pytest.raises(solver.BPError) as e:
         solver.prepare(configs.slab(n=12).copy(**opt))
     assert e.value.code == 10
@@ -233,3 +240,15 @@ def test_plan_rejects_out_of_range_options(field, value):
     setattr(prep.inputs, field, value)
     out = np.zeros((m.ny - 1, m.nx - 1))
     assert emu.emu_slide_beta(C.byref(prep.inputs), _p(u), _p(v), _p(out)) == 10
+
+
+def test_upstream_gradient_takes_the_higher_edge():
+    """First-order upstream: each vertex takes the edge gradient of the
+    higher pair of cells; on a plane tilted in x that is the plane's slope
+    at every vertex."""
+    m = configs.slab(n=16, theta_deg=0.5).copy(which_gradient=1, max_slope=1.0)
+    su = oracle.setup(m)
+    js, is_ = m.owned_vertex_slices()
+    slope = -np.tan(np.radians(0.5))
+    assert np.allclose(su["dusrf_dx"][js, is_], slope, rtol=1e-12)
+    assert np.all(su["dusrf_dy"][js, is_] == 0.0)
