@@ -63,6 +63,11 @@ extern "C" int bp_setup(const bp_model* m, bp_setup_arrays* o, double* uvel,
       (m->which_assemble_taud != 0 && m->which_assemble_taud != 1) ||
       (m->which_assemble_beta != 0 && m->which_assemble_beta != 1))
     return BP_ERR_ARGS;
+  // basal traction: constant, external or no slip here; the
+  // velocity-dependent laws through m->sliding; the other calcbeta options
+  // (BPMP, large, ISMIP-HOM C, the simple pattern) come in as beta_internal
+  // of a caller-built bp_inputs
+  if (!m->sliding && m->which_babc != 0 && m->which_babc != 5 && m->which_babc != 6) return BP_ERR_ARGS;
   if (m->sliding && (m->sliding->law != m->which_babc || !o->f_ground ||
                      (m->sliding->law == 10 && !o->flwa_basal_stag)))
     return BP_ERR_ARGS;

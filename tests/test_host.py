@@ -218,12 +218,13 @@ def test_singular_jacobian_is_reported_by_body_and_oracle():
 
 
 @pytest.mark.parametrize("opt", [dict(which_gradient=3), dict(which_ground=1), dict(which_gradient_margin=3),
-                                 dict(which_assemble_taud=2)])
+                                 dict(which_assemble_taud=2), dict(which_babc=1), dict(which_babc=9)])
 def test_setup_rejects_options_it_does_not_restate(opt):
     """The grounding-line parameterisation (which the reference does not
-    support either, glissade_grounding_line.F90:73) and unknown option
-    values are refused by the host mirror instead of computing something
-    else."""
+    support either, glissade_grounding_line.F90:73), calcbeta options the
+    mirror does not evaluate (BPMP; a velocity-dependent law without its
+    parameters) and unknown option values are refused by the host mirror
+    instead of computing something else."""
     with pytest.raises(solver.BPError) as e:
         solver.prepare(configs.slab(n=12).copy(**opt))
     assert e.value.code == 10
