@@ -1527,6 +1527,279 @@ void orc_setup_free(orc_setup *s) {
   free(s->ocean_mask); free(s->land_mask);
 }
 
+/* ---------------------------------------------------------------------
+ * Shallow-shelf (SSA) branch of glissade_velo_higher_solve: the 2-D
+ * solve (solve_2d, :1125-1128) for whichapprox = HO_APPROX_SSA.  The 2-D
+ * matrix (indxA_2d, 9 entries) is kept in the kA = 0 slice of the 27-entry
+ * layout with nz = 1; the 2-D matvec, PCG, Dirichlet, symmetry and
+ * nonzero-count routines of the reference are the 3-D ones at nz = 1 with
+ * the same loop orders (matvec_multiply_structured_2d :2651-2755 against
+ * _3d :2533-2647; pcg_solver_standard_2d :553-961 and chrongear_2d
+ * :1614-2146 against their 3-D forms; dirichlet_boundary_conditions_2d
+ * :8582-8764), so those are called with nz = 1.
+ * ------------------------------------------------------------------- */
+
+/* get_basis_function_derivatives_2d (:6583-6751). */
+static int basis_derivs_2d(const double *x, const double *y, int p, double *dx,
+                           double *dy, double *detJ) {
+  double J11 = 0.0, J12 = 0.0, J21 = 0.0, J22 = 0.0;
+  for (int n = 0; n < 4; ++n) {
+    J11 = J11 + dxr2[n][p] * x[n];
+    J12 = J12 + dxr2[n][p] * y[n];
+    J21 = J21 + dyr2[n][p] * x[n];
+    J22 = J22 + dyr2[n][p] * y[n];
+  }
+  const double d = J11 * J22 - J12 * J21;
+  *detJ = d;
+  if (!(fabs(d) > 0.0)) return ORC_ERR_SINGULAR_JAC;
+  const double i11 = J22 / d, i12 = -J12 / d, i21 = -J21 / d, i22 = J11 / d;
+  for (int n = 0; n < 4; ++n) {
+    dx[n] = i11 * dxr2[n][p] + i12 * dyr2[n][p];
+    dy[n] = i21 * dxr2[n][p] + i22 * dyr2[n][p];
+  }
+  return ORC_OK;
+}
+
+/* compute_effective_viscosity, SSA branch (:7199-7378) with the vertically
+ * averaged flow factor. */
+static double effective_viscosity_ssa(int whichefvs, double efvs_constant,
+                                      const double *dx, const double *dy,
+                                      const double *u, const double *v,
+                                      double flwafact) {
+  const double effstrain_min = 1.0e-8;
+  const double p_effstr = (1.0 - 3.0) / 3.0;
+  const double p2_effstr = p_effstr / 2.0;
+  if (whichefvs == ORC_EFVS_CONSTANT) return efvs_constant;
+  if (whichefvs == ORC_EFVS_FLOWFACT) {
+    const double scyr = 31536000.0;
+    double effstrain = (500.0 / scyr) / 200.0e3 * scyr;
+    return flwafact * pow(effstrain, p_effstr);
+  }
+  double ux = 0, uy = 0, vx = 0, vy = 0;
+  for (int n = 0; n < 4; ++n) {
+    ux = ux + dx[n] * u[n];
+    uy = uy + dy[n] * u[n];
+    vx = vx + dx[n] * v[n];
+    vy = vy + dy[n] * v[n];
+  }
+  double sq = effstrain_min * effstrain_min +
+              (ux * ux + vy * vy + ux * vy + 0.25 * ((vx + uy) * (vx + uy)));
+  return flwafact * pow(sq, p2_effstr);
+}
+
+/* assemble_stiffness_matrix_2d, SSA branch (:5208-5595): per active cell,
+ * 2x2 Gauss points, efvs from the vertically averaged flow factor
+ * (glissade_vertical_average, glissade_grid_operators.F90:1172-1236),
+ * element matrix with h efvs (compute_element_matrix :7868-7986), scatter
+ * by element_to_global_matrix_2d (:8058-8121); efvs(k,i,j) = the mean of
+ * the point values on every layer. */
+static int assemble_ssa(int nx, int ny, int nz, int nhalo, const double *sigma,
+                        const int *active_cell, const double *xVertex,
+                        const double *yVertex, const double *u2, const double *v2,
+                        const double *stagthck, const double *flwafact,
+                        int whichefvs, double efvs_constant, double *efvs,
+                        double *Auu, double *Auv, double *Avu, double *Avv) {
+  init_tables();
+  const double vol0 = 1.0e9;
+  const size_t nvx = (size_t)(nx - 1) * (ny - 1);
+  memset(Auu, 0, 27 * nvx * sizeof(double));
+  memset(Auv, 0, 27 * nvx * sizeof(double));
+  memset(Avu, 0, 27 * nvx * sizeof(double));
+  memset(Avv, 0, 27 * nvx * sizeof(double));
+  memset(efvs, 0, (size_t)(nz - 1) * nx * ny * sizeof(double));
+  for (int j = nhalo + 1; j <= ny - nhalo + 1; ++j)
+    for (int i = nhalo + 1; i <= nx - nhalo + 1; ++i) {
+      if (!active_cell[IC(i, j)]) continue;
+      double fl2 = 0.0;  /* vertical average, all cells (no mask) */
+      for (int k = 1; k <= nz - 1; ++k)
+        fl2 = fl2 + flwafact[IFL(k, i, j)] * (sigma[k] - sigma[k - 1]);
+      double Kuu[4][4] = {{0}}, Kuv[4][4] = {{0}}, Kvu[4][4] = {{0}}, Kvv[4][4] = {{0}};
+      double x[4], y[4], u[4], v[4], h[4], efvs_qp[4];
+      for (int n = 0; n < 4; ++n) {
+        const int iv = i + ishift[2][n], jv = j + jshift[2][n];
+        x[n] = xVertex[IV(iv, jv)];
+        y[n] = yVertex[IV(iv, jv)];
+        u[n] = u2[IV(iv, jv)];
+        v[n] = v2[IV(iv, jv)];
+        h[n] = stagthck[IV(iv, jv)];
+      }
+      for (int p = 0; p < 4; ++p) {
+        double ddx[4], ddy[4], detJ;
+        if (basis_derivs_2d(x, y, p, ddx, ddy, &detJ) != ORC_OK) return ORC_ERR_SINGULAR_JAC;
+        efvs_qp[p] = effective_viscosity_ssa(whichefvs, efvs_constant, ddx, ddy, u, v, fl2);
+        double h_qp = 0.0;
+        for (int n = 0; n < 4; ++n) h_qp = h_qp + phi2[n][p] * h[n];
+        const double f = h_qp * efvs_qp[p] * wqp2[p] * detJ / vol0;
+        for (int nc = 0; nc < 4; ++nc)
+          for (int nr = 0; nr < 4; ++nr) {
+            Kuu[nr][nc] = Kuu[nr][nc] + f * (4.0 * ddx[nr] * ddx[nc] + ddy[nr] * ddy[nc]);
+            Kuv[nr][nc] = Kuv[nr][nc] + f * (2.0 * ddx[nr] * ddy[nc] + ddy[nr] * ddx[nc]);
+            Kvu[nr][nc] = Kvu[nr][nc] + f * (2.0 * ddy[nr] * ddx[nc] + ddx[nr] * ddy[nc]);
+            Kvv[nr][nc] = Kvv[nr][nc] + f * (4.0 * ddy[nr] * ddy[nc] + ddx[nr] * ddx[nc]);
+          }
+      }
+      for (int k = 1; k <= nz - 1; ++k) {
+        double e = 0.0;
+        for (int p = 0; p < 4; ++p) e = e + efvs_qp[p];
+        efvs[IFL(k, i, j)] = e / 4;
+      }
+      for (int a = 0; a < 4; ++a)
+        for (int b = 0; b < 4; ++b) {
+          if (fabs(Kuu[a][b] - Kuu[b][a]) > 1.0e-10) return ORC_ERR_ASYMMETRIC_ELEMENT;
+          if (fabs(Kvv[a][b] - Kvv[b][a]) > 1.0e-10) return ORC_ERR_ASYMMETRIC_ELEMENT;
+          if (fabs(Kuv[a][b] - Kvu[b][a]) > 1.0e-10) return ORC_ERR_ASYMMETRIC_ELEMENT;
+        }
+      for (int nr = 0; nr < 4; ++nr) {
+        const int ii = i + ishift[2][nr], jj = j + jshift[2][nr];
+        for (int nc = 0; nc < 4; ++nc) {
+          const size_t a = ((size_t)IV(ii, jj)) * 27 + (size_t)(indxA(ishift[nr][nc], jshift[nr][nc], 0) - 1);
+          Auu[a] = Auu[a] + Kuu[nr][nc];
+          Auv[a] = Auv[a] + Kuv[nr][nc];
+          Avu[a] = Avu[a] + Kvu[nr][nc];
+          Avv[a] = Avv[a] + Kvv[nr][nc];
+        }
+      }
+    }
+  return ORC_OK;
+}
+
+/* compute_residual_velocity_2d (:9238-9351): no bed layer to leave out. */
+static double residual_velocity_2d(int nx, int ny, int periodic, int whichresid,
+                                   const double *u, const double *v,
+                                   const double *usav, const double *vsav) {
+  int ilo, ihi, jlo, jhi;
+  owned_range(nx, ny, periodic, &ilo, &ihi, &jlo, &jhi);
+  double r = 0.0;
+  long count = 0;
+  for (int j = jlo; j <= jhi; ++j)
+    for (int i = ilo; i <= ihi; ++i) {
+      const size_t x = IV(i, j);
+      const double speed = sqrt(u[x] * u[x] + v[x] * v[x]);
+      if (speed != 0.0) {
+        const double oldspeed = sqrt(usav[x] * usav[x] + vsav[x] * vsav[x]);
+        const double diff = fabs((oldspeed - speed) / speed);
+        if (whichresid == ORC_RESID_MEANU) { r = r + diff; ++count; }
+        else if (diff > r) r = diff;
+      }
+    }
+  if (whichresid == ORC_RESID_MEANU && count > 0) r = r / (double)count;
+  return r;
+}
+
+int orc_velo_ssa_solve(const orc_model *m, double *uvel, double *vvel,
+                       double *efvs, double *beta_internal, orc_stats *stats) {
+  const int nx = m->nx, ny = m->ny, nz = m->nz;
+  const size_t nvx = (size_t)(nx - 1) * (ny - 1), n3 = nvx * nz, nA = nvx * 27;
+  orc_setup s;
+  orc_setup_alloc(m, &s);
+  memset(stats, 0, sizeof(*stats));
+  int st = orc_setup_solve(m, &s, uvel, vvel);
+  if (st != ORC_OK) { orc_setup_free(&s); stats->status = st; return st; }
+  double *Auu = xalloc(nA * 8), *Auv = xalloc(nA * 8), *Avu = xalloc(nA * 8),
+         *Avv = xalloc(nA * 8), *bu = xalloc(nvx * 8), *bv = xalloc(nvx * 8),
+         *lu = xalloc(nvx * 8), *lv = xalloc(nvx * 8), *u2 = xalloc(nvx * 8),
+         *v2 = xalloc(nvx * 8), *us = xalloc(nvx * 8), *vs = xalloc(nvx * 8),
+         *u3 = xalloc(n3 * 8), *v3 = xalloc(n3 * 8);
+  int *um = calloc(nvx, sizeof(int)), *vm = calloc(nvx, sizeof(int));
+  for (int j = 1; j <= ny - 1; ++j)
+    for (int i = 1; i <= nx - 1; ++i) {
+      const size_t w = IV(i, j);
+      for (int k = 1; k <= nz; ++k) {  /* loadu_2d = sum over levels (:2123-2137) */
+        lu[w] = lu[w] + s.loadu[IX(k, i, j)];
+        lv[w] = lv[w] + s.loadv[IX(k, i, j)];
+      }
+      u2[w] = uvel[IX(nz, i, j)];  /* uvel_2d = uvel(nz,:,:) (:1179-1180) */
+      v2[w] = vvel[IX(nz, i, j)];
+      um[w] = s.umask_dirichlet[IX(nz, i, j)];  /* the bed level's masks (:2878) */
+      vm[w] = s.vmask_dirichlet[IX(nz, i, j)];
+    }
+  int counter = 0;
+  double outer_it_criterion = 1.0e10, outer_it_target = 1.0e-12;
+  const double L2_target = 1.0e-4, L2_target_relative = 1.0e-7, resid_target = 1.0e-4;
+  int status = ORC_OK;
+  while (outer_it_criterion >= outer_it_target && counter < m->maxiter_nonlinear) {
+    counter = counter + 1;
+    for (size_t w = 0; w < nvx; ++w)  /* ubas = uvel_2d for SSA (:2236-2239) */
+      for (int k = 1; k <= nz; ++k) { u3[w * nz + k - 1] = u2[w]; v3[w * nz + k - 1] = v2[w]; }
+    st = orc_calcbeta(m, &s, u3, v3, beta_internal);
+    if (st != ORC_OK) { status = st; break; }
+    memcpy(us, u2, nvx * 8);
+    memcpy(vs, v2, nvx * 8);
+    st = assemble_ssa(nx, ny, nz, m->nhalo, s.sigma, s.active_cell, s.xVertex, s.yVertex, u2, v2,
+                      s.stagthck, s.flwafact, m->which_efvs, m->efvs_constant, efvs, Auu, Auv, Avu,
+                      Avv);
+    if (st != ORC_OK) { status = st; break; }
+    if (m->which_babc != ORC_BABC_NO_SLIP)
+      basal_sliding_bc(nx, ny, 1, m->nhalo, m->dx, m->dy, s.active_cell, s.active_vertex,
+                       beta_internal, s.xVertex, s.yVertex, m->which_assemble_beta, Auu, Avv);
+    memcpy(bu, lu, nvx * 8);
+    memcpy(bv, lv, nvx * 8);
+    dirichlet_bc_3d(nx, ny, 1, m->nhalo, s.active_vertex, um, vm, u2, v2, Auu, Auv, Avu, Avv, bu, bv);
+    orc_halo_stag(nx, ny, 27, m->periodic, Auu);
+    orc_halo_stag(nx, ny, 27, m->periodic, Auv);
+    orc_halo_stag(nx, ny, 27, m->periodic, Avu);
+    orc_halo_stag(nx, ny, 27, m->periodic, Avv);
+    orc_halo_stag(nx, ny, 1, m->periodic, bu);
+    orc_halo_stag(nx, ny, 1, m->periodic, bv);
+    check_symmetry_assembled_3d(nx, ny, 1, m->periodic, s.active_vertex, Auu, Auv, Avu, Avv);
+    long nnz = count_nonzeros_3d(nx, ny, 1, m->periodic, s.active_vertex, Auu, Auv, Avu, Avv);
+    if (nnz == 0) {
+      memset(u2, 0, nvx * 8);
+      memset(v2, 0, nvx * 8);
+      status = ORC_ZERO_MATRIX;
+      break;
+    }
+    if (m->which_babc == ORC_BABC_NO_SLIP) {  /* SSA on a frozen bed: u = 0 (:3227-3240) */
+      memset(u2, 0, nvx * 8);
+      memset(v2, 0, nvx * 8);
+      stats->L2_norm = 0.0;
+      stats->L2_norm_relative = 0.0;
+    } else {
+      residual_vector_3d(nx, ny, 1, m->periodic, s.active_vertex, Auu, Auv, Avu, Avv, bu, bv, u2, v2,
+                         &stats->L2_norm, &stats->L2_norm_relative);
+      double err = 0.0;
+      int niters = 0;
+      if (m->which_sparse == ORC_SPARSE_PCG_CHRONGEAR)
+        st = orc_pcg_chrongear_3d(nx, ny, 1, m->periodic, s.active_vertex, Auu, Auv, Avu, Avv, bu,
+                                  bv, u2, v2, m->which_precond, m->pcg_maxiters, m->pcg_tol,
+                                  m->pcg_ncheck, &err, &niters);
+      else
+        st = orc_pcg_standard_3d(nx, ny, 1, m->periodic, s.active_vertex, Auu, Auv, Avu, Avv, bu,
+                                 bv, u2, v2, m->which_precond, m->pcg_maxiters, m->pcg_tol,
+                                 m->pcg_ncheck, &err, &niters);
+      stats->pcg_iters_total += niters;
+      stats->pcg_iters_last = niters;
+      stats->pcg_err_last = err;
+      if (st == ORC_ERR_NAN) { status = st; break; }
+    }
+    orc_halo_stag(nx, ny, 1, m->periodic, u2);
+    orc_halo_stag(nx, ny, 1, m->periodic, v2);
+    const double resid_velo = residual_velocity_2d(nx, ny, m->periodic, m->which_resid, u2, v2, us, vs);
+    stats->resid_velo = resid_velo;
+    if (m->which_resid == ORC_RESID_L2NORM) {
+      outer_it_criterion = stats->L2_norm; outer_it_target = L2_target;
+    } else if (m->which_resid == ORC_RESID_L2NORM_RELATIVE) {
+      outer_it_criterion = stats->L2_norm_relative; outer_it_target = L2_target_relative;
+    } else {
+      outer_it_criterion = resid_velo; outer_it_target = resid_target;
+    }
+  }
+  for (int j = 1; j <= ny - 1; ++j)  /* uvel(k,:,:) = uvel_2d for every level (:3745-3750) */
+    for (int i = 1; i <= nx - 1; ++i)
+      for (int k = 1; k <= nz; ++k) {
+        uvel[IX(k, i, j)] = u2[IV(i, j)];
+        vvel[IX(k, i, j)] = v2[IV(i, j)];
+      }
+  stats->picard_iters = counter;
+  stats->converged = (status == ORC_OK && counter < m->maxiter_nonlinear) ? 1 : 0;
+  if (status == ORC_OK && !stats->converged) status = ORC_WARN_PICARD_NOT_CONVERGED;
+  stats->status = status;
+  free(Auu); free(Auv); free(Avu); free(Avv); free(bu); free(bv); free(lu); free(lv);
+  free(u2); free(v2); free(us); free(vs); free(u3); free(v3); free(um); free(vm);
+  orc_setup_free(&s);
+  return status;
+}
+
 /* glissade_velo_higher_solve, 3-D Blatter-Pattyn branch with the native
  * PCG solvers (glissade_velo_higher.F90:654-3986). */
 int orc_velo_higher_solve(const orc_model *m, double *uvel, double *vvel,

@@ -157,6 +157,11 @@ int orc_pcg_chrongear_3d(int nx, int ny, int nz, int periodic,
                          int precond, int maxiters, double tolerance,
                          int ncheck, double *err, int *niters);
 
+/* glissade_velo_higher_solve, shallow-shelf (SSA) branch: the 2-D solve
+ * of the depth-integrated velocity, copied to every level. */
+int orc_velo_ssa_solve(const orc_model *m, double *uvel, double *vvel,
+                       double *efvs, double *beta_internal, orc_stats *stats);
+
 /* Post-solve diagnostics (glissade_velo_higher.F90:3847-3872). */
 int orc_internal_stress(int nx, int ny, int nz, int nhalo, const double *sigma,
                         const int *active_cell, const double *xVertex,

@@ -154,6 +154,20 @@ def velo_higher_solve(m, uvel=None, vvel=None):
     return u, v, efvs, beta, st.as_dict()
 
 
+def velo_ssa_solve(m, uvel=None, vvel=None):
+    """Shallow-shelf (SSA) branch of the solve; returns (uvel, vvel, efvs,
+    beta_internal, stats), the 2-D velocity on every level."""
+    keep = _Keep()
+    om = make_model(m, keep)
+    u = np.zeros(m.vshape3) if uvel is None else np.array(uvel, dtype=np.float64, copy=True)
+    v = np.zeros(m.vshape3) if vvel is None else np.array(vvel, dtype=np.float64, copy=True)
+    efvs = np.zeros((m.ny, m.nx, m.nz - 1))
+    beta = np.zeros((m.ny - 1, m.nx - 1))
+    st = OrcStats()
+    lib().orc_velo_ssa_solve(C.byref(om), _p(u), _p(v), _p(efvs), _p(beta), C.byref(st))
+    return u, v, efvs, beta, st.as_dict()
+
+
 def setup(m, uvel=None, vvel=None):
     """Setup of glissade_velo_higher_solve: returns dict of boundary inputs."""
     keep = _Keep()
