@@ -108,6 +108,7 @@ class BPModel:
     pcg_tol: float = 1.0e-8
     pcg_ncheck: int = 5
     sliding: Optional[SlidingLaw] = None  # velocity-dependent law (which_babc = sliding.law)
+    approx_ssa: int = 0  # 1: shallow-shelf 2-D solve (whichapprox = HO_APPROX_SSA)
     name: str = ""
 
     @property

@@ -343,6 +343,115 @@ BP_HD void row_assemble(const DevView& v, const RefTables& T, int col, int k,
   }
 }
 
+// ---------------------------------------------------------------------
+// Shallow-shelf (SSA) assembly: assemble_stiffness_matrix_2d, SSA branch
+// (:5208-5595).  One 2-D element per active cell (corners SW, SE, NE, NW =
+// the reference's 2-D node order), 2x2 Gauss points; nodes are columns
+// (nz = 1).  The element data of cell c sit where the 3-D elements' do:
+// point p at qp[(c * 8 + p) * 10], f then J^-1 (2 x 2, row-major).
+// ---------------------------------------------------------------------
+// Point p of cell c: get_basis_function_derivatives_2d (:6583-6751), the
+// SSA branch of compute_effective_viscosity with the vertically averaged
+// flow factor (v.flwafact[c]), and f = h efvs w detJ / vol0 with the
+// thickness interpolated to the point (:5507-5515, compute_element_matrix
+// :7868-7986).  false for a singular Jacobian.
+BP_HD bool qp2_element_point(const DevView& v, const RefTables& T, int c, int p, double* out,
+                             double* efvs_qp) {
+  const InstParams& ip = v.inst[v.cell_inst[c]];
+  const int ic = v.cell_ij[c], jc = v.cell_ij[v.ncells + c];
+  double x[4], y[4], u[4], w[4], h[4];
+  for (int n = 0; n < 4; ++n) {
+    const int iv = (n == 1 || n == 2) ? ic : ic - 1;
+    const int jv = n >= 2 ? jc : jc - 1;
+    x[n] = ip.dx * iv;
+    y[n] = ip.dy * jv;
+    h[n] = v.cell_h[n * v.ncells + c];
+    const int col = v.cell_cols[n * v.ncells + c];
+    if (col >= 0) {
+      const double2 xv = v.x[col];
+      u[n] = xv.x;
+      w[n] = xv.y;
+    } else {
+      u[n] = 0.0;
+      w[n] = 0.0;
+    }
+  }
+  double J11 = 0, J12 = 0, J21 = 0, J22 = 0;
+  for (int n = 0; n < 4; ++n) {
+    J11 += T.dxr2[p][n] * x[n];
+    J12 += T.dxr2[p][n] * y[n];
+    J21 += T.dyr2[p][n] * x[n];
+    J22 += T.dyr2[p][n] * y[n];
+  }
+  const double det = J11 * J22 - J12 * J21;
+  if (!(fabs(det) > 0.0)) return false;
+  const double i11 = J22 / det, i12 = -J12 / det, i21 = -J21 / det, i22 = J11 / det;
+  double g[6] = {0, 0, 0, 0, 0, 0};  // (du/dx, du/dy, -, dv/dx, dv/dy, -)
+  if (ip.which_efvs == 2) {
+    for (int n = 0; n < 4; ++n) {
+      const double dx = BP_FMA(i12, T.dyr2[p][n], i11 * T.dxr2[p][n]);
+      const double dy = BP_FMA(i22, T.dyr2[p][n], i21 * T.dxr2[p][n]);
+      g[0] += dx * u[n];
+      g[1] += dy * u[n];
+      g[3] += dx * w[n];
+      g[4] += dy * w[n];
+    }
+  }
+  // qp_efvs with no vertical shear is the SSA branch (:7326-7334)
+  const double efvs = qp_efvs(ip.which_efvs, ip.efvs_constant, v.flwafact[c], g);
+  double h_qp = 0.0;
+  for (int n = 0; n < 4; ++n) h_qp += T.phi2[p][n] * h[n];
+  *efvs_qp = efvs;
+  out[0] = h_qp * efvs * 1.0 * det / kVol0;
+  out[1] = i11; out[2] = i12; out[3] = i21; out[4] = i22;
+  return true;
+}
+
+// stencil index (0-based, kA = 0) into which the 2-D K(nr, nc) is summed
+BP_HD constexpr int elem_m2(int nr, int nc) {
+  return (node_di(nc) - node_di(nr) + 1) + 3 * (node_dj(nc) - node_dj(nr) + 1) + 9;
+}
+
+// Row NR of the 2-D element matrix in block B (the SSA terms of
+// compute_element_matrix: block_term without the vertical ones).
+template <int NR, int B>
+BP_HD void row_element2(const RefTables& T, const double* qpe, double* acc) {
+  double K[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int p = 0; p < 4; ++p) {
+    const double* q = qpe + p * 10;
+    const double f = BP_LD_RO(q + 0);
+    const double i11 = BP_LD_RO(q + 1), i12 = BP_LD_RO(q + 2), i21 = BP_LD_RO(q + 3), i22 = BP_LD_RO(q + 4);
+    double ax[4], ay[4];
+#pragma unroll
+    for (int n = 0; n < 4; ++n) {
+      ax[n] = BP_FMA(i12, T.dyr2[p][n], i11 * T.dxr2[p][n]);
+      ay[n] = BP_FMA(i22, T.dyr2[p][n], i21 * T.dxr2[p][n]);
+    }
+#pragma unroll
+    for (int nc = 0; nc < 4; ++nc)
+      K[nc] = BP_FMA(f, block_term<B>(ax[NR], ay[NR], 0.0, ax[nc], ay[nc], 0.0), K[nc]);
+  }
+#pragma unroll
+  for (int nc = 0; nc < 4; ++nc) acc[elem_m2(NR, nc)] += K[nc];
+}
+
+// The row of column col in block B gathered from its incident cells in the
+// reference's element order (element_to_global_matrix_2d :8058-8121).
+template <int B>
+BP_HD void row_assemble2(const DevView& v, const RefTables& T, int col, double* acc) {
+  const int nc = v.ncols;
+#pragma unroll
+  for (int m = 0; m < 27; ++m) acc[m] = 0.0;
+  const int c0 = v.col_cells[0 * nc + col];  // the vertex is the NE corner of c0,
+  const int c1 = v.col_cells[1 * nc + col];  // NW of c1, SE of c2, SW of c3
+  const int c2 = v.col_cells[2 * nc + col];
+  const int c3 = v.col_cells[3 * nc + col];
+  if (c0 >= 0) row_element2<2, B>(T, v.qp + (size_t)c0 * 80, acc);
+  if (c1 >= 0) row_element2<3, B>(T, v.qp + (size_t)c1 * 80, acc);
+  if (c2 >= 0) row_element2<1, B>(T, v.qp + (size_t)c2 * 80, acc);
+  if (c3 >= 0) row_element2<0, B>(T, v.qp + (size_t)c3 * 80, acc);
+}
+
 // calcbeta (glissade_basal_traction.F90:67-598) at one vertex for the
 // velocity-dependent laws, from the basal velocity (u, v) in m/a: the
 // speed with its 0.01 m/a floor (:181) and optional cap (:187-189), the law

@@ -84,6 +84,7 @@ struct InstState {
   int need_true;                // mixed: the next check computes the FP64 residual
   int restart;                  // mixed, Chronopoulos-Gear: next pass restarts (beta = 0)
   int last_true_iter;           // mixed: pcg_iter of the last refinement
+  int frozen;                   // SSA on a no-slip bed: velocity zero, no linear solve
 };
 
 // Global counters polled by the host.
@@ -104,6 +105,7 @@ struct DevView {
   int minb_k;              // Krylov matvecs (k_std_mv, k_cg_mv): the same, 0, 4 or 6
   int grid_k;              // CTAs of the Krylov matvecs (0 = one per tile)
   int dry;                 // autotuner pass: Krylov matvecs run every tile, leave the state alone
+  int ssa;                 // shallow-shelf 2-D solve: nz = 1, one 2-D element per cell
   unsigned long long* mv_nodes;  // [2] nodes through FP64 / FP32 Krylov matvecs (timing runs), or null
   const InstParams* inst;
   InstState* st;

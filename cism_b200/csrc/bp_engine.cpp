@@ -137,6 +137,7 @@ DevView make_view(Arena& a, cudaStream_t s, const HostPlan& p, bool with_cells, 
   DevView v;
   std::memset(&v, 0, sizeof(v));
   v.nz = p.nz; v.ncols = p.ncols; v.nnodes = p.nnodes; v.npad = p.npad;
+  v.ssa = p.ssa ? 1 : 0;
   v.ncells = p.ncells; v.nelem = p.nelem; v.ninst = p.ninst; v.ntiles = p.ntiles;
   int anyd = 0;
   for (uint8_t m : p.dmask) anyd |= (m != 0);
@@ -786,6 +787,10 @@ int bp_problem_diagnostics(bp_problem* P, int which_bfric, double* const* tau_xz
   bool want_tau = false;
   for (auto o : outs) want_tau = want_tau || o;
   if (!p.ncells) return BP_ERR_ARGS;  // matrix-level problems have no elements
+  if (p.ssa && want_tau) {  // the 3-D stress routine's SSA branch is not restated
+    c->err = "bp_problem_diagnostics: element stresses of 3-D Blatter-Pattyn solves only";
+    return BP_ERR_ARGS;
+  }
   const size_t ne = (size_t)p.nelem, nb = (size_t)std::max(p.ncells, p.ncols);
   double* d = P->arena->get<double>(c->stream, "diagnostics", (want_tau ? 6 * ne : 0) + nb);
   double* d_tau = want_tau ? d : nullptr;
@@ -1054,6 +1059,10 @@ int bp_assemble(bp_ctx* c, const bp_inputs* in, const double* uvel,
   std::string e;
   if (!build_plan(in, 1, &p, &e)) {
     c->err = e;
+    return BP_ERR_ARGS;
+  }
+  if (p.ssa) {  // the 2-D system has the 9-entry reference layout, not this one
+    c->err = "bp_assemble: 3-D Blatter-Pattyn systems only";
     return BP_ERR_ARGS;
   }
   DevView v = make_view(c->arena, c->stream, p, true, false);

@@ -253,14 +253,44 @@ __global__ void __launch_bounds__(256) k_asm_qp(DevView v) {
   if (p == 0) v.efvs[e] = s / 8.0;
 }
 
+// Pass 1 of the shallow-shelf assembly: one thread per (active cell, 2-D
+// point), the cell's viscosity the mean of its 4 points (:5539-5545).
+__global__ void __launch_bounds__(256) k_asm2_qp(DevView v) {
+  const long gtid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = (int)(gtid >> 2), p = (int)(gtid & 3);
+  bool valid = c < v.ncells;
+  int inst = 0;
+  if (valid) {
+    inst = v.cell_inst[c];
+    valid = v.st[inst].picard_active != 0;
+  }
+  const unsigned mask = __ballot_sync(0xffffffffu, valid);
+  if (!valid) return;
+  double out[5], eq = 0.0;
+  if (!qp2_element_point(v, c_T, c, p, out, &eq)) {
+    atomicExch(&v.st[inst].status, BP_ERR_SINGULAR_JAC);
+    eq = 0.0;
+    for (int i = 0; i < 5; ++i) out[i] = 0.0;
+  }
+  double* dst = v.qp + ((size_t)c * 8 + p) * 10;
+  for (int i = 0; i < 5; ++i) dst[i] = out[i];
+  const int lane0 = (threadIdx.x & 31) & ~3;
+  double sum = 0.0;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) sum += __shfl_sync(mask, eq, lane0 + q);
+  if (p == 0) v.efvs[c] = sum / 4.0;
+}
+
+
 // ---------------------------------------------------------------------
 // Assembly pass 2 + basal BC + Dirichlet BC: thread = (block B, node).
 // ---------------------------------------------------------------------
-template <int B>
+template <int B, bool SSA>
 __device__ __forceinline__ bool asm_row(const DevView& v, int n) {
   const int col = n / v.nz, k = n - col * v.nz;
   double acc[27];
-  row_assemble<B>(v, c_T, col, k, acc);
+  if (SSA) row_assemble2<B>(v, c_T, col, acc);
+  else row_assemble<B>(v, c_T, col, k, acc);
   row_basal<B>(v, c_T, col, k, acc);
   const double adj = row_dirichlet<B>(v, col, k, acc);
   bool nz = false;
@@ -280,6 +310,8 @@ __device__ __forceinline__ bool asm_row(const DevView& v, int n) {
   return nz;
 }
 
+// SSA: the 2-D rows of the shallow-shelf solve (nz = 1).
+template <bool SSA>
 __global__ void __launch_bounds__(kTile) k_asm_rows(DevView v) {
   const int B = blockIdx.y;
   for (int t = blockIdx.x; t < v.ntiles; t += gridDim.x) {
@@ -289,10 +321,10 @@ __global__ void __launch_bounds__(kTile) k_asm_rows(DevView v) {
     int nzl = 0;
     if (n < R.nend) {
       switch (B) {
-        case 0: nzl = asm_row<0>(v, n); break;
-        case 1: nzl = asm_row<1>(v, n); break;
-        case 2: nzl = asm_row<2>(v, n); break;
-        default: nzl = asm_row<3>(v, n); break;
+        case 0: nzl = asm_row<0, SSA>(v, n); break;
+        case 1: nzl = asm_row<1, SSA>(v, n); break;
+        case 2: nzl = asm_row<2, SSA>(v, n); break;
+        default: nzl = asm_row<3, SSA>(v, n); break;
       }
     }
     if (__syncthreads_or(nzl) && threadIdx.x == 0) atomicOr(&v.st[R.inst].nonzero, 1);
@@ -338,6 +370,18 @@ __global__ void __launch_bounds__(kTile) k_rhs(DevView v) {
         S.status = BP_ZERO_MATRIX;
         S.zero_x = 1;
         fail(v, S, BP_ZERO_MATRIX);
+      } else if (v.ssa && v.inst[inst].which_babc == 6) {
+        // SSA on a no-slip bed: the velocity is zero and nothing is solved
+        // (glissade_velo_higher.F90:3227-3240)
+        S.frozen = 1;
+        S.L2_norm = 0.0;
+        S.L2_rel = 0.0;
+        S.pcg_iter = 0;
+        pcg_stop(v, S, true);
+        if (S.refine_active) {
+          S.refine_active = 0;
+          atomicSub(&v.cnt->refine_active, 1);
+        }
       }
     });
   }
@@ -762,9 +806,11 @@ __global__ void __launch_bounds__(kTile) k_picard_check(DevView v) {
     }
     if (!S.picard_active) continue;
     const bool meanu = ip.which_resid == 2;
-    const bool nobed = ip.which_resid == 1 || meanu;
+    // the 2-D criterion has no bed layer to leave out (:9238-9351)
+    const bool nobed = !v.ssa && (ip.which_resid == 1 || meanu);
     double part[2] = {0.0, 0.0};
     if (n < R.nend) {
+      if (S.frozen) v.x[n] = make_double2(0.0, 0.0);  // SSA on a no-slip bed
       const int k = n % v.nz;
       if (!(nobed && k == v.nz - 1)) {
         const double2 x = v.x[n], o = v.usav[n];
@@ -920,14 +966,20 @@ void launch_slide_beta(const DevView& v, cudaStream_t s) {
   if (v.ncells > 0) k_cell_beta<<<(v.ncells + kTile - 1) / kTile, kTile, 0, s>>>(v);
 }
 void launch_asm_qp(const DevView& v, cudaStream_t s) {
-  if (v.nelem > 0) {
+  if (v.ssa) {
+    if (v.ncells > 0) {
+      const long threads = (long)v.ncells * 4;
+      k_asm2_qp<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(v);
+    }
+  } else if (v.nelem > 0) {
     const long threads = (long)v.nelem * 8;
     k_asm_qp<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(v);
   }
 }
 void launch_asm_rows(const DevView& v, cudaStream_t s) {
   dim3 g(tile_grid(v), 4);
-  k_asm_rows<<<g, kTile, 0, s>>>(v);
+  if (v.ssa) k_asm_rows<true><<<g, kTile, 0, s>>>(v);
+  else k_asm_rows<false><<<g, kTile, 0, s>>>(v);
 }
 void launch_rhs(const DevView& v, cudaStream_t s) { k_rhs<<<tile_grid(v), kTile, 0, s>>>(v); }
 void launch_assemble(const DevView& v, cudaStream_t s) {

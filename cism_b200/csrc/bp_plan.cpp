@@ -85,6 +85,7 @@ bool build_column_plan(int nx, int ny, int nz, int periodic,
   }
   *p = HostPlan();
   p->nz = nz;
+  p->nz_out = nz;
   p->ninst = 1;
   p->inst.resize(1);
   std::memset(&p->inst[0], 0, sizeof(InstParams));
@@ -224,9 +225,14 @@ void slide_vertex(const bp_sliding& L, int i, int j, int nx, double* c1, double*
 bool build_plan(const bp_inputs* in, int n, HostPlan* p, std::string* err) {
   if (n < 1 || !in) { *err = "no instances"; return false; }
   *p = HostPlan();
-  const int nz = in[0].nz;
-  if (nz < 2 || nz > kNzMax) { *err = "nz out of range (2..64)"; return false; }
+  const int nz_in = in[0].nz;
+  if (nz_in < 2 || nz_in > kNzMax) { *err = "nz out of range (2..64)"; return false; }
+  // the shallow-shelf solve has one unknown pair per column (solve_2d)
+  const bool ssa = in[0].approx_ssa != 0;
+  const int nz = ssa ? 1 : nz_in;
   p->nz = nz;
+  p->nz_out = nz_in;
+  p->ssa = ssa;
   p->ninst = n;
   p->inst.resize(n);
   std::vector<std::vector<std::pair<int, int>>> cols(n);
@@ -235,7 +241,12 @@ bool build_plan(const bp_inputs* in, int n, HostPlan* p, std::string* err) {
   // pass 1: columns and cells of every instance
   for (int b = 0; b < n; ++b) {
     const bp_inputs& I = in[b];
-    if (I.nz != nz) { *err = "all instances of a batch must share nz"; return false; }
+    if (I.nz != nz_in) { *err = "all instances of a batch must share nz"; return false; }
+    if ((I.approx_ssa != 0) != ssa) { *err = "all instances of a batch must share the approximation"; return false; }
+    if (ssa && I.which_precond == 2) {
+      *err = "the shallow-shelf solve takes which_precond 0 or 1";
+      return false;
+    }
     if (I.nhalo != 2) { *err = "nhalo must be 2"; return false; }
     if (I.nx < 6 || I.ny < 6) { *err = "grid too small"; return false; }
     if (I.pcg_variant != in[0].pcg_variant || I.pcg_ncheck != in[0].pcg_ncheck ||
@@ -297,14 +308,14 @@ bool build_plan(const bp_inputs* in, int n, HostPlan* p, std::string* err) {
     p->ncells += (int)cells[b].size();
   }
   const int NCELL = p->ncells;
-  p->nelem = NCELL * (nz - 1);
+  p->nelem = ssa ? NCELL : NCELL * (nz - 1);  // SSA: one 2-D element per cell
   p->cell_inst.resize(NCELL);
   p->cell_ij.resize(2 * (size_t)NCELL);
   p->cell_cols.resize(4 * (size_t)NCELL);
   p->cell_s.resize(4 * (size_t)NCELL);
   p->cell_h.resize(4 * (size_t)NCELL);
   p->cell_beta.resize(4 * (size_t)NCELL);
-  p->flwafact.resize((size_t)NCELL * (nz - 1));
+  p->flwafact.resize((size_t)p->nelem);
   int col_base = 0, cell_base = 0;
   for (int b = 0; b < n; ++b) {
     const bp_inputs& I = in[b];
@@ -315,7 +326,7 @@ bool build_plan(const bp_inputs* in, int n, HostPlan* p, std::string* err) {
     ip.efvs_constant = I.efvs_constant;
     ip.pcg_tol = I.pcg_tol;
     ip.inner_tol = I.inner_tol > 0.0 ? I.inner_tol : 1.0e-4;
-    for (int k = 0; k < nz; ++k) ip.sigma[k] = I.sigma[k];
+    for (int k = 0; k < nz_in; ++k) ip.sigma[k] = I.sigma[k];
     ip.which_efvs = I.which_efvs;
     ip.which_babc = I.which_babc;
     ip.which_assemble_beta = I.which_assemble_beta;
@@ -332,7 +343,8 @@ bool build_plan(const bp_inputs* in, int n, HostPlan* p, std::string* err) {
     ip.node_begin = col_base * nz; ip.node_end = (col_base + nc) * nz;
     const int ncl = (int)cells[b].size();
     ip.cell_begin = cell_base; ip.cell_end = cell_base + ncl;
-    ip.elem_begin = cell_base * (nz - 1); ip.elem_end = (cell_base + ncl) * (nz - 1);
+    const int epc = ssa ? 1 : nz - 1;  // elements per cell
+    ip.elem_begin = cell_base * epc; ip.elem_end = (cell_base + ncl) * epc;
     for (int c = 0; c < nc; ++c) {
       const int g = col_base + c;
       const int i = cols[b][c].first, j = cols[b][c].second;
@@ -357,11 +369,24 @@ bool build_plan(const bp_inputs* in, int n, HostPlan* p, std::string* err) {
       } else {
         p->col_beta[g] = I.beta_internal[vtx(i, j, nx)];
       }
-      for (int k = 0; k < nz; ++k) {
-        const size_t src = vtx(i, j, nx) * nz + k;
-        p->load[(size_t)g * nz + k] = double2{I.loadu[src], I.loadv[src]};
-        p->dmask[(size_t)g * nz + k] =
-            (uint8_t)((I.umask_dirichlet[src] == 1 ? 1 : 0) | (I.vmask_dirichlet[src] == 1 ? 2 : 0));
+      if (ssa) {
+        // load summed over the levels (:2123-2137); the bed level's
+        // Dirichlet masks (:2878)
+        double lu = 0.0, lv = 0.0;
+        for (int k = 0; k < nz_in; ++k) {
+          lu = lu + I.loadu[vtx(i, j, nx) * nz_in + k];
+          lv = lv + I.loadv[vtx(i, j, nx) * nz_in + k];
+        }
+        p->load[g] = double2{lu, lv};
+        const size_t bed = vtx(i, j, nx) * nz_in + (nz_in - 1);
+        p->dmask[g] = (uint8_t)((I.umask_dirichlet[bed] == 1 ? 1 : 0) | (I.vmask_dirichlet[bed] == 1 ? 2 : 0));
+      } else {
+        for (int k = 0; k < nz; ++k) {
+          const size_t src = vtx(i, j, nx) * nz + k;
+          p->load[(size_t)g * nz + k] = double2{I.loadu[src], I.loadv[src]};
+          p->dmask[(size_t)g * nz + k] =
+              (uint8_t)((I.umask_dirichlet[src] == 1 ? 1 : 0) | (I.vmask_dirichlet[src] == 1 ? 2 : 0));
+        }
       }
     }
     for (int c = 0; c < ncl; ++c) {
@@ -378,8 +403,15 @@ bool build_plan(const bp_inputs* in, int n, HostPlan* p, std::string* err) {
         p->cell_h[(size_t)q * NCELL + g] = I.stagthck[v];
         p->cell_beta[(size_t)q * NCELL + g] = I.sliding ? 0.0 : I.beta_internal[v];
       }
-      for (int k = 0; k < nz - 1; ++k)
-        p->flwafact[(size_t)g * (nz - 1) + k] = I.flwafact[cel(ic, jc, nx) * (nz - 1) + k];
+      if (ssa) {  // glissade_vertical_average (glissade_grid_operators.F90:1172-1236)
+        double f = 0.0;
+        for (int k = 0; k < nz_in - 1; ++k)
+          f = f + I.flwafact[cel(ic, jc, nx) * (nz_in - 1) + k] * (I.sigma[k + 1] - I.sigma[k]);
+        p->flwafact[g] = f;
+      } else {
+        for (int k = 0; k < nz - 1; ++k)
+          p->flwafact[(size_t)g * (nz - 1) + k] = I.flwafact[cel(ic, jc, nx) * (nz - 1) + k];
+      }
     }
     add_tiles(p, b, ip.node_begin, ip.node_end);
     col_base += nc;
@@ -395,6 +427,11 @@ void gather_velocity(const HostPlan& p, int b, const double* uvel,
   const int nx = p.nx[b], nz = p.nz, NC = p.ncols;
   for (int g = ip.col_begin; g < ip.col_end; ++g) {
     const int i = p.col_ij[g], j = p.col_ij[NC + g];
+    if (p.ssa) {  // uvel_2d = uvel(nz,:,:) (glissade_velo_higher.F90:1179-1180)
+      const size_t src = vtx(i, j, nx) * p.nz_out + (p.nz_out - 1);
+      x[g] = double2{uvel[src], vvel[src]};
+      continue;
+    }
     for (int k = 0; k < nz; ++k) {
       const size_t src = vtx(i, j, nx) * nz + k;
       x[(size_t)g * nz + k] = double2{uvel[src], vvel[src]};
@@ -419,20 +456,32 @@ void scatter_vector(const HostPlan& p, int b, const double2* x, double* vu,
 
 void scatter_velocity(const HostPlan& p, int b, const double2* x,
                       double* uvel, double* vvel) {
-  scatter_vector(p, b, x, uvel, vvel);
-  halo_stag(p.nx[b], p.ny[b], p.nz, p.periodic[b], uvel);
-  halo_stag(p.nx[b], p.ny[b], p.nz, p.periodic[b], vvel);
+  if (p.ssa) {  // the 2-D velocity on every level (:3745-3750)
+    const InstParams& ip = p.inst[b];
+    const int nx = p.nx[b], NC = p.ncols, L = p.nz_out;
+    for (int g = ip.col_begin; g < ip.col_end; ++g) {
+      const size_t w = vtx(p.col_ij[g], p.col_ij[NC + g], nx);
+      for (int k = 0; k < L; ++k) {
+        uvel[w * L + k] = x[g].x;
+        vvel[w * L + k] = x[g].y;
+      }
+    }
+  } else {
+    scatter_vector(p, b, x, uvel, vvel);
+  }
+  halo_stag(p.nx[b], p.ny[b], p.nz_out, p.periodic[b], uvel);
+  halo_stag(p.nx[b], p.ny[b], p.nz_out, p.periodic[b], vvel);
 }
 
 void scatter_efvs(const HostPlan& p, int b, const double* efvs_elem,
                   double* efvs) {
   const InstParams& ip = p.inst[b];
-  const int nx = p.nx[b], ny = p.ny[b], nz = p.nz, NCELL = p.ncells;
+  const int nx = p.nx[b], ny = p.ny[b], nz = p.nz_out, NCELL = p.ncells;
   std::memset(efvs, 0, sizeof(double) * (size_t)(nz - 1) * nx * ny);
   for (int g = ip.cell_begin; g < ip.cell_end; ++g) {
     const int ic = p.cell_ij[g], jc = p.cell_ij[NCELL + g];
-    for (int k = 0; k < nz - 1; ++k)
-      efvs[cel(ic, jc, nx) * (nz - 1) + k] = efvs_elem[(size_t)g * (nz - 1) + k];
+    for (int k = 0; k < nz - 1; ++k)  // SSA: the cell's value on every layer
+      efvs[cel(ic, jc, nx) * (nz - 1) + k] = efvs_elem[p.ssa ? (size_t)g : (size_t)g * (nz - 1) + k];
   }
 }
 

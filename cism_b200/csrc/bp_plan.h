@@ -23,7 +23,9 @@ OwnedRange owned_range(int nx, int ny, int periodic);
 int vertex_image(int i, int n, int periodic);
 
 struct HostPlan {
-  int nz = 0, ninst = 0;
+  int nz = 0, ninst = 0;   // nz: levels of the solve (1 for the shallow-shelf solve)
+  int nz_out = 0;          // levels of the velocity arrays (the model's nz)
+  bool ssa = false;        // shallow-shelf 2-D solve
   int ncols = 0, nnodes = 0, npad = 0, ncells = 0, nelem = 0, ntiles = 0;
   std::vector<InstParams> inst;
   std::vector<int> col_inst, col_nbr, col_cells, col_ij;

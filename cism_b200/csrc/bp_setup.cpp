@@ -413,6 +413,7 @@ extern "C" int bp_setup(const bp_model* m, bp_setup_arrays* o, double* uvel,
     in->pcg_maxiters = m->pcg_maxiters; in->pcg_ncheck = m->pcg_ncheck; in->pcg_tol = m->pcg_tol;
     in->precision = m->precision; in->inner_tol = m->inner_tol;
     in->sliding = m->sliding ? &o->sliding : nullptr;
+    in->approx_ssa = m->approx_ssa;
   }
   return BP_OK;
 }

@@ -69,7 +69,7 @@ class Inputs(C.Structure):
         ("which_assemble_beta", C.c_int), ("which_resid", C.c_int), ("pcg_variant", C.c_int),
         ("which_precond", C.c_int), ("maxiter_nonlinear", C.c_int), ("pcg_maxiters", C.c_int),
         ("pcg_ncheck", C.c_int), ("pcg_tol", C.c_double), ("precision", C.c_int),
-        ("inner_tol", C.c_double), ("sliding", C.POINTER(Sliding)),
+        ("inner_tol", C.c_double), ("sliding", C.POINTER(Sliding)), ("approx_ssa", C.c_int),
     ]
 
 
@@ -103,7 +103,7 @@ class Model(C.Structure):
         ("which_assemble_taud", C.c_int), ("which_ground", C.c_int),
         ("maxiter_nonlinear", C.c_int), ("pcg_maxiters", C.c_int), ("pcg_ncheck", C.c_int),
         ("pcg_tol", C.c_double), ("precision", C.c_int), ("inner_tol", C.c_double),
-        ("sliding", C.POINTER(Sliding)),
+        ("sliding", C.POINTER(Sliding)), ("approx_ssa", C.c_int),
     ]
 
 
@@ -207,6 +207,7 @@ def make_model_struct(m: configs.BPModel, precision: int = FP64, inner_tol: floa
         setattr(s, name, getattr(m, name))
     s.precision = precision
     s.inner_tol = inner_tol
+    s.approx_ssa = m.approx_ssa
     s.sliding = C.cast(None, C.POINTER(Sliding))
     if m.sliding is not None:
         if m.which_babc != m.sliding.law:

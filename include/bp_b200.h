@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define BP_ABI_VERSION 2
+#define BP_ABI_VERSION 3
 
 typedef struct bp_ctx bp_ctx;
 
@@ -126,6 +126,11 @@ typedef struct {
                                    (FP32-matrix Krylov solve between two FP64
                                    residuals; <= 0: 1e-4) */
   const bp_sliding *sliding;    /* NULL: beta_internal, fixed over the Picard loop */
+  int approx_ssa;               /* 1: shallow-shelf 2-D solve (whichapprox = HO_APPROX_SSA,
+                                   :1125-1128): one unknown pair per column, the
+                                   result copied to every level; 0: 3-D
+                                   Blatter-Pattyn.  Shared by a batch; the SSA
+                                   takes which_precond 0 or 1 */
 } bp_inputs;
 
 typedef struct {
@@ -295,6 +300,7 @@ typedef struct {
    * bp_setup computes its f_ground and flwa_basal_stag and takes topg, eus
    * and beta_grounded_min from this struct's fields above */
   const bp_sliding *sliding;
+  int approx_ssa;               /* as in bp_inputs */
 } bp_model;
 
 /* Caller-allocated outputs of the setup (sizes as in bp_inputs). */

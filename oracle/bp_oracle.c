@@ -1686,6 +1686,52 @@ static double residual_velocity_2d(int nx, int ny, int periodic, int whichresid,
   return r;
 }
 
+/* One assembled 2-D system of the SSA branch at (u2, v2) (nx-1,ny-1): the
+ * matrix in the kA = 0 slice of (27,1,nx-1,ny-1), b = the level-summed
+ * load with the basal term and the Dirichlet rows of the bed level's
+ * masks, halo-updated and symmetry-checked (:2703-2990). */
+int orc_assemble_ssa_system(const orc_model *m, const orc_setup *s,
+                            const double *beta_internal, const double *u2,
+                            const double *v2, double *efvs, double *Auu,
+                            double *Auv, double *Avu, double *Avv, double *bu,
+                            double *bv, long *nNonzeros) {
+  const int nx = m->nx, ny = m->ny, nz = m->nz;
+  const size_t nvx = (size_t)(nx - 1) * (ny - 1);
+  int st = assemble_ssa(nx, ny, nz, m->nhalo, s->sigma, s->active_cell, s->xVertex, s->yVertex, u2,
+                        v2, s->stagthck, s->flwafact, m->which_efvs, m->efvs_constant, efvs, Auu, Auv,
+                        Avu, Avv);
+  if (st != ORC_OK) return st;
+  if (m->which_babc != ORC_BABC_NO_SLIP)
+    basal_sliding_bc(nx, ny, 1, m->nhalo, m->dx, m->dy, s->active_cell, s->active_vertex,
+                     beta_internal, s->xVertex, s->yVertex, m->which_assemble_beta, Auu, Avv);
+  int *um = calloc(nvx, sizeof(int)), *vm = calloc(nvx, sizeof(int));
+  for (int j = 1; j <= ny - 1; ++j)
+    for (int i = 1; i <= nx - 1; ++i) {
+      const size_t w = IV(i, j);
+      double lu = 0.0, lv = 0.0;
+      for (int k = 1; k <= nz; ++k) {
+        lu = lu + s->loadu[IX(k, i, j)];
+        lv = lv + s->loadv[IX(k, i, j)];
+      }
+      bu[w] = lu;
+      bv[w] = lv;
+      um[w] = s->umask_dirichlet[IX(nz, i, j)];
+      vm[w] = s->vmask_dirichlet[IX(nz, i, j)];
+    }
+  dirichlet_bc_3d(nx, ny, 1, m->nhalo, s->active_vertex, um, vm, u2, v2, Auu, Auv, Avu, Avv, bu, bv);
+  free(um);
+  free(vm);
+  orc_halo_stag(nx, ny, 27, m->periodic, Auu);
+  orc_halo_stag(nx, ny, 27, m->periodic, Auv);
+  orc_halo_stag(nx, ny, 27, m->periodic, Avu);
+  orc_halo_stag(nx, ny, 27, m->periodic, Avv);
+  orc_halo_stag(nx, ny, 1, m->periodic, bu);
+  orc_halo_stag(nx, ny, 1, m->periodic, bv);
+  check_symmetry_assembled_3d(nx, ny, 1, m->periodic, s->active_vertex, Auu, Auv, Avu, Avv);
+  *nNonzeros = count_nonzeros_3d(nx, ny, 1, m->periodic, s->active_vertex, Auu, Auv, Avu, Avv);
+  return ORC_OK;
+}
+
 int orc_velo_ssa_solve(const orc_model *m, double *uvel, double *vvel,
                        double *efvs, double *beta_internal, orc_stats *stats) {
   const int nx = m->nx, ny = m->ny, nz = m->nz;
@@ -1697,21 +1743,12 @@ int orc_velo_ssa_solve(const orc_model *m, double *uvel, double *vvel,
   if (st != ORC_OK) { orc_setup_free(&s); stats->status = st; return st; }
   double *Auu = xalloc(nA * 8), *Auv = xalloc(nA * 8), *Avu = xalloc(nA * 8),
          *Avv = xalloc(nA * 8), *bu = xalloc(nvx * 8), *bv = xalloc(nvx * 8),
-         *lu = xalloc(nvx * 8), *lv = xalloc(nvx * 8), *u2 = xalloc(nvx * 8),
-         *v2 = xalloc(nvx * 8), *us = xalloc(nvx * 8), *vs = xalloc(nvx * 8),
-         *u3 = xalloc(n3 * 8), *v3 = xalloc(n3 * 8);
-  int *um = calloc(nvx, sizeof(int)), *vm = calloc(nvx, sizeof(int));
+         *u2 = xalloc(nvx * 8), *v2 = xalloc(nvx * 8), *us = xalloc(nvx * 8),
+         *vs = xalloc(nvx * 8), *u3 = xalloc(n3 * 8), *v3 = xalloc(n3 * 8);
   for (int j = 1; j <= ny - 1; ++j)
     for (int i = 1; i <= nx - 1; ++i) {
-      const size_t w = IV(i, j);
-      for (int k = 1; k <= nz; ++k) {  /* loadu_2d = sum over levels (:2123-2137) */
-        lu[w] = lu[w] + s.loadu[IX(k, i, j)];
-        lv[w] = lv[w] + s.loadv[IX(k, i, j)];
-      }
-      u2[w] = uvel[IX(nz, i, j)];  /* uvel_2d = uvel(nz,:,:) (:1179-1180) */
-      v2[w] = vvel[IX(nz, i, j)];
-      um[w] = s.umask_dirichlet[IX(nz, i, j)];  /* the bed level's masks (:2878) */
-      vm[w] = s.vmask_dirichlet[IX(nz, i, j)];
+      u2[IV(i, j)] = uvel[IX(nz, i, j)];  /* uvel_2d = uvel(nz,:,:) (:1179-1180) */
+      v2[IV(i, j)] = vvel[IX(nz, i, j)];
     }
   int counter = 0;
   double outer_it_criterion = 1.0e10, outer_it_target = 1.0e-12;
@@ -1725,24 +1762,9 @@ int orc_velo_ssa_solve(const orc_model *m, double *uvel, double *vvel,
     if (st != ORC_OK) { status = st; break; }
     memcpy(us, u2, nvx * 8);
     memcpy(vs, v2, nvx * 8);
-    st = assemble_ssa(nx, ny, nz, m->nhalo, s.sigma, s.active_cell, s.xVertex, s.yVertex, u2, v2,
-                      s.stagthck, s.flwafact, m->which_efvs, m->efvs_constant, efvs, Auu, Auv, Avu,
-                      Avv);
+    long nnz = 0;
+    st = orc_assemble_ssa_system(m, &s, beta_internal, u2, v2, efvs, Auu, Auv, Avu, Avv, bu, bv, &nnz);
     if (st != ORC_OK) { status = st; break; }
-    if (m->which_babc != ORC_BABC_NO_SLIP)
-      basal_sliding_bc(nx, ny, 1, m->nhalo, m->dx, m->dy, s.active_cell, s.active_vertex,
-                       beta_internal, s.xVertex, s.yVertex, m->which_assemble_beta, Auu, Avv);
-    memcpy(bu, lu, nvx * 8);
-    memcpy(bv, lv, nvx * 8);
-    dirichlet_bc_3d(nx, ny, 1, m->nhalo, s.active_vertex, um, vm, u2, v2, Auu, Auv, Avu, Avv, bu, bv);
-    orc_halo_stag(nx, ny, 27, m->periodic, Auu);
-    orc_halo_stag(nx, ny, 27, m->periodic, Auv);
-    orc_halo_stag(nx, ny, 27, m->periodic, Avu);
-    orc_halo_stag(nx, ny, 27, m->periodic, Avv);
-    orc_halo_stag(nx, ny, 1, m->periodic, bu);
-    orc_halo_stag(nx, ny, 1, m->periodic, bv);
-    check_symmetry_assembled_3d(nx, ny, 1, m->periodic, s.active_vertex, Auu, Auv, Avu, Avv);
-    long nnz = count_nonzeros_3d(nx, ny, 1, m->periodic, s.active_vertex, Auu, Auv, Avu, Avv);
     if (nnz == 0) {
       memset(u2, 0, nvx * 8);
       memset(v2, 0, nvx * 8);
@@ -1794,8 +1816,8 @@ int orc_velo_ssa_solve(const orc_model *m, double *uvel, double *vvel,
   stats->converged = (status == ORC_OK && counter < m->maxiter_nonlinear) ? 1 : 0;
   if (status == ORC_OK && !stats->converged) status = ORC_WARN_PICARD_NOT_CONVERGED;
   stats->status = status;
-  free(Auu); free(Auv); free(Avu); free(Avv); free(bu); free(bv); free(lu); free(lv);
-  free(u2); free(v2); free(us); free(vs); free(u3); free(v3); free(um); free(vm);
+  free(Auu); free(Auv); free(Avu); free(Avv); free(bu); free(bv);
+  free(u2); free(v2); free(us); free(vs); free(u3); free(v3);
   orc_setup_free(&s);
   return status;
 }

@@ -207,6 +207,14 @@ int orc_assemble_system(const orc_model *m, const orc_setup *s,
                         const double *vvel, double *efvs, double *Auu,
                         double *Auv, double *Avu, double *Avv, double *bu,
                         double *bv, long *nNonzeros);
+/* One assembled 2-D system of the shallow-shelf branch at a 2-D velocity
+ * ((nx-1,ny-1) arrays; the matrix in the kA = 0 slice of
+ * (27,1,nx-1,ny-1)). */
+int orc_assemble_ssa_system(const orc_model *m, const orc_setup *s,
+                            const double *beta_internal, const double *u2,
+                            const double *v2, double *efvs, double *Auu,
+                            double *Auv, double *Avu, double *Avv, double *bu,
+                            double *bv, long *nNonzeros);
 /* Whole glissade_velo_higher_solve, 3-D Blatter-Pattyn branch. */
 int orc_velo_higher_solve(const orc_model *m, double *uvel, double *vvel,
                           double *efvs, double *beta_internal,

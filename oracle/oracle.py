@@ -253,6 +253,24 @@ def basal_friction_heatflx(m, su, uvel, vvel, beta, which=1):
     return out
 
 
+def assemble_ssa_system(m, su, beta, u2, v2):
+    """One assembled shallow-shelf system at the 2-D velocity (u2, v2)
+    (ny-1, nx-1): A as four (ny-1, nx-1, 1, 27) arrays, b, efvs, nonzeros."""
+    keep, om, s = su["_keep"]
+    nx, ny, nz = m.nx, m.ny, m.nz
+    A = [np.zeros((ny - 1, nx - 1, 1, 27)) for _ in range(4)]
+    bu, bv = np.zeros((ny - 1, nx - 1)), np.zeros((ny - 1, nx - 1))
+    efvs = np.zeros((ny, nx, nz - 1))
+    nnz = C.c_long(0)
+    rc = lib().orc_assemble_ssa_system(C.byref(om), C.byref(s), _p(np.ascontiguousarray(beta, np.float64)),
+                                       _p(np.ascontiguousarray(u2, np.float64)),
+                                       _p(np.ascontiguousarray(v2, np.float64)), _p(efvs),
+                                       *[_p(a) for a in A], _p(bu), _p(bv), C.byref(nnz))
+    if rc != 0:
+        raise RuntimeError(f"orc_assemble_ssa_system failed: {rc}")
+    return A, bu, bv, efvs, nnz.value
+
+
 def matvec(m, active_vertex, A, xu, xv):
     nx, ny, nz = m.nx, m.ny, m.nz
     yu, yv = np.zeros((ny - 1, nx - 1, nz)), np.zeros((ny - 1, nx - 1, nz))

@@ -261,3 +261,63 @@ extern "C" int emu_diagnostics(const bp_inputs* in, const double* uvel, const do
   scatter_bfric(E.p, 0, which, bf.data(), bfricflx);
   return 0;
 }
+
+// One assembled shallow-shelf system at velocity (uvel, vvel) (the bed
+// level is the 2-D velocity) through the device's 2-D bodies: the matrix
+// in (27,1,nx-1,ny-1) and b (nx-1,ny-1); efvs (nz-1,nx,ny).  10 if the plan
+// rejects the inputs or they are not a shallow-shelf problem, 2 for a
+// singular Jacobian.
+extern "C" int emu_assemble_ssa(const bp_inputs* in, const double* uvel, const double* vvel,
+                                double* Auu, double* Auv, double* Avu, double* Avv, double* bu,
+                                double* bv, double* efvs) {
+  Emu E;
+  std::string err;
+  if (!build_plan(in, 1, &E.p, &err) || !E.p.ssa) return 10;
+  E.bind();
+  E.v.ssa = 1;
+  gather_velocity(E.p, 0, uvel, vvel, E.x.data());
+  RefTables T;
+  fill_ref_tables(&T);
+  for (int c = 0; c < E.p.ncells; ++c) {
+    double s = 0.0;
+    for (int p = 0; p < 4; ++p) {
+      double out[5], eq = 0.0;
+      if (!qp2_element_point(E.v, T, c, p, out, &eq)) return 2;
+      std::memcpy(&E.qp[((size_t)c * 8 + p) * 10], out, sizeof(out));
+      s += eq;
+    }
+    E.efvs[c] = s / 4.0;
+  }
+  const DevView& v = E.v;
+  double* Ad = reinterpret_cast<double*>(E.A.data());
+  for (int B = 0; B < 4; ++B)
+    for (int n = 0; n < v.nnodes; ++n) {
+      double acc[27];
+      double adj = 0.0;
+      switch (B) {
+        case 0: row_assemble2<0>(v, T, n, acc); row_basal<0>(v, T, n, 0, acc); adj = row_dirichlet<0>(v, n, 0, acc); break;
+        case 1: row_assemble2<1>(v, T, n, acc); row_basal<1>(v, T, n, 0, acc); adj = row_dirichlet<1>(v, n, 0, acc); break;
+        case 2: row_assemble2<2>(v, T, n, acc); row_basal<2>(v, T, n, 0, acc); adj = row_dirichlet<2>(v, n, 0, acc); break;
+        default: row_assemble2<3>(v, T, n, acc); row_basal<3>(v, T, n, 0, acc); adj = row_dirichlet<3>(v, n, 0, acc); break;
+      }
+      for (int m = 0; m < 27; ++m)
+        Ad[(((size_t)((B >> 1) * 27 + m)) * v.npad + n) * 2 + (B & 1)] = acc[m];
+      E.badj[(size_t)B * v.npad + n] = adj;
+    }
+  const size_t np = E.p.npad;
+  for (int n = 0; n < E.p.nnodes; ++n) {
+    const uint8_t dm = E.p.dmask[n];
+    double u = E.p.load[n].x - E.badj[n] - E.badj[np + n];
+    double w = E.p.load[n].y - E.badj[2 * np + n] - E.badj[3 * np + n];
+    if (dm & 1) u = E.x[n].x;
+    if (dm & 2) w = E.x[n].y;
+    E.b[n] = double2{u, w};
+  }
+  scatter_matrix(E.p, E.A.data(), Auu, Auv, Avu, Avv);
+  const size_t tot = (size_t)(in->nx - 1) * (in->ny - 1);
+  std::memset(bu, 0, tot * 8);
+  std::memset(bv, 0, tot * 8);
+  scatter_vector(E.p, 0, E.b.data(), bu, bv);
+  scatter_efvs(E.p, 0, E.efvs.data(), efvs);
+  return 0;
+}

@@ -10,13 +10,21 @@ u = rho g H tan(theta) / beta - rho g H A k cos(kx) / (4 eta H k^2 + beta):
 the uniform part exactly (no strain), the Fourier mode to the bilinear
 elements' second order.
 """
+import ctypes as C
 import math
+import os
 
 import numpy as np
 import pytest
 
-from cism_b200 import configs
+from cism_b200 import configs, solver
 from oracle import oracle
+
+from helpers import owned_active_rows, random_state
+
+EMU = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "tests", "hostemu",
+                   "libhostemu.so")
+_dp = C.POINTER(C.c_double)
 
 RHO_G = 910.0 * 9.81
 
@@ -89,3 +97,65 @@ def test_ssa_on_a_frozen_bed_is_zero():
     u, v, _, _, st = oracle.velo_ssa_solve(m)
     assert st["picard_iters"] == 1
     assert np.all(u == 0.0) and np.all(v == 0.0)
+
+
+def _p(a):
+    return a.ctypes.data_as(_dp)
+
+
+def _ssa_models():
+    m1, _, _, _ = _fourier_slab(24, which_efvs=configs.EFVS_NONLINEAR)
+    m1.name = "fourier_slab_glen"
+    m2 = configs.dome().copy(which_babc=configs.BABC_BETA_EXTERNAL)
+    m2.beta_external = np.full_like(m2.beta_external, 400.0)
+    m2.name = "dome_sliding"
+    m3 = configs.marine(n=32, dx=4000.0).copy(periodic=0, which_assemble_beta=configs.ASSEMBLE_STANDARD)
+    m3.name = "marine_outflow_standard_beta"
+    m4 = configs.dome(n=20).copy(which_babc=configs.BABC_BETA_EXTERNAL, which_efvs=configs.EFVS_FLOWFACT)
+    m4.beta_external = np.full_like(m4.beta_external, 200.0)
+    m4.kinbcmask = np.zeros((m4.ny - 1, m4.nx - 1), np.int32)
+    m4.kinbcmask[9:11, 9:11] = 1
+    m4.name = "dome_kinematic_flowfact"
+    return [m.copy(approx_ssa=1) for m in (m1, m2, m3, m4)]
+
+
+@pytest.mark.parametrize("m", _ssa_models(), ids=lambda m: m.name)
+def test_device_ssa_bodies_match_oracle(m):
+    """The device's 2-D assembly bodies (pass 1 per cell and point, the
+    9-point rows with the basal and Dirichlet terms) on the host plan,
+    compiled for the CPU, against the oracle's assembled shallow-shelf
+    system at a random velocity: 1e-13 relative."""
+    emu = C.CDLL(EMU)
+    prep, _, _ = solver.prepare(m)
+    su = oracle.setup(m)
+    u, v = random_state(m, su, seed=5, scale=30.0)
+    A, bu, bv, efvs, nnz = oracle.assemble_ssa_system(m, su, su["beta_internal"], u[..., -1], v[..., -1])
+    shp = (m.ny - 1, m.nx - 1, 1, 27)
+    E = [np.zeros(shp) for _ in range(4)]
+    ebu, ebv = np.zeros((m.ny - 1, m.nx - 1)), np.zeros((m.ny - 1, m.nx - 1))
+    eef = np.zeros((m.ny, m.nx, m.nz - 1))
+    rc = emu.emu_assemble_ssa(C.byref(prep.inputs), _p(np.ascontiguousarray(u)), _p(np.ascontiguousarray(v)),
+                              *[_p(a) for a in E], _p(ebu), _p(ebv), _p(eef))
+    assert rc == 0
+    rows = owned_active_rows(m, su["active_vertex"])
+    for a, e in zip(A, E):
+        assert np.max(np.abs(a[rows] - e[rows])) <= 1e-13 * np.max(np.abs(a[rows]))
+    scale = max(np.max(np.abs(bu[rows])), np.max(np.abs(bv[rows])))
+    assert np.max(np.abs(ebu[rows] - bu[rows])) <= 1e-13 * scale
+    assert np.max(np.abs(ebv[rows] - bv[rows])) <= 1e-13 * scale
+    assert np.max(np.abs(eef - efvs)) <= 1e-13 * np.max(np.abs(efvs))
+    # only the horizontal (kA = 0) entries are set: a 9-point operator
+    for e in E:
+        assert not np.any(e[..., :9]) and not np.any(e[..., 18:])
+
+
+def test_ssa_refuses_the_column_preconditioner():
+    """The reference's 2-D preconditioner setup knows the diagonal only
+    (setup_preconditioner_2d, glissade_velo_higher_pcg.F90:2269-2329); the
+    plan refuses which_precond = 2 for the shallow-shelf solve."""
+    emu = C.CDLL(EMU)
+    m = _ssa_models()[1]
+    prep, _, _ = solver.prepare(m.copy(which_precond=configs.PRECOND_SIA))
+    out = np.zeros((m.ny - 1, m.nx - 1))
+    u = np.zeros(m.vshape3)
+    assert emu.emu_slide_beta(C.byref(prep.inputs), _p(u), _p(u), _p(out)) == 10
