@@ -159,3 +159,28 @@ def test_ssa_refuses_the_column_preconditioner():
     out = np.zeros((m.ny - 1, m.nx - 1))
     u = np.zeros(m.vshape3)
     assert emu.emu_slide_beta(C.byref(prep.inputs), _p(u), _p(u), _p(out)) == 10
+
+
+# ---------------------------------------------------------------------------
+# GPU: the shallow-shelf Picard solve against the oracle
+# ---------------------------------------------------------------------------
+@pytest.mark.gpu
+@pytest.mark.parametrize("m", _ssa_models(), ids=lambda m: m.name)
+def test_device_ssa_picard_matches_oracle(ctx, m):
+    from helpers import rel_l2
+
+    m = m.copy(pcg_maxiters=3000)
+    u, v, efvs, st = ctx.velo_higher_solve(m)
+    uo, vo, eo, _, sto = oracle.velo_ssa_solve(m)
+    assert st["status"] == sto["status"] == 0, (st, sto)
+    assert st["picard_iters"] == sto["picard_iters"]
+    assert rel_l2([u, v], [uo, vo]) < 1e-8
+    assert np.abs(efvs - eo).max() <= 1e-6 * np.abs(eo).max()
+
+
+@pytest.mark.gpu
+def test_device_ssa_on_a_frozen_bed_is_zero(ctx):
+    m = configs.dome().copy(approx_ssa=1)
+    u, v, _, st = ctx.velo_higher_solve(m)
+    assert st["status"] == 0 and st["picard_iters"] == 1
+    assert np.all(u == 0.0) and np.all(v == 0.0)
