@@ -281,7 +281,6 @@ __global__ void __launch_bounds__(256) k_asm2_qp(DevView v) {
   if (p == 0) v.efvs[c] = sum / 4.0;
 }
 
-
 // ---------------------------------------------------------------------
 // Assembly pass 2 + basal BC + Dirichlet BC: thread = (block B, node).
 // ---------------------------------------------------------------------
