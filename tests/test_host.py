@@ -253,3 +253,29 @@ def test_upstream_gradient_takes_the_higher_edge():
     slope = -np.tan(np.radians(0.5))
     assert np.allclose(su["dusrf_dx"][js, is_], slope, rtol=1e-12)
     assert np.all(su["dusrf_dy"][js, is_] == 0.0)
+
+
+def _c_struct_fields(hdr, name):
+    """Field names, in order, of the typedef struct `name` in the header."""
+    end = re.search(r"\}\s*" + name + r";", hdr).start()
+    body = hdr[hdr.rindex("typedef struct {", 0, end) + len("typedef struct {"):end]
+    body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
+    names = []
+    for decl in body.split(";"):
+        decl = decl.strip()
+        if not decl:
+            continue
+        decl = re.sub(r"^(const\s+)?[A-Za-z_][A-Za-z0-9_]*\s*", "", decl)  # drop the type
+        for part in decl.split(","):
+            names.append(part.strip().lstrip("*").strip())
+    return names
+
+
+@pytest.mark.parametrize("cname,pystruct", [("bp_inputs", solver.Inputs), ("bp_stats", solver.Stats),
+                                            ("bp_model", solver.Model), ("bp_setup_arrays", solver.SetupArrays),
+                                            ("bp_sliding", solver.Sliding)])
+def test_ctypes_structs_follow_the_header(cname, pystruct):
+    """The Python binding's structs list the C ABI structs' fields in the
+    header's order (a drift would shift every later field)."""
+    hdr = open(os.path.join(ROOT, "include", "bp_b200.h")).read()
+    assert _c_struct_fields(hdr, cname) == [n for n, _ in pystruct._fields_]
