@@ -321,3 +321,17 @@ extern "C" int emu_assemble_ssa(const bp_inputs* in, const double* uvel, const d
   scatter_efvs(E.p, 0, E.efvs.data(), efvs);
   return 0;
 }
+
+// gather_velocity then scatter_velocity through the host plan of one
+// solve (the path of an initial guess into the device vector and of the
+// solution back out).  10 if the plan rejects the inputs.
+extern "C" int emu_velocity_roundtrip(const bp_inputs* in, const double* uvel, const double* vvel,
+                                      double* uout, double* vout) {
+  Emu E;
+  std::string err;
+  if (!build_plan(in, 1, &E.p, &err)) return 10;
+  E.bind();
+  gather_velocity(E.p, 0, uvel, vvel, E.x.data());
+  scatter_velocity(E.p, 0, E.x.data(), uout, vout);
+  return 0;
+}

@@ -184,3 +184,21 @@ def test_device_ssa_on_a_frozen_bed_is_zero(ctx):
     u, v, _, st = ctx.velo_higher_solve(m)
     assert st["status"] == 0 and st["picard_iters"] == 1
     assert np.all(u == 0.0) and np.all(v == 0.0)
+
+
+def test_ssa_plan_takes_the_bed_velocity_and_fills_every_level():
+    """The shallow-shelf plan starts from uvel(nz,:,:) (:1179-1180) and
+    hands the 2-D solution back on every level (:3745-3750), halo-updated;
+    vertices without a column keep what the caller's arrays held."""
+    emu = C.CDLL(EMU)
+    m = _ssa_models()[1]
+    prep, u, v = solver.prepare(m)
+    su = oracle.setup(m)
+    u, v = random_state(m, su, seed=8, scale=20.0)
+    uo, vo = np.zeros(m.vshape3), np.zeros(m.vshape3)
+    assert emu.emu_velocity_roundtrip(C.byref(prep.inputs), _p(np.ascontiguousarray(u)),
+                                      _p(np.ascontiguousarray(v)), _p(uo), _p(vo)) == 0
+    cols = owned_active_rows(m, su["active_vertex"])
+    for a, b in ((uo, u), (vo, v)):
+        assert np.array_equal(a[cols], np.repeat(b[cols][:, -1:], m.nz, axis=1))
+        assert np.array_equal(a, oracle.halo_stag(a, m.periodic))
