@@ -38,6 +38,8 @@ ASSEMBLE_STANDARD, ASSEMBLE_LOCAL = 0, 1
 (BABC_YIELD_PICARD, BABC_PSEUDO_PLASTIC, BABC_POWERLAW, BABC_COULOMB_FRICTION,
  BABC_COULOMB_POWERLAW_SCHOOF, BABC_COULOMB_POWERLAW_TSAI, BABC_POWERLAW_EFFECPRESS) = 2, 3, 9, 10, 11, 12, 13
 SLIDING_LAWS = (2, 3, 9, 10, 11, 12, 13)
+# the 2-D solves (whichapprox, glide_types.F90:255-259); 0 = the 3-D Blatter-Pattyn solve
+APPROX_SSA, APPROX_L1L2 = 1, 3
 
 
 @dataclasses.dataclass
@@ -108,7 +110,7 @@ class BPModel:
     pcg_tol: float = 1.0e-8
     pcg_ncheck: int = 5
     sliding: Optional[SlidingLaw] = None  # velocity-dependent law (which_babc = sliding.law)
-    approx_ssa: int = 0  # 1: shallow-shelf 2-D solve (whichapprox = HO_APPROX_SSA)
+    approx_2d: int = 0  # 2-D solve: APPROX_SSA (1) or APPROX_L1L2 (3); 0 = 3-D Blatter-Pattyn
     name: str = ""
 
     @property

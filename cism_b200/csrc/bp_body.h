@@ -350,13 +350,53 @@ BP_HD void row_assemble(const DevView& v, const RefTables& T, int col, int k,
 // (nz = 1).  The element data of cell c sit where the 3-D elements' do:
 // point p at qp[(c * 8 + p) * 10], f then J^-1 (2 x 2, row-major).
 // ---------------------------------------------------------------------
-// Point p of cell c: get_basis_function_derivatives_2d (:6583-6751), the
-// SSA branch of compute_effective_viscosity with the vertically averaged
-// flow factor (v.flwafact[c]), and f = h efvs w detJ / vol0 with the
-// thickness interpolated to the point (:5507-5515, compute_element_matrix
-// :7868-7986).  false for a singular Jacobian.
+// compute_effective_viscosity_L1L2 (:7382-7618): the viscosity ek[k] of
+// each layer k = 0..nl-1 at one point, from the strain rates g (as
+// qp_velocity_gradient), the surface slope (sx, sy) and the thickness h
+// there.  Glen's law (n = 3) solves x^3 + a x + b = 0 for x =
+// tau_parallel, a = tau_perp^2 = (rhoi grav h sigma(k+1) |grad s|)^2 and
+// b = -effstrain / A, by Cardano's formula (:7566-7600), the second root
+// in its first-order form -a / (3 |b|^(1/3)) when a^3/27 <= 1e-6 b^2/4;
+// efvs = 1 / (2 A (x^2 + tau_perp^2)).  Returns the column average
+// sum_k ek[k] (sigma(k+1) - sigma(k)) (:5474-5478).
+BP_HD double l1l2_point_efvs(const InstParams& ip, int nl, const double* flwa, const double* flwafact,
+                             const double* g, double sx, double sy, double h, double* ek) {
+  if (ip.which_efvs == 0) {
+    for (int k = 0; k < nl; ++k) ek[k] = ip.efvs_constant;
+  } else if (ip.which_efvs == 1) {
+    const double scyr = 31536000.0;
+    const double effstrain = (500.0 / scyr) / 200.0e3 * scyr;
+    for (int k = 0; k < nl; ++k) ek[k] = flwafact[k] * pow(effstrain, (1.0 - 3.0) / 3.0);
+  } else {
+    const double ux = g[0], uy = g[1], vx = g[3], vy = g[4];
+    const double smin = 1.0e-8;
+    const double effstrain = sqrt(smin * smin + ux * ux + vy * vy + ux * vy + 0.25 * ((vx + uy) * (vx + uy)));
+    const double grads = sqrt(sx * sx + sy * sy);
+    for (int k = 0; k < nl; ++k) {
+      const double tau_perp = ip.rhoi * ip.grav * (h * ip.sigma[k + 1]) * grads;
+      const double a = tau_perp * tau_perp;
+      const double b = -effstrain / flwa[k];
+      const double a3 = a * a * a / 27.0, b2 = b * b / 4.0;
+      const double c = sqrt(b2 + a3);
+      const double rootA = pow(-b / 2.0 + c, 1.0 / 3.0);
+      const double rootB = a3 > 1.0e-6 * b2 ? -pow(b / 2.0 + c, 1.0 / 3.0) : -a / (3.0 * pow(fabs(b), 1.0 / 3.0));
+      const double tp = rootA + rootB;
+      ek[k] = 1.0 / (2.0 * flwa[k] * (tp * tp + tau_perp * tau_perp));
+    }
+  }
+  double avg = 0.0;
+  for (int k = 0; k < nl; ++k) avg = avg + ek[k] * (ip.sigma[k + 1] - ip.sigma[k]);
+  return avg;
+}
+
+// Point p of cell c: get_basis_function_derivatives_2d (:6583-6751); the
+// shallow-shelf branch of compute_effective_viscosity with the vertically
+// averaged flow factor (v.flwafact[c]), or the L1L2 layer viscosities
+// (l1l2_point_efvs, written to ek) and their column average; f = h efvs w
+// detJ / vol0 with the thickness interpolated to the point (:5507-5515,
+// compute_element_matrix :7868-7986).  false for a singular Jacobian.
 BP_HD bool qp2_element_point(const DevView& v, const RefTables& T, int c, int p, double* out,
-                             double* efvs_qp) {
+                             double* efvs_qp, double* ek = nullptr) {
   const InstParams& ip = v.inst[v.cell_inst[c]];
   const int ic = v.cell_ij[c], jc = v.cell_ij[v.ncells + c];
   double x[4], y[4], u[4], w[4], h[4];
@@ -397,10 +437,22 @@ BP_HD bool qp2_element_point(const DevView& v, const RefTables& T, int c, int p,
       g[4] += dy * w[n];
     }
   }
-  // qp_efvs with no vertical shear is the SSA branch (:7326-7334)
-  const double efvs = qp_efvs(ip.which_efvs, ip.efvs_constant, v.flwafact[c], g);
   double h_qp = 0.0;
   for (int n = 0; n < 4; ++n) h_qp += T.phi2[p][n] * h[n];
+  double efvs;
+  if (v.l1l2) {
+    const int nl = v.nl;
+    double sx = 0.0, sy = 0.0;
+    for (int n = 0; n < 4; ++n) {
+      sx += T.phi2[p][n] * v.cell_ds[(size_t)n * v.ncells + c];
+      sy += T.phi2[p][n] * v.cell_ds[(size_t)(4 + n) * v.ncells + c];
+    }
+    efvs = l1l2_point_efvs(ip, nl, v.cell_flwa + (size_t)c * nl, v.flwafact + (size_t)c * nl, g, sx, sy, h_qp,
+                           ek);
+  } else {
+    // qp_efvs with no vertical shear is the SSA branch (:7326-7334)
+    efvs = qp_efvs(ip.which_efvs, ip.efvs_constant, v.flwafact[c], g);
+  }
   *efvs_qp = efvs;
   out[0] = h_qp * efvs * 1.0 * det / kVol0;
   out[1] = i11; out[2] = i12; out[3] = i21; out[4] = i22;
@@ -450,6 +502,134 @@ BP_HD void row_assemble2(const DevView& v, const RefTables& T, int col, double* 
   if (c1 >= 0) row_element2<3, B>(T, v.qp + (size_t)c1 * 80, acc);
   if (c2 >= 0) row_element2<1, B>(T, v.qp + (size_t)c2 * 80, acc);
   if (c3 >= 0) row_element2<0, B>(T, v.qp + (size_t)c3 * 80, acc);
+}
+
+// ---------------------------------------------------------------------
+// L1L2 3-D velocity: compute_3d_velocity_L1L2 (:5834-6356), the vertex
+// method (edge_velocity = .false.), after the Picard loop.
+// ---------------------------------------------------------------------
+// Cell c: the strain rates of the basal velocity at the cell centre
+// (get_basis_function_derivatives_2d with the centre derivatives
+// :589-597), eps_parallel, and per layer k tau_parallel = 2 efvs
+// eps_parallel and w1..w3 = E_k (2 ux + vy, uy + vx, 2 vy + ux), E_k the
+// integral of efvs from the surface to the base of layer k; written to
+// v.lw[(q * nl + k) * ncells + c], q = 0 tau_parallel, 1..3 w1..w3.
+BP_HD void l1l2_cell(const DevView& v, int c) {
+  const InstParams& ip = v.inst[v.cell_inst[c]];
+  const int ic = v.cell_ij[c], jc = v.cell_ij[v.ncells + c], nl = v.nl;
+  const double dxr[4] = {-0.25, 0.25, 0.25, -0.25}, dyr[4] = {-0.25, -0.25, 0.25, 0.25};
+  double x[4], y[4], u[4], w[4];
+  for (int n = 0; n < 4; ++n) {
+    const int iv = (n == 1 || n == 2) ? ic : ic - 1;
+    const int jv = n >= 2 ? jc : jc - 1;
+    x[n] = ip.dx * iv;
+    y[n] = ip.dy * jv;
+    const int col = v.cell_cols[n * v.ncells + c];
+    u[n] = col >= 0 ? v.x[col].x : 0.0;
+    w[n] = col >= 0 ? v.x[col].y : 0.0;
+  }
+  double J11 = 0, J12 = 0, J21 = 0, J22 = 0;
+  for (int n = 0; n < 4; ++n) {
+    J11 += dxr[n] * x[n];
+    J12 += dxr[n] * y[n];
+    J21 += dyr[n] * x[n];
+    J22 += dyr[n] * y[n];
+  }
+  const double det = J11 * J22 - J12 * J21;
+  double ux = 0.0, uy = 0.0, vx = 0.0, vy = 0.0;
+  if (fabs(det) > 0.0) {
+    const double i11 = J22 / det, i12 = -J12 / det, i21 = -J21 / det, i22 = J11 / det;
+    for (int n = 0; n < 4; ++n) {
+      const double dx = i11 * dxr[n] + i12 * dyr[n];
+      const double dy = i21 * dxr[n] + i22 * dyr[n];
+      ux += dx * u[n];
+      uy += dy * u[n];
+      vx += dx * w[n];
+      vy += dy * w[n];
+    }
+  }
+  const double eps = sqrt(ux * ux + vy * vy + ux * vy + 0.25 * ((vx + uy) * (vx + uy)));
+  const double H = v.cell_thck[c];
+  const size_t NC = (size_t)v.ncells, st = (size_t)nl * NC;
+  double E = 0.0;
+  for (int k = 0; k < nl; ++k) {
+    const double e = v.efvs[(size_t)c * nl + k];
+    E = E + e * (ip.sigma[k + 1] - ip.sigma[k]) * H;
+    const size_t o = (size_t)k * NC + c;
+    v.lw[o] = 2.0 * e * eps;
+    v.lw[st + o] = E * (2.0 * ux + vy);
+    v.lw[2 * st + o] = E * (uy + vx);
+    v.lw[3 * st + o] = E * (2.0 * vy + ux);
+  }
+}
+
+// glissade_gradient with gradient_margin = 1 (glissade_grid_operators.F90:
+// 235-410) at a vertex: the mean of the two edge differences (a, b) whose
+// cells both hold ice, the one such edge, or zero.
+BP_HD double l1l2_edges(double a, double b, bool ma, bool mb) {
+  if (ma && mb) return (a + b) / 2.0;
+  if (ma) return a;
+  if (mb) return b;
+  return 0.0;
+}
+
+// Column col: per layer k from the bed up, tau_xz, tau_yz at the layer
+// midpoint (the shallow-ice stress -rhoi grav depth grad s plus the
+// gradients of w1..w3 over the four cells), A and tau_parallel staggered
+// over the ice cells (glissade_stagger margin 1, NW NE SW SE), and u(k) =
+// u(k+1) + 2 A tau_eff^2 (sigma(k+1) - sigma(k)) H tau_xz (tau_eff^(n-1)
+// with n = 3); a prescribed basal vertex keeps the basal velocity on every
+// level.  Writes v.x3[col * (nl + 1) + k], k = nl the bed.
+BP_HD void l1l2_column(const DevView& v, int col) {
+  const InstParams& ip = v.inst[v.col_inst[col]];
+  const int nl = v.nl, nc = v.ncols;
+  const size_t NCELL = (size_t)v.ncells, st = (size_t)nl * NCELL;
+  // cells SW (i,j), SE (i+1,j), NW (i,j+1), NE (i+1,j+1)
+  const int cs[4] = {v.col_cells[col], v.col_cells[nc + col], v.col_cells[2 * nc + col],
+                     v.col_cells[3 * nc + col]};
+  const bool sw = cs[0] >= 0, se = cs[1] >= 0, nw = cs[2] >= 0, ne = cs[3] >= 0;
+  const double sx = v.col_ds[col], sy = v.col_ds[nc + col], H = v.col_h[col];
+  const uint8_t dm = v.dmask[col];
+  const double2 ub = v.x[col];
+  double2* out = v.x3 + (size_t)col * (nl + 1);
+  out[nl] = ub;
+  double2 up = ub;
+  for (int k = nl - 1; k >= 0; --k) {
+    double f[4][4];  // [quantity][cell]
+    for (int q = 0; q < 4; ++q)
+      for (int m = 0; m < 4; ++m) f[q][m] = cs[m] >= 0 ? v.lw[q * st + (size_t)k * NCELL + cs[m]] : 0.0;
+    double d[3][2];
+    for (int q = 0; q < 3; ++q) {
+      const double* g = f[q + 1];
+      d[q][0] = l1l2_edges((g[3] - g[2]) / ip.dx, (g[1] - g[0]) / ip.dx, ne && nw, se && sw);
+      d[q][1] = l1l2_edges((g[3] - g[1]) / ip.dy, (g[2] - g[0]) / ip.dy, ne && se, nw && sw);
+    }
+    const double depth = 0.5 * (ip.sigma[k] + ip.sigma[k + 1]) * H;
+    const double txz = -ip.rhoi * ip.grav * depth * sx + 2.0 * d[0][0] + d[1][1];
+    const double tyz = -ip.rhoi * ip.grav * depth * sy + d[1][0] + 2.0 * d[2][1];
+    const int cnt = (int)nw + (int)ne + (int)sw + (int)se;
+    double tp = 0.0, fa = 0.0;
+    if (cnt > 0) {
+      double a = 0.0, t = 0.0;
+      const int order[4] = {2, 3, 0, 1};  // NW, NE, SW, SE
+      for (int o = 0; o < 4; ++o) {
+        const int m = order[o];
+        if (cs[m] >= 0) {
+          t = t + f[0][m];
+          a = a + v.cell_flwa[(size_t)cs[m] * nl + k];
+        }
+      }
+      tp = t / (double)cnt;
+      fa = a / (double)cnt;
+    }
+    const double tes = tp * tp + txz * txz + tyz * tyz;
+    const double fact = 2.0 * fa * tes * (ip.sigma[k + 1] - ip.sigma[k]) * H;
+    double2 cur;
+    cur.x = (dm & 1) ? ub.x : up.x + fact * txz;
+    cur.y = (dm & 2) ? ub.y : up.y + fact * tyz;
+    out[k] = cur;
+    up = cur;
+  }
 }
 
 // calcbeta (glissade_basal_traction.F90:67-598) at one vertex for the

@@ -61,6 +61,7 @@ struct InstParams {
   int cell_begin, cell_end;
   int elem_begin, elem_end;
   SlideParams slide;
+  double rhoi, grav;            // L1L2: tau_perp = rhoi grav depth |grad s|
 };
 
 // Per-instance solver state (device-resident, written by finalizers).
@@ -84,7 +85,7 @@ struct InstState {
   int need_true;                // mixed: the next check computes the FP64 residual
   int restart;                  // mixed, Chronopoulos-Gear: next pass restarts (beta = 0)
   int last_true_iter;           // mixed: pcg_iter of the last refinement
-  int frozen;                   // SSA on a no-slip bed: velocity zero, no linear solve
+  int frozen;                   // 2-D solve on a no-slip bed: 2-D velocity zero, no linear solve
 };
 
 // Global counters polled by the host.
@@ -105,7 +106,9 @@ struct DevView {
   int minb_k;              // Krylov matvecs (k_std_mv, k_cg_mv): the same, 0, 4 or 6
   int grid_k;              // CTAs of the Krylov matvecs (0 = one per tile)
   int dry;                 // autotuner pass: Krylov matvecs run every tile, leave the state alone
-  int ssa;                 // shallow-shelf 2-D solve: nz = 1, one 2-D element per cell
+  int solve2d;             // 2-D solve (shallow-shelf or L1L2): nz = 1, one 2-D element per cell
+  int l1l2;                // L1L2: layer viscosities, 3-D velocity reconstructed after the loop
+  int nl;                  // L1L2: layers of the velocity arrays (the model's nz - 1)
   unsigned long long* mv_nodes;  // [2] nodes through FP64 / FP32 Krylov matvecs (timing runs), or null
   const InstParams* inst;
   InstState* st;
@@ -127,14 +130,22 @@ struct DevView {
   const double* cell_s;    // [4][ncells] stagusrf at the corners
   const double* cell_h;    // [4][ncells] stagthck at the corners
   double* cell_beta;       // [4][ncells] beta_internal at the corners (sliding law: 0 where no column)
-  const double* flwafact;  // [ncells*(nz-1)]
+  const double* flwafact;  // [nelem] (shallow-shelf: the column average per cell; L1L2: [ncells][nl])
+  // L1L2 (null otherwise)
+  const double* cell_flwa; // [ncells][nl] flow factor A
+  const double* cell_thck; // [ncells] cell thickness
+  const double* cell_ds;   // [2][4][ncells] surface gradient (x, y) at the corners
+  const double* col_ds;    // [2][ncols] surface gradient at the column's vertex
+  const double* col_h;     // [ncols] stagthck at the column's vertex
+  double* lw;              // [4][nl][ncells] tau_parallel, w1, w2, w3 of the reconstruction
+  double2* x3;             // [ncols][nl+1] reconstructed velocity (k = nl the bed)
   // tiles
   const int* tile_start;   // [ntiles] first node (tiles hold whole columns)
   const int* tile_end;     // [ntiles] one past the last node
   const int* tile_inst;    // [ntiles]
   // assembly / matrix
   double* qp;              // [nelem*8*10]: f, Jinv(3x3) per quadrature point
-  double* efvs;            // [nelem]
+  double* efvs;            // [nelem]; L1L2 [ncells][nl]
   // FP64 matrix, (u,v) pairs: h = 0 the u-row (Auu, Auv), h = 1 the v-row
   // (Avu, Avv).  Full storage [2][27][npad]; symmetric storage [2][14][npad]
   // holds stencil offsets m = 13..26 (diagonal first), the lower half being

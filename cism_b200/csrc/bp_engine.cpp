@@ -137,7 +137,9 @@ DevView make_view(Arena& a, cudaStream_t s, const HostPlan& p, bool with_cells, 
   DevView v;
   std::memset(&v, 0, sizeof(v));
   v.nz = p.nz; v.ncols = p.ncols; v.nnodes = p.nnodes; v.npad = p.npad;
-  v.ssa = p.ssa ? 1 : 0;
+  v.solve2d = p.solve2d ? 1 : 0;
+  v.l1l2 = p.l1l2 ? 1 : 0;
+  v.nl = p.nz_out - 1;
   v.ncells = p.ncells; v.nelem = p.nelem; v.ninst = p.ninst; v.ntiles = p.ntiles;
   int anyd = 0;
   for (uint8_t m : p.dmask) anyd |= (m != 0);
@@ -173,7 +175,16 @@ DevView make_view(Arena& a, cudaStream_t s, const HostPlan& p, bool with_cells, 
     UP(double, "cell_beta", p.cell_beta, cell_beta);
     UP(double, "flwafact", p.flwafact, flwafact);
     v.qp = a.get<double>(s, "qp", (size_t)p.nelem * 80);
-    v.efvs = a.get<double>(s, "efvs", p.nelem);
+    v.efvs = a.get<double>(s, "efvs", p.nefvs);
+    if (p.l1l2) {
+      UP(double, "cell_flwa", p.cell_flwa, cell_flwa);
+      UP(double, "cell_thck", p.cell_thck, cell_thck);
+      UP(double, "cell_ds", p.cell_ds, cell_ds);
+      UP(double, "col_ds", p.col_ds, col_ds);
+      UP(double, "col_h", p.col_h, col_h);
+      v.lw = a.get<double>(s, "l1l2_work", 4 * (size_t)v.nl * std::max(p.ncells, 1));
+      v.x3 = a.get<double2>(s, "x3", (size_t)std::max(p.ncols, 1) * (v.nl + 1));
+    }
     v.badj = a.get<double>(s, "badj", 4 * np);
   }
   UP(int, "tile_start", p.tile_start, tile_start);
@@ -625,6 +636,7 @@ void problem_run(bp_problem* P) {
   CK(cudaMemcpyAsync(P->v.x, P->x0, sizeof(double2) * P->plan.npad, cudaMemcpyDeviceToDevice, c->stream));
   init_state(c->stream, P->v, P->plan, true, false);
   run_picard(P);
+  if (P->v.l1l2) launch_l1l2_velocity(P->v, c->stream);  // compute_3d_velocity_L1L2 (:3773-3801)
   CK(cudaEventRecord(c->t2, c->stream));
   CK(cudaMemcpyAsync(P->state.data(), P->v.st, sizeof(InstState) * P->plan.ninst,
                      cudaMemcpyDeviceToHost, c->stream));
@@ -639,18 +651,26 @@ void problem_run(bp_problem* P) {
 
 void problem_get(bp_problem* P, double* const* uvel, double* const* vvel, double* const* efvs) {
   const HostPlan& p = P->plan;
-  std::vector<double2> x(p.npad);
-  CK(cudaMemcpyAsync(x.data(), P->v.x, sizeof(double2) * p.npad, cudaMemcpyDeviceToHost, P->c->stream));
+  // L1L2: the reconstructed 3-D velocity, else the solution vector
+  const size_t nx = p.l1l2 ? (size_t)p.ncols * p.nz_out : (size_t)p.npad;
+  std::vector<double2> x(std::max<size_t>(nx, 1));
+  if (nx > 0)
+    CK(cudaMemcpyAsync(x.data(), p.l1l2 ? P->v.x3 : P->v.x, sizeof(double2) * nx, cudaMemcpyDeviceToHost,
+                       P->c->stream));
   std::vector<double> ef;
   if (efvs) {
-    ef.resize(std::max(p.nelem, 1));
-    if (p.nelem > 0)
-      CK(cudaMemcpyAsync(ef.data(), P->v.efvs, sizeof(double) * p.nelem, cudaMemcpyDeviceToHost, P->c->stream));
+    ef.resize(std::max(p.nefvs, 1));
+    if (p.nefvs > 0)
+      CK(cudaMemcpyAsync(ef.data(), P->v.efvs, sizeof(double) * p.nefvs, cudaMemcpyDeviceToHost, P->c->stream));
   }
   CK(cudaStreamSynchronize(P->c->stream));
-  P->d2h_bytes = sizeof(double2) * (double)p.nnodes + (efvs ? sizeof(double) * (double)p.nelem : 0.0);
+  P->d2h_bytes = sizeof(double2) * (double)(p.l1l2 ? nx : (size_t)p.nnodes) +
+                 (efvs ? sizeof(double) * (double)p.nefvs : 0.0);
   for (int b = 0; b < p.ninst; ++b) {
-    if (uvel && vvel) scatter_velocity(p, b, x.data(), uvel[b], vvel[b]);
+    if (uvel && vvel) {
+      if (p.l1l2) scatter_velocity_3d(p, b, x.data(), uvel[b], vvel[b]);
+      else scatter_velocity(p, b, x.data(), uvel[b], vvel[b]);
+    }
     if (efvs && efvs[b]) scatter_efvs(p, b, ef.data(), efvs[b]);
   }
 }
@@ -787,7 +807,7 @@ int bp_problem_diagnostics(bp_problem* P, int which_bfric, double* const* tau_xz
   bool want_tau = false;
   for (auto o : outs) want_tau = want_tau || o;
   if (!p.ncells) return BP_ERR_ARGS;  // matrix-level problems have no elements
-  if (p.ssa && want_tau) {  // the 3-D stress routine's SSA branch is not restated
+  if (p.solve2d && want_tau) {  // the stress routine's 2-D branches are not restated
     c->err = "bp_problem_diagnostics: element stresses of 3-D Blatter-Pattyn solves only";
     return BP_ERR_ARGS;
   }
@@ -1061,7 +1081,7 @@ int bp_assemble(bp_ctx* c, const bp_inputs* in, const double* uvel,
     c->err = e;
     return BP_ERR_ARGS;
   }
-  if (p.ssa) {  // the 2-D system has the 9-entry reference layout, not this one
+  if (p.solve2d) {  // the 2-D system has the 9-entry reference layout, not this one
     c->err = "bp_assemble: 3-D Blatter-Pattyn systems only";
     return BP_ERR_ARGS;
   }

@@ -266,8 +266,9 @@ __global__ void __launch_bounds__(256) k_asm2_qp(DevView v) {
   }
   const unsigned mask = __ballot_sync(0xffffffffu, valid);
   if (!valid) return;
-  double out[5], eq = 0.0;
-  if (!qp2_element_point(v, c_T, c, p, out, &eq)) {
+  double out[5], eq = 0.0, ek[kNzMax - 1];
+  const bool ok = qp2_element_point(v, c_T, c, p, out, &eq, ek);
+  if (!ok) {
     atomicExch(&v.st[inst].status, BP_ERR_SINGULAR_JAC);
     eq = 0.0;
     for (int i = 0; i < 5; ++i) out[i] = 0.0;
@@ -275,20 +276,44 @@ __global__ void __launch_bounds__(256) k_asm2_qp(DevView v) {
   double* dst = v.qp + ((size_t)c * 8 + p) * 10;
   for (int i = 0; i < 5; ++i) dst[i] = out[i];
   const int lane0 = (threadIdx.x & 31) & ~3;
+  if (v.l1l2) {  // efvs(k) = the mean of the layer's point values (:5565-5572)
+    for (int k = 0; k < v.nl; ++k) {
+      const double e = ok ? ek[k] : 0.0;
+      double sum = 0.0;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) sum += __shfl_sync(mask, e, lane0 + q);
+      if (p == 0) v.efvs[(size_t)c * v.nl + k] = sum / 4.0;
+    }
+    return;
+  }
   double sum = 0.0;
 #pragma unroll
   for (int q = 0; q < 4; ++q) sum += __shfl_sync(mask, eq, lane0 + q);
   if (p == 0) v.efvs[c] = sum / 4.0;
 }
 
+// L1L2 3-D velocity after the Picard loop (compute_3d_velocity_L1L2,
+// glissade_velo_higher.F90:5834-6356): the cell pass (l1l2_cell), then
+// one thread per column integrates from the bed up (l1l2_column).  Run
+// once per solve; bounded by the nl * 4 cell values each column reads.
+__global__ void __launch_bounds__(256) k_l1l2_cells(DevView v) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < v.ncells) l1l2_cell(v, c);
+}
+
+__global__ void __launch_bounds__(256) k_l1l2_columns(DevView v) {
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col < v.ncols) l1l2_column(v, col);
+}
+
 // ---------------------------------------------------------------------
 // Assembly pass 2 + basal BC + Dirichlet BC: thread = (block B, node).
 // ---------------------------------------------------------------------
-template <int B, bool SSA>
+template <int B, bool D2>
 __device__ __forceinline__ bool asm_row(const DevView& v, int n) {
   const int col = n / v.nz, k = n - col * v.nz;
   double acc[27];
-  if (SSA) row_assemble2<B>(v, c_T, col, acc);
+  if (D2) row_assemble2<B>(v, c_T, col, acc);
   else row_assemble<B>(v, c_T, col, k, acc);
   row_basal<B>(v, c_T, col, k, acc);
   const double adj = row_dirichlet<B>(v, col, k, acc);
@@ -309,8 +334,8 @@ __device__ __forceinline__ bool asm_row(const DevView& v, int n) {
   return nz;
 }
 
-// SSA: the 2-D rows of the shallow-shelf solve (nz = 1).
-template <bool SSA>
+// D2: the rows of the 2-D solves (shallow-shelf, L1L2; nz = 1).
+template <bool D2>
 __global__ void __launch_bounds__(kTile) k_asm_rows(DevView v) {
   const int B = blockIdx.y;
   for (int t = blockIdx.x; t < v.ntiles; t += gridDim.x) {
@@ -320,10 +345,10 @@ __global__ void __launch_bounds__(kTile) k_asm_rows(DevView v) {
     int nzl = 0;
     if (n < R.nend) {
       switch (B) {
-        case 0: nzl = asm_row<0, SSA>(v, n); break;
-        case 1: nzl = asm_row<1, SSA>(v, n); break;
-        case 2: nzl = asm_row<2, SSA>(v, n); break;
-        default: nzl = asm_row<3, SSA>(v, n); break;
+        case 0: nzl = asm_row<0, D2>(v, n); break;
+        case 1: nzl = asm_row<1, D2>(v, n); break;
+        case 2: nzl = asm_row<2, D2>(v, n); break;
+        default: nzl = asm_row<3, D2>(v, n); break;
       }
     }
     if (__syncthreads_or(nzl) && threadIdx.x == 0) atomicOr(&v.st[R.inst].nonzero, 1);
@@ -369,8 +394,8 @@ __global__ void __launch_bounds__(kTile) k_rhs(DevView v) {
         S.status = BP_ZERO_MATRIX;
         S.zero_x = 1;
         fail(v, S, BP_ZERO_MATRIX);
-      } else if (v.ssa && v.inst[inst].which_babc == 6) {
-        // SSA on a no-slip bed: the velocity is zero and nothing is solved
+      } else if (v.solve2d && v.inst[inst].which_babc == 6) {
+        // 2-D solve on a no-slip bed: the 2-D velocity is zero and nothing is solved
         // (glissade_velo_higher.F90:3227-3240)
         S.frozen = 1;
         S.L2_norm = 0.0;
@@ -806,10 +831,10 @@ __global__ void __launch_bounds__(kTile) k_picard_check(DevView v) {
     if (!S.picard_active) continue;
     const bool meanu = ip.which_resid == 2;
     // the 2-D criterion has no bed layer to leave out (:9238-9351)
-    const bool nobed = !v.ssa && (ip.which_resid == 1 || meanu);
+    const bool nobed = !v.solve2d && (ip.which_resid == 1 || meanu);
     double part[2] = {0.0, 0.0};
     if (n < R.nend) {
-      if (S.frozen) v.x[n] = make_double2(0.0, 0.0);  // SSA on a no-slip bed
+      if (S.frozen) v.x[n] = make_double2(0.0, 0.0);  // 2-D solve on a no-slip bed
       const int k = n % v.nz;
       if (!(nobed && k == v.nz - 1)) {
         const double2 x = v.x[n], o = v.usav[n];
@@ -965,7 +990,7 @@ void launch_slide_beta(const DevView& v, cudaStream_t s) {
   if (v.ncells > 0) k_cell_beta<<<(v.ncells + kTile - 1) / kTile, kTile, 0, s>>>(v);
 }
 void launch_asm_qp(const DevView& v, cudaStream_t s) {
-  if (v.ssa) {
+  if (v.solve2d) {
     if (v.ncells > 0) {
       const long threads = (long)v.ncells * 4;
       k_asm2_qp<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(v);
@@ -977,10 +1002,14 @@ void launch_asm_qp(const DevView& v, cudaStream_t s) {
 }
 void launch_asm_rows(const DevView& v, cudaStream_t s) {
   dim3 g(tile_grid(v), 4);
-  if (v.ssa) k_asm_rows<true><<<g, kTile, 0, s>>>(v);
+  if (v.solve2d) k_asm_rows<true><<<g, kTile, 0, s>>>(v);
   else k_asm_rows<false><<<g, kTile, 0, s>>>(v);
 }
 void launch_rhs(const DevView& v, cudaStream_t s) { k_rhs<<<tile_grid(v), kTile, 0, s>>>(v); }
+void launch_l1l2_velocity(const DevView& v, cudaStream_t s) {
+  if (v.ncells > 0) k_l1l2_cells<<<(unsigned)((v.ncells + 255) / 256), 256, 0, s>>>(v);
+  if (v.ncols > 0) k_l1l2_columns<<<(unsigned)((v.ncols + 255) / 256), 256, 0, s>>>(v);
+}
 void launch_assemble(const DevView& v, cudaStream_t s) {
   launch_asm_qp(v, s);
   launch_asm_rows(v, s);

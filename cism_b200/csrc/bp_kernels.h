@@ -20,6 +20,9 @@ void launch_assemble(const DevView& v, cudaStream_t s);
 void launch_asm_qp(const DevView& v, cudaStream_t s);
 void launch_asm_rows(const DevView& v, cudaStream_t s);
 void launch_rhs(const DevView& v, cudaStream_t s);
+// L1L2: the 3-D velocity v.x3 from the basal velocity v.x and the layer
+// viscosities v.efvs of the last assembly
+void launch_l1l2_velocity(const DevView& v, cudaStream_t s);
 // Residual modes (MV_INIT, MV_CHECK, MV_REFINE) run with (minb, grid_cap),
 // the Krylov matvecs (MV_STD_A, MV_CG_FIRST, MV_CG1) with (minb_k, grid_k).
 void launch_mv(int mode, const DevView& v, cudaStream_t s);

@@ -227,12 +227,16 @@ bool build_plan(const bp_inputs* in, int n, HostPlan* p, std::string* err) {
   *p = HostPlan();
   const int nz_in = in[0].nz;
   if (nz_in < 2 || nz_in > kNzMax) { *err = "nz out of range (2..64)"; return false; }
-  // the shallow-shelf solve has one unknown pair per column (solve_2d)
-  const bool ssa = in[0].approx_ssa != 0;
-  const int nz = ssa ? 1 : nz_in;
+  // the 2-D solves (shallow-shelf, L1L2) have one unknown pair per column
+  // (solve_2d, glissade_velo_higher.F90:1125-1128)
+  const int approx = in[0].approx_2d;
+  if (approx != 0 && approx != 1 && approx != 3) { *err = "approx_2d must be 0, 1 (SSA) or 3 (L1L2)"; return false; }
+  const bool solve2d = approx != 0, l1l2 = approx == 3;
+  const int nz = solve2d ? 1 : nz_in, nl = nz_in - 1;
   p->nz = nz;
   p->nz_out = nz_in;
-  p->ssa = ssa;
+  p->solve2d = solve2d;
+  p->l1l2 = l1l2;
   p->ninst = n;
   p->inst.resize(n);
   std::vector<std::vector<std::pair<int, int>>> cols(n);
@@ -242,9 +246,13 @@ bool build_plan(const bp_inputs* in, int n, HostPlan* p, std::string* err) {
   for (int b = 0; b < n; ++b) {
     const bp_inputs& I = in[b];
     if (I.nz != nz_in) { *err = "all instances of a batch must share nz"; return false; }
-    if ((I.approx_ssa != 0) != ssa) { *err = "all instances of a batch must share the approximation"; return false; }
-    if (ssa && I.which_precond == 2) {
-      *err = "the shallow-shelf solve takes which_precond 0 or 1";
+    if (I.approx_2d != approx) { *err = "all instances of a batch must share the approximation"; return false; }
+    if (solve2d && I.which_precond == 2) {
+      *err = "the 2-D solves take which_precond 0 or 1";
+      return false;
+    }
+    if (l1l2 && (!I.l1l2 || !I.l1l2->thck || !I.l1l2->flwa || !I.l1l2->dusrf_dx || !I.l1l2->dusrf_dy)) {
+      *err = "the L1L2 solve needs l1l2 with thck, flwa, dusrf_dx and dusrf_dy";
       return false;
     }
     if (I.nhalo != 2) { *err = "nhalo must be 2"; return false; }
@@ -308,14 +316,22 @@ bool build_plan(const bp_inputs* in, int n, HostPlan* p, std::string* err) {
     p->ncells += (int)cells[b].size();
   }
   const int NCELL = p->ncells;
-  p->nelem = ssa ? NCELL : NCELL * (nz - 1);  // SSA: one 2-D element per cell
+  p->nelem = solve2d ? NCELL : NCELL * (nz - 1);  // 2-D: one element per cell
+  p->nefvs = l1l2 ? NCELL * nl : p->nelem;
   p->cell_inst.resize(NCELL);
   p->cell_ij.resize(2 * (size_t)NCELL);
   p->cell_cols.resize(4 * (size_t)NCELL);
   p->cell_s.resize(4 * (size_t)NCELL);
   p->cell_h.resize(4 * (size_t)NCELL);
   p->cell_beta.resize(4 * (size_t)NCELL);
-  p->flwafact.resize((size_t)p->nelem);
+  p->flwafact.resize((size_t)(solve2d && !l1l2 ? NCELL : NCELL * nl));
+  if (l1l2) {
+    p->cell_flwa.resize((size_t)NCELL * nl);
+    p->cell_thck.resize(NCELL);
+    p->cell_ds.resize(8 * (size_t)NCELL);
+    p->col_ds.resize(2 * (size_t)NC);
+    p->col_h.resize(NC);
+  }
   int col_base = 0, cell_base = 0;
   for (int b = 0; b < n; ++b) {
     const bp_inputs& I = in[b];
@@ -338,12 +354,16 @@ bool build_plan(const bp_inputs* in, int n, HostPlan* p, std::string* err) {
     ip.ncheck = I.pcg_ncheck > 0 ? I.pcg_ncheck : 5;
     ip.maxiter_nonlinear = I.maxiter_nonlinear;
     if (I.sliding) slide_params(*I.sliding, &ip.slide, err);
+    if (l1l2) {
+      ip.rhoi = I.l1l2->rhoi;
+      ip.grav = I.l1l2->grav;
+    }
     const int nc = (int)cols[b].size();
     ip.col_begin = col_base; ip.col_end = col_base + nc;
     ip.node_begin = col_base * nz; ip.node_end = (col_base + nc) * nz;
     const int ncl = (int)cells[b].size();
     ip.cell_begin = cell_base; ip.cell_end = cell_base + ncl;
-    const int epc = ssa ? 1 : nz - 1;  // elements per cell
+    const int epc = solve2d ? 1 : nz - 1;  // elements per cell
     ip.elem_begin = cell_base * epc; ip.elem_end = (cell_base + ncl) * epc;
     for (int c = 0; c < nc; ++c) {
       const int g = col_base + c;
@@ -369,7 +389,12 @@ bool build_plan(const bp_inputs* in, int n, HostPlan* p, std::string* err) {
       } else {
         p->col_beta[g] = I.beta_internal[vtx(i, j, nx)];
       }
-      if (ssa) {
+      if (l1l2) {
+        p->col_ds[g] = I.l1l2->dusrf_dx[vtx(i, j, nx)];
+        p->col_ds[(size_t)NC + g] = I.l1l2->dusrf_dy[vtx(i, j, nx)];
+        p->col_h[g] = I.stagthck[vtx(i, j, nx)];
+      }
+      if (solve2d) {
         // load summed over the levels (:2123-2137); the bed level's
         // Dirichlet masks (:2878)
         double lu = 0.0, lv = 0.0;
@@ -402,15 +427,23 @@ bool build_plan(const bp_inputs* in, int n, HostPlan* p, std::string* err) {
         p->cell_s[(size_t)q * NCELL + g] = I.stagusrf[v];
         p->cell_h[(size_t)q * NCELL + g] = I.stagthck[v];
         p->cell_beta[(size_t)q * NCELL + g] = I.sliding ? 0.0 : I.beta_internal[v];
+        if (l1l2) {
+          p->cell_ds[(size_t)q * NCELL + g] = I.l1l2->dusrf_dx[v];
+          p->cell_ds[(size_t)(4 + q) * NCELL + g] = I.l1l2->dusrf_dy[v];
+        }
       }
-      if (ssa) {  // glissade_vertical_average (glissade_grid_operators.F90:1172-1236)
+      if (l1l2) {
+        p->cell_thck[g] = I.l1l2->thck[cel(ic, jc, nx)];
+        for (int k = 0; k < nl; ++k) p->cell_flwa[(size_t)g * nl + k] = I.l1l2->flwa[cel(ic, jc, nx) * nl + k];
+      }
+      if (solve2d && !l1l2) {  // glissade_vertical_average (glissade_grid_operators.F90:1172-1236)
         double f = 0.0;
         for (int k = 0; k < nz_in - 1; ++k)
           f = f + I.flwafact[cel(ic, jc, nx) * (nz_in - 1) + k] * (I.sigma[k + 1] - I.sigma[k]);
         p->flwafact[g] = f;
-      } else {
-        for (int k = 0; k < nz - 1; ++k)
-          p->flwafact[(size_t)g * (nz - 1) + k] = I.flwafact[cel(ic, jc, nx) * (nz - 1) + k];
+      } else {  // per layer (3-D elements; the L1L2 layer viscosities)
+        for (int k = 0; k < nl; ++k)
+          p->flwafact[(size_t)g * nl + k] = I.flwafact[cel(ic, jc, nx) * nl + k];
       }
     }
     add_tiles(p, b, ip.node_begin, ip.node_end);
@@ -427,7 +460,7 @@ void gather_velocity(const HostPlan& p, int b, const double* uvel,
   const int nx = p.nx[b], nz = p.nz, NC = p.ncols;
   for (int g = ip.col_begin; g < ip.col_end; ++g) {
     const int i = p.col_ij[g], j = p.col_ij[NC + g];
-    if (p.ssa) {  // uvel_2d = uvel(nz,:,:) (glissade_velo_higher.F90:1179-1180)
+    if (p.solve2d) {  // uvel_2d = uvel(nz,:,:) (glissade_velo_higher.F90:1179-1180)
       const size_t src = vtx(i, j, nx) * p.nz_out + (p.nz_out - 1);
       x[g] = double2{uvel[src], vvel[src]};
       continue;
@@ -456,7 +489,7 @@ void scatter_vector(const HostPlan& p, int b, const double2* x, double* vu,
 
 void scatter_velocity(const HostPlan& p, int b, const double2* x,
                       double* uvel, double* vvel) {
-  if (p.ssa) {  // the 2-D velocity on every level (:3745-3750)
+  if (p.solve2d) {  // the 2-D velocity on every level (:3745-3750)
     const InstParams& ip = p.inst[b];
     const int nx = p.nx[b], NC = p.ncols, L = p.nz_out;
     for (int g = ip.col_begin; g < ip.col_end; ++g) {
@@ -473,6 +506,24 @@ void scatter_velocity(const HostPlan& p, int b, const double2* x,
   halo_stag(p.nx[b], p.ny[b], p.nz_out, p.periodic[b], vvel);
 }
 
+void scatter_velocity_3d(const HostPlan& p, int b, const double2* x3,
+                         double* uvel, double* vvel) {
+  const InstParams& ip = p.inst[b];
+  const int nx = p.nx[b], ny = p.ny[b], NC = p.ncols, L = p.nz_out;
+  const size_t nvert = (size_t)(nx - 1) * (ny - 1);
+  for (size_t w = 0; w < nvert; ++w)
+    for (int k = 0; k < L - 1; ++k) uvel[w * L + k] = vvel[w * L + k] = 0.0;
+  for (int g = ip.col_begin; g < ip.col_end; ++g) {
+    const size_t w = vtx(p.col_ij[g], p.col_ij[NC + g], nx);
+    for (int k = 0; k < L; ++k) {
+      uvel[w * L + k] = x3[(size_t)g * L + k].x;
+      vvel[w * L + k] = x3[(size_t)g * L + k].y;
+    }
+  }
+  halo_stag(nx, ny, L, p.periodic[b], uvel);
+  halo_stag(nx, ny, L, p.periodic[b], vvel);
+}
+
 void scatter_efvs(const HostPlan& p, int b, const double* efvs_elem,
                   double* efvs) {
   const InstParams& ip = p.inst[b];
@@ -480,8 +531,9 @@ void scatter_efvs(const HostPlan& p, int b, const double* efvs_elem,
   std::memset(efvs, 0, sizeof(double) * (size_t)(nz - 1) * nx * ny);
   for (int g = ip.cell_begin; g < ip.cell_end; ++g) {
     const int ic = p.cell_ij[g], jc = p.cell_ij[NCELL + g];
-    for (int k = 0; k < nz - 1; ++k)  // SSA: the cell's value on every layer
-      efvs[cel(ic, jc, nx) * (nz - 1) + k] = efvs_elem[p.ssa ? (size_t)g : (size_t)g * (nz - 1) + k];
+    for (int k = 0; k < nz - 1; ++k)  // shallow-shelf: the cell's value on every layer
+      efvs[cel(ic, jc, nx) * (nz - 1) + k] =
+          efvs_elem[p.solve2d && !p.l1l2 ? (size_t)g : (size_t)g * (nz - 1) + k];
   }
 }
 

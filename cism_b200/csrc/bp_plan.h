@@ -23,9 +23,11 @@ OwnedRange owned_range(int nx, int ny, int periodic);
 int vertex_image(int i, int n, int periodic);
 
 struct HostPlan {
-  int nz = 0, ninst = 0;   // nz: levels of the solve (1 for the shallow-shelf solve)
+  int nz = 0, ninst = 0;   // nz: levels of the solve (1 for the 2-D solves)
   int nz_out = 0;          // levels of the velocity arrays (the model's nz)
-  bool ssa = false;        // shallow-shelf 2-D solve
+  bool solve2d = false;    // 2-D solve: shallow-shelf or L1L2
+  bool l1l2 = false;       // L1L2 (the 3-D velocity reconstructed after the loop)
+  int nefvs = 0;           // length of the element viscosity array (L1L2: ncells * (nz_out - 1))
   int ncols = 0, nnodes = 0, npad = 0, ncells = 0, nelem = 0, ntiles = 0;
   std::vector<InstParams> inst;
   std::vector<int> col_inst, col_nbr, col_cells, col_ij;
@@ -36,6 +38,7 @@ struct HostPlan {
   std::vector<uint8_t> dmask;
   std::vector<int> cell_inst, cell_ij, cell_cols;
   std::vector<double> cell_s, cell_h, cell_beta, flwafact;
+  std::vector<double> cell_flwa, cell_thck, cell_ds, col_ds, col_h;  // L1L2 only
   std::vector<int> tile_start, tile_end, tile_inst;
   // per-instance grid sizes, for scatters
   std::vector<int> nx, ny, periodic;
@@ -63,6 +66,11 @@ void gather_velocity(const HostPlan& p, int b, const double* uvel,
                      const double* vvel, double2* x);
 void scatter_velocity(const HostPlan& p, int b, const double2* x,
                       double* uvel, double* vvel);
+// L1L2: the reconstructed velocity [ncols][nz_out] of instance b -> uvel,
+// vvel (nz,nx-1,ny-1), zero on levels 1..nz-1 away from the columns, then
+// the halo update (glissade_velo_higher.F90:3773-3801)
+void scatter_velocity_3d(const HostPlan& p, int b, const double2* x3,
+                         double* uvel, double* vvel);
 // element-averaged viscosity -> efvs (nz-1,nx,ny), zero elsewhere
 void scatter_efvs(const HostPlan& p, int b, const double* efvs_elem,
                   double* efvs);

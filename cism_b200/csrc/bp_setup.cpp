@@ -71,6 +71,9 @@ extern "C" int bp_setup(const bp_model* m, bp_setup_arrays* o, double* uvel,
   if (m->sliding && (m->sliding->law != m->which_babc || !o->f_ground ||
                      (m->sliding->law == 10 && !o->flwa_basal_stag)))
     return BP_ERR_ARGS;
+  // 3-D Blatter-Pattyn, or the shallow-shelf or L1L2 2-D solve
+  if (m->approx_2d != 0 && m->approx_2d != 1 && m->approx_2d != 3) return BP_ERR_ARGS;
+  if (m->approx_2d == 3 && (!o->dusrf_dx || !o->dusrf_dy)) return BP_ERR_ARGS;
   const Cells C{nx, ny};
   const Verts V{nx, ny};
   const size_t ncell = (size_t)nx * ny, nvert = (size_t)(nx - 1) * (ny - 1), n3 = nvert * nz;
@@ -174,6 +177,10 @@ extern "C" int bp_setup(const bp_model* m, bp_setup_arrays* o, double* uvel,
     }
   bp::halo_stag(nx, ny, 1, m->periodic, dsdx.data());
   bp::halo_stag(nx, ny, 1, m->periodic, dsdy.data());
+  if (m->approx_2d == 3) {  // the L1L2 viscosity and reconstruction read it
+    std::memcpy(o->dusrf_dx, dsdx.data(), nvert * sizeof(double));
+    std::memcpy(o->dusrf_dy, dsdy.data(), nvert * sizeof(double));
+  }
 
   // get_vertex_geometry, :4163-4313
   std::memset(o->active_cell, 0, ncell * sizeof(int));
@@ -413,7 +420,16 @@ extern "C" int bp_setup(const bp_model* m, bp_setup_arrays* o, double* uvel,
     in->pcg_maxiters = m->pcg_maxiters; in->pcg_ncheck = m->pcg_ncheck; in->pcg_tol = m->pcg_tol;
     in->precision = m->precision; in->inner_tol = m->inner_tol;
     in->sliding = m->sliding ? &o->sliding : nullptr;
-    in->approx_ssa = m->approx_ssa;
+    in->approx_2d = m->approx_2d;
+    if (m->approx_2d == 3) {
+      o->l1l2.thck = m->thck;
+      o->l1l2.flwa = m->flwa;
+      o->l1l2.dusrf_dx = o->dusrf_dx;
+      o->l1l2.dusrf_dy = o->dusrf_dy;
+      o->l1l2.rhoi = m->rhoi;
+      o->l1l2.grav = m->grav;
+      in->l1l2 = &o->l1l2;
+    }
   }
   return BP_OK;
 }
@@ -427,6 +443,7 @@ extern "C" int bp_velo_higher_solve(bp_ctx* ctx, const bp_model* m, double* uvel
       fl((size_t)(m->nz - 1) * ncell), lu(n3), lv(n3);
   std::vector<int> ac(ncell), av(nvert), um(n3), vm(n3);
   std::vector<double> fg(m->sliding ? nvert : 0), fbs(m->sliding ? nvert : 0);
+  std::vector<double> gx(m->approx_2d == 3 ? nvert : 0), gy(m->approx_2d == 3 ? nvert : 0);
   bp_setup_arrays o{};
   o.sigma = sigma.data(); o.stagusrf = su.data(); o.stagthck = sh.data();
   o.beta_internal = beta.data(); o.flwafact = fl.data(); o.active_cell = ac.data();
@@ -435,6 +452,10 @@ extern "C" int bp_velo_higher_solve(bp_ctx* ctx, const bp_model* m, double* uvel
   if (m->sliding) {
     o.f_ground = fg.data();
     o.flwa_basal_stag = fbs.data();
+  }
+  if (m->approx_2d == 3) {
+    o.dusrf_dx = gx.data();
+    o.dusrf_dy = gy.data();
   }
   bp_inputs in;
   const int rc = bp_setup(m, &o, uvel, vvel, &in);

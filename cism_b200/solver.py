@@ -58,6 +58,12 @@ class Sliding(C.Structure):
     ]
 
 
+class L1L2(C.Structure):
+    """bp_l1l2: the fields of the L1L2 solve beyond the shallow-shelf ones."""
+    _fields_ = [("thck", _dp), ("flwa", _dp), ("dusrf_dx", _dp), ("dusrf_dy", _dp),
+                ("rhoi", C.c_double), ("grav", C.c_double)]
+
+
 class Inputs(C.Structure):
     _fields_ = [
         ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("nhalo", C.c_int),
@@ -69,7 +75,8 @@ class Inputs(C.Structure):
         ("which_assemble_beta", C.c_int), ("which_resid", C.c_int), ("pcg_variant", C.c_int),
         ("which_precond", C.c_int), ("maxiter_nonlinear", C.c_int), ("pcg_maxiters", C.c_int),
         ("pcg_ncheck", C.c_int), ("pcg_tol", C.c_double), ("precision", C.c_int),
-        ("inner_tol", C.c_double), ("sliding", C.POINTER(Sliding)), ("approx_ssa", C.c_int),
+        ("inner_tol", C.c_double), ("sliding", C.POINTER(Sliding)), ("approx_2d", C.c_int),
+        ("l1l2", C.POINTER(L1L2)),
     ]
 
 
@@ -103,7 +110,7 @@ class Model(C.Structure):
         ("which_assemble_taud", C.c_int), ("which_ground", C.c_int),
         ("maxiter_nonlinear", C.c_int), ("pcg_maxiters", C.c_int), ("pcg_ncheck", C.c_int),
         ("pcg_tol", C.c_double), ("precision", C.c_int), ("inner_tol", C.c_double),
-        ("sliding", C.POINTER(Sliding)), ("approx_ssa", C.c_int),
+        ("sliding", C.POINTER(Sliding)), ("approx_2d", C.c_int),
     ]
 
 
@@ -111,7 +118,8 @@ class SetupArrays(C.Structure):
     _fields_ = [("sigma", _dp), ("stagusrf", _dp), ("stagthck", _dp), ("beta_internal", _dp),
                 ("flwafact", _dp), ("active_cell", _ip), ("active_vertex", _ip),
                 ("loadu", _dp), ("loadv", _dp), ("umask_dirichlet", _ip), ("vmask_dirichlet", _ip),
-                ("f_ground", _dp), ("flwa_basal_stag", _dp), ("sliding", Sliding)]
+                ("f_ground", _dp), ("flwa_basal_stag", _dp), ("sliding", Sliding),
+                ("dusrf_dx", _dp), ("dusrf_dy", _dp), ("l1l2", L1L2)]
 
 
 SETUP_ARRAYS = [k for k, _ in SetupArrays._fields_[:11]]
@@ -207,7 +215,7 @@ def make_model_struct(m: configs.BPModel, precision: int = FP64, inner_tol: floa
         setattr(s, name, getattr(m, name))
     s.precision = precision
     s.inner_tol = inner_tol
-    s.approx_ssa = m.approx_ssa
+    s.approx_2d = m.approx_2d
     s.sliding = C.cast(None, C.POINTER(Sliding))
     if m.sliding is not None:
         if m.which_babc != m.sliding.law:
@@ -254,6 +262,10 @@ def prepare(m: configs.BPModel, uvel=None, vvel=None, precision: int = FP64,
         arrays["f_ground"] = np.zeros((ny - 1, nx - 1))
         arrays["flwa_basal_stag"] = np.zeros((ny - 1, nx - 1))
         sa.f_ground, sa.flwa_basal_stag = _p(arrays["f_ground"]), _p(arrays["flwa_basal_stag"])
+    if m.approx_2d == configs.APPROX_L1L2:
+        arrays["dusrf_dx"] = np.zeros((ny - 1, nx - 1))
+        arrays["dusrf_dy"] = np.zeros((ny - 1, nx - 1))
+        sa.dusrf_dx, sa.dusrf_dy = _p(arrays["dusrf_dx"]), _p(arrays["dusrf_dy"])
     ms, keep = make_model_struct(m, precision, inner_tol)
     u = np.zeros(m.vshape3) if uvel is None else np.array(uvel, np.float64, copy=True)
     v = np.zeros(m.vshape3) if vvel is None else np.array(vvel, np.float64, copy=True)

@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define BP_ABI_VERSION 3
+#define BP_ABI_VERSION 4
 
 typedef struct bp_ctx bp_ctx;
 
@@ -89,6 +89,21 @@ typedef struct {
   double pseudo_plastic_bedmin, pseudo_plastic_bedmax;   /* m */
 } bp_sliding;
 
+/* Fields of the L1L2 solve (whichapprox = HO_APPROX_L1L2) beyond the
+ * shallow-shelf ones.  The layer viscosities of
+ * compute_effective_viscosity_L1L2 (glissade_velo_higher.F90:7382-7618)
+ * read the flow factor, the surface gradient and the thickness; the 3-D
+ * velocity reconstruction compute_3d_velocity_L1L2 (:5834-6356) the cell
+ * thickness and the same gradient.  The reconstruction's ice mask is taken
+ * as active_cell, which it equals at every owned vertex under the default
+ * which_ho_calving_front (active_ice_mask = ice_mask). */
+typedef struct {
+  const double *thck;                 /* (nx,ny) m */
+  const double *flwa;                 /* (nz-1,nx,ny) Pa^-3 a^-1 */
+  const double *dusrf_dx, *dusrf_dy;  /* (nx-1,ny-1) surface gradient of the setup (:1582) */
+  double rhoi, grav;                  /* kg m^-3, m s^-2 */
+} bp_l1l2;
+
 /* Boundary inputs of one solve: what the setup part of
  * glissade_velo_higher_solve (:987-2199) has computed when the Picard loop
  * starts (:2206).  beta_internal is the calcbeta result for the
@@ -126,11 +141,14 @@ typedef struct {
                                    (FP32-matrix Krylov solve between two FP64
                                    residuals; <= 0: 1e-4) */
   const bp_sliding *sliding;    /* NULL: beta_internal, fixed over the Picard loop */
-  int approx_ssa;               /* 1: shallow-shelf 2-D solve (whichapprox = HO_APPROX_SSA,
-                                   :1125-1128): one unknown pair per column, the
-                                   result copied to every level; 0: 3-D
-                                   Blatter-Pattyn.  Shared by a batch; the SSA
-                                   takes which_precond 0 or 1 */
+  int approx_2d;                /* the 2-D solves (solve_2d, :1125-1128), one unknown
+                                   pair per column: 1 shallow-shelf (HO_APPROX_SSA),
+                                   the result copied to every level; 3 L1L2
+                                   (HO_APPROX_L1L2), the basal velocity and the 3-D
+                                   velocity reconstructed from it (needs l1l2).
+                                   0: the 3-D Blatter-Pattyn solve.  Shared by a
+                                   batch; the 2-D solves take which_precond 0 or 1 */
+  const bp_l1l2 *l1l2;          /* approx_2d = 3 only */
 } bp_inputs;
 
 typedef struct {
@@ -300,7 +318,7 @@ typedef struct {
    * bp_setup computes its f_ground and flwa_basal_stag and takes topg, eus
    * and beta_grounded_min from this struct's fields above */
   const bp_sliding *sliding;
-  int approx_ssa;               /* as in bp_inputs */
+  int approx_2d;                /* as in bp_inputs; bp_setup fills the L1L2 fields */
 } bp_model;
 
 /* Caller-allocated outputs of the setup (sizes as in bp_inputs). */
@@ -317,6 +335,10 @@ typedef struct {
    * flwa_basal_stag ((nx-1,ny-1) each), and the law handed to the solve */
   double *f_ground, *flwa_basal_stag;
   bp_sliding sliding;
+  /* L1L2 only: outputs the surface gradient ((nx-1,ny-1) each) and the
+   * L1L2 fields handed to the solve */
+  double *dusrf_dx, *dusrf_dy;
+  bp_l1l2 l1l2;
 } bp_setup_arrays;
 
 /* Masks, staggering, surface gradient, vertex geometry, flow factor, load

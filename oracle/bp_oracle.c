@@ -1539,25 +1539,34 @@ void orc_setup_free(orc_setup *s) {
  * :8582-8764), so those are called with nz = 1.
  * ------------------------------------------------------------------- */
 
-/* get_basis_function_derivatives_2d (:6583-6751). */
-static int basis_derivs_2d(const double *x, const double *y, int p, double *dx,
-                           double *dy, double *detJ) {
+/* get_basis_function_derivatives_2d (:6583-6751) with the reference
+ * element's derivatives dxr, dyr at one point (a quadrature point, or the
+ * element centre, :589-597). */
+static int basis_derivs_2d_at(const double *x, const double *y, const double *dxr,
+                              const double *dyr, double *dx, double *dy, double *detJ) {
   double J11 = 0.0, J12 = 0.0, J21 = 0.0, J22 = 0.0;
   for (int n = 0; n < 4; ++n) {
-    J11 = J11 + dxr2[n][p] * x[n];
-    J12 = J12 + dxr2[n][p] * y[n];
-    J21 = J21 + dyr2[n][p] * x[n];
-    J22 = J22 + dyr2[n][p] * y[n];
+    J11 = J11 + dxr[n] * x[n];
+    J12 = J12 + dxr[n] * y[n];
+    J21 = J21 + dyr[n] * x[n];
+    J22 = J22 + dyr[n] * y[n];
   }
   const double d = J11 * J22 - J12 * J21;
   *detJ = d;
   if (!(fabs(d) > 0.0)) return ORC_ERR_SINGULAR_JAC;
   const double i11 = J22 / d, i12 = -J12 / d, i21 = -J21 / d, i22 = J11 / d;
   for (int n = 0; n < 4; ++n) {
-    dx[n] = i11 * dxr2[n][p] + i12 * dyr2[n][p];
-    dy[n] = i21 * dxr2[n][p] + i22 * dyr2[n][p];
+    dx[n] = i11 * dxr[n] + i12 * dyr[n];
+    dy[n] = i21 * dxr[n] + i22 * dyr[n];
   }
   return ORC_OK;
+}
+
+static int basis_derivs_2d(const double *x, const double *y, int p, double *dx,
+                           double *dy, double *detJ) {
+  double dxr[4], dyr[4];
+  for (int n = 0; n < 4; ++n) { dxr[n] = dxr2[n][p]; dyr[n] = dyr2[n][p]; }
+  return basis_derivs_2d_at(x, y, dxr, dyr, dx, dy, detJ);
 }
 
 /* compute_effective_viscosity, SSA branch (:7199-7378) with the vertically
@@ -1587,18 +1596,78 @@ static double effective_viscosity_ssa(int whichefvs, double efvs_constant,
   return flwafact * pow(sq, p2_effstr);
 }
 
-/* assemble_stiffness_matrix_2d, SSA branch (:5208-5595): per active cell,
- * 2x2 Gauss points, efvs from the vertically averaged flow factor
- * (glissade_vertical_average, glissade_grid_operators.F90:1172-1236),
+/* compute_effective_viscosity_L1L2 (:7382-7618): the viscosity of each
+ * layer k = 1..nz-1 at one quadrature point (phi, dx, dy its basis values
+ * and derivatives; u, v, h, dsdx, dsdy the corner values).  With Glen's
+ * law (n = 3) tau_parallel solves x^3 + a x + b = 0, a = tau_perp^2 =
+ * (rhoi grav (h sigma(k+1)) |grad s|)^2, b = -effstrain / A, by Cardano's
+ * formula: x = (-b/2 + c)^(1/3) - (b/2 + c)^(1/3), c = sqrt(b^2/4 +
+ * a^3/27), the second root in its first-order form -a / (3 |b|^(1/3))
+ * when a^3/27 <= 1e-6 b^2/4; then efvs = 1 / (2 A (x^2 + tau_perp^2)). */
+static void effective_viscosity_l1l2(int whichefvs, double efvs_constant, int nz,
+                                     const double *sigma, int p, const double *dx,
+                                     const double *dy, const double *u, const double *v,
+                                     const double *h, const double *dsdx, const double *dsdy,
+                                     const double *flwa, const double *flwafact, double rhoi,
+                                     double grav, double *efvs) {
+  const double effstrain_min = 1.0e-8;
+  const double p_effstr = (1.0 - 3.0) / 3.0;
+  if (whichefvs == ORC_EFVS_CONSTANT) {
+    for (int k = 0; k < nz - 1; ++k) efvs[k] = efvs_constant;
+    return;
+  }
+  if (whichefvs == ORC_EFVS_FLOWFACT) {
+    const double scyr = 31536000.0;
+    const double effstrain = (500.0 / scyr) / 200.0e3 * scyr;
+    for (int k = 0; k < nz - 1; ++k) efvs[k] = flwafact[k] * pow(effstrain, p_effstr);
+    return;
+  }
+  double ux = 0.0, uy = 0.0, vx = 0.0, vy = 0.0, sx = 0.0, sy = 0.0, thck = 0.0;
+  for (int n = 0; n < 4; ++n) {
+    ux = ux + dx[n] * u[n];
+    uy = uy + dy[n] * u[n];
+    vx = vx + dx[n] * v[n];
+    vy = vy + dy[n] * v[n];
+    sx = sx + phi2[n][p] * dsdx[n];
+    sy = sy + phi2[n][p] * dsdy[n];
+    thck = thck + phi2[n][p] * h[n];
+  }
+  const double effstrainsq = effstrain_min * effstrain_min + ux * ux + vy * vy + ux * vy +
+                             0.25 * ((vx + uy) * (vx + uy));
+  const double effstrain = sqrt(effstrainsq);
+  for (int k = 1; k <= nz - 1; ++k) {
+    const double depth = thck * sigma[k];
+    const double grads = sqrt(sx * sx + sy * sy);
+    const double tau_perp = rhoi * grav * depth * grads;
+    const double a = tau_perp * tau_perp;
+    const double b = -effstrain / flwa[k - 1];
+    const double c = sqrt(b * b / 4.0 + a * a * a / 27.0);
+    const double rootA = pow(-b / 2.0 + c, 1.0 / 3.0);
+    double rootB;
+    if (a * a * a / 27.0 > 1.0e-6 * (b * b / 4.0))
+      rootB = -pow(b / 2.0 + c, 1.0 / 3.0);
+    else
+      rootB = -a / (3.0 * pow(fabs(b), 1.0 / 3.0));
+    const double tau_parallel = rootA + rootB;
+    efvs[k - 1] = 1.0 / (2.0 * flwa[k - 1] * (tau_parallel * tau_parallel + tau_perp * tau_perp));
+  }
+}
+
+/* assemble_stiffness_matrix_2d (:5208-5595), SSA and L1L2 branches: per
+ * active cell, 2x2 Gauss points; the SSA efvs from the vertically averaged
+ * flow factor (glissade_vertical_average, glissade_grid_operators.F90:
+ * 1172-1236), the L1L2 efvs of each layer (effective_viscosity_l1l2)
+ * averaged over the column with the weights sigma(k+1) - sigma(k); the
  * element matrix with h efvs (compute_element_matrix :7868-7986), scatter
  * by element_to_global_matrix_2d (:8058-8121); efvs(k,i,j) = the mean of
- * the point values on every layer. */
-static int assemble_ssa(int nx, int ny, int nz, int nhalo, const double *sigma,
-                        const int *active_cell, const double *xVertex,
-                        const double *yVertex, const double *u2, const double *v2,
-                        const double *stagthck, const double *flwafact,
-                        int whichefvs, double efvs_constant, double *efvs,
-                        double *Auu, double *Auv, double *Avu, double *Avv) {
+ * the point values of layer k (SSA: the one value on every layer). */
+static int assemble_2d(int approx, int nx, int ny, int nz, int nhalo, const double *sigma,
+                       const int *active_cell, const double *xVertex,
+                       const double *yVertex, const double *u2, const double *v2,
+                       const double *stagthck, const double *flwafact, const double *flwa,
+                       const double *dusrf_dx, const double *dusrf_dy, double rhoi,
+                       double grav, int whichefvs, double efvs_constant, double *efvs,
+                       double *Auu, double *Auv, double *Avu, double *Avv) {
   init_tables();
   const double vol0 = 1.0e9;
   const size_t nvx = (size_t)(nx - 1) * (ny - 1);
@@ -1607,6 +1676,7 @@ static int assemble_ssa(int nx, int ny, int nz, int nhalo, const double *sigma,
   memset(Avu, 0, 27 * nvx * sizeof(double));
   memset(Avv, 0, 27 * nvx * sizeof(double));
   memset(efvs, 0, (size_t)(nz - 1) * nx * ny * sizeof(double));
+  double *eq = malloc((size_t)4 * (nz - 1) * sizeof(double));  /* efvs_qp(k,p) */
   for (int j = nhalo + 1; j <= ny - nhalo + 1; ++j)
     for (int i = nhalo + 1; i <= nx - nhalo + 1; ++i) {
       if (!active_cell[IC(i, j)]) continue;
@@ -1614,7 +1684,7 @@ static int assemble_ssa(int nx, int ny, int nz, int nhalo, const double *sigma,
       for (int k = 1; k <= nz - 1; ++k)
         fl2 = fl2 + flwafact[IFL(k, i, j)] * (sigma[k] - sigma[k - 1]);
       double Kuu[4][4] = {{0}}, Kuv[4][4] = {{0}}, Kvu[4][4] = {{0}}, Kvv[4][4] = {{0}};
-      double x[4], y[4], u[4], v[4], h[4], efvs_qp[4];
+      double x[4], y[4], u[4], v[4], h[4], sx[4], sy[4], efvs_qp[4];
       for (int n = 0; n < 4; ++n) {
         const int iv = i + ishift[2][n], jv = j + jshift[2][n];
         x[n] = xVertex[IV(iv, jv)];
@@ -1622,11 +1692,22 @@ static int assemble_ssa(int nx, int ny, int nz, int nhalo, const double *sigma,
         u[n] = u2[IV(iv, jv)];
         v[n] = v2[IV(iv, jv)];
         h[n] = stagthck[IV(iv, jv)];
+        sx[n] = dusrf_dx ? dusrf_dx[IV(iv, jv)] : 0.0;
+        sy[n] = dusrf_dy ? dusrf_dy[IV(iv, jv)] : 0.0;
       }
       for (int p = 0; p < 4; ++p) {
         double ddx[4], ddy[4], detJ;
-        if (basis_derivs_2d(x, y, p, ddx, ddy, &detJ) != ORC_OK) return ORC_ERR_SINGULAR_JAC;
-        efvs_qp[p] = effective_viscosity_ssa(whichefvs, efvs_constant, ddx, ddy, u, v, fl2);
+        if (basis_derivs_2d(x, y, p, ddx, ddy, &detJ) != ORC_OK) { free(eq); return ORC_ERR_SINGULAR_JAC; }
+        if (approx == ORC_APPROX_L1L2) {
+          double *ek = eq + (size_t)p * (nz - 1);
+          effective_viscosity_l1l2(whichefvs, efvs_constant, nz, sigma, p, ddx, ddy, u, v, h, sx, sy,
+                                   &flwa[IFL(1, i, j)], &flwafact[IFL(1, i, j)], rhoi, grav, ek);
+          efvs_qp[p] = 0.0;
+          for (int k = 1; k <= nz - 1; ++k) efvs_qp[p] = efvs_qp[p] + ek[k - 1] * (sigma[k] - sigma[k - 1]);
+        } else {
+          efvs_qp[p] = effective_viscosity_ssa(whichefvs, efvs_constant, ddx, ddy, u, v, fl2);
+          for (int k = 1; k <= nz - 1; ++k) eq[(size_t)p * (nz - 1) + k - 1] = efvs_qp[p];
+        }
         double h_qp = 0.0;
         for (int n = 0; n < 4; ++n) h_qp = h_qp + phi2[n][p] * h[n];
         const double f = h_qp * efvs_qp[p] * wqp2[p] * detJ / vol0;
@@ -1640,14 +1721,14 @@ static int assemble_ssa(int nx, int ny, int nz, int nhalo, const double *sigma,
       }
       for (int k = 1; k <= nz - 1; ++k) {
         double e = 0.0;
-        for (int p = 0; p < 4; ++p) e = e + efvs_qp[p];
+        for (int p = 0; p < 4; ++p) e = e + eq[(size_t)p * (nz - 1) + k - 1];
         efvs[IFL(k, i, j)] = e / 4;
       }
       for (int a = 0; a < 4; ++a)
         for (int b = 0; b < 4; ++b) {
-          if (fabs(Kuu[a][b] - Kuu[b][a]) > 1.0e-10) return ORC_ERR_ASYMMETRIC_ELEMENT;
-          if (fabs(Kvv[a][b] - Kvv[b][a]) > 1.0e-10) return ORC_ERR_ASYMMETRIC_ELEMENT;
-          if (fabs(Kuv[a][b] - Kvu[b][a]) > 1.0e-10) return ORC_ERR_ASYMMETRIC_ELEMENT;
+          if (fabs(Kuu[a][b] - Kuu[b][a]) > 1.0e-10) { free(eq); return ORC_ERR_ASYMMETRIC_ELEMENT; }
+          if (fabs(Kvv[a][b] - Kvv[b][a]) > 1.0e-10) { free(eq); return ORC_ERR_ASYMMETRIC_ELEMENT; }
+          if (fabs(Kuv[a][b] - Kvu[b][a]) > 1.0e-10) { free(eq); return ORC_ERR_ASYMMETRIC_ELEMENT; }
         }
       for (int nr = 0; nr < 4; ++nr) {
         const int ii = i + ishift[2][nr], jj = j + jshift[2][nr];
@@ -1660,7 +1741,139 @@ static int assemble_ssa(int nx, int ny, int nz, int nhalo, const double *sigma,
         }
       }
     }
+  free(eq);
   return ORC_OK;
+}
+
+/* compute_3d_velocity_L1L2 (:5834-6356), the vertex method (edge_velocity
+ * = .false.): from the basal velocity (uvel, vvel)(nz,:,:) and the layer
+ * viscosities of the last assembly, at cell centres the strain rates,
+ * tau_parallel = 2 efvs eps_parallel and the integral of efvs from the top
+ * of the column to the base of each layer; at the owned active vertices
+ * the shear stresses tau_xz, tau_yz of each layer midpoint (the SIA stress
+ * plus the horizontal gradients of the integrated membrane stresses,
+ * glissade_gradient with the ice mask, margin 1) and the upward integral
+ * u(k) = u(k+1) + 2 A tau_eff^2 (sigma(k+1) - sigma(k)) H tau_xz with A
+ * and tau_parallel staggered over the ice cells (glissade_stagger margin
+ * 1) and tau_eff^(n-1) = tau_eff^2 for n = 3.  Levels 1..nz-1 are zero
+ * elsewhere; prescribed basal vertices keep the basal value on every
+ * level.  Ends with the halo update (:3800-3801). */
+static double grad_edges(double a, double b, int ma, int mb) {
+  if (ma && mb) return (a + b) / 2.0;
+  if (ma) return a;
+  if (mb) return b;
+  return 0.0;
+}
+
+/* glissade_gradient (glissade_grid_operators.F90:235-410) with
+ * gradient_margin = 1: at each vertex the mean of the two edge differences
+ * whose cells both hold ice, the one such edge, or zero. */
+static void glissade_gradient_margin1(int nx, int ny, double dx, double dy, const double *f,
+                                      double *df_dx, double *df_dy, const int *ice_mask) {
+  for (int j = 1; j <= ny - 1; ++j)
+    for (int i = 1; i <= nx - 1; ++i) {
+      const int sw = ice_mask[IC(i, j)], se = ice_mask[IC(i + 1, j)];
+      const int nw = ice_mask[IC(i, j + 1)], ne = ice_mask[IC(i + 1, j + 1)];
+      const double north = (f[IC(i + 1, j + 1)] - f[IC(i, j + 1)]) / dx;
+      const double south = (f[IC(i + 1, j)] - f[IC(i, j)]) / dx;
+      df_dx[IV(i, j)] = grad_edges(north, south, ne == 1 && nw == 1, se == 1 && sw == 1);
+      const double east = (f[IC(i + 1, j + 1)] - f[IC(i + 1, j)]) / dy;
+      const double west = (f[IC(i, j + 1)] - f[IC(i, j)]) / dy;
+      df_dy[IV(i, j)] = grad_edges(east, west, ne == 1 && se == 1, nw == 1 && sw == 1);
+    }
+}
+
+static void velocity_3d_l1l2(int nx, int ny, int nz, int nhalo, int periodic, const double *sigma,
+                             double dx, double dy, const int *ice_mask, const int *active_cell,
+                             const int *active_vertex, const int *umask_bed, const int *vmask_bed,
+                             const double *xVertex, const double *yVertex, const double *thck,
+                             const double *stagthck, const double *dusrf_dx,
+                             const double *dusrf_dy, const double *flwa, const double *efvs,
+                             double rhoi, double grav, double *uvel, double *vvel) {
+  init_tables();
+  const size_t nc = (size_t)nx * ny, nl = (size_t)(nz - 1), nvx = (size_t)(nx - 1) * (ny - 1);
+  double *ux = calloc(nc, 8), *uy = calloc(nc, 8), *vx = calloc(nc, 8), *vy = calloc(nc, 8);
+  double *tau_par = calloc(nl * nc, 8), *eint = calloc(nl * nc, 8);
+  double *w1 = calloc(nc, 8), *w2 = calloc(nc, 8), *w3 = calloc(nc, 8), *lay = calloc(nc, 8);
+  double *txz = calloc(nl * nvx, 8), *tyz = calloc(nl * nvx, 8);
+  double *d1x = calloc(nvx, 8), *d1y = calloc(nvx, 8), *d2x = calloc(nvx, 8), *d2y = calloc(nvx, 8),
+         *d3x = calloc(nvx, 8), *d3y = calloc(nvx, 8), *stp = calloc(nvx, 8), *stf = calloc(nvx, 8);
+  const double dxr_ctr[4] = {-(1.0 - 0.0) / 4.0, (1.0 - 0.0) / 4.0, (1.0 + 0.0) / 4.0, -(1.0 + 0.0) / 4.0};
+  const double dyr_ctr[4] = {-(1.0 - 0.0) / 4.0, -(1.0 + 0.0) / 4.0, (1.0 + 0.0) / 4.0, (1.0 - 0.0) / 4.0};
+#define L3(k, i, j) (IC(i, j) * nl + ((size_t)(k) - 1))
+#define LV(k, i, j) (IV(i, j) * nl + ((size_t)(k) - 1))
+  for (int j = nhalo + 1; j <= ny - nhalo + 1; ++j)
+    for (int i = nhalo + 1; i <= nx - nhalo + 1; ++i) {
+      if (!active_cell[IC(i, j)]) continue;
+      double x[4], y[4], u[4], v[4], ddx[4], ddy[4], detJ;
+      for (int n = 0; n < 4; ++n) {
+        const int iv = i + ishift[2][n], jv = j + jshift[2][n];
+        x[n] = xVertex[IV(iv, jv)];
+        y[n] = yVertex[IV(iv, jv)];
+        u[n] = uvel[IX(nz, iv, jv)];
+        v[n] = vvel[IX(nz, iv, jv)];
+      }
+      basis_derivs_2d_at(x, y, dxr_ctr, dyr_ctr, ddx, ddy, &detJ);
+      const size_t c = IC(i, j);
+      for (int n = 0; n < 4; ++n) {
+        ux[c] = ux[c] + ddx[n] * u[n];
+        uy[c] = uy[c] + ddy[n] * u[n];
+        vx[c] = vx[c] + ddx[n] * v[n];
+        vy[c] = vy[c] + ddy[n] * v[n];
+      }
+      const double eps = sqrt(ux[c] * ux[c] + vy[c] * vy[c] + ux[c] * vy[c] +
+                              0.25 * ((vx[c] + uy[c]) * (vx[c] + uy[c])));
+      for (int k = 1; k <= nz - 1; ++k) tau_par[L3(k, i, j)] = 2.0 * efvs[IFL(k, i, j)] * eps;
+      eint[L3(1, i, j)] = efvs[IFL(1, i, j)] * (sigma[1] - sigma[0]) * thck[c];
+      for (int k = 2; k <= nz - 1; ++k)
+        eint[L3(k, i, j)] = eint[L3(k - 1, i, j)] + efvs[IFL(k, i, j)] * (sigma[k] - sigma[k - 1]) * thck[c];
+    }
+  int ilo, ihi, jlo, jhi;
+  owned_range(nx, ny, periodic, &ilo, &ihi, &jlo, &jhi);
+  for (int k = 1; k <= nz - 1; ++k) {
+    for (size_t c = 0; c < nc; ++c) {
+      w1[c] = eint[c * nl + k - 1] * (2.0 * ux[c] + vy[c]);
+      w2[c] = eint[c * nl + k - 1] * (uy[c] + vx[c]);
+      w3[c] = eint[c * nl + k - 1] * (2.0 * vy[c] + ux[c]);
+    }
+    glissade_gradient_margin1(nx, ny, dx, dy, w1, d1x, d1y, ice_mask);
+    glissade_gradient_margin1(nx, ny, dx, dy, w2, d2x, d2y, ice_mask);
+    glissade_gradient_margin1(nx, ny, dx, dy, w3, d3x, d3y, ice_mask);
+    for (int j = jlo; j <= jhi; ++j)
+      for (int i = ilo; i <= ihi; ++i) {
+        const size_t w = IV(i, j);
+        if (!active_vertex[w]) continue;
+        const double depth = 0.5 * (sigma[k - 1] + sigma[k]) * stagthck[w];
+        txz[LV(k, i, j)] = -rhoi * grav * depth * dusrf_dx[w] + 2.0 * d1x[w] + d2y[w];
+        tyz[LV(k, i, j)] = -rhoi * grav * depth * dusrf_dy[w] + d2x[w] + 2.0 * d3y[w];
+      }
+  }
+  for (int j = 1; j <= ny - 1; ++j)
+    for (int i = 1; i <= nx - 1; ++i)
+      for (int k = 1; k <= nz - 1; ++k) { uvel[IX(k, i, j)] = 0.0; vvel[IX(k, i, j)] = 0.0; }
+  for (int k = nz - 1; k >= 1; --k) {
+    for (size_t c = 0; c < nc; ++c) lay[c] = tau_par[c * nl + k - 1];
+    orc_stagger(nx, ny, lay, stp, ice_mask, 1);
+    for (size_t c = 0; c < nc; ++c) lay[c] = flwa[c * nl + k - 1];
+    orc_stagger(nx, ny, lay, stf, ice_mask, 1);
+    for (int j = jlo; j <= jhi; ++j)
+      for (int i = ilo; i <= ihi; ++i) {
+        const size_t w = IV(i, j);
+        if (!active_vertex[w]) continue;
+        const double tx = txz[LV(k, i, j)], ty = tyz[LV(k, i, j)];
+        const double tau_eff_sq = stp[w] * stp[w] + tx * tx + ty * ty;
+        const double fact = 2.0 * stf[w] * tau_eff_sq * (sigma[k] - sigma[k - 1]) * stagthck[w];
+        uvel[IX(k, i, j)] = umask_bed[w] == 1 ? uvel[IX(nz, i, j)] : uvel[IX(k + 1, i, j)] + fact * tx;
+        vvel[IX(k, i, j)] = vmask_bed[w] == 1 ? vvel[IX(nz, i, j)] : vvel[IX(k + 1, i, j)] + fact * ty;
+      }
+  }
+#undef L3
+#undef LV
+  orc_halo_stag(nx, ny, nz, periodic, uvel);
+  orc_halo_stag(nx, ny, nz, periodic, vvel);
+  free(ux); free(uy); free(vx); free(vy); free(tau_par); free(eint);
+  free(w1); free(w2); free(w3); free(lay); free(txz); free(tyz);
+  free(d1x); free(d1y); free(d2x); free(d2y); free(d3x); free(d3y); free(stp); free(stf);
 }
 
 /* compute_residual_velocity_2d (:9238-9351): no bed layer to leave out. */
@@ -1686,20 +1899,22 @@ static double residual_velocity_2d(int nx, int ny, int periodic, int whichresid,
   return r;
 }
 
-/* One assembled 2-D system of the SSA branch at (u2, v2) (nx-1,ny-1): the
+/* One assembled 2-D system of the SSA or L1L2 branch at (u2, v2) (nx-1,ny-1): the
  * matrix in the kA = 0 slice of (27,1,nx-1,ny-1), b = the level-summed
  * load with the basal term and the Dirichlet rows of the bed level's
  * masks, halo-updated and symmetry-checked (:2703-2990). */
-int orc_assemble_ssa_system(const orc_model *m, const orc_setup *s,
-                            const double *beta_internal, const double *u2,
-                            const double *v2, double *efvs, double *Auu,
-                            double *Auv, double *Avu, double *Avv, double *bu,
-                            double *bv, long *nNonzeros) {
+int orc_assemble_2d_system(const orc_model *m, const orc_setup *s, int approx,
+                           const double *beta_internal, const double *u2,
+                           const double *v2, double *efvs, double *Auu,
+                           double *Auv, double *Avu, double *Avv, double *bu,
+                           double *bv, long *nNonzeros) {
   const int nx = m->nx, ny = m->ny, nz = m->nz;
   const size_t nvx = (size_t)(nx - 1) * (ny - 1);
-  int st = assemble_ssa(nx, ny, nz, m->nhalo, s->sigma, s->active_cell, s->xVertex, s->yVertex, u2,
-                        v2, s->stagthck, s->flwafact, m->which_efvs, m->efvs_constant, efvs, Auu, Auv,
-                        Avu, Avv);
+  if (approx != ORC_APPROX_SSA && approx != ORC_APPROX_L1L2) return ORC_ERR_ARGS;
+  int st = assemble_2d(approx, nx, ny, nz, m->nhalo, s->sigma, s->active_cell, s->xVertex,
+                       s->yVertex, u2, v2, s->stagthck, s->flwafact, m->flwa, s->dusrf_dx,
+                       s->dusrf_dy, m->rhoi, m->grav, m->which_efvs, m->efvs_constant, efvs, Auu,
+                       Auv, Avu, Avv);
   if (st != ORC_OK) return st;
   if (m->which_babc != ORC_BABC_NO_SLIP)
     basal_sliding_bc(nx, ny, 1, m->nhalo, m->dx, m->dy, s->active_cell, s->active_vertex,
@@ -1732,9 +1947,28 @@ int orc_assemble_ssa_system(const orc_model *m, const orc_setup *s,
   return ORC_OK;
 }
 
-int orc_velo_ssa_solve(const orc_model *m, double *uvel, double *vvel,
-                       double *efvs, double *beta_internal, orc_stats *stats) {
+int orc_velocity_3d_l1l2(const orc_model *m, const orc_setup *s, const double *efvs,
+                         double *uvel, double *vvel) {
   const int nx = m->nx, ny = m->ny, nz = m->nz;
+  const size_t nvx = (size_t)(nx - 1) * (ny - 1);
+  int *um = malloc(nvx * sizeof(int)), *vm = malloc(nvx * sizeof(int));
+  for (size_t w = 0; w < nvx; ++w) {
+    um[w] = s->umask_dirichlet[w * nz + (nz - 1)];
+    vm[w] = s->vmask_dirichlet[w * nz + (nz - 1)];
+  }
+  velocity_3d_l1l2(nx, ny, nz, m->nhalo, m->periodic, s->sigma, m->dx, m->dy, s->ice_mask,
+                   s->active_cell, s->active_vertex, um, vm, s->xVertex, s->yVertex, m->thck,
+                   s->stagthck, s->dusrf_dx, s->dusrf_dy, m->flwa, efvs, m->rhoi, m->grav, uvel,
+                   vvel);
+  free(um);
+  free(vm);
+  return ORC_OK;
+}
+
+int orc_velo_2d_solve(const orc_model *m, int approx, double *uvel, double *vvel,
+                      double *efvs, double *beta_internal, orc_stats *stats) {
+  const int nx = m->nx, ny = m->ny, nz = m->nz;
+  if (approx != ORC_APPROX_SSA && approx != ORC_APPROX_L1L2) return ORC_ERR_ARGS;
   const size_t nvx = (size_t)(nx - 1) * (ny - 1), n3 = nvx * nz, nA = nvx * 27;
   orc_setup s;
   orc_setup_alloc(m, &s);
@@ -1763,7 +1997,8 @@ int orc_velo_ssa_solve(const orc_model *m, double *uvel, double *vvel,
     memcpy(us, u2, nvx * 8);
     memcpy(vs, v2, nvx * 8);
     long nnz = 0;
-    st = orc_assemble_ssa_system(m, &s, beta_internal, u2, v2, efvs, Auu, Auv, Avu, Avv, bu, bv, &nnz);
+    st = orc_assemble_2d_system(m, &s, approx, beta_internal, u2, v2, efvs, Auu, Auv, Avu, Avv, bu,
+                                bv, &nnz);
     if (st != ORC_OK) { status = st; break; }
     if (nnz == 0) {
       memset(u2, 0, nvx * 8);
@@ -1771,7 +2006,7 @@ int orc_velo_ssa_solve(const orc_model *m, double *uvel, double *vvel,
       status = ORC_ZERO_MATRIX;
       break;
     }
-    if (m->which_babc == ORC_BABC_NO_SLIP) {  /* SSA on a frozen bed: u = 0 (:3227-3240) */
+    if (m->which_babc == ORC_BABC_NO_SLIP) {  /* frozen bed: u_2d = 0 (:3227-3240) */
       memset(u2, 0, nvx * 8);
       memset(v2, 0, nvx * 8);
       stats->L2_norm = 0.0;
@@ -1806,12 +2041,16 @@ int orc_velo_ssa_solve(const orc_model *m, double *uvel, double *vvel,
       outer_it_criterion = resid_velo; outer_it_target = resid_target;
     }
   }
-  for (int j = 1; j <= ny - 1; ++j)  /* uvel(k,:,:) = uvel_2d for every level (:3745-3750) */
+  /* SSA: uvel(k,:,:) = uvel_2d for every level (:3745-3750); L1L2:
+   * uvel(nz,:,:) = uvel_2d and the 3-D reconstruction (:3759-3801) */
+  for (int j = 1; j <= ny - 1; ++j)
     for (int i = 1; i <= nx - 1; ++i)
       for (int k = 1; k <= nz; ++k) {
         uvel[IX(k, i, j)] = u2[IV(i, j)];
         vvel[IX(k, i, j)] = v2[IV(i, j)];
       }
+  if (approx == ORC_APPROX_L1L2 && (status == ORC_OK || status == ORC_ZERO_MATRIX))
+    orc_velocity_3d_l1l2(m, &s, efvs, uvel, vvel);
   stats->picard_iters = counter;
   stats->converged = (status == ORC_OK && counter < m->maxiter_nonlinear) ? 1 : 0;
   if (status == ORC_OK && !stats->converged) status = ORC_WARN_PICARD_NOT_CONVERGED;

@@ -38,7 +38,8 @@ enum {
   ORC_GRADIENT_MARGIN_LAND = 0, ORC_GRADIENT_MARGIN_HYBRID = 1,
   ORC_GRADIENT_MARGIN_MARINE = 2,
   ORC_ASSEMBLE_STANDARD = 0, ORC_ASSEMBLE_LOCAL = 1,
-  ORC_GROUND_NO_GLP = 0, ORC_GROUND_ALL = 2
+  ORC_GROUND_NO_GLP = 0, ORC_GROUND_ALL = 2,
+  ORC_APPROX_SSA = 1, ORC_APPROX_L1L2 = 3
 };
 
 /* Status codes shared with the product's C ABI. */
@@ -157,10 +158,12 @@ int orc_pcg_chrongear_3d(int nx, int ny, int nz, int periodic,
                          int precond, int maxiters, double tolerance,
                          int ncheck, double *err, int *niters);
 
-/* glissade_velo_higher_solve, shallow-shelf (SSA) branch: the 2-D solve
- * of the depth-integrated velocity, copied to every level. */
-int orc_velo_ssa_solve(const orc_model *m, double *uvel, double *vvel,
-                       double *efvs, double *beta_internal, orc_stats *stats);
+/* glissade_velo_higher_solve, 2-D branches (solve_2d, :1125-1128):
+ * approx = ORC_APPROX_SSA, the depth-integrated velocity copied to every
+ * level; ORC_APPROX_L1L2, the basal velocity of the L1L2 equations and the
+ * 3-D velocity reconstructed from it. */
+int orc_velo_2d_solve(const orc_model *m, int approx, double *uvel, double *vvel,
+                      double *efvs, double *beta_internal, orc_stats *stats);
 
 /* Post-solve diagnostics (glissade_velo_higher.F90:3847-3872). */
 int orc_internal_stress(int nx, int ny, int nz, int nhalo, const double *sigma,
@@ -207,14 +210,19 @@ int orc_assemble_system(const orc_model *m, const orc_setup *s,
                         const double *vvel, double *efvs, double *Auu,
                         double *Auv, double *Avu, double *Avv, double *bu,
                         double *bv, long *nNonzeros);
-/* One assembled 2-D system of the shallow-shelf branch at a 2-D velocity
- * ((nx-1,ny-1) arrays; the matrix in the kA = 0 slice of
+/* One assembled 2-D system of the SSA or L1L2 branch (approx) at a 2-D
+ * velocity ((nx-1,ny-1) arrays; the matrix in the kA = 0 slice of
  * (27,1,nx-1,ny-1)). */
-int orc_assemble_ssa_system(const orc_model *m, const orc_setup *s,
-                            const double *beta_internal, const double *u2,
-                            const double *v2, double *efvs, double *Auu,
-                            double *Auv, double *Avu, double *Avv, double *bu,
-                            double *bv, long *nNonzeros);
+int orc_assemble_2d_system(const orc_model *m, const orc_setup *s, int approx,
+                           const double *beta_internal, const double *u2,
+                           const double *v2, double *efvs, double *Auu,
+                           double *Auv, double *Avu, double *Avv, double *bu,
+                           double *bv, long *nNonzeros);
+/* compute_3d_velocity_L1L2 and the halo update that follows it: levels
+ * 1..nz-1 of (uvel, vvel) from the basal level nz and the layer
+ * viscosities efvs (nz-1,nx,ny) of the last assembly. */
+int orc_velocity_3d_l1l2(const orc_model *m, const orc_setup *s, const double *efvs,
+                         double *uvel, double *vvel);
 /* Whole glissade_velo_higher_solve, 3-D Blatter-Pattyn branch. */
 int orc_velo_higher_solve(const orc_model *m, double *uvel, double *vvel,
                           double *efvs, double *beta_internal,

@@ -154,9 +154,14 @@ def velo_higher_solve(m, uvel=None, vvel=None):
     return u, v, efvs, beta, st.as_dict()
 
 
-def velo_ssa_solve(m, uvel=None, vvel=None):
-    """Shallow-shelf (SSA) branch of the solve; returns (uvel, vvel, efvs,
-    beta_internal, stats), the 2-D velocity on every level."""
+APPROX_SSA, APPROX_L1L2 = 1, 3  # whichapprox, libglide/glide_types.F90:255-259
+
+
+def velo_2d_solve(m, approx, uvel=None, vvel=None):
+    """A 2-D branch of the solve (approx = APPROX_SSA or APPROX_L1L2);
+    returns (uvel, vvel, efvs, beta_internal, stats): the SSA velocity on
+    every level, or the L1L2 basal velocity with the 3-D velocity
+    reconstructed above it."""
     keep = _Keep()
     om = make_model(m, keep)
     u = np.zeros(m.vshape3) if uvel is None else np.array(uvel, dtype=np.float64, copy=True)
@@ -164,8 +169,20 @@ def velo_ssa_solve(m, uvel=None, vvel=None):
     efvs = np.zeros((m.ny, m.nx, m.nz - 1))
     beta = np.zeros((m.ny - 1, m.nx - 1))
     st = OrcStats()
-    lib().orc_velo_ssa_solve(C.byref(om), _p(u), _p(v), _p(efvs), _p(beta), C.byref(st))
+    rc = lib().orc_velo_2d_solve(C.byref(om), approx, _p(u), _p(v), _p(efvs), _p(beta), C.byref(st))
+    if rc == 10:
+        raise RuntimeError("orc_velo_2d_solve: bad arguments")
     return u, v, efvs, beta, st.as_dict()
+
+
+def velo_ssa_solve(m, uvel=None, vvel=None):
+    """Shallow-shelf (SSA) branch of the solve."""
+    return velo_2d_solve(m, APPROX_SSA, uvel, vvel)
+
+
+def velo_l1l2_solve(m, uvel=None, vvel=None):
+    """L1L2 branch of the solve."""
+    return velo_2d_solve(m, APPROX_L1L2, uvel, vvel)
 
 
 def setup(m, uvel=None, vvel=None):
@@ -253,8 +270,8 @@ def basal_friction_heatflx(m, su, uvel, vvel, beta, which=1):
     return out
 
 
-def assemble_ssa_system(m, su, beta, u2, v2):
-    """One assembled shallow-shelf system at the 2-D velocity (u2, v2)
+def assemble_2d_system(m, su, beta, u2, v2, approx=APPROX_SSA):
+    """One assembled 2-D system (SSA or L1L2) at the 2-D velocity (u2, v2)
     (ny-1, nx-1): A as four (ny-1, nx-1, 1, 27) arrays, b, efvs, nonzeros."""
     keep, om, s = su["_keep"]
     nx, ny, nz = m.nx, m.ny, m.nz
@@ -262,13 +279,29 @@ def assemble_ssa_system(m, su, beta, u2, v2):
     bu, bv = np.zeros((ny - 1, nx - 1)), np.zeros((ny - 1, nx - 1))
     efvs = np.zeros((ny, nx, nz - 1))
     nnz = C.c_long(0)
-    rc = lib().orc_assemble_ssa_system(C.byref(om), C.byref(s), _p(np.ascontiguousarray(beta, np.float64)),
-                                       _p(np.ascontiguousarray(u2, np.float64)),
-                                       _p(np.ascontiguousarray(v2, np.float64)), _p(efvs),
-                                       *[_p(a) for a in A], _p(bu), _p(bv), C.byref(nnz))
+    rc = lib().orc_assemble_2d_system(C.byref(om), C.byref(s), approx,
+                                      _p(np.ascontiguousarray(beta, np.float64)),
+                                      _p(np.ascontiguousarray(u2, np.float64)),
+                                      _p(np.ascontiguousarray(v2, np.float64)), _p(efvs),
+                                      *[_p(a) for a in A], _p(bu), _p(bv), C.byref(nnz))
     if rc != 0:
-        raise RuntimeError(f"orc_assemble_ssa_system failed: {rc}")
+        raise RuntimeError(f"orc_assemble_2d_system failed: {rc}")
     return A, bu, bv, efvs, nnz.value
+
+
+def assemble_ssa_system(m, su, beta, u2, v2):
+    return assemble_2d_system(m, su, beta, u2, v2, APPROX_SSA)
+
+
+def velocity_3d_l1l2(m, su, efvs, uvel, vvel):
+    """compute_3d_velocity_L1L2 (+ halo update): levels 1..nz-1 of copies
+    of (uvel, vvel) from their basal level and the layer viscosities."""
+    keep, om, s = su["_keep"]
+    u = np.array(uvel, dtype=np.float64, copy=True)
+    v = np.array(vvel, dtype=np.float64, copy=True)
+    lib().orc_velocity_3d_l1l2(C.byref(om), C.byref(s), _p(np.ascontiguousarray(efvs, np.float64)),
+                               _p(u), _p(v))
+    return u, v
 
 
 def matvec(m, active_vertex, A, xu, xv):

@@ -17,12 +17,15 @@ struct Emu {
   HostPlan p;
   std::vector<InstParams> inst;
   std::vector<InstState> st;
-  std::vector<double> qp, efvs, badj;
-  std::vector<double2> A, x, b;
+  std::vector<double> qp, efvs, badj, lw;
+  std::vector<double2> A, x, b, x3;
   DevView v;
   void bind() {
     std::memset(&v, 0, sizeof(v));
     v.nz = p.nz; v.ncols = p.ncols; v.nnodes = p.nnodes; v.npad = p.npad;
+    v.solve2d = p.solve2d ? 1 : 0;
+    v.l1l2 = p.l1l2 ? 1 : 0;
+    v.nl = p.nz_out - 1;
     v.ncells = p.ncells; v.nelem = p.nelem; v.ninst = p.ninst; v.ntiles = p.ntiles;
     int anyd = 0;
     for (auto m : p.dmask) anyd |= m != 0;
@@ -36,7 +39,13 @@ struct Emu {
     v.cell_cols = p.cell_cols.data(); v.cell_s = p.cell_s.data(); v.cell_h = p.cell_h.data();
     v.cell_beta = p.cell_beta.data(); v.flwafact = p.flwafact.data();
     qp.assign((size_t)p.nelem * 80, 0.0); v.qp = qp.data();
-    efvs.assign(std::max(p.nelem, 1), 0.0); v.efvs = efvs.data();
+    efvs.assign(std::max(p.nefvs, 1), 0.0); v.efvs = efvs.data();
+    if (p.l1l2) {
+      v.cell_flwa = p.cell_flwa.data(); v.cell_thck = p.cell_thck.data(); v.cell_ds = p.cell_ds.data();
+      v.col_ds = p.col_ds.data(); v.col_h = p.col_h.data();
+      lw.assign(4 * (size_t)v.nl * std::max(p.ncells, 1), 0.0); v.lw = lw.data();
+      x3.assign((size_t)std::max(p.ncols, 1) * (v.nl + 1), double2{0, 0}); v.x3 = x3.data();
+    }
     badj.assign(4 * (size_t)p.npad, 0.0); v.badj = badj.data();
     A.assign(2 * 27 * (size_t)p.npad, double2{0, 0}); v.A = A.data();
     x.assign(p.npad, double2{0, 0}); v.x = x.data();
@@ -262,31 +271,36 @@ extern "C" int emu_diagnostics(const bp_inputs* in, const double* uvel, const do
   return 0;
 }
 
-// One assembled shallow-shelf system at velocity (uvel, vvel) (the bed
-// level is the 2-D velocity) through the device's 2-D bodies: the matrix
-// in (27,1,nx-1,ny-1) and b (nx-1,ny-1); efvs (nz-1,nx,ny).  10 if the plan
-// rejects the inputs or they are not a shallow-shelf problem, 2 for a
-// singular Jacobian.
-extern "C" int emu_assemble_ssa(const bp_inputs* in, const double* uvel, const double* vvel,
-                                double* Auu, double* Auv, double* Avu, double* Avv, double* bu,
-                                double* bv, double* efvs) {
+// One assembled 2-D system (shallow-shelf or L1L2) at velocity (uvel,
+// vvel) (the bed level is the 2-D velocity) through the device's 2-D
+// bodies: the matrix in (27,1,nx-1,ny-1) and b (nx-1,ny-1); efvs
+// (nz-1,nx,ny).  10 if the plan rejects the inputs or they are not a 2-D
+// problem, 2 for a singular Jacobian.
+extern "C" int emu_assemble_2d(const bp_inputs* in, const double* uvel, const double* vvel,
+                               double* Auu, double* Auv, double* Avu, double* Avv, double* bu,
+                               double* bv, double* efvs) {
   Emu E;
   std::string err;
-  if (!build_plan(in, 1, &E.p, &err) || !E.p.ssa) return 10;
+  if (!build_plan(in, 1, &E.p, &err) || !E.p.solve2d) return 10;
   E.bind();
-  E.v.ssa = 1;
   gather_velocity(E.p, 0, uvel, vvel, E.x.data());
   RefTables T;
   fill_ref_tables(&T);
+  const int nl = E.v.nl;
   for (int c = 0; c < E.p.ncells; ++c) {
-    double s = 0.0;
+    double s = 0.0, sk[kNzMax] = {0.0};
     for (int p = 0; p < 4; ++p) {
-      double out[5], eq = 0.0;
-      if (!qp2_element_point(E.v, T, c, p, out, &eq)) return 2;
+      double out[5], eq = 0.0, ek[kNzMax];
+      if (!qp2_element_point(E.v, T, c, p, out, &eq, ek)) return 2;
       std::memcpy(&E.qp[((size_t)c * 8 + p) * 10], out, sizeof(out));
       s += eq;
+      if (E.p.l1l2)
+        for (int k = 0; k < nl; ++k) sk[k] += ek[k];
     }
-    E.efvs[c] = s / 4.0;
+    if (E.p.l1l2)
+      for (int k = 0; k < nl; ++k) E.efvs[(size_t)c * nl + k] = sk[k] / 4.0;
+    else
+      E.efvs[c] = s / 4.0;
   }
   const DevView& v = E.v;
   double* Ad = reinterpret_cast<double*>(E.A.data());
@@ -319,6 +333,31 @@ extern "C" int emu_assemble_ssa(const bp_inputs* in, const double* uvel, const d
   std::memset(bv, 0, tot * 8);
   scatter_vector(E.p, 0, E.b.data(), bu, bv);
   scatter_efvs(E.p, 0, E.efvs.data(), efvs);
+  return 0;
+}
+
+// The L1L2 3-D velocity through the device's reconstruction bodies
+// (l1l2_cell over the cells, l1l2_column over the columns) and the host
+// scatter: basal velocity from the bed level of (uvel, vvel), layer
+// viscosities efvs (nz-1,nx,ny); (uout, vout) (nz,nx-1,ny-1) keep their
+// bed level away from the columns.  10 if the plan rejects the inputs or
+// they are not an L1L2 problem.
+extern "C" int emu_velocity_3d_l1l2(const bp_inputs* in, const double* uvel, const double* vvel,
+                                    const double* efvs, double* uout, double* vout) {
+  Emu E;
+  std::string err;
+  if (!build_plan(in, 1, &E.p, &err) || !E.p.l1l2) return 10;
+  E.bind();
+  gather_velocity(E.p, 0, uvel, vvel, E.x.data());
+  const int nl = E.v.nl, NCELL = E.p.ncells, nx = in->nx;
+  for (int c = 0; c < NCELL; ++c) {
+    const int ic = E.p.cell_ij[c], jc = E.p.cell_ij[NCELL + c];
+    for (int k = 0; k < nl; ++k)
+      E.efvs[(size_t)c * nl + k] = efvs[((size_t)(jc - 1) * nx + (ic - 1)) * nl + k];
+  }
+  for (int c = 0; c < NCELL; ++c) l1l2_cell(E.v, c);
+  for (int col = 0; col < E.p.ncols; ++col) l1l2_column(E.v, col);
+  scatter_velocity_3d(E.p, 0, E.x3.data(), uout, vout);
   return 0;
 }
 

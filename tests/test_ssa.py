@@ -116,7 +116,7 @@ def _ssa_models():
     m4.kinbcmask = np.zeros((m4.ny - 1, m4.nx - 1), np.int32)
     m4.kinbcmask[9:11, 9:11] = 1
     m4.name = "dome_kinematic_flowfact"
-    return [m.copy(approx_ssa=1) for m in (m1, m2, m3, m4)]
+    return [m.copy(approx_2d=configs.APPROX_SSA) for m in (m1, m2, m3, m4)]
 
 
 @pytest.mark.parametrize("m", _ssa_models(), ids=lambda m: m.name)
@@ -134,7 +134,7 @@ def test_device_ssa_bodies_match_oracle(m):
     E = [np.zeros(shp) for _ in range(4)]
     ebu, ebv = np.zeros((m.ny - 1, m.nx - 1)), np.zeros((m.ny - 1, m.nx - 1))
     eef = np.zeros((m.ny, m.nx, m.nz - 1))
-    rc = emu.emu_assemble_ssa(C.byref(prep.inputs), _p(np.ascontiguousarray(u)), _p(np.ascontiguousarray(v)),
+    rc = emu.emu_assemble_2d(C.byref(prep.inputs), _p(np.ascontiguousarray(u)), _p(np.ascontiguousarray(v)),
                               *[_p(a) for a in E], _p(ebu), _p(ebv), _p(eef))
     assert rc == 0
     rows = owned_active_rows(m, su["active_vertex"])
@@ -180,7 +180,7 @@ def test_device_ssa_picard_matches_oracle(ctx, m):
 
 @pytest.mark.gpu
 def test_device_ssa_on_a_frozen_bed_is_zero(ctx):
-    m = configs.dome().copy(approx_ssa=1)
+    m = configs.dome().copy(approx_2d=configs.APPROX_SSA)
     u, v, _, st = ctx.velo_higher_solve(m)
     assert st["status"] == 0 and st["picard_iters"] == 1
     assert np.all(u == 0.0) and np.all(v == 0.0)
