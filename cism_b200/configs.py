@@ -39,7 +39,7 @@ ASSEMBLE_STANDARD, ASSEMBLE_LOCAL = 0, 1
  BABC_COULOMB_POWERLAW_SCHOOF, BABC_COULOMB_POWERLAW_TSAI, BABC_POWERLAW_EFFECPRESS) = 2, 3, 9, 10, 11, 12, 13
 SLIDING_LAWS = (2, 3, 9, 10, 11, 12, 13)
 # the 2-D solves (whichapprox, glide_types.F90:255-259); 0 = the 3-D Blatter-Pattyn solve
-APPROX_SSA, APPROX_L1L2 = 1, 3
+APPROX_SSA, APPROX_L1L2, APPROX_DIVA = 1, 3, 4
 
 
 @dataclasses.dataclass
@@ -110,7 +110,10 @@ class BPModel:
     pcg_tol: float = 1.0e-8
     pcg_ncheck: int = 5
     sliding: Optional[SlidingLaw] = None  # velocity-dependent law (which_babc = sliding.law)
-    approx_2d: int = 0  # 2-D solve: APPROX_SSA (1) or APPROX_L1L2 (3); 0 = 3-D Blatter-Pattyn
+    approx_2d: int = 0  # 2-D solve: APPROX_SSA (1), APPROX_L1L2 (3) or APPROX_DIVA (4); 0 = 3-D Blatter-Pattyn
+    # DIVA: the state of the last solve (uvel_2d, vvel_2d, btractx, btracty
+    # (ny-1, nx-1); efvs (ny, nx, nz-1)); None or a missing key = zero
+    diva_state: Optional[dict] = None
     name: str = ""
 
     @property

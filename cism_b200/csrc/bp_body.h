@@ -389,12 +389,47 @@ BP_HD double l1l2_point_efvs(const InstParams& ip, int nl, const double* flwa, c
   return avg;
 }
 
+// compute_effective_viscosity_diva (:7622-7864), the default non-cubic
+// form: the viscosity of each layer k at one point from the horizontal
+// strain rates g of the mean velocity and the vertical shear (du/dz,
+// dv/dz) = (taux, tauy) stagsigma(k) / efvs_old(k), (taux, tauy) the basal
+// traction at the point.  ek: in the last assembly's values (0 = none yet:
+// the value at the 1e-8 /a strain-rate floor), out the new ones.  Returns
+// the column average sum_k ek[k] (sigma(k+1) - sigma(k)).
+BP_HD double diva_point_efvs(const InstParams& ip, int nl, const double* flwafact, const double* g,
+                             double taux, double tauy, double* ek) {
+  const double p_effstr = (1.0 - 3.0) / 3.0;
+  if (ip.which_efvs == 0) {
+    for (int k = 0; k < nl; ++k) ek[k] = ip.efvs_constant;
+  } else if (ip.which_efvs == 1) {
+    const double scyr = 31536000.0;
+    const double effstrain = (500.0 / scyr) / 200.0e3 * scyr;
+    for (int k = 0; k < nl; ++k) ek[k] = flwafact[k] * pow(effstrain, p_effstr);
+  } else {
+    const double ux = g[0], uy = g[1], vx = g[3], vy = g[4];
+    const double smin = 1.0e-8;
+    for (int k = 0; k < nl; ++k) {
+      if (ek[k] == 0.0) ek[k] = flwafact[k] * pow(smin, p_effstr);
+      const double stagsigma = (ip.sigma[k] + ip.sigma[k + 1]) / 2.0;
+      const double du_dz = taux * stagsigma / ek[k];
+      const double dv_dz = tauy * stagsigma / ek[k];
+      const double sq = smin * smin + ux * ux + vy * vy + ux * vy + 0.25 * ((vx + uy) * (vx + uy)) +
+                        0.25 * (du_dz * du_dz + dv_dz * dv_dz);
+      ek[k] = flwafact[k] * pow(sq, p_effstr / 2);
+    }
+  }
+  double avg = 0.0;
+  for (int k = 0; k < nl; ++k) avg = avg + ek[k] * (ip.sigma[k + 1] - ip.sigma[k]);
+  return avg;
+}
+
 // Point p of cell c: get_basis_function_derivatives_2d (:6583-6751); the
 // shallow-shelf branch of compute_effective_viscosity with the vertically
-// averaged flow factor (v.flwafact[c]), or the L1L2 layer viscosities
-// (l1l2_point_efvs, written to ek) and their column average; f = h efvs w
-// detJ / vol0 with the thickness interpolated to the point (:5507-5515,
-// compute_element_matrix :7868-7986).  false for a singular Jacobian.
+// averaged flow factor (v.flwafact[c]), or the L1L2 or DIVA layer
+// viscosities (written to ek; DIVA also updates v.eq3) and their column
+// average; f = h efvs w detJ / vol0 with the thickness interpolated to the
+// point (:5507-5515, compute_element_matrix :7868-7986).  false for a
+// singular Jacobian.
 BP_HD bool qp2_element_point(const DevView& v, const RefTables& T, int c, int p, double* out,
                              double* efvs_qp, double* ek = nullptr) {
   const InstParams& ip = v.inst[v.cell_inst[c]];
@@ -449,6 +484,20 @@ BP_HD bool qp2_element_point(const DevView& v, const RefTables& T, int c, int p,
     }
     efvs = l1l2_point_efvs(ip, nl, v.cell_flwa + (size_t)c * nl, v.flwafact + (size_t)c * nl, g, sx, sy, h_qp,
                            ek);
+  } else if (v.diva) {
+    // basal traction at the point from the corners' columns (zero outside
+    // an outflow domain, where beta_eff is zero)
+    const int nl = v.nl;
+    double taux = 0.0, tauy = 0.0;
+    for (int n = 0; n < 4; ++n) {
+      const int col = v.cell_cols[n * v.ncells + c];
+      taux += T.phi2[p][n] * (col >= 0 ? v.col_bt[col].x : 0.0);
+      tauy += T.phi2[p][n] * (col >= 0 ? v.col_bt[col].y : 0.0);
+    }
+    double* e3 = v.eq3 + ((size_t)c * 4 + p) * nl;
+    for (int k = 0; k < nl; ++k) ek[k] = e3[k];
+    efvs = diva_point_efvs(ip, nl, v.flwafact + (size_t)c * nl, g, taux, tauy, ek);
+    for (int k = 0; k < nl; ++k) e3[k] = ek[k];
   } else {
     // qp_efvs with no vertical shear is the SSA branch (:7326-7334)
     efvs = qp_efvs(ip.which_efvs, ip.efvs_constant, v.flwafact[c], g);
@@ -632,6 +681,93 @@ BP_HD void l1l2_column(const DevView& v, int col) {
   }
 }
 
+// ---------------------------------------------------------------------
+// DIVA (Goldberg 2011): omega, beta_eff and the 3-D velocity.
+// ---------------------------------------------------------------------
+// compute_integrals_diva (:5601-5726) of cell c from its point viscosities
+// v.eq3: per point the integral of depth / efvs from the bed up to each
+// level, averaged over the points (omega_k, over H), and its
+// layer-midpoint integral over the column (omega, over H).
+BP_HD void diva_cell_integrals(const DevView& v, int c) {
+  const InstParams& ip = v.inst[v.cell_inst[c]];
+  const int nl = v.nl;
+  const double H = v.cell_thck[c];
+  const double* eq = v.eq3 + (size_t)c * 4 * nl;
+  double* omk = v.cell_omk + (size_t)c * (nl + 1);
+  double run[4] = {0.0, 0.0, 0.0, 0.0};
+  omk[nl] = 0.0;
+  for (int k = nl - 1; k >= 0; --k) {
+    const double depth = 0.5 * (ip.sigma[k] + ip.sigma[k + 1]);
+    const double dz = (ip.sigma[k + 1] - ip.sigma[k]) * H;
+    double s = 0.0;
+    for (int p = 0; p < 4; ++p) {
+      run[p] = run[p] + depth / eq[(size_t)p * nl + k] * dz;
+      s = s + run[p];
+    }
+    omk[k] = s / 4.0;
+  }
+  double om = 0.0;
+  for (int k = 0; k < nl; ++k) om = om + 0.5 * (omk[k] + omk[k + 1]) * (ip.sigma[k + 1] - ip.sigma[k]);
+  v.cell_om[c] = om;
+}
+
+// glissade_stagger with stagger_margin 1 over the ice-plus-land cells of
+// column col (NW, NE, SW, SE) of a cell value val(cell) (zero for a cell
+// the device does not hold: ice-free land).
+template <typename F>
+BP_HD double diva_stagger(const DevView& v, int col, F val) {
+  const int nc = v.ncols;
+  const uint8_t bits = v.col_ipl[col];
+  const int order[4] = {2, 3, 0, 1};
+  double s = 0.0;
+  int n = 0;
+  for (int o = 0; o < 4; ++o) {
+    const int q = order[o];
+    if (!((bits >> q) & 1)) continue;
+    const int cell = v.col_cells[q * nc + col];
+    s = s + (cell >= 0 ? val(cell) : 0.0);
+    ++n;
+  }
+  return n > 0 ? s / (double)n : 0.0;
+}
+
+// beta_eff of column col (Goldberg 2011 eq. 40-41, :2750-2790): omega
+// staggered to the vertex, beta_eff = beta / (1 + beta omega), or 1 /
+// omega on a no-slip bed (0 where omega is 0).
+BP_HD void diva_column_beta(const DevView& v, int col) {
+  const InstParams& ip = v.inst[v.col_inst[col]];
+  const double so = diva_stagger(v, col, [&](int cell) { return v.cell_om[cell]; });
+  const double beta = v.col_beta[col];
+  v.col_somega[col] = so;
+  v.col_beff[col] = ip.which_babc == 6 ? (so > 0.0 ? 1.0 / so : 0.0) : beta / (1.0 + beta * so);
+}
+
+// After the linear solve (:3658-3696): the basal traction tau_b = beta_eff
+// u_mean and compute_3d_velocity_diva (:5730-5830) for the mean velocity:
+// u(bed) = u_mean - tau_b omega, u(k) = u(bed) + tau_b omega_k(k) with
+// omega_k staggered level by level.
+BP_HD void diva_column_velocity(const DevView& v, int col) {
+  const int nl = v.nl;
+  const double2 um = v.x[col];
+  const double be = v.col_beff[col], so = v.col_somega[col];
+  double2 bt;
+  bt.x = be * um.x;
+  bt.y = be * um.y;
+  v.col_bt[col] = bt;
+  double2* out = v.x3 + (size_t)col * (nl + 1);
+  double2 ub;
+  ub.x = um.x - bt.x * so;
+  ub.y = um.y - bt.y * so;
+  out[nl] = ub;
+  for (int k = 0; k < nl; ++k) {
+    const double sk = diva_stagger(v, col, [&](int cell) { return v.cell_omk[(size_t)cell * (nl + 1) + k]; });
+    double2 u;
+    u.x = ub.x + bt.x * sk;
+    u.y = ub.y + bt.y * sk;
+    out[k] = u;
+  }
+}
+
 // calcbeta (glissade_basal_traction.F90:67-598) at one vertex for the
 // velocity-dependent laws, from the basal velocity (u, v) in m/a: the
 // speed with its 0.01 m/a floor (:181) and optional cap (:187-189), the law
@@ -691,9 +827,10 @@ BP_HD void row_basal(const DevView& v, const RefTables& T, int col, int k,
   if (B != 0 && B != 3) return;
   if (k != v.nz - 1) return;
   const InstParams& ip = v.inst[v.col_inst[col]];
-  if (ip.which_babc == 6) return;  // HO_BABC_NO_SLIP: no basal term
+  // HO_BABC_NO_SLIP: no basal term, except for DIVA (beta_eff = 1/omega)
+  if (ip.which_babc == 6 && !v.diva) return;
   if (ip.which_assemble_beta == 1) {  // HO_ASSEMBLE_BETA_LOCAL
-    acc[13] += ip.dx * ip.dy / kVol0 * v.col_beta[col];
+    acc[13] += ip.dx * ip.dy / kVol0 * (v.diva ? v.col_beff[col] : v.col_beta[col]);
     return;
   }
   // standard: 2x2 face quadrature of beta * phi_r * phi_c on each bed face;

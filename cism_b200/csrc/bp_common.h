@@ -108,6 +108,7 @@ struct DevView {
   int dry;                 // autotuner pass: Krylov matvecs run every tile, leave the state alone
   int solve2d;             // 2-D solve (shallow-shelf or L1L2): nz = 1, one 2-D element per cell
   int l1l2;                // L1L2: layer viscosities, 3-D velocity reconstructed after the loop
+  int diva;                // DIVA: point viscosities carried between iterations, beta_eff, 3-D velocity each iteration
   int nl;                  // L1L2: layers of the velocity arrays (the model's nz - 1)
   unsigned long long* mv_nodes;  // [2] nodes through FP64 / FP32 Krylov matvecs (timing runs), or null
   const InstParams* inst;
@@ -138,7 +139,15 @@ struct DevView {
   const double* col_ds;    // [2][ncols] surface gradient at the column's vertex
   const double* col_h;     // [ncols] stagthck at the column's vertex
   double* lw;              // [4][nl][ncells] tau_parallel, w1, w2, w3 of the reconstruction
-  double2* x3;             // [ncols][nl+1] reconstructed velocity (k = nl the bed)
+  double2* x3;             // [ncols][nl+1] reconstructed velocity (k = nl the bed); L1L2 and DIVA
+  // DIVA (null otherwise)
+  double* eq3;             // [ncells][4][nl] viscosity of each layer at each point (efvs_qp_3d)
+  double* cell_omk;        // [ncells][nl+1] omega_k (Goldberg eq. 32, over H) per level
+  double* cell_om;         // [ncells] omega (eq. 35, over H)
+  const uint8_t* col_ipl;  // [ncols] ice-plus-land mask of the column's cells, bit q for cell q of col_cells
+  double* col_somega;      // [ncols] omega staggered to the column
+  double* col_beff;        // [ncols] beta_eff (the basal term of the 2-D system)
+  double2* col_bt;         // [ncols] basal traction (btractx, btracty)
   // tiles
   const int* tile_start;   // [ntiles] first node (tiles hold whole columns)
   const int* tile_end;     // [ntiles] one past the last node

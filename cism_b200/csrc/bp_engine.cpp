@@ -106,6 +106,11 @@ struct bp_problem {
   bp::DevView v;
   bool mixed = false;
   double2* x0 = nullptr;
+  // DIVA: the starting 3-D velocity, point viscosities and traction, copied
+  // into the working arrays at the start of every run
+  double2* x3_0 = nullptr;
+  double* eq3_0 = nullptr;
+  double2* bt0 = nullptr;
   cudaGraphExec_t chunk_graph = nullptr;
   cudaGraphExec_t inner_graph = nullptr;
   bool use_graphs = true;
@@ -139,6 +144,7 @@ DevView make_view(Arena& a, cudaStream_t s, const HostPlan& p, bool with_cells, 
   v.nz = p.nz; v.ncols = p.ncols; v.nnodes = p.nnodes; v.npad = p.npad;
   v.solve2d = p.solve2d ? 1 : 0;
   v.l1l2 = p.l1l2 ? 1 : 0;
+  v.diva = p.diva ? 1 : 0;
   v.nl = p.nz_out - 1;
   v.ncells = p.ncells; v.nelem = p.nelem; v.ninst = p.ninst; v.ntiles = p.ntiles;
   int anyd = 0;
@@ -184,6 +190,19 @@ DevView make_view(Arena& a, cudaStream_t s, const HostPlan& p, bool with_cells, 
       UP(double, "col_h", p.col_h, col_h);
       v.lw = a.get<double>(s, "l1l2_work", 4 * (size_t)v.nl * std::max(p.ncells, 1));
       v.x3 = a.get<double2>(s, "x3", (size_t)std::max(p.ncols, 1) * (v.nl + 1));
+    }
+    if (p.diva) {
+      UP(double, "cell_thck", p.cell_thck, cell_thck);
+      UP(uint8_t, "col_ipl", p.col_ipl, col_ipl);
+      v.x3 = a.get<double2>(s, "x3", (size_t)std::max(p.ncols, 1) * (v.nl + 1));
+      v.eq3 = a.get<double>(s, "eq3", (size_t)std::max(p.ncells, 1) * 4 * v.nl);
+      v.cell_omk = a.get<double>(s, "cell_omk", (size_t)std::max(p.ncells, 1) * (v.nl + 1));
+      v.cell_om = a.get<double>(s, "cell_om", p.ncells);
+      v.col_somega = a.get<double>(s, "col_somega", p.ncols);
+      v.col_beff = a.get<double>(s, "col_beff", p.ncols);
+      v.col_bt = a.get<double2>(s, "col_bt", p.ncols);
+      upload(s, a.get<double>(s, "eq3_0", p.eq3_0.size()), p.eq3_0);
+      upload(s, a.get<double2>(s, "bt0", p.col_bt0.size()), p.col_bt0);
     }
     v.badj = a.get<double>(s, "badj", 4 * np);
   }
@@ -536,10 +555,12 @@ void run_picard(bp_problem* P) {
     L(P, C_OTHER, [&] { launch_save_usav(v, s); });
     if (p.any_sliding) L(P, C_OTHER, [&] { launch_slide_beta(v, s); });
     L(P, C_ASM1, [&] { launch_asm_qp(v, s); });
+    if (v.diva) L(P, C_ASM1, [&] { launch_diva_beta(v, s); });  // omega, beta_eff (:2742-2857)
     L(P, C_ASM2, [&] { launch_asm_rows(v, s); });
     L(P, C_RHS, [&] { launch_rhs(v, s); });
     if (!P->tuned) autotune(P);
     linear_solve(P);
+    if (v.diva) L(P, C_OTHER, [&] { launch_diva_velocity(v, s); });  // traction, 3-D velocity (:3658-3696)
     L(P, C_OTHER, [&] { launch_picard_check(v, s); });
     snapshot(c, v, 0);
     if (wait_snapshot(c, 0).picard_active <= 0) break;
@@ -602,6 +623,13 @@ bp_problem* problem_new(bp_ctx* c, Arena* arena, int n, const bp_inputs* in, std
   P->h2d_bytes = g_h2d;
   P->x0 = P->arena->get<double2>(c->stream, "x0", P->plan.npad);
   CK(cudaMemsetAsync(P->x0, 0, sizeof(double2) * P->plan.npad, c->stream));
+  if (P->plan.diva) {
+    const size_t n3 = (size_t)std::max(P->plan.ncols, 1) * P->plan.nz_out;
+    P->x3_0 = P->arena->get<double2>(c->stream, "x3_0", n3);
+    CK(cudaMemsetAsync(P->x3_0, 0, sizeof(double2) * n3, c->stream));
+    P->eq3_0 = P->arena->get<double>(c->stream, "eq3_0", P->plan.eq3_0.size());
+    P->bt0 = P->arena->get<double2>(c->stream, "bt0", P->plan.col_bt0.size());
+  }
   P->state.resize(n);
   return P;
 }
@@ -620,6 +648,13 @@ void problem_set_guess(bp_problem* P, double* const* uvel, double* const* vvel) 
   for (int b = 0; b < P->plan.ninst; ++b) gather_velocity(P->plan, b, uvel[b], vvel[b], x.data());
   CK(cudaMemcpyAsync(P->x0, x.data(), sizeof(double2) * P->plan.npad, cudaMemcpyHostToDevice, P->c->stream));
   P->h2d_bytes += sizeof(double2) * (double)P->plan.nnodes;
+  std::vector<double2> x3;
+  if (P->plan.diva && P->plan.ncols > 0) {  // the first iteration's sliding law reads its bed level
+    x3.assign((size_t)P->plan.ncols * P->plan.nz_out, double2{0.0, 0.0});
+    for (int b = 0; b < P->plan.ninst; ++b) gather_velocity_3d(P->plan, b, uvel[b], vvel[b], x3.data());
+    CK(cudaMemcpyAsync(P->x3_0, x3.data(), sizeof(double2) * x3.size(), cudaMemcpyHostToDevice, P->c->stream));
+    P->h2d_bytes += sizeof(double2) * (double)x3.size();
+  }
   CK(cudaStreamSynchronize(P->c->stream));
 }
 
@@ -634,6 +669,15 @@ void problem_run(bp_problem* P) {
   }
   CK(cudaEventRecord(c->t1, c->stream));
   CK(cudaMemcpyAsync(P->v.x, P->x0, sizeof(double2) * P->plan.npad, cudaMemcpyDeviceToDevice, c->stream));
+  if (P->v.diva && P->plan.ncols > 0) {
+    CK(cudaMemcpyAsync(P->v.x3, P->x3_0, sizeof(double2) * (size_t)P->plan.ncols * P->plan.nz_out,
+                       cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(P->v.col_bt, P->bt0, sizeof(double2) * P->plan.col_bt0.size(), cudaMemcpyDeviceToDevice,
+                       c->stream));
+    if (!P->plan.eq3_0.empty())
+      CK(cudaMemcpyAsync(P->v.eq3, P->eq3_0, sizeof(double) * P->plan.eq3_0.size(), cudaMemcpyDeviceToDevice,
+                         c->stream));
+  }
   init_state(c->stream, P->v, P->plan, true, false);
   run_picard(P);
   if (P->v.l1l2) launch_l1l2_velocity(P->v, c->stream);  // compute_3d_velocity_L1L2 (:3773-3801)
@@ -651,12 +695,20 @@ void problem_run(bp_problem* P) {
 
 void problem_get(bp_problem* P, double* const* uvel, double* const* vvel, double* const* efvs) {
   const HostPlan& p = P->plan;
-  // L1L2: the reconstructed 3-D velocity, else the solution vector
-  const size_t nx = p.l1l2 ? (size_t)p.ncols * p.nz_out : (size_t)p.npad;
+  // L1L2 and DIVA: the 3-D velocity, else the solution vector
+  const bool v3 = p.l1l2 || p.diva;
+  const size_t nx = v3 ? (size_t)p.ncols * p.nz_out : (size_t)p.npad;
   std::vector<double2> x(std::max<size_t>(nx, 1));
   if (nx > 0)
-    CK(cudaMemcpyAsync(x.data(), p.l1l2 ? P->v.x3 : P->v.x, sizeof(double2) * nx, cudaMemcpyDeviceToHost,
+    CK(cudaMemcpyAsync(x.data(), v3 ? P->v.x3 : P->v.x, sizeof(double2) * nx, cudaMemcpyDeviceToHost,
                        P->c->stream));
+  std::vector<double2> x2, bt;  // DIVA: the mean velocity and the traction
+  if (p.diva && p.ncols > 0) {
+    x2.resize(p.ncols);
+    bt.resize(p.ncols);
+    CK(cudaMemcpyAsync(x2.data(), P->v.x, sizeof(double2) * p.ncols, cudaMemcpyDeviceToHost, P->c->stream));
+    CK(cudaMemcpyAsync(bt.data(), P->v.col_bt, sizeof(double2) * p.ncols, cudaMemcpyDeviceToHost, P->c->stream));
+  }
   std::vector<double> ef;
   if (efvs) {
     ef.resize(std::max(p.nefvs, 1));
@@ -664,13 +716,14 @@ void problem_get(bp_problem* P, double* const* uvel, double* const* vvel, double
       CK(cudaMemcpyAsync(ef.data(), P->v.efvs, sizeof(double) * p.nefvs, cudaMemcpyDeviceToHost, P->c->stream));
   }
   CK(cudaStreamSynchronize(P->c->stream));
-  P->d2h_bytes = sizeof(double2) * (double)(p.l1l2 ? nx : (size_t)p.nnodes) +
-                 (efvs ? sizeof(double) * (double)p.nefvs : 0.0);
+  P->d2h_bytes = sizeof(double2) * (double)(v3 ? nx : (size_t)p.nnodes) +
+                 (efvs ? sizeof(double) * (double)p.nefvs : 0.0) + sizeof(double2) * 2.0 * (double)x2.size();
   for (int b = 0; b < p.ninst; ++b) {
     if (uvel && vvel) {
-      if (p.l1l2) scatter_velocity_3d(p, b, x.data(), uvel[b], vvel[b]);
+      if (v3) scatter_velocity_3d(p, b, x.data(), uvel[b], vvel[b]);
       else scatter_velocity(p, b, x.data(), uvel[b], vvel[b]);
     }
+    if (p.diva) scatter_diva(p, b, x2.empty() ? nullptr : x2.data(), bt.empty() ? nullptr : bt.data());
     if (efvs && efvs[b]) scatter_efvs(p, b, ef.data(), efvs[b]);
   }
 }
@@ -807,6 +860,10 @@ int bp_problem_diagnostics(bp_problem* P, int which_bfric, double* const* tau_xz
   bool want_tau = false;
   for (auto o : outs) want_tau = want_tau || o;
   if (!p.ncells) return BP_ERR_ARGS;  // matrix-level problems have no elements
+  if (p.diva) {  // the basal velocity is not the solution vector there
+    c->err = "bp_problem_diagnostics: not for DIVA solves";
+    return BP_ERR_ARGS;
+  }
   if (p.solve2d && want_tau) {  // the stress routine's 2-D branches are not restated
     c->err = "bp_problem_diagnostics: element stresses of 3-D Blatter-Pattyn solves only";
     return BP_ERR_ARGS;

@@ -187,7 +187,8 @@ __global__ void __launch_bounds__(kTile) k_slide_beta(DevView v) {
     InstState& S = v.st[inst];
     if (!S.picard_active || ip.slide.law == 0) continue;
     const size_t nc = (size_t)v.ncols;
-    const double2 ub = v.x[(size_t)col * v.nz + v.nz - 1];
+    // the basal velocity: DIVA's 3-D one (:2240-2243), else the bed node
+    const double2 ub = v.diva ? v.x3[(size_t)col * (v.nl + 1) + v.nl] : v.x[(size_t)col * v.nz + v.nz - 1];
     const double beta = slide_beta(ip.slide, v.col_slide[col], v.col_slide[nc + col],
                                    v.col_slide[2 * nc + col], ub.x, ub.y);
     if (!(beta >= 0.0) && (S.status == BP_OK || S.status == BP_WARN_PCG_NOT_CONVERGED))
@@ -276,7 +277,7 @@ __global__ void __launch_bounds__(256) k_asm2_qp(DevView v) {
   double* dst = v.qp + ((size_t)c * 8 + p) * 10;
   for (int i = 0; i < 5; ++i) dst[i] = out[i];
   const int lane0 = (threadIdx.x & 31) & ~3;
-  if (v.l1l2) {  // efvs(k) = the mean of the layer's point values (:5565-5572)
+  if (v.l1l2 || v.diva) {  // efvs(k) = the mean of the layer's point values (:5565-5572)
     for (int k = 0; k < v.nl; ++k) {
       const double e = ok ? ek[k] : 0.0;
       double sum = 0.0;
@@ -304,6 +305,35 @@ __global__ void __launch_bounds__(256) k_l1l2_cells(DevView v) {
 __global__ void __launch_bounds__(256) k_l1l2_columns(DevView v) {
   const int col = blockIdx.x * blockDim.x + threadIdx.x;
   if (col < v.ncols) l1l2_column(v, col);
+}
+
+// DIVA, every Picard iteration of an active instance: after assembly pass
+// 1 the cells' omega integrals (k_diva_cells), beta_eff at the columns
+// (k_diva_beta) and at the bed-face corners for the standard basal
+// assembly (k_diva_cell_beta); after the linear solve the traction and
+// the 3-D velocity (k_diva_velocity).
+__global__ void __launch_bounds__(256) k_diva_cells(DevView v) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < v.ncells && v.st[v.cell_inst[c]].picard_active) diva_cell_integrals(v, c);
+}
+
+__global__ void __launch_bounds__(256) k_diva_beta(DevView v) {
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col < v.ncols && v.st[v.col_inst[col]].picard_active) diva_column_beta(v, col);
+}
+
+__global__ void __launch_bounds__(256) k_diva_cell_beta(DevView v) {
+  const int cell = blockIdx.x * blockDim.x + threadIdx.x;
+  if (cell >= v.ncells || !v.st[v.cell_inst[cell]].picard_active) return;
+  for (int q = 0; q < 4; ++q) {
+    const int col = v.cell_cols[(size_t)q * v.ncells + cell];
+    v.cell_beta[(size_t)q * v.ncells + cell] = col >= 0 ? v.col_beff[col] : 0.0;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_diva_velocity(DevView v) {
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col < v.ncols && v.st[v.col_inst[col]].picard_active) diva_column_velocity(v, col);
 }
 
 // ---------------------------------------------------------------------
@@ -394,7 +424,7 @@ __global__ void __launch_bounds__(kTile) k_rhs(DevView v) {
         S.status = BP_ZERO_MATRIX;
         S.zero_x = 1;
         fail(v, S, BP_ZERO_MATRIX);
-      } else if (v.solve2d && v.inst[inst].which_babc == 6) {
+      } else if (v.solve2d && !v.diva && v.inst[inst].which_babc == 6) {
         // 2-D solve on a no-slip bed: the 2-D velocity is zero and nothing is solved
         // (glissade_velo_higher.F90:3227-3240)
         S.frozen = 1;
@@ -1006,6 +1036,14 @@ void launch_asm_rows(const DevView& v, cudaStream_t s) {
   else k_asm_rows<false><<<g, kTile, 0, s>>>(v);
 }
 void launch_rhs(const DevView& v, cudaStream_t s) { k_rhs<<<tile_grid(v), kTile, 0, s>>>(v); }
+void launch_diva_beta(const DevView& v, cudaStream_t s) {
+  if (v.ncells > 0) k_diva_cells<<<(unsigned)((v.ncells + 255) / 256), 256, 0, s>>>(v);
+  if (v.ncols > 0) k_diva_beta<<<(unsigned)((v.ncols + 255) / 256), 256, 0, s>>>(v);
+  if (v.ncells > 0) k_diva_cell_beta<<<(unsigned)((v.ncells + 255) / 256), 256, 0, s>>>(v);
+}
+void launch_diva_velocity(const DevView& v, cudaStream_t s) {
+  if (v.ncols > 0) k_diva_velocity<<<(unsigned)((v.ncols + 255) / 256), 256, 0, s>>>(v);
+}
 void launch_l1l2_velocity(const DevView& v, cudaStream_t s) {
   if (v.ncells > 0) k_l1l2_cells<<<(unsigned)((v.ncells + 255) / 256), 256, 0, s>>>(v);
   if (v.ncols > 0) k_l1l2_columns<<<(unsigned)((v.ncols + 255) / 256), 256, 0, s>>>(v);

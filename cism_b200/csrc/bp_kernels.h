@@ -23,6 +23,10 @@ void launch_rhs(const DevView& v, cudaStream_t s);
 // L1L2: the 3-D velocity v.x3 from the basal velocity v.x and the layer
 // viscosities v.efvs of the last assembly
 void launch_l1l2_velocity(const DevView& v, cudaStream_t s);
+// DIVA: omega and beta_eff after assembly pass 1; the traction and 3-D
+// velocity v.x3 after the linear solve
+void launch_diva_beta(const DevView& v, cudaStream_t s);
+void launch_diva_velocity(const DevView& v, cudaStream_t s);
 // Residual modes (MV_INIT, MV_CHECK, MV_REFINE) run with (minb, grid_cap),
 // the Krylov matvecs (MV_STD_A, MV_CG_FIRST, MV_CG1) with (minb_k, grid_k).
 void launch_mv(int mode, const DevView& v, cudaStream_t s);

@@ -230,13 +230,17 @@ bool build_plan(const bp_inputs* in, int n, HostPlan* p, std::string* err) {
   // the 2-D solves (shallow-shelf, L1L2) have one unknown pair per column
   // (solve_2d, glissade_velo_higher.F90:1125-1128)
   const int approx = in[0].approx_2d;
-  if (approx != 0 && approx != 1 && approx != 3) { *err = "approx_2d must be 0, 1 (SSA) or 3 (L1L2)"; return false; }
-  const bool solve2d = approx != 0, l1l2 = approx == 3;
+  if (approx != 0 && approx != 1 && approx != 3 && approx != 4) {
+    *err = "approx_2d must be 0, 1 (SSA), 3 (L1L2) or 4 (DIVA)";
+    return false;
+  }
+  const bool solve2d = approx != 0, l1l2 = approx == 3, diva = approx == 4;
   const int nz = solve2d ? 1 : nz_in, nl = nz_in - 1;
   p->nz = nz;
   p->nz_out = nz_in;
   p->solve2d = solve2d;
   p->l1l2 = l1l2;
+  p->diva = diva;
   p->ninst = n;
   p->inst.resize(n);
   std::vector<std::vector<std::pair<int, int>>> cols(n);
@@ -255,6 +259,12 @@ bool build_plan(const bp_inputs* in, int n, HostPlan* p, std::string* err) {
       *err = "the L1L2 solve needs l1l2 with thck, flwa, dusrf_dx and dusrf_dy";
       return false;
     }
+    if (diva && (!I.diva || !I.diva->uvel_2d || !I.diva->vvel_2d || !I.diva->btractx || !I.diva->btracty ||
+                 !I.diva->thck || !I.diva->ice_plus_land_mask)) {
+      *err = "the DIVA solve needs diva with uvel_2d, vvel_2d, btractx, btracty, thck and ice_plus_land_mask";
+      return false;
+    }
+    if (diva) p->diva_io.push_back(*I.diva);
     if (I.nhalo != 2) { *err = "nhalo must be 2"; return false; }
     if (I.nx < 6 || I.ny < 6) { *err = "grid too small"; return false; }
     if (I.pcg_variant != in[0].pcg_variant || I.pcg_ncheck != in[0].pcg_ncheck ||
@@ -317,14 +327,22 @@ bool build_plan(const bp_inputs* in, int n, HostPlan* p, std::string* err) {
   }
   const int NCELL = p->ncells;
   p->nelem = solve2d ? NCELL : NCELL * (nz - 1);  // 2-D: one element per cell
-  p->nefvs = l1l2 ? NCELL * nl : p->nelem;
+  p->nefvs = (l1l2 || diva) ? NCELL * nl : p->nelem;
   p->cell_inst.resize(NCELL);
   p->cell_ij.resize(2 * (size_t)NCELL);
   p->cell_cols.resize(4 * (size_t)NCELL);
   p->cell_s.resize(4 * (size_t)NCELL);
   p->cell_h.resize(4 * (size_t)NCELL);
   p->cell_beta.resize(4 * (size_t)NCELL);
-  p->flwafact.resize((size_t)(solve2d && !l1l2 ? NCELL : NCELL * nl));
+  const bool ssa = solve2d && !l1l2 && !diva;
+  p->flwafact.resize((size_t)(ssa ? NCELL : NCELL * nl));
+  if (diva) {
+    p->cell_thck.resize(NCELL);
+    p->eq3_0.resize((size_t)NCELL * 4 * nl);
+    p->x2d_0.resize(NC);
+    p->col_bt0.resize(NC);
+    p->col_ipl.resize(NC);
+  }
   if (l1l2) {
     p->cell_flwa.resize((size_t)NCELL * nl);
     p->cell_thck.resize(NCELL);
@@ -389,6 +407,17 @@ bool build_plan(const bp_inputs* in, int n, HostPlan* p, std::string* err) {
       } else {
         p->col_beta[g] = I.beta_internal[vtx(i, j, nx)];
       }
+      if (diva) {
+        const size_t w = vtx(i, j, nx);
+        p->x2d_0[g] = double2{I.diva->uvel_2d[w], I.diva->vvel_2d[w]};
+        p->col_bt0[g] = double2{I.diva->btractx[w], I.diva->btracty[w]};
+        uint8_t bits = 0;
+        for (int q = 0; q < 4; ++q)
+          if (ci[q] >= 1 && ci[q] <= nx && cj[q] >= 1 && cj[q] <= ny &&
+              I.diva->ice_plus_land_mask[cel(ci[q], cj[q], nx)] == 1)
+            bits |= (uint8_t)(1u << q);
+        p->col_ipl[g] = bits;
+      }
       if (l1l2) {
         p->col_ds[g] = I.l1l2->dusrf_dx[vtx(i, j, nx)];
         p->col_ds[(size_t)NC + g] = I.l1l2->dusrf_dy[vtx(i, j, nx)];
@@ -436,7 +465,13 @@ bool build_plan(const bp_inputs* in, int n, HostPlan* p, std::string* err) {
         p->cell_thck[g] = I.l1l2->thck[cel(ic, jc, nx)];
         for (int k = 0; k < nl; ++k) p->cell_flwa[(size_t)g * nl + k] = I.l1l2->flwa[cel(ic, jc, nx) * nl + k];
       }
-      if (solve2d && !l1l2) {  // glissade_vertical_average (glissade_grid_operators.F90:1172-1236)
+      if (diva) {  // efvs_qp_3d starts from the last solve's efvs on every point (:1166-1170)
+        p->cell_thck[g] = I.diva->thck[cel(ic, jc, nx)];
+        for (int q = 0; q < 4; ++q)
+          for (int k = 0; k < nl; ++k)
+            p->eq3_0[((size_t)g * 4 + q) * nl + k] = I.diva->efvs ? I.diva->efvs[cel(ic, jc, nx) * nl + k] : 0.0;
+      }
+      if (ssa) {  // glissade_vertical_average (glissade_grid_operators.F90:1172-1236)
         double f = 0.0;
         for (int k = 0; k < nz_in - 1; ++k)
           f = f + I.flwafact[cel(ic, jc, nx) * (nz_in - 1) + k] * (I.sigma[k + 1] - I.sigma[k]);
@@ -460,6 +495,10 @@ void gather_velocity(const HostPlan& p, int b, const double* uvel,
   const int nx = p.nx[b], nz = p.nz, NC = p.ncols;
   for (int g = ip.col_begin; g < ip.col_end; ++g) {
     const int i = p.col_ij[g], j = p.col_ij[NC + g];
+    if (p.diva) {  // the carried-over mean velocity (:1173-1180)
+      x[g] = p.x2d_0[g];
+      continue;
+    }
     if (p.solve2d) {  // uvel_2d = uvel(nz,:,:) (glissade_velo_higher.F90:1179-1180)
       const size_t src = vtx(i, j, nx) * p.nz_out + (p.nz_out - 1);
       x[g] = double2{uvel[src], vvel[src]};
@@ -524,6 +563,35 @@ void scatter_velocity_3d(const HostPlan& p, int b, const double2* x3,
   halo_stag(nx, ny, L, p.periodic[b], vvel);
 }
 
+void gather_velocity_3d(const HostPlan& p, int b, const double* uvel,
+                        const double* vvel, double2* x3) {
+  const InstParams& ip = p.inst[b];
+  const int nx = p.nx[b], NC = p.ncols, L = p.nz_out;
+  for (int g = ip.col_begin; g < ip.col_end; ++g) {
+    const size_t w = vtx(p.col_ij[g], p.col_ij[NC + g], nx);
+    for (int k = 0; k < L; ++k) x3[(size_t)g * L + k] = double2{uvel[w * L + k], vvel[w * L + k]};
+  }
+}
+
+void scatter_diva(const HostPlan& p, int b, const double2* x, const double2* bt) {
+  const InstParams& ip = p.inst[b];
+  const bp_diva& D = p.diva_io[b];
+  const int nx = p.nx[b], ny = p.ny[b], NC = p.ncols;
+  const size_t nvert = (size_t)(nx - 1) * (ny - 1);
+  for (size_t w = 0; w < nvert; ++w) D.uvel_2d[w] = D.vvel_2d[w] = D.btractx[w] = D.btracty[w] = 0.0;
+  for (int g = ip.col_begin; g < ip.col_end; ++g) {
+    const size_t w = vtx(p.col_ij[g], p.col_ij[NC + g], nx);
+    D.uvel_2d[w] = x[g].x;
+    D.vvel_2d[w] = x[g].y;
+    D.btractx[w] = bt[g].x;
+    D.btracty[w] = bt[g].y;
+  }
+  halo_stag(nx, ny, 1, p.periodic[b], D.uvel_2d);
+  halo_stag(nx, ny, 1, p.periodic[b], D.vvel_2d);
+  halo_stag(nx, ny, 1, p.periodic[b], D.btractx);
+  halo_stag(nx, ny, 1, p.periodic[b], D.btracty);
+}
+
 void scatter_efvs(const HostPlan& p, int b, const double* efvs_elem,
                   double* efvs) {
   const InstParams& ip = p.inst[b];
@@ -533,7 +601,7 @@ void scatter_efvs(const HostPlan& p, int b, const double* efvs_elem,
     const int ic = p.cell_ij[g], jc = p.cell_ij[NCELL + g];
     for (int k = 0; k < nz - 1; ++k)  // shallow-shelf: the cell's value on every layer
       efvs[cel(ic, jc, nx) * (nz - 1) + k] =
-          efvs_elem[p.solve2d && !p.l1l2 ? (size_t)g : (size_t)g * (nz - 1) + k];
+          efvs_elem[p.solve2d && !p.l1l2 && !p.diva ? (size_t)g : (size_t)g * (nz - 1) + k];
   }
 }
 

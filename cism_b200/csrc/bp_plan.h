@@ -27,6 +27,7 @@ struct HostPlan {
   int nz_out = 0;          // levels of the velocity arrays (the model's nz)
   bool solve2d = false;    // 2-D solve: shallow-shelf or L1L2
   bool l1l2 = false;       // L1L2 (the 3-D velocity reconstructed after the loop)
+  bool diva = false;       // DIVA (3-D velocity, traction and point viscosities every iteration)
   int nefvs = 0;           // length of the element viscosity array (L1L2: ncells * (nz_out - 1))
   int ncols = 0, nnodes = 0, npad = 0, ncells = 0, nelem = 0, ntiles = 0;
   std::vector<InstParams> inst;
@@ -38,7 +39,14 @@ struct HostPlan {
   std::vector<uint8_t> dmask;
   std::vector<int> cell_inst, cell_ij, cell_cols;
   std::vector<double> cell_s, cell_h, cell_beta, flwafact;
-  std::vector<double> cell_flwa, cell_thck, cell_ds, col_ds, col_h;  // L1L2 only
+  std::vector<double> cell_flwa, cell_thck, cell_ds, col_ds, col_h;  // L1L2 only (cell_thck: DIVA too)
+  // DIVA only: starting point viscosities [ncells][4][nl], mean velocity
+  // and traction [ncols], the columns' ice-plus-land bits, and each
+  // instance's state arrays (written back with the result)
+  std::vector<double> eq3_0;
+  std::vector<double2> x2d_0, col_bt0;
+  std::vector<uint8_t> col_ipl;
+  std::vector<bp_diva> diva_io;
   std::vector<int> tile_start, tile_end, tile_inst;
   // per-instance grid sizes, for scatters
   std::vector<int> nx, ny, periodic;
@@ -66,6 +74,13 @@ void gather_velocity(const HostPlan& p, int b, const double* uvel,
                      const double* vvel, double2* x);
 void scatter_velocity(const HostPlan& p, int b, const double2* x,
                       double* uvel, double* vvel);
+// DIVA: the 3-D velocity [ncols][nz_out] of instance b from the bed level
+// of (uvel, vvel) (the first iteration's sliding law reads it)
+void gather_velocity_3d(const HostPlan& p, int b, const double* uvel,
+                        const double* vvel, double2* x3);
+// DIVA: the mean velocity x and traction bt [ncols] of instance b into its
+// bp_diva arrays (zero away from the columns, then the halo update)
+void scatter_diva(const HostPlan& p, int b, const double2* x, const double2* bt);
 // L1L2: the reconstructed velocity [ncols][nz_out] of instance b -> uvel,
 // vvel (nz,nx-1,ny-1), zero on levels 1..nz-1 away from the columns, then
 // the halo update (glissade_velo_higher.F90:3773-3801)

@@ -71,9 +71,13 @@ extern "C" int bp_setup(const bp_model* m, bp_setup_arrays* o, double* uvel,
   if (m->sliding && (m->sliding->law != m->which_babc || !o->f_ground ||
                      (m->sliding->law == 10 && !o->flwa_basal_stag)))
     return BP_ERR_ARGS;
-  // 3-D Blatter-Pattyn, or the shallow-shelf or L1L2 2-D solve
-  if (m->approx_2d != 0 && m->approx_2d != 1 && m->approx_2d != 3) return BP_ERR_ARGS;
+  // 3-D Blatter-Pattyn, or the shallow-shelf, L1L2 or DIVA 2-D solve
+  if (m->approx_2d != 0 && m->approx_2d != 1 && m->approx_2d != 3 && m->approx_2d != 4) return BP_ERR_ARGS;
   if (m->approx_2d == 3 && (!o->dusrf_dx || !o->dusrf_dy)) return BP_ERR_ARGS;
+  const bool diva = m->approx_2d == 4;
+  if (diva && (!m->diva || !m->diva->uvel_2d || !m->diva->vvel_2d || !m->diva->btractx ||
+               !m->diva->btracty || !o->ice_plus_land_mask))
+    return BP_ERR_ARGS;
   const Cells C{nx, ny};
   const Verts V{nx, ny};
   const size_t ncell = (size_t)nx * ny, nvert = (size_t)(nx - 1) * (ny - 1), n3 = nvert * nz;
@@ -92,13 +96,18 @@ extern "C" int bp_setup(const bp_model* m, bp_setup_arrays* o, double* uvel,
   std::memset(o->umask_dirichlet, 0, n3 * sizeof(int));
   std::memset(o->vmask_dirichlet, 0, n3 * sizeof(int));
   for (size_t v = 0; v < nvert; ++v) {
-    const bool noslip = m->which_babc == 6;
+    // DIVA takes a no-slip bed through beta_eff = 1/omega (:1274-1278)
+    const bool noslip = m->which_babc == 6 && !diva;
     const bool kin = m->kinbcmask && m->kinbcmask[v] == 1;
     for (int k = 0; k < nz; ++k)
       if (kin || (noslip && k == nz - 1)) {
         o->umask_dirichlet[v * nz + k] = 1;
         o->vmask_dirichlet[v * nz + k] = 1;
       }
+    if (kin && diva) {  // a 2-D solve's Dirichlet column starts from its bed velocity (:1300-1303)
+      m->diva->uvel_2d[v] = uvel[v * nz + nz - 1];
+      m->diva->vvel_2d[v] = vvel[v * nz + nz - 1];
+    }
   }
 
   // masks, glissade_masks.F90:55-457 (no sub-grid calving front)
@@ -114,6 +123,8 @@ extern "C" int bp_setup(const bp_model* m, bp_setup_arrays* o, double* uvel,
   const std::vector<int>& active_ice = ice;
   std::vector<int> ipl(ncell);
   for (size_t c = 0; c < ncell; ++c) ipl[c] = active_ice[c] || land[c];
+  if (diva)
+    for (size_t c = 0; c < ncell; ++c) o->ice_plus_land_mask[c] = ipl[c];
 
   // glissade_stagger with stagger_margin = 1, glissade_grid_operators.F90:60-148
   auto stagger = [&](const double* var, double* out) {
@@ -195,8 +206,10 @@ extern "C" int bp_setup(const bp_model* m, bp_setup_arrays* o, double* uvel,
   const bp::OwnedRange R = bp::owned_range(nx, ny, m->periodic);
   for (int j = R.jlo; j <= R.jhi; ++j)
     for (int i = R.ilo; i <= R.ihi; ++i)
-      if (!o->active_vertex[V(i, j)])
+      if (!o->active_vertex[V(i, j)]) {
         for (int k = 0; k < nz; ++k) uvel[V(i, j) * nz + k] = vvel[V(i, j) * nz + k] = 0.0;
+        if (diva) m->diva->uvel_2d[V(i, j)] = m->diva->vvel_2d[V(i, j)] = 0.0;
+      }
 
   // flwafact = 0.5 A^(-1/n), :1919-1939
   std::memset(o->flwafact, 0, (size_t)(nz - 1) * ncell * sizeof(double));
@@ -430,6 +443,12 @@ extern "C" int bp_setup(const bp_model* m, bp_setup_arrays* o, double* uvel,
       o->l1l2.grav = m->grav;
       in->l1l2 = &o->l1l2;
     }
+    if (diva) {
+      o->diva = *m->diva;
+      o->diva.thck = m->thck;
+      o->diva.ice_plus_land_mask = o->ice_plus_land_mask;
+      in->diva = &o->diva;
+    }
   }
   return BP_OK;
 }
@@ -444,6 +463,7 @@ extern "C" int bp_velo_higher_solve(bp_ctx* ctx, const bp_model* m, double* uvel
   std::vector<int> ac(ncell), av(nvert), um(n3), vm(n3);
   std::vector<double> fg(m->sliding ? nvert : 0), fbs(m->sliding ? nvert : 0);
   std::vector<double> gx(m->approx_2d == 3 ? nvert : 0), gy(m->approx_2d == 3 ? nvert : 0);
+  std::vector<int> iplm(m->approx_2d == 4 ? ncell : 0);
   bp_setup_arrays o{};
   o.sigma = sigma.data(); o.stagusrf = su.data(); o.stagthck = sh.data();
   o.beta_internal = beta.data(); o.flwafact = fl.data(); o.active_cell = ac.data();
@@ -457,6 +477,7 @@ extern "C" int bp_velo_higher_solve(bp_ctx* ctx, const bp_model* m, double* uvel
     o.dusrf_dx = gx.data();
     o.dusrf_dy = gy.data();
   }
+  if (m->approx_2d == 4) o.ice_plus_land_mask = iplm.data();
   bp_inputs in;
   const int rc = bp_setup(m, &o, uvel, vvel, &in);
   if (rc != BP_OK) return rc;

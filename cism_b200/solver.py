@@ -64,6 +64,12 @@ class L1L2(C.Structure):
                 ("rhoi", C.c_double), ("grav", C.c_double)]
 
 
+class Diva(C.Structure):
+    """bp_diva: the state a DIVA solve carries from one solve to the next."""
+    _fields_ = [("uvel_2d", _dp), ("vvel_2d", _dp), ("btractx", _dp), ("btracty", _dp), ("efvs", _dp),
+                ("thck", _dp), ("ice_plus_land_mask", _ip)]
+
+
 class Inputs(C.Structure):
     _fields_ = [
         ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("nhalo", C.c_int),
@@ -76,7 +82,7 @@ class Inputs(C.Structure):
         ("which_precond", C.c_int), ("maxiter_nonlinear", C.c_int), ("pcg_maxiters", C.c_int),
         ("pcg_ncheck", C.c_int), ("pcg_tol", C.c_double), ("precision", C.c_int),
         ("inner_tol", C.c_double), ("sliding", C.POINTER(Sliding)), ("approx_2d", C.c_int),
-        ("l1l2", C.POINTER(L1L2)),
+        ("l1l2", C.POINTER(L1L2)), ("diva", C.POINTER(Diva)),
     ]
 
 
@@ -110,7 +116,7 @@ class Model(C.Structure):
         ("which_assemble_taud", C.c_int), ("which_ground", C.c_int),
         ("maxiter_nonlinear", C.c_int), ("pcg_maxiters", C.c_int), ("pcg_ncheck", C.c_int),
         ("pcg_tol", C.c_double), ("precision", C.c_int), ("inner_tol", C.c_double),
-        ("sliding", C.POINTER(Sliding)), ("approx_2d", C.c_int),
+        ("sliding", C.POINTER(Sliding)), ("approx_2d", C.c_int), ("diva", C.POINTER(Diva)),
     ]
 
 
@@ -119,7 +125,8 @@ class SetupArrays(C.Structure):
                 ("flwafact", _dp), ("active_cell", _ip), ("active_vertex", _ip),
                 ("loadu", _dp), ("loadv", _dp), ("umask_dirichlet", _ip), ("vmask_dirichlet", _ip),
                 ("f_ground", _dp), ("flwa_basal_stag", _dp), ("sliding", Sliding),
-                ("dusrf_dx", _dp), ("dusrf_dy", _dp), ("l1l2", L1L2)]
+                ("dusrf_dx", _dp), ("dusrf_dy", _dp), ("l1l2", L1L2),
+                ("ice_plus_land_mask", _ip), ("diva", Diva)]
 
 
 SETUP_ARRAYS = [k for k, _ in SetupArrays._fields_[:11]]
@@ -267,6 +274,20 @@ def prepare(m: configs.BPModel, uvel=None, vvel=None, precision: int = FP64,
         arrays["dusrf_dy"] = np.zeros((ny - 1, nx - 1))
         sa.dusrf_dx, sa.dusrf_dy = _p(arrays["dusrf_dx"]), _p(arrays["dusrf_dy"])
     ms, keep = make_model_struct(m, precision, inner_tol)
+    if m.approx_2d == configs.APPROX_DIVA:
+        # the carried-over state (copies: the setup and the solve write them)
+        st0 = m.diva_state or {}
+        vs = (ny - 1, nx - 1)
+        for name, shape in (("uvel_2d", vs), ("vvel_2d", vs), ("btractx", vs), ("btracty", vs),
+                            ("efvs_in", (ny, nx, nz - 1))):
+            a = st0.get(name[:-3] if name == "efvs_in" else name)
+            arrays[name] = np.zeros(shape) if a is None else np.array(a, np.float64, copy=True)
+        arrays["ice_plus_land_mask"] = np.zeros((ny, nx), np.int32)
+        sa.ice_plus_land_mask = _p(arrays["ice_plus_land_mask"])
+        dv = Diva(_p(arrays["uvel_2d"]), _p(arrays["vvel_2d"]), _p(arrays["btractx"]), _p(arrays["btracty"]),
+                  _p(arrays["efvs_in"]), C.cast(None, _dp), C.cast(None, _ip))
+        keep.append(dv)
+        ms.diva = C.pointer(dv)
     u = np.zeros(m.vshape3) if uvel is None else np.array(uvel, np.float64, copy=True)
     v = np.zeros(m.vshape3) if vvel is None else np.array(vvel, np.float64, copy=True)
     inp = Inputs()
@@ -319,7 +340,10 @@ class Context:
         rc = lib().bp_solve(self.h, C.byref(prep.inputs), _p(u), _p(v),
                             _p(efvs) if efvs is not None else C.cast(None, _dp), C.byref(st))
         self._check(rc)
-        return u, v, efvs, st.as_dict()
+        out = st.as_dict()
+        if m.approx_2d == configs.APPROX_DIVA:  # the state written back for the next solve
+            out["diva"] = {k: prep.arrays[k].copy() for k in ("uvel_2d", "vvel_2d", "btractx", "btracty")}
+        return u, v, efvs, out
 
     def velo_higher_solve(self, m: configs.BPModel, uvel=None, vvel=None, precision: int = FP64,
                           inner_tol: float = 1e-4):

@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define BP_ABI_VERSION 4
+#define BP_ABI_VERSION 5
 
 typedef struct bp_ctx bp_ctx;
 
@@ -104,6 +104,32 @@ typedef struct {
   double rhoi, grav;                  /* kg m^-3, m s^-2 */
 } bp_l1l2;
 
+/* State of the DIVA solve (whichapprox = HO_APPROX_DIVA, after Goldberg
+ * 2011; glissade_velo_higher.F90:2742-2857, 3658-3696, 5601-5830,
+ * 7622-7864).  The 2-D system is solved for the depth-mean velocity with
+ * the basal term beta_eff = beta / (1 + beta omega) (1 / omega on a
+ * no-slip bed); the layer viscosities come from the last iteration's
+ * vertical shear, tau_b sigma / efvs_old; after every linear solve the
+ * basal traction tau_b = beta_eff u_mean and the 3-D velocity u(k) =
+ * u_mean - tau_b omega + tau_b omega_k(k) are formed, and the next
+ * iteration's sliding law reads that 3-D basal velocity.  The mean
+ * velocity, the traction and the viscosities carry over from one solve to
+ * the next, so the arrays below are read on entry and (uvel_2d, vvel_2d,
+ * btractx, btracty) written back with the result.  The setup leaves a
+ * Dirichlet column's mean velocity at its basal velocity (:1300-1303) and
+ * zeroes it at owned inactive vertices (:1700-1711); a no-slip bed sets no
+ * basal Dirichlet mask here (:1274-1278). */
+typedef struct {
+  double *uvel_2d, *vvel_2d;         /* (nx-1,ny-1) m/a, mean velocity: in the last solve's, out this one's */
+  double *btractx, *btracty;         /* (nx-1,ny-1) Pa, basal traction: in/out */
+  const double *efvs;                /* (nz-1,nx,ny) Pa a, the last solve's layer viscosities (0 = none),
+                                        halo-updated as the reference's caller leaves them (a periodic
+                                        halo cell's omega is computed from its own values; the
+                                        reference copies its image's, equal for such inputs) */
+  const double *thck;                /* (nx,ny) m */
+  const int *ice_plus_land_mask;     /* (nx,ny), the staggering mask of omega (:1486-1496) */
+} bp_diva;
+
 /* Boundary inputs of one solve: what the setup part of
  * glissade_velo_higher_solve (:987-2199) has computed when the Picard loop
  * starts (:2206).  beta_internal is the calcbeta result for the
@@ -145,10 +171,14 @@ typedef struct {
                                    pair per column: 1 shallow-shelf (HO_APPROX_SSA),
                                    the result copied to every level; 3 L1L2
                                    (HO_APPROX_L1L2), the basal velocity and the 3-D
-                                   velocity reconstructed from it (needs l1l2).
-                                   0: the 3-D Blatter-Pattyn solve.  Shared by a
-                                   batch; the 2-D solves take which_precond 0 or 1 */
+                                   velocity reconstructed from it (needs l1l2);
+                                   4 DIVA (HO_APPROX_DIVA), the mean velocity and
+                                   the 3-D velocity (needs diva).  0: the 3-D
+                                   Blatter-Pattyn solve.  Shared by a batch; the
+                                   2-D solves take which_precond 0 or 1 */
   const bp_l1l2 *l1l2;          /* approx_2d = 3 only */
+  const bp_diva *diva;          /* approx_2d = 4 only; its outputs are written by
+                                   bp_solve, bp_batch_solve and bp_problem_get */
 } bp_inputs;
 
 typedef struct {
@@ -319,6 +349,10 @@ typedef struct {
    * and beta_grounded_min from this struct's fields above */
   const bp_sliding *sliding;
   int approx_2d;                /* as in bp_inputs; bp_setup fills the L1L2 fields */
+  /* DIVA: the carried-over state (uvel_2d, vvel_2d, btractx, btracty,
+   * efvs; thck and the mask are filled by bp_setup, which also applies the
+   * Dirichlet and inactive-vertex rules to uvel_2d, vvel_2d) */
+  const bp_diva *diva;
 } bp_model;
 
 /* Caller-allocated outputs of the setup (sizes as in bp_inputs). */
@@ -339,6 +373,10 @@ typedef struct {
    * L1L2 fields handed to the solve */
   double *dusrf_dx, *dusrf_dy;
   bp_l1l2 l1l2;
+  /* DIVA only: outputs the ice-plus-land mask ((nx,ny)) and the DIVA
+   * state handed to the solve */
+  int *ice_plus_land_mask;
+  bp_diva diva;
 } bp_setup_arrays;
 
 /* Masks, staggering, surface gradient, vertex geometry, flow factor, load

@@ -1653,6 +1653,93 @@ static void effective_viscosity_l1l2(int whichefvs, double efvs_constant, int nz
   }
 }
 
+/* compute_effective_viscosity_diva (:7622-7864), the default non-cubic
+ * form: the viscosity of each layer k at one quadrature point from the
+ * horizontal strain rates of the mean velocity and the vertical shear
+ * (du/dz, dv/dz) = tau_b stagsigma(k) / efvs_old(k), tau_b the basal
+ * traction interpolated to the point; efvs (in: the last assembly's
+ * value, 0 = none yet, then the value at the 1e-8 /a strain-rate floor;
+ * out: the new value). */
+static void effective_viscosity_diva(int whichefvs, double efvs_constant, int nz,
+                                     const double *sigma, int p, const double *dx,
+                                     const double *dy, const double *u, const double *v,
+                                     const double *bx, const double *by,
+                                     const double *flwafact, double *efvs) {
+  const double effstrain_min = 1.0e-8;
+  const double p_effstr = (1.0 - 3.0) / 3.0;
+  const double p2_effstr = p_effstr / 2;
+  if (whichefvs == ORC_EFVS_CONSTANT) {
+    for (int k = 0; k < nz - 1; ++k) efvs[k] = efvs_constant;
+    return;
+  }
+  if (whichefvs == ORC_EFVS_FLOWFACT) {
+    const double scyr = 31536000.0;
+    const double effstrain = (500.0 / scyr) / 200.0e3 * scyr;
+    for (int k = 0; k < nz - 1; ++k) efvs[k] = flwafact[k] * pow(effstrain, p_effstr);
+    return;
+  }
+  double ux = 0.0, uy = 0.0, vx = 0.0, vy = 0.0, taux = 0.0, tauy = 0.0;
+  for (int n = 0; n < 4; ++n) {
+    ux = ux + dx[n] * u[n];
+    uy = uy + dy[n] * u[n];
+    vx = vx + dx[n] * v[n];
+    vy = vy + dy[n] * v[n];
+    taux = taux + phi2[n][p] * bx[n];
+    tauy = tauy + phi2[n][p] * by[n];
+  }
+  for (int k = 1; k <= nz - 1; ++k) {
+    if (efvs[k - 1] == 0.0) efvs[k - 1] = flwafact[k - 1] * pow(effstrain_min, p_effstr);
+    const double stagsigma = (sigma[k - 1] + sigma[k]) / 2.0;
+    const double du_dz = taux * stagsigma / efvs[k - 1];
+    const double dv_dz = tauy * stagsigma / efvs[k - 1];
+    const double effstrainsq = effstrain_min * effstrain_min + ux * ux + vy * vy + ux * vy +
+                               0.25 * ((vx + uy) * (vx + uy)) + 0.25 * (du_dz * du_dz + dv_dz * dv_dz);
+    efvs[k - 1] = flwafact[k - 1] * pow(effstrainsq, p2_effstr);
+  }
+}
+
+/* compute_integrals_diva (:5601-5726): per quadrature point the integral
+ * of depth / efvs from the bed up to each level, averaged over the points
+ * (omega_k, Goldberg 2011 eq. 32, over H), and its layer-midpoint integral
+ * over the column (omega, eq. 35 over H).  eq holds the cell's point
+ * viscosities [p][k]. */
+static void integrals_diva(int nz, const double *sigma, double thck, const double *eq,
+                           double *omega_k, double *omega) {
+  double okp[4][65];
+  for (int p = 0; p < 4; ++p) {
+    okp[p][nz - 1] = 0.0;
+    for (int k = nz - 1; k >= 1; --k) {  /* layer k between levels k and k+1 (1-based) */
+      const double depth = 0.5 * (sigma[k - 1] + sigma[k]);
+      const double dz = (sigma[k] - sigma[k - 1]) * thck;
+      okp[p][k - 1] = okp[p][k] + depth / eq[(size_t)p * (nz - 1) + (k - 1)] * dz;
+    }
+  }
+  for (int k = 0; k < nz; ++k) {
+    double s = 0.0;
+    for (int p = 0; p < 4; ++p) s = s + okp[p][k];
+    omega_k[k] = s / 4;
+  }
+  double om = 0.0;
+  for (int k = 1; k <= nz - 1; ++k) {
+    const double layer_avg = 0.5 * (omega_k[k - 1] + omega_k[k]);
+    const double dz = sigma[k] - sigma[k - 1];
+    om = om + layer_avg * dz;
+  }
+  *omega = om;
+}
+
+/* DIVA state of one 2-D assembly: the viscosity of each layer at each
+ * point efvs_qp_3d (in: the last assembly's, out: this one's), the basal
+ * traction at the vertices, the cell thickness, and the integrals the
+ * assembly produces. */
+typedef struct {
+  double *eq3;                   /* (nz-1,4,nx,ny) */
+  const double *btx, *bty;       /* (nx-1,ny-1) */
+  const double *thck;            /* (nx,ny) */
+  double *omega_k;               /* (nz,nx,ny) */
+  double *omega;                 /* (nx,ny) */
+} diva_state;
+
 /* assemble_stiffness_matrix_2d (:5208-5595), SSA and L1L2 branches: per
  * active cell, 2x2 Gauss points; the SSA efvs from the vertically averaged
  * flow factor (glissade_vertical_average, glissade_grid_operators.F90:
@@ -1666,8 +1753,9 @@ static int assemble_2d(int approx, int nx, int ny, int nz, int nhalo, const doub
                        const double *yVertex, const double *u2, const double *v2,
                        const double *stagthck, const double *flwafact, const double *flwa,
                        const double *dusrf_dx, const double *dusrf_dy, double rhoi,
-                       double grav, int whichefvs, double efvs_constant, double *efvs,
-                       double *Auu, double *Auv, double *Avu, double *Avv) {
+                       double grav, const diva_state *dv, int whichefvs,
+                       double efvs_constant, double *efvs, double *Auu, double *Auv,
+                       double *Avu, double *Avv) {
   init_tables();
   const double vol0 = 1.0e9;
   const size_t nvx = (size_t)(nx - 1) * (ny - 1);
@@ -1676,6 +1764,10 @@ static int assemble_2d(int approx, int nx, int ny, int nz, int nhalo, const doub
   memset(Avu, 0, 27 * nvx * sizeof(double));
   memset(Avv, 0, 27 * nvx * sizeof(double));
   memset(efvs, 0, (size_t)(nz - 1) * nx * ny * sizeof(double));
+  if (dv) {  /* allocated and zeroed once per solve in the reference (:1155-1164) */
+    memset(dv->omega_k, 0, (size_t)nz * nx * ny * sizeof(double));
+    memset(dv->omega, 0, (size_t)nx * ny * sizeof(double));
+  }
   double *eq = malloc((size_t)4 * (nz - 1) * sizeof(double));  /* efvs_qp(k,p) */
   for (int j = nhalo + 1; j <= ny - nhalo + 1; ++j)
     for (int i = nhalo + 1; i <= nx - nhalo + 1; ++i) {
@@ -1684,7 +1776,7 @@ static int assemble_2d(int approx, int nx, int ny, int nz, int nhalo, const doub
       for (int k = 1; k <= nz - 1; ++k)
         fl2 = fl2 + flwafact[IFL(k, i, j)] * (sigma[k] - sigma[k - 1]);
       double Kuu[4][4] = {{0}}, Kuv[4][4] = {{0}}, Kvu[4][4] = {{0}}, Kvv[4][4] = {{0}};
-      double x[4], y[4], u[4], v[4], h[4], sx[4], sy[4], efvs_qp[4];
+      double x[4], y[4], u[4], v[4], h[4], sx[4], sy[4], bx[4], by[4], efvs_qp[4];
       for (int n = 0; n < 4; ++n) {
         const int iv = i + ishift[2][n], jv = j + jshift[2][n];
         x[n] = xVertex[IV(iv, jv)];
@@ -1694,6 +1786,8 @@ static int assemble_2d(int approx, int nx, int ny, int nz, int nhalo, const doub
         h[n] = stagthck[IV(iv, jv)];
         sx[n] = dusrf_dx ? dusrf_dx[IV(iv, jv)] : 0.0;
         sy[n] = dusrf_dy ? dusrf_dy[IV(iv, jv)] : 0.0;
+        bx[n] = dv ? dv->btx[IV(iv, jv)] : 0.0;
+        by[n] = dv ? dv->bty[IV(iv, jv)] : 0.0;
       }
       for (int p = 0; p < 4; ++p) {
         double ddx[4], ddy[4], detJ;
@@ -1704,6 +1798,16 @@ static int assemble_2d(int approx, int nx, int ny, int nz, int nhalo, const doub
                                    &flwa[IFL(1, i, j)], &flwafact[IFL(1, i, j)], rhoi, grav, ek);
           efvs_qp[p] = 0.0;
           for (int k = 1; k <= nz - 1; ++k) efvs_qp[p] = efvs_qp[p] + ek[k - 1] * (sigma[k] - sigma[k - 1]);
+        } else if (approx == ORC_APPROX_DIVA) {
+          double *ek = eq + (size_t)p * (nz - 1);
+          double *e3 = dv->eq3 + (IC(i, j) * 4 + (size_t)p) * (size_t)(nz - 1);
+          effective_viscosity_diva(whichefvs, efvs_constant, nz, sigma, p, ddx, ddy, u, v, bx, by,
+                                   &flwafact[IFL(1, i, j)], e3);
+          efvs_qp[p] = 0.0;
+          for (int k = 1; k <= nz - 1; ++k) {
+            ek[k - 1] = e3[k - 1];
+            efvs_qp[p] = efvs_qp[p] + ek[k - 1] * (sigma[k] - sigma[k - 1]);
+          }
         } else {
           efvs_qp[p] = effective_viscosity_ssa(whichefvs, efvs_constant, ddx, ddy, u, v, fl2);
           for (int k = 1; k <= nz - 1; ++k) eq[(size_t)p * (nz - 1) + k - 1] = efvs_qp[p];
@@ -1719,6 +1823,9 @@ static int assemble_2d(int approx, int nx, int ny, int nz, int nhalo, const doub
             Kvv[nr][nc] = Kvv[nr][nc] + f * (4.0 * ddy[nr] * ddy[nc] + ddx[nr] * ddx[nc]);
           }
       }
+      if (approx == ORC_APPROX_DIVA)
+        integrals_diva(nz, sigma, dv->thck[IC(i, j)], eq, &dv->omega_k[IC(i, j) * (size_t)nz],
+                       &dv->omega[IC(i, j)]);
       for (int k = 1; k <= nz - 1; ++k) {
         double e = 0.0;
         for (int p = 0; p < 4; ++p) e = e + eq[(size_t)p * (nz - 1) + k - 1];
@@ -1913,8 +2020,8 @@ int orc_assemble_2d_system(const orc_model *m, const orc_setup *s, int approx,
   if (approx != ORC_APPROX_SSA && approx != ORC_APPROX_L1L2) return ORC_ERR_ARGS;
   int st = assemble_2d(approx, nx, ny, nz, m->nhalo, s->sigma, s->active_cell, s->xVertex,
                        s->yVertex, u2, v2, s->stagthck, s->flwafact, m->flwa, s->dusrf_dx,
-                       s->dusrf_dy, m->rhoi, m->grav, m->which_efvs, m->efvs_constant, efvs, Auu,
-                       Auv, Avu, Avv);
+                       s->dusrf_dy, m->rhoi, m->grav, NULL, m->which_efvs, m->efvs_constant, efvs,
+                       Auu, Auv, Avu, Avv);
   if (st != ORC_OK) return st;
   if (m->which_babc != ORC_BABC_NO_SLIP)
     basal_sliding_bc(nx, ny, 1, m->nhalo, m->dx, m->dy, s->active_cell, s->active_vertex,
@@ -2057,6 +2164,224 @@ int orc_velo_2d_solve(const orc_model *m, int approx, double *uvel, double *vvel
   stats->status = status;
   free(Auu); free(Auv); free(Avu); free(Avv); free(bu); free(bv);
   free(u2); free(v2); free(us); free(vs); free(u3); free(v3);
+  orc_setup_free(&s);
+  return status;
+}
+
+/* DIVA: the ice-plus-land mask of the setup (:1486-1496), with which
+ * omega and omega_k are staggered. */
+static void ice_plus_land(const orc_model *m, const orc_setup *s, int *ipl) {
+  const size_t nc = (size_t)m->nx * m->ny;
+  for (size_t c = 0; c < nc; ++c) ipl[c] = (s->ice_mask[c] == 1 || s->land_mask[c] == 1) ? 1 : 0;
+}
+
+/* One assembled DIVA system (:2703-2990) at the mean velocity (u2, v2):
+ * the assembly updates efvs_qp_3d (eq3, in/out) from the basal traction
+ * (btx, bty) and gives omega_k (nz,nx,ny) and omega (nx,ny); omega is
+ * halo-updated and staggered over the ice-plus-land cells; beta_eff =
+ * beta / (1 + beta stag_omega), or 1 / stag_omega on a no-slip bed (0
+ * where stag_omega = 0) (Goldberg 2011 eq. 40-41, :2750-2790), enters the
+ * basal term; then the bed level's Dirichlet rows, halo update and
+ * symmetry check as for the other 2-D solves. */
+int orc_assemble_diva_system(const orc_model *m, const orc_setup *s, const double *beta_internal,
+                             const double *u2, const double *v2, const double *btx,
+                             const double *bty, double *eq3, double *efvs, double *omega_k,
+                             double *omega, double *beta_eff, double *Auu, double *Auv,
+                             double *Avu, double *Avv, double *bu, double *bv, long *nNonzeros) {
+  const int nx = m->nx, ny = m->ny, nz = m->nz;
+  const size_t nvx = (size_t)(nx - 1) * (ny - 1), nc = (size_t)nx * ny;
+  diva_state dv = {eq3, btx, bty, m->thck, omega_k, omega};
+  int st = assemble_2d(ORC_APPROX_DIVA, nx, ny, nz, m->nhalo, s->sigma, s->active_cell, s->xVertex,
+                       s->yVertex, u2, v2, s->stagthck, s->flwafact, m->flwa, NULL, NULL, m->rhoi,
+                       m->grav, &dv, m->which_efvs, m->efvs_constant, efvs, Auu, Auv, Avu, Avv);
+  if (st != ORC_OK) return st;
+  orc_halo_cell_real(nx, ny, m->periodic, omega, 0.0, 0.0);
+  int *ipl = malloc(nc * sizeof(int));
+  double *so = malloc(nvx * sizeof(double));
+  ice_plus_land(m, s, ipl);
+  orc_stagger(nx, ny, omega, so, ipl, 1);
+  for (size_t w = 0; w < nvx; ++w) {
+    if (m->which_babc == ORC_BABC_NO_SLIP)
+      beta_eff[w] = so[w] > 0.0 ? 1.0 / so[w] : 0.0;
+    else
+      beta_eff[w] = beta_internal[w] / (1.0 + beta_internal[w] * so[w]);
+  }
+  free(ipl);
+  free(so);
+  basal_sliding_bc(nx, ny, 1, m->nhalo, m->dx, m->dy, s->active_cell, s->active_vertex, beta_eff,
+                   s->xVertex, s->yVertex, m->which_assemble_beta, Auu, Avv);
+  int *um = calloc(nvx, sizeof(int)), *vm = calloc(nvx, sizeof(int));
+  for (int j = 1; j <= ny - 1; ++j)
+    for (int i = 1; i <= nx - 1; ++i) {
+      const size_t w = IV(i, j);
+      double lu = 0.0, lv = 0.0;
+      for (int k = 1; k <= nz; ++k) {
+        lu = lu + s->loadu[IX(k, i, j)];
+        lv = lv + s->loadv[IX(k, i, j)];
+      }
+      bu[w] = lu;
+      bv[w] = lv;
+      um[w] = s->umask_dirichlet[IX(nz, i, j)];
+      vm[w] = s->vmask_dirichlet[IX(nz, i, j)];
+    }
+  dirichlet_bc_3d(nx, ny, 1, m->nhalo, s->active_vertex, um, vm, u2, v2, Auu, Auv, Avu, Avv, bu, bv);
+  free(um);
+  free(vm);
+  orc_halo_stag(nx, ny, 27, m->periodic, Auu);
+  orc_halo_stag(nx, ny, 27, m->periodic, Auv);
+  orc_halo_stag(nx, ny, 27, m->periodic, Avu);
+  orc_halo_stag(nx, ny, 27, m->periodic, Avv);
+  orc_halo_stag(nx, ny, 1, m->periodic, bu);
+  orc_halo_stag(nx, ny, 1, m->periodic, bv);
+  check_symmetry_assembled_3d(nx, ny, 1, m->periodic, s->active_vertex, Auu, Auv, Avu, Avv);
+  *nNonzeros = count_nonzeros_3d(nx, ny, 1, m->periodic, s->active_vertex, Auu, Auv, Avu, Avv);
+  return ORC_OK;
+}
+
+/* The DIVA step after each linear solve (:3658-3696): the basal traction
+ * beta_eff u_mean at every vertex, omega_k staggered over the
+ * ice-plus-land cells level by level (no halo update first, as there),
+ * and compute_3d_velocity_diva (:5730-5830) for the mean velocity
+ * (diva_level_index = 0): at active vertices u(nz) = u_mean - tau_b
+ * stag_omega, u(k) = u(nz) + tau_b stag_omega_k(k); then the halo update.
+ * omega is taken halo-updated, as orc_assemble_diva_system leaves it. */
+int orc_velocity_3d_diva(const orc_model *m, const orc_setup *s, const double *beta_eff,
+                         const double *omega_k, const double *omega, const double *u2,
+                         const double *v2, double *btx, double *bty, double *uvel,
+                         double *vvel) {
+  const int nx = m->nx, ny = m->ny, nz = m->nz;
+  const size_t nvx = (size_t)(nx - 1) * (ny - 1), nc = (size_t)nx * ny;
+  for (size_t w = 0; w < nvx; ++w) {
+    btx[w] = beta_eff[w] * u2[w];
+    bty[w] = beta_eff[w] * v2[w];
+  }
+  int *ipl = malloc(nc * sizeof(int));
+  double *lay = malloc(nc * sizeof(double)), *sok = malloc(nvx * nz * sizeof(double)),
+         *so = malloc(nvx * sizeof(double)), *t = malloc(nvx * sizeof(double));
+  ice_plus_land(m, s, ipl);
+  for (int k = 1; k <= nz; ++k) {
+    for (size_t c = 0; c < nc; ++c) lay[c] = omega_k[c * nz + (k - 1)];
+    orc_stagger(nx, ny, lay, t, ipl, 1);
+    for (size_t w = 0; w < nvx; ++w) sok[w * nz + (k - 1)] = t[w];
+  }
+  orc_stagger(nx, ny, omega, so, ipl, 1);
+  for (int j = 1; j <= ny - 1; ++j)
+    for (int i = 1; i <= nx - 1; ++i) {
+      const size_t w = IV(i, j);
+      if (!s->active_vertex[w]) continue;
+      uvel[IX(nz, i, j)] = u2[w] - btx[w] * so[w];
+      vvel[IX(nz, i, j)] = v2[w] - bty[w] * so[w];
+      for (int k = 1; k <= nz - 1; ++k) {
+        uvel[IX(k, i, j)] = uvel[IX(nz, i, j)] + btx[w] * sok[w * nz + (k - 1)];
+        vvel[IX(k, i, j)] = vvel[IX(nz, i, j)] + bty[w] * sok[w * nz + (k - 1)];
+      }
+    }
+  orc_halo_stag(nx, ny, nz, m->periodic, uvel);
+  orc_halo_stag(nx, ny, nz, m->periodic, vvel);
+  free(ipl); free(lay); free(sok); free(so); free(t);
+  return ORC_OK;
+}
+
+/* glissade_velo_higher_solve, DIVA branch (whichapprox = HO_APPROX_DIVA):
+ * the mean velocity (uvel_2d, vvel_2d: in, the last solve's; out, this
+ * one's) from the 2-D system with beta_eff, the 3-D velocity and basal
+ * traction (btractx, btracty: in/out) after every iteration, efvs (in:
+ * the last solve's layer viscosities, the start of efvs_qp_3d, :1166-1170;
+ * out: this solve's).  calcbeta reads the 3-D basal velocity (:2240-2243);
+ * a no-slip bed enters through beta_eff, not the Dirichlet masks
+ * (:1274-1278); Dirichlet columns start from the bed velocity (:1300-1303)
+ * and inactive owned vertices from zero (:1700-1711). */
+int orc_velo_diva_solve(const orc_model *m, double *uvel, double *vvel, double *uvel_2d,
+                        double *vvel_2d, double *btractx, double *btracty, double *efvs,
+                        double *beta_internal, orc_stats *stats) {
+  const int nx = m->nx, ny = m->ny, nz = m->nz;
+  const size_t nvx = (size_t)(nx - 1) * (ny - 1), nc = (size_t)nx * ny, nA = nvx * 27;
+  orc_setup s;
+  orc_setup_alloc(m, &s);
+  memset(stats, 0, sizeof(*stats));
+  int st = orc_setup_solve(m, &s, uvel, vvel);
+  if (st != ORC_OK) { orc_setup_free(&s); stats->status = st; return st; }
+  for (int j = 1; j <= ny - 1; ++j)
+    for (int i = 1; i <= nx - 1; ++i) {
+      const size_t w = IV(i, j);
+      const int kin = m->kinbcmask && m->kinbcmask[w] == 1;
+      if (!kin) {  /* no bed mask for a no-slip DIVA solve */
+        s.umask_dirichlet[IX(nz, i, j)] = 0;
+        s.vmask_dirichlet[IX(nz, i, j)] = 0;
+      } else {
+        uvel_2d[w] = uvel[IX(nz, i, j)];
+        vvel_2d[w] = vvel[IX(nz, i, j)];
+      }
+    }
+  int ilo, ihi, jlo, jhi;
+  owned_range(nx, ny, m->periodic, &ilo, &ihi, &jlo, &jhi);
+  for (int j = jlo; j <= jhi; ++j)
+    for (int i = ilo; i <= ihi; ++i)
+      if (!s.active_vertex[IV(i, j)]) { uvel_2d[IV(i, j)] = 0.0; vvel_2d[IV(i, j)] = 0.0; }
+  double *eq3 = xalloc((size_t)4 * (nz - 1) * nc * 8), *omk = xalloc((size_t)nz * nc * 8),
+         *om = xalloc(nc * 8), *be = xalloc(nvx * 8);
+  for (size_t c = 0; c < nc; ++c)
+    for (int p = 0; p < 4; ++p)
+      for (int k = 0; k < nz - 1; ++k) eq3[(c * 4 + p) * (nz - 1) + k] = efvs[c * (nz - 1) + k];
+  double *Auu = xalloc(nA * 8), *Auv = xalloc(nA * 8), *Avu = xalloc(nA * 8),
+         *Avv = xalloc(nA * 8), *bu = xalloc(nvx * 8), *bv = xalloc(nvx * 8),
+         *us = xalloc(nvx * 8), *vs = xalloc(nvx * 8);
+  int counter = 0;
+  double outer_it_criterion = 1.0e10, outer_it_target = 1.0e-12;
+  const double L2_target = 1.0e-4, L2_target_relative = 1.0e-7, resid_target = 1.0e-4;
+  int status = ORC_OK;
+  while (outer_it_criterion >= outer_it_target && counter < m->maxiter_nonlinear) {
+    counter = counter + 1;
+    st = orc_calcbeta(m, &s, uvel, vvel, beta_internal);  /* ubas = uvel(nz,:,:) */
+    if (st != ORC_OK) { status = st; break; }
+    memcpy(us, uvel_2d, nvx * 8);
+    memcpy(vs, vvel_2d, nvx * 8);
+    long nnz = 0;
+    st = orc_assemble_diva_system(m, &s, beta_internal, uvel_2d, vvel_2d, btractx, btracty, eq3, efvs,
+                                  omk, om, be, Auu, Auv, Avu, Avv, bu, bv, &nnz);
+    if (st != ORC_OK) { status = st; break; }
+    if (nnz == 0) {
+      memset(uvel_2d, 0, nvx * 8);
+      memset(vvel_2d, 0, nvx * 8);
+      status = ORC_ZERO_MATRIX;
+      break;
+    }
+    residual_vector_3d(nx, ny, 1, m->periodic, s.active_vertex, Auu, Auv, Avu, Avv, bu, bv, uvel_2d,
+                       vvel_2d, &stats->L2_norm, &stats->L2_norm_relative);
+    double err = 0.0;
+    int niters = 0;
+    if (m->which_sparse == ORC_SPARSE_PCG_CHRONGEAR)
+      st = orc_pcg_chrongear_3d(nx, ny, 1, m->periodic, s.active_vertex, Auu, Auv, Avu, Avv, bu, bv,
+                                uvel_2d, vvel_2d, m->which_precond, m->pcg_maxiters, m->pcg_tol,
+                                m->pcg_ncheck, &err, &niters);
+    else
+      st = orc_pcg_standard_3d(nx, ny, 1, m->periodic, s.active_vertex, Auu, Auv, Avu, Avv, bu, bv,
+                               uvel_2d, vvel_2d, m->which_precond, m->pcg_maxiters, m->pcg_tol,
+                               m->pcg_ncheck, &err, &niters);
+    stats->pcg_iters_total += niters;
+    stats->pcg_iters_last = niters;
+    stats->pcg_err_last = err;
+    if (st == ORC_ERR_NAN) { status = st; break; }
+    orc_halo_stag(nx, ny, 1, m->periodic, uvel_2d);
+    orc_halo_stag(nx, ny, 1, m->periodic, vvel_2d);
+    const double resid_velo =
+        residual_velocity_2d(nx, ny, m->periodic, m->which_resid, uvel_2d, vvel_2d, us, vs);
+    stats->resid_velo = resid_velo;
+    orc_velocity_3d_diva(m, &s, be, omk, om, uvel_2d, vvel_2d, btractx, btracty, uvel, vvel);
+    if (m->which_resid == ORC_RESID_L2NORM) {
+      outer_it_criterion = stats->L2_norm; outer_it_target = L2_target;
+    } else if (m->which_resid == ORC_RESID_L2NORM_RELATIVE) {
+      outer_it_criterion = stats->L2_norm_relative; outer_it_target = L2_target_relative;
+    } else {
+      outer_it_criterion = resid_velo; outer_it_target = resid_target;
+    }
+  }
+  stats->picard_iters = counter;
+  stats->converged = (status == ORC_OK && counter < m->maxiter_nonlinear) ? 1 : 0;
+  if (status == ORC_OK && !stats->converged) status = ORC_WARN_PICARD_NOT_CONVERGED;
+  stats->status = status;
+  free(eq3); free(omk); free(om); free(be);
+  free(Auu); free(Auv); free(Avu); free(Avv); free(bu); free(bv); free(us); free(vs);
   orc_setup_free(&s);
   return status;
 }

@@ -39,7 +39,7 @@ enum {
   ORC_GRADIENT_MARGIN_MARINE = 2,
   ORC_ASSEMBLE_STANDARD = 0, ORC_ASSEMBLE_LOCAL = 1,
   ORC_GROUND_NO_GLP = 0, ORC_GROUND_ALL = 2,
-  ORC_APPROX_SSA = 1, ORC_APPROX_L1L2 = 3
+  ORC_APPROX_SSA = 1, ORC_APPROX_L1L2 = 3, ORC_APPROX_DIVA = 4
 };
 
 /* Status codes shared with the product's C ABI. */
@@ -223,6 +223,24 @@ int orc_assemble_2d_system(const orc_model *m, const orc_setup *s, int approx,
  * viscosities efvs (nz-1,nx,ny) of the last assembly. */
 int orc_velocity_3d_l1l2(const orc_model *m, const orc_setup *s, const double *efvs,
                          double *uvel, double *vvel);
+/* DIVA (Goldberg 2011): one assembled system at the mean velocity with
+ * the traction (btx, bty); eq3 (nz-1,4,nx,ny) efvs_qp_3d in/out; outputs
+ * efvs (nz-1,nx,ny), omega_k (nz,nx,ny), omega (nx,ny, halo-updated) and
+ * beta_eff (nx-1,ny-1). */
+int orc_assemble_diva_system(const orc_model *m, const orc_setup *s, const double *beta_internal,
+                             const double *u2, const double *v2, const double *btx,
+                             const double *bty, double *eq3, double *efvs, double *omega_k,
+                             double *omega, double *beta_eff, double *Auu, double *Auv,
+                             double *Avu, double *Avv, double *bu, double *bv, long *nNonzeros);
+/* The step after a DIVA linear solve: traction, 3-D velocity, halo. */
+int orc_velocity_3d_diva(const orc_model *m, const orc_setup *s, const double *beta_eff,
+                         const double *omega_k, const double *omega, const double *u2,
+                         const double *v2, double *btx, double *bty, double *uvel,
+                         double *vvel);
+/* Whole DIVA solve: uvel_2d, vvel_2d, btractx, btracty and efvs in/out. */
+int orc_velo_diva_solve(const orc_model *m, double *uvel, double *vvel, double *uvel_2d,
+                        double *vvel_2d, double *btractx, double *btracty, double *efvs,
+                        double *beta_internal, orc_stats *stats);
 /* Whole glissade_velo_higher_solve, 3-D Blatter-Pattyn branch. */
 int orc_velo_higher_solve(const orc_model *m, double *uvel, double *vvel,
                           double *efvs, double *beta_internal,

@@ -185,6 +185,31 @@ def velo_l1l2_solve(m, uvel=None, vvel=None):
     return velo_2d_solve(m, APPROX_L1L2, uvel, vvel)
 
 
+def velo_diva_solve(m, uvel=None, vvel=None, uvel_2d=None, vvel_2d=None, btractx=None, btracty=None,
+                    efvs=None):
+    """DIVA branch of the solve.  The mean velocity (uvel_2d, vvel_2d), the
+    basal traction (btractx, btracty) and efvs are the last solve's (zero
+    by default) on entry; returns (uvel, vvel, efvs, beta_internal, stats,
+    extra) with extra = dict(uvel_2d, vvel_2d, btractx, btracty)."""
+    keep = _Keep()
+    om = make_model(m, keep)
+    vs = (m.ny - 1, m.nx - 1)
+
+    def arr(a, shape):
+        return np.zeros(shape) if a is None else np.array(a, dtype=np.float64, copy=True)
+
+    u, v = arr(uvel, m.vshape3), arr(vvel, m.vshape3)
+    u2, v2, bx, by = arr(uvel_2d, vs), arr(vvel_2d, vs), arr(btractx, vs), arr(btracty, vs)
+    ef = arr(efvs, (m.ny, m.nx, m.nz - 1))
+    beta = np.zeros(vs)
+    st = OrcStats()
+    rc = lib().orc_velo_diva_solve(C.byref(om), _p(u), _p(v), _p(u2), _p(v2), _p(bx), _p(by), _p(ef),
+                                   _p(beta), C.byref(st))
+    if rc == 10:
+        raise RuntimeError("orc_velo_diva_solve: bad arguments")
+    return u, v, ef, beta, st.as_dict(), dict(uvel_2d=u2, vvel_2d=v2, btractx=bx, btracty=by)
+
+
 def setup(m, uvel=None, vvel=None):
     """Setup of glissade_velo_higher_solve: returns dict of boundary inputs."""
     keep = _Keep()
@@ -302,6 +327,42 @@ def velocity_3d_l1l2(m, su, efvs, uvel, vvel):
     lib().orc_velocity_3d_l1l2(C.byref(om), C.byref(s), _p(np.ascontiguousarray(efvs, np.float64)),
                                _p(u), _p(v))
     return u, v
+
+
+def assemble_diva_system(m, su, beta, u2, v2, btx, bty, eq3):
+    """One assembled DIVA system at the mean velocity (u2, v2) with the
+    traction (btx, bty); eq3 (ny, nx, 4, nz-1) is efvs_qp_3d, updated in
+    place.  Returns A, bu, bv, efvs, omega_k (ny, nx, nz), omega (ny, nx),
+    beta_eff (ny-1, nx-1), nonzeros."""
+    keep, om, s = su["_keep"]
+    nx, ny, nz = m.nx, m.ny, m.nz
+    A = [np.zeros((ny - 1, nx - 1, 1, 27)) for _ in range(4)]
+    bu, bv = np.zeros((ny - 1, nx - 1)), np.zeros((ny - 1, nx - 1))
+    efvs = np.zeros((ny, nx, nz - 1))
+    omk, omg, be = np.zeros((ny, nx, nz)), np.zeros((ny, nx)), np.zeros((ny - 1, nx - 1))
+    assert eq3.dtype == np.float64 and eq3.flags["C_CONTIGUOUS"] and eq3.shape == (ny, nx, 4, nz - 1)
+    nnz = C.c_long(0)
+    c = np.ascontiguousarray
+    rc = lib().orc_assemble_diva_system(C.byref(om), C.byref(s), _p(c(beta, np.float64)), _p(c(u2, np.float64)),
+                                        _p(c(v2, np.float64)), _p(c(btx, np.float64)), _p(c(bty, np.float64)),
+                                        _p(eq3), _p(efvs), _p(omk), _p(omg), _p(be), *[_p(a) for a in A],
+                                        _p(bu), _p(bv), C.byref(nnz))
+    if rc != 0:
+        raise RuntimeError(f"orc_assemble_diva_system failed: {rc}")
+    return A, bu, bv, efvs, omk, omg, be, nnz.value
+
+
+def velocity_3d_diva(m, su, beta_eff, omega_k, omega, u2, v2, uvel, vvel):
+    """The step after a DIVA linear solve: returns (btx, bty, uvel, vvel)."""
+    keep, om, s = su["_keep"]
+    c = np.ascontiguousarray
+    bx, by = np.zeros((m.ny - 1, m.nx - 1)), np.zeros((m.ny - 1, m.nx - 1))
+    u = np.array(uvel, dtype=np.float64, copy=True)
+    v = np.array(vvel, dtype=np.float64, copy=True)
+    lib().orc_velocity_3d_diva(C.byref(om), C.byref(s), _p(c(beta_eff, np.float64)), _p(c(omega_k, np.float64)),
+                               _p(c(omega, np.float64)), _p(c(u2, np.float64)), _p(c(v2, np.float64)),
+                               _p(bx), _p(by), _p(u), _p(v))
+    return bx, by, u, v
 
 
 def matvec(m, active_vertex, A, xu, xv):

@@ -17,14 +17,15 @@ struct Emu {
   HostPlan p;
   std::vector<InstParams> inst;
   std::vector<InstState> st;
-  std::vector<double> qp, efvs, badj, lw;
-  std::vector<double2> A, x, b, x3;
+  std::vector<double> qp, efvs, badj, lw, eq3, omk, om, somega, beff;
+  std::vector<double2> A, x, b, x3, bt;
   DevView v;
   void bind() {
     std::memset(&v, 0, sizeof(v));
     v.nz = p.nz; v.ncols = p.ncols; v.nnodes = p.nnodes; v.npad = p.npad;
     v.solve2d = p.solve2d ? 1 : 0;
     v.l1l2 = p.l1l2 ? 1 : 0;
+    v.diva = p.diva ? 1 : 0;
     v.nl = p.nz_out - 1;
     v.ncells = p.ncells; v.nelem = p.nelem; v.ninst = p.ninst; v.ntiles = p.ntiles;
     int anyd = 0;
@@ -45,6 +46,17 @@ struct Emu {
       v.col_ds = p.col_ds.data(); v.col_h = p.col_h.data();
       lw.assign(4 * (size_t)v.nl * std::max(p.ncells, 1), 0.0); v.lw = lw.data();
       x3.assign((size_t)std::max(p.ncols, 1) * (v.nl + 1), double2{0, 0}); v.x3 = x3.data();
+    }
+    if (p.diva) {
+      const size_t nc = (size_t)std::max(p.ncells, 1), ncol = (size_t)std::max(p.ncols, 1);
+      v.cell_thck = p.cell_thck.data(); v.col_ipl = p.col_ipl.data();
+      eq3 = p.eq3_0; eq3.resize(std::max<size_t>(eq3.size(), 1)); v.eq3 = eq3.data();
+      omk.assign(nc * (v.nl + 1), 0.0); v.cell_omk = omk.data();
+      om.assign(nc, 0.0); v.cell_om = om.data();
+      somega.assign(ncol, 0.0); v.col_somega = somega.data();
+      beff.assign(ncol, 0.0); v.col_beff = beff.data();
+      bt = p.col_bt0; bt.resize(ncol); v.col_bt = bt.data();
+      x3.assign(ncol * (v.nl + 1), double2{0, 0}); v.x3 = x3.data();
     }
     badj.assign(4 * (size_t)p.npad, 0.0); v.badj = badj.data();
     A.assign(2 * 27 * (size_t)p.npad, double2{0, 0}); v.A = A.data();
@@ -358,6 +370,96 @@ extern "C" int emu_velocity_3d_l1l2(const bp_inputs* in, const double* uvel, con
   for (int c = 0; c < NCELL; ++c) l1l2_cell(E.v, c);
   for (int col = 0; col < E.p.ncols; ++col) l1l2_column(E.v, col);
   scatter_velocity_3d(E.p, 0, E.x3.data(), uout, vout);
+  return 0;
+}
+
+// One DIVA iteration's device bodies on the host plan, without the linear
+// solve: assembly pass 1 with the point viscosities (qp2_element_point,
+// diva_point_efvs), the cell integrals, beta_eff, the rows with the basal
+// and Dirichlet terms, then the traction and 3-D velocity of the mean
+// velocity it started from (diva_column_velocity) and the scatters.  The
+// mean velocity, traction and viscosities come from in->diva; outputs:
+// the matrix and b as emu_assemble_2d, efvs (nz-1,nx,ny), eq3
+// (4*(nz-1),nx,ny), omega_k (nz,nx,ny), omega (nx,ny), beta_eff
+// (nx-1,ny-1), the 3-D velocity (uout, vout: their bed level kept away from
+// the columns) and in->diva's uvel_2d .. btracty written back.
+extern "C" int emu_diva_step(const bp_inputs* in, double* Auu, double* Auv, double* Avu, double* Avv,
+                             double* bu, double* bv, double* efvs, double* eq3, double* omega_k,
+                             double* omega, double* beta_eff, double* uout, double* vout) {
+  Emu E;
+  std::string err;
+  if (!build_plan(in, 1, &E.p, &err) || !E.p.diva) return 10;
+  E.bind();
+  std::vector<double> dummy((size_t)in->nz * (in->nx - 1) * (in->ny - 1), 0.0);
+  gather_velocity(E.p, 0, dummy.data(), dummy.data(), E.x.data());
+  RefTables T;
+  fill_ref_tables(&T);
+  const int nl = E.v.nl, NCELL = E.p.ncells, NC = E.p.ncols, nx = in->nx, ny = in->ny;
+  for (int c = 0; c < NCELL; ++c) {
+    double sk[kNzMax] = {0.0};
+    for (int p = 0; p < 4; ++p) {
+      double out[5], eq = 0.0, ek[kNzMax];
+      if (!qp2_element_point(E.v, T, c, p, out, &eq, ek)) return 2;
+      std::memcpy(&E.qp[((size_t)c * 8 + p) * 10], out, sizeof(out));
+      for (int k = 0; k < nl; ++k) sk[k] += ek[k];
+    }
+    for (int k = 0; k < nl; ++k) E.efvs[(size_t)c * nl + k] = sk[k] / 4.0;
+  }
+  for (int c = 0; c < NCELL; ++c) diva_cell_integrals(E.v, c);
+  for (int col = 0; col < NC; ++col) diva_column_beta(E.v, col);
+  for (int c = 0; c < NCELL; ++c)
+    for (int q = 0; q < 4; ++q) {
+      const int col = E.p.cell_cols[(size_t)q * NCELL + c];
+      E.p.cell_beta[(size_t)q * NCELL + c] = col >= 0 ? E.beff[col] : 0.0;
+    }
+  const DevView& v = E.v;
+  double* Ad = reinterpret_cast<double*>(E.A.data());
+  for (int B = 0; B < 4; ++B)
+    for (int n = 0; n < v.nnodes; ++n) {
+      double acc[27];
+      double adj = 0.0;
+      switch (B) {
+        case 0: row_assemble2<0>(v, T, n, acc); row_basal<0>(v, T, n, 0, acc); adj = row_dirichlet<0>(v, n, 0, acc); break;
+        case 1: row_assemble2<1>(v, T, n, acc); row_basal<1>(v, T, n, 0, acc); adj = row_dirichlet<1>(v, n, 0, acc); break;
+        case 2: row_assemble2<2>(v, T, n, acc); row_basal<2>(v, T, n, 0, acc); adj = row_dirichlet<2>(v, n, 0, acc); break;
+        default: row_assemble2<3>(v, T, n, acc); row_basal<3>(v, T, n, 0, acc); adj = row_dirichlet<3>(v, n, 0, acc); break;
+      }
+      for (int m = 0; m < 27; ++m)
+        Ad[(((size_t)((B >> 1) * 27 + m)) * v.npad + n) * 2 + (B & 1)] = acc[m];
+      E.badj[(size_t)B * v.npad + n] = adj;
+    }
+  const size_t np = E.p.npad;
+  for (int n = 0; n < E.p.nnodes; ++n) {
+    const uint8_t dm = E.p.dmask[n];
+    double u = E.p.load[n].x - E.badj[n] - E.badj[np + n];
+    double w = E.p.load[n].y - E.badj[2 * np + n] - E.badj[3 * np + n];
+    if (dm & 1) u = E.x[n].x;
+    if (dm & 2) w = E.x[n].y;
+    E.b[n] = double2{u, w};
+  }
+  scatter_matrix(E.p, E.A.data(), Auu, Auv, Avu, Avv);
+  const size_t nvert = (size_t)(nx - 1) * (ny - 1), ncell = (size_t)nx * ny;
+  std::memset(bu, 0, nvert * 8);
+  std::memset(bv, 0, nvert * 8);
+  scatter_vector(E.p, 0, E.b.data(), bu, bv);
+  scatter_efvs(E.p, 0, E.efvs.data(), efvs);
+  std::memset(eq3, 0, ncell * 4 * nl * 8);
+  std::memset(omega_k, 0, ncell * (nl + 1) * 8);
+  std::memset(omega, 0, ncell * 8);
+  std::memset(beta_eff, 0, nvert * 8);
+  for (int c = 0; c < NCELL; ++c) {
+    const size_t cc = (size_t)(E.p.cell_ij[NCELL + c] - 1) * nx + (E.p.cell_ij[c] - 1);
+    for (int i = 0; i < 4 * nl; ++i) eq3[cc * 4 * nl + i] = E.eq3[(size_t)c * 4 * nl + i];
+    for (int k = 0; k <= nl; ++k) omega_k[cc * (nl + 1) + k] = E.omk[(size_t)c * (nl + 1) + k];
+    omega[cc] = E.om[c];
+  }
+  for (int col = 0; col < NC; ++col) {
+    const size_t w = (size_t)(E.p.col_ij[NC + col] - 1) * (nx - 1) + (E.p.col_ij[col] - 1);
+    beta_eff[w] = E.beff[col];
+  }
+  for (int col = 0; col < NC; ++col) diva_column_velocity(E.v, col);
+  scatter_velocity_3d(E.p, 0, E.x3.data(), uout, vout);
+  scatter_diva(E.p, 0, E.x.data(), E.bt.data());
   return 0;
 }
 
