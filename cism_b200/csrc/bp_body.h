@@ -198,13 +198,16 @@ BP_HD bool qp_element_point(const DevView& v, const RefTables& T, int e, int p,
                     v.flwafact[e], out, efvs_qp);
 }
 
-// compute_internal_stress (:6968-7195), 3-D higher-order branch, for
-// element e at the current velocity: the velocity gradient and the
-// effective viscosity at the 8 quadrature points (assembly's arithmetic),
-// tau_xz = efvs du/dz, tau_yz = efvs dv/dz, tau_xx = 2 efvs du/dx,
-// tau_yy = 2 efvs dv/dy, tau_xy = efvs (dv/dx + du/dy), each averaged, and
-// tau_eff from the averages.  tau = {xz, yz, xx, yy, xy, eff}; false for a
-// singular Jacobian.
+// compute_internal_stress (:6968-7195) for element e at the current 3-D
+// velocity: the velocity gradient and the effective viscosity at the 8
+// quadrature points (assembly's arithmetic), tau_xz = efvs du/dz, tau_yz =
+// efvs dv/dz, tau_xx = 2 efvs du/dx, tau_yy = 2 efvs dv/dy, tau_xy = efvs
+// (dv/dx + du/dy), each averaged, and tau_eff from the averages.  The
+// shallow-shelf solve takes the horizontal gradients only and its
+// viscosity branch (:7110-7116, :7325-7338); L1L2 takes the element's
+// layer viscosity v.efvs[e] at every point (:7135-7139); Blatter-Pattyn
+// and DIVA the 3-D gradients and viscosity.  tau = {xz, yz, xx, yy, xy,
+// eff}; false for a singular Jacobian.
 BP_HD bool stress_element(const DevView& v, const RefTables& T, int e, double* tau) {
   double x[8], y[8], z[8], u[8], w[8];
   const InstParams& ip = elem_gather(v, e, x, y, z, u, w);
@@ -213,7 +216,11 @@ BP_HD bool stress_element(const DevView& v, const RefTables& T, int e, double* t
     double Ji[9], det, g[6];
     if (!qp_jacobian_inverse(T, p, x, y, z, Ji, &det)) return false;
     qp_velocity_gradient(T, p, Ji, u, w, g);
-    const double efvs = qp_efvs(ip.which_efvs, ip.efvs_constant, v.flwafact[e], g);
+    if (v.solve2d && !v.l1l2 && !v.diva) {
+      g[2] = 0.0;
+      g[5] = 0.0;
+    }
+    const double efvs = v.l1l2 ? v.efvs[e] : qp_efvs(ip.which_efvs, ip.efvs_constant, v.flwafact[e], g);
     txz = txz + efvs * g[2];
     tyz = tyz + efvs * g[5];
     txx = txx + 2.0 * efvs * g[0];

@@ -860,19 +860,30 @@ int bp_problem_diagnostics(bp_problem* P, int which_bfric, double* const* tau_xz
   bool want_tau = false;
   for (auto o : outs) want_tau = want_tau || o;
   if (!p.ncells) return BP_ERR_ARGS;  // matrix-level problems have no elements
-  if (p.diva) {  // the basal velocity is not the solution vector there
-    c->err = "bp_problem_diagnostics: not for DIVA solves";
-    return BP_ERR_ARGS;
+  // 2-D solves: the 3-D elements over the model's levels with the 3-D
+  // velocity (L1L2, DIVA: the one the solve formed; shallow-shelf: its
+  // solution on every level) and, for the shallow-shelf stresses, the flow
+  // factor of each layer; DIVA's bed-face corners take beta_internal again
+  // (the loop left beta_eff there)
+  double2* x3 = P->v.x3;
+  const double* fl = nullptr;
+  if (p.solve2d && !p.l1l2 && !p.diva) {
+    x3 = P->arena->get<double2>(c->stream, "diag_x3", (size_t)std::max(p.ncols, 1) * p.nz_out);
+    launch_levels_from_2d(P->v, x3, p.nz_out, c->stream);
+    double* f = P->arena->get<double>(c->stream, "diag_flwafact", p.flwafact_layers.size());
+    upload(c->stream, f, p.flwafact_layers);
+    fl = f;
   }
-  if (p.solve2d && want_tau) {  // the stress routine's 2-D branches are not restated
-    c->err = "bp_problem_diagnostics: element stresses of 3-D Blatter-Pattyn solves only";
-    return BP_ERR_ARGS;
+  if (p.diva) {
+    if (p.any_sliding) launch_corner_beta(P->v, c->stream);
+    else upload(c->stream, P->v.cell_beta, p.cell_beta);
   }
-  const size_t ne = (size_t)p.nelem, nb = (size_t)std::max(p.ncells, p.ncols);
+  const DevView dv = diagnostics_view(P->v, p, x3, fl);
+  const size_t ne = (size_t)diagnostic_elements(p), nb = (size_t)std::max(p.ncells, p.ncols);
   double* d = P->arena->get<double>(c->stream, "diagnostics", (want_tau ? 6 * ne : 0) + nb);
   double* d_tau = want_tau ? d : nullptr;
   double* d_bf = bfricflx ? d + (want_tau ? 6 * ne : 0) : nullptr;
-  launch_diagnostics(P->v, which_bfric, d_tau, d_bf, c->stream);
+  launch_diagnostics(dv, which_bfric, d_tau, d_bf, c->stream);
   std::vector<double> tau(d_tau ? 6 * ne : 0), bf(d_bf ? nb : 0);
   if (d_tau) CK(cudaMemcpyAsync(tau.data(), d_tau, sizeof(double) * tau.size(), cudaMemcpyDeviceToHost, c->stream));
   if (d_bf) CK(cudaMemcpyAsync(bf.data(), d_bf, sizeof(double) * bf.size(), cudaMemcpyDeviceToHost, c->stream));

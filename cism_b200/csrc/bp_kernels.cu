@@ -1165,6 +1165,32 @@ void launch_dinv(const DevView& v, int precond, cudaStream_t s) {
   k_dinv<<<tile_grid(v), kTile, 0, s>>>(v, precond);
 }
 void launch_bb(const DevView& v, cudaStream_t s) { k_bb<<<tile_grid(v), kTile, 0, s>>>(v); }
+// The 3-D velocity of a shallow-shelf solve (its 2-D solution on every
+// level, :3745-3750) for the post-solve diagnostics.
+__global__ void __launch_bounds__(256) k_levels_from_2d(DevView v, double2* x3, int L) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < (long)v.ncols * L) x3[t] = v.x[t / L];
+}
+
+// The bed-face corner betas from the columns' beta_internal (0 where a
+// corner has no column) for every cell.
+__global__ void __launch_bounds__(256) k_corner_beta(DevView v) {
+  const int cell = blockIdx.x * blockDim.x + threadIdx.x;
+  if (cell >= v.ncells) return;
+  for (int q = 0; q < 4; ++q) {
+    const int col = v.cell_cols[(size_t)q * v.ncells + cell];
+    v.cell_beta[(size_t)q * v.ncells + cell] = col >= 0 ? v.col_beta[col] : 0.0;
+  }
+}
+
+void launch_levels_from_2d(const DevView& v, double2* x3, int L, cudaStream_t s) {
+  const long n = (long)v.ncols * L;
+  if (n > 0) k_levels_from_2d<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(v, x3, L);
+}
+void launch_corner_beta(const DevView& v, cudaStream_t s) {
+  if (v.ncells > 0) k_corner_beta<<<(unsigned)((v.ncells + 255) / 256), 256, 0, s>>>(v);
+}
+
 void launch_diagnostics(const DevView& v, int which_bfric, double* tau, double* bf, cudaStream_t s) {
   if (tau && v.nelem > 0) k_internal_stress<<<(v.nelem + 255) / 256, 256, 0, s>>>(v, tau);
   const int n = which_bfric == 0 ? v.ncells : v.ncols;

@@ -45,6 +45,10 @@ void launch_bb(const DevView& v, cudaStream_t s);
 // element stresses into tau[6][nelem] and the basal frictional heat flux
 // into bf ([ncells] for which_bfric 0, [ncols] for 1); either may be null
 void launch_diagnostics(const DevView& v, int which_bfric, double* tau, double* bf, cudaStream_t s);
+// a shallow-shelf solve's 2-D solution on each of L levels, x3 [ncols][L]
+void launch_levels_from_2d(const DevView& v, double2* x3, int L, cudaStream_t s);
+// cell_beta from col_beta (0 at a corner without a column), every cell
+void launch_corner_beta(const DevView& v, cudaStream_t s);
 // store: 0 full FP64, 1 symmetric FP64, 2 symmetric FP32; minb: 0, 6 or 8
 // resident CTAs per SM; grid: CTAs (0 = one per tile).  -1 if unavailable.
 int launch_tune_mv(int store, int minb, int grid, const DevView& v, cudaStream_t s);

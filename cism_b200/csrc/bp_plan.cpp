@@ -336,6 +336,7 @@ bool build_plan(const bp_inputs* in, int n, HostPlan* p, std::string* err) {
   p->cell_beta.resize(4 * (size_t)NCELL);
   const bool ssa = solve2d && !l1l2 && !diva;
   p->flwafact.resize((size_t)(ssa ? NCELL : NCELL * nl));
+  if (ssa) p->flwafact_layers.resize((size_t)NCELL * nl);
   if (diva) {
     p->cell_thck.resize(NCELL);
     p->eq3_0.resize((size_t)NCELL * 4 * nl);
@@ -470,6 +471,10 @@ bool build_plan(const bp_inputs* in, int n, HostPlan* p, std::string* err) {
         for (int q = 0; q < 4; ++q)
           for (int k = 0; k < nl; ++k)
             p->eq3_0[((size_t)g * 4 + q) * nl + k] = I.diva->efvs ? I.diva->efvs[cel(ic, jc, nx) * nl + k] : 0.0;
+      }
+      if (ssa) {
+        for (int k = 0; k < nl; ++k)
+          p->flwafact_layers[(size_t)g * nl + k] = I.flwafact[cel(ic, jc, nx) * nl + k];
       }
       if (ssa) {  // glissade_vertical_average (glissade_grid_operators.F90:1172-1236)
         double f = 0.0;
@@ -715,8 +720,8 @@ void halo_cells(int nx, int ny, int periodic, double* a) {
 void scatter_elements(const HostPlan& p, int b, const double* vals, int nv,
                       double* const* out) {
   const InstParams& ip = p.inst[b];
-  const int nx = p.nx[b], ny = p.ny[b], nz = p.nz, NCELL = p.ncells;
-  const size_t ne = (size_t)p.nelem;
+  const int nx = p.nx[b], ny = p.ny[b], nz = p.nz_out, NCELL = p.ncells;
+  const size_t ne = (size_t)diagnostic_elements(p);
   for (int f = 0; f < nv; ++f) {
     if (!out[f]) continue;
     std::memset(out[f], 0, sizeof(double) * (size_t)(nz - 1) * nx * ny);
@@ -726,6 +731,16 @@ void scatter_elements(const HostPlan& p, int b, const double* vals, int nv,
         out[f][cel(ic, jc, nx) * (nz - 1) + k] = vals[(size_t)f * ne + (size_t)g * (nz - 1) + k];
     }
   }
+}
+
+DevView diagnostics_view(const DevView& v, const HostPlan& p, double2* x3, const double* flwafact_layers) {
+  if (!p.solve2d) return v;
+  DevView d = v;
+  d.nz = p.nz_out;
+  d.nelem = diagnostic_elements(p);
+  d.x = x3;
+  if (!p.l1l2 && !p.diva) d.flwafact = flwafact_layers;
+  return d;
 }
 
 void scatter_bfric(const HostPlan& p, int b, int which, const double* vals,

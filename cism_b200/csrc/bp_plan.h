@@ -40,6 +40,7 @@ struct HostPlan {
   std::vector<int> cell_inst, cell_ij, cell_cols;
   std::vector<double> cell_s, cell_h, cell_beta, flwafact;
   std::vector<double> cell_flwa, cell_thck, cell_ds, col_ds, col_h;  // L1L2 only (cell_thck: DIVA too)
+  std::vector<double> flwafact_layers;  // shallow-shelf: [ncells][nz_out-1], for the element stresses
   // DIVA only: starting point viscosities [ncells][4][nl], mean velocity
   // and traction [ncols], the columns' ice-plus-land bits, and each
   // instance's state arrays (written back with the result)
@@ -107,6 +108,15 @@ void scatter_vector(const HostPlan& p, int b, const double2* v, double* vu,
 void halo_stag(int nx, int ny, int nlead, int periodic, double* a);
 // parallel_halo for an (nx, ny) cell field (parallel_slap.F90:1790-1860).
 void halo_cells(int nx, int ny, int periodic, double* a);
+
+// Elements of the post-solve diagnostics: cells x (nz_out - 1) layers (the
+// 3-D elements of any solve, 2-D ones included).
+inline int diagnostic_elements(const HostPlan& p) { return p.ncells * (p.nz_out - 1); }
+// The device view of the post-solve diagnostics of a 2-D solve: the 3-D
+// elements over the nz_out levels, the 3-D velocity x3 [ncols][nz_out]
+// and, for the shallow-shelf solve, the per-layer flow factor
+// (flwafact_layers on the device); a 3-D solve's view is returned as is.
+DevView diagnostics_view(const DevView& v, const HostPlan& p, double2* x3, const double* flwafact_layers);
 
 // Post-solve diagnostics of instance b to the reference layout: nv element
 // fields vals[v][nelem] -> out[v] (nz-1,nx,ny), zero outside active cells

@@ -555,6 +555,24 @@ int orc_internal_stress(int nx, int ny, int nz, int nhalo, const double *sigma,
                         const double *vvel, double *tau_xz, double *tau_yz,
                         double *tau_xx, double *tau_yy, double *tau_xy,
                         double *tau_eff) {
+  return orc_internal_stress_approx(nx, ny, nz, nhalo, sigma, active_cell, xVertex, yVertex,
+                                    stagusrf, stagthck, flwafact, NULL, whichefvs, efvs_constant,
+                                    ORC_APPROX_BP, uvel, vvel, tau_xz, tau_yz, tau_xx, tau_yy,
+                                    tau_xy, tau_eff);
+}
+
+/* compute_internal_stress for approximation approx (:7100-7147): the SSA
+ * takes the horizontal gradients only and its viscosity branch
+ * (:7325-7338); L1L2 takes the element's layer viscosity efvs(k,i,j) at
+ * every point; Blatter-Pattyn and DIVA the 3-D gradients and viscosity. */
+int orc_internal_stress_approx(int nx, int ny, int nz, int nhalo, const double *sigma,
+                               const int *active_cell, const double *xVertex,
+                               const double *yVertex, const double *stagusrf,
+                               const double *stagthck, const double *flwafact,
+                               const double *efvs, int whichefvs, double efvs_constant,
+                               int approx, const double *uvel, const double *vvel,
+                               double *tau_xz, double *tau_yz, double *tau_xx, double *tau_yy,
+                               double *tau_xy, double *tau_eff) {
   init_tables();
   const size_t ne = (size_t)(nz - 1) * nx * ny;
   memset(tau_xz, 0, ne * sizeof(double));
@@ -590,8 +608,22 @@ int orc_internal_stress(int nx, int ny, int nz, int nhalo, const double *sigma,
             dv_dy = dv_dy + ddy[n] * v[n];
             dv_dz = dv_dz + ddz[n] * v[n];
           }
-          const double efvs_qp = effective_viscosity(whichefvs, efvs_constant, ddx, ddy, ddz,
-                                                     u, v, flwafact[e]);
+          double efvs_qp;
+          if (approx == ORC_APPROX_SSA) {
+            du_dz = 0.0;
+            dv_dz = 0.0;
+            if (whichefvs == ORC_EFVS_NONLINEAR) {
+              const double sq = 1.0e-8 * 1.0e-8 + (du_dx * du_dx + dv_dy * dv_dy + du_dx * dv_dy +
+                                                   0.25 * ((dv_dx + du_dy) * (dv_dx + du_dy)));
+              efvs_qp = flwafact[e] * pow(sq, ((1.0 - 3.0) / 3.0) / 2.0);
+            } else {
+              efvs_qp = effective_viscosity(whichefvs, efvs_constant, ddx, ddy, ddz, u, v, flwafact[e]);
+            }
+          } else if (approx == ORC_APPROX_L1L2) {
+            efvs_qp = efvs[e];
+          } else {
+            efvs_qp = effective_viscosity(whichefvs, efvs_constant, ddx, ddy, ddz, u, v, flwafact[e]);
+          }
           tau_xz[e] = tau_xz[e] + efvs_qp * du_dz;
           tau_yz[e] = tau_yz[e] + efvs_qp * dv_dz;
           tau_xx[e] = tau_xx[e] + 2.0 * efvs_qp * du_dx;

@@ -39,7 +39,7 @@ enum {
   ORC_GRADIENT_MARGIN_MARINE = 2,
   ORC_ASSEMBLE_STANDARD = 0, ORC_ASSEMBLE_LOCAL = 1,
   ORC_GROUND_NO_GLP = 0, ORC_GROUND_ALL = 2,
-  ORC_APPROX_SSA = 1, ORC_APPROX_L1L2 = 3, ORC_APPROX_DIVA = 4
+  ORC_APPROX_SSA = 1, ORC_APPROX_BP = 2, ORC_APPROX_L1L2 = 3, ORC_APPROX_DIVA = 4
 };
 
 /* Status codes shared with the product's C ABI. */
@@ -174,6 +174,14 @@ int orc_internal_stress(int nx, int ny, int nz, int nhalo, const double *sigma,
                         const double *vvel, double *tau_xz, double *tau_yz,
                         double *tau_xx, double *tau_yy, double *tau_xy,
                         double *tau_eff);
+int orc_internal_stress_approx(int nx, int ny, int nz, int nhalo, const double *sigma,
+                               const int *active_cell, const double *xVertex,
+                               const double *yVertex, const double *stagusrf,
+                               const double *stagthck, const double *flwafact,
+                               const double *efvs, int whichefvs, double efvs_constant,
+                               int approx, const double *uvel, const double *vvel,
+                               double *tau_xz, double *tau_yz, double *tau_xx, double *tau_yy,
+                               double *tau_xy, double *tau_eff);
 void orc_basal_friction_heatflx(int nx, int ny, int nz, int nhalo, int periodic,
                                 const int *active_cell, const int *active_vertex,
                                 const double *uvel, const double *vvel,

@@ -264,17 +264,20 @@ def assemble_system(m, su, uvel, vvel):
     return A, bu, bv, efvs, nnz.value
 
 
-def internal_stress(m, su, uvel, vvel):
-    """compute_internal_stress at velocity (uvel, vvel): dict of the six
-    stresses, each (ny, nx, nz-1)."""
+def internal_stress(m, su, uvel, vvel, approx=2, efvs=None):
+    """compute_internal_stress at velocity (uvel, vvel) for approximation
+    approx (2 Blatter-Pattyn; APPROX_SSA, APPROX_L1L2 with the layer
+    viscosities efvs, 4 DIVA): dict of the six stresses, each (ny, nx, nz-1)."""
     nx, ny, nz = m.nx, m.ny, m.nz
     names = ("tau_xz", "tau_yz", "tau_xx", "tau_yy", "tau_xy", "tau_eff")
     outs = {k: np.zeros((ny, nx, nz - 1)) for k in names}
-    fn = lib().orc_internal_stress
-    fn.argtypes = [C.c_int] * 4 + [_dp, _ip, _dp, _dp, _dp, _dp, _dp, C.c_int, C.c_double, _dp, _dp] + [_dp] * 6
+    fn = lib().orc_internal_stress_approx
+    fn.argtypes = ([C.c_int] * 4 + [_dp, _ip, _dp, _dp, _dp, _dp, _dp, _dp, C.c_int, C.c_double, C.c_int,
+                                    _dp, _dp] + [_dp] * 6)
+    ef = np.zeros((ny, nx, nz - 1)) if efvs is None else np.ascontiguousarray(efvs, np.float64)
     rc = fn(nx, ny, nz, 2, _p(su["sigma"]), _p(su["active_cell"], _ip), _p(su["xVertex"]), _p(su["yVertex"]),
-            _p(su["stagusrf"]), _p(su["stagthck"]), _p(su["flwafact"]), m.which_efvs, m.efvs_constant,
-            _p(np.ascontiguousarray(uvel, np.float64)), _p(np.ascontiguousarray(vvel, np.float64)),
+            _p(su["stagusrf"]), _p(su["stagthck"]), _p(su["flwafact"]), _p(ef), m.which_efvs, m.efvs_constant,
+            approx, _p(np.ascontiguousarray(uvel, np.float64)), _p(np.ascontiguousarray(vvel, np.float64)),
             *[_p(outs[k]) for k in names])
     if rc != 0:
         raise RuntimeError(f"orc_internal_stress failed: {rc}")

@@ -247,10 +247,32 @@ extern "C" int emu_slide_beta(const bp_inputs* in, const double* uvel, const dou
 // element stresses (nz-1,nx,ny) and bfricflx (nx,ny) by method which.
 // beta (nx-1,ny-1), when given, replaces the plan's betas: each column
 // takes its vertex's value, each cell corner its column's (0 without one).
+static int diagnostics(const bp_inputs* in, const double* uvel, const double* vvel, const double* efvs,
+                       const double* beta, int which, double* tau_xz, double* tau_yz, double* tau_xx,
+                       double* tau_yy, double* tau_xy, double* tau_eff, double* bfricflx);
+
 extern "C" int emu_diagnostics(const bp_inputs* in, const double* uvel, const double* vvel,
                                const double* beta, int which, double* tau_xz, double* tau_yz,
                                double* tau_xx, double* tau_yy, double* tau_xy, double* tau_eff,
                                double* bfricflx) {
+  return diagnostics(in, uvel, vvel, nullptr, beta, which, tau_xz, tau_yz, tau_xx, tau_yy, tau_xy, tau_eff,
+                     bfricflx);
+}
+
+// The same for a 2-D solve (shallow-shelf, L1L2, DIVA): the 3-D elements
+// over the model's levels with the 3-D velocity (uvel, vvel) through the
+// engine's diagnostics view; efvs (nz-1,nx,ny) is the L1L2 layer viscosity.
+extern "C" int emu_diagnostics_2d(const bp_inputs* in, const double* uvel, const double* vvel,
+                                  const double* efvs, int which, double* tau_xz, double* tau_yz,
+                                  double* tau_xx, double* tau_yy, double* tau_xy, double* tau_eff,
+                                  double* bfricflx) {
+  return diagnostics(in, uvel, vvel, efvs, nullptr, which, tau_xz, tau_yz, tau_xx, tau_yy, tau_xy, tau_eff,
+                     bfricflx);
+}
+
+static int diagnostics(const bp_inputs* in, const double* uvel, const double* vvel, const double* efvs,
+                       const double* beta, int which, double* tau_xz, double* tau_yz, double* tau_xx,
+                       double* tau_yy, double* tau_xy, double* tau_eff, double* bfricflx) {
   Emu E;
   std::string err;
   if (!build_plan(in, 1, &E.p, &err)) return 10;
@@ -266,17 +288,28 @@ extern "C" int emu_diagnostics(const bp_inputs* in, const double* uvel, const do
   }
   E.bind();
   gather_velocity(E.p, 0, uvel, vvel, E.x.data());
+  // a 2-D solve: its 3-D velocity and, for L1L2, its layer viscosities
+  std::vector<double2> x3(E.p.solve2d ? (size_t)std::max(NC, 1) * E.p.nz_out : 0);
+  if (E.p.solve2d) gather_velocity_3d(E.p, 0, uvel, vvel, x3.data());
+  if (E.p.l1l2 && efvs) {
+    const int nl = E.v.nl;
+    for (int c = 0; c < NCELL; ++c) {
+      const size_t cc = (size_t)(E.p.cell_ij[NCELL + c] - 1) * nx + (E.p.cell_ij[c] - 1);
+      for (int k = 0; k < nl; ++k) E.efvs[(size_t)c * nl + k] = efvs[cc * nl + k];
+    }
+  }
+  const DevView v = diagnostics_view(E.v, E.p, x3.data(), E.p.flwafact_layers.data());
   RefTables T;
   fill_ref_tables(&T);
-  const size_t ne = (size_t)E.p.nelem;
+  const size_t ne = (size_t)diagnostic_elements(E.p);
   std::vector<double> tau(6 * ne), bf((size_t)std::max(NCELL, NC));
-  for (int e = 0; e < E.p.nelem; ++e) {
+  for (size_t e = 0; e < ne; ++e) {
     double t[6];
-    if (!stress_element(E.v, T, e, t)) return 2;
+    if (!stress_element(v, T, (int)e, t)) return 2;
     for (int q = 0; q < 6; ++q) tau[(size_t)q * ne + e] = t[q];
   }
   const int n = which == 0 ? NCELL : NC;
-  for (int i = 0; i < n; ++i) bf[i] = which == 0 ? bfric_cell(E.v, T, i) : bfric_vertex(E.v, i);
+  for (int i = 0; i < n; ++i) bf[i] = which == 0 ? bfric_cell(v, T, i) : bfric_vertex(v, i);
   double* outs[6] = {tau_xz, tau_yz, tau_xx, tau_yy, tau_xy, tau_eff};
   scatter_elements(E.p, 0, tau.data(), 6, outs);
   scatter_bfric(E.p, 0, which, bf.data(), bfricflx);

@@ -6,8 +6,9 @@ CPU: the device's per-element and per-cell/column bodies with the
 engine's scatters (compiled for the CPU by tests/hostemu) against the
 oracle's restatement at random halo-consistent velocities, relative 1e-12
 (the bodies form the basis-function derivatives with fused multiply-adds,
-the restatement without).  GPU: bp_problem_diagnostics at a converged
-solution against the oracle at that solution, relative 1e-10.
+the restatement without), for the 3-D solve and for the 3-D elements of
+the 2-D solves (shallow-shelf, L1L2, DIVA).  GPU: bp_problem_diagnostics at
+a converged solution against the oracle at that solution, relative 1e-10.
 """
 import ctypes as C
 import os
@@ -114,6 +115,53 @@ def test_stress_of_a_uniform_shear_is_exact():
         assert np.max(np.abs(ref[k])) <= 1e-12 * m.efvs_constant * a
 
 
+def _models_2d():
+    out = []
+    for approx, name in ((configs.APPROX_SSA, "ssa"), (configs.APPROX_L1L2, "l1l2"),
+                         (configs.APPROX_DIVA, "diva")):
+        m = MODELS[0].copy(approx_2d=approx)
+        m.name = f"dome_sliding_{name}"
+        out.append(m)
+        m = configs.marine(n=32, dx=4000.0).copy(periodic=0, approx_2d=approx,
+                                                 which_assemble_beta=configs.ASSEMBLE_STANDARD)
+        m.name = f"marine_outflow_{name}"
+        out.append(m)
+    return out
+
+
+@pytest.mark.parametrize("which", [0, 1])
+@pytest.mark.parametrize("m", _models_2d(), ids=lambda m: m.name)
+def test_diagnostic_bodies_of_2d_solves_match_oracle(m, which):
+    """compute_internal_stress's shallow-shelf branch (horizontal gradients
+    and viscosity only), its L1L2 branch (the layer viscosity efvs(k,i,j)
+    at every point) and the 3-D branch for DIVA, on the 3-D elements of a
+    2-D solve through the engine's diagnostics view, against the oracle at
+    a random 3-D velocity; the heat flux from its basal level."""
+    emu = C.CDLL(EMU)
+    prep, _, _ = solver.prepare(m)
+    su = oracle.setup(m)
+    u, v = random_state(m, su, seed=6, scale=50.0)
+    rng = np.random.default_rng(7)
+    efvs = rng.uniform(1e5, 1e7, (m.ny, m.nx, m.nz - 1))
+    for k in range(m.nz - 1):
+        efvs[..., k] = configs.halo_fill_cells(np.ascontiguousarray(efvs[..., k]), m.periodic)
+    tau = {k: np.full((m.ny, m.nx, m.nz - 1), np.nan) for k in NAMES}
+    bf = np.full((m.ny, m.nx), np.nan)
+    rc = emu.emu_diagnostics_2d(C.byref(prep.inputs), _p(np.ascontiguousarray(u)), _p(np.ascontiguousarray(v)),
+                                _p(efvs), which, *[_p(tau[k]) for k in NAMES], _p(bf))
+    assert rc == 0
+    ref = oracle.internal_stress(m, su, u, v, approx=m.approx_2d, efvs=efvs)
+    for k in NAMES:
+        assert np.all(np.isfinite(tau[k])), k
+        assert _close(tau[k], ref[k], 1e-12), k
+    if m.approx_2d == configs.APPROX_SSA:
+        assert not ref["tau_xz"].any() and not ref["tau_yz"].any()
+    else:
+        assert np.max(np.abs(ref["tau_xz"])) > 0.0
+    rbf = oracle.basal_friction_heatflx(m, su, u, v, su["beta_internal"], which)
+    assert _close(bf, rbf, 1e-12)
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("which", [0, 1])
 def test_device_diagnostics_at_solution_match_oracle(ctx, which):
@@ -133,3 +181,27 @@ def test_device_diagnostics_at_solution_match_oracle(ctx, which):
             assert _close(d[k], ref[k], 1e-10), k
         rbf = oracle.basal_friction_heatflx(m, su, us[0], vs[0], su["beta_internal"], which)
         assert _close(d["bfricflx"], rbf, 1e-10)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("m", _models_2d()[::2], ids=lambda m: m.name)
+def test_device_diagnostics_of_2d_solves_match_oracle(ctx, m):
+    """bp_problem_diagnostics after a shallow-shelf, L1L2 or DIVA solve: the
+    3-D elements with the solve's 3-D velocity (and L1L2's layer
+    viscosities) against the oracle at that solution, relative 1e-10."""
+    m = m.copy(pcg_maxiters=3000)
+    prep, u0, v0 = solver.prepare(m)
+    prob = ctx.problem([prep])
+    prob.set_guess([u0], [v0])
+    st = prob.run()[0]
+    assert st["status"] == 0, st
+    us, vs, es = prob.get(want_efvs=True)
+    su = oracle.setup(m)
+    for which in (0, 1):
+        d = prob.diagnostics(which)[0]
+        ref = oracle.internal_stress(m, su, us[0], vs[0], approx=m.approx_2d, efvs=es[0])
+        for k in NAMES:
+            assert _close(d[k], ref[k], 1e-10), k
+        rbf = oracle.basal_friction_heatflx(m, su, us[0], vs[0], su["beta_internal"], which)
+        assert _close(d["bfricflx"], rbf, 1e-10)
+    prob.close()
