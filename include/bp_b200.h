@@ -282,14 +282,17 @@ int bp_problem_destroy(bp_problem *p);
 /* Post-solve diagnostics of glissade_velo_higher_solve (:3847-3872),
  * computed on the device at the solution of the last bp_problem_run, per
  * instance (arrays of n pointers; any may be NULL):
- *  - compute_internal_stress (:6968-7195), 3-D higher-order branch: the
- *    stresses tau_xz, tau_yz, tau_xx, tau_yy, tau_xy and tau_eff (Pa) at
- *    element centres, (nz-1,nx,ny), zero outside active cells;
+ *  - compute_internal_stress (:6968-7195): the stresses tau_xz, tau_yz,
+ *    tau_xx, tau_yy, tau_xy and tau_eff (Pa) at element centres,
+ *    (nz-1,nx,ny), zero outside active cells, from the 3-D velocity; the
+ *    branch of the solve's approximation (:7100-7147: shallow-shelf
+ *    horizontal gradients and viscosity, L1L2 the layer viscosity, else
+ *    the 3-D ones);
  *  - compute_basal_friction_heatflx (:6755-6964): bfricflx (W/m^2) at cell
  *    centres (nx,ny), by the finite-element face quadrature
  *    (which_bfric = 0) or at vertices unstaggered to cells (1, the
- *    reference's default which_ho_assemble_bfric), with the beta of the
- *    last Picard iteration. */
+ *    reference's default which_ho_assemble_bfric), with the beta_internal
+ *    of the last Picard iteration and the 3-D basal velocity. */
 int bp_problem_diagnostics(bp_problem *p, int which_bfric, double *const *tau_xz,
                            double *const *tau_yz, double *const *tau_xx,
                            double *const *tau_yy, double *const *tau_xy,
