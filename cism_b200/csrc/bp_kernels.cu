@@ -256,6 +256,9 @@ __global__ void __launch_bounds__(256) k_asm_qp(DevView v) {
 
 // Pass 1 of the shallow-shelf assembly: one thread per (active cell, 2-D
 // point), the cell's viscosity the mean of its 4 points (:5539-5545).
+// LAYERS: the L1L2 and DIVA solves, with a viscosity per layer (kept in
+// a per-thread array the shallow-shelf instance does without).
+template <bool LAYERS>
 __global__ void __launch_bounds__(256) k_asm2_qp(DevView v) {
   const long gtid = (long)blockIdx.x * blockDim.x + threadIdx.x;
   const int c = (int)(gtid >> 2), p = (int)(gtid & 3);
@@ -267,8 +270,8 @@ __global__ void __launch_bounds__(256) k_asm2_qp(DevView v) {
   }
   const unsigned mask = __ballot_sync(0xffffffffu, valid);
   if (!valid) return;
-  double out[5], eq = 0.0, ek[kNzMax - 1];
-  const bool ok = qp2_element_point(v, c_T, c, p, out, &eq, ek);
+  double out[5], eq = 0.0, ek[LAYERS ? kNzMax - 1 : 1];
+  const bool ok = qp2_element_point(v, c_T, c, p, out, &eq, LAYERS ? ek : nullptr);
   if (!ok) {
     atomicExch(&v.st[inst].status, BP_ERR_SINGULAR_JAC);
     eq = 0.0;
@@ -277,7 +280,7 @@ __global__ void __launch_bounds__(256) k_asm2_qp(DevView v) {
   double* dst = v.qp + ((size_t)c * 8 + p) * 10;
   for (int i = 0; i < 5; ++i) dst[i] = out[i];
   const int lane0 = (threadIdx.x & 31) & ~3;
-  if (v.l1l2 || v.diva) {  // efvs(k) = the mean of the layer's point values (:5565-5572)
+  if (LAYERS) {  // efvs(k) = the mean of the layer's point values (:5565-5572)
     for (int k = 0; k < v.nl; ++k) {
       const double e = ok ? ek[k] : 0.0;
       double sum = 0.0;
@@ -1023,7 +1026,8 @@ void launch_asm_qp(const DevView& v, cudaStream_t s) {
   if (v.solve2d) {
     if (v.ncells > 0) {
       const long threads = (long)v.ncells * 4;
-      k_asm2_qp<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(v);
+      if (v.l1l2 || v.diva) k_asm2_qp<true><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(v);
+      else k_asm2_qp<false><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(v);
     }
   } else if (v.nelem > 0) {
     const long threads = (long)v.nelem * 8;
