@@ -496,6 +496,20 @@ extern "C" int emu_diva_step(const bp_inputs* in, double* Auu, double* Auv, doub
   return 0;
 }
 
+// sizeof of a C ABI struct by name (0 for an unknown name), for the
+// binding's layout test.
+extern "C" long emu_sizeof(const char* name) {
+  const std::string n(name);
+  if (n == "bp_inputs") return (long)sizeof(bp_inputs);
+  if (n == "bp_stats") return (long)sizeof(bp_stats);
+  if (n == "bp_model") return (long)sizeof(bp_model);
+  if (n == "bp_setup_arrays") return (long)sizeof(bp_setup_arrays);
+  if (n == "bp_sliding") return (long)sizeof(bp_sliding);
+  if (n == "bp_l1l2") return (long)sizeof(bp_l1l2);
+  if (n == "bp_diva") return (long)sizeof(bp_diva);
+  return 0;
+}
+
 // gather_velocity then scatter_velocity through the host plan of one
 // solve (the path of an initial guess into the device vector and of the
 // solution back out).  10 if the plan rejects the inputs.

@@ -273,9 +273,16 @@ def _c_struct_fields(hdr, name):
 
 @pytest.mark.parametrize("cname,pystruct", [("bp_inputs", solver.Inputs), ("bp_stats", solver.Stats),
                                             ("bp_model", solver.Model), ("bp_setup_arrays", solver.SetupArrays),
-                                            ("bp_sliding", solver.Sliding)])
+                                            ("bp_sliding", solver.Sliding), ("bp_l1l2", solver.L1L2),
+                                            ("bp_diva", solver.Diva)])
 def test_ctypes_structs_follow_the_header(cname, pystruct):
     """The Python binding's structs list the C ABI structs' fields in the
     header's order (a drift would shift every later field)."""
     hdr = open(os.path.join(ROOT, "include", "bp_b200.h")).read()
     assert _c_struct_fields(hdr, cname) == [n for n, _ in pystruct._fields_]
+    # and the same size as the C compiler lays it out (a field of the wrong
+    # type would shift the ones after it)
+    emu = C.CDLL(os.path.join(ROOT, "tests", "hostemu", "libhostemu.so"))
+    emu.emu_sizeof.restype = C.c_long
+    emu.emu_sizeof.argtypes = [C.c_char_p]
+    assert emu.emu_sizeof(cname.encode()) == C.sizeof(pystruct)
