@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "bp_body.h"
+#include "bp_oracle.h"
 #include "bp_plan.h"
 
 using namespace bp;
@@ -493,6 +494,152 @@ extern "C" int emu_diva_step(const bp_inputs* in, double* Auu, double* Auv, doub
   for (int col = 0; col < NC; ++col) diva_column_velocity(E.v, col);
   scatter_velocity_3d(E.p, 0, E.x3.data(), uout, vout);
   scatter_diva(E.p, 0, E.x.data(), E.bt.data());
+  return 0;
+}
+
+// The whole Picard loop of a 2-D solve (shallow-shelf, L1L2, DIVA) through
+// the device bodies in the engine's launch order (run_picard: the sliding
+// law, assembly pass 1, DIVA's omega and beta_eff, the rows and b, the
+// linear solve, DIVA's traction and 3-D velocity, the Picard criterion;
+// the L1L2 reconstruction after the loop), with the oracle's PCG standing
+// in for the device's on the reference layout.  Outputs as bp_solve (the
+// 3-D velocity, efvs; DIVA's state written back) and the Picard count.
+// which_resid 0-2 only.  10 if the plan rejects the inputs or they are not
+// a 2-D problem.
+extern "C" int emu_picard_2d(const bp_inputs* in, const double* uvel, const double* vvel, double* uout,
+                             double* vout, double* efvs, int* picard_iters) {
+  Emu E;
+  std::string err;
+  if (!build_plan(in, 1, &E.p, &err) || !E.p.solve2d || in->which_resid > 2) return 10;
+  E.bind();
+  const DevView& v = E.v;
+  const HostPlan& P = E.p;
+  const InstParams& ip = P.inst[0];
+  const int nx = in->nx, ny = in->ny, NC = P.ncols, NCELL = P.ncells, nl = v.nl;
+  const size_t nvert = (size_t)(nx - 1) * (ny - 1), np = P.npad;
+  gather_velocity(P, 0, uvel, vvel, E.x.data());
+  if (P.diva) gather_velocity_3d(P, 0, uvel, vvel, E.x3.data());
+  RefTables T;
+  fill_ref_tables(&T);
+  std::vector<double2> usav(E.x);
+  std::vector<double> Auu(27 * nvert), Auv(27 * nvert), Avu(27 * nvert), Avv(27 * nvert);
+  std::vector<double> bu(nvert), bv(nvert), xu(nvert), xv(nvert);
+  int it = 0;
+  for (it = 1; it <= ip.maxiter_nonlinear; ++it) {
+    usav = E.x;
+    if (ip.slide.law != 0) {  // k_slide_beta, k_cell_beta
+      for (int col = 0; col < NC; ++col) {
+        const double2 ub = P.diva ? E.x3[(size_t)col * (nl + 1) + nl] : E.x[col];
+        E.p.col_beta[col] = slide_beta(ip.slide, P.col_slide[col], P.col_slide[(size_t)NC + col],
+                                       P.col_slide[2 * (size_t)NC + col], ub.x, ub.y);
+        if (!(E.p.col_beta[col] >= 0.0)) return 9;
+      }
+      for (int c = 0; c < NCELL; ++c)
+        for (int q = 0; q < 4; ++q) {
+          const int col = P.cell_cols[(size_t)q * NCELL + c];
+          E.p.cell_beta[(size_t)q * NCELL + c] = col >= 0 ? P.col_beta[col] : 0.0;
+        }
+    }
+    for (int c = 0; c < NCELL; ++c) {  // k_asm2_qp
+      double s = 0.0, sk[kNzMax] = {0.0};
+      for (int p = 0; p < 4; ++p) {
+        double out[5], eq = 0.0, ek[kNzMax];
+        if (!qp2_element_point(v, T, c, p, out, &eq, ek)) return 2;
+        std::memcpy(&E.qp[((size_t)c * 8 + p) * 10], out, sizeof(out));
+        s += eq;
+        if (P.l1l2 || P.diva)
+          for (int k = 0; k < nl; ++k) sk[k] += ek[k];
+      }
+      if (P.l1l2 || P.diva)
+        for (int k = 0; k < nl; ++k) E.efvs[(size_t)c * nl + k] = sk[k] / 4.0;
+      else
+        E.efvs[c] = s / 4.0;
+    }
+    if (P.diva) {  // k_diva_cells, k_diva_beta, k_diva_cell_beta
+      for (int c = 0; c < NCELL; ++c) diva_cell_integrals(v, c);
+      for (int col = 0; col < NC; ++col) diva_column_beta(v, col);
+      for (int c = 0; c < NCELL; ++c)
+        for (int q = 0; q < 4; ++q) {
+          const int col = P.cell_cols[(size_t)q * NCELL + c];
+          E.p.cell_beta[(size_t)q * NCELL + c] = col >= 0 ? E.beff[col] : 0.0;
+        }
+    }
+    double* Ad = reinterpret_cast<double*>(E.A.data());  // k_asm_rows<true>
+    for (int B = 0; B < 4; ++B)
+      for (int n = 0; n < v.nnodes; ++n) {
+        double acc[27];
+        double adj = 0.0;
+        switch (B) {
+          case 0: row_assemble2<0>(v, T, n, acc); row_basal<0>(v, T, n, 0, acc); adj = row_dirichlet<0>(v, n, 0, acc); break;
+          case 1: row_assemble2<1>(v, T, n, acc); row_basal<1>(v, T, n, 0, acc); adj = row_dirichlet<1>(v, n, 0, acc); break;
+          case 2: row_assemble2<2>(v, T, n, acc); row_basal<2>(v, T, n, 0, acc); adj = row_dirichlet<2>(v, n, 0, acc); break;
+          default: row_assemble2<3>(v, T, n, acc); row_basal<3>(v, T, n, 0, acc); adj = row_dirichlet<3>(v, n, 0, acc); break;
+        }
+        for (int m = 0; m < 27; ++m) Ad[(((size_t)((B >> 1) * 27 + m)) * np + n) * 2 + (B & 1)] = acc[m];
+        E.badj[(size_t)B * np + n] = adj;
+      }
+    for (int n = 0; n < v.nnodes; ++n) {  // k_rhs
+      const uint8_t dm = P.dmask[n];
+      double u = P.load[n].x - E.badj[n] - E.badj[np + n];
+      double w = P.load[n].y - E.badj[2 * np + n] - E.badj[3 * np + n];
+      if (dm & 1) u = E.x[n].x;
+      if (dm & 2) w = E.x[n].y;
+      E.b[n] = double2{u, w};
+    }
+    if (!P.diva && ip.which_babc == 6) {  // a frozen bed: nothing is solved
+      for (int n = 0; n < v.nnodes; ++n) E.x[n] = double2{0.0, 0.0};
+    } else {  // the linear solve on the reference layout
+      scatter_matrix(P, E.A.data(), Auu.data(), Auv.data(), Avu.data(), Avv.data());
+      for (double* a : {Auu.data(), Auv.data(), Avu.data(), Avv.data()}) halo_stag(nx, ny, 27, P.periodic[0], a);
+      std::fill(bu.begin(), bu.end(), 0.0);
+      std::fill(bv.begin(), bv.end(), 0.0);
+      std::fill(xu.begin(), xu.end(), 0.0);
+      std::fill(xv.begin(), xv.end(), 0.0);
+      scatter_vector(P, 0, E.b.data(), bu.data(), bv.data());
+      scatter_vector(P, 0, E.x.data(), xu.data(), xv.data());
+      for (double* a : {bu.data(), bv.data(), xu.data(), xv.data()}) halo_stag(nx, ny, 1, P.periodic[0], a);
+      std::vector<int> av(in->active_vertex, in->active_vertex + nvert);
+      double perr = 0.0;
+      int nit = 0;
+      const int st = ip.variant == 3
+          ? orc_pcg_chrongear_3d(nx, ny, 1, P.periodic[0], av.data(), Auu.data(), Auv.data(), Avu.data(),
+                                 Avv.data(), bu.data(), bv.data(), xu.data(), xv.data(), ip.precond,
+                                 ip.pcg_maxiters, ip.pcg_tol, ip.ncheck, &perr, &nit)
+          : orc_pcg_standard_3d(nx, ny, 1, P.periodic[0], av.data(), Auu.data(), Auv.data(), Avu.data(),
+                                Avv.data(), bu.data(), bv.data(), xu.data(), xv.data(), ip.precond,
+                                ip.pcg_maxiters, ip.pcg_tol, ip.ncheck, &perr, &nit);
+      if (st == ORC_ERR_NAN) return 1;
+      for (int col = 0; col < NC; ++col) {
+        const size_t w = (size_t)(P.col_ij[NC + col] - 1) * (nx - 1) + (P.col_ij[col] - 1);
+        E.x[col] = double2{xu[w], xv[w]};
+      }
+    }
+    if (P.diva)  // k_diva_velocity
+      for (int col = 0; col < NC; ++col) diva_column_velocity(v, col);
+    double r = 0.0, rsum = 0.0;  // k_picard_check (2-D: no bed layer to leave out)
+    long cnt = 0;
+    for (int n = 0; n < v.nnodes; ++n) {
+      const double speed = std::sqrt(E.x[n].x * E.x[n].x + E.x[n].y * E.x[n].y);
+      if (speed != 0.0) {
+        const double old = std::sqrt(usav[n].x * usav[n].x + usav[n].y * usav[n].y);
+        const double d = std::fabs((old - speed) / speed);
+        r = std::max(r, d);
+        rsum += d;
+        ++cnt;
+      }
+    }
+    const double crit = ip.which_resid == 2 ? (cnt > 0 ? rsum / cnt : 0.0) : r;
+    if (!(crit >= 1.0e-4)) break;
+  }
+  *picard_iters = std::min(it, ip.maxiter_nonlinear);
+  if (P.l1l2) {
+    for (int c = 0; c < NCELL; ++c) l1l2_cell(v, c);
+    for (int col = 0; col < NC; ++col) l1l2_column(v, col);
+  }
+  if (P.l1l2 || P.diva) scatter_velocity_3d(P, 0, E.x3.data(), uout, vout);
+  else scatter_velocity(P, 0, E.x.data(), uout, vout);
+  if (P.diva) scatter_diva(P, 0, E.x.data(), E.bt.data());
+  scatter_efvs(P, 0, E.efvs.data(), efvs);
   return 0;
 }
 

@@ -202,3 +202,22 @@ def test_ssa_plan_takes_the_bed_velocity_and_fills_every_level():
     for a, b in ((uo, u), (vo, v)):
         assert np.array_equal(a[cols], np.repeat(b[cols][:, -1:], m.nz, axis=1))
         assert np.array_equal(a, oracle.halo_stag(a, m.periodic))
+
+
+@pytest.mark.parametrize("m", _ssa_models(), ids=lambda m: m.name)
+def test_emulated_ssa_picard_loop_matches_oracle(m):
+    """The device's shallow-shelf steps in the engine's order (the oracle's
+    PCG as the linear solver) against the oracle's solve: the same Picard
+    count and velocity to 1e-9."""
+    from helpers import rel_l2
+    from test_velocity_l1l2 import emulated_picard
+
+    m = m.copy(pcg_maxiters=3000)
+    u, v, ef, it, _ = emulated_picard(m)
+    uo, vo, eo, _, sto = oracle.velo_ssa_solve(m)
+    assert sto["status"] == 0 and it == sto["picard_iters"]
+    assert rel_l2([u, v], [uo, vo]) < 1e-9
+    # 1e-6 as on the GPU: where the flow is nearly plug flow the strain rate
+    # is a small difference of large speeds, so velocities equal to 1e-9
+    # give viscosities equal to about 1e-8 there
+    assert np.abs(ef - eo).max() <= 1e-6 * np.abs(eo).max()

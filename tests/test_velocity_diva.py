@@ -277,3 +277,43 @@ def test_device_diva_uniform_slab_profile(ctx):
     e = tb / beta + tb * _omega_k(s, H, lambda k, d: eta)
     js, is_ = m.owned_vertex_slices()
     assert np.abs(u[js, is_, :] - e).max() <= 1e-10 * e.max()
+
+
+@pytest.mark.parametrize("m", _diva_models(), ids=lambda m: m.name)
+def test_emulated_diva_picard_loop_matches_oracle(m):
+    """The composition of the device's DIVA steps (the point viscosities
+    carried between iterations, beta_eff before the rows, the traction and
+    3-D velocity after each solve, the sliding law reading the 3-D basal
+    velocity) in the engine's order, the oracle's PCG as the linear solver,
+    against the oracle's solve from the same carried-over state: the same
+    Picard count; the 3-D velocity, mean velocity and traction to 1e-9."""
+    from helpers import rel_l2
+    from test_velocity_l1l2 import emulated_picard
+
+    m = m.copy(pcg_maxiters=3000)
+    su = oracle.setup(m)
+    _, _, st0 = _random_diva_state(m, su, 2)
+    st0 = {k: a * 0.1 for k, a in st0.items()}  # a nearby start, as the last solve's would be
+    m = m.copy(diva_state=st0)
+    u, v, ef, it, prep = emulated_picard(m)
+    uo, vo, eo, _, sto, ex = oracle.velo_diva_solve(m, **st0)
+    assert sto["status"] == 0 and it == sto["picard_iters"]
+    assert rel_l2([u, v], [uo, vo]) < 1e-9
+    A_ = prep.arrays
+    assert rel_l2([A_["uvel_2d"], A_["vvel_2d"]], [ex["uvel_2d"], ex["vvel_2d"]]) < 1e-9
+    assert rel_l2([A_["btractx"], A_["btracty"]], [ex["btractx"], ex["btracty"]]) < 1e-9
+    assert np.abs(ef - eo).max() <= 1e-6 * np.abs(eo).max()
+
+
+def test_emulated_diva_with_a_sliding_law_matches_oracle():
+    """A power-law bed under DIVA: the law reads the 3-D basal velocity of
+    the previous iteration."""
+    from helpers import rel_l2
+    from test_velocity_l1l2 import emulated_picard
+
+    m = configs.with_sliding(configs.slab(n=16), configs.BABC_POWERLAW, seed=3).copy(
+        approx_2d=configs.APPROX_DIVA, pcg_maxiters=3000)
+    u, v, ef, it, prep = emulated_picard(m)
+    uo, vo, eo, _, sto, ex = oracle.velo_diva_solve(m)
+    assert sto["status"] == 0 and it == sto["picard_iters"] and it > 2
+    assert rel_l2([u, v], [uo, vo]) < 1e-9

@@ -250,3 +250,35 @@ def test_device_l1l2_no_slip_bed_is_zero(ctx):
     u, v, _, st = ctx.velo_higher_solve(m)
     assert st["status"] == 0 and st["picard_iters"] == 1
     assert np.all(u == 0.0) and np.all(v == 0.0)
+
+
+def emulated_picard(m, uvel=None, vvel=None):
+    """The 2-D Picard loop through the device bodies in the engine's launch
+    order, the oracle's PCG as its linear solver (tests/hostemu
+    emu_picard_2d): (uvel, vvel, efvs, picard iterations, prepared)."""
+    emu = C.CDLL(EMU)
+    prep, u, v = solver.prepare(m, uvel, vvel)
+    uo, vo = np.ascontiguousarray(u.copy()), np.ascontiguousarray(v.copy())
+    ef = np.zeros((m.ny, m.nx, m.nz - 1))
+    it = C.c_int(0)
+    rc = emu.emu_picard_2d(C.byref(prep.inputs), _p(np.ascontiguousarray(u)), _p(np.ascontiguousarray(v)),
+                           _p(uo), _p(vo), _p(ef), C.byref(it))
+    assert rc == 0
+    return uo, vo, ef, it.value, prep
+
+
+@pytest.mark.parametrize("m", _l1l2_models(), ids=lambda m: m.name)
+def test_emulated_l1l2_picard_loop_matches_oracle(m):
+    """The composition of the device's L1L2 steps (the loop order, the
+    layer viscosities, the reconstruction after the loop) against the
+    oracle's solve: the same Picard count and the 3-D velocity to 1e-9."""
+    from helpers import rel_l2
+
+    m = m.copy(pcg_maxiters=3000)
+    u, v, ef, it, _ = emulated_picard(m)
+    uo, vo, eo, _, sto = oracle.velo_l1l2_solve(m)
+    assert sto["status"] == 0 and it == sto["picard_iters"]
+    assert rel_l2([u, v], [uo, vo]) < 1e-9
+    # 1e-6 as on the GPU: the Cardano switch amplifies last-bit strain-rate
+    # differences up to 1e6 (see the assembly test above)
+    assert np.abs(ef - eo).max() <= 1e-6 * np.abs(eo).max()
