@@ -497,20 +497,20 @@ extern "C" int emu_diva_step(const bp_inputs* in, double* Auu, double* Auv, doub
   return 0;
 }
 
-// The whole Picard loop of a 2-D solve (shallow-shelf, L1L2, DIVA) through
-// the device bodies in the engine's launch order (run_picard: the sliding
+// The whole Picard loop of a solve (3-D, or 2-D: shallow-shelf, L1L2, DIVA)
+// through the device bodies in the engine's launch order (run_picard: the sliding
 // law, assembly pass 1, DIVA's omega and beta_eff, the rows and b, the
 // linear solve, DIVA's traction and 3-D velocity, the Picard criterion;
 // the L1L2 reconstruction after the loop), with the oracle's PCG standing
 // in for the device's on the reference layout.  Outputs as bp_solve (the
 // 3-D velocity, efvs; DIVA's state written back) and the Picard count.
-// which_resid 0-2 only.  10 if the plan rejects the inputs or they are not
-// a 2-D problem.
+// which_resid 0-2 only.  10 if the plan rejects the inputs.
 extern "C" int emu_picard_2d(const bp_inputs* in, const double* uvel, const double* vvel, double* uout,
                              double* vout, double* efvs, int* picard_iters) {
   Emu E;
   std::string err;
-  if (!build_plan(in, 1, &E.p, &err) || !E.p.solve2d || in->which_resid > 2) return 10;
+  if (!build_plan(in, 1, &E.p, &err) || in->which_resid > 2) return 10;
+  const bool d3 = !E.p.solve2d;  // the 3-D Blatter-Pattyn loop (k_asm_qp, k_asm_rows<false>)
   E.bind();
   const DevView& v = E.v;
   const HostPlan& P = E.p;
@@ -522,14 +522,15 @@ extern "C" int emu_picard_2d(const bp_inputs* in, const double* uvel, const doub
   RefTables T;
   fill_ref_tables(&T);
   std::vector<double2> usav(E.x);
-  std::vector<double> Auu(27 * nvert), Auv(27 * nvert), Avu(27 * nvert), Avv(27 * nvert);
-  std::vector<double> bu(nvert), bv(nvert), xu(nvert), xv(nvert);
+  const size_t n3 = nvert * (size_t)v.nz;
+  std::vector<double> Auu(27 * n3), Auv(27 * n3), Avu(27 * n3), Avv(27 * n3);
+  std::vector<double> bu(n3), bv(n3), xu(n3), xv(n3);
   int it = 0;
   for (it = 1; it <= ip.maxiter_nonlinear; ++it) {
     usav = E.x;
     if (ip.slide.law != 0) {  // k_slide_beta, k_cell_beta
       for (int col = 0; col < NC; ++col) {
-        const double2 ub = P.diva ? E.x3[(size_t)col * (nl + 1) + nl] : E.x[col];
+        const double2 ub = P.diva ? E.x3[(size_t)col * (nl + 1) + nl] : E.x[(size_t)col * v.nz + v.nz - 1];
         E.p.col_beta[col] = slide_beta(ip.slide, P.col_slide[col], P.col_slide[(size_t)NC + col],
                                        P.col_slide[2 * (size_t)NC + col], ub.x, ub.y);
         if (!(E.p.col_beta[col] >= 0.0)) return 9;
@@ -540,7 +541,17 @@ extern "C" int emu_picard_2d(const bp_inputs* in, const double* uvel, const doub
           E.p.cell_beta[(size_t)q * NCELL + c] = col >= 0 ? P.col_beta[col] : 0.0;
         }
     }
-    for (int c = 0; c < NCELL; ++c) {  // k_asm2_qp
+    for (int e = 0; d3 && e < P.nelem; ++e) {  // k_asm_qp
+      double s = 0.0;
+      for (int p = 0; p < 8; ++p) {
+        double out[10], eq = 0.0;
+        if (!qp_element_point(v, T, e, p, out, &eq)) return 2;
+        std::memcpy(&E.qp[((size_t)e * 8 + p) * 10], out, sizeof(out));
+        s += eq;
+      }
+      E.efvs[e] = s / 8.0;
+    }
+    for (int c = 0; !d3 && c < NCELL; ++c) {  // k_asm2_qp
       double s = 0.0, sk[kNzMax] = {0.0};
       for (int p = 0; p < 4; ++p) {
         double out[5], eq = 0.0, ek[kNzMax];
@@ -569,11 +580,16 @@ extern "C" int emu_picard_2d(const bp_inputs* in, const double* uvel, const doub
       for (int n = 0; n < v.nnodes; ++n) {
         double acc[27];
         double adj = 0.0;
+        const int col = n / v.nz, k = n - col * v.nz;
         switch (B) {
-          case 0: row_assemble2<0>(v, T, n, acc); row_basal<0>(v, T, n, 0, acc); adj = row_dirichlet<0>(v, n, 0, acc); break;
-          case 1: row_assemble2<1>(v, T, n, acc); row_basal<1>(v, T, n, 0, acc); adj = row_dirichlet<1>(v, n, 0, acc); break;
-          case 2: row_assemble2<2>(v, T, n, acc); row_basal<2>(v, T, n, 0, acc); adj = row_dirichlet<2>(v, n, 0, acc); break;
-          default: row_assemble2<3>(v, T, n, acc); row_basal<3>(v, T, n, 0, acc); adj = row_dirichlet<3>(v, n, 0, acc); break;
+          case 0: if (d3) row_assemble<0>(v, T, col, k, acc); else row_assemble2<0>(v, T, col, acc);
+                  row_basal<0>(v, T, col, k, acc); adj = row_dirichlet<0>(v, col, k, acc); break;
+          case 1: if (d3) row_assemble<1>(v, T, col, k, acc); else row_assemble2<1>(v, T, col, acc);
+                  row_basal<1>(v, T, col, k, acc); adj = row_dirichlet<1>(v, col, k, acc); break;
+          case 2: if (d3) row_assemble<2>(v, T, col, k, acc); else row_assemble2<2>(v, T, col, acc);
+                  row_basal<2>(v, T, col, k, acc); adj = row_dirichlet<2>(v, col, k, acc); break;
+          default: if (d3) row_assemble<3>(v, T, col, k, acc); else row_assemble2<3>(v, T, col, acc);
+                   row_basal<3>(v, T, col, k, acc); adj = row_dirichlet<3>(v, col, k, acc); break;
         }
         for (int m = 0; m < 27; ++m) Ad[(((size_t)((B >> 1) * 27 + m)) * np + n) * 2 + (B & 1)] = acc[m];
         E.badj[(size_t)B * np + n] = adj;
@@ -586,39 +602,42 @@ extern "C" int emu_picard_2d(const bp_inputs* in, const double* uvel, const doub
       if (dm & 2) w = E.x[n].y;
       E.b[n] = double2{u, w};
     }
-    if (!P.diva && ip.which_babc == 6) {  // a frozen bed: nothing is solved
+    if (!d3 && !P.diva && ip.which_babc == 6) {  // a frozen bed: nothing is solved
       for (int n = 0; n < v.nnodes; ++n) E.x[n] = double2{0.0, 0.0};
     } else {  // the linear solve on the reference layout
+      const int nzs = v.nz;
       scatter_matrix(P, E.A.data(), Auu.data(), Auv.data(), Avu.data(), Avv.data());
-      for (double* a : {Auu.data(), Auv.data(), Avu.data(), Avv.data()}) halo_stag(nx, ny, 27, P.periodic[0], a);
+      for (double* a : {Auu.data(), Auv.data(), Avu.data(), Avv.data()}) halo_stag(nx, ny, 27 * nzs, P.periodic[0], a);
       std::fill(bu.begin(), bu.end(), 0.0);
       std::fill(bv.begin(), bv.end(), 0.0);
       std::fill(xu.begin(), xu.end(), 0.0);
       std::fill(xv.begin(), xv.end(), 0.0);
       scatter_vector(P, 0, E.b.data(), bu.data(), bv.data());
       scatter_vector(P, 0, E.x.data(), xu.data(), xv.data());
-      for (double* a : {bu.data(), bv.data(), xu.data(), xv.data()}) halo_stag(nx, ny, 1, P.periodic[0], a);
+      for (double* a : {bu.data(), bv.data(), xu.data(), xv.data()}) halo_stag(nx, ny, nzs, P.periodic[0], a);
       std::vector<int> av(in->active_vertex, in->active_vertex + nvert);
       double perr = 0.0;
       int nit = 0;
       const int st = ip.variant == 3
-          ? orc_pcg_chrongear_3d(nx, ny, 1, P.periodic[0], av.data(), Auu.data(), Auv.data(), Avu.data(),
+          ? orc_pcg_chrongear_3d(nx, ny, nzs, P.periodic[0], av.data(), Auu.data(), Auv.data(), Avu.data(),
                                  Avv.data(), bu.data(), bv.data(), xu.data(), xv.data(), ip.precond,
                                  ip.pcg_maxiters, ip.pcg_tol, ip.ncheck, &perr, &nit)
-          : orc_pcg_standard_3d(nx, ny, 1, P.periodic[0], av.data(), Auu.data(), Auv.data(), Avu.data(),
+          : orc_pcg_standard_3d(nx, ny, nzs, P.periodic[0], av.data(), Auu.data(), Auv.data(), Avu.data(),
                                 Avv.data(), bu.data(), bv.data(), xu.data(), xv.data(), ip.precond,
                                 ip.pcg_maxiters, ip.pcg_tol, ip.ncheck, &perr, &nit);
       if (st == ORC_ERR_NAN) return 1;
       for (int col = 0; col < NC; ++col) {
         const size_t w = (size_t)(P.col_ij[NC + col] - 1) * (nx - 1) + (P.col_ij[col] - 1);
-        E.x[col] = double2{xu[w], xv[w]};
+        for (int k = 0; k < nzs; ++k) E.x[(size_t)col * nzs + k] = double2{xu[w * nzs + k], xv[w * nzs + k]};
       }
     }
     if (P.diva)  // k_diva_velocity
       for (int col = 0; col < NC; ++col) diva_column_velocity(v, col);
     double r = 0.0, rsum = 0.0;  // k_picard_check (2-D: no bed layer to leave out)
     long cnt = 0;
+    const bool nobed = d3 && (ip.which_resid == 1 || ip.which_resid == 2);
     for (int n = 0; n < v.nnodes; ++n) {
+      if (nobed && n % v.nz == v.nz - 1) continue;
       const double speed = std::sqrt(E.x[n].x * E.x[n].x + E.x[n].y * E.x[n].y);
       if (speed != 0.0) {
         const double old = std::sqrt(usav[n].x * usav[n].x + usav[n].y * usav[n].y);

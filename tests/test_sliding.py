@@ -285,3 +285,19 @@ def test_nan_beta_from_sliding_law_is_reported(ctx):
     with pytest.raises(solver.BPError) as e:
         ctx.velo_higher_solve(_nan_beta_model())
     assert e.value.code == 9
+
+
+@pytest.mark.parametrize("law", configs.SLIDING_LAWS)
+def test_emulated_picard_loop_with_a_sliding_law_matches_oracle(law):
+    """The 3-D Picard loop through the device bodies in the engine's order
+    (k_slide_beta from the bed nodes, k_cell_beta, assembly, the rows), the
+    oracle's PCG as the linear solver, against the oracle's solve: the same
+    Picard count and the velocity to 1e-9."""
+    from helpers import rel_l2
+    from test_velocity_l1l2 import emulated_picard
+
+    m = configs.with_sliding(configs.slab(n=16), law, seed=2).copy(pcg_maxiters=2000)
+    u, v, ef, it, _ = emulated_picard(m)
+    uo, vo, eo, _, sto = oracle.velo_higher_solve(m)
+    assert sto["status"] == 0 and it == sto["picard_iters"], (it, sto)
+    assert rel_l2([u, v], [uo, vo]) < 1e-9
