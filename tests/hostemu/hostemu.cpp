@@ -505,7 +505,7 @@ extern "C" int emu_diva_step(const bp_inputs* in, double* Auu, double* Auv, doub
 // in for the device's on the reference layout.  Outputs as bp_solve (the
 // 3-D velocity, efvs; DIVA's state written back) and the Picard count.
 // which_resid 0-2 only.  10 if the plan rejects the inputs.
-extern "C" int emu_picard_2d(const bp_inputs* in, const double* uvel, const double* vvel, double* uout,
+extern "C" int emu_picard(const bp_inputs* in, const double* uvel, const double* vvel, double* uout,
                              double* vout, double* efvs, int* picard_iters) {
   Emu E;
   std::string err;

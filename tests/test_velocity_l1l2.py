@@ -255,13 +255,13 @@ def test_device_l1l2_no_slip_bed_is_zero(ctx):
 def emulated_picard(m, uvel=None, vvel=None):
     """The 2-D Picard loop through the device bodies in the engine's launch
     order, the oracle's PCG as its linear solver (tests/hostemu
-    emu_picard_2d): (uvel, vvel, efvs, picard iterations, prepared)."""
+    emu_picard): (uvel, vvel, efvs, picard iterations, prepared)."""
     emu = C.CDLL(EMU)
     prep, u, v = solver.prepare(m, uvel, vvel)
     uo, vo = np.ascontiguousarray(u.copy()), np.ascontiguousarray(v.copy())
     ef = np.zeros((m.ny, m.nx, m.nz - 1))
     it = C.c_int(0)
-    rc = emu.emu_picard_2d(C.byref(prep.inputs), _p(np.ascontiguousarray(u)), _p(np.ascontiguousarray(v)),
+    rc = emu.emu_picard(C.byref(prep.inputs), _p(np.ascontiguousarray(u)), _p(np.ascontiguousarray(v)),
                            _p(uo), _p(vo), _p(ef), C.byref(it))
     assert rc == 0
     return uo, vo, ef, it.value, prep
