@@ -317,3 +317,20 @@ def test_emulated_diva_with_a_sliding_law_matches_oracle():
     uo, vo, eo, _, sto, ex = oracle.velo_diva_solve(m)
     assert sto["status"] == 0 and it == sto["picard_iters"] and it > 2
     assert rel_l2([u, v], [uo, vo]) < 1e-9
+
+
+@pytest.mark.gpu
+def test_device_diva_state_carries_over(ctx):
+    """A second device solve from the state the first one wrote back starts
+    at the fixed point, as the oracle's does."""
+    from helpers import rel_l2
+
+    m = _slab().copy(pcg_maxiters=3000)
+    u, v, efvs, st = ctx.velo_higher_solve(m)
+    assert st["status"] == 0 and st["picard_iters"] > 5
+    m2 = m.copy(diva_state=dict(st["diva"], efvs=efvs))
+    u2, v2, _, st2 = ctx.velo_higher_solve(m2, uvel=u, vvel=v)
+    uo, vo, eo, _, sto, ex = oracle.velo_diva_solve(m)
+    uo2, vo2, _, _, sto2, _ = oracle.velo_diva_solve(m, uo, vo, efvs=eo, **ex)
+    assert st2["status"] == 0 and st2["picard_iters"] == sto2["picard_iters"] <= 2
+    assert rel_l2([u2, v2], [uo2, vo2]) < 1e-8
