@@ -334,3 +334,20 @@ def test_device_diva_state_carries_over(ctx):
     uo2, vo2, _, _, sto2, _ = oracle.velo_diva_solve(m, uo, vo, efvs=eo, **ex)
     assert st2["status"] == 0 and st2["picard_iters"] == sto2["picard_iters"] <= 2
     assert rel_l2([u2, v2], [uo2, vo2]) < 1e-8
+
+
+def test_emulated_diva_state_carries_over():
+    """The emulated device loop from the state its first solve wrote back
+    (through the plan's scatters and the binding) needs the oracle's
+    iteration count, at most two."""
+    from helpers import rel_l2
+    from test_velocity_l1l2 import emulated_picard
+
+    m = _slab().copy(pcg_maxiters=3000)
+    u, v, ef, it, prep = emulated_picard(m)
+    st = {k: prep.arrays[k].copy() for k in ("uvel_2d", "vvel_2d", "btractx", "btracty")}
+    u2, v2, _, it2, _ = emulated_picard(m.copy(diva_state=dict(st, efvs=ef)), u, v)
+    uo, vo, eo, _, sto, ex = oracle.velo_diva_solve(m)
+    uo2, vo2, _, _, sto2, _ = oracle.velo_diva_solve(m, uo, vo, efvs=eo, **ex)
+    assert it == sto["picard_iters"] and it2 == sto2["picard_iters"] <= 2
+    assert rel_l2([u2, v2], [uo2, vo2]) < 1e-9
