@@ -449,6 +449,59 @@ def with_sliding(m: BPModel, law: int, seed: int = 0, n_scale: float = 0.8, **pa
     return m.copy(which_babc=law, sliding=sl, name=f"{m.name}_law{law}")
 
 
+def raymond_stream(n_stream: int = 25, nz: int = 2, half_width: float = 25.0e3, along: float = 30.0e3,
+                   thickness: float = 1000.0, dsdx: float = -1.0e-3, flwa: float = 1.0e-16,
+                   tau_stream: float = 5.2e3, tau_strong: float = 0.7e5) -> BPModel:
+    """The reference's idealised ice stream (tests/stream/runStream.py:124-360,
+    its doubly periodic form, kinflag = 0): a slab of thickness H on a bed
+    sloping at dsdx along x, a till yield stress (which_ho_babc = 2) of
+    tau_stream inside |y| < half_width and tau_strong (above the driving
+    stress) outside, uniform along flow, 5 H of strong bed on each side,
+    Glen's law with a uniform rate factor, Chronopoulos-Gear PCG with the
+    diagonal preconditioner, local basal assembly, no grounded minimum of
+    beta (stream.config).  The stream edges fall on vertex rows.  Raymond's
+    (2000) solution :func:`raymond_uvel` is its analytic profile.
+    """
+    dy = 2.0 * half_width / n_stream
+    dx = dy
+    n_strong = int(np.floor(5.0 * thickness / dy + 0.5))  # the script's round(), halves away from zero
+    gy = n_stream + 2 * n_strong
+    gx = int(round(along / dx))
+    L = gx * dx
+    x1 = dx * np.arange(gx)
+    topg_owned = np.tile(1000.0 + dsdx * x1, (gy, 1))
+    usrf = halo_fill_cells(_embed(topg_owned + thickness), offset_ew=-dsdx * L)
+    thck = halo_fill_cells(_embed(np.full((gy, gx), thickness)))
+    topg = usrf - thck
+    ny, nx = thck.shape
+    # vertex row j (the NE corner of cell row j) sits at y0 = dy (j + 1) - dy gy / 2
+    y0 = dy * (np.arange(gy) + 1) - dy * gy / 2.0
+    tau = np.where(np.abs(y0) >= half_width, tau_strong, tau_stream)
+    yield_stress = _vertex_from_owned(np.tile(tau[:, None], (1, gx)))
+    sl = SlidingLaw(law=BABC_YIELD_PICARD, yield_stress=yield_stress)
+    return BPModel(nx=nx, ny=ny, nz=nz, dx=dx, dy=dy, thck=thck, usrf=usrf, topg=topg,
+                   flwa=np.full((ny, nx, nz - 1), flwa), beta_external=np.zeros((ny - 1, nx - 1)),
+                   eus=0.0, thklim=1.0, beta_grounded_min=0.0, which_babc=BABC_YIELD_PICARD, sliding=sl,
+                   which_efvs=EFVS_NONLINEAR, which_sparse=SPARSE_PCG_CHRONGEAR, which_precond=PRECOND_DIAG,
+                   which_assemble_beta=ASSEMBLE_LOCAL, maxiter_nonlinear=300,
+                   name=f"raymond_stream{gx}x{gy}x{nz}")
+
+
+def raymond_uvel(y: np.ndarray, half_width: float = 25.0e3, thickness: float = 1000.0,
+                 dsdx: float = -1.0e-3, flwa: float = 1.0e-16, tau_stream: float = 5.2e3,
+                 tau_strong: float = 0.7e5, rhoi: float = 910.0, grav: float = 9.81) -> np.ndarray:
+    """Raymond's (2000) ice-stream velocity across the stream (the
+    reference's raymond_uvel, tests/stream/runStream.py:166-172): u =
+    2 A / (n+1) ((tau_d - tau_0) / H)^n (w^(n+1) - |y|^(n+1)), n = 3, zero
+    where the bed is stronger than the driving stress tau_d."""
+    n = 3.0
+    taud = -rhoi * grav * thickness * dsdx
+    tau0 = np.where(np.abs(y) >= half_width, tau_strong, tau_stream)
+    tau0 = np.minimum(tau0, taud)
+    u = 2.0 * flwa / (n + 1.0) * ((taud - tau0) / thickness) ** n * (half_width ** (n + 1) - np.abs(y) ** (n + 1))
+    return np.maximum(u, 0.0)
+
+
 def random_slab(rng: np.random.Generator, n: int = 96, dx: float = 500.0, nz: int = 11) -> BPModel:
     """A member of the periodic-slab family of the learned guess's training
     and held-out sets: the slab above with a random slope (0.05-0.2 deg),
