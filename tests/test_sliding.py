@@ -301,3 +301,25 @@ def test_emulated_picard_loop_with_a_sliding_law_matches_oracle(law):
     uo, vo, eo, _, sto = oracle.velo_higher_solve(m)
     assert sto["status"] == 0 and it == sto["picard_iters"], (it, sto)
     assert rel_l2([u, v], [uo, vo]) < 1e-9
+
+
+@pytest.mark.parametrize("law", [configs.BABC_POWERLAW, configs.BABC_COULOMB_POWERLAW_SCHOOF,
+                                 configs.BABC_PSEUDO_PLASTIC])
+@pytest.mark.parametrize("approx", [configs.APPROX_SSA, configs.APPROX_L1L2, configs.APPROX_DIVA],
+                         ids=["ssa", "l1l2", "diva"])
+def test_emulated_2d_picard_loop_with_a_sliding_law_matches_oracle(approx, law):
+    """The sliding laws inside the 2-D solves: the shallow-shelf and L1L2
+    laws read the 2-D (basal) velocity, DIVA's the 3-D basal velocity of the
+    previous iteration; the device bodies in the engine's order against the
+    oracle's solve."""
+    from helpers import rel_l2
+    from test_velocity_l1l2 import emulated_picard
+
+    m = configs.with_sliding(configs.slab(n=16), law, seed=5).copy(approx_2d=approx, pcg_maxiters=2000)
+    u, v, ef, it, _ = emulated_picard(m)
+    if approx == configs.APPROX_DIVA:
+        uo, vo, eo, _, sto, _ = oracle.velo_diva_solve(m)
+    else:
+        uo, vo, eo, _, sto = oracle.velo_2d_solve(m, approx)
+    assert sto["status"] == 0 and it == sto["picard_iters"] and it > 2, (it, sto)
+    assert rel_l2([u, v], [uo, vo]) < 1e-8
