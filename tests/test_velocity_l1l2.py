@@ -282,3 +282,24 @@ def test_emulated_l1l2_picard_loop_matches_oracle(m):
     # 1e-6 as on the GPU: the Cardano switch amplifies last-bit strain-rate
     # differences up to 1e6 (see the assembly test above)
     assert np.abs(ef - eo).max() <= 1e-6 * np.abs(eo).max()
+
+
+@pytest.mark.parametrize("resid", [0, 1, 2])
+@pytest.mark.parametrize("approx", [0, configs.APPROX_L1L2], ids=["bp", "l1l2"])
+def test_emulated_picard_criteria_match_oracle(approx, resid):
+    """The Picard criteria (which_ho_resid 0 max, 1 max without the bed
+    level, 2 mean; the 2-D solves have no bed level to leave out) with the
+    Chronopoulos-Gear PCG, through the emulated device loop."""
+    from helpers import rel_l2
+
+    m = configs.dome(n=15, nz=6, radius=12.0e3, hmax=1000.0).copy(
+        which_babc=configs.BABC_BETA_EXTERNAL, which_resid=resid, approx_2d=approx,
+        which_sparse=configs.SPARSE_PCG_CHRONGEAR, pcg_maxiters=2000)
+    m.beta_external = np.full_like(m.beta_external, 400.0)
+    u, v, _, it, _ = emulated_picard(m)
+    if approx:
+        uo, vo, _, _, sto = oracle.velo_l1l2_solve(m)
+    else:
+        uo, vo, _, _, sto = oracle.velo_higher_solve(m)
+    assert sto["status"] == 0 and it == sto["picard_iters"]
+    assert rel_l2([u, v], [uo, vo]) < 1e-9
