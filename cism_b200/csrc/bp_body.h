@@ -180,7 +180,7 @@ BP_HD const InstParams& elem_gather(const DevView& v, int e, double* x, double* 
     z[n] = s - ip.sigma[lev] * h;
     const int col = v.cell_cols[corner * v.ncells + cell];
     if (col >= 0) {
-      const double2 xv = v.x[(size_t)col * nz + lev];
+      const double2 xv = v.x[node_of(v, col, lev)];
       u[n] = xv.x; w[n] = xv.y;
     } else {
       u[n] = 0.0; w[n] = 0.0;
@@ -246,7 +246,7 @@ BP_HD double bfric_cell(const DevView& v, const RefTables& T, int cell) {
   for (int q = 0; q < 4; ++q) {  // SW, SE, NE, NW = the reference's 2-D node order
     const int col = v.cell_cols[q * v.ncells + cell];
     if (col >= 0) {
-      const double2 xb = v.x[(size_t)col * nz + nz - 1];
+      const double2 xb = v.x[node_of(v, col, nz - 1)];
       u[q] = xb.x;
       w[q] = xb.y;
     } else {
@@ -270,7 +270,7 @@ BP_HD double bfric_cell(const DevView& v, const RefTables& T, int cell) {
 }
 
 BP_HD double bfric_vertex(const DevView& v, int col) {
-  const double2 xb = v.x[(size_t)col * v.nz + v.nz - 1];
+  const double2 xb = v.x[node_of(v, col, v.nz - 1)];
   return v.col_beta[col] * (xb.x * xb.x + xb.y * xb.y) / 31536000.0;
 }
 
@@ -450,7 +450,7 @@ BP_HD bool qp2_element_point(const DevView& v, const RefTables& T, int c, int p,
     h[n] = v.cell_h[n * v.ncells + c];
     const int col = v.cell_cols[n * v.ncells + c];
     if (col >= 0) {
-      const double2 xv = v.x[col];
+      const double2 xv = v.x[v.col_node[col]];
       u[n] = xv.x;
       w[n] = xv.y;
     } else {
@@ -581,8 +581,8 @@ BP_HD void l1l2_cell(const DevView& v, int c) {
     x[n] = ip.dx * iv;
     y[n] = ip.dy * jv;
     const int col = v.cell_cols[n * v.ncells + c];
-    u[n] = col >= 0 ? v.x[col].x : 0.0;
-    w[n] = col >= 0 ? v.x[col].y : 0.0;
+    u[n] = col >= 0 ? v.x[v.col_node[col]].x : 0.0;
+    w[n] = col >= 0 ? v.x[v.col_node[col]].y : 0.0;
   }
   double J11 = 0, J12 = 0, J21 = 0, J22 = 0;
   for (int n = 0; n < 4; ++n) {
@@ -645,8 +645,8 @@ BP_HD void l1l2_column(const DevView& v, int col) {
                      v.col_cells[3 * nc + col]};
   const bool sw = cs[0] >= 0, se = cs[1] >= 0, nw = cs[2] >= 0, ne = cs[3] >= 0;
   const double sx = v.col_ds[col], sy = v.col_ds[nc + col], H = v.col_h[col];
-  const uint8_t dm = v.dmask[col];
-  const double2 ub = v.x[col];
+  const uint8_t dm = v.dmask[v.col_node[col]];
+  const double2 ub = v.x[v.col_node[col]];
   double2* out = v.x3 + (size_t)col * (nl + 1);
   out[nl] = ub;
   double2 up = ub;
@@ -755,7 +755,7 @@ BP_HD void diva_column_beta(const DevView& v, int col) {
 // omega_k staggered level by level.
 BP_HD void diva_column_velocity(const DevView& v, int col) {
   const int nl = v.nl;
-  const double2 um = v.x[col];
+  const double2 um = v.x[v.col_node[col]];
   const double be = v.col_beff[col], so = v.col_somega[col];
   double2 bt;
   bt.x = be * um.x;
@@ -882,7 +882,7 @@ BP_HD void row_basal(const DevView& v, const RefTables& T, int col, int k,
 template <int B>
 BP_HD double row_dirichlet(const DevView& v, int col, int k, double* acc) {
   const int nz = v.nz, nc = v.ncols;
-  const uint8_t me = v.dmask[(size_t)col * nz + k];
+  const uint8_t me = v.dmask[node_of(v, col, k)];
   const bool ur = me & 1, vr = me & 2;
   const bool row_presc = (B <= 1) ? ur : vr;
   double adj = 0.0;
@@ -899,7 +899,7 @@ BP_HD double row_dirichlet(const DevView& v, int col, int k, double* acc) {
       continue;
     }
     if (!inb) continue;
-    const size_t nn = (size_t)cn * nz + kn;
+    const size_t nn = node_of(v, cn, kn);
     const uint8_t pm = v.dmask[nn];
     if (diag) {
       // the reference zeroes the u-v coupling at a node whose other
@@ -929,9 +929,9 @@ BP_HD double2 matvec_row(const DevView& v, const Mat* A, int col, int k, size_t 
                          const Src& src) {
   const int nz = v.nz, nc = v.ncols;
   const size_t np = (size_t)v.npad;
-  int cn[9];
+  int cn[9];  // the neighbours' nodes at level 0
 #pragma unroll
-  for (int q = 0; q < 9; ++q) cn[q] = v.col_nbr[q * nc + col];
+  for (int q = 0; q < 9; ++q) cn[q] = v.col_nbn[q * nc + col];
   double yu = 0.0, yv = 0.0;
 #pragma unroll
   for (int kA = -1; kA <= 1; ++kA) {
@@ -943,7 +943,7 @@ BP_HD double2 matvec_row(const DevView& v, const Mat* A, int col, int k, size_t 
       const int m = (kA + 1) * 9 + q;
       const Mat au = BP_LD_STREAM(A + (size_t)m * np + n);
       const Mat av = BP_LD_STREAM(A + (size_t)(27 + m) * np + n);
-      const double2 s = src((size_t)cn[q] * nz + kn);
+      const double2 s = src((size_t)cn[q] + ((size_t)kn << v.lsh));
       yu += (double)au.x * s.x + (double)au.y * s.y;
       yv += (double)av.x * s.x + (double)av.y * s.y;
     }
@@ -971,9 +971,9 @@ BP_HD double2 matvec_row_sym(const DevView& v, const double2* A, int col, int k,
                              const Src& src) {
   const int nz = v.nz, nc = v.ncols;
   const size_t np = (size_t)v.npad;
-  int cn[9];
+  int cn[9];  // the neighbours' nodes at level 0
 #pragma unroll
-  for (int q = 0; q < 9; ++q) cn[q] = v.col_nbr[q * nc + col];
+  for (int q = 0; q < 9; ++q) cn[q] = v.col_nbn[q * nc + col];
   double yu = 0.0, yv = 0.0;
 #pragma unroll
   for (int kA = -1; kA <= 1; ++kA) {
@@ -983,7 +983,7 @@ BP_HD double2 matvec_row_sym(const DevView& v, const double2* A, int col, int k,
     for (int q = 0; q < 9; ++q) {
       const int m = (kA + 1) * 9 + q;
       const bool ok = kin && cn[q] >= 0;
-      const size_t p = ok ? (size_t)cn[q] * nz + kn : n;  // in-bounds stand-in when absent
+      const size_t p = ok ? (size_t)cn[q] + ((size_t)kn << v.lsh) : n;  // in-bounds stand-in when absent
       double2 s = src(p);
       if (!ok) s = double2{0.0, 0.0};
       if (m >= 13) {
@@ -1020,7 +1020,7 @@ BP_HD void sia_coefs(const DevView& v, size_t n, int k, int h, double* sub, doub
       *sup = 0.0;
     }
     if (k > 0) {
-      const double2 l = v.A[(size_t)(h * 14 + 9) * np + n - 1];
+      const double2 l = v.A[(size_t)(h * 14 + 9) * np + n - v.W];  // the node at k-1
       *sub = h ? l.y : l.x;
     } else {
       *sub = 0.0;
@@ -1069,8 +1069,8 @@ BP_HD void make_a32_row(const DevView& v, int col, int k, size_t n) {
     const double2 a = v.A[(size_t)mm * np + n], b = v.A[(size_t)(14 + mm) * np + n];
     v.A32[(size_t)mm * np + n] = float4{(float)a.x, (float)a.y, (float)b.x, (float)b.y};
   }
-  int cn[9];
-  for (int q = 0; q < 9; ++q) cn[q] = v.col_nbr[q * nc + col];
+  int cn[9];  // the neighbours' nodes at level 0
+  for (int q = 0; q < 9; ++q) cn[q] = v.col_nbn[q * nc + col];
   double euu = 0.0, euv = 0.0, evu = 0.0, evv = 0.0;
   for (int m = 0; m < 27; ++m) {
     if (m == 13) continue;
@@ -1083,7 +1083,7 @@ BP_HD void make_a32_row(const DevView& v, int col, int k, size_t n) {
       evu += rd_err32(b.x);
       evv += rd_err32(b.y);
     } else {
-      const size_t p = (size_t)cn[q] * nz + kn;
+      const size_t p = (size_t)cn[q] + ((size_t)kn << v.lsh);
       const double2 b0 = v.A[(size_t)(13 - m) * np + p], b1 = v.A[(size_t)(27 - m) * np + p];
       euu += rd_err32(b0.x);
       euv += rd_err32(b1.x);
@@ -1103,9 +1103,9 @@ BP_HD double2 matvec_row_sym32(const DevView& v, const float4* A, int col, int k
                                const Src& src) {
   const int nz = v.nz, nc = v.ncols;
   const size_t np = (size_t)v.npad;
-  int cn[9];
+  int cn[9];  // the neighbours' nodes at level 0
 #pragma unroll
-  for (int q = 0; q < 9; ++q) cn[q] = v.col_nbr[q * nc + col];
+  for (int q = 0; q < 9; ++q) cn[q] = v.col_nbn[q * nc + col];
   double yu = 0.0, yv = 0.0;
 #pragma unroll
   for (int kA = -1; kA <= 1; ++kA) {
@@ -1115,7 +1115,7 @@ BP_HD double2 matvec_row_sym32(const DevView& v, const float4* A, int col, int k
     for (int q = 0; q < 9; ++q) {
       const int m = (kA + 1) * 9 + q;
       const bool ok = kin && cn[q] >= 0;
-      const size_t p = ok ? (size_t)cn[q] * nz + kn : n;
+      const size_t p = ok ? (size_t)cn[q] + ((size_t)kn << v.lsh) : n;
       double2 s = src(p);
       if (!ok) s = double2{0.0, 0.0};
       if (m == 13) {

@@ -6,8 +6,15 @@
 // glissade_velo_higher_pcg.F90:2605-2612).  The halo of the reference's
 // local grid disappears: a periodic image map turns halo vertices into the
 // owned vertices they copy (parallel_slap.F90:2807-2925), so every stencil
-// neighbour is an owned column or absent.  Node n = col * nz + k (k = 0 is
-// the upper surface, k = nz-1 the bed, as in the reference).  Elements are
+// neighbour is an owned column or absent.  Levels k = 0 (the upper surface)
+// to nz-1 (the bed), as in the reference.  Node layout: each instance's
+// columns are cut into blocks of W consecutive columns (W a power of two,
+// W * nz <= kTile), and a block's nodes are stored level-major, node
+// (col, k) = col_node[col] + k * W, so that consecutive columns at one
+// level are consecutive in memory: a warp reading 32 columns of a level
+// reads contiguous vectors and coefficients, and a column's levels are W
+// apart.  Blocks never span two instances; the slots of an instance's last
+// block past its columns are holes that no kernel touches.  Elements are
 // the reference's active cells (i,j in [nhalo+1, n-nhalo+1]) times nz-1
 // layers; their geometry is taken from the halo'd vertex arrays so periodic
 // surface offsets are preserved.
@@ -99,6 +106,7 @@ struct Counters {
 // Device view of a compiled problem (all pointers are device pointers).
 struct DevView {
   int nz, ncols, nnodes, npad, ncells, nelem, ninst, ntiles;
+  int W, lsh;              // column block width (power of two, W * nz <= kTile) and log2 W
   int any_dirichlet;       // any prescribed node in the problem
   int sym;                 // matrix stored as its 14 upper stencil offsets (exactly symmetric)
   int minb;                // residual kernels: resident CTAs per SM they are built for (0 or 4)
@@ -117,6 +125,8 @@ struct DevView {
   // columns
   const int* col_inst;     // [ncols]
   const int* col_nbr;      // [9][ncols], q = (jA+1)*3 + (iA+1); -1 = none
+  const int* col_node;     // [ncols] node of (col, level 0); node (col, k) = col_node[col] + k * W
+  const int* col_nbn;      // [9][ncols] col_node of each stencil neighbour; -1 = none
   const int* col_cells;    // [4][ncols], cells (i,j),(i+1,j),(i,j+1),(i+1,j+1)
   const int* col_ij;       // [2][ncols], halo'd Fortran vertex indices
   double* col_beta;        // [ncols] beta_internal (recomputed each Picard iteration with a sliding law)
@@ -148,10 +158,12 @@ struct DevView {
   double* col_somega;      // [ncols] omega staggered to the column
   double* col_beff;        // [ncols] beta_eff (the basal term of the 2-D system)
   double2* col_bt;         // [ncols] basal traction (btractx, btracty)
-  // tiles
-  const int* tile_start;   // [ntiles] first node (tiles hold whole columns)
-  const int* tile_end;     // [ntiles] one past the last node
+  // tiles: one per column block
+  const int* tile_start;   // [ntiles] first node of the block
+  const int* tile_end;     // [ntiles] tile_start + W * nz
   const int* tile_inst;    // [ntiles]
+  const int* tile_ncols;   // [ntiles] columns in the block (the slots past them are holes)
+  const int* tile_col0;    // [ntiles] first column of the block
   // assembly / matrix
   double* qp;              // [nelem*8*10]: f, Jinv(3x3) per quadrature point
   double* efvs;            // [nelem]; L1L2 [ncells][nl]
@@ -178,6 +190,19 @@ struct DevView {
   double* partials;        // [3][ntiles]
   unsigned* tile_counter;  // [ninst]
 };
+
+// Node of (col, k) in the blocked level-major layout.
+BP_HD size_t node_of(const DevView& v, int col, int k) {
+  return (size_t)v.col_node[col] + ((size_t)k << v.lsh);
+}
+
+// Column block width for nz levels: the largest power of two W with
+// W * nz <= kTile.
+BP_HD int block_width(int nz) {
+  int w = 1;
+  while (2 * w * nz <= kTile) w *= 2;
+  return w;
+}
 
 // indxA_3d (glissade_velo_higher.F90:599-619), 0-based: iA fastest.
 BP_HD int stencil_index(int iA, int jA, int kA) { return (iA + 1) + 3 * (jA + 1) + 9 * (kA + 1); }

@@ -142,6 +142,7 @@ DevView make_view(Arena& a, cudaStream_t s, const HostPlan& p, bool with_cells, 
   DevView v;
   std::memset(&v, 0, sizeof(v));
   v.nz = p.nz; v.ncols = p.ncols; v.nnodes = p.nnodes; v.npad = p.npad;
+  v.W = p.W; v.lsh = p.lsh;
   v.solve2d = p.solve2d ? 1 : 0;
   v.l1l2 = p.l1l2 ? 1 : 0;
   v.diva = p.diva ? 1 : 0;
@@ -166,6 +167,8 @@ DevView make_view(Arena& a, cudaStream_t s, const HostPlan& p, bool with_cells, 
   v.cnt = a.get<Counters>(s, "cnt", 1);
   UP(int, "col_inst", p.col_inst, col_inst);
   UP(int, "col_nbr", p.col_nbr, col_nbr);
+  UP(int, "col_node", p.col_node, col_node);
+  UP(int, "col_nbn", p.col_nbn, col_nbn);
   UP(int, "col_cells", p.col_cells, col_cells);
   UP(int, "col_ij", p.col_ij, col_ij);
   UP(double, "col_beta", p.col_beta, col_beta);
@@ -209,6 +212,8 @@ DevView make_view(Arena& a, cudaStream_t s, const HostPlan& p, bool with_cells, 
   UP(int, "tile_start", p.tile_start, tile_start);
   UP(int, "tile_end", p.tile_end, tile_end);
   UP(int, "tile_inst", p.tile_inst, tile_inst);
+  UP(int, "tile_ncols", p.tile_ncols, tile_ncols);
+  UP(int, "tile_col0", p.tile_col0, tile_col0);
 #undef UP
   v.A = a.get<double2>(s, "A", (v.sym ? 2 * 14 : 2 * 27) * np);
   v.x = a.get<double2>(s, "x", np);
@@ -220,6 +225,9 @@ DevView make_view(Arena& a, cudaStream_t s, const HostPlan& p, bool with_cells, 
   v.Az = a.get<double2>(s, "Az", np);
   v.Dinv = a.get<double2>(s, "Dinv", np);
   v.usav = a.get<double2>(s, "usav", np);
+  // the hole slots of the node vectors stay zero
+  for (double2* vec : {v.x, v.b, v.r, v.d0, v.z, v.q, v.Az, v.Dinv, v.usav})
+    CK(cudaMemsetAsync(vec, 0, sizeof(double2) * np, s));
   if (mixed && v.sym) {
     float4* blk = a.get<float4>(s, "A32", 16 * np);  // A32 then A32d: one L2 window
     v.A32 = blk;
@@ -878,7 +886,14 @@ int bp_problem_diagnostics(bp_problem* P, int which_bfric, double* const* tau_xz
     if (p.any_sliding) launch_corner_beta(P->v, c->stream);
     else upload(c->stream, P->v.cell_beta, p.cell_beta);
   }
-  const DevView dv = diagnostics_view(P->v, p, x3, fl);
+  int* cn3 = nullptr;
+  if (p.solve2d) {  // x3 is [ncols][nz_out]
+    std::vector<int> h3(std::max(p.ncols, 1));
+    for (int c = 0; c < p.ncols; ++c) h3[c] = c * p.nz_out;
+    cn3 = P->arena->get<int>(c->stream, "diag_col_node", h3.size());
+    upload(c->stream, cn3, h3);
+  }
+  const DevView dv = diagnostics_view(P->v, p, x3, fl, cn3);
   const size_t ne = (size_t)diagnostic_elements(p), nb = (size_t)std::max(p.ncells, p.ncols);
   double* d = P->arena->get<double>(c->stream, "diagnostics", (want_tau ? 6 * ne : 0) + nb);
   double* d_tau = want_tau ? d : nullptr;

@@ -116,7 +116,7 @@ __device__ __forceinline__ void fail(const DevView& v, InstState& S, int code) {
 __device__ __forceinline__ bool is_nan(double x) { return x != x; }
 
 struct TileRange {
-  int inst, n0, nend;
+  int inst, n0, nend, ncols, col0;
 };
 
 // Programmatic dependent launch: the PCG kernels are launched so that the
@@ -132,8 +132,20 @@ __device__ __forceinline__ TileRange tile_range(const DevView& v, int t) {
   r.inst = v.tile_inst[t];
   r.n0 = v.tile_start[t];
   r.nend = v.tile_end[t];
+  r.ncols = v.tile_ncols[t];
+  r.col0 = v.tile_col0[t];
   return r;
 }
+
+// Thread i of a tile's CTA owns node n0 + i: level i >> lsh, column col0 +
+// (i & (W-1)); the slots past the block's columns are holes.
+__device__ __forceinline__ bool tile_mine(const DevView& v, const TileRange& R, int i) {
+  return R.n0 + i < R.nend && (i & (v.W - 1)) < R.ncols;
+}
+__device__ __forceinline__ int tile_col(const DevView& v, const TileRange& R, int i) {
+  return R.col0 + (i & (v.W - 1));
+}
+__device__ __forceinline__ int tile_k(const DevView& v, int i) { return i >> v.lsh; }
 
 // ---------------------------------------------------------------------
 // Picard iteration start (one CTA): counter, reset of the PCG state.
@@ -188,7 +200,7 @@ __global__ void __launch_bounds__(kTile) k_slide_beta(DevView v) {
     if (!S.picard_active || ip.slide.law == 0) continue;
     const size_t nc = (size_t)v.ncols;
     // the basal velocity: DIVA's 3-D one (:2240-2243), else the bed node
-    const double2 ub = v.diva ? v.x3[(size_t)col * (v.nl + 1) + v.nl] : v.x[(size_t)col * v.nz + v.nz - 1];
+    const double2 ub = v.diva ? v.x3[(size_t)col * (v.nl + 1) + v.nl] : v.x[node_of(v, col, v.nz - 1)];
     const double beta = slide_beta(ip.slide, v.col_slide[col], v.col_slide[nc + col],
                                    v.col_slide[2 * nc + col], ub.x, ub.y);
     if (!(beta >= 0.0) && (S.status == BP_OK || S.status == BP_WARN_PCG_NOT_CONVERGED))
@@ -217,7 +229,7 @@ __global__ void __launch_bounds__(kTile) k_save_usav(DevView v) {
     const TileRange R = tile_range(v, t);
     if (!v.st[R.inst].picard_active) continue;
     const int n = R.n0 + threadIdx.x;
-    if (n < R.nend) v.usav[n] = v.x[n];
+    if (tile_mine(v, R, threadIdx.x)) v.usav[n] = v.x[n];
   }
 }
 
@@ -343,8 +355,7 @@ __global__ void __launch_bounds__(256) k_diva_velocity(DevView v) {
 // Assembly pass 2 + basal BC + Dirichlet BC: thread = (block B, node).
 // ---------------------------------------------------------------------
 template <int B, bool D2>
-__device__ __forceinline__ bool asm_row(const DevView& v, int n) {
-  const int col = n / v.nz, k = n - col * v.nz;
+__device__ __forceinline__ bool asm_row(const DevView& v, int n, int col, int k) {
   double acc[27];
   if (D2) row_assemble2<B>(v, c_T, col, acc);
   else row_assemble<B>(v, c_T, col, k, acc);
@@ -376,12 +387,13 @@ __global__ void __launch_bounds__(kTile) k_asm_rows(DevView v) {
     if (!v.st[R.inst].picard_active) continue;
     const int n = R.n0 + threadIdx.x;
     int nzl = 0;
-    if (n < R.nend) {
+    if (tile_mine(v, R, threadIdx.x)) {
+      const int col = tile_col(v, R, threadIdx.x), k = tile_k(v, threadIdx.x);
       switch (B) {
-        case 0: nzl = asm_row<0, D2>(v, n); break;
-        case 1: nzl = asm_row<1, D2>(v, n); break;
-        case 2: nzl = asm_row<2, D2>(v, n); break;
-        default: nzl = asm_row<3, D2>(v, n); break;
+        case 0: nzl = asm_row<0, D2>(v, n, col, k); break;
+        case 1: nzl = asm_row<1, D2>(v, n, col, k); break;
+        case 2: nzl = asm_row<2, D2>(v, n, col, k); break;
+        default: nzl = asm_row<3, D2>(v, n, col, k); break;
       }
     }
     if (__syncthreads_or(nzl) && threadIdx.x == 0) atomicOr(&v.st[R.inst].nonzero, 1);
@@ -398,7 +410,7 @@ __global__ void __launch_bounds__(kTile) k_rhs(DevView v) {
     const InstParams& ip = v.inst[R.inst];
     const int n = R.n0 + threadIdx.x;
     double part[1] = {0.0};
-    if (n < R.nend) {
+    if (tile_mine(v, R, threadIdx.x)) {
       const size_t np = (size_t)v.npad;
       const uint8_t dm = v.dmask[n];
       const double2 ld = v.load[n];
@@ -457,22 +469,24 @@ struct SiaTile {
 
 __device__ __forceinline__ double2 sia_tile(const DevView& v, const TileRange& R, double2 r) {
   __shared__ SiaTile T;
-  const int i = threadIdx.x, len = R.nend - R.n0, nz = v.nz;
-  if (i < len) {
+  const int i = threadIdx.x, nz = v.nz;
+  const bool mine = tile_mine(v, R, i);
+  // shared memory holds the tile column by column: j = c * nz + k
+  const int k = tile_k(v, i), j = (i & (v.W - 1)) * nz + k;
+  if (mine) {
     const size_t n = (size_t)R.n0 + i;
-    const int k = i % nz;  // tiles start on a column boundary
-    T.s[2 * i] = r.x;
-    T.s[2 * i + 1] = r.y;
-    sia_coefs(v, n, k, 0, &T.sub[0][i], &T.dg[0][i], &T.sup[0][i]);
-    sia_coefs(v, n, k, 1, &T.sub[1][i], &T.dg[1][i], &T.sup[1][i]);
+    T.s[2 * j] = r.x;
+    T.s[2 * j + 1] = r.y;
+    sia_coefs(v, n, k, 0, &T.sub[0][j], &T.dg[0][j], &T.sup[0][j]);
+    sia_coefs(v, n, k, 1, &T.sub[1][j], &T.dg[1][j], &T.sup[1][j]);
   }
   __syncthreads();
-  if (i < 2 * (len / nz)) {
+  if (i < 2 * R.ncols) {
     const int c = i >> 1, h = i & 1, b = c * nz;
     sia_column(nz, &T.sub[h][b], &T.dg[h][b], &T.sup[h][b], &T.s[2 * b + h], 2);
   }
   __syncthreads();
-  const double2 z = i < len ? make_double2(T.s[2 * i], T.s[2 * i + 1]) : make_double2(0.0, 0.0);
+  const double2 z = mine ? make_double2(T.s[2 * j], T.s[2 * j + 1]) : make_double2(0.0, 0.0);
   __syncthreads();  // T is reused by the CTA's next tile
   return z;
 }
@@ -541,11 +555,11 @@ __global__ void __launch_bounds__(kTile, MINB) k_resid(DevView v) {
     const InstState& S0 = v.st[R.inst];
     if (!S0.pcg_active || (MODE == MV_REFINE && !S0.need_true)) continue;
     const int n = R.n0 + threadIdx.x;
-    const bool mine = n < R.nend;
+    const bool mine = tile_mine(v, R, threadIdx.x);
     double part[2] = {0.0, 0.0};
     double2 r = make_double2(0.0, 0.0);
     if (mine) {
-      const int col = n / v.nz, k = n - col * v.nz;
+      const int col = tile_col(v, R, threadIdx.x), k = tile_k(v, threadIdx.x);
       const double2 y = mv_row<ST64>(v, col, k, n, v.x);
       const double2 b = v.b[n];
       r = make_double2(b.x - y.x, b.y - y.y);
@@ -608,7 +622,7 @@ template <int STORE>
 __device__ __forceinline__ void count_tile(const DevView& v, const InstState& S, const TileRange& R) {
   if (v.mv_nodes && !v.dry && threadIdx.x == 0) {
     const bool f32 = STORE == ST_SYM32 && !S.krylov_fp64;
-    atomicAdd(&v.mv_nodes[f32 ? 1 : 0], (unsigned long long)(R.nend - R.n0));
+    atomicAdd(&v.mv_nodes[f32 ? 1 : 0], (unsigned long long)R.ncols * v.nz);
   }
 }
 
@@ -626,8 +640,8 @@ __global__ void __launch_bounds__(kTile, MINB) k_std_mv(DevView v) {
     count_tile<STORE>(v, S0, R);
     const int n = R.n0 + threadIdx.x;
     double part[1] = {0.0};
-    if (n < R.nend) {
-      const int col = n / v.nz, k = n - col * v.nz;
+    if (tile_mine(v, R, threadIdx.x)) {
+      const int col = tile_col(v, R, threadIdx.x), k = tile_k(v, threadIdx.x);
       const double2 y = krylov_row<STORE>(v, S0, col, k, n, v.d0);
       const double2 d = v.d0[n];
       v.q[n] = y;
@@ -655,7 +669,7 @@ __global__ void __launch_bounds__(kTile) k_std_update(DevView v) {
     if (!S.pcg_active) continue;
     const int n = R.n0 + threadIdx.x;
     const double alpha = S.alpha;
-    const bool mine = n < R.nend;
+    const bool mine = tile_mine(v, R, threadIdx.x);
     double part[2] = {0.0, 0.0};
     double2 r = make_double2(0.0, 0.0);
     if (mine) {
@@ -704,7 +718,7 @@ __global__ void __launch_bounds__(kTile) k_std_dir(DevView v) {
     const InstState& S = v.st[R.inst];
     if (!S.pcg_active) continue;
     const int n = R.n0 + threadIdx.x;
-    if (n >= R.nend) continue;
+    if (!tile_mine(v, R, threadIdx.x)) continue;
     const double2 z = v.z[n];
     if (S.pcg_iter == 1) {
       v.d0[n] = z;
@@ -730,8 +744,8 @@ __global__ void __launch_bounds__(kTile, MINB) k_cg_mv(DevView v) {
     count_tile<STORE>(v, S0, R);
     const int n = R.n0 + threadIdx.x;
     double part[3] = {0.0, 0.0, 0.0};
-    if (n < R.nend) {
-      const int col = n / v.nz, k = n - col * v.nz;
+    if (tile_mine(v, R, threadIdx.x)) {
+      const int col = tile_col(v, R, threadIdx.x), k = tile_k(v, threadIdx.x);
       const double2 y = krylov_row<STORE>(v, S0, col, k, n, v.z);
       const double2 z = v.z[n], r = v.r[n];
       if (FIRST) {
@@ -792,7 +806,7 @@ __global__ void __launch_bounds__(kTile) k_cg_first_update(DevView v) {
     const InstState& S = v.st[R.inst];
     if (!S.pcg_active) continue;
     const int n = R.n0 + threadIdx.x;
-    const bool mine = n < R.nend;
+    const bool mine = tile_mine(v, R, threadIdx.x);
     const double alpha = S.alpha;
     double2 r = make_double2(0.0, 0.0);
     if (mine) {
@@ -821,7 +835,7 @@ __global__ void __launch_bounds__(kTile) k_cg_update(DevView v) {
     const InstState& S = v.st[R.inst];
     if (!S.pcg_active) continue;
     const int n = R.n0 + threadIdx.x;
-    const bool mine = n < R.nend;
+    const bool mine = tile_mine(v, R, threadIdx.x);
     const bool keep_r = !CHECK && !S.need_true;  // a refinement recomputes r and z
     const double alpha = S.alpha, beta = S.beta;
     double2 r = make_double2(0.0, 0.0);
@@ -857,8 +871,9 @@ __global__ void __launch_bounds__(kTile) k_picard_check(DevView v) {
     InstState& S = v.st[R.inst];
     const InstParams& ip = v.inst[R.inst];
     const int n = R.n0 + threadIdx.x;
+    const bool mine = tile_mine(v, R, threadIdx.x);
     if (S.zero_x) {
-      if (n < R.nend) v.x[n] = make_double2(0.0, 0.0);
+      if (mine) v.x[n] = make_double2(0.0, 0.0);
       continue;
     }
     if (!S.picard_active) continue;
@@ -866,9 +881,9 @@ __global__ void __launch_bounds__(kTile) k_picard_check(DevView v) {
     // the 2-D criterion has no bed layer to leave out (:9238-9351)
     const bool nobed = !v.solve2d && (ip.which_resid == 1 || meanu);
     double part[2] = {0.0, 0.0};
-    if (n < R.nend) {
+    if (mine) {
       if (S.frozen) v.x[n] = make_double2(0.0, 0.0);  // 2-D solve on a no-slip bed
-      const int k = n % v.nz;
+      const int k = tile_k(v, threadIdx.x);
       if (!(nobed && k == v.nz - 1)) {
         const double2 x = v.x[n], o = v.usav[n];
         const double speed = sqrt(x.x * x.x + x.y * x.y);
@@ -912,8 +927,8 @@ __global__ void __launch_bounds__(kTile) k_make_a32(DevView v) {
     const TileRange R = tile_range(v, t);
     if (!v.st[R.inst].pcg_active) continue;
     const int n = R.n0 + threadIdx.x;
-    if (n >= R.nend) continue;
-    const int col = n / v.nz, k = n - col * v.nz;
+    if (!tile_mine(v, R, threadIdx.x)) continue;
+    const int col = tile_col(v, R, threadIdx.x), k = tile_k(v, threadIdx.x);
     make_a32_row(v, col, k, (size_t)n);
   }
 }
@@ -947,8 +962,8 @@ __global__ void __launch_bounds__(kTile) k_matvec_plain(DevView v, const double2
   for (int t = blockIdx.x; t < v.ntiles; t += gridDim.x) {
     const TileRange R = tile_range(v, t);
     const int n = R.n0 + threadIdx.x;
-    if (n >= R.nend) continue;
-    const int col = n / v.nz, k = n - col * v.nz;
+    if (!tile_mine(v, R, threadIdx.x)) continue;
+    const int col = tile_col(v, R, threadIdx.x), k = tile_k(v, threadIdx.x);
     y[n] = v.sym ? matvec_row_sym(v, v.A, col, k, n, SrcX{x}) : matvec_row(v, v.A, col, k, n, SrcX{x});
   }
 }
@@ -960,8 +975,8 @@ __global__ void __launch_bounds__(kTile, MINB) k_tune_mv(DevView v) {
   for (int t = blockIdx.x; t < v.ntiles; t += gridDim.x) {
     const TileRange R = tile_range(v, t);
     const int n = R.n0 + threadIdx.x;
-    if (n >= R.nend) continue;
-    const int col = n / v.nz, k = n - col * v.nz;
+    if (!tile_mine(v, R, threadIdx.x)) continue;
+    const int col = tile_col(v, R, threadIdx.x), k = tile_k(v, threadIdx.x);
     v.Az[n] = mv_row<STORE>(v, col, k, n, v.x);
   }
 }
@@ -971,7 +986,7 @@ __global__ void __launch_bounds__(kTile) k_dinv(DevView v, int precond) {
   for (int t = blockIdx.x; t < v.ntiles; t += gridDim.x) {
     const TileRange R = tile_range(v, t);
     const int n = R.n0 + threadIdx.x;
-    if (n >= R.nend) continue;
+    if (!tile_mine(v, R, threadIdx.x)) continue;
     const size_t np = (size_t)v.npad;
     double2 di = make_double2(1.0, 1.0);
     (void)np;
@@ -990,7 +1005,7 @@ __global__ void __launch_bounds__(kTile) k_bb(DevView v) {
     const TileRange R = tile_range(v, t);
     const int n = R.n0 + threadIdx.x;
     double part[1] = {0.0};
-    if (n < R.nend) {
+    if (tile_mine(v, R, threadIdx.x)) {
       const double2 b = v.b[n];
       part[0] = b.x * b.x + b.y * b.y;
     }
@@ -1173,7 +1188,7 @@ void launch_bb(const DevView& v, cudaStream_t s) { k_bb<<<tile_grid(v), kTile, 0
 // level, :3745-3750) for the post-solve diagnostics.
 __global__ void __launch_bounds__(256) k_levels_from_2d(DevView v, double2* x3, int L) {
   const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < (long)v.ncols * L) x3[t] = v.x[t / L];
+  if (t < (long)v.ncols * L) x3[t] = v.x[v.col_node[t / L]];
 }
 
 // The bed-face corner betas from the columns' beta_internal (0 where a

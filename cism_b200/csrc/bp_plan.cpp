@@ -41,17 +41,39 @@ void add_columns(int nx, int ny, int nz, int periodic, const int* active_vertex,
   (void)inst_index;
 }
 
-// Tiles hold whole columns (as many as fit in kTile nodes), so a CTA can
-// run the column solves of the SIA preconditioner on its own tile.
-void add_tiles(HostPlan* p, int b, int node_begin, int node_end) {
-  const int step = std::max(1, kTile / std::max(1, p->nz)) * std::max(1, p->nz);
-  p->inst[b].tile_begin = (int)p->tile_start.size();
-  for (int s = node_begin; s < node_end; s += step) {
-    p->tile_start.push_back(s);
-    p->tile_end.push_back(std::min(s + step, node_end));
+// Blocks of W consecutive columns of instance b, one tile each (W * nz <=
+// kTile nodes, whole columns, so a CTA can run the column solves of the SIA
+// preconditioner on its own tile); sets the columns' nodes and the
+// instance's tile and node ranges.
+void add_tiles(HostPlan* p, int b, int col_begin, int ncols) {
+  const int W = p->W, span = W * p->nz;
+  InstParams& ip = p->inst[b];
+  ip.tile_begin = (int)p->tile_start.size();
+  ip.node_begin = ip.tile_begin * span;
+  for (int c0 = 0; c0 < ncols; c0 += W) {
+    const int t = (int)p->tile_start.size();
+    p->tile_start.push_back(t * span);
+    p->tile_end.push_back((t + 1) * span);
     p->tile_inst.push_back(b);
+    p->tile_ncols.push_back(std::min(W, ncols - c0));
+    p->tile_col0.push_back(col_begin + c0);
+    for (int c = c0; c < std::min(ncols, c0 + W); ++c) p->col_node[col_begin + c] = t * span + (c - c0);
   }
-  p->inst[b].tile_end = (int)p->tile_start.size();
+  ip.tile_end = (int)p->tile_start.size();
+  ip.node_end = ip.tile_end * span;
+}
+
+// The neighbours' nodes at level 0, after every column has its node.
+void fill_nbn(HostPlan* p) {
+  const size_t NC = (size_t)p->ncols;
+  p->col_nbn.resize(9 * NC);
+  for (size_t i = 0; i < 9 * NC; ++i) p->col_nbn[i] = p->col_nbr[i] >= 0 ? p->col_node[p->col_nbr[i]] : -1;
+}
+
+void set_block_width(HostPlan* p) {
+  p->W = block_width(p->nz);
+  p->lsh = 0;
+  while ((1 << p->lsh) < p->W) ++p->lsh;
 }
 
 }  // namespace
@@ -86,6 +108,7 @@ bool build_column_plan(int nx, int ny, int nz, int periodic,
   *p = HostPlan();
   p->nz = nz;
   p->nz_out = nz;
+  set_block_width(p);
   p->ninst = 1;
   p->inst.resize(1);
   std::memset(&p->inst[0], 0, sizeof(InstParams));
@@ -96,7 +119,7 @@ bool build_column_plan(int nx, int ny, int nz, int periodic,
   const int nc = (int)cols.size();
   p->ncols = nc;
   p->nnodes = nc * nz;
-  p->npad = round_up(std::max(p->nnodes, 1), 64);
+  p->col_node.assign(nc, 0);
   p->col_inst.assign(nc, 0);
   p->col_ij.resize(2 * (size_t)nc);
   p->col_nbr.resize(9 * (size_t)nc);
@@ -112,11 +135,12 @@ bool build_column_plan(int nx, int ny, int nz, int periodic,
   }
   InstParams& ip = p->inst[0];
   ip.col_begin = 0; ip.col_end = nc;
-  ip.node_begin = 0; ip.node_end = nc * nz;
-  add_tiles(p, 0, 0, nc * nz);
+  add_tiles(p, 0, 0, nc);
+  fill_nbn(p);
   p->ntiles = (int)p->tile_start.size();
-  p->load.assign(p->nnodes, double2{0.0, 0.0});
-  p->dmask.assign(p->nnodes, 0);
+  p->npad = round_up(std::max(p->ntiles * p->W * nz, 1), 64);
+  p->load.assign(p->npad, double2{0.0, 0.0});
+  p->dmask.assign(p->npad, 0);
   return true;
 }
 
@@ -238,6 +262,7 @@ bool build_plan(const bp_inputs* in, int n, HostPlan* p, std::string* err) {
   const int nz = solve2d ? 1 : nz_in, nl = nz_in - 1;
   p->nz = nz;
   p->nz_out = nz_in;
+  set_block_width(p);
   p->solve2d = solve2d;
   p->l1l2 = l1l2;
   p->diva = diva;
@@ -302,15 +327,18 @@ bool build_plan(const bp_inputs* in, int n, HostPlan* p, std::string* err) {
   // global columns
   const int NC = p->ncols;
   p->nnodes = NC * nz;
-  p->npad = round_up(std::max(p->nnodes, 1), 64);
+  int nblocks = 0;
+  for (int b = 0; b < n; ++b) nblocks += ((int)cols[b].size() + p->W - 1) / p->W;
+  p->npad = round_up(std::max(nblocks * p->W * nz, 1), 64);
+  p->col_node.assign(NC, 0);
   p->col_inst.resize(NC);
   p->col_ij.resize(2 * (size_t)NC);
   p->col_nbr.resize(9 * (size_t)NC);
   p->col_cells.assign(4 * (size_t)NC, -1);
   p->col_beta.resize(NC);
   if (p->any_sliding) p->col_slide.assign(3 * (size_t)NC, 0.0);
-  p->load.resize(p->nnodes);
-  p->dmask.resize(p->nnodes);
+  p->load.assign(p->npad, double2{0.0, 0.0});
+  p->dmask.assign(p->npad, 0);
   // cells: count first (cell ids must be global)
   std::vector<std::vector<int>> cellid(n);
   for (int b = 0; b < n; ++b) {
@@ -379,7 +407,7 @@ bool build_plan(const bp_inputs* in, int n, HostPlan* p, std::string* err) {
     }
     const int nc = (int)cols[b].size();
     ip.col_begin = col_base; ip.col_end = col_base + nc;
-    ip.node_begin = col_base * nz; ip.node_end = (col_base + nc) * nz;
+    add_tiles(p, b, col_base, nc);
     const int ncl = (int)cells[b].size();
     ip.cell_begin = cell_base; ip.cell_end = cell_base + ncl;
     const int epc = solve2d ? 1 : nz - 1;  // elements per cell
@@ -432,14 +460,14 @@ bool build_plan(const bp_inputs* in, int n, HostPlan* p, std::string* err) {
           lu = lu + I.loadu[vtx(i, j, nx) * nz_in + k];
           lv = lv + I.loadv[vtx(i, j, nx) * nz_in + k];
         }
-        p->load[g] = double2{lu, lv};
+        p->load[p->col_node[g]] = double2{lu, lv};
         const size_t bed = vtx(i, j, nx) * nz_in + (nz_in - 1);
-        p->dmask[g] = (uint8_t)((I.umask_dirichlet[bed] == 1 ? 1 : 0) | (I.vmask_dirichlet[bed] == 1 ? 2 : 0));
+        p->dmask[p->col_node[g]] = (uint8_t)((I.umask_dirichlet[bed] == 1 ? 1 : 0) | (I.vmask_dirichlet[bed] == 1 ? 2 : 0));
       } else {
         for (int k = 0; k < nz; ++k) {
           const size_t src = vtx(i, j, nx) * nz + k;
-          p->load[(size_t)g * nz + k] = double2{I.loadu[src], I.loadv[src]};
-          p->dmask[(size_t)g * nz + k] =
+          p->load[node_of(*p, g, k)] = double2{I.loadu[src], I.loadv[src]};
+          p->dmask[node_of(*p, g, k)] =
               (uint8_t)((I.umask_dirichlet[src] == 1 ? 1 : 0) | (I.vmask_dirichlet[src] == 1 ? 2 : 0));
         }
       }
@@ -486,10 +514,10 @@ bool build_plan(const bp_inputs* in, int n, HostPlan* p, std::string* err) {
           p->flwafact[(size_t)g * nl + k] = I.flwafact[cel(ic, jc, nx) * nl + k];
       }
     }
-    add_tiles(p, b, ip.node_begin, ip.node_end);
     col_base += nc;
     cell_base += ncl;
   }
+  fill_nbn(p);
   p->ntiles = (int)p->tile_start.size();
   return true;
 }
@@ -501,17 +529,17 @@ void gather_velocity(const HostPlan& p, int b, const double* uvel,
   for (int g = ip.col_begin; g < ip.col_end; ++g) {
     const int i = p.col_ij[g], j = p.col_ij[NC + g];
     if (p.diva) {  // the carried-over mean velocity (:1173-1180)
-      x[g] = p.x2d_0[g];
+      x[p.col_node[g]] = p.x2d_0[g];
       continue;
     }
     if (p.solve2d) {  // uvel_2d = uvel(nz,:,:) (glissade_velo_higher.F90:1179-1180)
       const size_t src = vtx(i, j, nx) * p.nz_out + (p.nz_out - 1);
-      x[g] = double2{uvel[src], vvel[src]};
+      x[p.col_node[g]] = double2{uvel[src], vvel[src]};
       continue;
     }
     for (int k = 0; k < nz; ++k) {
       const size_t src = vtx(i, j, nx) * nz + k;
-      x[(size_t)g * nz + k] = double2{uvel[src], vvel[src]};
+      x[node_of(p, g, k)] = double2{uvel[src], vvel[src]};
     }
   }
 }
@@ -524,7 +552,7 @@ void scatter_vector(const HostPlan& p, int b, const double2* x, double* vu,
     const int i = p.col_ij[g], j = p.col_ij[NC + g];
     for (int k = 0; k < nz; ++k) {
       const size_t dst = vtx(i, j, nx) * nz + k;
-      const double2 v = x[(size_t)g * nz + k];
+      const double2 v = x[node_of(p, g, k)];
       if (vu) vu[dst] = v.x;
       if (vv) vv[dst] = v.y;
     }
@@ -538,9 +566,10 @@ void scatter_velocity(const HostPlan& p, int b, const double2* x,
     const int nx = p.nx[b], NC = p.ncols, L = p.nz_out;
     for (int g = ip.col_begin; g < ip.col_end; ++g) {
       const size_t w = vtx(p.col_ij[g], p.col_ij[NC + g], nx);
+      const double2 xg = x[p.col_node[g]];
       for (int k = 0; k < L; ++k) {
-        uvel[w * L + k] = x[g].x;
-        vvel[w * L + k] = x[g].y;
+        uvel[w * L + k] = xg.x;
+        vvel[w * L + k] = xg.y;
       }
     }
   } else {
@@ -586,8 +615,8 @@ void scatter_diva(const HostPlan& p, int b, const double2* x, const double2* bt)
   for (size_t w = 0; w < nvert; ++w) D.uvel_2d[w] = D.vvel_2d[w] = D.btractx[w] = D.btracty[w] = 0.0;
   for (int g = ip.col_begin; g < ip.col_end; ++g) {
     const size_t w = vtx(p.col_ij[g], p.col_ij[NC + g], nx);
-    D.uvel_2d[w] = x[g].x;
-    D.vvel_2d[w] = x[g].y;
+    D.uvel_2d[w] = x[p.col_node[g]].x;
+    D.vvel_2d[w] = x[p.col_node[g]].y;
     D.btractx[w] = bt[g].x;
     D.btracty[w] = bt[g].y;
   }
@@ -617,7 +646,7 @@ void gather_matrix(const HostPlan& p, const double* Auu, const double* Auv,
   for (int g = 0; g < NC; ++g) {
     const int i = p.col_ij[g], j = p.col_ij[NC + g];
     for (int k = 0; k < nz; ++k) {
-      const size_t n = (size_t)g * nz + k;
+      const size_t n = node_of(p, g, k);
       const size_t base = (vtx(i, j, nx) * nz + k) * 27;
       for (int m = 0; m < 27; ++m) {
         A[(size_t)m * np + n] = double2{Auu[base + m], Auv[base + m]};
@@ -636,7 +665,7 @@ void scatter_matrix(const HostPlan& p, const double2* A, double* Auu,
   for (int g = 0; g < NC; ++g) {
     const int i = p.col_ij[g], j = p.col_ij[NC + g];
     for (int k = 0; k < nz; ++k) {
-      const size_t n = (size_t)g * nz + k;
+      const size_t n = node_of(p, g, k);
       const size_t base = (vtx(i, j, nx) * nz + k) * 27;
       for (int m = 0; m < 27; ++m) {
         const double2 u = A[(size_t)m * np + n], v = A[(size_t)(27 + m) * np + n];
@@ -658,7 +687,7 @@ void scatter_matrix_sym(const HostPlan& p, const double2* A, double* Auu,
   for (int g = 0; g < NC; ++g) {
     const int i = p.col_ij[g], j = p.col_ij[NC + g];
     for (int k = 0; k < nz; ++k) {
-      const size_t n = (size_t)g * nz + k;
+      const size_t n = node_of(p, g, k);
       const size_t base = (vtx(i, j, nx) * nz + k) * 27;
       for (int m = 0; m < 27; ++m) {
         double uu, uv, vu, vv;
@@ -670,7 +699,7 @@ void scatter_matrix_sym(const HostPlan& p, const double2* A, double* Auu,
           const int cn = p.col_nbr[(size_t)((jA + 1) * 3 + (iA + 1)) * NC + g];
           const int kn = k + kA;
           if (cn < 0 || kn < 0 || kn >= nz) continue;
-          const size_t pn = (size_t)cn * nz + kn;
+          const size_t pn = node_of(p, cn, kn);
           const double2 b0 = A[(size_t)(13 - m) * np + pn], b1 = A[(size_t)(14 + 13 - m) * np + pn];
           uu = b0.x; uv = b1.x; vu = b0.y; vv = b1.y;
         }
@@ -690,7 +719,7 @@ void gather_matrix_sym(const HostPlan& p, const double* Auu, const double* Auv,
   for (int g = 0; g < NC; ++g) {
     const int i = p.col_ij[g], j = p.col_ij[NC + g];
     for (int k = 0; k < nz; ++k) {
-      const size_t n = (size_t)g * nz + k;
+      const size_t n = node_of(p, g, k);
       const size_t base = (vtx(i, j, nx) * nz + k) * 27;
       for (int m = 13; m < 27; ++m) {
         A[(size_t)(m - 13) * np + n] = double2{Auu[base + m], Auv[base + m]};
@@ -733,12 +762,16 @@ void scatter_elements(const HostPlan& p, int b, const double* vals, int nv,
   }
 }
 
-DevView diagnostics_view(const DevView& v, const HostPlan& p, double2* x3, const double* flwafact_layers) {
+DevView diagnostics_view(const DevView& v, const HostPlan& p, double2* x3, const double* flwafact_layers,
+                         const int* col_node3) {
   if (!p.solve2d) return v;
   DevView d = v;
   d.nz = p.nz_out;
   d.nelem = diagnostic_elements(p);
-  d.x = x3;
+  d.x = x3;  // [ncols][nz_out]: node (col, k) = col * nz_out + k
+  d.W = 1;
+  d.lsh = 0;
+  d.col_node = col_node3;
   if (!p.l1l2 && !p.diva) d.flwafact = flwafact_layers;
   return d;
 }

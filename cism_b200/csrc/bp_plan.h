@@ -30,8 +30,10 @@ struct HostPlan {
   bool diva = false;       // DIVA (3-D velocity, traction and point viscosities every iteration)
   int nefvs = 0;           // length of the element viscosity array (L1L2: ncells * (nz_out - 1))
   int ncols = 0, nnodes = 0, npad = 0, ncells = 0, nelem = 0, ntiles = 0;
+  int W = 1, lsh = 0;      // column block width and log2 (bp_common.h: node layout)
   std::vector<InstParams> inst;
   std::vector<int> col_inst, col_nbr, col_cells, col_ij;
+  std::vector<int> col_node, col_nbn;  // node of (col, 0); the neighbours' col_node [9][ncols]
   std::vector<double> col_beta;
   std::vector<double> col_slide;  // [3][ncols] (f_ground, c1, c2) when any instance has a sliding law
   bool any_sliding = false;
@@ -48,10 +50,15 @@ struct HostPlan {
   std::vector<double2> x2d_0, col_bt0;
   std::vector<uint8_t> col_ipl;
   std::vector<bp_diva> diva_io;
-  std::vector<int> tile_start, tile_end, tile_inst;
+  std::vector<int> tile_start, tile_end, tile_inst, tile_ncols, tile_col0;
   // per-instance grid sizes, for scatters
   std::vector<int> nx, ny, periodic;
 };
+
+// Node of (col, k) (the blocked level-major layout of bp_common.h).
+inline size_t node_of(const HostPlan& p, int col, int k) {
+  return (size_t)p.col_node[col] + ((size_t)k << p.lsh);
+}
 
 // Columns only (matrix-level entry points): fills columns, neighbours and
 // tiles of one instance; cells are left empty.
@@ -115,8 +122,11 @@ inline int diagnostic_elements(const HostPlan& p) { return p.ncells * (p.nz_out 
 // The device view of the post-solve diagnostics of a 2-D solve: the 3-D
 // elements over the nz_out levels, the 3-D velocity x3 [ncols][nz_out]
 // and, for the shallow-shelf solve, the per-layer flow factor
-// (flwafact_layers on the device); a 3-D solve's view is returned as is.
-DevView diagnostics_view(const DevView& v, const HostPlan& p, double2* x3, const double* flwafact_layers);
+// (flwafact_layers on the device); x3's node of (col, k) is col * nz_out + k,
+// so col_node3 holds col * nz_out per column.  A 3-D solve's view is
+// returned as is.
+DevView diagnostics_view(const DevView& v, const HostPlan& p, double2* x3, const double* flwafact_layers,
+                         const int* col_node3);
 
 // Post-solve diagnostics of instance b to the reference layout: nv element
 // fields vals[v][nelem] -> out[v] (nz-1,nx,ny), zero outside active cells

@@ -24,6 +24,10 @@ struct Emu {
   void bind() {
     std::memset(&v, 0, sizeof(v));
     v.nz = p.nz; v.ncols = p.ncols; v.nnodes = p.nnodes; v.npad = p.npad;
+    v.W = p.W; v.lsh = p.lsh;
+    v.col_node = p.col_node.data(); v.col_nbn = p.col_nbn.data();
+    v.tile_start = p.tile_start.data(); v.tile_end = p.tile_end.data(); v.tile_inst = p.tile_inst.data();
+    v.tile_ncols = p.tile_ncols.data(); v.tile_col0 = p.tile_col0.data();
     v.solve2d = p.solve2d ? 1 : 0;
     v.l1l2 = p.l1l2 ? 1 : 0;
     v.diva = p.diva ? 1 : 0;
@@ -66,12 +70,19 @@ struct Emu {
   }
 };
 
+// Every node (n, col, k) of a plan, column by column (the engine's layout:
+// node_of).
+template <typename F>
+void each_node(const HostPlan& p, F f) {
+  for (int c = 0; c < p.ncols; ++c)
+    for (int k = 0; k < p.nz; ++k) f(node_of(p, c, k), c, k);
+}
+
 template <int B>
 void rows(Emu& E, const RefTables& T) {
   const DevView& v = E.v;
   double* Ad = reinterpret_cast<double*>(E.A.data());
-  for (int n = 0; n < v.nnodes; ++n) {
-    const int col = n / v.nz, k = n - col * v.nz;
+  each_node(E.p, [&](size_t n, int col, int k) {
     double acc[27];
     row_assemble<B>(v, T, col, k, acc);
     row_basal<B>(v, T, col, k, acc);
@@ -79,7 +90,7 @@ void rows(Emu& E, const RefTables& T) {
     for (int m = 0; m < 27; ++m)
       Ad[(((size_t)((B >> 1) * 27 + m)) * v.npad + n) * 2 + (B & 1)] = acc[m];
     E.badj[(size_t)B * v.npad + n] = adj;
-  }
+  });
 }
 }  // namespace
 
@@ -105,7 +116,7 @@ extern "C" int emu_assemble(const bp_inputs* in, const double* uvel, const doubl
   }
   rows<0>(E, T); rows<1>(E, T); rows<2>(E, T); rows<3>(E, T);
   const size_t np = E.p.npad;
-  for (int n = 0; n < E.p.nnodes; ++n) {
+  for (int n = 0; n < E.p.npad; ++n) {  // the hole slots are zero
     const uint8_t dm = E.p.dmask[n];
     double u = E.p.load[n].x - E.badj[n] - E.badj[np + n];
     double w = E.p.load[n].y - E.badj[2 * np + n] - E.badj[3 * np + n];
@@ -139,16 +150,15 @@ extern "C" int emu_matvec_sym(int nx, int ny, int nz, int periodic, const int* a
   E.v.A = As.data();
   E.v.A32 = A32.data();
   E.v.A32d = A32d.data();
-  for (int n = 0; n < E.p.nnodes; ++n) make_a32_row(E.v, n / nz, n % nz, (size_t)n);
+  each_node(E.p, [&](size_t n, int col, int k) { make_a32_row(E.v, col, k, n); });
   gather_velocity(E.p, 0, xu, xv, E.x.data());
   std::vector<double2> y(E.p.npad, double2{0, 0});
   const double2* xs = E.x.data();
   auto src = [xs](size_t m) { return xs[m]; };
-  for (int n = 0; n < E.p.nnodes; ++n) {
-    const int col = n / nz, k = n - col * nz;
-    y[n] = fp32 ? matvec_row_sym32(E.v, A32.data(), col, k, (size_t)n, src)
-                : matvec_row_sym(E.v, As.data(), col, k, (size_t)n, src);
-  }
+  each_node(E.p, [&](size_t n, int col, int k) {
+    y[n] = fp32 ? matvec_row_sym32(E.v, A32.data(), col, k, n, src)
+                : matvec_row_sym(E.v, As.data(), col, k, n, src);
+  });
   const size_t tot = (size_t)nz * (nx - 1) * (ny - 1);
   std::memset(yu, 0, tot * 8);
   std::memset(yv, 0, tot * 8);
@@ -169,10 +179,7 @@ extern "C" int emu_matvec(int nx, int ny, int nz, int periodic, const int* activ
   std::vector<double2> y(E.p.npad, double2{0, 0});
   const double2* xs = E.x.data();
   auto src = [xs](size_t m) { return xs[m]; };
-  for (int n = 0; n < E.p.nnodes; ++n) {
-    const int col = n / nz, k = n - col * nz;
-    y[n] = matvec_row(E.v, E.A.data(), col, k, (size_t)n, src);
-  }
+  each_node(E.p, [&](size_t n, int col, int k) { y[n] = matvec_row(E.v, E.A.data(), col, k, n, src); });
   const size_t tot = (size_t)nz * (nx - 1) * (ny - 1);
   std::memset(yu, 0, tot * 8);
   std::memset(yv, 0, tot * 8);
@@ -205,12 +212,12 @@ extern "C" int emu_sia_apply(int nx, int ny, int nz, int periodic, const int* ac
   for (int c = 0; c < E.p.ncols; ++c) {
     for (int h = 0; h < 2; ++h) {
       for (int k = 0; k < nz; ++k) {
-        const size_t n = (size_t)c * nz + k;
+        const size_t n = node_of(E.p, c, k);
         sia_coefs(E.v, n, k, h, &sub[k], &dg[k], &sup[k]);
         s[k] = h ? E.x[n].y : E.x[n].x;
       }
       sia_column(nz, sub.data(), dg.data(), sup.data(), s.data(), 1);
-      for (int k = 0; k < nz; ++k) (h ? z[(size_t)c * nz + k].y : z[(size_t)c * nz + k].x) = s[k];
+      for (int k = 0; k < nz; ++k) (h ? z[node_of(E.p, c, k)].y : z[node_of(E.p, c, k)].x) = s[k];
     }
   }
   const size_t tot = (size_t)nz * (nx - 1) * (ny - 1);
@@ -234,7 +241,7 @@ extern "C" int emu_slide_beta(const bp_inputs* in, const double* uvel, const dou
   const int nz = E.p.nz, NC = E.p.ncols, nx = in->nx;
   const SlideParams& sp = E.p.inst[0].slide;
   for (int c = 0; c < NC; ++c) {
-    const double2 ub = E.x[(size_t)c * nz + nz - 1];
+    const double2 ub = E.x[node_of(E.p, c, nz - 1)];
     const double b = slide_beta(sp, E.p.col_slide[c], E.p.col_slide[(size_t)NC + c],
                                 E.p.col_slide[2 * (size_t)NC + c], ub.x, ub.y);
     const int i = E.p.col_ij[c], j = E.p.col_ij[NC + c];
@@ -299,7 +306,9 @@ static int diagnostics(const bp_inputs* in, const double* uvel, const double* vv
       for (int k = 0; k < nl; ++k) E.efvs[(size_t)c * nl + k] = efvs[cc * nl + k];
     }
   }
-  const DevView v = diagnostics_view(E.v, E.p, x3.data(), E.p.flwafact_layers.data());
+  std::vector<int> cn3(std::max(NC, 1));
+  for (int c = 0; c < NC; ++c) cn3[c] = c * E.p.nz_out;
+  const DevView v = diagnostics_view(E.v, E.p, x3.data(), E.p.flwafact_layers.data(), cn3.data());
   RefTables T;
   fill_ref_tables(&T);
   const size_t ne = (size_t)diagnostic_elements(E.p);
@@ -351,21 +360,22 @@ extern "C" int emu_assemble_2d(const bp_inputs* in, const double* uvel, const do
   const DevView& v = E.v;
   double* Ad = reinterpret_cast<double*>(E.A.data());
   for (int B = 0; B < 4; ++B)
-    for (int n = 0; n < v.nnodes; ++n) {
+    for (int col = 0; col < v.ncols; ++col) {
+      const size_t n = (size_t)v.col_node[col];
       double acc[27];
       double adj = 0.0;
       switch (B) {
-        case 0: row_assemble2<0>(v, T, n, acc); row_basal<0>(v, T, n, 0, acc); adj = row_dirichlet<0>(v, n, 0, acc); break;
-        case 1: row_assemble2<1>(v, T, n, acc); row_basal<1>(v, T, n, 0, acc); adj = row_dirichlet<1>(v, n, 0, acc); break;
-        case 2: row_assemble2<2>(v, T, n, acc); row_basal<2>(v, T, n, 0, acc); adj = row_dirichlet<2>(v, n, 0, acc); break;
-        default: row_assemble2<3>(v, T, n, acc); row_basal<3>(v, T, n, 0, acc); adj = row_dirichlet<3>(v, n, 0, acc); break;
+        case 0: row_assemble2<0>(v, T, col, acc); row_basal<0>(v, T, col, 0, acc); adj = row_dirichlet<0>(v, col, 0, acc); break;
+        case 1: row_assemble2<1>(v, T, col, acc); row_basal<1>(v, T, col, 0, acc); adj = row_dirichlet<1>(v, col, 0, acc); break;
+        case 2: row_assemble2<2>(v, T, col, acc); row_basal<2>(v, T, col, 0, acc); adj = row_dirichlet<2>(v, col, 0, acc); break;
+        default: row_assemble2<3>(v, T, col, acc); row_basal<3>(v, T, col, 0, acc); adj = row_dirichlet<3>(v, col, 0, acc); break;
       }
       for (int m = 0; m < 27; ++m)
         Ad[(((size_t)((B >> 1) * 27 + m)) * v.npad + n) * 2 + (B & 1)] = acc[m];
       E.badj[(size_t)B * v.npad + n] = adj;
     }
   const size_t np = E.p.npad;
-  for (int n = 0; n < E.p.nnodes; ++n) {
+  for (int n = 0; n < E.p.npad; ++n) {  // the hole slots are zero
     const uint8_t dm = E.p.dmask[n];
     double u = E.p.load[n].x - E.badj[n] - E.badj[np + n];
     double w = E.p.load[n].y - E.badj[2 * np + n] - E.badj[3 * np + n];
@@ -449,21 +459,22 @@ extern "C" int emu_diva_step(const bp_inputs* in, double* Auu, double* Auv, doub
   const DevView& v = E.v;
   double* Ad = reinterpret_cast<double*>(E.A.data());
   for (int B = 0; B < 4; ++B)
-    for (int n = 0; n < v.nnodes; ++n) {
+    for (int col = 0; col < v.ncols; ++col) {
+      const size_t n = (size_t)v.col_node[col];
       double acc[27];
       double adj = 0.0;
       switch (B) {
-        case 0: row_assemble2<0>(v, T, n, acc); row_basal<0>(v, T, n, 0, acc); adj = row_dirichlet<0>(v, n, 0, acc); break;
-        case 1: row_assemble2<1>(v, T, n, acc); row_basal<1>(v, T, n, 0, acc); adj = row_dirichlet<1>(v, n, 0, acc); break;
-        case 2: row_assemble2<2>(v, T, n, acc); row_basal<2>(v, T, n, 0, acc); adj = row_dirichlet<2>(v, n, 0, acc); break;
-        default: row_assemble2<3>(v, T, n, acc); row_basal<3>(v, T, n, 0, acc); adj = row_dirichlet<3>(v, n, 0, acc); break;
+        case 0: row_assemble2<0>(v, T, col, acc); row_basal<0>(v, T, col, 0, acc); adj = row_dirichlet<0>(v, col, 0, acc); break;
+        case 1: row_assemble2<1>(v, T, col, acc); row_basal<1>(v, T, col, 0, acc); adj = row_dirichlet<1>(v, col, 0, acc); break;
+        case 2: row_assemble2<2>(v, T, col, acc); row_basal<2>(v, T, col, 0, acc); adj = row_dirichlet<2>(v, col, 0, acc); break;
+        default: row_assemble2<3>(v, T, col, acc); row_basal<3>(v, T, col, 0, acc); adj = row_dirichlet<3>(v, col, 0, acc); break;
       }
       for (int m = 0; m < 27; ++m)
         Ad[(((size_t)((B >> 1) * 27 + m)) * v.npad + n) * 2 + (B & 1)] = acc[m];
       E.badj[(size_t)B * v.npad + n] = adj;
     }
   const size_t np = E.p.npad;
-  for (int n = 0; n < E.p.nnodes; ++n) {
+  for (int n = 0; n < E.p.npad; ++n) {  // the hole slots are zero
     const uint8_t dm = E.p.dmask[n];
     double u = E.p.load[n].x - E.badj[n] - E.badj[np + n];
     double w = E.p.load[n].y - E.badj[2 * np + n] - E.badj[3 * np + n];
@@ -530,7 +541,7 @@ extern "C" int emu_picard(const bp_inputs* in, const double* uvel, const double*
     usav = E.x;
     if (ip.slide.law != 0) {  // k_slide_beta, k_cell_beta
       for (int col = 0; col < NC; ++col) {
-        const double2 ub = P.diva ? E.x3[(size_t)col * (nl + 1) + nl] : E.x[(size_t)col * v.nz + v.nz - 1];
+        const double2 ub = P.diva ? E.x3[(size_t)col * (nl + 1) + nl] : E.x[node_of(P, col, v.nz - 1)];
         E.p.col_beta[col] = slide_beta(ip.slide, P.col_slide[col], P.col_slide[(size_t)NC + col],
                                        P.col_slide[2 * (size_t)NC + col], ub.x, ub.y);
         if (!(E.p.col_beta[col] >= 0.0)) return 9;
@@ -577,10 +588,9 @@ extern "C" int emu_picard(const bp_inputs* in, const double* uvel, const double*
     }
     double* Ad = reinterpret_cast<double*>(E.A.data());  // k_asm_rows<true>
     for (int B = 0; B < 4; ++B)
-      for (int n = 0; n < v.nnodes; ++n) {
+      each_node(P, [&](size_t n, int col, int k) {
         double acc[27];
         double adj = 0.0;
-        const int col = n / v.nz, k = n - col * v.nz;
         switch (B) {
           case 0: if (d3) row_assemble<0>(v, T, col, k, acc); else row_assemble2<0>(v, T, col, acc);
                   row_basal<0>(v, T, col, k, acc); adj = row_dirichlet<0>(v, col, k, acc); break;
@@ -593,8 +603,8 @@ extern "C" int emu_picard(const bp_inputs* in, const double* uvel, const double*
         }
         for (int m = 0; m < 27; ++m) Ad[(((size_t)((B >> 1) * 27 + m)) * np + n) * 2 + (B & 1)] = acc[m];
         E.badj[(size_t)B * np + n] = adj;
-      }
-    for (int n = 0; n < v.nnodes; ++n) {  // k_rhs
+      });
+    for (int n = 0; n < (int)np; ++n) {  // k_rhs (the hole slots are zero)
       const uint8_t dm = P.dmask[n];
       double u = P.load[n].x - E.badj[n] - E.badj[np + n];
       double w = P.load[n].y - E.badj[2 * np + n] - E.badj[3 * np + n];
@@ -603,7 +613,7 @@ extern "C" int emu_picard(const bp_inputs* in, const double* uvel, const double*
       E.b[n] = double2{u, w};
     }
     if (!d3 && !P.diva && ip.which_babc == 6) {  // a frozen bed: nothing is solved
-      for (int n = 0; n < v.nnodes; ++n) E.x[n] = double2{0.0, 0.0};
+      for (int n = 0; n < (int)np; ++n) E.x[n] = double2{0.0, 0.0};
     } else {  // the linear solve on the reference layout
       const int nzs = v.nz;
       scatter_matrix(P, E.A.data(), Auu.data(), Auv.data(), Avu.data(), Avv.data());
@@ -628,7 +638,7 @@ extern "C" int emu_picard(const bp_inputs* in, const double* uvel, const double*
       if (st == ORC_ERR_NAN) return 1;
       for (int col = 0; col < NC; ++col) {
         const size_t w = (size_t)(P.col_ij[NC + col] - 1) * (nx - 1) + (P.col_ij[col] - 1);
-        for (int k = 0; k < nzs; ++k) E.x[(size_t)col * nzs + k] = double2{xu[w * nzs + k], xv[w * nzs + k]};
+        for (int k = 0; k < nzs; ++k) E.x[node_of(P, col, k)] = double2{xu[w * nzs + k], xv[w * nzs + k]};
       }
     }
     if (P.diva)  // k_diva_velocity
@@ -636,8 +646,8 @@ extern "C" int emu_picard(const bp_inputs* in, const double* uvel, const double*
     double r = 0.0, rsum = 0.0;  // k_picard_check (2-D: no bed layer to leave out)
     long cnt = 0;
     const bool nobed = d3 && (ip.which_resid == 1 || ip.which_resid == 2);
-    for (int n = 0; n < v.nnodes; ++n) {
-      if (nobed && n % v.nz == v.nz - 1) continue;
+    each_node(P, [&](size_t n, int, int k) {
+      if (nobed && k == v.nz - 1) return;
       const double speed = std::sqrt(E.x[n].x * E.x[n].x + E.x[n].y * E.x[n].y);
       if (speed != 0.0) {
         const double old = std::sqrt(usav[n].x * usav[n].x + usav[n].y * usav[n].y);
@@ -646,7 +656,7 @@ extern "C" int emu_picard(const bp_inputs* in, const double* uvel, const double*
         rsum += d;
         ++cnt;
       }
-    }
+    });
     const double crit = ip.which_resid == 2 ? (cnt > 0 ? rsum / cnt : 0.0) : r;
     if (!(crit >= 1.0e-4)) break;
   }
