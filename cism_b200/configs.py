@@ -340,7 +340,10 @@ def gaussian_random_field(rng: np.random.Generator, shape, dx: float, corr_len: 
 def marine(n: int = 400, dx: float = 4000.0, nz: int = 11, seed: int = 2, peak: float = 3000.0,
            radius_frac: float = 0.45, front_thickness: float = 200.0, flwa: float = 1.0e-16,
            rhoi: float = 917.0, rhoo: float = 1028.0, beta_median: float = 1.0e3,
-           beta_sigma_ln: float = 1.0) -> BPModel:
+           beta_sigma_ln: float = 1.0, bed_mean: float = -200.0, bed_std: float = 600.0,
+           bed_corr: float = 40.0e3, trough_depth: float = 1500.0, trough_dir: int = 0,
+           trough_width: float = 60.0e3, beta_corr: float = 20.0e3, ny_cells: Optional[int] = None,
+           rng: Optional[np.random.Generator] = None) -> BPModel:
     """Marine ice sheet with grounding line and floating shelf (workload:
     400x400, dx = 4 km, 11 levels).
 
@@ -353,31 +356,59 @@ def marine(n: int = 400, dx: float = 4000.0, nz: int = 11, seed: int = 2, peak: 
     where rhoi H < -rhoo (b - eus).  beta is log-normal (median beta_median,
     sigma_ln, correlation length 20 km) and calcbeta zeroes it under the
     shelf through f_ground.  Chronopoulos-Gear PCG.
+
+    The keyword arguments past beta_sigma_ln vary the family for the
+    learned guess's training set (random_marine); their defaults are the
+    workload's.  trough_dir turns the trough toward the east (0), north (1),
+    west (2) or south (3) edge; ny_cells makes the domain non-square (the
+    radius then follows the shorter side).
     """
-    rng = np.random.default_rng(seed)
-    L = n * dx
-    xc = _cell_centres(n, dx)
-    X, Y = np.meshgrid(xc, xc)
-    c = L / 2.0
-    bed = -200.0 + 600.0 * gaussian_random_field(rng, (n, n), dx, 40.0e3)
-    ramp = np.clip((X - c) / (L / 2.0), 0.0, 1.0)
-    bed -= 1500.0 * ramp * np.exp(-((Y - c) ** 2) / (2 * 60.0e3 ** 2))
-    R = radius_frac * L
-    r2 = (X - c) ** 2 + (Y - c) ** 2
+    rng = np.random.default_rng(seed) if rng is None else rng
+    gx, gy = n, (n if ny_cells is None else ny_cells)
+    xc = _cell_centres(gx, dx)
+    yc = _cell_centres(gy, dx)
+    X, Y = np.meshgrid(xc, yc)
+    cx, cy = gx * dx / 2.0, gy * dx / 2.0
+    bed = bed_mean + bed_std * gaussian_random_field(rng, (gy, gx), dx, bed_corr)
+    along, across, half = [((X - cx), (Y - cy), cx), ((Y - cy), (X - cx), cy),
+                           ((cx - X), (Y - cy), cx), ((cy - Y), (X - cx), cy)][trough_dir % 4]
+    ramp = np.clip(along / half, 0.0, 1.0)
+    bed -= trough_depth * ramp * np.exp(-(across ** 2) / (2 * trough_width ** 2))
+    R = radius_frac * min(gx, gy) * dx
+    r2 = (X - cx) ** 2 + (Y - cy) ** 2
     H = peak * np.maximum(0.0, 1.0 - r2 / R ** 2)
     H = np.where(H >= front_thickness, H, 0.0)
     topg = halo_fill_cells(_embed(bed))
     thck = halo_fill_cells(_embed(H))
     usrf = calc_lsrf_usrf(thck, topg, 0.0, rhoi, rhoo)
     ny, nx = thck.shape
-    lnb = gaussian_random_field(rng, (n, n), dx, 20.0e3)
+    lnb = gaussian_random_field(rng, (gy, gx), dx, beta_corr)
     beta_v = beta_median * np.exp(beta_sigma_ln * lnb)
     beta_ext = _vertex_from_owned(beta_v)
     return BPModel(nx=nx, ny=ny, nz=nz, dx=dx, dy=dx, thck=thck, usrf=usrf, topg=topg,
                    flwa=np.full((ny, nx, nz - 1), flwa), beta_external=beta_ext,
                    eus=0.0, thklim=1.0, rhoi=rhoi, rhoo=rhoo, which_babc=BABC_BETA_EXTERNAL,
                    which_sparse=SPARSE_PCG_CHRONGEAR, which_precond=PRECOND_DIAG,
-                   which_resid=RESID_MAXU, pcg_maxiters=5000, name=f"marine{n}x{n}x{nz}")
+                   which_resid=RESID_MAXU, pcg_maxiters=5000, name=f"marine{gx}x{gy}x{nz}")
+
+
+def random_marine(rng: np.random.Generator, n: int = 256, dx: float = 2000.0, nz: int = 11,
+                  ny_cells: Optional[int] = None) -> BPModel:
+    """A member of the learned guess's training family around the marine
+    workload: the same generator with random peak thickness (2000-3500 m),
+    radius (0.35-0.48 of the domain), bed mean (-400-0 m), standard
+    deviation (300-800 m) and correlation length (20-60 km), trough depth
+    (0-1500 m) and direction, median beta (10^2.5-10^3.5 Pa a/m), its log
+    spread (0.5-1.5) and correlation length (10-40 km), and rate factor
+    (0.5-2 x 1e-16)."""
+    kw = dict(peak=rng.uniform(2000.0, 3500.0), radius_frac=rng.uniform(0.35, 0.48),
+              bed_mean=rng.uniform(-400.0, 0.0), bed_std=rng.uniform(300.0, 800.0),
+              bed_corr=rng.uniform(20.0e3, 60.0e3), trough_depth=rng.uniform(0.0, 1500.0),
+              trough_dir=int(rng.integers(0, 4)), beta_median=10.0 ** rng.uniform(2.5, 3.5),
+              beta_sigma_ln=rng.uniform(0.5, 1.5), beta_corr=rng.uniform(10.0e3, 40.0e3),
+              flwa=1.0e-16 * np.exp(rng.uniform(np.log(0.5), np.log(2.0))))
+    m = marine(n=n, dx=dx, nz=nz, ny_cells=ny_cells, rng=rng, **kw)
+    return m.copy(name=f"rmarine{m.nx - 4}x{m.ny - 4}")
 
 
 def ensemble(count: int = 256, seed: int = 3, lo: int = 32, hi: int = 192, dx: float = 2000.0,

@@ -233,7 +233,19 @@ DevView make_view(Arena& a, cudaStream_t s, const HostPlan& p, bool with_cells, 
     v.A32 = blk;
     v.A32d = reinterpret_cast<double2*>(blk + 14 * np);
   }
-  v.partials = a.get<double>(s, "partials", 3 * (size_t)std::max(p.ntiles, 1));
+  v.partials = a.get<double>(s, "partials", 3 * 4 * (size_t)std::max(p.ntiles, 1));
+  // Krylov matvecs by column march where a warp holds whole tiles (W <= 32,
+  // nz >= 8), in as many level chunks (<= 4) as give about 16 warps per SM;
+  // BP_MARCH=0 keeps the thread-per-node kernels
+  const char* me = std::getenv("BP_MARCH");
+  v.march = (p.W <= 32 && v.sym && !(me && me[0] == '0')) ? 1 : 0;
+  {
+    const long warps = ((long)p.ntiles * p.W + 31) / 32;
+    const long target = 148L * 16;
+    long nch = warps > 0 ? (target + warps - 1) / warps : 1;
+    if (const char* ce = std::getenv("BP_MARCH_CHUNKS")) nch = std::atoi(ce);
+    v.mv_chunks = (int)std::max(1L, std::min({nch, 4L, (long)std::max(1, p.nz / 2)}));
+  }
   v.tile_counter = a.get<unsigned>(s, "tile_counter", p.ninst);
   CK(cudaMemsetAsync(v.tile_counter, 0, sizeof(unsigned) * p.ninst, s));
   return v;

@@ -381,6 +381,76 @@ def guess_from_output(m: configs.BPModel, out: np.ndarray):
     return configs.halo_fill_stag(u, m.periodic), configs.halo_fill_stag(v, m.periodic)
 
 
+# ---------------------------------------------------------------------
+# fields of a prepared solve (the outputs of bp_setup, which a caller of the
+# C ABI also holds): the features of the marine-family network
+# ---------------------------------------------------------------------
+VOL0 = 1.0e9  # the solver's volume scale (glissade_velo_higher.F90:1111)
+
+
+def input_features(m: configs.BPModel, arrays: dict) -> np.ndarray:
+    """[ny_owned][nx_owned][5] at the owned vertices from bp_setup's arrays:
+    thickness stagthck (km), the driving stress -- the gravity load summed
+    over the column, per horizontal area (1e5 Pa) -- in x and y, log10 of
+    beta_internal (clamped to >= 1), and the ice mask (+1 where beta_internal
+    > 0, i.e. grounded ice, -1 floating ice, 0 no active vertex).  Zero at
+    vertices that are not active.  The surface and bed enter through the
+    driving stress and the grounded/floating mask: the load vector carries
+    rho g H grad s and the calving-front pressure, and stays continuous across
+    a periodic seam where the surface itself jumps.  The column sums run
+    level by level, as the device does."""
+    js, is_ = m.owned_vertex_slices()
+    act = np.asarray(arrays["active_vertex"])[js, is_] != 0
+    H = np.asarray(arrays["stagthck"])[js, is_]
+    lu = np.asarray(arrays["loadu"])[js, is_]
+    lv = np.asarray(arrays["loadv"])[js, is_]
+    su = np.zeros(H.shape)
+    sv = np.zeros(H.shape)
+    for k in range(lu.shape[-1]):
+        su = su + lu[..., k]
+        sv = sv + lv[..., k]
+    area = VOL0 / (m.dx * m.dy) * 1.0e-5
+    beta = np.asarray(arrays["beta_internal"])[js, is_]
+    f = np.stack([H / 1000.0, su * area, sv * area, np.log10(np.maximum(beta, 1.0)),
+                  np.where(beta > 0.0, 1.0, -1.0)], axis=-1)
+    return np.where(act[..., None], f, 0.0)
+
+
+def normalized_input(model: "UNet", f: np.ndarray) -> np.ndarray:
+    """input_features (padded) -> the network's input: (f - in_shift) *
+    in_scale at the active vertices (mask channel +-1), zero elsewhere."""
+    act = (f[..., 4] != 0.0)[..., None]
+    return np.where(act, (f - model.in_shift) * model.in_scale, 0.0)
+
+
+def padded_shape(gy: int, gx: int):
+    """The network's grid for an owned grid of gy x gx vertices: both sides
+    rounded up to multiples of 8 (three 2 x 2 poolings)."""
+    return ceil8(gy), ceil8(gx)
+
+
+def pad_grid(f: np.ndarray) -> np.ndarray:
+    """[gy][gx][C] -> [ceil8(gy)][ceil8(gx)][C], zero past the owned grid."""
+    gy, gx = f.shape[:2]
+    py, px = padded_shape(gy, gx)
+    out = np.zeros((py, px) + f.shape[2:], dtype=f.dtype)
+    out[:gy, :gx] = f
+    return out
+
+
+def guess_from_grid(m: configs.BPModel, out: np.ndarray, active: np.ndarray):
+    """Network output on the padded grid [py][px][>= 2 nz] -> halo'd (uvel,
+    vvel), zero at vertices that are not active."""
+    js, is_ = m.owned_vertex_slices()
+    u = np.zeros(m.vshape3)
+    v = np.zeros(m.vshape3)
+    gy, gx = u[js, is_].shape[:2]
+    act = (np.asarray(active)[js, is_] != 0)[..., None]
+    u[js, is_] = np.where(act, out[:gy, :gx, 0:2 * m.nz:2], 0.0)
+    v[js, is_] = np.where(act, out[:gy, :gx, 1:2 * m.nz:2], 0.0)
+    return configs.halo_fill_stag(u, m.periodic), configs.halo_fill_stag(v, m.periodic)
+
+
 def predict(net: UNet, models: Sequence[configs.BPModel]):
     """Guesses (uvel, vvel) for domains of one owned-grid size and border type."""
     torch = _torch()
