@@ -22,10 +22,16 @@
 
 #include "bp_b200.h"
 #include "bp_common.h"
+#include "bp_guess.h"
 #include "bp_kernels.h"
 #include "bp_plan.h"
 
 namespace {
+
+// A learned guess that cannot run (no network loaded, or its launch failed).
+struct GuessError {
+  const char* what;
+};
 
 struct CudaError {
   cudaError_t e;
@@ -96,6 +102,8 @@ struct bp_ctx {
   // autotuner results: (node bucket, nz, storage, precision, PCG variant)
   // -> (minb, grid) of the residual kernels, (minb_k, grid_k) of the Krylov matvecs
   std::map<std::tuple<int, int, int, int, int>, std::array<int, 4>> tuned;
+  bp::GuessNet* net = nullptr;     // the learned guess's network (bp_guess_load)
+  int net_launches = 0;            // kernels the network launched (bp_guess_launches)
 };
 
 struct bp_problem {
@@ -172,6 +180,7 @@ DevView make_view(Arena& a, cudaStream_t s, const HostPlan& p, bool with_cells, 
   UP(int, "col_cells", p.col_cells, col_cells);
   UP(int, "col_ij", p.col_ij, col_ij);
   UP(double, "col_beta", p.col_beta, col_beta);
+  UP(double, "col_h", p.col_h, col_h);
   if (p.any_sliding) UP(double, "col_slide", p.col_slide, col_slide);
   UP(double2, "load", p.load, load);
   UP(uint8_t, "dmask", p.dmask, dmask);
@@ -190,7 +199,7 @@ DevView make_view(Arena& a, cudaStream_t s, const HostPlan& p, bool with_cells, 
       UP(double, "cell_thck", p.cell_thck, cell_thck);
       UP(double, "cell_ds", p.cell_ds, cell_ds);
       UP(double, "col_ds", p.col_ds, col_ds);
-      UP(double, "col_h", p.col_h, col_h);
+
       v.lw = a.get<double>(s, "l1l2_work", 4 * (size_t)v.nl * std::max(p.ncells, 1));
       v.x3 = a.get<double2>(s, "x3", (size_t)std::max(p.ncols, 1) * (v.nl + 1));
     }
@@ -665,9 +674,18 @@ void problem_free(bp_problem* P) {
 
 void problem_set_guess(bp_problem* P, double* const* uvel, double* const* vvel) {
   std::vector<double2> x(P->plan.npad, double2{0.0, 0.0});
-  for (int b = 0; b < P->plan.ninst; ++b) gather_velocity(P->plan, b, uvel[b], vvel[b], x.data());
+  std::vector<int> learned;
+  for (int b = 0; b < P->plan.ninst; ++b) {
+    if (P->plan.guess_mode[b] == BP_GUESS_LEARNED) learned.push_back(b);
+    else gather_velocity(P->plan, b, uvel[b], vvel[b], x.data());
+  }
   CK(cudaMemcpyAsync(P->x0, x.data(), sizeof(double2) * P->plan.npad, cudaMemcpyHostToDevice, P->c->stream));
   P->h2d_bytes += sizeof(double2) * (double)P->plan.nnodes;
+  if (!learned.empty()) {  // the network's guess straight into x0, on the device
+    if (!P->c->net) throw GuessError{"guess_mode = BP_GUESS_LEARNED needs bp_guess_load"};
+    if (guess_net_run(P->c->net, P->plan, P->v, learned, P->x0, P->c->stream, &P->c->net_launches) != BP_OK)
+      throw GuessError{"the learned guess failed"};
+  }
   std::vector<double2> x3;
   if (P->plan.diva && P->plan.ncols > 0) {  // the first iteration's sliding law reads its bed level
     x3.assign((size_t)P->plan.ncols * P->plan.nz_out, double2{0.0, 0.0});
@@ -723,10 +741,10 @@ void problem_get(bp_problem* P, double* const* uvel, double* const* vvel, double
     CK(cudaMemcpyAsync(x.data(), v3 ? P->v.x3 : P->v.x, sizeof(double2) * nx, cudaMemcpyDeviceToHost,
                        P->c->stream));
   std::vector<double2> x2, bt;  // DIVA: the mean velocity and the traction
-  if (p.diva && p.ncols > 0) {
-    x2.resize(p.ncols);
+  if (p.diva && p.ncols > 0) {  // the mean velocity in node order (col_node), the traction per column
+    x2.resize(p.npad);
     bt.resize(p.ncols);
-    CK(cudaMemcpyAsync(x2.data(), P->v.x, sizeof(double2) * p.ncols, cudaMemcpyDeviceToHost, P->c->stream));
+    CK(cudaMemcpyAsync(x2.data(), P->v.x, sizeof(double2) * p.npad, cudaMemcpyDeviceToHost, P->c->stream));
     CK(cudaMemcpyAsync(bt.data(), P->v.col_bt, sizeof(double2) * p.ncols, cudaMemcpyDeviceToHost, P->c->stream));
   }
   std::vector<double> ef;
@@ -737,7 +755,7 @@ void problem_get(bp_problem* P, double* const* uvel, double* const* vvel, double
   }
   CK(cudaStreamSynchronize(P->c->stream));
   P->d2h_bytes = sizeof(double2) * (double)(v3 ? nx : (size_t)p.nnodes) +
-                 (efvs ? sizeof(double) * (double)p.nefvs : 0.0) + sizeof(double2) * 2.0 * (double)x2.size();
+                 (efvs ? sizeof(double) * (double)p.nefvs : 0.0) + sizeof(double2) * 2.0 * (double)bt.size();
   for (int b = 0; b < p.ninst; ++b) {
     if (uvel && vvel) {
       if (v3) scatter_velocity_3d(p, b, x.data(), uvel[b], vvel[b]);
@@ -797,6 +815,7 @@ int bp_destroy(bp_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   c->arena.release();
+  if (c->net) guess_net_free(c->net);
   if (c->h_cnt) cudaFreeHost(c->h_cnt);
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);
@@ -821,6 +840,10 @@ const char* bp_last_error(const bp_ctx* c) { return c ? c->err.c_str() : "no con
     c_->err = std::string(e.what) + ": " + cudaGetErrorString(e.e);    \
     return BP_ERR_CUDA;                                                \
   }                                                                    \
+  catch (const GuessError& e) {                                        \
+    c_->err = e.what;                                                  \
+    return BP_ERR_ARGS;                                                \
+  }                                                                    \
   return BP_ERR_CUDA;
 
 int bp_problem_create(bp_ctx* c, int n, const bp_inputs* in, bp_problem** out) {
@@ -844,11 +867,42 @@ int bp_problem_create(bp_ctx* c, int n, const bp_inputs* in, bp_problem** out) {
 int bp_problem_set_guess(bp_problem* P, double* const* uvel, double* const* vvel) {
   if (!P) return BP_ERR_ARGS;
   GUARD_BEGIN(P->c)
-  if (!uvel || !vvel) return BP_ERR_ARGS;
+  for (int b = 0; b < P->plan.ninst; ++b)
+    if (P->plan.guess_mode[b] != BP_GUESS_LEARNED && (!uvel || !vvel || !uvel[b] || !vvel[b])) return BP_ERR_ARGS;
   problem_set_guess(P, uvel, vvel);
+  CK(cudaStreamSynchronize(P->c->stream));
   return BP_OK;
   GUARD_END
 }
+
+int bp_problem_get_guess(bp_problem* P, double* const* uvel, double* const* vvel) {
+  if (!P) return BP_ERR_ARGS;
+  GUARD_BEGIN(P->c)
+  if (!uvel || !vvel || P->plan.l1l2 || P->plan.diva) return BP_ERR_ARGS;
+  std::vector<double2> x(P->plan.npad);
+  CK(cudaMemcpyAsync(x.data(), P->x0, sizeof(double2) * P->plan.npad, cudaMemcpyDeviceToHost, P->c->stream));
+  CK(cudaStreamSynchronize(P->c->stream));
+  for (int b = 0; b < P->plan.ninst; ++b) scatter_velocity(P->plan, b, x.data(), uvel[b], vvel[b]);
+  return BP_OK;
+  GUARD_END
+}
+
+int bp_guess_load(bp_ctx* c, const char* path) {
+  GUARD_BEGIN(c)
+  if (!path) return BP_ERR_ARGS;
+  std::string err;
+  bp::GuessNet* N = guess_net_load(path, &err);
+  if (!N) {
+    c->err = err;
+    return BP_ERR_ARGS;
+  }
+  if (c->net) guess_net_free(c->net);
+  c->net = N;
+  return BP_OK;
+  GUARD_END
+}
+
+int bp_guess_launches(bp_ctx* c) { return c ? c->net_launches : 0; }
 
 int bp_problem_run(bp_problem* P, bp_stats* stats) {
   if (!P) return BP_ERR_ARGS;

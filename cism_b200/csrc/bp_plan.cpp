@@ -320,6 +320,11 @@ bool build_plan(const bp_inputs* in, int n, HostPlan* p, std::string* err) {
       }
       p->any_sliding = true;
     }
+    if (I.guess_mode != BP_GUESS_GIVEN && (I.guess_mode != BP_GUESS_LEARNED || solve2d)) {
+      *err = "guess_mode must be BP_GUESS_GIVEN, or BP_GUESS_LEARNED for the 3-D solve";
+      return false;
+    }
+    p->guess_mode.push_back(I.guess_mode);
     p->nx.push_back(I.nx); p->ny.push_back(I.ny); p->periodic.push_back(I.periodic);
     add_columns(I.nx, I.ny, nz, I.periodic, I.active_vertex, b, p, &cms[b], &cols[b]);
     p->ncols += (int)cols[b].size();
@@ -331,6 +336,7 @@ bool build_plan(const bp_inputs* in, int n, HostPlan* p, std::string* err) {
   for (int b = 0; b < n; ++b) nblocks += ((int)cols[b].size() + p->W - 1) / p->W;
   p->npad = round_up(std::max(nblocks * p->W * nz, 1), 64);
   p->col_node.assign(NC, 0);
+  p->col_h.resize(NC);
   p->col_inst.resize(NC);
   p->col_ij.resize(2 * (size_t)NC);
   p->col_nbr.resize(9 * (size_t)NC);
@@ -377,7 +383,6 @@ bool build_plan(const bp_inputs* in, int n, HostPlan* p, std::string* err) {
     p->cell_thck.resize(NCELL);
     p->cell_ds.resize(8 * (size_t)NCELL);
     p->col_ds.resize(2 * (size_t)NC);
-    p->col_h.resize(NC);
   }
   int col_base = 0, cell_base = 0;
   for (int b = 0; b < n; ++b) {
@@ -418,6 +423,7 @@ bool build_plan(const bp_inputs* in, int n, HostPlan* p, std::string* err) {
       p->col_inst[g] = b;
       p->col_ij[g] = i;
       p->col_ij[NC + g] = j;
+      p->col_h[g] = I.stagthck[vtx(i, j, nx)];
       for (int jA = -1; jA <= 1; ++jA)
         for (int iA = -1; iA <= 1; ++iA)
           p->col_nbr[(size_t)((jA + 1) * 3 + (iA + 1)) * NC + g] = cms[b].lookup(i + iA, j + jA);
@@ -450,7 +456,6 @@ bool build_plan(const bp_inputs* in, int n, HostPlan* p, std::string* err) {
       if (l1l2) {
         p->col_ds[g] = I.l1l2->dusrf_dx[vtx(i, j, nx)];
         p->col_ds[(size_t)NC + g] = I.l1l2->dusrf_dy[vtx(i, j, nx)];
-        p->col_h[g] = I.stagthck[vtx(i, j, nx)];
       }
       if (solve2d) {
         // load summed over the levels (:2123-2137); the bed level's

@@ -41,7 +41,8 @@ struct HostPlan {
   std::vector<uint8_t> dmask;
   std::vector<int> cell_inst, cell_ij, cell_cols;
   std::vector<double> cell_s, cell_h, cell_beta, flwafact;
-  std::vector<double> cell_flwa, cell_thck, cell_ds, col_ds, col_h;  // L1L2 only (cell_thck: DIVA too)
+  std::vector<double> cell_flwa, cell_thck, cell_ds, col_ds;  // L1L2 only (cell_thck: DIVA too)
+  std::vector<double> col_h;  // stagthck at the column's vertex (L1L2, the learned guess)
   std::vector<double> flwafact_layers;  // shallow-shelf: [ncells][nz_out-1], for the element stresses
   // DIVA only: starting point viscosities [ncells][4][nl], mean velocity
   // and traction [ncols], the columns' ice-plus-land bits, and each
@@ -51,6 +52,7 @@ struct HostPlan {
   std::vector<uint8_t> col_ipl;
   std::vector<bp_diva> diva_io;
   std::vector<int> tile_start, tile_end, tile_inst, tile_ncols, tile_col0;
+  std::vector<int> guess_mode;  // per instance, bp_guess_mode
   // per-instance grid sizes, for scatters
   std::vector<int> nx, ny, periodic;
 };

@@ -307,7 +307,30 @@ class UNet:
         return out
 
     def save(self, path: str):
+        """The weights as .npz, and beside them the same as .bin for the C ABI."""
         np.savez_compressed(path, **self.state_dict())
+        if path.endswith(".npz"):
+            self.save_bin(path[:-4] + ".bin")
+
+    def save_bin(self, path: str):
+        """The weights in the flat binary form the C-ABI guess reads
+        (bp_guess_load): magic "BPUNET1" + NUL; int32 version 1, n_in, n_out,
+        levels, the channels, the number of convolutions; float32 in_shift
+        [n_in], in_scale [n_in], out_scale; per convolution (encoder levels,
+        decoder levels, head) int32 cin, cout, k3, act, K and float32 w
+        [cout][K], b [cout].  Little-endian."""
+        convs = self.convs()
+        hdr = [1, N_IN, self.n_out, len(self.channels)] + list(self.channels) + [len(convs)]
+        with open(path, "wb") as f:
+            f.write(b"BPUNET1\0")
+            f.write(np.asarray(hdr, dtype="<i4").tobytes())
+            f.write(np.asarray(self.in_shift, dtype="<f4").tobytes())
+            f.write(np.asarray(self.in_scale, dtype="<f4").tobytes())
+            f.write(np.asarray([self.out_scale], dtype="<f4").tobytes())
+            for cv in convs:
+                f.write(np.asarray([cv.cin, cv.cout, int(cv.k3), int(cv.act), cv.K], dtype="<i4").tobytes())
+                f.write(np.ascontiguousarray(cv.w.cpu().numpy(), dtype="<f4").tobytes())
+                f.write(np.ascontiguousarray(cv.b.cpu().numpy(), dtype="<f4").tobytes())
 
     @classmethod
     def load(cls, path: str) -> "UNet":

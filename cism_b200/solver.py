@@ -82,8 +82,11 @@ class Inputs(C.Structure):
         ("which_precond", C.c_int), ("maxiter_nonlinear", C.c_int), ("pcg_maxiters", C.c_int),
         ("pcg_ncheck", C.c_int), ("pcg_tol", C.c_double), ("precision", C.c_int),
         ("inner_tol", C.c_double), ("sliding", C.POINTER(Sliding)), ("approx_2d", C.c_int),
-        ("l1l2", C.POINTER(L1L2)), ("diva", C.POINTER(Diva)),
+        ("l1l2", C.POINTER(L1L2)), ("diva", C.POINTER(Diva)), ("guess_mode", C.c_int),
     ]
+
+
+GUESS_GIVEN, GUESS_LEARNED = 0, 1  # bp_guess_mode
 
 
 class Stats(C.Structure):
@@ -169,6 +172,9 @@ def lib():
         L.bp_problem_diagnostics.argtypes = [C.c_void_p, C.c_int] + [C.POINTER(_dp)] * 7
         L.bp_timer_start.argtypes = [C.c_void_p]
         L.bp_timer_stop.argtypes = [C.c_void_p, C.POINTER(C.c_float)]
+        L.bp_guess_load.argtypes = [C.c_void_p, C.c_char_p]
+        L.bp_guess_launches.argtypes = [C.c_void_p]
+        L.bp_problem_get_guess.argtypes = [C.c_void_p, C.POINTER(_dp), C.POINTER(_dp)]
         _lib = L
     return _lib
 
@@ -252,8 +258,10 @@ def sliding_struct(law: "configs.SlidingLaw", f) -> Sliding:
 
 
 def prepare(m: configs.BPModel, uvel=None, vvel=None, precision: int = FP64,
-            inner_tol: float = 1e-4) -> tuple:
-    """Host setup (bp_setup): returns (Prepared, uvel, vvel)."""
+            inner_tol: float = 1e-4, guess_mode: int = GUESS_GIVEN) -> tuple:
+    """Host setup (bp_setup): returns (Prepared, uvel, vvel).  guess_mode =
+    GUESS_LEARNED makes the solve start from the network loaded into the
+    context (Context.load_guess) instead of (uvel, vvel)."""
     nx, ny, nz = m.nx, m.ny, m.nz
     arrays = {
         "sigma": np.zeros(nz), "stagusrf": np.zeros((ny - 1, nx - 1)),
@@ -294,6 +302,7 @@ def prepare(m: configs.BPModel, uvel=None, vvel=None, precision: int = FP64,
     rc = lib().bp_setup(C.byref(ms), C.byref(sa), _p(u), _p(v), C.byref(inp))
     if rc != 0:
         raise BPError(rc, "in bp_setup")
+    inp.guess_mode = guess_mode
     return Prepared(m, arrays, inp, (keep, ms, sa)), u, v
 
 
@@ -329,6 +338,18 @@ class Context:
             msg = lib().bp_last_error(self.h)
             raise BPError(rc, msg.decode() if msg else "")
         return rc
+
+    # -- learned initial guess (bp_guess_load) -------------------------------
+    def load_guess(self, path: str):
+        """Load the U-Net weights (.bin; a .npz path means the .bin beside it)
+        into the context; inputs with guess_mode = GUESS_LEARNED then start
+        from the network's guess, formed on the device."""
+        if path.endswith(".npz"):
+            path = path[:-4] + ".bin"
+        self._check(lib().bp_guess_load(self.h, path.encode()), allow=(0,))
+
+    def guess_launches(self) -> int:
+        return int(lib().bp_guess_launches(self.h))
 
     # -- whole solve --------------------------------------------------------
     def solve_prepared(self, prep: Prepared, uvel, vvel, want_efvs=True):
@@ -434,11 +455,23 @@ class Problem:
         self.h = h
 
     def set_guess(self, uvels, vvels):
-        us = [_f64(u) for u in uvels]
-        vs = [_f64(v) for v in vvels]
-        rc = lib().bp_problem_set_guess(self.h, (_dp * self.n)(*[_p(a) for a in us]),
+        """Initial guesses per instance; None for an instance whose inputs ask
+        for the learned guess (guess_mode = GUESS_LEARNED)."""
+        us = [None if u is None else _f64(u) for u in uvels]
+        vs = [None if v is None else _f64(v) for v in vvels]
+        ptr = lambda a: C.cast(None, _dp) if a is None else _p(a)
+        rc = lib().bp_problem_set_guess(self.h, (_dp * self.n)(*[ptr(a) for a in us]),
+                                        (_dp * self.n)(*[ptr(a) for a in vs]))
+        self.ctx._check(rc, allow=(0,))
+
+    def get_guess(self):
+        """The stored initial guess of each instance (3-D solves)."""
+        us = [np.zeros(p.model.vshape3) for p in self.preps]
+        vs = [np.zeros(p.model.vshape3) for p in self.preps]
+        rc = lib().bp_problem_get_guess(self.h, (_dp * self.n)(*[_p(a) for a in us]),
                                         (_dp * self.n)(*[_p(a) for a in vs]))
         self.ctx._check(rc, allow=(0,))
+        return us, vs
 
     def run(self):
         st = (Stats * self.n)()

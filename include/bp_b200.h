@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define BP_ABI_VERSION 5
+#define BP_ABI_VERSION 6
 
 typedef struct bp_ctx bp_ctx;
 
@@ -49,6 +49,11 @@ typedef enum {
 } bp_status;
 
 typedef enum { BP_FP64 = 0, BP_MIXED = 1 } bp_precision;
+
+/* Start of the Picard loop: the caller's velocity (as the reference, which
+ * starts from the last time step's, glissade.F90:1919-1987), or the
+ * learned guess of the network loaded by bp_guess_load. */
+typedef enum { BP_GUESS_GIVEN = 0, BP_GUESS_LEARNED = 1 } bp_guess_mode;
 
 /* Velocity-dependent sliding law: calcbeta
  * (libglissade/glissade_basal_traction.F90:67-598) evaluated on the device
@@ -179,6 +184,9 @@ typedef struct {
   const bp_l1l2 *l1l2;          /* approx_2d = 3 only */
   const bp_diva *diva;          /* approx_2d = 4 only; its outputs are written by
                                    bp_solve, bp_batch_solve and bp_problem_get */
+  int guess_mode;               /* bp_guess_mode; BP_GUESS_LEARNED (the 3-D solve
+                                   only) replaces uvel/vvel on entry by the network's
+                                   guess, computed on the device; needs bp_guess_load */
 } bp_inputs;
 
 typedef struct {
@@ -268,10 +276,32 @@ int bp_residual_noalloc(int nx, int ny, int nz, int periodic,
  * ------------------------------------------------------------------ */
 typedef struct bp_problem bp_problem;
 
+/* ------------------------------------------------------------------
+ * Learned initial guess.  No counterpart in the reference, whose Picard
+ * loop starts from the velocity the caller passes (glissade.F90:1919-1987
+ * keeps the last time step's).  bp_guess_load reads the weights of a
+ * trained U-Net (the .bin file beside cism_b200/weights/unet_marine.npz)
+ * into the context; then an input with guess_mode = BP_GUESS_LEARNED
+ * starts from the network's estimate of the velocity, computed on the
+ * device from that input's own device data (thickness, gravity load, beta,
+ * active vertices) and written straight into the solve's initial guess.
+ * The solve itself is unchanged and converges to the same tolerances.
+ * Returns BP_ERR_ARGS (message in bp_last_error) for a missing or
+ * malformed file.
+ * ------------------------------------------------------------------ */
+int bp_guess_load(bp_ctx *ctx, const char *path);
+/* Kernels launched by the network since the context was created. */
+int bp_guess_launches(bp_ctx *ctx);
+
 int bp_problem_create(bp_ctx *ctx, int n, const bp_inputs *in, bp_problem **out);
 /* Upload an initial guess (n arrays (nz,nx-1,ny-1)); it is kept on the
- * device and restored at the start of every bp_problem_run. */
+ * device and restored at the start of every bp_problem_run.  Instances
+ * whose inputs set guess_mode = BP_GUESS_LEARNED take the network's guess
+ * instead, formed on the device (their array pointers may be NULL). */
 int bp_problem_set_guess(bp_problem *p, double *const *uvel, double *const *vvel);
+/* The stored initial guess of each instance, scattered like the solution
+ * (3-D solves). */
+int bp_problem_get_guess(bp_problem *p, double *const *uvel, double *const *vvel);
 /* Run the Picard solve from the stored guess entirely on device data;
  * stats (array of n, may be NULL) are filled at the end. */
 int bp_problem_run(bp_problem *p, bp_stats *stats);
