@@ -1,24 +1,35 @@
 #!/usr/bin/env python
 """Converged Blatter-Pattyn velocity solves per second on B200.
 
-Workload (default): the periodic slab on a sliding bed, 160 x 160 cells,
-dx = 0.5 km, 11 sigma levels, beta = 1000 + 1000 sin(2 pi x/L) sin(2 pi y/L),
-Glen n = 3, A = 1e-16; Picard to 1e-4 max relative speed change, every
-linear solve to a relative residual of 1e-8.  A "step" is one full
-converged solve from a zero initial guess.  Synthetic seeded inputs (no
-dataset is used).
+Default workload (c4): the learned-guess evaluation set -- held-out marine
+ice sheets drawn as the large marine configuration (seeded Gaussian-random
+bed with a trough, parabolic 3000 m sheet with a calving front, log-normal
+beta, zero under the shelf) at 256 x 256 cells, dx = 2 km, 11 sigma
+levels, Glen n = 3; `--batch` domains (default 8).  Every linear solve to
+a relative residual of 1e-8; the Picard loop to the reference's relative
+nonlinear residual criterion (which_ho_resid = 4: |A(u)u - b| / |b| < 1e-7
+before the last linear solve), whose answer does not depend on the start
+(two starts agree to ~1e-10), so every path can be held to 1e-6 of the
+plain FP64 answer.  A "step" solves every domain of the workload once.
+Synthetic seeded inputs; no dataset is used.
 
-Paths: plain FP64 GPU solve ("fp64") and FP32-inner / FP64-refined solve
-("mixed").  The headline `value` is the fastest path whose final relative
-residual is below 1e-8 and whose velocity is within 1e-6 relative L2 of
-the FP64 solution; every path is reported under "paths".
+Paths: the plain FP64 path (P: the workload's PCG variant, diagonal
+preconditioner, zero start, one domain at a time) and the additions --
+mixed precision (FP32-inner / FP64-refined), the SIA column
+preconditioner (the reference's default), batching (all domains in one
+resident problem), the learned guess (the U-Net behind the C ABI).  The
+headline `value` is learned + mixed + batched (with the column
+preconditioner and Chronopoulos-Gear); `paths` lists every path with its
+iterations and its distance to P's answer.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload c4|c2|c1|c0|c3] [--batch B]
 
 With N > 1 (torchrun) every rank solves its own replica (the solve does
 not shard across GPUs); value = all ranks' solves / max rank time.
-`--impl reference` times the CPU oracle (a restatement of the reference's
-Fortran, which cannot be compiled here) on the box's host cores.
+`--impl reference` times the CPU oracle (a C restatement of the
+reference's Fortran, which cannot be compiled here) single-threaded on
+one host core, on bounded samples of the same workload.
 """
 from __future__ import annotations
 
@@ -38,48 +49,139 @@ sys.path.insert(0, ROOT)
 METRIC = "converged velocity solves/sec @1e-8 rel resid: learned+mixed vs plain FP64, 1 B200"
 UNIT = "solves/s"
 WORKLOAD_DESC = {
-    "c1": "periodic slab 160x160 cells x 11 levels, dx=0.5 km, sinusoidal beta, Glen n=3 (BP Picard+PCG)",
-    "c0": "parabolic dome 31x31 cells x 10 levels, dx=2 km, no-slip bed (BP Picard+PCG)",
-    "c2": "marine ice sheet 400x400 cells x 11 levels, dx=4 km, grounding line + shelf (BP Picard+CG-PCG)",
+    "c4": "held-out marine ice sheets 256x256 cells x 11 levels, dx=2 km, grounding line + shelf + calving front "
+          "(drawn as the 400x400 marine configuration); learned guess + mixed + batched vs plain FP64",
+    "c2": "marine ice sheet 400x400 cells x 11 levels, dx=4 km, grounding line + shelf + calving front",
+    "c1": "periodic slab 160x160 cells x 11 levels, dx=0.5 km, sinusoidal beta, Glen n=3",
+    "c0": "parabolic dome 31x31 cells x 10 levels, dx=2 km, no-slip bed",
+    "c3": "ensemble of domes and slabs, 32-192 cells per side x 11 levels, dx=2 km, log-normal beta",
 }
-# FP64 Picard/PCG iteration counts of one converged solve of each workload
-# (the same algorithm runs in the oracle; the parity tests check the counts
-# agree).  Used to extrapolate the bounded CPU samples to whole solves.
+PICARD = {"l2rel": 4, "maxu": 0}
+PICARD_DESC = {4: "relative nonlinear residual |A(u)u-b|/|b| < 1e-7 (which_ho_resid = 4)",
+               0: "max relative speed change < 1e-4 (which_ho_resid = 0)"}
+# per-domain Picard / PCG iteration counts of the plain FP64 path, by
+# workload, used to extrapolate the bounded CPU samples to whole solves
 ITERATION_COUNTS = os.path.join(ROOT, "profiles", "iteration_counts.json")
+WEIGHTS = {"c4": "unet_marine", "c2": "unet_marine"}
+HELDOUT_SEED = 70000  # past every training seed of the marine network
+ASM_FLOP_PER_ELEMENT = 18.1e3  # 8 quadrature points x ~2.2k + scatter (FP64)
 
 
-def parse_args():
+def parse_args(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c1", choices=sorted(WORKLOAD_DESC))
-    ap.add_argument("--precision", default="best",
-                    help="best | fp64 | mixed, with optional sia_/learned_ start and _colpc preconditioner")
-    ap.add_argument("--pcg-maxiters", type=int, default=3000)
+    ap.add_argument("--workload", default="c4", choices=sorted(WORKLOAD_DESC))
+    ap.add_argument("--batch", type=int, default=8, help="c4 / c3: domains of the workload")
+    ap.add_argument("--picard", default="l2rel", choices=sorted(PICARD))
+    ap.add_argument("--paths", default="all", help="comma-separated path names, or all")
+    ap.add_argument("--other-steps", type=int, default=1, help="timed steps of the non-headline paths")
+    ap.add_argument("--pcg-maxiters", type=int, default=5000)
     ap.add_argument("--refine-eta", type=float, default=1e-4,
                     help="mixed path: residual reduction of one FP32 refinement cycle")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--batch-family", default="slab", choices=["slab", "c3"])
-    ap.add_argument("--batch-eval", type=int, default=0,
-                    help="measure B: N held-out slabs, plain one at a time vs learned+mixed batched")
     ap.add_argument("--profile-run", action="store_true",
-                    help="one untimed solve (for ncu launch lists / captures)")
+                    help="one untimed run of --paths (first path) (for ncu launch lists / captures)")
     ap.add_argument("--picard-cap", type=int, default=0,
                     help="with --profile-run: stop after this many Picard iterations")
-    ap.add_argument("--kernel-sweep", action="store_true",
-                    help="time matvec storage / occupancy / grid variants on the workload")
-    return ap.parse_args()
+    return ap.parse_args(argv)
 
 
-def make_model(name, pcg_maxiters):
+# ---------------------------------------------------------------------------
+# workloads and paths
+# ---------------------------------------------------------------------------
+def make_models(args):
     from cism_b200 import configs
 
-    m = configs.workload(name)
+    w = args.workload
+    if w == "c4":
+        ms = [configs.marine(n=256, dx=2000.0, seed=HELDOUT_SEED + i) for i in range(args.batch)]
+    elif w == "c3":
+        ms = configs.ensemble(count=args.batch)
+    else:
+        ms = [configs.workload(w)]
     # the reference hard-codes maxiters = 200 (glissade_velo_higher_pcg.F90:67-69),
     # which does not reach 1e-8 on these systems; the metric needs converged solves
-    return m.copy(pcg_maxiters=pcg_maxiters)
+    return [m.copy(pcg_maxiters=args.pcg_maxiters, which_resid=PICARD[args.picard]) for m in ms]
+
+
+class Path:
+    """One way of solving the workload: start (zero | learned), precision,
+    preconditioner (the workload's | SIA column), PCG variant (the
+    workload's | Chronopoulos-Gear), batched (all domains in one resident
+    problem) or one domain at a time."""
+
+    def __init__(self, name, start, mixed, colpc, cg, batched):
+        self.name, self.start, self.mixed, self.colpc, self.cg, self.batched = name, start, mixed, colpc, cg, batched
+
+    def model(self, m):
+        from cism_b200 import configs
+
+        if self.colpc:
+            m = m.copy(which_precond=configs.PRECOND_SIA)
+        if self.cg:
+            m = m.copy(which_sparse=configs.SPARSE_PCG_CHRONGEAR)
+        return m
+
+    def describe(self):
+        return {"start": self.start, "precision": "fp32-inner/fp64-refined" if self.mixed else "fp64",
+                "preconditioner": "sia_column" if self.colpc else "workload's (diagonal)",
+                "pcg": "chronopoulos_gear" if self.cg else "workload's",
+                "domains": "batched in one problem" if self.batched else "one at a time"}
+
+
+def paths_for(args, have_net):
+    multi = args.workload in ("c4", "c3")
+    P = [Path("plain_fp64", "zero", False, False, False, False),
+         Path("fp64_colpc", "zero", False, True, False, False),
+         Path("mixed_colpc_cg" + ("_batched" if multi else ""), "zero", True, True, True, multi)]
+    if have_net:
+        P += [Path("learned_fp64_colpc" + ("_batched" if multi else ""), "learned", False, True, False, multi),
+              Path("learned_mixed_colpc_cg" + ("_batched" if multi else ""), "learned", True, True, True, multi)]
+    if args.paths != "all":
+        want = args.paths.split(",")
+        P = [p for p in P if p.name in want]
+    return P
+
+
+def headline_name(paths):
+    names = [p.name for p in paths]
+    for n in names[::-1]:
+        if n.startswith("learned_mixed"):
+            return n
+    return names[-1]
+
+
+def weights_path(workload):
+    name = WEIGHTS.get(workload)
+    if not name:
+        return None
+    p = os.path.join(ROOT, "cism_b200", "weights", name + ".bin")
+    return p if os.path.exists(p) else None
+
+
+def workload_stats(models):
+    """Columns and nodes of the workload (host setup only)."""
+    import numpy as np
+
+    from cism_b200 import solver
+
+    cols = 0
+    for m in models:
+        prep, _, _ = solver.prepare(m)
+        js, is_ = m.owned_vertex_slices()
+        cols += int(np.count_nonzero(np.asarray(prep.arrays["active_vertex"])[js, is_]))
+    return cols, cols * models[0].nz
+
+
+def config_dict(args, models, cols, nodes, world=1):
+    return {"workload": WORKLOAD_DESC[args.workload], "name": args.workload, "domains": len(models),
+            "columns": cols, "nodes": nodes, "pcg_maxiters": args.pcg_maxiters, "pcg_tol": 1e-8,
+            "picard_criterion": PICARD_DESC[PICARD[args.picard]],
+            "l2": "inputs larger than L2 (FP64 matrix %.0f MB > 126 MB)" % (nodes * 448 / 1e6),
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
 
 
 # ---------------------------------------------------------------------------
@@ -198,28 +300,29 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def matvec_traffic(nodes, precision):
-    """DRAM bytes per launch of the dominant kernel from the committed ncu
-    summary (bytes per node, scaled to this workload), or None."""
+def committed_traffic(precision):
+    """DRAM bytes per node of the dominant kernel from the committed ncu
+    summary (profiles/ncu_traffic.json), or None."""
     p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     if not os.path.exists(p):
         return None
     d = json.load(open(p))
-    k = d.get("fp32_inner" if "mixed" in precision.split("_") else "fp64_pcg")
-    if not k:
-        return None
-    return k["dram_bytes_per_node"] * nodes
+    k = d.get("fp32_inner" if precision == "mixed" else "fp64_pcg")
+    return k if k else None
 
 
 # ---------------------------------------------------------------------------
-# CPU baseline: bounded sample of the oracle, extrapolated to a whole solve
+# CPU baseline: bounded sample of the oracle, extrapolated to whole solves
 # ---------------------------------------------------------------------------
-def cpu_sample(workload, pcg_maxiters, counts, iters=(20, 200)):
+def cpu_sample(m, counts, iters=(20, 60)):
+    """Setup, one assembly and two PCG runs of the oracle (the checker, a C
+    restatement of the reference) on domain m, 1 thread; the per-iteration
+    time and the fixed costs extrapolated to `counts` (Picard, PCG)
+    iterations of a converged solve."""
     import numpy as np
 
     from oracle import oracle  # the checker
 
-    m = make_model(workload, pcg_maxiters)
     t0 = time.perf_counter()
     su = oracle.setup(m)
     t_setup = time.perf_counter() - t0
@@ -234,58 +337,110 @@ def cpu_sample(workload, pcg_maxiters, counts, iters=(20, 200)):
                    variant=m.which_sparse if m.which_sparse in (2, 3) else 2, maxiters=it, tol=0.0)
         ts.append(time.perf_counter() - t0)
     t_iter = (ts[1] - ts[0]) / (iters[1] - iters[0])
-    t_pcg_fixed = ts[0] - iters[0] * t_iter  # preconditioner setup + initial residual
-    P, I = counts["picard_iters"], counts["pcg_iters_total"]
-    t_solve = t_setup + P * (t_asm + t_pcg_fixed) + I * t_iter
-    sample = (f"oracle port (C, 1 thread): setup + one assembly + {iters[0]} and {iters[1]} PCG "
-              f"iterations of the {workload} system, extrapolated to {P} Picard / {I} PCG iterations "
-              f"per converged solve")
-    return {"solves_per_s": 1.0 / t_solve, "t_setup": t_setup, "t_assembly": t_asm,
-            "t_pcg_iter": t_iter, "t_solve_est": t_solve, "sample": sample,
+    t_pcg_fixed = max(ts[0] - iters[0] * t_iter, 0.0)  # preconditioner setup + initial residual
+    Pc, I = counts
+    t_solve = t_setup + Pc * (t_asm + t_pcg_fixed) + I * t_iter
+    return {"t_solve_est": t_solve, "t_setup": t_setup, "t_assembly": t_asm, "t_pcg_iter": t_iter,
             "sample_seconds": t_setup + t_asm + sum(ts)}
 
 
 def load_counts(workload):
     if os.path.exists(ITERATION_COUNTS):
         d = json.load(open(ITERATION_COUNTS))
-        if workload in d:
-            return d[workload]
+        return d.get(workload)
     return None
 
 
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
-def _net_launches():
-    mod = sys.modules.get("cism_b200.net")
-    return mod.LAUNCHES if mod is not None else 0
+def run_path(ctx, path, models, args, D, steps, warmup, weights, clocks=None):
+    """Time `steps` steps of one path (each solves every domain once);
+    returns timings, stats, solutions and, for batched paths, the problem."""
+    import numpy as np
+
+    from cism_b200 import solver
+
+    prec = solver.MIXED if path.mixed else solver.FP64
+    mode = solver.GUESS_LEARNED if path.start == "learned" else solver.GUESS_GIVEN
+    ms_ = [path.model(m) for m in models]
+    preps = [solver.prepare(m, precision=prec, inner_tol=args.refine_eta, guess_mode=mode)[0] for m in ms_]
+    zeros = [np.zeros(m.vshape3) for m in ms_]
+    probs = [ctx.problem(preps)] if path.batched else [ctx.problem([p]) for p in preps]
+
+    def guesses(pb):
+        return [None if mode == solver.GUESS_LEARNED else z for z in zeros[:pb.n]]
+
+    def step():
+        sts = []
+        for pb in probs:
+            pb.set_guess(guesses(pb), guesses(pb))  # learned: the network runs on the device here
+            sts += pb.run()
+        return sts
+
+    for _ in range(warmup):
+        step()
+    D.barrier()
+    g0 = ctx.guess_launches()
+    if clocks:
+        clocks.start()
+    ctx.timer_start()
+    t0 = time.perf_counter()
+    sts = [step() for _ in range(steps)][-1]
+    wall = (time.perf_counter() - t0) * 1000.0
+    ms = ctx.timer_stop()
+    ck = clocks.stop() if clocks else None
+    D.barrier()
+    guess_launches = (ctx.guess_launches() - g0) // max(1, steps)
+    ms = D.max(max(ms, wall))
+    sols = []
+    for pb in probs:
+        us, vs, _ = pb.get()
+        sols += list(zip(us, vs))
+    return {"ms": ms, "ms_per_step": ms / steps, "steps": steps, "stats": sts, "sols": sols, "probs": probs,
+            "preps": preps, "clocks": ck, "guess_launches_per_step": guess_launches}
 
 
-def path_spec(path, m):
-    """(start, precision, model) of a bench path: 'fp64' | 'mixed' with an
-    optional start prefix ('sia_', 'learned_') and suffix '_colpc' for the
-    SIA column preconditioner (the reference's default which_ho_precond = 2)
-    in place of the workload's configured diagonal one; '_cg' for the
-    Chronopoulos-Gear PCG variant."""
-    from cism_b200 import configs, solver
+def kernel_profile(res, models):
+    """One timing run (CUDA events around every launch, graphs off) of a
+    path's problems: Krylov matvec time and bytes, assembly time, launches."""
+    import numpy as np
 
-    parts = path.split("_")
-    start = parts[0] if parts[0] in ("sia", "learned") else "zero"
-    prec = solver.MIXED if "mixed" in parts else solver.FP64
-    mp = m.copy(which_precond=configs.PRECOND_SIA) if "colpc" in parts else m
-    if "cg" in parts:  # the single-reduction Chronopoulos-Gear recurrence
-        mp = mp.copy(which_sparse=configs.SPARSE_PCG_CHRONGEAR)
-    return start, prec, mp
+    t_mv = n_mv = t_asm = n_asm = 0.0
+    n64 = n32 = 0.0
+    launches = 0
+    info = None
+    for pb in res["probs"]:
+        pb.timing(True)
+        g = [None if p.inputs.guess_mode else np.zeros(p.model.vshape3) for p in pb.preps]
+        pb.set_guess(g, g)
+        pb.run()
+        kt = pb.kernel_times()
+        a, b, minb, grid = pb.mv_nodes()
+        n64 += a
+        n32 += b
+        t_mv += kt["pcg_matvec_fp64"][0]
+        n_mv += kt["pcg_matvec_fp64"][1]
+        t_asm += kt["assembly_qp"][0] + kt["assembly_rows"][0]
+        n_asm += kt["assembly_rows"][1]
+        launches += sum(n for _, n in kt.values())
+        pb.timing(False)
+        inf = pb.info()
+        if info is None:
+            info = dict(inf)
+        else:
+            for k in ("nodes", "columns", "elements", "matvec_bytes_fp64", "matvec_bytes_fp32"):
+                info[k] += inf[k]
+    return {"t_mv_ms": t_mv, "n_mv": n_mv, "n64": n64, "n32": n32, "t_asm_ms": t_asm, "n_asm": n_asm,
+            "launches": launches, "info": info}
 
 
-def load_guess_net(m):
-    """The trained U-Net for the workload's domain family, if shipped."""
-    path = os.path.join(ROOT, "cism_b200", "weights", "unet_slab.npz")
-    if not (m.periodic and os.path.exists(path)):
-        return None
-    from cism_b200 import net
+def rel_l2(a, b):
+    import numpy as np
 
-    return net.UNet.load(path)
+    num = math.sqrt(float(np.sum((a[0] - b[0]) ** 2 + (a[1] - b[1]) ** 2)))
+    den = math.sqrt(float(np.sum(b[0] ** 2 + b[1] ** 2)))
+    return num / den if den > 0 else num
 
 
 def run_ours(args, D):
@@ -294,417 +449,206 @@ def run_ours(args, D):
     from cism_b200 import solver
 
     ctx = solver.Context(D.local)
-    m = make_model(args.workload, args.pcg_maxiters)
-    net_model = load_guess_net(m)
-    if args.precision == "best":
-        paths = ["fp64", "mixed", "sia_fp64", "fp64_colpc"]
-        if net_model is not None:
-            paths += ["learned_fp64", "learned_mixed", "learned_fp64_colpc", "learned_mixed_colpc",
-                      "learned_mixed_colpc_cg"]
-    else:
-        paths = [args.precision]
+    models = make_models(args)
+    weights = weights_path(args.workload)
+    if weights:
+        ctx.load_guess(weights)
+    paths = paths_for(args, weights is not None)
+    head = headline_name(paths)
     res = {}
-    sol = {}
-    for path in paths:
-        start, prec, mp = path_spec(path, m)
-        prep, u0, v0 = solver.prepare(mp, precision=prec, inner_tol=args.refine_eta)
-        prob = ctx.problem([prep])
-
-        def make_guess():
-            # the guess is part of every timed step (network inference included)
-            if start == "learned":
-                from cism_b200 import guess
-                return guess.learned_guesses(net_model, [mp])[0]
-            if start == "sia":
-                from cism_b200 import guess
-                return guess.sia_guess(mp)
-            return u0, v0
-
-        def step():
-            gu, gv = make_guess()
-            prob.set_guess([gu], [gv])
-            return prob.run()[0]
-
-        for _ in range(args.warmup):
-            step()
-        D.barrier()
-        clocks = Clocks(D.local)
-        clocks.start()
-        ctx.timer_start()
-        t0 = time.perf_counter()
-        net_l0 = _net_launches()
-        sts = [step() for _ in range(args.steps)]
-        wall = (time.perf_counter() - t0) * 1000.0
-        net_launches = (_net_launches() - net_l0) // max(1, args.steps)
-        ms = ctx.timer_stop()
-        ck = clocks.stop()
-        D.barrier()
-        # device time of the solver stream; with a guess computed on the host
-        # or by the network on another stream, the wall time of the steps
-        ms_max = D.max(ms if start == "zero" else max(ms, wall))
-        us, vs, _ = prob.get()
-        sol[path] = (us[0], vs[0])
-        guess_err = None
-        if start != "zero":  # the guess against this path's converged answer, owned vertices
-            gu, gv = make_guess()
-            js, is_ = mp.owned_vertex_slices()
-            du, dv = (gu - us[0])[js, is_], (gv - vs[0])[js, is_]
-            guess_err = math.sqrt(float(np.sum(du ** 2 + dv ** 2)) /
-                                  float(np.sum(us[0][js, is_] ** 2 + vs[0][js, is_] ** 2)))
-        st = sts[-1]
-        # kernel timing pass (CUDA events around every launch, graphs off)
-        prob.timing(True)
-        st_t = prob.run()[0]
-        kt = prob.kernel_times()
-        n64, n32, minb, grid = prob.mv_nodes()
-        prob.timing(False)
-        info = prob.info()
-        info.update({"mv_nodes_fp64": n64, "mv_nodes_fp32": n32, "tuned_minb": minb, "tuned_grid": grid})
-        launches = sum(n for _, n in kt.values()) + net_launches
-        res[path] = {"value": D.world * args.steps / (ms_max / 1000.0), "ms_per_step": ms_max / args.steps,
-                     "make_guess": make_guess, "guess_rel_err": guess_err,
-                     "status": st["status"], "picard_iters": st["picard_iters"],
-                     "pcg_iters_total": st["pcg_iters_total"], "refine_steps": st["refine_steps_total"],
-                     "final_rel_resid": st["pcg_err_last"], "kernel_times": kt, "info": info,
-                     "launches_per_step": launches, "clocks": ck, "prep": prep, "prob": prob,
-                     "u0": u0, "v0": v0, "timing_status": st_t["status"]}
-    # accuracy of each path against the FP64 solution
-    if "fp64" in sol:
-        uf, vf = sol["fp64"]
-        den = math.sqrt(float(np.sum(uf ** 2 + vf ** 2)))
-        for path, (u, v) in sol.items():
-            res[path]["rel_l2_vs_fp64"] = math.sqrt(float(np.sum((u - uf) ** 2 + (v - vf) ** 2))) / den
-    # accepted: the reference's convergence criteria met (Picard max speed
-    # change < 1e-4, last linear solve < 1e-8) and, from the same start, the
-    # FP64 answer within 1e-6; from another start the Picard iteration stops
-    # at a different point of the same tolerance, so there within 1e-3
-    ok = [p for p in paths if res[p]["status"] == 0 and res[p]["final_rel_resid"] < 1e-8
-          and res[p].get("rel_l2_vs_fp64", 0.0) <= (1e-6 if p in ("fp64", "mixed") else 1e-3)]
-    # from the same start with another preconditioner the linear solves stop
-    # at other points of the same 1e-8 tolerance: also within 1e-3
-    head = max(ok, key=lambda p: res[p]["value"]) if ok else paths[0]
+    for p in paths:
+        is_head = p.name == head
+        res[p.name] = run_path(ctx, p, models, args, D, args.steps if is_head else args.other_steps,
+                               args.warmup if is_head else 1, weights,
+                               clocks=Clocks(D.local) if is_head else None)
     H = res[head]
-    # e2e: the C-ABI call with host buffers (plan, H2D, solve, D2H per step)
-    prep = H["prep"]
+    ref_sol = res["plain_fp64"]["sols"] if "plain_fp64" in res else H["sols"]
+    nd = len(models)
+    out_paths = {}
+    for p in paths:
+        r = res[p.name]
+        sts = r["stats"]
+        errs = [rel_l2(a, b) for a, b in zip(r["sols"], ref_sol)]
+        out_paths[p.name] = p.describe() | {
+            "value": round(nd * D.world / (r["ms_per_step"] / 1000.0), 4),
+            "ms_per_step": round(r["ms_per_step"], 2), "steps": r["steps"],
+            "status": sorted({int(s["status"]) for s in sts}),
+            "picard_iters_mean": round(float(np.mean([s["picard_iters"] for s in sts])), 2),
+            "pcg_iters_mean": round(float(np.mean([s["pcg_iters_total"] for s in sts])), 1),
+            "final_rel_resid_max": float("%.3e" % max(s["pcg_err_last"] for s in sts)),
+            "rel_l2_vs_plain_fp64_max": float("%.3e" % max(errs))}
+    # accepted: every domain converged (status 0, last linear solve < 1e-8)
+    # and within 1e-6 relative L2 of the plain FP64 answer
+    hd = out_paths[head]
+    ok = hd["status"] == [0] and hd["final_rel_resid_max"] < 1e-8 and hd["rel_l2_vs_plain_fp64_max"] <= 1e-6
+    # e2e: the C-ABI call a user makes (bp_batch_solve on host arrays: the
+    # guess, H2D, the solve and D2H inside every step)
+    hp = [p for p in paths if p.name == head][0]
+    preps = H["preps"]
+    zeros = [np.zeros(p.model.vshape3) for p in preps]
+    groups = [list(range(len(preps)))] if hp.batched else [[i] for i in range(len(preps))]
+
+    def e2e_step():
+        st = []
+        for g in groups:  # uvel/vvel: the start (unless learned) in, the solution out
+            st += ctx.batch_solve([preps[i] for i in g], [zeros[i] for i in g], [zeros[i] for i in g])[3]
+        return st
+
     for _ in range(max(1, args.warmup // 2)):
-        gu, gv = H["make_guess"]()
-        ctx.solve_prepared(prep, gu, gv, want_efvs=False)
+        e2e_step()
     D.barrier()
     ctx.timer_start()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        gu, gv = H["make_guess"]()
-        _, _, _, st_e = ctx.solve_prepared(prep, gu, gv, want_efvs=False)
-    ms_e = ctx.timer_stop()
-    wall_e = (time.perf_counter() - t0) * 1000.0
+        st_e = e2e_step()
+    ms_e = max(ctx.timer_stop(), (time.perf_counter() - t0) * 1000.0)
     D.barrier()
-    ms_e = D.max(max(ms_e, wall_e))
-    e2e = {"value": D.world * args.steps / (ms_e / 1000.0), "unit": UNIT,
-           "h2d_bytes_per_step": int(st_e["h2d_bytes"]), "d2h_bytes_per_step": int(st_e["d2h_bytes"]),
-           "call": "guess (host fields -> network on the GPU -> host) + bp_solve (C ABI) on host arrays"
-                   if head.startswith("learned") else "bp_solve (C ABI) on host arrays"}
-    # roofline of the dominant kernel: the Krylov matvec (FP32 matrix until
-    # the true residual reaches the switch tolerance on the mixed path)
-    kms, kn = H["kernel_times"]["pcg_matvec_fp64"]
-    info = H["info"]
+    ms_e = D.max(ms_e)
+    e2e = {"value": round(nd * D.world * args.steps / (ms_e / 1000.0), 4), "unit": UNIT,
+           "h2d_bytes_per_step": int(sum(s["h2d_bytes"] for s in st_e)),
+           "d2h_bytes_per_step": int(sum(s["d2h_bytes"] for s in st_e)),
+           "call": "bp_batch_solve (C ABI) on host arrays, learned guess formed on the device inside the call"
+                   if hp.start == "learned" else "bp_batch_solve (C ABI) on host arrays"}
+    # roofline of the dominant kernel and assembly FLOP/s (timing run)
+    kp = kernel_profile(H, models)
+    info = kp["info"]
     N = info["nodes"]
-    b64 = info["matvec_bytes_fp64"] / N
-    b32 = info["matvec_bytes_fp32"] / N
-    total_bytes = info["mv_nodes_fp64"] * b64 + info["mv_nodes_fp32"] * b32
-    bytes_launch = total_bytes / max(kn, 1)
+    b64, b32 = info["matvec_bytes_fp64"] / N, info["matvec_bytes_fp32"] / N
+    total_bytes = kp["n64"] * b64 + kp["n32"] * b32
     peak, peak_src = measured_peaks()
-    avg_s = (kms / max(kn, 1)) / 1000.0
-    achieved = total_bytes / (kms / 1000.0) / 1e9 if kn else 0.0
-    traffic = matvec_traffic(N, head)
+    achieved = total_bytes / (kp["t_mv_ms"] / 1000.0) / 1e9 if kp["n_mv"] else 0.0
+    tr = committed_traffic("mixed" if hp.mixed else "fp64")
     roof = {"bound": "hbm",
-            "kernel": (("k_cg_mv" if "cg" in head.split("_") else "k_std_mv") +
-                       ("<ST_SYM32> (Krylov matvec, FP32 symmetric matrix, row-sum compensated FP64 diagonal)"
-                        if "mixed" in head.split("_") else "<ST_SYM> (Krylov matvec, FP64 symmetric matrix)")),
+            "kernel": "k_krylov_march<%s> (Krylov matvec, column march, %s)" % (
+                "MV_CG1" if hp.cg else "MV_STD_A",
+                "FP32 half storage + compensated FP64 diagonal" if hp.mixed else "FP64 half storage"),
             "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-            "frac": round(achieved / peak, 4), "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)",
-            "traffic": traffic, "algorithmic_bytes_per_launch": round(bytes_launch),
-            "avg_launch_us": round(avg_s * 1e6, 2), "launches_timed": kn,
-            "fp32_share": round(info["mv_nodes_fp32"] / max(1.0, info["mv_nodes_fp32"] + info["mv_nodes_fp64"]), 3),
-            "autotuned": {"min_ctas_per_sm": info["tuned_minb"], "grid": info["tuned_grid"]}}
+            "frac": round(achieved / peak, 4) if peak else None,
+            "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)",
+            "traffic": round(tr["dram_bytes_per_node"] * N) if tr else None,
+            "traffic_source": (tr["source"] + "; bytes per node scaled to this workload's nodes") if tr else None,
+            "algorithmic_bytes_per_launch": round(total_bytes / max(kp["n_mv"], 1)),
+            "algorithmic_bytes_per_node": {"fp32": b32, "fp64": b64},
+            "avg_launch_us": round(kp["t_mv_ms"] / max(kp["n_mv"], 1) * 1e3, 2),
+            "launches_timed": int(kp["n_mv"]),
+            "fp32_share": round(kp["n32"] / max(1.0, kp["n32"] + kp["n64"]), 3)}
+    asm_flop = info["elements"] * ASM_FLOP_PER_ELEMENT
+    asm = {"flop_per_assembly": asm_flop, "ms_per_assembly": round(kp["t_asm_ms"] / max(kp["n_asm"], 1), 3),
+           "achieved_tflops": round(asm_flop / (kp["t_asm_ms"] / max(kp["n_asm"], 1) / 1000.0) / 1e12, 3)
+           if kp["n_asm"] else None,
+           "peak_tflops": 37.0, "peak_source": "nominal FP64 (no measured FP64 peak on this pool)",
+           "flop_count": "18.1k FP64 flops per element (8 quadrature points x Jacobian, inverse, strain, "
+                         "viscosity and 64 block pairs x 28, plus the row gather)"}
+    if asm["achieved_tflops"] is not None:
+        asm["frac"] = round(asm["achieved_tflops"] / asm["peak_tflops"], 4)
+    cols, nodes = info["columns"], info["nodes"]
     out = {
-        "metric": METRIC, "value": round(H["value"], 4), "unit": UNIT, "n_gpus": D.world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(H["ms_per_step"], 3),
+        "metric": METRIC, "value": out_paths[head]["value"], "unit": UNIT, "n_gpus": D.world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": out_paths[head]["ms_per_step"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": ("f32+f64" if "mixed" in head.split("_") else "f64") + ("+bf16" if head.startswith("learned") else ""),
+        "dtype": ("f32+f64" if hp.mixed else "f64") + ("+bf16" if hp.start == "learned" else ""),
         "data": "synthetic (seeded geometry generator, no dataset)",
-        "config": {"workload": WORKLOAD_DESC[args.workload], "name": args.workload, "path": head,
-                   "nodes": H["info"]["nodes"], "columns": H["info"]["columns"],
-                   "pcg_maxiters": args.pcg_maxiters, "pcg_tol": 1e-8, "picard_tol": 1e-4,
-                   "l2": "inputs larger than L2 (FP64 matrix %.0f MB > 126 MB)" % (
-                       H["info"]["nodes"] * 864 / 1e6),
-                   "parallelism": f"replicas x{D.world}" if D.world > 1 else "single GPU"},
-        "e2e": e2e,
-        "roofline": roof,
-        "gpu_launches": H["launches_per_step"] * args.steps,
-        "clocks": H["clocks"],
-        "paths": {p: {k: (round(v, 6) if isinstance(v, float) else v) for k, v in r.items()
-                      if k in ("value", "ms_per_step", "status", "picard_iters", "pcg_iters_total",
-                               "refine_steps")}
-                  | {"final_rel_resid": float("%.3e" % r["final_rel_resid"]),
-                     "start": path_spec(p, m)[0],
-                     "preconditioner": "sia_column" if "colpc" in p else "diagonal",
-                     "pcg": "chronopoulos_gear" if "cg" in p.split("_") else "standard",
-                     "rel_l2_vs_fp64": float("%.3e" % r.get("rel_l2_vs_fp64", 0.0)),
-                     "guess_rel_err": (float("%.3e" % r["guess_rel_err"]) if r.get("guess_rel_err") is not None
-                                       else None)}
-                  for p, r in res.items()},
+        "config": config_dict(args, models, cols, nodes, D.world) | {"path": head},
+        "accepted": bool(ok),
+        "e2e": e2e, "roofline": roof, "assembly": asm,
+        "gpu_launches": (kp["launches"] + H["guess_launches_per_step"]) * args.steps,
+        "clocks": H["clocks"], "paths": out_paths,
     }
-    if "fp64" in res and head != "fp64":
-        out["speedup_vs_plain_fp64"] = round(H["value"] / res["fp64"]["value"], 3)
-    if D.rank == 0 and D.world == 1 and not args.no_cpu_baseline:
-        counts = {"picard_iters": res.get("fp64", H)["picard_iters"],
-                  "pcg_iters_total": res.get("fp64", H)["pcg_iters_total"]}
-        cs = cpu_sample(args.workload, args.pcg_maxiters, counts)
-        out["cpu_baseline"] = {"value": round(cs["solves_per_s"], 8), "unit": UNIT, "cores": 1,
-                               "kind": "port", "sample": cs["sample"],
-                               "sample_seconds": round(cs["sample_seconds"], 1)}
+    if "plain_fp64" in res:
+        out["speedup_vs_plain_fp64"] = round(out_paths[head]["value"] / out_paths["plain_fp64"]["value"], 3)
+    if "fp64_colpc" in res:
+        out["speedup_vs_plain_fp64_same_preconditioner"] = round(
+            out_paths[head]["value"] / out_paths["fp64_colpc"]["value"], 3)
+    if D.rank == 0 and D.world == 1 and not args.no_cpu_baseline and "plain_fp64" in res:
+        st0 = res["plain_fp64"]["stats"][0]
+        cs = cpu_sample(models[0], (st0["picard_iters"], st0["pcg_iters_total"]))
+        out["cpu_baseline"] = {
+            "value": round(1.0 / cs["t_solve_est"], 8), "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": (f"oracle (C restatement of the reference, 1 thread): setup, one assembly and 20 / 60 PCG "
+                       f"iterations of domain 0, extrapolated to its plain-FP64 counts ({st0['picard_iters']} "
+                       f"Picard, {st0['pcg_iters_total']} PCG); profiles/cpu_oracle_validation.md checks the "
+                       f"extrapolation against fully converged oracle solves"),
+            "sample_seconds": round(cs["sample_seconds"], 1)}
     for r in res.values():
-        r["prob"].close()
+        for pb in r["probs"]:
+            pb.close()
     ctx.close()
     return out
 
 
 # ---------------------------------------------------------------------------
-# reference arm: the oracle (restatement of the reference Fortran) on the
-# host cores, one bounded sample per worker process
+# reference arm: the oracle (restatement of the reference Fortran) on one
+# host core, bounded samples extrapolated with the recorded iteration counts
 # ---------------------------------------------------------------------------
-def _ref_worker(a):
-    workload, maxit, counts = a
-    sys.path.insert(0, ROOT)
-    return cpu_sample(workload, maxit, counts, iters=(10, 40))
-
-
 def run_reference(args, D):
     if D.rank != 0:
         return None
-    import multiprocessing as mp
-
-    counts = load_counts(args.workload)
+    models = make_models(args)
+    counts = load_counts(f"{args.workload}/{args.picard}")
     if counts is None:
         return {"impl": "reference", "unavailable": "no recorded iteration counts for this workload"}
-    ncores = os.cpu_count() or 1
-    workers = max(1, min(ncores, 16))
-    ctx = mp.get_context("spawn")
-    vals = []
-    with ctx.Pool(workers) as pool:
-        for step in range(args.warmup + args.steps):
-            r = pool.map(_ref_worker, [(args.workload, args.pcg_maxiters, counts)] * workers)
-            if step >= args.warmup:
-                vals.append(sum(x["solves_per_s"] for x in r))
-            last = r[0]
-    v = statistics.median(vals)
-    sample = (f"{workers} concurrent oracle processes (1 thread each, {ncores} host cores), each: "
-              + last["sample"])
+    vals, walls = [], []
+    for step in range(args.warmup + args.steps):
+        i = step % len(models)
+        c = counts["per_domain"][i % len(counts["per_domain"])]
+        t0 = time.perf_counter()
+        cs = cpu_sample(models[i], (c["picard_iters"], c["pcg_iters_total"]))
+        if step >= args.warmup:
+            vals.append(cs["t_solve_est"])
+            walls.append(time.perf_counter() - t0)
+    v = len(vals) / sum(vals)
+    cols, nodes = workload_stats(models)
+    sample = (f"oracle (C restatement of the reference's Fortran, which cannot be compiled here), 1 process, "
+              f"1 thread on {os.cpu_count()} host cores: per step setup, one assembly and 20 / 60 PCG iterations "
+              f"of one domain, extrapolated to that domain's recorded plain-FP64 Picard / PCG counts "
+              f"({counts['source']})")
     return {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": D.world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1000.0 / v if v else None, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD_DESC[args.workload], "name": args.workload},
+            "warmup": args.warmup, "ms_per_step": round(statistics.mean(walls) * 1000.0, 1),
+            "value_basis": "extrapolated: value = domains / sum of the extrapolated solve times; ms_per_step is "
+                           "the sample's own wall time",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config_dict(args, models, cols, nodes, D.world) | {"path": "plain_fp64"},
             "impl": "reference",
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": workers, "kind": "port", "sample": sample},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
 def profile_run(args):
-    """One solve of the workload through the resident-problem API, untimed."""
+    """One untimed run of the first selected path (for ncu)."""
     from cism_b200 import solver
 
-    m = make_model(args.workload, args.pcg_maxiters)
+    models = make_models(args)
     if args.picard_cap > 0:
-        m = m.copy(maxiter_nonlinear=args.picard_cap)
-    start, prec, m = path_spec(args.precision, m)
+        models = [m.copy(maxiter_nonlinear=args.picard_cap) for m in models]
     ctx = solver.Context(0)
-    prep, u0, v0 = solver.prepare(m, precision=prec, inner_tol=args.refine_eta)
-    if args.precision.startswith("learned"):
-        from cism_b200 import guess
-        u0, v0 = guess.learned_guesses(load_guess_net(m), [m])[0]
-    elif args.precision.startswith("sia"):
-        from cism_b200 import guess
-        u0, v0 = guess.sia_guess(m)
-    prob = ctx.problem([prep])
-    prob.set_guess([u0], [v0])
-    st = prob.run()[0]
-    print(json.dumps({"profile_run": args.workload, "precision": args.precision,
-                      "status": st["status"], "picard_iters": st["picard_iters"],
-                      "pcg_iters_total": st["pcg_iters_total"]}), flush=True)
-    prob.close()
+    w = weights_path(args.workload)
+    if w:
+        ctx.load_guess(w)
+    p = paths_for(args, w is not None)[0]
+
+    class _D:
+        world, rank = 1, 0
+
+        def barrier(self):
+            pass
+
+        def max(self, x):
+            return x
+
+    r = run_path(ctx, p, models, args, _D(), 1, 0, w)
+    sts = r["stats"]
+    print(json.dumps({"profile_run": args.workload, "path": p.name, "status": sorted({s["status"] for s in sts}),
+                      "picard_iters": [s["picard_iters"] for s in sts],
+                      "pcg_iters_total": [s["pcg_iters_total"] for s in sts]}), flush=True)
+    for pb in r["probs"]:
+        pb.close()
     ctx.close()
 
 
-def batch_eval(args):
-    """B: N held-out members of the c1 family (160 x 160 periodic slabs,
-    seeded outside the training seeds) solved (a) one at a time by the
-    plain FP64 path (zero start, diagonal preconditioner, standard PCG) and
-    (b) all in one resident problem by the learned + mixed path (column
-    preconditioner, Chronopoulos-Gear), the network's inference for the
-    whole batch included.  Each pass timed once after a warm-up pass (max of
-    device and wall time); prints one JSON line."""
-    import numpy as np
-
-    from cism_b200 import configs, guess, solver
-
-    n = args.batch_eval
-    rng = np.random.default_rng(90210)
-    models = [configs.random_slab(rng, n=160).copy(pcg_maxiters=args.pcg_maxiters) for _ in range(n)]
-    ctx = solver.Context(0)
-    net_model = load_guess_net(models[0])
-    plain = []
-    for m in models:
-        prep, u0, v0 = solver.prepare(m)
-        prob = ctx.problem([prep])
-        prob.set_guess([u0], [v0])
-        prob.run()  # warm-up (autotune, graphs)
-        plain.append(prob)
-    t0 = time.perf_counter()
-    ctx.timer_start()
-    sts_a = [p.run()[0] for p in plain]
-    ms_a = max(ctx.timer_stop(), (time.perf_counter() - t0) * 1000.0)
-    sols_a = [p.get()[:2] for p in plain]
-    for p in plain:
-        p.close()
-    mb = [m.copy(which_precond=configs.PRECOND_SIA, which_sparse=configs.SPARSE_PCG_CHRONGEAR) for m in models]
-    preps = [solver.prepare(m, precision=solver.MIXED, inner_tol=args.refine_eta)[0] for m in mb]
-    prob = ctx.problem(preps)
-    gs = guess.learned_guesses(net_model, mb)
-    prob.set_guess([g[0] for g in gs], [g[1] for g in gs])
-    prob.run()  # warm-up
-    t0 = time.perf_counter()
-    ctx.timer_start()
-    gs = guess.learned_guesses(net_model, mb)
-    prob.set_guess([g[0] for g in gs], [g[1] for g in gs])
-    sts_b = prob.run()
-    ms_b = max(ctx.timer_stop(), (time.perf_counter() - t0) * 1000.0)
-    us, vs, _ = prob.get()
-    prob.close()
-    err = []
-    for (ua, va), u, v in zip(sols_a, us, vs):
-        a = np.concatenate([ua[0].ravel(), va[0].ravel()])
-        b = np.concatenate([u.ravel(), v.ravel()])
-        err.append(float(np.linalg.norm(a - b) / np.linalg.norm(a)))
-
-    def summary(sts, ms):
-        return {"solves_per_s": n / (ms / 1000.0), "ms": ms,
-                "pcg_iters_mean": float(np.mean([s["pcg_iters_total"] for s in sts])),
-                "picard_mean": float(np.mean([s["picard_iters"] for s in sts]))}
-
-    out = {"batch_eval": n, "domains": "160x160x11 periodic slabs (c1 family, held-out seeds)",
-           "plain_fp64_sequential": summary(sts_a, ms_a),
-           "learned_mixed_colpc_cg_batched": summary(sts_b, ms_b),
-           "status": sorted({int(s["status"]) for s in sts_a + sts_b}),
-           "max_rel_l2_vs_plain": max(err)}
-    out["speedup"] = out["learned_mixed_colpc_cg_batched"]["solves_per_s"] / out["plain_fp64_sequential"]["solves_per_s"]
-    print(json.dumps(out), flush=True)
-    ctx.close()
-
-
-def batch_eval_c3(args):
-    """B on the ensemble configuration: N domes and slabs of 32-192 cells
-    per side (dx 2 km, 11 levels, log-normal beta perturbations), zero
-    start, solved (a) one at a time by the plain FP64 path, (b) all in one
-    resident problem by the same FP64 solver, (c) all in one problem by the
-    mixed solver with the column preconditioner and Chronopoulos-Gear.
-    Prints one JSON line."""
-    import numpy as np
-
-    from cism_b200 import configs, solver
-
-    n = args.batch_eval
-    models = [m.copy(pcg_maxiters=args.pcg_maxiters) for m in configs.ensemble(count=n)]
-    ctx = solver.Context(0)
-    sols_a, sts_a = [], []
-    t0 = time.perf_counter()
-    for m in models:
-        prep, u0, v0 = solver.prepare(m)
-        prob = ctx.problem([prep])
-        prob.set_guess([u0], [v0])
-        sts_a.append(prob.run()[0])
-        sols_a.append(prob.get()[:2])
-        prob.close()
-    ms_a = (time.perf_counter() - t0) * 1000.0
-
-    def batched(ms_, prec):
-        preps = [solver.prepare(m, precision=prec, inner_tol=args.refine_eta) for m in ms_]
-        prob = ctx.problem([p_[0] for p_ in preps])
-        prob.set_guess([p_[1] for p_ in preps], [p_[2] for p_ in preps])
-        t1 = time.perf_counter()
-        ctx.timer_start()
-        sts = prob.run()
-        ms = max(ctx.timer_stop(), (time.perf_counter() - t1) * 1000.0)
-        us, vs, _ = prob.get()
-        prob.close()
-        err = max(float(np.linalg.norm(np.concatenate([(u - ua[0]).ravel(), (v - va[0]).ravel()])) /
-                        max(np.linalg.norm(np.concatenate([ua[0].ravel(), va[0].ravel()])), 1e-300))
-                  for (ua, va), u, v in zip(sols_a, us, vs))
-        return sts, ms, err
-
-    sts_b, ms_b, err_b = batched(models, solver.FP64)
-    mc = [m.copy(which_precond=configs.PRECOND_SIA, which_sparse=configs.SPARSE_PCG_CHRONGEAR) for m in models]
-    sts_c, ms_c, err_c = batched(mc, solver.MIXED)
-
-    def summary(sts, ms):
-        return {"solves_per_s": n / (ms / 1000.0), "ms": ms,
-                "pcg_iters_mean": float(np.mean([s["pcg_iters_total"] for s in sts])),
-                "picard_mean": float(np.mean([s["picard_iters"] for s in sts])),
-                "status": sorted({int(s["status"]) for s in sts})}
-
-    out = {"batch_eval_c3": n, "domains": "ensemble: domes and slabs, 32-192 cells per side, dx 2 km, 11 levels",
-           "plain_fp64_sequential": summary(sts_a, ms_a),
-           "plain_fp64_batched": summary(sts_b, ms_b) | {"max_rel_l2_vs_sequential": err_b},
-           "mixed_colpc_cg_batched": summary(sts_c, ms_c) | {"max_rel_l2_vs_sequential": err_c}}
-    out["speedup_batched_fp64"] = ms_a / ms_b
-    out["speedup_batched_mixed_colpc_cg"] = ms_a / ms_c
-    print(json.dumps(out), flush=True)
-    ctx.close()
-
-
-def kernel_sweep(args):
-    """Matvec variants on the workload's assembled matrix (one Picard iteration)."""
-    from cism_b200 import solver
-
-    ctx = solver.Context(0)
-    peak, _ = measured_peaks()
-    out = []
-    for storage in ("sym", "full"):
-        os.environ["BP_MATRIX_STORAGE"] = storage
-        m = make_model(args.workload, args.pcg_maxiters).copy(maxiter_nonlinear=1)
-        prep, u0, v0 = solver.prepare(m)
-        prob = ctx.problem([prep])
-        prob.set_guess([u0], [v0])
-        prob.run()
-        N = prob.info()["nodes"]
-        sms = 148
-        for store in ((1, 2) if storage == "sym" else (0,)):
-            coef = 56 if store else 108
-            wb = 4 if store == 2 else 8
-            nbytes = N * (coef * wb + 32)
-            for minb in (0, 4, 6, 8):
-                for grid in (0, 4 * sms, 8 * sms):
-                    ms = prob.tune_mv(store, minb, grid, reps=50)
-                    if ms is None:
-                        continue
-                    out.append({"store": ["full64", "sym64", "sym32"][store], "minb": minb, "grid": grid,
-                                "us": round(ms * 1e3, 2), "GBps": round(nbytes / (ms / 1e3) / 1e9, 1),
-                                "frac": round(nbytes / (ms / 1e3) / 1e9 / peak, 3)})
-                    print(json.dumps(out[-1]), flush=True)
-        prob.close()
-    os.environ.pop("BP_MATRIX_STORAGE", None)
-    ctx.close()
-
-
-def main():
-    args = parse_args()
+def main(argv=None):
+    args = parse_args(argv)
     if args.profile_run:
         profile_run(args)
-        return
-    if args.batch_eval > 0:
-        (batch_eval_c3 if args.batch_family == "c3" else batch_eval)(args)
-        return
-    if args.kernel_sweep:
-        kernel_sweep(args)
         return
     D = Dist(args.gpus)
     try:

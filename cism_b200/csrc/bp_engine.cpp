@@ -121,6 +121,12 @@ struct bp_problem {
   double2* bt0 = nullptr;
   cudaGraphExec_t chunk_graph = nullptr;
   cudaGraphExec_t inner_graph = nullptr;
+  // the device-resident Picard loop (one graph with nested WHILE nodes) and
+  // its pass counters (Picard, PCG chunks); loop_state: 0 not built yet, 1
+  // built, -1 unavailable (the host-driven loop runs)
+  cudaGraphExec_t loop_graph = nullptr;
+  int* loop_iter = nullptr;
+  int loop_state = 0;
   bool use_graphs = true;
   Timing timing;
   bool tuned = false;
@@ -381,7 +387,35 @@ void enqueue_chunk(bp_problem* P, int variant, int ncheck) {
   for (int j = 0; j < ncheck; ++j) enqueue_iteration(P, variant, j == ncheck - 1);
 }
 
-// FP64 PCG for all instances with pcg_active, after MV_INIT.
+// Start of the PCG for the instances with pcg_active (after MV_INIT):
+// d = z for the standard PCG; for Chronopoulos-Gear its first pass and the
+// iterations before the first check (pcg:1304-1405).  Returns the number
+// of the next iteration, which starts a check chunk.
+int pcg_head(bp_problem* P) {
+  const HostPlan& p = P->plan;
+  const DevView& v = P->v;
+  bp_ctx* c = P->c;
+  const int variant = p.inst[0].variant;
+  const int ncheck = std::max(1, p.inst[0].ncheck);
+  int n = 1;
+  if (variant == 3) {
+    L(P, C_MV, [&] { launch_mv(MV_CG_FIRST, v, c->stream); });
+    L(P, C_UPD, [&] { launch_cg_first_update(v, c->stream); });
+    n = 2;
+    while ((n - 1) % ncheck != 0) {
+      enqueue_iteration(P, variant, (n % ncheck) == 0);
+      ++n;
+    }
+  } else {
+    L(P, C_UPD, [&] { launch_std_dir(v, c->stream); });  // d = z
+  }
+  return n;
+}
+
+// FP64 PCG for all instances with pcg_active, after MV_INIT: the head,
+// then check chunks until the device counter shows no active instance (the
+// host learns it one chunk late; the extra chunk's kernels find no active
+// instance and return at once).
 void run_pcg_fp64(bp_problem* P) {
   const HostPlan& p = P->plan;
   const DevView& v = P->v;
@@ -389,27 +423,14 @@ void run_pcg_fp64(bp_problem* P) {
   const int variant = p.inst[0].variant;
   const int ncheck = std::max(1, p.inst[0].ncheck);
   const int maxit = max_pcg_iters(p);
-  int n = 1;
-  if (variant == 3) {
-    L(P, C_MV, [&] { launch_mv(MV_CG_FIRST, v, c->stream); });
-    L(P, C_UPD, [&] { launch_cg_first_update(v, c->stream); });
-    n = 2;
-  } else {
-    L(P, C_UPD, [&] { launch_std_dir(v, c->stream); });  // d = z
-  }
-  int chunk = 0;
+  int n = pcg_head(P);
+  snapshot(c, v, 0);
+  int chunk = 1;
   while (n <= maxit + 1) {
-    if ((n - 1) % ncheck == 0) {
-      enqueue_chunk(P, variant, ncheck);
-      n += ncheck;
-    } else {  // head chunk of the Chronopoulos-Gear variant
-      do {
-        enqueue_iteration(P, variant, (n % ncheck) == 0);
-        ++n;
-      } while ((n - 1) % ncheck != 0);
-    }
+    enqueue_chunk(P, variant, ncheck);
+    n += ncheck;
     snapshot(c, v, chunk & 1);
-    if (chunk >= 1 && wait_snapshot(c, (chunk - 1) & 1).pcg_active <= 0) break;
+    if (wait_snapshot(c, (chunk - 1) & 1).pcg_active <= 0) break;
     ++chunk;
   }
   CK(cudaGetLastError());
@@ -571,26 +592,170 @@ struct L2Pin {
   }
 };
 
-void run_picard(bp_problem* P) {
-  const L2Pin pin(P);
+// One Picard iteration up to its linear solve: calcbeta for a sliding law,
+// assembly (glissade_velo_higher.F90:2502-3119), the right-hand side, then
+// (after the autotuner on the first assembly of a problem) the FP32 copy,
+// the initial residual (:3191-3220) and the PCG head.
+void picard_head(bp_problem* P, bool tune) {
   const HostPlan& p = P->plan;
   const DevView& v = P->v;
+  cudaStream_t s = P->c->stream;
+  L(P, C_OTHER, [&] { launch_picard_begin(v, s); });
+  L(P, C_OTHER, [&] { launch_save_usav(v, s); });
+  if (p.any_sliding) L(P, C_OTHER, [&] { launch_slide_beta(v, s); });
+  L(P, C_ASM1, [&] { launch_asm_qp(v, s); });
+  if (v.diva) L(P, C_ASM1, [&] { launch_diva_beta(v, s); });  // omega, beta_eff (:2742-2857)
+  L(P, C_ASM2, [&] { launch_asm_rows(v, s); });
+  L(P, C_RHS, [&] { launch_rhs(v, s); });
+  if (tune && !P->tuned) autotune(P);
+  if (P->v.A32) L(P, C_OTHER, [&] { launch_make_a32(P->v, s); });
+  L(P, C_CHECK, [&] { launch_mv(MV_INIT, P->v, s); });
+}
+
+// The rest of a Picard iteration after its linear solve: DIVA's traction
+// and 3-D velocity (:3658-3696), the Picard criterion (:3700-3727).
+void picard_tail(bp_problem* P) {
+  const DevView& v = P->v;
+  cudaStream_t s = P->c->stream;
+  if (v.diva) L(P, C_OTHER, [&] { launch_diva_velocity(v, s); });
+  L(P, C_OTHER, [&] { launch_picard_check(v, s); });
+}
+
+int max_picard_iters(const HostPlan& p) {
+  int m = 1;
+  for (const auto& ip : p.inst) m = std::max(m, ip.maxiter_nonlinear);
+  return m;
+}
+
+// The whole Picard loop as one CUDA graph that stays on the device:
+//   reset -> WHILE (some instance in Picard, passes < cap) {
+//     picard_head, PCG head, reset -> WHILE (some instance in PCG, chunks < cap) {
+//       one check chunk of ncheck iterations; count }
+//     picard_tail; count }
+// The loop conditions are set by one-thread kernels (cudaGraphSetConditional)
+// from the device counters the solve kernels keep, and each loop also stops
+// after a pass cap above what the instances' own caps (maxiter_nonlinear,
+// pcg_maxiters) allow, so the graph always ends.  The kernels are the host
+// loop's, in its order, so the results are the same; the host waits once,
+// after the graph.  Returns false where the graph cannot be built here
+// (the host-driven loop then runs).
+bool build_loop_graph(bp_problem* P, bool pdl) {
+  const HostPlan& p = P->plan;
+  const DevView& v = P->v;
+  cudaStream_t s = P->c->stream;
+  const int variant = p.inst[0].variant;
+  const int ncheck = std::max(1, p.inst[0].ncheck);
+  const int cap_picard = max_picard_iters(p) + 1;
+  const int cap_chunks = max_pcg_iters(p) / ncheck + 3;
+  if (!P->loop_iter) P->loop_iter = P->arena->get<int>(s, "loop_iter", 2);
+  int* it = P->loop_iter;
+  const auto mode = cudaStreamCaptureModeThreadLocal;
+  cudaGraph_t g = nullptr;
+  bool capturing = false;
+  set_pdl(pdl);
+  bool ok = false;
+  try {
+    CK(cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle hP, hK;
+    CK(cudaGraphConditionalHandleCreate(&hP, g, 0, 0));
+    CK(cudaStreamBeginCaptureToGraph(s, g, nullptr, nullptr, 0, mode));
+    capturing = true;
+    launch_loop_cond(hP, v, true, it, cap_picard, true, s);
+    CK(cudaStreamEndCapture(s, &g));
+    capturing = false;
+    cudaGraphNode_t start;
+    size_t nn = 1;
+    CK(cudaGraphGetNodes(g, &start, &nn));
+    cudaGraphNodeParams wp = {};
+    wp.type = cudaGraphNodeTypeConditional;
+    wp.conditional.handle = hP;
+    wp.conditional.type = cudaGraphCondTypeWhile;
+    wp.conditional.size = 1;
+    cudaGraphNode_t wP;
+    CK(cudaGraphAddNode(&wP, g, &start, 1, &wp));
+    cudaGraph_t bP = wp.conditional.phGraph_out[0];
+    CK(cudaGraphConditionalHandleCreate(&hK, bP, 0, 0));
+    // Picard body, up to the PCG loop
+    CK(cudaStreamBeginCaptureToGraph(s, bP, nullptr, nullptr, 0, mode));
+    capturing = true;
+    picard_head(P, false);
+    pcg_head(P);
+    launch_loop_cond(hK, v, false, it + 1, cap_chunks, true, s);
+    cudaStreamCaptureStatus cs;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    CK(cudaStreamGetCaptureInfo(s, &cs, nullptr, nullptr, &deps, &nd));
+    std::vector<cudaGraphNode_t> last(deps, deps + nd);
+    CK(cudaStreamEndCapture(s, &bP));
+    capturing = false;
+    cudaGraphNodeParams wk = {};
+    wk.type = cudaGraphNodeTypeConditional;
+    wk.conditional.handle = hK;
+    wk.conditional.type = cudaGraphCondTypeWhile;
+    wk.conditional.size = 1;
+    cudaGraphNode_t wK;
+    CK(cudaGraphAddNode(&wK, bP, last.data(), last.size(), &wk));
+    cudaGraph_t bK = wk.conditional.phGraph_out[0];
+    // PCG body: one check chunk
+    CK(cudaStreamBeginCaptureToGraph(s, bK, nullptr, nullptr, 0, mode));
+    capturing = true;
+    for (int j = 0; j < ncheck; ++j) enqueue_iteration(P, variant, j == ncheck - 1);
+    launch_loop_cond(hK, v, false, it + 1, cap_chunks, false, s);
+    CK(cudaStreamEndCapture(s, &bK));
+    capturing = false;
+    // the rest of the Picard body, after the PCG loop
+    CK(cudaStreamBeginCaptureToGraph(s, bP, &wK, nullptr, 1, mode));
+    capturing = true;
+    picard_tail(P);
+    launch_loop_cond(hP, v, true, it, cap_picard, false, s);
+    CK(cudaStreamEndCapture(s, &bP));
+    capturing = false;
+    ok = cudaGraphInstantiate(&P->loop_graph, g, 0) == cudaSuccess;
+  } catch (const CudaError&) {
+    ok = false;
+  }
+  if (capturing) {
+    cudaGraph_t junk = nullptr;
+    cudaStreamEndCapture(s, &junk);
+  }
+  set_pdl(true);
+  if (g) cudaGraphDestroy(g);
+  cudaGetLastError();  // a failed build leaves no sticky error: it only returned codes
+  if (!ok) P->loop_graph = nullptr;
+  return ok;
+}
+
+// BP_DEVICE_LOOP=0 keeps the host-driven Picard loop.
+bool device_loop_wanted(const bp_problem* P) {
+  const char* e = std::getenv("BP_DEVICE_LOOP");
+  return P->use_graphs && !P->timing.on && P->loop_state >= 0 && !(e && e[0] == '0');
+}
+
+bool run_device_loop(bp_problem* P) {
+  if (P->loop_state == 0) {
+    // programmatic edges inside the loop bodies where the driver takes them
+    const bool ok = build_loop_graph(P, true) || build_loop_graph(P, false);
+    P->loop_state = ok ? 1 : -1;
+    if (std::getenv("BP_TUNE_LOG"))
+      std::fprintf(stderr, "device Picard loop: %s\n", ok ? "built" : "unavailable, host loop");
+    if (!ok) return false;
+  }
+  CK(cudaGraphLaunch(P->loop_graph, P->c->stream));
+  return true;
+}
+
+void run_picard(bp_problem* P) {
+  const L2Pin pin(P);
+  const DevView& v = P->v;
   bp_ctx* c = P->c;
-  cudaStream_t s = c->stream;
-  int max_picard = 1;
-  for (const auto& ip : p.inst) max_picard = std::max(max_picard, ip.maxiter_nonlinear);
+  const int max_picard = max_picard_iters(P->plan);
   for (int it = 0; it < max_picard; ++it) {
-    L(P, C_OTHER, [&] { launch_picard_begin(v, s); });
-    L(P, C_OTHER, [&] { launch_save_usav(v, s); });
-    if (p.any_sliding) L(P, C_OTHER, [&] { launch_slide_beta(v, s); });
-    L(P, C_ASM1, [&] { launch_asm_qp(v, s); });
-    if (v.diva) L(P, C_ASM1, [&] { launch_diva_beta(v, s); });  // omega, beta_eff (:2742-2857)
-    L(P, C_ASM2, [&] { launch_asm_rows(v, s); });
-    L(P, C_RHS, [&] { launch_rhs(v, s); });
-    if (!P->tuned) autotune(P);
-    linear_solve(P);
-    if (v.diva) L(P, C_OTHER, [&] { launch_diva_velocity(v, s); });  // traction, 3-D velocity (:3658-3696)
-    L(P, C_OTHER, [&] { launch_picard_check(v, s); });
+    // the device loop takes over once the problem is tuned (the first run's
+    // first assembly runs the autotuner on the host)
+    if (P->tuned && device_loop_wanted(P) && run_device_loop(P)) break;
+    picard_head(P, true);
+    run_pcg_fp64(P);
+    picard_tail(P);
     snapshot(c, v, 0);
     if (wait_snapshot(c, 0).picard_active <= 0) break;
   }
@@ -667,6 +832,7 @@ void problem_free(bp_problem* P) {
   if (!P) return;
   if (P->chunk_graph) cudaGraphExecDestroy(P->chunk_graph);
   if (P->inner_graph) cudaGraphExecDestroy(P->inner_graph);
+  if (P->loop_graph) cudaGraphExecDestroy(P->loop_graph);
   P->timing.destroy();
   P->own.release();
   delete P;
@@ -1071,19 +1237,17 @@ int bp_problem_info(bp_problem* P, long* nodes, long* cols, long* elems, double*
   if (nodes) *nodes = P->plan.nnodes;
   if (cols) *cols = P->plan.ncols;
   if (elems) *elems = P->plan.nelem;
-  // algorithmic bytes of one fused PCG matvec launch per node:
-  // standard: 108 FP64 coefficients + r, D^-1, d_old read + d, q written
-  // Chronopoulos-Gear: 108 coefficients + r, D^-1 read + Az written
-  // coefficients read per node: symmetric storage streams the 14 upper
-  // stencil offsets (the lower half is re-read from neighbours, from L2)
-  // vectors of the Krylov matvec kernel: source read + result written
-  // (+ the vectors of its fused dots: d for the standard PCG, r and z for
-  // Chronopoulos-Gear)
+  // algorithmic bytes of one Krylov matvec launch per node: the stored
+  // matrix once -- FP64 half storage 14 offsets x 2 rows x (u, v) doubles =
+  // 448 B (full rows 864 B); FP32 half storage 13 offsets x 4 floats +
+  // the FP64 diagonal block 32 B = 240 B; the lower half is re-read from
+  // the neighbours' rows, in cache -- plus the vectors: the source read and
+  // the result written (standard PCG: d, q), and for Chronopoulos-Gear r
+  // read for the fused dots (z, r, Az)
   const bool cg = P->plan.inst[0].variant == 3;
   const double vec = (cg ? 3.0 : 2.0) * 16.0;
-  const double coef = P->v.sym ? 14.0 * 4.0 : 27.0 * 4.0;
-  if (mvb64) *mvb64 = N * (coef * 8.0 + vec);
-  if (mvb32) *mvb32 = N * (coef * 4.0 + vec);
+  if (mvb64) *mvb64 = N * ((P->v.sym ? 448.0 : 864.0) + vec);
+  if (mvb32) *mvb32 = N * (240.0 + vec);
   return BP_OK;
 }
 

@@ -1332,12 +1332,15 @@ void launch_assemble(const DevView& v, cudaStream_t s) {
   launch_rhs(v, s);
 }
 // PCG kernels are launched as programmatic dependents of their stream
-// predecessor (BP_PDL=0 turns this off), and with the problem's L2
-// access-policy window when it has one.
-static const bool g_pdl = [] {
+// predecessor (BP_PDL=0 turns this off, and so does set_pdl(false), e.g.
+// while a graph that cannot hold programmatic edges is captured), and with
+// the problem's L2 access-policy window when it has one.
+static const bool g_pdl_env = [] {
   const char* e = std::getenv("BP_PDL");
   return !(e && e[0] == '0');
 }();
+static thread_local bool g_pdl_on = true;
+void set_pdl(bool on) { g_pdl_on = on; }
 
 static void launch_pcg(void (*kernel)(DevView), int g, cudaStream_t s, const DevView& v) {
   cudaLaunchConfig_t cfg = {};
@@ -1347,7 +1350,7 @@ static void launch_pcg(void (*kernel)(DevView), int g, cudaStream_t s, const Dev
   cfg.stream = s;
   cudaLaunchAttribute at[2];
   unsigned na = 0;
-  if (g_pdl) {
+  if (g_pdl_env && g_pdl_on) {
     at[na].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     at[na].val.programmaticStreamSerializationAllowed = 1;
     ++na;
@@ -1462,6 +1465,20 @@ void launch_cg_update(bool check, const DevView& v, cudaStream_t s) {
 }
 void launch_picard_check(const DevView& v, cudaStream_t s) {
   k_picard_check<<<tile_grid(v), kTile, 0, s>>>(v);
+}
+
+// Conditions of the device-resident loops (CUDA-graph WHILE nodes).  One
+// thread: count this pass in *iter (reset to 0 by `reset`) and keep
+// looping while some instance is active (counter *active > 0) and fewer
+// than `cap` passes ran, so every loop ends after at most `cap` passes.
+__global__ void k_loop_cond(cudaGraphConditionalHandle h, const int* active, int* iter, int cap, int reset) {
+  const int it = reset ? (*iter = 0) : ++*iter;
+  cudaGraphSetConditional(h, (*active > 0 && it < cap) ? 1u : 0u);
+}
+void launch_loop_cond(cudaGraphConditionalHandle h, const DevView& v, bool picard, int* iter, int cap, bool reset,
+                      cudaStream_t s) {
+  const int* active = picard ? &v.cnt->picard_active : &v.cnt->pcg_active;
+  k_loop_cond<<<1, 1, 0, s>>>(h, active, iter, cap, reset ? 1 : 0);
 }
 void launch_make_a32(const DevView& v, cudaStream_t s) { k_make_a32<<<tile_grid(v), kTile, 0, s>>>(v); }
 void launch_matvec_plain(const DevView& v, const double2* x, double2* y, cudaStream_t s) {

@@ -38,6 +38,14 @@ void launch_std_dir(const DevView& v, cudaStream_t s);
 void launch_cg_first_update(const DevView& v, cudaStream_t s);
 void launch_cg_update(bool check, const DevView& v, cudaStream_t s);
 void launch_picard_check(const DevView& v, cudaStream_t s);
+// Condition of a device-resident WHILE loop (graph conditional handle h):
+// *iter counts the passes (reset: set to 0); h = 1 while the counter
+// v.cnt->picard_active (picard) or pcg_active is positive and *iter < cap.
+void launch_loop_cond(cudaGraphConditionalHandle h, const DevView& v, bool picard, int* iter, int cap, bool reset,
+                      cudaStream_t s);
+// Programmatic dependent launch of the PCG kernels on (default) or off,
+// for the launches of the calling thread.
+void set_pdl(bool on);
 void launch_make_a32(const DevView& v, cudaStream_t s);
 void launch_matvec_plain(const DevView& v, const double2* x, double2* y, cudaStream_t s);
 void launch_dinv(const DevView& v, int precond, cudaStream_t s);

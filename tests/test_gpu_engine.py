@@ -1,0 +1,175 @@
+"""GPU tests of the engine's execution paths: the column-march Krylov
+matvec against the per-node kernels, the device-resident Picard loop
+against the host-driven one, and the learned guess behind the C ABI
+against the network's Python forward.
+
+Tolerances: march vs per-node on one assembled system with a fixed PCG
+iteration count, 1e-11 relative L2 (the dot products sum in another order);
+device loop vs host loop, bitwise (the same kernels in the same order); the
+C-ABI guess vs the Python forward of the same weights, 1e-6 relative
+(identical arithmetic and BF16 rounding points; a last-bit difference of
+log10 can move one BF16 input by one unit).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from cism_b200 import configs, solver
+
+from helpers import rel_l2, small_models
+
+pytestmark = pytest.mark.gpu
+
+MODELS = {m.name: m for m in small_models()}
+
+
+class _Env:
+    """Set environment switches the engine reads when it builds a problem or
+    starts a run, and restore them."""
+
+    def __init__(self, **kw):
+        self.kw = kw
+        self.old = {}
+
+    def __enter__(self):
+        for k, v in self.kw.items():
+            self.old[k] = os.environ.get(k)
+            os.environ[k] = v
+
+    def __exit__(self, *a):
+        for k, v in self.old.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+
+
+def _one_picard_fixed_pcg(ctx, m, precision):
+    """One Picard iteration from a fixed start with exactly 40 PCG
+    iterations (tolerance 0): assembly, FP32 copy and 40 Krylov passes."""
+    m = m.copy(maxiter_nonlinear=1, pcg_maxiters=40, pcg_tol=0.0)
+    rng = np.random.default_rng(5)
+    prep, _, _ = solver.prepare(m, precision=precision)
+    av = prep.arrays["active_vertex"].astype(bool)[..., None]
+    u0 = configs.halo_fill_stag(50.0 * rng.standard_normal(m.vshape3) * av, m.periodic)
+    v0 = configs.halo_fill_stag(50.0 * rng.standard_normal(m.vshape3) * av, m.periodic)
+    prob = ctx.problem([prep])
+    prob.set_guess([u0], [v0])
+    st = prob.run()[0]
+    u, v, _ = prob.get()
+    prob.close()
+    return u[0], v[0], st
+
+
+@pytest.mark.parametrize("variant", [configs.SPARSE_PCG_STANDARD, configs.SPARSE_PCG_CHRONGEAR])
+@pytest.mark.parametrize("precision", [solver.FP64, solver.MIXED])
+@pytest.mark.parametrize("name", list(MODELS))
+def test_march_matvec_matches_per_node(ctx, name, precision, variant):
+    m = MODELS[name].copy(which_sparse=variant)
+    with _Env(BP_MARCH="0"):
+        ua, va, sa = _one_picard_fixed_pcg(ctx, m, precision)
+    ub, vb, sb = _one_picard_fixed_pcg(ctx, m, precision)  # column march (default)
+    assert sa["pcg_iters_total"] == sb["pcg_iters_total"] == 40
+    assert rel_l2([ub, vb], [ua, va]) < 1e-11
+
+
+@pytest.mark.parametrize("chunks", ["1", "3"])
+def test_march_level_chunks(ctx, chunks):
+    # the column split into level chunks (several warps per column block)
+    m = MODELS["marine40x40x11"]
+    with _Env(BP_MARCH="0"):
+        ua, va, _ = _one_picard_fixed_pcg(ctx, m, solver.MIXED)
+    with _Env(BP_MARCH_CHUNKS=chunks):
+        ub, vb, _ = _one_picard_fixed_pcg(ctx, m, solver.MIXED)
+    assert rel_l2([ub, vb], [ua, va]) < 1e-11
+
+
+@pytest.mark.parametrize("precision", [solver.FP64, solver.MIXED])
+def test_device_loop_equals_host_loop(ctx, precision):
+    m = configs.marine(n=40, dx=4000.0).copy(pcg_maxiters=2000, which_resid=configs.RESID_L2NORM_RELATIVE,
+                                             which_precond=configs.PRECOND_SIA)
+    prep, u0, v0 = solver.prepare(m, precision=precision)
+    out = {}
+    for loop in ("0", "1"):
+        with _Env(BP_DEVICE_LOOP=loop):
+            prob = ctx.problem([prep])
+            prob.set_guess([u0], [v0])
+            prob.run()  # first run: the autotuner, then the device loop takes over
+            prob.set_guess([u0], [v0])
+            st = prob.run()[0]  # a whole run in the device loop
+            u, v, _ = prob.get()
+            prob.close()
+        out[loop] = (u[0], v[0], st)
+    (ua, va, sa), (ub, vb, sb) = out["0"], out["1"]
+    assert sa["status"] == sb["status"] == 0
+    assert (sa["picard_iters"], sa["pcg_iters_total"]) == (sb["picard_iters"], sb["pcg_iters_total"])
+    assert np.array_equal(ua, ub) and np.array_equal(va, vb)
+
+
+def _random_network(seed=3):
+    from cism_b200 import net
+
+    model = net.UNet(n_out=24, seed=seed)
+    model.in_shift = np.array([1.0, 0.1, -0.1, 2.5, 0.0], np.float32)
+    model.in_scale = np.array([0.8, 0.5, 0.5, 1.2, 1.0], np.float32)
+    model.out_scale = 35.0
+    return model
+
+
+def test_learned_guess_c_abi_matches_python(ctx, tmp_path):
+    torch = pytest.importorskip("torch")
+    from cism_b200 import net
+
+    model = _random_network()
+    path = str(tmp_path / "net.npz")
+    model.save(path)
+    ctx.load_guess(path)
+    ms = [configs.marine(n=40, dx=4000.0, seed=s) for s in (11, 12)]
+    preps = [solver.prepare(m, guess_mode=solver.GUESS_LEARNED)[0] for m in ms]
+    prob = ctx.problem(preps)
+    n0 = ctx.guess_launches()
+    prob.set_guess([None, None], [None, None])
+    assert ctx.guess_launches() > n0
+    gu, gv = prob.get_guess()
+    prob.close()
+    # the Python forward of the same weights on the same features
+    F = np.stack([net.normalized_input(model, net.pad_grid(net.input_features(m, p.arrays)))
+                  for m, p in zip(ms, preps)])
+    x = torch.tensor(F, dtype=torch.float32, device="cuda").to(torch.bfloat16).contiguous()
+    out = model.forward(x, int(ms[0].periodic), train=False).cpu().numpy() * model.out_scale
+    for m, p, o, u, v in zip(ms, preps, out, gu, gv):
+        pu, pv = net.guess_from_grid(m, o, p.arrays["active_vertex"])
+        av = p.arrays["active_vertex"].astype(bool)
+        assert np.abs(pu).max() > 0.0
+        assert rel_l2([u[av], v[av]], [pu[av], pv[av]]) < 1e-6
+
+
+def test_learned_start_converges_to_the_plain_answer(ctx, tmp_path):
+    pytest.importorskip("torch")
+    model = _random_network(seed=4)
+    path = str(tmp_path / "net.npz")
+    model.save(path)
+    ctx.load_guess(path)
+    m = configs.marine(n=40, dx=4000.0, seed=7).copy(pcg_maxiters=2000, which_resid=configs.RESID_L2NORM_RELATIVE)
+    prep, u0, v0 = solver.prepare(m)
+    u, v, _, st = ctx.solve_prepared(prep, u0, v0, want_efvs=False)
+    prep_l, _, _ = solver.prepare(m, precision=solver.MIXED, guess_mode=solver.GUESS_LEARNED)
+    ul, vl, _, stl = ctx.solve_prepared(prep_l, np.zeros_like(u0), np.zeros_like(v0), want_efvs=False)
+    assert st["status"] == stl["status"] == 0
+    # the relative-residual criterion ends both at the same point
+    assert rel_l2([ul, vl], [u, v]) < 1e-6
+
+
+def test_learned_guess_needs_a_network():
+    c = solver.Context(0)
+    try:
+        m = configs.marine(n=40, dx=4000.0)
+        prep, u0, v0 = solver.prepare(m, guess_mode=solver.GUESS_LEARNED)
+        with pytest.raises(solver.BPError) as e:
+            c.solve_prepared(prep, u0, v0)
+        assert e.value.code == 10
+        with pytest.raises(solver.BPError):
+            c.load_guess("/nonexistent/weights.bin")
+    finally:
+        c.close()
