@@ -107,6 +107,7 @@ struct Counters {
 struct DevView {
   int nz, ncols, nnodes, npad, ncells, nelem, ninst, ntiles;
   int W, lsh;              // column block width (power of two, W * nz <= kTile) and log2 W
+  int tile_threads;        // CTA size of the tile kernels: W * nz rounded up to whole warps
   int any_dirichlet;       // any prescribed node in the problem
   int sym;                 // matrix stored as its 14 upper stencil offsets (exactly symmetric)
   int minb;                // residual kernels: resident CTAs per SM they are built for (0 or 4)

@@ -157,6 +157,7 @@ DevView make_view(Arena& a, cudaStream_t s, const HostPlan& p, bool with_cells, 
   std::memset(&v, 0, sizeof(v));
   v.nz = p.nz; v.ncols = p.ncols; v.nnodes = p.nnodes; v.npad = p.npad;
   v.W = p.W; v.lsh = p.lsh;
+  v.tile_threads = std::min(kTile, (p.W * p.nz + 31) / 32 * 32);
   v.solve2d = p.solve2d ? 1 : 0;
   v.l1l2 = p.l1l2 ? 1 : 0;
   v.diva = p.diva ? 1 : 0;

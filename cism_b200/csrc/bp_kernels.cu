@@ -1,6 +1,6 @@
 // bp_kernels.cu -- sm_100a kernels of the Blatter-Pattyn solve.
 //
-// All node kernels walk tiles of kTile consecutive nodes (one tile per CTA
+// All node kernels walk tiles of at most kTile consecutive nodes (one tile per CTA
 // iteration, grid-stride, so the same code runs as a one-shot grid or as a
 // persistent grid).  A tile never spans two instances, so per-instance
 // reductions are: block reduce -> per-tile partial -> the last CTA of the
@@ -1291,7 +1291,7 @@ cudaError_t upload_ref_tables() {
 }
 
 void launch_picard_begin(const DevView& v, cudaStream_t s) { k_picard_begin<<<1, 256, 0, s>>>(v); }
-void launch_save_usav(const DevView& v, cudaStream_t s) { k_save_usav<<<tile_grid(v), kTile, 0, s>>>(v); }
+void launch_save_usav(const DevView& v, cudaStream_t s) { k_save_usav<<<tile_grid(v), v.tile_threads, 0, s>>>(v); }
 void launch_slide_beta(const DevView& v, cudaStream_t s) {
   if (v.ncols > 0) k_slide_beta<<<(v.ncols + kTile - 1) / kTile, kTile, 0, s>>>(v);
   if (v.ncells > 0) k_cell_beta<<<(v.ncells + kTile - 1) / kTile, kTile, 0, s>>>(v);
@@ -1310,10 +1310,10 @@ void launch_asm_qp(const DevView& v, cudaStream_t s) {
 }
 void launch_asm_rows(const DevView& v, cudaStream_t s) {
   dim3 g(tile_grid(v), 4);
-  if (v.solve2d) k_asm_rows<true><<<g, kTile, 0, s>>>(v);
-  else k_asm_rows<false><<<g, kTile, 0, s>>>(v);
+  if (v.solve2d) k_asm_rows<true><<<g, v.tile_threads, 0, s>>>(v);
+  else k_asm_rows<false><<<g, v.tile_threads, 0, s>>>(v);
 }
-void launch_rhs(const DevView& v, cudaStream_t s) { k_rhs<<<tile_grid(v), kTile, 0, s>>>(v); }
+void launch_rhs(const DevView& v, cudaStream_t s) { k_rhs<<<tile_grid(v), v.tile_threads, 0, s>>>(v); }
 void launch_diva_beta(const DevView& v, cudaStream_t s) {
   if (v.ncells > 0) k_diva_cells<<<(unsigned)((v.ncells + 255) / 256), 256, 0, s>>>(v);
   if (v.ncols > 0) k_diva_beta<<<(unsigned)((v.ncols + 255) / 256), 256, 0, s>>>(v);
@@ -1342,10 +1342,10 @@ static const bool g_pdl_env = [] {
 static thread_local bool g_pdl_on = true;
 void set_pdl(bool on) { g_pdl_on = on; }
 
-static void launch_pcg(void (*kernel)(DevView), int g, cudaStream_t s, const DevView& v) {
+static void launch_pcg(void (*kernel)(DevView), int g, cudaStream_t s, const DevView& v, int block = 0) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(g);
-  cfg.blockDim = dim3(kTile);
+  cfg.blockDim = dim3(block > 0 ? block : v.tile_threads);
   cfg.dynamicSmemBytes = 0;
   cfg.stream = s;
   cudaLaunchAttribute at[2];
@@ -1427,7 +1427,7 @@ static void launch_march(int mode, const DevView& v, cudaStream_t s) {
   TileKernel k;
   if (v.A32) k = g_march_minb == 2 ? march_kernel<ST_SYM32, 2>(mode) : march_kernel<ST_SYM32, 1>(mode);
   else k = g_march_minb == 2 ? march_kernel<ST_SYM, 2>(mode) : march_kernel<ST_SYM, 1>(mode);
-  launch_pcg(k, g, s, v);
+  launch_pcg(k, g, s, v, kTile);  // 8 warps, each its own column slots
 }
 
 void launch_mv(int mode, const DevView& v, cudaStream_t s) {
@@ -1448,7 +1448,7 @@ void launch_mv(int mode, const DevView& v, cudaStream_t s) {
 }
 int krylov_resident_ctas(const DevView& v, int mode, int minb) {
   int n = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, krylov_kernel_for(v, mode, minb), kTile, 0) !=
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, krylov_kernel_for(v, mode, minb), v.tile_threads, 0) !=
       cudaSuccess)
     return 0;
   return n;
@@ -1464,7 +1464,7 @@ void launch_cg_update(bool check, const DevView& v, cudaStream_t s) {
   launch_pcg(check ? k_cg_update<true> : k_cg_update<false>, tile_grid(v), s, v);
 }
 void launch_picard_check(const DevView& v, cudaStream_t s) {
-  k_picard_check<<<tile_grid(v), kTile, 0, s>>>(v);
+  k_picard_check<<<tile_grid(v), v.tile_threads, 0, s>>>(v);
 }
 
 // Conditions of the device-resident loops (CUDA-graph WHILE nodes).  One
@@ -1480,14 +1480,14 @@ void launch_loop_cond(cudaGraphConditionalHandle h, const DevView& v, bool picar
   const int* active = picard ? &v.cnt->picard_active : &v.cnt->pcg_active;
   k_loop_cond<<<1, 1, 0, s>>>(h, active, iter, cap, reset ? 1 : 0);
 }
-void launch_make_a32(const DevView& v, cudaStream_t s) { k_make_a32<<<tile_grid(v), kTile, 0, s>>>(v); }
+void launch_make_a32(const DevView& v, cudaStream_t s) { k_make_a32<<<tile_grid(v), v.tile_threads, 0, s>>>(v); }
 void launch_matvec_plain(const DevView& v, const double2* x, double2* y, cudaStream_t s) {
-  k_matvec_plain<<<tile_grid(v), kTile, 0, s>>>(v, x, y);
+  k_matvec_plain<<<tile_grid(v), v.tile_threads, 0, s>>>(v, x, y);
 }
 void launch_dinv(const DevView& v, int precond, cudaStream_t s) {
-  k_dinv<<<tile_grid(v), kTile, 0, s>>>(v, precond);
+  k_dinv<<<tile_grid(v), v.tile_threads, 0, s>>>(v, precond);
 }
-void launch_bb(const DevView& v, cudaStream_t s) { k_bb<<<tile_grid(v), kTile, 0, s>>>(v); }
+void launch_bb(const DevView& v, cudaStream_t s) { k_bb<<<tile_grid(v), v.tile_threads, 0, s>>>(v); }
 // The 3-D velocity of a shallow-shelf solve (its 2-D solution on every
 // level, :3745-3750) for the post-solve diagnostics.
 __global__ void __launch_bounds__(256) k_levels_from_2d(DevView v, double2* x3, int L) {
@@ -1521,7 +1521,7 @@ void launch_diagnostics(const DevView& v, int which_bfric, double* tau, double* 
 }
 int launch_tune_mv(int store, int minb, int grid, const DevView& v, cudaStream_t s) {
   const int g = grid > 0 ? grid : tile_grid(v);
-#define TUNE(ST, MB) k_tune_mv<ST, MB><<<g, kTile, 0, s>>>(v)
+#define TUNE(ST, MB) k_tune_mv<ST, MB><<<g, v.tile_threads, 0, s>>>(v)
   if (store == ST_FULL && !v.sym) {
     if (minb == 8) TUNE(ST_FULL, 8); else if (minb == 6) TUNE(ST_FULL, 6);
     else if (minb == 4) TUNE(ST_FULL, 4); else TUNE(ST_FULL, 0);

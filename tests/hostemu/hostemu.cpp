@@ -25,6 +25,7 @@ struct Emu {
     std::memset(&v, 0, sizeof(v));
     v.nz = p.nz; v.ncols = p.ncols; v.nnodes = p.nnodes; v.npad = p.npad;
     v.W = p.W; v.lsh = p.lsh;
+    v.tile_threads = std::min(kTile, (p.W * p.nz + 31) / 32 * 32);
     v.col_node = p.col_node.data(); v.col_nbn = p.col_nbn.data();
     v.tile_start = p.tile_start.data(); v.tile_end = p.tile_end.data(); v.tile_inst = p.tile_inst.data();
     v.tile_ncols = p.tile_ncols.data(); v.tile_col0 = p.tile_col0.data();
