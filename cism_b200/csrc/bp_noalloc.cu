@@ -19,8 +19,10 @@
 // process and to each device, and every call reuses it: two calls whose
 // work overlaps on the GPU (different streams, or different host threads on
 // one device) race on the partial sums and give wrong norms.  Serialise
-// them.  The first call on a device looks up the array's device address
-// (cudaGetSymbolAddress); make that first call before any stream capture.
+// them.  The first call on a device (and the first after the device's
+// context was torn down and made again, e.g. by cudaDeviceReset) looks up
+// the array's device address (cudaGetSymbolAddress); make that call before
+// any stream capture.
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -137,8 +139,31 @@ k_resid_ref_layout(int nx, int ny, int nz, int periodic, const int* __restrict__
   }
 }
 
-// Device address of the scratch array on the current device (looked up
-// once per device).
+// The CUDA context current on the calling thread (the driver's
+// cuCtxGetCurrent, reached through the runtime so that no driver library
+// is linked), or null when it cannot be asked.
+using CtxGetCurrent = int (*)(void**);
+void* current_context() {
+  static CtxGetCurrent fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<CtxGetCurrent>(f);
+  }();
+  void* c = nullptr;
+  if (!fn || fn(&c) != 0) return nullptr;
+  return c;
+}
+
+void* g_na_ctx[kNaMaxDevices] = {nullptr};
+
+// Device address of the scratch array on the current device, looked up
+// once per device and context: after cudaDeviceReset (or any teardown of
+// the device's context) the module is loaded again into the new context,
+// where the array may sit at another address, so a change of the current
+// context triggers a new lookup.
 NaScratch* scratch_for_current_device(int* status) {
   int dev = -1;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNaMaxDevices) {
@@ -146,7 +171,8 @@ NaScratch* scratch_for_current_device(int* status) {
     return nullptr;
   }
   std::lock_guard<std::mutex> lock(g_na_mutex);
-  if (!g_na_ptr[dev]) {
+  void* ctx = current_context();
+  if (!g_na_ptr[dev] || !ctx || ctx != g_na_ctx[dev]) {
     void* p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_na_scratch);
     if (e != cudaSuccess || !p) {
@@ -156,6 +182,7 @@ NaScratch* scratch_for_current_device(int* status) {
       return nullptr;
     }
     g_na_ptr[dev] = static_cast<NaScratch*>(p);
+    g_na_ctx[dev] = current_context();  // current now that the lookup made the runtime initialise it
   }
   *status = BP_OK;
   return g_na_ptr[dev];

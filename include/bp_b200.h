@@ -259,8 +259,9 @@ int bp_assemble(bp_ctx *ctx, const bp_inputs *in, const double *uvel,
  * is a fixed file-scope device array shared by all calls: at most
  * nz*(nx-1)*(ny-1) = 16,777,216 rows (larger: BP_ERR_ARGS); calls that
  * overlap on the GPU race on it and must be serialised; the first call on
- * a device looks up the array's address and should precede any stream
- * capture. */
+ * a device, and the first after its context was made again (e.g. after
+ * cudaDeviceReset), looks up the array's address and should precede any
+ * stream capture. */
 int bp_residual_noalloc(int nx, int ny, int nz, int periodic,
                         const int *active_vertex, const double *Auu,
                         const double *Auv, const double *Avu, const double *Avv,

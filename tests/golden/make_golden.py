@@ -33,5 +33,28 @@ def main():
     print("wrote", os.listdir(HERE))
 
 
+# every SUB-th owned vertex in each direction, all levels
+SUB = 4
+
+
+def c1_fixture():
+    """The full-size periodic slab (160 x 160 x 11) solved by the oracle
+    (about 14 CPU-minutes): its Picard and PCG counts, the velocity at every
+    SUB-th owned vertex in each direction and whole-field checksums (sum and
+    sum of squares of u and v over the owned vertices)."""
+    m = configs.workload("c1").copy(pcg_maxiters=3000)
+    u, v, efvs, beta, st = oracle.velo_higher_solve(m)
+    js, is_ = m.owned_vertex_slices()
+    uo, vo = u[js, is_], v[js, is_]
+    np.savez_compressed(os.path.join(HERE, "c1_picard_oracle.npz"), sub=SUB,
+                        u_sub=uo[::SUB, ::SUB], v_sub=vo[::SUB, ::SUB],
+                        sums=np.array([uo.sum(), vo.sum(), (uo ** 2).sum(), (vo ** 2).sum()]),
+                        picard_iters=st["picard_iters"], pcg_iters_total=st["pcg_iters_total"])
+    print("wrote c1_picard_oracle.npz", st)
+
+
 if __name__ == "__main__":
-    main()
+    if "--c1" in sys.argv:
+        c1_fixture()
+    else:
+        main()
