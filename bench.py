@@ -5,7 +5,7 @@ Default workload (c4): the learned-guess evaluation set -- held-out marine
 ice sheets drawn as the large marine configuration (seeded Gaussian-random
 bed with a trough, parabolic 3000 m sheet with a calving front, log-normal
 beta, zero under the shelf) at 256 x 256 cells, dx = 2 km, 11 sigma
-levels, Glen n = 3; `--batch` domains (default 8).  Every linear solve to
+levels, Glen n = 3; `--batch` domains (default 4).  Every linear solve to
 a relative residual of 1e-8; the Picard loop to the reference's relative
 nonlinear residual criterion (which_ho_resid = 4: |A(u)u - b| / |b| < 1e-7
 before the last linear solve), whose answer does not depend on the start
@@ -13,14 +13,13 @@ before the last linear solve), whose answer does not depend on the start
 plain FP64 answer.  A "step" solves every domain of the workload once.
 Synthetic seeded inputs; no dataset is used.
 
-Paths: the plain FP64 path (P: the workload's PCG variant, diagonal
-preconditioner, zero start, one domain at a time) and the additions --
-mixed precision (FP32-inner / FP64-refined), the SIA column
-preconditioner (the reference's default), batching (all domains in one
-resident problem), the learned guess (the U-Net behind the C ABI).  The
-headline `value` is learned + mixed + batched (with the column
-preconditioner and Chronopoulos-Gear); `paths` lists every path with its
-iterations and its distance to P's answer.
+Paths: the plain FP64 path (P: FP64, zero start, one domain at a time,
+with the workload's solver -- for the marine workloads the reference's
+default SIA column preconditioner and Chronopoulos-Gear PCG) and the
+additions: mixed precision (FP32-inner / FP64-refined), batching (all
+domains in one resident problem) and the learned guess (the U-Net behind
+the C ABI).  The headline `value` is learned + mixed + batched; `paths`
+lists every path with its iterations and its distance to P's answer.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--workload c4|c2|c1|c0|c3] [--batch B]
@@ -74,7 +73,7 @@ def parse_args(argv=None):
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c4", choices=sorted(WORKLOAD_DESC))
-    ap.add_argument("--batch", type=int, default=8, help="c4 / c3: domains of the workload")
+    ap.add_argument("--batch", type=int, default=4, help="c4 / c3: domains of the workload")
     ap.add_argument("--picard", default="l2rel", choices=sorted(PICARD))
     ap.add_argument("--paths", default="all", help="comma-separated path names, or all")
     ap.add_argument("--other-steps", type=int, default=1, help="timed steps of the non-headline paths")
@@ -102,6 +101,8 @@ def make_models(args):
         ms = configs.ensemble(count=args.batch)
     else:
         ms = [configs.workload(w)]
+    if w in ("c4", "c2"):  # the reference's default preconditioner (glide_types.F90:698)
+        ms = [m.copy(which_precond=configs.PRECOND_SIA) for m in ms]
     # the reference hard-codes maxiters = 200 (glissade_velo_higher_pcg.F90:67-69),
     # which does not reach 1e-8 on these systems; the metric needs converged solves
     return [m.copy(pcg_maxiters=args.pcg_maxiters, which_resid=PICARD[args.picard]) for m in ms]
@@ -109,40 +110,63 @@ def make_models(args):
 
 class Path:
     """One way of solving the workload: start (zero | learned), precision,
-    preconditioner (the workload's | SIA column), PCG variant (the
-    workload's | Chronopoulos-Gear), batched (all domains in one resident
-    problem) or one domain at a time."""
+    preconditioner (None: the workload's; "diag" | "sia" to override), PCG
+    variant (the workload's | Chronopoulos-Gear), batched (all domains in
+    one resident problem) or one domain at a time."""
 
-    def __init__(self, name, start, mixed, colpc, cg, batched):
-        self.name, self.start, self.mixed, self.colpc, self.cg, self.batched = name, start, mixed, colpc, cg, batched
+    def __init__(self, name, start, mixed, precond, cg, batched):
+        self.name, self.start, self.mixed, self.precond, self.cg, self.batched = (name, start, mixed, precond,
+                                                                                 cg, batched)
 
     def model(self, m):
         from cism_b200 import configs
 
-        if self.colpc:
+        if self.precond == "sia":
             m = m.copy(which_precond=configs.PRECOND_SIA)
+        elif self.precond == "diag":
+            m = m.copy(which_precond=configs.PRECOND_DIAG)
         if self.cg:
             m = m.copy(which_sparse=configs.SPARSE_PCG_CHRONGEAR)
         return m
 
-    def describe(self):
+    def describe(self, m):
+        from cism_b200 import configs
+
+        mm = self.model(m)
         return {"start": self.start, "precision": "fp32-inner/fp64-refined" if self.mixed else "fp64",
-                "preconditioner": "sia_column" if self.colpc else "workload's (diagonal)",
-                "pcg": "chronopoulos_gear" if self.cg else "workload's",
+                "preconditioner": "sia_column" if mm.which_precond == configs.PRECOND_SIA else "diagonal",
+                "pcg": "chronopoulos_gear" if mm.which_sparse == configs.SPARSE_PCG_CHRONGEAR else "standard",
                 "domains": "batched in one problem" if self.batched else "one at a time"}
 
 
 def paths_for(args, have_net):
+    """The marine workloads (c4, c2) solve with the reference's default
+    preconditioner (the SIA column one, which_ho_precond = 2) and the
+    Chronopoulos-Gear PCG every reference higher-order test uses, so P and
+    the additions share the preconditioner; plain_fp64_diag (by --paths)
+    is P with the diagonal one.  c0 and c1 specify the diagonal
+    preconditioner and the standard PCG; their additions also swap in the
+    column preconditioner and Chronopoulos-Gear (fp64_colpc isolates that)."""
     multi = args.workload in ("c4", "c3")
-    P = [Path("plain_fp64", "zero", False, False, False, False),
-         Path("fp64_colpc", "zero", False, True, False, False),
-         Path("mixed_colpc_cg" + ("_batched" if multi else ""), "zero", True, True, True, multi)]
-    if have_net:
-        P += [Path("learned_fp64_colpc" + ("_batched" if multi else ""), "learned", False, True, False, multi),
-              Path("learned_mixed_colpc_cg" + ("_batched" if multi else ""), "learned", True, True, True, multi)]
+    sfx = "_batched" if multi else ""
+    if args.workload in ("c4", "c2"):
+        P = [Path("plain_fp64", "zero", False, None, False, False),
+             Path("mixed" + sfx, "zero", True, None, False, multi)]
+        if have_net:
+            P += [Path("learned_fp64" + sfx, "learned", False, None, False, multi),
+                  Path("learned_mixed" + sfx, "learned", True, None, False, multi)]
+        extra = [Path("plain_fp64_diag", "zero", False, "diag", False, False)]
+    else:
+        P = [Path("plain_fp64", "zero", False, None, False, False),
+             Path("fp64_colpc", "zero", False, "sia", False, False),
+             Path("mixed_colpc_cg" + sfx, "zero", True, "sia", True, multi)]
+        if have_net:
+            P += [Path("learned_fp64_colpc" + sfx, "learned", False, "sia", False, multi),
+                  Path("learned_mixed_colpc_cg" + sfx, "learned", True, "sia", True, multi)]
+        extra = []
     if args.paths != "all":
         want = args.paths.split(",")
-        P = [p for p in P if p.name in want]
+        P = [p for p in P + extra if p.name in want]
     return P
 
 
@@ -469,7 +493,7 @@ def run_ours(args, D):
         r = res[p.name]
         sts = r["stats"]
         errs = [rel_l2(a, b) for a, b in zip(r["sols"], ref_sol)]
-        out_paths[p.name] = p.describe() | {
+        out_paths[p.name] = p.describe(models[0]) | {
             "value": round(nd * D.world / (r["ms_per_step"] / 1000.0), 4),
             "ms_per_step": round(r["ms_per_step"], 2), "steps": r["steps"],
             "status": sorted({int(s["status"]) for s in sts}),
@@ -494,17 +518,17 @@ def run_ours(args, D):
             st += ctx.batch_solve([preps[i] for i in g], [zeros[i] for i in g], [zeros[i] for i in g])[3]
         return st
 
-    for _ in range(max(1, args.warmup // 2)):
-        e2e_step()
+    e2e_steps = min(args.steps, 3)  # the same work as the timed steps, fewer of them
+    e2e_step()
     D.barrier()
     ctx.timer_start()
     t0 = time.perf_counter()
-    for _ in range(args.steps):
+    for _ in range(e2e_steps):
         st_e = e2e_step()
     ms_e = max(ctx.timer_stop(), (time.perf_counter() - t0) * 1000.0)
     D.barrier()
     ms_e = D.max(ms_e)
-    e2e = {"value": round(nd * D.world * args.steps / (ms_e / 1000.0), 4), "unit": UNIT,
+    e2e = {"value": round(nd * D.world * e2e_steps / (ms_e / 1000.0), 4), "unit": UNIT, "steps": e2e_steps,
            "h2d_bytes_per_step": int(sum(s["h2d_bytes"] for s in st_e)),
            "d2h_bytes_per_step": int(sum(s["d2h_bytes"] for s in st_e)),
            "call": "bp_batch_solve (C ABI) on host arrays, learned guess formed on the device inside the call"
@@ -556,7 +580,7 @@ def run_ours(args, D):
     }
     if "plain_fp64" in res:
         out["speedup_vs_plain_fp64"] = round(out_paths[head]["value"] / out_paths["plain_fp64"]["value"], 3)
-    if "fp64_colpc" in res:
+    if "fp64_colpc" in res:  # c0, c1: the plain path with the additions' preconditioner
         out["speedup_vs_plain_fp64_same_preconditioner"] = round(
             out_paths[head]["value"] / out_paths["fp64_colpc"]["value"], 3)
     if D.rank == 0 and D.world == 1 and not args.no_cpu_baseline and "plain_fp64" in res:

@@ -1035,20 +1035,51 @@ BP_HD void sia_coefs(const DevView& v, size_t n, int k, int h, double* sub, doub
   }
 }
 
-// easy_sia_solver / tridiag_solver (pcg:2759-2904) for one column of nz
-// levels: the Thomas algorithm in the reference's order.  s holds r on
-// entry and z on exit (stride apart); sup is overwritten with the
-// elimination factors gamma.
-BP_HD void sia_column(int nz, const double* sub, const double* dg, double* sup, double* s, int stride) {
-  double beta = dg[0];
-  s[0] = s[0] / beta;
-  for (int k = 1; k < nz; ++k) {
-    const double gam = sup[k - 1] / beta;
-    sup[k - 1] = gam;
-    beta = dg[k] - sub[k] * gam;
-    s[k * stride] = (s[k * stride] - sub[k] * s[(k - 1) * stride]) / beta;
+// easy_sia_solver / tridiag_solver (pcg:2759-2904) in two halves.  The
+// Thomas algorithm's forward elimination depends on the matrix only: per
+// level k its pivot beta_k (beta_0 = d_0, beta_k = d_k - a_k gamma_k) and
+// multiplier gamma_k = c_{k-1} / beta_{k-1} (gamma_0 = 0), with a, d, c the
+// sub-, main and super-diagonal.  sia_factor_column forms them once per
+// linear solve into v.sia_f [3][npad] ((a, beta, gamma) per node, u and v
+// components); every preconditioner application then runs the two sweeps
+// (sia_solve) in the reference's order and operations, so the result is
+// that of the reference's solver bitwise.
+BP_HD void sia_factor_column(const DevView& v, int col, int h) {
+  const size_t np = (size_t)v.npad;
+  double beta = 0.0, sup_prev = 0.0;
+  for (int k = 0; k < v.nz; ++k) {
+    const size_t n = node_of(v, col, k);
+    double sub, dg, sup;
+    sia_coefs(v, n, k, h, &sub, &dg, &sup);
+    double gam = 0.0;
+    if (k == 0) {
+      beta = dg;
+    } else {
+      gam = sup_prev / beta;
+      beta = dg - sub * gam;
+    }
+    sup_prev = sup;
+    double* f = reinterpret_cast<double*>(v.sia_f);
+    f[(n) * 2 + h] = sub;
+    f[(np + n) * 2 + h] = beta;
+    f[(2 * np + n) * 2 + h] = gam;
   }
-  for (int k = nz - 2; k >= 0; --k) s[k * stride] = s[k * stride] - sup[k] * s[(k + 1) * stride];
+}
+
+// The two sweeps for one column and component h: s holds r on entry and z
+// on exit, level k at s[k * stride]; node(k) is the column's node at level
+// k (its factors in v.sia_f).
+template <typename NodeOf>
+BP_HD void sia_solve(const DevView& v, int nz, int h, NodeOf node, double* s, int stride) {
+  const size_t np = (size_t)v.npad;
+  const double* f = reinterpret_cast<const double*>(v.sia_f);
+  size_t n = node(0);
+  s[0] = s[0] / f[(np + n) * 2 + h];
+  for (int k = 1; k < nz; ++k) {
+    n = node(k);
+    s[k * stride] = (s[k * stride] - f[n * 2 + h] * s[(k - 1) * stride]) / f[(np + n) * 2 + h];
+  }
+  for (int k = nz - 2; k >= 0; --k) s[k * stride] = s[k * stride] - f[(2 * np + node(k + 1)) * 2 + h] * s[(k + 1) * stride];
 }
 
 // FP32 copy of row n of the symmetric matrix for the mixed-precision

@@ -115,8 +115,6 @@ struct DevView {
   int minb_k;              // Krylov matvecs (k_std_mv, k_cg_mv): the same, 0, 4 or 6
   int grid_k;              // CTAs of the Krylov matvecs (0 = one per tile)
   int dry;                 // autotuner pass: Krylov matvecs run every tile, leave the state alone
-  int march;               // Krylov matvecs by column march (k_krylov_march), 0 = thread per node
-  int mv_chunks;           // column march: level chunks per column (1..4)
   int solve2d;             // 2-D solve (shallow-shelf or L1L2): nz = 1, one 2-D element per cell
   int l1l2;                // L1L2: layer viscosities, 3-D velocity reconstructed after the loop
   int diva;                // DIVA: point viscosities carried between iterations, beta_eff, 3-D velocity each iteration
@@ -187,10 +185,11 @@ struct DevView {
   size_t l2_bytes;
   float l2_hit;
   double* badj;            // [4][npad] Dirichlet column moves per block
+  double2* sia_f;          // [3][npad] SIA column preconditioner factors (a, beta, gamma), (u, v); or null
   // vectors (per node, (u,v) pairs)
   double2 *x, *b, *r, *z, *d0, *q, *Az, *Dinv, *usav;
   // reductions
-  double* partials;        // [3][ntiles * 4] (the column march: one per tile and level chunk)
+  double* partials;        // [3][ntiles]
   unsigned* tile_counter;  // [ninst]
 };
 

@@ -244,24 +244,15 @@ DevView make_view(Arena& a, cudaStream_t s, const HostPlan& p, bool with_cells, 
   // the hole slots of the node vectors stay zero
   for (double2* vec : {v.x, v.b, v.r, v.d0, v.z, v.q, v.Az, v.Dinv, v.usav})
     CK(cudaMemsetAsync(vec, 0, sizeof(double2) * np, s));
+  bool any_sia = false;
+  for (const auto& ip : p.inst) any_sia = any_sia || ip.precond == 2;
+  v.sia_f = any_sia ? a.get<double2>(s, "sia_f", 3 * np) : nullptr;
   if (mixed && v.sym) {
     float4* blk = a.get<float4>(s, "A32", 16 * np);  // A32 then A32d: one L2 window
     v.A32 = blk;
     v.A32d = reinterpret_cast<double2*>(blk + 14 * np);
   }
-  v.partials = a.get<double>(s, "partials", 3 * 4 * (size_t)std::max(p.ntiles, 1));
-  // Krylov matvecs by column march where a warp holds whole tiles (W <= 32,
-  // nz >= 8), in as many level chunks (<= 4) as give about 16 warps per SM;
-  // BP_MARCH=0 keeps the thread-per-node kernels
-  const char* me = std::getenv("BP_MARCH");
-  v.march = (p.W <= 32 && v.sym && !(me && me[0] == '0')) ? 1 : 0;
-  {
-    const long warps = ((long)p.ntiles * p.W + 31) / 32;
-    const long target = 148L * 16;
-    long nch = warps > 0 ? (target + warps - 1) / warps : 1;
-    if (const char* ce = std::getenv("BP_MARCH_CHUNKS")) nch = std::atoi(ce);
-    v.mv_chunks = (int)std::max(1L, std::min({nch, 4L, (long)std::max(1, p.nz / 2)}));
-  }
+  v.partials = a.get<double>(s, "partials", 3 * (size_t)std::max(p.ntiles, 1));
   v.tile_counter = a.get<unsigned>(s, "tile_counter", p.ninst);
   CK(cudaMemsetAsync(v.tile_counter, 0, sizeof(unsigned) * p.ninst, s));
   return v;
@@ -608,6 +599,7 @@ void picard_head(bp_problem* P, bool tune) {
   if (v.diva) L(P, C_ASM1, [&] { launch_diva_beta(v, s); });  // omega, beta_eff (:2742-2857)
   L(P, C_ASM2, [&] { launch_asm_rows(v, s); });
   L(P, C_RHS, [&] { launch_rhs(v, s); });
+  if (v.sia_f) L(P, C_OTHER, [&] { launch_sia_factor(v, s); });
   if (tune && !P->tuned) autotune(P);
   if (P->v.A32) L(P, C_OTHER, [&] { launch_make_a32(P->v, s); });
   L(P, C_CHECK, [&] { launch_mv(MV_INIT, P->v, s); });
@@ -1336,6 +1328,7 @@ int bp_pcg(bp_ctx* c, int nx, int ny, int nz, int periodic,
   CK(cudaMemcpyAsync(v.x, x.data(), sizeof(double2) * P.plan.npad, cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(v.b, b.data(), sizeof(double2) * P.plan.npad, cudaMemcpyHostToDevice, c->stream));
   init_state(c->stream, v, P.plan, false, true);
+  launch_sia_factor(v, c->stream);
   launch_dinv(v, precond, c->stream);
   launch_bb(v, c->stream);
   linear_solve(&P);

@@ -458,13 +458,13 @@ __global__ void __launch_bounds__(kTile) k_rhs(DevView v) {
 
 // ---------------------------------------------------------------------
 // SIA column preconditioner on a tile of whole columns: every thread puts
-// its node's r and tridiagonal coefficients into shared memory, one thread
-// per (column, component) runs the Thomas solve, every thread takes back
-// its z.  Called by all threads of the CTA (uniform per tile).
+// its node's r into shared memory, one thread per (column, component) runs
+// the two Thomas sweeps with the factors of the linear solve (sia_solve),
+// every thread takes back its z.  Called by all threads of the CTA
+// (uniform per tile).
 // ---------------------------------------------------------------------
 struct SiaTile {
   double s[2 * kTile];
-  double sub[2][kTile], dg[2][kTile], sup[2][kTile];
 };
 
 __device__ __forceinline__ double2 sia_tile(const DevView& v, const TileRange& R, double2 r) {
@@ -474,16 +474,14 @@ __device__ __forceinline__ double2 sia_tile(const DevView& v, const TileRange& R
   // shared memory holds the tile column by column: j = c * nz + k
   const int k = tile_k(v, i), j = (i & (v.W - 1)) * nz + k;
   if (mine) {
-    const size_t n = (size_t)R.n0 + i;
     T.s[2 * j] = r.x;
     T.s[2 * j + 1] = r.y;
-    sia_coefs(v, n, k, 0, &T.sub[0][j], &T.dg[0][j], &T.sup[0][j]);
-    sia_coefs(v, n, k, 1, &T.sub[1][j], &T.dg[1][j], &T.sup[1][j]);
   }
   __syncthreads();
   if (i < 2 * R.ncols) {
-    const int c = i >> 1, h = i & 1, b = c * nz;
-    sia_column(nz, &T.sub[h][b], &T.dg[h][b], &T.sup[h][b], &T.s[2 * b + h], 2);
+    const int c = i >> 1, h = i & 1, lsh = v.lsh;
+    const size_t n0 = (size_t)R.n0 + c;
+    sia_solve(v, nz, h, [&](int kk) { return n0 + ((size_t)kk << lsh); }, &T.s[2 * c * nz + h], 2);
   }
   __syncthreads();
   const double2 z = mine ? make_double2(T.s[2 * j], T.s[2 * j + 1]) : make_double2(0.0, 0.0);
@@ -805,257 +803,6 @@ __global__ void __launch_bounds__(kTile, MINB) k_cg_mv(DevView v) {
   }
 }
 
-// ---------------------------------------------------------------------
-// Krylov matvec by column march (the solve's dominant kernel).  A warp
-// holds 32 consecutive column slots (32 / W whole tiles); each thread walks
-// down its column through one chunk of levels [k0, k1) (v.mv_chunks chunks
-// per column).  The blocked layout makes every load of the warp a run of
-// consecutive nodes.  The source values of the column and of its j-1 and
-// j+1 row neighbours (the centre of each stencil row) are kept for levels
-// k-1, k, k+1, so a level costs three source loads; the i-1 and i+1
-// neighbours come from the adjacent lanes by shuffles wherever the adjacent
-// lane holds exactly that column (checked by node), else from memory.  In
-// FP32 storage the transposed entries toward the row's own k-1 neighbours
-// (offsets 3, 4, 5) and toward the i-1 neighbour (offset 12) come from the
-// previous level's and the adjacent lane's own entries.  The summation order
-// over the 27 offsets is the reference's (kA, jA, iA), as in the per-node
-// rows.  Dot products: per tile and chunk, summed in order by the last
-// arrival of the instance (march_finish).
-// ---------------------------------------------------------------------
-__device__ __forceinline__ double2 shfl_d2(double2 a, int src) {
-  return make_double2(__shfl_sync(0xffffffffu, a.x, src), __shfl_sync(0xffffffffu, a.y, src));
-}
-__device__ __forceinline__ float4 shfl_f4(float4 a, int src) {
-  return make_float4(__shfl_sync(0xffffffffu, a.x, src), __shfl_sync(0xffffffffu, a.y, src),
-                     __shfl_sync(0xffffffffu, a.z, src), __shfl_sync(0xffffffffu, a.w, src));
-}
-
-// Partial sums of the W-lane groups of a warp (one tile each) for level
-// chunk ch; the last arrival of an instance (ntiles x nch partials) sums
-// them in (tile, chunk) order and calls fin.  Called by all 32 lanes;
-// `active` is uniform within a group.
-template <int NV, typename Fin>
-__device__ __forceinline__ void march_finish(const DevView& v, int t, int ch, int inst, bool active,
-                                             double (&val)[NV], Fin fin) {
-  const int W = v.W, nch = v.mv_chunks;
-  const int lane = threadIdx.x & 31, g0 = lane & ~(W - 1);
-#pragma unroll
-  for (int i = 0; i < NV; ++i)
-    for (int o = W >> 1; o > 0; o >>= 1) val[i] += __shfl_xor_sync(0xffffffffu, val[i], o);
-  int last = 0;
-  if (lane == g0 && active) {
-#pragma unroll
-    for (int i = 0; i < NV; ++i) v.partials[(size_t)i * v.ntiles * 4 + (size_t)t * nch + ch] = val[i];
-    __threadfence();
-    const InstParams& ip = v.inst[inst];
-    const unsigned nparts = (unsigned)((ip.tile_end - ip.tile_begin) * nch);
-    last = atomicAdd(&v.tile_counter[inst], 1u) == nparts - 1 ? 1 : 0;
-  }
-  last = __shfl_sync(0xffffffffu, last, g0);
-  if (last) {
-    __threadfence();
-    const unsigned gmask = W == 32 ? 0xffffffffu : (((1u << W) - 1u) << g0);
-    const InstParams& ip = v.inst[inst];
-    double sum[NV];
-#pragma unroll
-    for (int i = 0; i < NV; ++i) sum[i] = 0.0;
-    for (int q = ip.tile_begin * nch + (lane - g0); q < ip.tile_end * nch; q += W)
-#pragma unroll
-      for (int i = 0; i < NV; ++i) sum[i] += __ldcg(v.partials + (size_t)i * v.ntiles * 4 + q);
-#pragma unroll
-    for (int i = 0; i < NV; ++i)
-      for (int o = W >> 1; o > 0; o >>= 1) sum[i] += __shfl_xor_sync(gmask, sum[i], o);
-    if (lane == g0) {
-      v.tile_counter[inst] = 0;
-      fin(inst, sum);
-      __threadfence();
-    }
-  }
-}
-
-// MODE: MV_STD_A (q = A d, (d, q)), MV_CG_FIRST (d = z, q = A z) or MV_CG1
-// (Az = A z), the last two with (r, z), (A z, z), (r, r).  STORE: ST_SYM or
-// ST_SYM32; a mixed instance whose Krylov matvec fell back to FP64
-// (krylov_fp64) takes the per-node FP64 row on its lanes.
-template <int MODE, int STORE, int MINB>
-__global__ void __launch_bounds__(kTile, MINB) k_krylov_march(DevView v) {
-  pdl_wait();
-  pdl_launch_next();
-  constexpr bool F32 = STORE == ST_SYM32;
-  constexpr int NV = MODE == MV_STD_A ? 1 : 3;
-  const double2* __restrict__ src = MODE == MV_STD_A ? v.d0 : v.z;
-  const int lane = threadIdx.x & 31;
-  const int W = v.W, lsh = v.lsh, nz = v.nz, nch = v.mv_chunks, nc = v.ncols;
-  const size_t np = (size_t)v.npad;
-  const int tpw = 32 >> lsh;  // tiles per warp
-  const int nwarp = (v.ntiles + tpw - 1) / tpw;
-  const int per = (nz + nch - 1) / nch;
-  const int up = (lane + 31) & 31, dn = (lane + 1) & 31;
-  for (int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; gw < nwarp * nch;
-       gw += (gridDim.x * blockDim.x) >> 5) {
-    const int wi = gw / nch, ch = gw - wi * nch;
-    const int t = wi * tpw + (lane >> lsh), c = lane & (W - 1);
-    int inst = 0, col = -1;
-    bool active = false, f64lane = false;
-    if (t < v.ntiles) {
-      inst = v.tile_inst[t];
-      const InstState& S = v.st[inst];
-      active = S.pcg_active || v.dry;
-      if (c < v.tile_ncols[t]) col = v.tile_col0[t] + c;
-      f64lane = F32 && S.krylov_fp64;
-    }
-    const bool valid = active && col >= 0;
-    if (v.mv_nodes && !v.dry && valid && c == 0 && ch == 0)
-      atomicAdd(&v.mv_nodes[F32 && !f64lane ? 1 : 0], (unsigned long long)v.tile_ncols[t] * nz);
-    const int k0 = min(nz, ch * per), k1 = min(nz, k0 + per);
-    int cn[9];  // the neighbours' nodes at level 0
-#pragma unroll
-    for (int q = 0; q < 9; ++q) cn[q] = valid ? v.col_nbn[q * nc + col] : -1;
-    const int n0 = valid ? v.col_node[col] : -1;
-    const int ctr[3] = {cn[1], n0, cn[7]};
-    bool lok[3], rok[3];
-#pragma unroll
-    for (int r = 0; r < 3; ++r) {
-      const int cu = __shfl_sync(0xffffffffu, ctr[r], up), cd = __shfl_sync(0xffffffffu, ctr[r], dn);
-      lok[r] = lane > 0 && cn[3 * r] >= 0 && cn[3 * r] == cu;
-      rok[r] = lane < 31 && cn[3 * r + 2] >= 0 && cn[3 * r + 2] == cd;
-    }
-    double2 w[3][3];  // source of the row centres at levels k-1, k, k+1
-#pragma unroll
-    for (int r = 0; r < 3; ++r)
-#pragma unroll
-      for (int tt = 0; tt < 2; ++tt) {
-        const int kn = k0 - 1 + tt;
-        w[r][tt] = (ctr[r] >= 0 && kn >= 0 && kn < nz) ? src[(size_t)ctr[r] + ((size_t)kn << lsh)]
-                                                        : make_double2(0.0, 0.0);
-      }
-    float4 keep[3];  // FP32: own entries of offsets 21, 22, 23 at level k-1
-#pragma unroll
-    for (int tt = 0; tt < 3; ++tt)
-      keep[tt] = (F32 && valid && k0 > 0)
-                     ? BP_LD_RO(v.A32 + (size_t)(8 + tt) * np + (size_t)n0 + ((size_t)(k0 - 1) << lsh))
-                     : make_float4(0.f, 0.f, 0.f, 0.f);
-    double part[NV];
-#pragma unroll
-    for (int i = 0; i < NV; ++i) part[i] = 0.0;
-    for (int k = k0; k < k1; ++k) {
-#pragma unroll
-      for (int r = 0; r < 3; ++r)
-        w[r][2] = (ctr[r] >= 0 && k + 1 < nz) ? src[(size_t)ctr[r] + ((size_t)(k + 1) << lsh)]
-                                              : make_double2(0.0, 0.0);
-      const size_t n = valid ? (size_t)n0 + ((size_t)k << lsh) : 0;
-      float4 own[14];
-      if (F32) {
-#pragma unroll
-        for (int j = 1; j < 14; ++j)
-          own[j] = valid ? BP_LD_RO(v.A32 + (size_t)j * np + n) : make_float4(0.f, 0.f, 0.f, 0.f);
-      }
-      double yu = 0.0, yv = 0.0;
-#pragma unroll
-      for (int kA = -1; kA <= 1; ++kA) {
-        const int kn = k + kA;
-        const bool kin = kn >= 0 && kn < nz;
-#pragma unroll
-        for (int r = 0; r < 3; ++r) {
-          const double2 cv = w[r][kA + 1];
-          const double2 lv = shfl_d2(cv, up), rv = shfl_d2(cv, dn);
-          float4 tl = make_float4(0.f, 0.f, 0.f, 0.f), tc = tl, tr = tl;
-          if (F32 && r == 1 && kA == -1) {  // offsets 3, 4, 5: m' = 23, 22, 21 of (k-1, i-1 / i / i+1)
-            tl = shfl_f4(keep[2], up);
-            tc = keep[1];
-            tr = shfl_f4(keep[0], dn);
-          }
-          if (F32 && r == 1 && kA == 0) tl = shfl_f4(own[1], up);  // offset 12: m' = 14 of (k, i-1)
-#pragma unroll
-          for (int iA = -1; iA <= 1; ++iA) {
-            const int q = 3 * r + iA + 1, m = (kA + 1) * 9 + q;
-            const bool ok = valid && kin && cn[q] >= 0;
-            const size_t p = ok ? (size_t)cn[q] + ((size_t)kn << lsh) : n;
-            double2 sv;
-            if (iA == 0) sv = cv;
-            else if (iA < 0) sv = lok[r] ? lv : (ok ? src[p] : make_double2(0.0, 0.0));
-            else sv = rok[r] ? rv : (ok ? src[p] : make_double2(0.0, 0.0));
-            if (!ok) sv = make_double2(0.0, 0.0);
-            if (F32) {
-              if (m == 13) {
-                const double2 a0 = valid ? BP_LD_RO(v.A32d + n) : make_double2(0.0, 0.0);
-                const double2 a1 = valid ? BP_LD_RO(v.A32d + np + n) : make_double2(0.0, 0.0);
-                yu += a0.x * sv.x + a0.y * sv.y;
-                yv += a1.x * sv.x + a1.y * sv.y;
-              } else if (m > 13) {
-                const float4 a = own[m - 13];
-                yu += (double)a.x * sv.x + (double)a.y * sv.y;
-                yv += (double)a.z * sv.x + (double)a.w * sv.y;
-              } else {
-                bool kept = false;
-                float4 b = make_float4(0.f, 0.f, 0.f, 0.f);
-                if (r == 1 && kA == -1) {
-                  kept = iA == 0 || (iA < 0 ? lok[1] : rok[1]);
-                  b = iA < 0 ? tl : (iA == 0 ? tc : tr);
-                } else if (r == 1 && kA == 0 && iA < 0) {
-                  kept = lok[1];
-                  b = tl;
-                }
-                if (!kept) b = ok ? BP_LD_RO(v.A32 + (size_t)(13 - m) * np + p) : make_float4(0.f, 0.f, 0.f, 0.f);
-                yu += (double)b.x * sv.x + (double)b.z * sv.y;
-                yv += (double)b.y * sv.x + (double)b.w * sv.y;
-              }
-            } else {
-              if (m >= 13) {
-                const double2 a0 = valid ? BP_LD_RO(v.A + (size_t)(m - 13) * np + n) : make_double2(0.0, 0.0);
-                const double2 a1 = valid ? BP_LD_RO(v.A + (size_t)(14 + m - 13) * np + n) : make_double2(0.0, 0.0);
-                yu += a0.x * sv.x + a0.y * sv.y;
-                yv += a1.x * sv.x + a1.y * sv.y;
-              } else {
-                const double2 b0 = ok ? BP_LD_RO(v.A + (size_t)(13 - m) * np + p) : make_double2(0.0, 0.0);
-                const double2 b1 = ok ? BP_LD_RO(v.A + (size_t)(14 + 13 - m) * np + p) : make_double2(0.0, 0.0);
-                yu += b0.x * sv.x + b1.x * sv.y;
-                yv += b0.y * sv.x + b1.y * sv.y;
-              }
-            }
-          }
-        }
-      }
-      double2 y = make_double2(yu, yv);
-      if (F32 && f64lane && valid) y = matvec_row_sym(v, v.A, col, k, n, SrcX{src});
-      if (valid) {
-        const double2 z = w[1][1];
-        if (MODE == MV_STD_A) {
-          v.q[n] = y;
-          part[0] += z.x * y.x + z.y * y.y;
-        } else {
-          const double2 rr = v.r[n];
-          if (MODE == MV_CG_FIRST) {
-            v.d0[n] = z;
-            v.q[n] = y;
-          } else {
-            v.Az[n] = y;
-          }
-          part[0] += rr.x * z.x + rr.y * z.y;
-          part[1 % NV] += y.x * z.x + y.y * z.y;
-          part[2 % NV] += rr.x * rr.x + rr.y * rr.y;
-        }
-      }
-      if (F32) {
-        keep[0] = own[8];
-        keep[1] = own[9];
-        keep[2] = own[10];
-      }
-#pragma unroll
-      for (int r = 0; r < 3; ++r) {
-        w[r][0] = w[r][1];
-        w[r][1] = w[r][2];
-      }
-    }
-    const bool tile_on = t < v.ntiles && active;
-    march_finish<NV>(v, t < v.ntiles ? t : 0, ch, inst, tile_on, part, [&](int in, const double* sm) {
-      if (MODE == MV_STD_A) std_mv_fin(v, in, sm);
-      else if (MODE == MV_CG_FIRST) cg_mv_fin<true>(v, in, sm);
-      else cg_mv_fin<false>(v, in, sm);
-    });
-  }
-}
-
 // Chronopoulos-Gear first-pass update: x += alpha d; r -= alpha q; z = D^-1 r.
 __global__ void __launch_bounds__(kTile) k_cg_first_update(DevView v) {
   pdl_wait();
@@ -1190,6 +937,18 @@ __global__ void __launch_bounds__(kTile) k_make_a32(DevView v) {
     const int col = tile_col(v, R, threadIdx.x), k = tile_k(v, threadIdx.x);
     make_a32_row(v, col, k, (size_t)n);
   }
+}
+
+// Factors of the SIA column preconditioner for the linear solve ahead:
+// one thread per (column, component) of the instances that use it and are
+// solving (sia_factor_column).
+__global__ void __launch_bounds__(256) k_sia_factor(DevView v) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 2L * v.ncols) return;
+  const int col = (int)(t >> 1), h = (int)(t & 1);
+  const int inst = v.col_inst[col];
+  if (v.inst[inst].precond != 2 || !v.st[inst].pcg_active) return;
+  sia_factor_column(v, col, h);
 }
 
 // Post-solve diagnostics (glissade_velo_higher.F90:3847-3872) at the
@@ -1406,35 +1165,7 @@ static void launch_resid_minb(int mode, const DevView& v, cudaStream_t s, int g)
   if (v.minb == 4) launch_resid_store<STORE, 4>(mode, v, s, g);
   else launch_resid_store<STORE, 0>(mode, v, s, g);
 }
-template <int STORE, int MINB>
-static TileKernel march_kernel(int mode) {
-  switch (mode) {
-    case MV_STD_A: return k_krylov_march<MV_STD_A, STORE, MINB>;
-    case MV_CG_FIRST: return k_krylov_march<MV_CG_FIRST, STORE, MINB>;
-    default: return k_krylov_march<MV_CG1, STORE, MINB>;
-  }
-}
-// Column march: CTAs of 8 warps, one warp per (32 column slots, level chunk);
-// BP_MARCH_MINB=2 builds for two resident CTAs per SM.
-static const int g_march_minb = [] {
-  const char* e = std::getenv("BP_MARCH_MINB");
-  return e ? std::atoi(e) : 1;
-}();
-static void launch_march(int mode, const DevView& v, cudaStream_t s) {
-  const int tpw = 32 >> v.lsh;
-  const long warps = (long)((v.ntiles + tpw - 1) / tpw) * v.mv_chunks;
-  const int g = (int)std::max(1L, (warps + 7) / 8);
-  TileKernel k;
-  if (v.A32) k = g_march_minb == 2 ? march_kernel<ST_SYM32, 2>(mode) : march_kernel<ST_SYM32, 1>(mode);
-  else k = g_march_minb == 2 ? march_kernel<ST_SYM, 2>(mode) : march_kernel<ST_SYM, 1>(mode);
-  launch_pcg(k, g, s, v, kTile);  // 8 warps, each its own column slots
-}
-
 void launch_mv(int mode, const DevView& v, cudaStream_t s) {
-  if (is_krylov(mode) && v.march) {
-    launch_march(mode, v, s);
-    return;
-  }
   if (is_krylov(mode)) {
     int g = v.ntiles > 0 ? v.ntiles : 1;
     if (v.grid_k > 0 && g > v.grid_k) g = v.grid_k;
@@ -1481,6 +1212,9 @@ void launch_loop_cond(cudaGraphConditionalHandle h, const DevView& v, bool picar
   k_loop_cond<<<1, 1, 0, s>>>(h, active, iter, cap, reset ? 1 : 0);
 }
 void launch_make_a32(const DevView& v, cudaStream_t s) { k_make_a32<<<tile_grid(v), v.tile_threads, 0, s>>>(v); }
+void launch_sia_factor(const DevView& v, cudaStream_t s) {
+  if (v.sia_f && v.ncols > 0) k_sia_factor<<<(unsigned)((2L * v.ncols + 255) / 256), 256, 0, s>>>(v);
+}
 void launch_matvec_plain(const DevView& v, const double2* x, double2* y, cudaStream_t s) {
   k_matvec_plain<<<tile_grid(v), v.tile_threads, 0, s>>>(v, x, y);
 }

@@ -47,6 +47,9 @@ void launch_loop_cond(cudaGraphConditionalHandle h, const DevView& v, bool picar
 // for the launches of the calling thread.
 void set_pdl(bool on);
 void launch_make_a32(const DevView& v, cudaStream_t s);
+// The SIA column preconditioner's factors (v.sia_f) of the solving
+// instances that use it, from the assembled matrix.
+void launch_sia_factor(const DevView& v, cudaStream_t s);
 void launch_matvec_plain(const DevView& v, const double2* x, double2* y, cudaStream_t s);
 void launch_dinv(const DevView& v, int precond, cudaStream_t s);
 void launch_bb(const DevView& v, cudaStream_t s);

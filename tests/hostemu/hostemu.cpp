@@ -208,16 +208,21 @@ extern "C" int emu_sia_apply(int nx, int ny, int nz, int periodic, const int* ac
     gather_matrix(E.p, Auu, Auv, Avu, Avv, E.A.data());
   }
   gather_velocity(E.p, 0, ru, rv, E.x.data());
-  std::vector<double> s(2 * (size_t)nz), sub(nz), dg(nz), sup(nz);
+  // the factors of the linear solve (k_sia_factor), then the two sweeps per
+  // column and component (sia_tile)
+  std::vector<double2> f(3 * (size_t)E.p.npad, double2{0, 0});
+  E.v.sia_f = f.data();
+  for (int c = 0; c < E.p.ncols; ++c)
+    for (int h = 0; h < 2; ++h) sia_factor_column(E.v, c, h);
+  std::vector<double> s((size_t)nz);
   std::vector<double2> z(E.p.npad, double2{0, 0});
   for (int c = 0; c < E.p.ncols; ++c) {
     for (int h = 0; h < 2; ++h) {
       for (int k = 0; k < nz; ++k) {
         const size_t n = node_of(E.p, c, k);
-        sia_coefs(E.v, n, k, h, &sub[k], &dg[k], &sup[k]);
         s[k] = h ? E.x[n].y : E.x[n].x;
       }
-      sia_column(nz, sub.data(), dg.data(), sup.data(), s.data(), 1);
+      sia_solve(E.v, nz, h, [&](int k) { return node_of(E.p, c, k); }, s.data(), 1);
       for (int k = 0; k < nz; ++k) (h ? z[node_of(E.p, c, k)].y : z[node_of(E.p, c, k)].x) = s[k];
     }
   }

@@ -1,12 +1,10 @@
-"""GPU tests of the engine's execution paths: the column-march Krylov
-matvec against the per-node kernels, the device-resident Picard loop
-against the host-driven one, and the learned guess behind the C ABI
+"""GPU tests of the engine's execution paths: the device-resident Picard
+loop against the host-driven one, and the learned guess behind the C ABI
 against the network's Python forward.
 
-Tolerances: march vs per-node on one assembled system with a fixed PCG
-iteration count, 1e-11 relative L2 (the dot products sum in another order);
-device loop vs host loop, bitwise (the same kernels in the same order); the
-C-ABI guess vs the Python forward of the same weights, 1e-6 relative
+Tolerances: device loop vs host loop, bitwise (the same kernels in the
+same order); the C-ABI guess vs the Python forward of the same weights,
+1e-6 relative
 (identical arithmetic and BF16 rounding points; a last-bit difference of
 log10 can move one BF16 input by one unit).
 """
@@ -43,46 +41,6 @@ class _Env:
                 os.environ.pop(k, None)
             else:
                 os.environ[k] = v
-
-
-def _one_picard_fixed_pcg(ctx, m, precision):
-    """One Picard iteration from a fixed start with exactly 40 PCG
-    iterations (tolerance 0): assembly, FP32 copy and 40 Krylov passes."""
-    m = m.copy(maxiter_nonlinear=1, pcg_maxiters=40, pcg_tol=0.0)
-    rng = np.random.default_rng(5)
-    prep, _, _ = solver.prepare(m, precision=precision)
-    av = prep.arrays["active_vertex"].astype(bool)[..., None]
-    u0 = configs.halo_fill_stag(50.0 * rng.standard_normal(m.vshape3) * av, m.periodic)
-    v0 = configs.halo_fill_stag(50.0 * rng.standard_normal(m.vshape3) * av, m.periodic)
-    prob = ctx.problem([prep])
-    prob.set_guess([u0], [v0])
-    st = prob.run()[0]
-    u, v, _ = prob.get()
-    prob.close()
-    return u[0], v[0], st
-
-
-@pytest.mark.parametrize("variant", [configs.SPARSE_PCG_STANDARD, configs.SPARSE_PCG_CHRONGEAR])
-@pytest.mark.parametrize("precision", [solver.FP64, solver.MIXED])
-@pytest.mark.parametrize("name", list(MODELS))
-def test_march_matvec_matches_per_node(ctx, name, precision, variant):
-    m = MODELS[name].copy(which_sparse=variant)
-    with _Env(BP_MARCH="0"):
-        ua, va, sa = _one_picard_fixed_pcg(ctx, m, precision)
-    ub, vb, sb = _one_picard_fixed_pcg(ctx, m, precision)  # column march (default)
-    assert sa["pcg_iters_total"] == sb["pcg_iters_total"] == 40
-    assert rel_l2([ub, vb], [ua, va]) < 1e-11
-
-
-@pytest.mark.parametrize("chunks", ["1", "3"])
-def test_march_level_chunks(ctx, chunks):
-    # the column split into level chunks (several warps per column block)
-    m = MODELS["marine40x40x11"]
-    with _Env(BP_MARCH="0"):
-        ua, va, _ = _one_picard_fixed_pcg(ctx, m, solver.MIXED)
-    with _Env(BP_MARCH_CHUNKS=chunks):
-        ub, vb, _ = _one_picard_fixed_pcg(ctx, m, solver.MIXED)
-    assert rel_l2([ub, vb], [ua, va]) < 1e-11
 
 
 @pytest.mark.parametrize("precision", [solver.FP64, solver.MIXED])
