@@ -500,7 +500,9 @@ def run_ours(args, D):
             "picard_iters_mean": round(float(np.mean([s["picard_iters"] for s in sts])), 2),
             "pcg_iters_mean": round(float(np.mean([s["pcg_iters_total"] for s in sts])), 1),
             "final_rel_resid_max": float("%.3e" % max(s["pcg_err_last"] for s in sts)),
-            "rel_l2_vs_plain_fp64_max": float("%.3e" % max(errs))}
+            "rel_l2_vs_plain_fp64_max": float("%.3e" % max(errs)),
+            "per_domain": [{"picard_iters": int(s["picard_iters"]), "pcg_iters_total": int(s["pcg_iters_total"])}
+                           for s in sts]}
     # accepted: every domain converged (status 0, last linear solve < 1e-8)
     # and within 1e-6 relative L2 of the plain FP64 answer
     hd = out_paths[head]

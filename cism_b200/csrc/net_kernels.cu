@@ -2,8 +2,9 @@
 // U-Net over the vertex grid, trained and run on the device.
 //
 // Activations are NHWC ([pixel][channel]) in BF16; every contraction is a
-// tensor-core GEMM (mma.sync m16n8k16, BF16 operands, FP32 accumulation)
-// over K-contiguous operands:
+// tensor-core GEMM on tcgen05 (k_gemm_tc: BF16 operands from shared memory,
+// FP32 accumulator in tensor memory; the mma.sync kernel k_gemm_tn remains
+// for comparison) over K-contiguous operands:
 //   forward  Y[P][Cout]  = col(X)[P][K] . W[Cout][K]^T            (K = 9 Cin)
 //   dgrad    dcol[P][K]  = dY[P][Cout] . WT[K][Cout]^T, then col2im
 //   wgrad    dW[Cout][K] = dYT[Cout][P] . colT[K][P]^T
@@ -16,6 +17,8 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstdlib>
+#include <cstring>
 
 namespace {
 
@@ -387,18 +390,212 @@ inline unsigned grid_for(long long n) {
   return (unsigned)(g < 1 ? 1 : g);
 }
 
+// ---------------------------------------------------------------------
+// The same GEMM on the 5th-generation tensor cores (tcgen05): one CTA of
+// four warps per 128 x 64 tile of C, its FP32 accumulator in tensor memory
+// (64 of the SM's 512 TMEM columns, lane = row), the operands staged in
+// shared memory in the K-major no-swizzle core-matrix layout (8 rows x 16
+// bytes per 128-byte core matrix) that the UMMA shared-memory descriptor
+// describes, two stages deep: while the tensor core multiplies one 64-deep
+// K slice the threads load the next.  One thread issues the four K = 16
+// tcgen05.mma of a slice and commits them to the stage's mbarrier; the
+// stage is refilled once that barrier completes.  The epilogue reads the
+// accumulator with tcgen05.ld (warp w: rows 32w..32w+31) and adds the bias
+// (and C).  Every wait is bounded: past the limit the kernel raises
+// g_tc_err, stops issuing, frees its tensor memory and returns.
+// ---------------------------------------------------------------------
+constexpr int TC_BM = 128, TC_BN = 64, TC_BK = 64;
+constexpr int TC_A_BYTES = TC_BM * TC_BK * 2, TC_B_BYTES = TC_BN * TC_BK * 2;
+constexpr int TC_STAGE = TC_A_BYTES + TC_B_BYTES;  // 24 KB; two stages in 48 KB of dynamic shared memory
+
+__device__ int g_tc_err = 0;  // a wait of k_gemm_tc ran out (read and cleared by bpnet_gemm_status)
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// UMMA shared-memory descriptor, K-major, no swizzle: start address, leading
+// byte offset (between the two 16-byte K chunks of one K = 16 step), stride
+// byte offset (between 8-row groups), version 1, base offset 0, layout 0.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | ((uint64_t)1 << 46);
+}
+
+// Instruction descriptor of kind::f16: FP32 accumulator (bits 4-5 = 1), A
+// and B BF16 (bits 7-9, 10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4
+// at bit 24.
+constexpr uint32_t TC_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TC_BN >> 3) << 17) |
+                              ((uint32_t)(TC_BM >> 4) << 24);
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  for (int i = 0; i < (1 << 24); ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  atomicExch(&g_tc_err, 1);
+  return false;
+}
+
+__global__ void __launch_bounds__(128) k_gemm_tc(const bf16* __restrict__ A, const bf16* __restrict__ B,
+                                                 float* __restrict__ C, const float* __restrict__ bias,
+                                                 int M, int N, int K, int lda, int ldb, int ldc,
+                                                 int accum) {
+  extern __shared__ __align__(1024) uint8_t tc_smem[];
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ uint32_t tmem_slot;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int m0 = blockIdx.y * TC_BM, n0 = blockIdx.x * TC_BN;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                 "r"(TC_BN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar[0])));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar[1])));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_slot;
+  const int nk = (K + TC_BK - 1) / TC_BK;
+  bool ok = true;
+  for (int it = 0; it < nk; ++it) {
+    const int st = it & 1;
+    uint8_t* As = tc_smem + st * TC_STAGE;
+    uint8_t* Bs = As + TC_A_BYTES;
+    if (it >= 2) ok = mbar_wait(smem_u32(&bar[st]), ((it - 2) >> 1) & 1);  // the stage's last slice is done
+    if (!__syncthreads_and(ok)) {
+      ok = false;
+      break;
+    }
+    const int k0 = it * TC_BK;
+    for (int c = tid; c < TC_BM * 8; c += 128) {  // 128 rows x 8 chunks of 8 K elements
+      const int r = c >> 3, kc = c & 7, gm = m0 + r, gk = k0 + kc * 8;
+      uint4 val = make_uint4(0u, 0u, 0u, 0u);
+      if (gm < M && gk < K) val = __ldg(reinterpret_cast<const uint4*>(A + (size_t)gm * lda + gk));
+      *reinterpret_cast<uint4*>(As + (kc * (TC_BM / 8) + (r >> 3)) * 128 + (r & 7) * 16) = val;
+    }
+    for (int c = tid; c < TC_BN * 8; c += 128) {
+      const int r = c >> 3, kc = c & 7, gn = n0 + r, gk = k0 + kc * 8;
+      uint4 val = make_uint4(0u, 0u, 0u, 0u);
+      if (gn < N && gk < K) val = __ldg(reinterpret_cast<const uint4*>(B + (size_t)gn * ldb + gk));
+      *reinterpret_cast<uint4*>(Bs + (kc * (TC_BN / 8) + (r >> 3)) * 128 + (r & 7) * 16) = val;
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // the tensor core reads through the async proxy
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+      for (int s = 0; s < TC_BK / 16; ++s) {
+        if (k0 + 16 * s >= K) break;
+        const uint64_t ad = umma_desc(smem_u32(As) + 2 * s * (TC_BM / 8) * 128, (TC_BM / 8) * 128, 128);
+        const uint64_t bd = umma_desc(smem_u32(Bs) + 2 * s * (TC_BN / 8) * 128, (TC_BN / 8) * 128, 128);
+        const uint32_t acc = (it > 0 || s > 0) ? 1u : 0u;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+            ::"r"(tmem), "l"(ad), "l"(bd), "r"(TC_IDESC), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       smem_u32(&bar[st]))
+                   : "memory");
+    }
+  }
+  // the last commit completes after every multiply of the tile
+  if (ok) ok = mbar_wait(smem_u32(&bar[(nk - 1) & 1]), ((nk - 1) >> 1) & 1);
+  ok = __syncthreads_and(ok);
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (ok) {
+    const int row = m0 + warp * 32 + (tid & 31);
+#pragma unroll
+    for (int c0 = 0; c0 < TC_BN; c0 += 32) {
+      uint32_t v[32];
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+          "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+            "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
+            "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
+            "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+          : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (row < M) {
+        float* crow = C + (size_t)row * ldc;
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+          const int col = n0 + c0 + j;
+          if (col < N) {
+            float r = __uint_as_float(v[j]);
+            if (bias) r += bias[col];
+            if (accum) r += crow[col];
+            crow[col] = r;
+          }
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_BN));
+}
+
 }  // namespace
 
 extern "C" {
 
-// Returns 0, or 10 for arguments the kernel does not take.
+// Returns 0, or 10 for arguments the kernel does not take.  The tcgen05
+// kernel (k_gemm_tc); BPNET_GEMM=mma selects the mma.sync one.
 int bpnet_gemm_tn(const void* A, const void* B, float* C, const float* bias, int M, int N, int K, int lda,
                   int ldb, int ldc, int accum, void* stream) {
+  if (M <= 0 || N <= 0 || K <= 0 || (K % 8) || (lda % 8) || (ldb % 8)) return 10;
+  static const bool use_mma = [] {
+    const char* e = std::getenv("BPNET_GEMM");
+    return e && std::strcmp(e, "mma") == 0;
+  }();
+  static const bool smem_ok =  // 48 KB of dynamic shared memory: two stages
+      cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * TC_STAGE) == cudaSuccess;
+  if (!smem_ok) return 6;
+  if (use_mma) {
+    dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
+    k_gemm_tn<<<grid, 128, 0, (cudaStream_t)stream>>>((const bf16*)A, (const bf16*)B, C, bias, M, N, K, lda,
+                                                       ldb, ldc, accum);
+  } else {
+    dim3 grid((N + TC_BN - 1) / TC_BN, (M + TC_BM - 1) / TC_BM);
+    k_gemm_tc<<<grid, 128, 2 * TC_STAGE, (cudaStream_t)stream>>>((const bf16*)A, (const bf16*)B, C, bias, M, N,
+                                                                 K, lda, ldb, ldc, accum);
+  }
+  return cudaGetLastError() == cudaSuccess ? 0 : 6;
+}
+
+// The mma.sync kernel (the comparison of the tcgen05 one).
+int bpnet_gemm_tn_mma(const void* A, const void* B, float* C, const float* bias, int M, int N, int K, int lda,
+                      int ldb, int ldc, int accum, void* stream) {
   if (M <= 0 || N <= 0 || K <= 0 || (K % 8) || (lda % 8) || (ldb % 8)) return 10;
   dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
   k_gemm_tn<<<grid, 128, 0, (cudaStream_t)stream>>>((const bf16*)A, (const bf16*)B, C, bias, M, N, K, lda,
                                                      ldb, ldc, accum);
   return cudaGetLastError() == cudaSuccess ? 0 : 6;
+}
+
+// 1 if a wait of the tcgen05 GEMM ran out since the last call (and clears
+// it), 0 if not, 6 on a CUDA error.
+int bpnet_gemm_status(void* stream) {
+  int e = 0, z = 0;
+  if (cudaMemcpyFromSymbolAsync(&e, g_tc_err, sizeof(int), 0, cudaMemcpyDeviceToHost, (cudaStream_t)stream) !=
+          cudaSuccess ||
+      cudaMemcpyToSymbolAsync(g_tc_err, &z, sizeof(int), 0, cudaMemcpyHostToDevice, (cudaStream_t)stream) !=
+          cudaSuccess ||
+      cudaStreamSynchronize((cudaStream_t)stream) != cudaSuccess)
+    return 6;
+  return e;
 }
 
 int bpnet_im2col(const void* X, void* col, int B, int H, int W, int C, int Kp, int periodic, void* stream) {

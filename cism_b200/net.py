@@ -42,6 +42,8 @@ def lib():
         vp, i, ll, f = C.c_void_p, C.c_int, C.c_longlong, C.c_float
         sig = {
             "bpnet_gemm_tn": [vp, vp, vp, vp, i, i, i, i, i, i, i, vp],
+            "bpnet_gemm_tn_mma": [vp, vp, vp, vp, i, i, i, i, i, i, i, vp],
+            "bpnet_gemm_status": [vp],
             "bpnet_im2col": [vp, vp, i, i, i, i, i, i, vp],
             "bpnet_col2im": [vp, vp, i, i, i, i, i, i, vp],
             "bpnet_transpose": [vp, vp, i, i, vp],
@@ -97,10 +99,16 @@ def ceil8(x: int) -> int:
     return (x + 7) // 8 * 8
 
 
-def gemm_tn(A, B, out, bias, M, N, K, lda, ldb, ldc, accum=False):
-    """out[M][N] (FP32) = A[M][K] . B[N][K]^T (+ bias) (+ out); BF16 operands."""
-    _ck(lib().bpnet_gemm_tn(_p(A), _p(B), _p(out), _p(bias), M, N, K, lda, ldb, ldc, int(accum), _s()),
-        "bpnet_gemm_tn")
+def gemm_tn(A, B, out, bias, M, N, K, lda, ldb, ldc, accum=False, kernel="tc"):
+    """out[M][N] (FP32) = A[M][K] . B[N][K]^T (+ bias) (+ out); BF16 operands.
+    kernel "tc": the tcgen05 kernel; "mma": the mma.sync one."""
+    fn = lib().bpnet_gemm_tn if kernel == "tc" else lib().bpnet_gemm_tn_mma
+    _ck(fn(_p(A), _p(B), _p(out), _p(bias), M, N, K, lda, ldb, ldc, int(accum), _s()), "bpnet_gemm_tn")
+
+
+def gemm_status() -> int:
+    """1 if a bounded wait of the tcgen05 GEMM ran out since the last call."""
+    return int(lib().bpnet_gemm_status(_s()))
 
 
 def transpose(x, ldo: Optional[int] = None):

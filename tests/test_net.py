@@ -102,8 +102,12 @@ def _device_setup(periodic, B=2, H=16, W=24, channels=(8, 8, 16, 16), n_out=8, s
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("shape", [(64, 64, 64), (100, 40, 72), (7, 130, 8), (256, 96, 1160)])
-def test_gemm_matches_bf16_product(shape):
+@pytest.mark.parametrize("kernel", ["tc", "mma"])
+@pytest.mark.parametrize("shape", [(64, 64, 64), (100, 40, 72), (7, 130, 8), (256, 96, 1160), (300, 24, 48),
+                                   (96, 1440, 64), (130, 64, 1000)])
+def test_gemm_matches_bf16_product(shape, kernel):
+    # the tcgen05 kernel (128 x 64 tiles, K slices of 64 in two stages) and
+    # the mma.sync one against the FP64 product of the same BF16 operands
     torch = pytest.importorskip("torch")
     from cism_b200 import net as netmod
 
@@ -116,11 +120,12 @@ def test_gemm_matches_bf16_product(shape):
     bt = torch.tensor(b, dtype=torch.float32, device="cuda").to(torch.bfloat16).contiguous()
     out = torch.empty((M, N), dtype=torch.float32, device="cuda")
     biast = torch.tensor(bias, device="cuda")
-    netmod.gemm_tn(at, bt, out, biast, M, N, K, K, K, N)
+    netmod.gemm_tn(at, bt, out, biast, M, N, K, K, K, N, kernel=kernel)
     ref = a @ b.T + bias
     assert rel_l2(out.cpu().numpy(), ref) < 1e-5
-    netmod.gemm_tn(at, bt, out, None, M, N, K, K, K, N, accum=True)
+    netmod.gemm_tn(at, bt, out, None, M, N, K, K, K, N, accum=True, kernel=kernel)
     assert rel_l2(out.cpu().numpy(), 2 * (a @ b.T) + bias) < 1e-5
+    assert netmod.gemm_status() == 0  # no bounded wait of the tcgen05 kernel ran out
 
 
 @pytest.mark.gpu
