@@ -545,8 +545,8 @@ def run_ours(args, D):
     achieved = total_bytes / (kp["t_mv_ms"] / 1000.0) / 1e9 if kp["n_mv"] else 0.0
     tr = committed_traffic("mixed" if hp.mixed else "fp64")
     roof = {"bound": "hbm",
-            "kernel": "k_krylov_march<%s> (Krylov matvec, column march, %s)" % (
-                "MV_CG1" if hp.cg else "MV_STD_A",
+            "kernel": "%s (Krylov matvec, thread per node, %s)" % (
+                "k_cg_mv" if hp.cg else "k_std_mv",
                 "FP32 half storage + compensated FP64 diagonal" if hp.mixed else "FP64 half storage"),
             "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4) if peak else None,

@@ -7,7 +7,10 @@ and PCG iteration counts.  This script times a whole converged oracle solve
 of a workload (one thread) and the bench's sample extrapolated with that
 solve's own counts, and prints both as one JSON line per workload.
 
-    python oracle/validate_cpu_baseline.py c0 c1 [--resid 0|4]
+    python oracle/validate_cpu_baseline.py c0 c1 c4 [--resid 0|4]
+
+c4 is the bench's first marine domain (256 x 256 cells, dx = 2 km, the
+column preconditioner), built by bench.make_models as the bench builds it.
 """
 import argparse
 import json
@@ -25,11 +28,11 @@ def main():
     ap.add_argument("--resid", type=int, default=4)
     a = ap.parse_args()
     import bench
-    from cism_b200 import configs
     from oracle import oracle
 
+    picard = {v: k for k, v in bench.PICARD.items()}[a.resid]
     for w in a.workloads:
-        m = configs.workload(w).copy(pcg_maxiters=5000, which_resid=a.resid)
+        m = bench.make_models(bench.parse_args(["--workload", w, "--batch", "1", "--picard", picard]))[0]
         t0 = time.perf_counter()
         _, _, _, _, st = oracle.velo_higher_solve(m)
         full = time.perf_counter() - t0
