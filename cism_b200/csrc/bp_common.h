@@ -112,7 +112,7 @@ struct DevView {
   int sym;                 // matrix stored as its 14 upper stencil offsets (exactly symmetric)
   int minb;                // residual kernels: resident CTAs per SM they are built for (0 or 4)
   int grid_cap;            // CTAs of the tile kernels (0 = one per tile)
-  int minb_k;              // Krylov matvecs (k_std_mv, k_cg_mv): the same, 0, 4 or 6
+  int minb_k;              // Krylov matvecs (k_std_mv, k_cg_mv): the same, 0, 4, 6 or 8
   int grid_k;              // CTAs of the Krylov matvecs (0 = one per tile)
   int dry;                 // autotuner pass: Krylov matvecs run every tile, leave the state alone
   int solve2d;             // 2-D solve (shallow-shelf or L1L2): nz = 1, one 2-D element per cell

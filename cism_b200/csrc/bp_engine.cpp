@@ -515,7 +515,7 @@ void autotune(bp_problem* P) {
   };
   {
     const DryPass dry(v);
-    for (int mb : {0, 4, 6}) {
+    for (int mb : {0, 4, 6, 8}) {
       const int res = krylov_resident_ctas(v, mode, mb);
       if (res <= 0) continue;
       for (int g : {0, res * c->num_sms}) {

@@ -458,13 +458,15 @@ __global__ void __launch_bounds__(kTile) k_rhs(DevView v) {
 
 // ---------------------------------------------------------------------
 // SIA column preconditioner on a tile of whole columns: every thread puts
-// its node's r into shared memory, one thread per (column, component) runs
-// the two Thomas sweeps with the factors of the linear solve (sia_solve),
-// every thread takes back its z.  Called by all threads of the CTA
-// (uniform per tile).
+// its node's r and its node's factors (a, beta, gamma for u and v) into
+// shared memory, one thread per (column, component) runs the two Thomas
+// sweeps from there (sia_sweeps), every thread takes back its z.  The
+// sweeps are a chain of dependent steps; with the factors staged by
+// coalesced loads beforehand, no step of the chain waits on global memory.
+// Called by all threads of the CTA (uniform per tile).
 // ---------------------------------------------------------------------
 struct SiaTile {
-  double s[2 * kTile];
+  double s[2 * kTile], a[2 * kTile], b[2 * kTile], g[2 * kTile];
 };
 
 __device__ __forceinline__ double2 sia_tile(const DevView& v, const TileRange& R, double2 r) {
@@ -474,14 +476,22 @@ __device__ __forceinline__ double2 sia_tile(const DevView& v, const TileRange& R
   // shared memory holds the tile column by column: j = c * nz + k
   const int k = tile_k(v, i), j = (i & (v.W - 1)) * nz + k;
   if (mine) {
+    const size_t n = (size_t)R.n0 + i, np = (size_t)v.npad;
+    const double2 fa = v.sia_f[n], fb = v.sia_f[np + n], fg = v.sia_f[2 * np + n];
     T.s[2 * j] = r.x;
     T.s[2 * j + 1] = r.y;
+    T.a[2 * j] = fa.x;
+    T.a[2 * j + 1] = fa.y;
+    T.b[2 * j] = fb.x;
+    T.b[2 * j + 1] = fb.y;
+    T.g[2 * j] = fg.x;
+    T.g[2 * j + 1] = fg.y;
   }
   __syncthreads();
   if (i < 2 * R.ncols) {
-    const int c = i >> 1, h = i & 1, lsh = v.lsh;
-    const size_t n0 = (size_t)R.n0 + c;
-    sia_solve(v, nz, h, [&](int kk) { return n0 + ((size_t)kk << lsh); }, &T.s[2 * c * nz + h], 2);
+    const int c = i >> 1, h = i & 1, o = 2 * c * nz + h;
+    sia_sweeps(
+        nz, [&](int kk) { return SiaFac{T.a[o + 2 * kk], T.b[o + 2 * kk], T.g[o + 2 * kk]}; }, &T.s[o], 2);
   }
   __syncthreads();
   const double2 z = mine ? make_double2(T.s[2 * j], T.s[2 * j + 1]) : make_double2(0.0, 0.0);
@@ -609,10 +619,23 @@ __global__ void __launch_bounds__(kTile, MINB) k_resid(DevView v) {
 // Krylov matvec of the mixed path: FP32 matrix unless the instance's
 // refinement stalled (krylov_fp64), FP64 then.  In timing runs the nodes
 // through each precision are counted, to turn the measured time into bytes.
+// The FP64 Krylov matvec of an instance whose FP32 refinement stalled,
+// out of line: inlined, its registers would count against every launch of
+// the FP32 kernel, which is sized to fit 32 registers per thread.
+struct MvGeom {
+  int nz, ncols, npad, lsh;
+  const int* col_nbn;
+};
+__device__ __noinline__ double2 mv_row_sym64_call(MvGeom g, const double2* A, int col, int k, size_t n,
+                                                  const double2* s) {
+  return matvec_row_sym(g, A, col, k, n, SrcX{s});
+}
+
 template <int STORE>
 __device__ __forceinline__ double2 krylov_row(const DevView& v, const InstState& S, int col, int k,
                                               size_t n, const double2* s) {
-  if (STORE == ST_SYM32 && S.krylov_fp64) return mv_row<ST_SYM>(v, col, k, n, s);
+  if (STORE == ST_SYM32 && S.krylov_fp64)
+    return mv_row_sym64_call(MvGeom{v.nz, v.ncols, v.npad, v.lsh, v.col_nbn}, v.A, col, k, n, s);
   return mv_row<STORE>(v, col, k, n, s);
 }
 
@@ -1148,6 +1171,7 @@ static TileKernel krylov_kernel(int mode) {
 }
 template <int STORE>
 static TileKernel krylov_kernel_st(int mode, int minb) {
+  if (minb == 8) return krylov_kernel<STORE, 8>(mode);
   if (minb == 6) return krylov_kernel<STORE, 6>(mode);
   if (minb == 4) return krylov_kernel<STORE, 4>(mode);
   return krylov_kernel<STORE, 0>(mode);

@@ -84,39 +84,43 @@ def make_marine_set(ctx, sizes, count: int, seed: int, batch: int, log=None, dea
     """`count` members of the marine family, sizes drawn from `sizes`,
     solved (mixed precision, column preconditioner, Chronopoulos-Gear, the
     relative-residual Picard criterion) in problems of `batch` same-size
-    domains.  Returns per size: (models, padded features, padded targets,
+    domains, the sizes taken in turn so that a deadline cuts every size
+    alike.  Returns per size: (models, padded features, padded targets,
     padded masks of the active vertices)."""
     rng = np.random.default_rng(seed)
     plan = [int(rng.choice(sizes)) for _ in range(count)]
+    per_size = {n: [configs.random_marine(rng, n=n).copy(**MARINE_SOLVE) for _ in range(plan.count(n))]
+                for n in sorted(set(plan))}
+    chunks = {n: [ms[i:i + batch] for i in range(0, len(ms), batch)] for n, ms in per_size.items()}
+    order = []  # round robin over the sizes
+    for r in range(max(len(c) for c in chunks.values())):
+        order += [(n, c[r]) for n, c in chunks.items() if r < len(c)]
     out = {}
     t0 = time.time()
-    for n in sorted(set(plan)):
-        k = plan.count(n)
-        models = [configs.random_marine(rng, n=n).copy(**MARINE_SOLVE) for _ in range(k)]
-        for i in range(0, k, batch):
-            if deadline is not None and time.time() > deadline:
-                break
-            grp = models[i:i + batch]
-            us, vs, sts, _, arrs = solve_models(ctx, grp, precision=solver.MIXED, batch=batch, keep_arrays=True)
-            M, F, T, K = out.setdefault(n, ([], [], [], []))
-            for m, u, v, st, a in zip(grp, us, vs, sts, arrs):
-                if st["status"] != 0:
-                    continue
-                M.append(m)
-                F.append(net.pad_grid(net.input_features(m, a)).astype(np.float32))
-                T.append(net.pad_grid(net.velocity_targets(m, u, v)).astype(np.float32))
-                js, is_ = m.owned_vertex_slices()
-                K.append(net.pad_grid((np.asarray(a["active_vertex"])[js, is_] != 0).astype(np.float32)[..., None])[..., 0])
-            if log:
-                log(f"  {n}x{n}: {len(M)} solved ({time.time() - t0:.0f} s)")
+    for n, grp in order:
+        if deadline is not None and time.time() > deadline:
+            break
+        us, vs, sts, _, arrs = solve_models(ctx, grp, precision=solver.MIXED, batch=batch, keep_arrays=True)
+        M, F, T, K = out.setdefault(n, ([], [], [], []))
+        for m, u, v, st, a in zip(grp, us, vs, sts, arrs):
+            if st["status"] != 0:
+                continue
+            M.append(m)
+            F.append(net.pad_grid(net.input_features(m, a)).astype(np.float32))
+            T.append(net.pad_grid(net.velocity_targets(m, u, v)).astype(np.float32))
+            js, is_ = m.owned_vertex_slices()
+            K.append(net.pad_grid((np.asarray(a["active_vertex"])[js, is_] != 0).astype(np.float32)[..., None])[..., 0])
+        if log:
+            log(f"  {n}x{n}: {len(M)} solved ({time.time() - t0:.0f} s)")
     return {n: (M, np.stack(F), np.stack(T), np.stack(K)) for n, (M, F, T, K) in out.items() if M}
 
 
 def train(model: net.UNet, groups, epochs: int, lr: float, batch: int, seed: int, log=None, periodic: int = 1,
           deadline=None):
     """groups: list of (features [N,H,W,5], targets [N,H,W,C][, masks
-    [N,H,W]]) of one size each, already normalised.  Adam with cosine
-    decay of the step size; stops at the deadline (time.time()) if given."""
+    [N,H,W]]) of one size each, already normalised.  Adam; the step size
+    ramps up linearly over the first 3% of the schedule, then decays as a
+    cosine; stops at the deadline (time.time()) if given."""
     import torch
 
     rng = np.random.default_rng(seed)
@@ -153,7 +157,9 @@ def train(model: net.UNet, groups, epochs: int, lr: float, batch: int, seed: int
             frac = t / total
             if deadline is not None:  # the schedule also follows the time left
                 frac = max(frac, (time.time() - t_start) / max(deadline - t_start, 1.0))
-            step = lr * 0.5 * (1.0 + math.cos(math.pi * min(frac, 1.0)))
+            warm = 0.03
+            step = (lr * frac / warm if frac < warm else
+                    lr * 0.5 * (1.0 + math.cos(math.pi * min((frac - warm) / (1.0 - warm), 1.0))))
             model.adam(step, t)
             el += loss
         hist.append(el / len(order))
@@ -292,7 +298,7 @@ def main(argv=None):
     ap.add_argument("--train160", type=int, default=128)
     ap.add_argument("--heldout", type=int, default=8)
     ap.add_argument("--epochs", type=int, default=200)
-    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--lr", type=float, default=6e-4)
     ap.add_argument("--batch", type=int, default=8)
     ap.add_argument("--seed", type=int, default=11)
     ap.add_argument("--report", default=None)
