@@ -350,6 +350,75 @@ BP_HD void row_assemble(const DevView& v, const RefTables& T, int col, int k,
   }
 }
 
+// Element-centric form of pass 2, in two steps with row_element's
+// arithmetic regrouped.  element_row_blocks: row nr (a corner, 0..7) of an
+// element's four 8 x 8 blocks, K[B * 8 + nc], each entry accumulated over
+// the quadrature points in order with row_element's operations, so that it
+// is bitwise the value row_element adds; the physical basis gradients of a
+// point are formed once for all four blocks.  row_gather: the row of node
+// (col,k) in block B, summed from the stored element rows in
+// row_assemble's element order, so the assembled row is bitwise
+// row_assemble's.  Ke holds [element][B][nr][nc].
+BP_HD void element_row_blocks(const RefTables& T, const double* qpe, int nr, double* K) {
+#pragma unroll
+  for (int i = 0; i < 32; ++i) K[i] = 0.0;
+  for (int p = 0; p < 8; ++p) {
+    const double* q = qpe + p * 10;
+    const double f = BP_LD_RO(q + 0);
+    const double i00 = BP_LD_RO(q + 1), i01 = BP_LD_RO(q + 2), i02 = BP_LD_RO(q + 3);
+    const double i10 = BP_LD_RO(q + 4), i11 = BP_LD_RO(q + 5), i12 = BP_LD_RO(q + 6);
+    const double i20 = BP_LD_RO(q + 7), i21 = BP_LD_RO(q + 8), i22 = BP_LD_RO(q + 9);
+    const double ar = T.dxr[p][nr], br = T.dyr[p][nr], cr = T.dzr[p][nr];
+    const double axr = BP_FMA(i02, cr, BP_FMA(i01, br, i00 * ar));
+    const double ayr = BP_FMA(i12, cr, BP_FMA(i11, br, i10 * ar));
+    const double azr = BP_FMA(i22, cr, BP_FMA(i21, br, i20 * ar));
+#pragma unroll
+    for (int nc = 0; nc < 8; ++nc) {
+      const double a = T.dxr[p][nc], b = T.dyr[p][nc], c = T.dzr[p][nc];
+      const double ax = BP_FMA(i02, c, BP_FMA(i01, b, i00 * a));
+      const double ay = BP_FMA(i12, c, BP_FMA(i11, b, i10 * a));
+      const double az = BP_FMA(i22, c, BP_FMA(i21, b, i20 * a));
+      K[nc] = BP_FMA(f, block_term<0>(axr, ayr, azr, ax, ay, az), K[nc]);
+      K[8 + nc] = BP_FMA(f, block_term<1>(axr, ayr, azr, ax, ay, az), K[8 + nc]);
+      K[16 + nc] = BP_FMA(f, block_term<2>(axr, ayr, azr, ax, ay, az), K[16 + nc]);
+      K[24 + nc] = BP_FMA(f, block_term<3>(axr, ayr, azr, ax, ay, az), K[24 + nc]);
+    }
+  }
+}
+
+template <int NR, int B>
+BP_HD void gather_element(const double* Ke, int e, double* acc) {
+  const double* r = Ke + ((size_t)e * 4 + B) * 64 + NR * 8;
+#pragma unroll
+  for (int nc = 0; nc < 8; ++nc) acc[elem_m(NR, nc)] += BP_LD_RO(r + nc);
+}
+
+template <int B>
+BP_HD void row_gather(const DevView& v, const double* Ke, int col, int k, double* acc) {
+  const int nz = v.nz, nc = v.ncols;
+#pragma unroll
+  for (int m = 0; m < 27; ++m) acc[m] = 0.0;
+  const int c0 = v.col_cells[0 * nc + col], c1 = v.col_cells[1 * nc + col];
+  const int c2 = v.col_cells[2 * nc + col], c3 = v.col_cells[3 * nc + col];
+  const bool lo = k >= 1, up = k <= nz - 2;
+  if (c0 >= 0) {
+    if (lo) gather_element<2, B>(Ke, elem_of(c0, k - 1, nz), acc);
+    if (up) gather_element<6, B>(Ke, elem_of(c0, k, nz), acc);
+  }
+  if (c1 >= 0) {
+    if (lo) gather_element<3, B>(Ke, elem_of(c1, k - 1, nz), acc);
+    if (up) gather_element<7, B>(Ke, elem_of(c1, k, nz), acc);
+  }
+  if (c2 >= 0) {
+    if (lo) gather_element<1, B>(Ke, elem_of(c2, k - 1, nz), acc);
+    if (up) gather_element<5, B>(Ke, elem_of(c2, k, nz), acc);
+  }
+  if (c3 >= 0) {
+    if (lo) gather_element<0, B>(Ke, elem_of(c3, k - 1, nz), acc);
+    if (up) gather_element<4, B>(Ke, elem_of(c3, k, nz), acc);
+  }
+}
+
 // ---------------------------------------------------------------------
 // Shallow-shelf (SSA) assembly: assemble_stiffness_matrix_2d, SSA branch
 // (:5208-5595).  One 2-D element per active cell (corners SW, SE, NE, NW =

@@ -167,6 +167,7 @@ struct DevView {
   const int* tile_col0;    // [ntiles] first column of the block
   // assembly / matrix
   double* qp;              // [nelem*8*10]: f, Jinv(3x3) per quadrature point
+  double* Ke;              // [nelem][4][8][8] element blocks (3-D element-centric assembly) or null
   double* efvs;            // [nelem]; L1L2 [ncells][nl]
   // FP64 matrix, (u,v) pairs: h = 0 the u-row (Auu, Auv), h = 1 the v-row
   // (Avu, Avv).  Full storage [2][27][npad]; symmetric storage [2][14][npad]

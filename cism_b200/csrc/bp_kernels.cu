@@ -354,10 +354,29 @@ __global__ void __launch_bounds__(256) k_diva_velocity(DevView v) {
 // ---------------------------------------------------------------------
 // Assembly pass 2 + basal BC + Dirichlet BC: thread = (block B, node).
 // ---------------------------------------------------------------------
-template <int B, bool D2>
+enum { ASM_ROWS = 0, ASM_GATHER = 1, ASM_2D = 2 };
+
+// Element-centric pass 2a: thread = (element, corner nr); the corner's rows
+// of the element's four blocks (element_row_blocks) into Ke, the eight
+// threads of an element writing 64 consecutive doubles per block.
+__global__ void __launch_bounds__(256, 2) k_asm_elem(DevView v) {
+  const long gtid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int e = (int)(gtid >> 3), nr = (int)(gtid & 7);
+  if (e >= v.nelem) return;
+  if (!v.st[v.cell_inst[e / (v.nz - 1)]].picard_active) return;
+  double K[32];
+  element_row_blocks(c_T, v.qp + (size_t)e * 80, nr, K);
+  double2* out = reinterpret_cast<double2*>(v.Ke + (size_t)e * 256 + nr * 8);
+#pragma unroll
+  for (int b = 0; b < 4; ++b)
+#pragma unroll
+    for (int i = 0; i < 4; ++i) out[b * 32 + i] = make_double2(K[b * 8 + 2 * i], K[b * 8 + 2 * i + 1]);
+}
+template <int B, int MODE>
 __device__ __forceinline__ bool asm_row(const DevView& v, int n, int col, int k) {
   double acc[27];
-  if (D2) row_assemble2<B>(v, c_T, col, acc);
+  if (MODE == ASM_2D) row_assemble2<B>(v, c_T, col, acc);
+  else if (MODE == ASM_GATHER) row_gather<B>(v, v.Ke, col, k, acc);
   else row_assemble<B>(v, c_T, col, k, acc);
   row_basal<B>(v, c_T, col, k, acc);
   const double adj = row_dirichlet<B>(v, col, k, acc);
@@ -378,8 +397,10 @@ __device__ __forceinline__ bool asm_row(const DevView& v, int n, int col, int k)
   return nz;
 }
 
-// D2: the rows of the 2-D solves (shallow-shelf, L1L2; nz = 1).
-template <bool D2>
+// MODE: ASM_ROWS (3-D, each row integrates its incident elements),
+// ASM_GATHER (3-D, each row sums the element rows k_asm_elem stored) or
+// ASM_2D (the rows of the 2-D solves: shallow-shelf, L1L2; nz = 1).
+template <int MODE>
 __global__ void __launch_bounds__(kTile) k_asm_rows(DevView v) {
   const int B = blockIdx.y;
   for (int t = blockIdx.x; t < v.ntiles; t += gridDim.x) {
@@ -390,10 +411,10 @@ __global__ void __launch_bounds__(kTile) k_asm_rows(DevView v) {
     if (tile_mine(v, R, threadIdx.x)) {
       const int col = tile_col(v, R, threadIdx.x), k = tile_k(v, threadIdx.x);
       switch (B) {
-        case 0: nzl = asm_row<0, D2>(v, n, col, k); break;
-        case 1: nzl = asm_row<1, D2>(v, n, col, k); break;
-        case 2: nzl = asm_row<2, D2>(v, n, col, k); break;
-        default: nzl = asm_row<3, D2>(v, n, col, k); break;
+        case 0: nzl = asm_row<0, MODE>(v, n, col, k); break;
+        case 1: nzl = asm_row<1, MODE>(v, n, col, k); break;
+        case 2: nzl = asm_row<2, MODE>(v, n, col, k); break;
+        default: nzl = asm_row<3, MODE>(v, n, col, k); break;
       }
     }
     if (__syncthreads_or(nzl) && threadIdx.x == 0) atomicOr(&v.st[R.inst].nonzero, 1);
@@ -1092,8 +1113,14 @@ void launch_asm_qp(const DevView& v, cudaStream_t s) {
 }
 void launch_asm_rows(const DevView& v, cudaStream_t s) {
   dim3 g(tile_grid(v), 4);
-  if (v.solve2d) k_asm_rows<true><<<g, v.tile_threads, 0, s>>>(v);
-  else k_asm_rows<false><<<g, v.tile_threads, 0, s>>>(v);
+  if (v.solve2d) {
+    k_asm_rows<ASM_2D><<<g, v.tile_threads, 0, s>>>(v);
+  } else if (v.Ke) {
+    if (v.nelem > 0) k_asm_elem<<<(unsigned)(((long)v.nelem * 8 + 255) / 256), 256, 0, s>>>(v);
+    k_asm_rows<ASM_GATHER><<<g, v.tile_threads, 0, s>>>(v);
+  } else {
+    k_asm_rows<ASM_ROWS><<<g, v.tile_threads, 0, s>>>(v);
+  }
 }
 void launch_rhs(const DevView& v, cudaStream_t s) { k_rhs<<<tile_grid(v), v.tile_threads, 0, s>>>(v); }
 void launch_diva_beta(const DevView& v, cudaStream_t s) {

@@ -79,13 +79,16 @@ void each_node(const HostPlan& p, F f) {
     for (int k = 0; k < p.nz; ++k) f(node_of(p, c, k), c, k);
 }
 
+// Ke: the element blocks of the element-centric form (row_gather), or
+// null for the row-integrating form (row_assemble).
 template <int B>
-void rows(Emu& E, const RefTables& T) {
+void rows(Emu& E, const RefTables& T, const double* Ke) {
   const DevView& v = E.v;
   double* Ad = reinterpret_cast<double*>(E.A.data());
   each_node(E.p, [&](size_t n, int col, int k) {
     double acc[27];
-    row_assemble<B>(v, T, col, k, acc);
+    if (Ke) row_gather<B>(v, Ke, col, k, acc);
+    else row_assemble<B>(v, T, col, k, acc);
     row_basal<B>(v, T, col, k, acc);
     const double adj = row_dirichlet<B>(v, col, k, acc);
     for (int m = 0; m < 27; ++m)
@@ -95,9 +98,11 @@ void rows(Emu& E, const RefTables& T) {
 }
 }  // namespace
 
-extern "C" int emu_assemble(const bp_inputs* in, const double* uvel, const double* vvel,
-                            double* Auu, double* Auv, double* Avu, double* Avv, double* bu,
-                            double* bv, double* efvs) {
+// gather = 1: pass 2 in the element-centric form (element_row_blocks for
+// every element and corner, then row_gather), as k_asm_elem + k_asm_rows.
+extern "C" int emu_assemble_form(const bp_inputs* in, const double* uvel, const double* vvel,
+                                 double* Auu, double* Auv, double* Avu, double* Avv, double* bu,
+                                 double* bv, double* efvs, int gather) {
   Emu E;
   std::string err;
   if (!build_plan(in, 1, &E.p, &err)) return 10;
@@ -115,7 +120,19 @@ extern "C" int emu_assemble(const bp_inputs* in, const double* uvel, const doubl
     }
     E.efvs[e] = s / 8.0;
   }
-  rows<0>(E, T); rows<1>(E, T); rows<2>(E, T); rows<3>(E, T);
+  std::vector<double> Ke;
+  if (gather) {
+    Ke.assign((size_t)E.p.nelem * 256, 0.0);
+    for (int e = 0; e < E.p.nelem; ++e)
+      for (int nr = 0; nr < 8; ++nr) {
+        double K[32];
+        element_row_blocks(T, &E.qp[(size_t)e * 80], nr, K);
+        for (int b = 0; b < 4; ++b)
+          for (int nc = 0; nc < 8; ++nc) Ke[(size_t)e * 256 + b * 64 + nr * 8 + nc] = K[b * 8 + nc];
+      }
+  }
+  const double* ke = gather ? Ke.data() : nullptr;
+  rows<0>(E, T, ke); rows<1>(E, T, ke); rows<2>(E, T, ke); rows<3>(E, T, ke);
   const size_t np = E.p.npad;
   for (int n = 0; n < E.p.npad; ++n) {  // the hole slots are zero
     const uint8_t dm = E.p.dmask[n];
@@ -132,6 +149,12 @@ extern "C" int emu_assemble(const bp_inputs* in, const double* uvel, const doubl
   scatter_vector(E.p, 0, E.b.data(), bu, bv);
   scatter_efvs(E.p, 0, E.efvs.data(), efvs);
   return 0;
+}
+
+extern "C" int emu_assemble(const bp_inputs* in, const double* uvel, const double* vvel,
+                            double* Auu, double* Auv, double* Avu, double* Avv, double* bu,
+                            double* bv, double* efvs) {
+  return emu_assemble_form(in, uvel, vvel, Auu, Auv, Avu, Avv, bu, bv, efvs, 0);
 }
 
 // Symmetric storage (14 upper offsets; fp32 = 1 for the packed FP32 copy).

@@ -95,6 +95,30 @@ def test_kernel_bodies_match_oracle(m):
     assert rel_l2([eyu, eyv], [yu, yv]) < 1e-14
 
 
+@pytest.mark.parametrize("m", MODELS, ids=lambda m: m.name)
+def test_element_centric_assembly_is_bitwise_the_row_form(m):
+    """Pass 2 of the assembly in its element-centric form (each element's
+    four blocks formed once, k_asm_elem, then summed per row in the
+    reference's element order) gives the matrix, the right-hand side and
+    the viscosity of the row-integrating form bit for bit."""
+    emu = C.CDLL(EMU)
+    prep, _, _ = solver.prepare(m)
+    su, u, v, A, bu, bv, efvs = oracle_system(m, seed=4, scale=10.0)
+    outs = []
+    for gather in (0, 1):
+        E = [np.zeros((m.ny - 1, m.nx - 1, m.nz, 27)) for _ in range(4)]
+        ebu, ebv = np.zeros(m.vshape3), np.zeros(m.vshape3)
+        eef = np.zeros((m.ny, m.nx, m.nz - 1))
+        rc = emu.emu_assemble_form(C.byref(prep.inputs), _p(np.ascontiguousarray(u)),
+                                   _p(np.ascontiguousarray(v)), *[_p(a) for a in E], _p(ebu), _p(ebv),
+                                   _p(eef), C.c_int(gather))
+        assert rc == 0
+        outs.append(E + [ebu, ebv, eef])
+    assert np.count_nonzero(outs[0][0]) > 0
+    for a, b in zip(*outs):
+        assert np.array_equal(a, b)
+
+
 @pytest.mark.parametrize("m", MODELS[:4], ids=lambda m: m.name)
 def test_symmetric_storage_matvec_bodies(m):
     """The device's half-storage matvec (lower stencil half read from the
