@@ -574,7 +574,7 @@ def run_ours(args, D):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": ("f32+f64" if hp.mixed else "f64") + ("+bf16" if hp.start == "learned" else ""),
         "data": "synthetic (seeded geometry generator, no dataset)",
-        "config": config_dict(args, models, cols, nodes, D.world) | {"path": head},
+        "config": config_dict(args, models, cols, nodes, D.world), "path": head,
         "accepted": bool(ok),
         "e2e": e2e, "roofline": roof, "assembly": asm,
         "gpu_launches": (kp["launches"] + H["guess_launches_per_step"]) * args.steps,
@@ -586,14 +586,21 @@ def run_ours(args, D):
         out["speedup_vs_plain_fp64_same_preconditioner"] = round(
             out_paths[head]["value"] / out_paths["fp64_colpc"]["value"], 3)
     if D.rank == 0 and D.world == 1 and not args.no_cpu_baseline and "plain_fp64" in res:
-        st0 = res["plain_fp64"]["stats"][0]
-        cs = cpu_sample(models[0], (st0["picard_iters"], st0["pcg_iters_total"]))
+        # the oracle's own counts for domain 0 where recorded, else the GPU FP64 path's
+        rec = load_counts(f"{args.workload}/{args.picard}")
+        if rec:
+            c0 = rec["per_domain"][0]
+            counts, src = (c0["picard_iters"], c0["pcg_iters_total"]), "the oracle's converged-solve counts"
+        else:
+            st0 = res["plain_fp64"]["stats"][0]
+            counts, src = (st0["picard_iters"], st0["pcg_iters_total"]), "the GPU FP64 path's counts"
+        cs = cpu_sample(models[0], counts)
         out["cpu_baseline"] = {
             "value": round(1.0 / cs["t_solve_est"], 8), "unit": UNIT, "cores": 1, "kind": "port",
             "sample": (f"oracle (C restatement of the reference, 1 thread): setup, one assembly and 20 / 60 PCG "
-                       f"iterations of domain 0, extrapolated to its plain-FP64 counts ({st0['picard_iters']} "
-                       f"Picard, {st0['pcg_iters_total']} PCG); profiles/cpu_oracle_validation.md checks the "
-                       f"extrapolation against fully converged oracle solves"),
+                       f"iterations of domain 0, extrapolated to {src} ({counts[0]} Picard, {counts[1]} PCG); "
+                       f"profiles/cpu_oracle_validation.md checks the extrapolation against fully converged "
+                       f"oracle solves"),
             "sample_seconds": round(cs["sample_seconds"], 1)}
     for r in res.values():
         for pb in r["probs"]:
@@ -633,7 +640,7 @@ def run_reference(args, D):
             "value_basis": "extrapolated: value = domains / sum of the extrapolated solve times; ms_per_step is "
                            "the sample's own wall time",
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": config_dict(args, models, cols, nodes, D.world) | {"path": "plain_fp64"},
+            "config": config_dict(args, models, cols, nodes, D.world), "path": "plain_fp64 (oracle, CPU)",
             "impl": "reference",
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
