@@ -97,7 +97,7 @@ GuessNet* guess_net_load(const char* path, std::string* err) {
   int hdr[4];
   GuessNet* N = new GuessNet();
   bool ok = rd(magic, 8) && std::memcmp(magic, "BPUNET1", 8) == 0 && rd(hdr, sizeof(hdr)) && hdr[0] == 1 &&
-            hdr[1] == 5 && hdr[2] > 0 && hdr[2] % 8 == 0 && hdr[3] >= 1 && hdr[3] <= 8;
+            (hdr[1] == 5 || hdr[1] == 6) && hdr[2] > 0 && hdr[2] % 8 == 0 && hdr[3] >= 1 && hdr[3] <= 8;
   int nconv = 0;
   if (ok) {
     N->nin = hdr[1];
@@ -125,6 +125,7 @@ GuessNet* guess_net_load(const char* path, std::string* err) {
     N->convs.push_back(c);
   }
   std::fclose(f);
+  ok = ok && !N->convs.empty() && N->convs[0].cin == N->nin;
   if (!ok) {
     *err = std::string("malformed U-Net weights file ") + path;
     delete N;
@@ -138,7 +139,7 @@ void guess_net_free(GuessNet* N) { delete N; }
 namespace {
 
 // Features of one instance's active columns, normalised and rounded to
-// BF16, into grid b of x [B][H][W][5] (the grid is zeroed beforehand).
+// BF16, into grid b of x [B][H][W][nin] (the grid is zeroed beforehand).
 // The arithmetic follows net.input_features / net.normalized_input.
 __global__ void k_guess_features(DevView v, int col_begin, int col_end, int ilo, int jlo, int H, int W, int b,
                                  double area, GuessNorm nrm, bf16* x) {
@@ -151,11 +152,22 @@ __global__ void k_guess_features(DevView v, int col_begin, int col_end, int ilo,
     sv = sv + l.y;
   }
   const double beta = v.col_beta[col];
-  const double f[5] = {v.col_h[col] / 1000.0, su * area, sv * area, log10(fmax(beta, 1.0)), beta > 0.0 ? 1.0 : -1.0};
+  double f[6] = {v.col_h[col] / 1000.0, su * area, sv * area, log10(fmax(beta, 1.0)), beta > 0.0 ? 1.0 : -1.0, 0.0};
+  if (nrm.nin > 5) {  // mean flwafact over the layers of the column's active cells (SW, SE, NW, NE of the vertex)
+    double sf = 0.0, cnt = 0.0;
+    for (int q = 0; q < 4; ++q) {
+      const int c = v.col_cells[q * v.ncols + col];
+      if (c < 0) continue;
+      for (int k = 0; k < v.nz - 1; ++k) {
+        sf = sf + v.flwafact[(size_t)c * (v.nz - 1) + k];
+        cnt = cnt + 1.0;
+      }
+    }
+    f[5] = cnt > 0.0 ? log10(sf / cnt) : 0.0;
+  }
   const int gi = v.col_ij[col] - ilo, gj = v.col_ij[v.ncols + col] - jlo;
-  bf16* dst = x + (((size_t)b * H + gj) * W + gi) * 5;
-#pragma unroll
-  for (int c = 0; c < 5; ++c)
+  bf16* dst = x + (((size_t)b * H + gj) * W + gi) * nrm.nin;
+  for (int c = 0; c < nrm.nin; ++c)
     dst[c] = __float2bfloat16_rn(__double2float_rn((f[c] - (double)nrm.shift[c]) * (double)nrm.scale[c]));
 }
 
@@ -255,7 +267,8 @@ int guess_net_run(GuessNet* N, const HostPlan& p, const DevView& v, const std::v
   int nlaunch = 0;
   if (p.solve2d || p.nz * 2 > N->nout) return BP_ERR_ARGS;
   GuessNorm nrm;
-  for (int c = 0; c < 5; ++c) {
+  nrm.nin = N->nin;
+  for (int c = 0; c < N->nin; ++c) {
     nrm.shift[c] = N->shift[c];
     nrm.scale[c] = N->scale[c];
   }
@@ -268,9 +281,9 @@ int guess_net_run(GuessNet* N, const HostPlan& p, const DevView& v, const std::v
   for (auto& g : groups) {
     const int H = std::get<0>(g.first), W = std::get<1>(g.first), per = std::get<2>(g.first);
     const int B = (int)g.second.size();
-    bf16* x = (bf16*)N->get("input", sizeof(bf16) * (size_t)B * H * W * 5);
+    bf16* x = (bf16*)N->get("input", sizeof(bf16) * (size_t)B * H * W * N->nin);
     if (!x) return BP_ERR_CUDA;
-    if (cudaMemsetAsync(x, 0, sizeof(bf16) * (size_t)B * H * W * 5, s) != cudaSuccess) return BP_ERR_CUDA;
+    if (cudaMemsetAsync(x, 0, sizeof(bf16) * (size_t)B * H * W * N->nin, s) != cudaSuccess) return BP_ERR_CUDA;
     for (int bi = 0; bi < B; ++bi) {
       const int b = g.second[bi];
       const InstParams& ip = p.inst[b];

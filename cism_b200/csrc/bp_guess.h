@@ -11,9 +11,11 @@ namespace bp {
 
 struct GuessNet;
 
-// Input normalisation of the network (per feature).
+// Input normalisation of the network (per feature); nin is 5 or 6 (the
+// sixth feature: log10 of the mean flow-law factor around the vertex).
 struct GuessNorm {
-  float shift[5], scale[5];
+  float shift[6], scale[6];
+  int nin;
 };
 
 // Loads the weights file that net.UNet.save_bin writes and uploads them to

@@ -29,7 +29,7 @@ from . import configs
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libbpnet.so")
 CHANNELS = (32, 64, 96, 128)
-N_IN = 5
+N_IN = 6  # input channels of the marine-family network (input_features); 5-input networks load too
 _lib = None
 
 
@@ -214,13 +214,14 @@ class Conv:
 class UNet:
     """The U-Net; ``n_out`` output channels (a multiple of 8)."""
 
-    def __init__(self, n_out: int = 24, seed: int = 0, channels: Sequence[int] = CHANNELS):
+    def __init__(self, n_out: int = 24, seed: int = 0, channels: Sequence[int] = CHANNELS, n_in: int = N_IN):
         rng = np.random.default_rng(seed)
         c = list(channels)
         self.channels = c
         self.n_out = n_out
+        self.n_in = n_in
         self.enc = []
-        cin = N_IN
+        cin = n_in
         for ch in c:
             self.enc.append([Conv(cin, ch, True, True, rng), Conv(ch, ch, True, True, rng)])
             cin = ch
@@ -228,8 +229,8 @@ class UNet:
         for lv in range(len(c) - 2, -1, -1):
             self.dec.append([Conv(c[lv + 1] + c[lv], c[lv], True, True, rng), Conv(c[lv], c[lv], True, True, rng)])
         self.head = Conv(c[0], n_out, False, False, rng)
-        self.in_shift = np.zeros(N_IN, np.float32)
-        self.in_scale = np.ones(N_IN, np.float32)
+        self.in_shift = np.zeros(n_in, np.float32)
+        self.in_scale = np.ones(n_in, np.float32)
         self.out_scale = 1.0
 
     def convs(self) -> List[Conv]:
@@ -239,13 +240,13 @@ class UNet:
         return sum(cv.params() for cv in self.convs())
 
     def forward(self, x, periodic: int, train: bool = False):
-        """x: BF16 [B][H][W][5] (H, W multiples of 8); FP32 [B][H][W][n_out]."""
+        """x: BF16 [B][H][W][n_in] (H, W multiples of 8); FP32 [B][H][W][n_out]."""
         torch = _torch()
         B, H, W, _ = x.shape
         assert H % 8 == 0 and W % 8 == 0
         nl = len(self.channels)
         shapes = [(B, H >> lv, W >> lv) for lv in range(nl)]
-        cur = x.reshape(-1, N_IN)
+        cur = x.reshape(-1, self.n_in)
         skips = []
         for lv in range(nl):
             if lv > 0:
@@ -328,7 +329,7 @@ class UNet:
         decoder levels, head) int32 cin, cout, k3, act, K and float32 w
         [cout][K], b [cout].  Little-endian."""
         convs = self.convs()
-        hdr = [1, N_IN, self.n_out, len(self.channels)] + list(self.channels) + [len(convs)]
+        hdr = [1, self.n_in, self.n_out, len(self.channels)] + list(self.channels) + [len(convs)]
         with open(path, "wb") as f:
             f.write(b"BPUNET1\0")
             f.write(np.asarray(hdr, dtype="<i4").tobytes())
@@ -344,7 +345,8 @@ class UNet:
     def load(cls, path: str) -> "UNet":
         torch = _torch()
         d = np.load(path)
-        net = cls(n_out=int(d["n_out"]), channels=tuple(int(c) for c in d["channels"]))
+        n_in = int(d["in_shift"].shape[0])
+        net = cls(n_out=int(d["n_out"]), channels=tuple(int(c) for c in d["channels"]), n_in=n_in)
         for i, cv in enumerate(net.convs()):
             cv.w.copy_(torch.tensor(d[f"w{i}"]))
             cv.b.copy_(torch.tensor(d[f"b{i}"]))
@@ -419,17 +421,20 @@ def guess_from_output(m: configs.BPModel, out: np.ndarray):
 VOL0 = 1.0e9  # the solver's volume scale (glissade_velo_higher.F90:1111)
 
 
-def input_features(m: configs.BPModel, arrays: dict) -> np.ndarray:
-    """[ny_owned][nx_owned][5] at the owned vertices from bp_setup's arrays:
-    thickness stagthck (km), the driving stress -- the gravity load summed
-    over the column, per horizontal area (1e5 Pa) -- in x and y, log10 of
-    beta_internal (clamped to >= 1), and the ice mask (+1 where beta_internal
-    > 0, i.e. grounded ice, -1 floating ice, 0 no active vertex).  Zero at
+def input_features(m: configs.BPModel, arrays: dict, n_in: int = N_IN) -> np.ndarray:
+    """[ny_owned][nx_owned][n_in] at the owned vertices from bp_setup's
+    arrays: thickness stagthck (km), the driving stress -- the gravity load
+    summed over the column, per horizontal area (1e5 Pa) -- in x and y,
+    log10 of beta_internal (clamped to >= 1), the ice mask (+1 where
+    beta_internal > 0, i.e. grounded ice, -1 floating ice, 0 no active
+    vertex) and (sixth channel) log10 of the mean flow-law factor flwafact =
+    0.5 A^(-1/n) over the layers of the vertex's active cells.  Zero at
     vertices that are not active.  The surface and bed enter through the
     driving stress and the grounded/floating mask: the load vector carries
     rho g H grad s and the calving-front pressure, and stays continuous across
-    a periodic seam where the surface itself jumps.  The column sums run
-    level by level, as the device does."""
+    a periodic seam where the surface itself jumps.  The sums run in the
+    device's order (level by level; cells SW, SE, NW, NE of the vertex, each
+    layer by layer)."""
     js, is_ = m.owned_vertex_slices()
     act = np.asarray(arrays["active_vertex"])[js, is_] != 0
     H = np.asarray(arrays["stagthck"])[js, is_]
@@ -442,8 +447,21 @@ def input_features(m: configs.BPModel, arrays: dict) -> np.ndarray:
         sv = sv + lv[..., k]
     area = VOL0 / (m.dx * m.dy) * 1.0e-5
     beta = np.asarray(arrays["beta_internal"])[js, is_]
-    f = np.stack([H / 1000.0, su * area, sv * area, np.log10(np.maximum(beta, 1.0)),
-                  np.where(beta > 0.0, 1.0, -1.0)], axis=-1)
+    chans = [H / 1000.0, su * area, sv * area, np.log10(np.maximum(beta, 1.0)), np.where(beta > 0.0, 1.0, -1.0)]
+    if n_in > 5:
+        fl = np.asarray(arrays["flwafact"])
+        ac = np.asarray(arrays["active_cell"]) != 0
+        j0, j1, i0, i1 = js.start, js.stop, is_.start, is_.stop
+        sf = np.zeros(H.shape)
+        cnt = np.zeros(H.shape)
+        for dj, di in ((0, 0), (0, 1), (1, 0), (1, 1)):  # the cells of which the vertex is the NE, NW, SE, SW corner
+            a = ac[j0 + dj:j1 + dj, i0 + di:i1 + di]
+            for k in range(fl.shape[-1]):
+                sf = sf + np.where(a, fl[j0 + dj:j1 + dj, i0 + di:i1 + di, k], 0.0)
+                cnt = cnt + np.where(a, 1.0, 0.0)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            chans.append(np.where(cnt > 0, np.log10(np.where(cnt > 0, sf / np.maximum(cnt, 1.0), 1.0)), 0.0))
+    f = np.stack(chans[:n_in], axis=-1)
     return np.where(act[..., None], f, 0.0)
 
 

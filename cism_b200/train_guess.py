@@ -80,7 +80,7 @@ MARINE_SOLVE = dict(which_resid=configs.RESID_L2NORM_RELATIVE, pcg_maxiters=5000
                     which_precond=configs.PRECOND_SIA, which_sparse=configs.SPARSE_PCG_CHRONGEAR)
 
 
-def make_marine_set(ctx, sizes, count: int, seed: int, batch: int, log=None, deadline=None):
+def make_marine_set(ctx, sizes, count: int, seed: int, batch: int, log=None, deadline=None, n_in: int = net.N_IN):
     """`count` members of the marine family, sizes drawn from `sizes`,
     solved (mixed precision, column preconditioner, Chronopoulos-Gear, the
     relative-residual Picard criterion) in problems of `batch` same-size
@@ -106,7 +106,7 @@ def make_marine_set(ctx, sizes, count: int, seed: int, batch: int, log=None, dea
             if st["status"] != 0:
                 continue
             M.append(m)
-            F.append(net.pad_grid(net.input_features(m, a)).astype(np.float32))
+            F.append(net.pad_grid(net.input_features(m, a, n_in)).astype(np.float32))
             T.append(net.pad_grid(net.velocity_targets(m, u, v)).astype(np.float32))
             js, is_ = m.owned_vertex_slices()
             K.append(net.pad_grid((np.asarray(a["active_vertex"])[js, is_] != 0).astype(np.float32)[..., None])[..., 0])
@@ -209,7 +209,8 @@ def learned_marine(model: net.UNet, models, arrays):
     """The network's guesses for same-size non-periodic domains."""
     import torch
 
-    F = np.stack([net.normalized_input(model, net.pad_grid(net.input_features(m, a))) for m, a in zip(models, arrays)])
+    F = np.stack([net.normalized_input(model, net.pad_grid(net.input_features(m, a, model.n_in)))
+                  for m, a in zip(models, arrays)])
     x = torch.tensor(F, dtype=torch.float32, device="cuda").to(torch.bfloat16)
     out = model.forward(x.contiguous(), int(models[0].periodic), train=False).cpu().numpy() * model.out_scale
     return [net.guess_from_grid(m, o, a["active_vertex"]) for m, o, a in zip(models, out, arrays)]
@@ -255,7 +256,7 @@ def main_marine(a, log):
     log(f"solved {ntrain} training domains in {t_data:.0f} s")
     model = net.UNet(n_out=24, seed=a.seed)
     act = np.concatenate([v[3].reshape(-1) for v in sets.values()]) > 0
-    allf = np.concatenate([v[1].reshape(-1, net.N_IN) for v in sets.values()])[act]
+    allf = np.concatenate([v[1].reshape(-1, model.n_in) for v in sets.values()])[act]
     allt = np.concatenate([v[2].reshape(-1, 24) for v in sets.values()])[act]
     shift = allf.mean(axis=0)
     scale = 1.0 / np.maximum(allf.std(axis=0), 1e-6)
@@ -319,8 +320,8 @@ def main(argv=None):
         if count > 0:
             sets.append(make_set(ctx, count, n, sd, batch=16 if n == 96 else 8))
             log(f"solved {len(sets[-1][0])} training domains of {n}x{n} ({time.time() - t0:.0f} s)")
-    model = net.UNet(n_out=24, seed=a.seed)
-    allf = np.concatenate([s[1].reshape(-1, net.N_IN) for s in sets])
+    model = net.UNet(n_out=24, seed=a.seed, n_in=5)  # the slab family's five features (net.features)
+    allf = np.concatenate([s[1].reshape(-1, 5) for s in sets])
     allt = np.concatenate([s[2].reshape(-1, 24) for s in sets])
     shift = allf.mean(axis=0)
     scale = 1.0 / np.maximum(allf.std(axis=0), 1e-6)

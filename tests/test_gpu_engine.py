@@ -65,21 +65,23 @@ def test_device_loop_equals_host_loop(ctx, precision):
     assert np.array_equal(ua, ub) and np.array_equal(va, vb)
 
 
-def _random_network(seed=3):
+def _random_network(seed=3, n_in=6):
     from cism_b200 import net
 
-    model = net.UNet(n_out=24, seed=seed)
-    model.in_shift = np.array([1.0, 0.1, -0.1, 2.5, 0.0], np.float32)
-    model.in_scale = np.array([0.8, 0.5, 0.5, 1.2, 1.0], np.float32)
+    model = net.UNet(n_out=24, seed=seed, n_in=n_in)
+    model.in_shift = np.array([1.0, 0.1, -0.1, 2.5, 0.0, 4.0][:n_in], np.float32)
+    model.in_scale = np.array([0.8, 0.5, 0.5, 1.2, 1.0, 2.0][:n_in], np.float32)
     model.out_scale = 35.0
     return model
 
 
-def test_learned_guess_c_abi_matches_python(ctx, tmp_path):
+@pytest.mark.parametrize("n_in", [5, 6])
+def test_learned_guess_c_abi_matches_python(ctx, tmp_path, n_in):
+    """Five inputs, or six with the flow-law factor channel."""
     torch = pytest.importorskip("torch")
     from cism_b200 import net
 
-    model = _random_network()
+    model = _random_network(n_in=n_in)
     path = str(tmp_path / "net.npz")
     model.save(path)
     ctx.load_guess(path)
@@ -92,7 +94,7 @@ def test_learned_guess_c_abi_matches_python(ctx, tmp_path):
     gu, gv = prob.get_guess()
     prob.close()
     # the Python forward of the same weights on the same features
-    F = np.stack([net.normalized_input(model, net.pad_grid(net.input_features(m, p.arrays)))
+    F = np.stack([net.normalized_input(model, net.pad_grid(net.input_features(m, p.arrays, n_in)))
                   for m, p in zip(ms, preps)])
     x = torch.tensor(F, dtype=torch.float32, device="cuda").to(torch.bfloat16).contiguous()
     out = model.forward(x, int(ms[0].periodic), train=False).cpu().numpy() * model.out_scale
