@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <algorithm>
 #include <cstdlib>
 #include <cstring>
 
@@ -441,10 +442,13 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
   return false;
 }
 
+// Split K: CTA z of the grid covers K slices [z * kchunk, min(K, (z + 1) *
+// kchunk)) (kchunk a multiple of TC_BK) and writes its partial product to
+// C + z * cstride; gridDim.z = 1 is the whole K with bias and accumulation.
 __global__ void __launch_bounds__(128) k_gemm_tc(const bf16* __restrict__ A, const bf16* __restrict__ B,
                                                  float* __restrict__ C, const float* __restrict__ bias,
                                                  int M, int N, int K, int lda, int ldb, int ldc,
-                                                 int accum) {
+                                                 int accum, int kchunk, long long cstride) {
   extern __shared__ __align__(1024) uint8_t tc_smem[];
   __shared__ __align__(8) uint64_t bar[2];
   __shared__ uint32_t tmem_slot;
@@ -464,7 +468,9 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const bf16* __restrict__ A, con
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_slot;
-  const int nk = (K + TC_BK - 1) / TC_BK;
+  const int kbeg = blockIdx.z * kchunk, kend = min(K, kbeg + kchunk);
+  C += (size_t)blockIdx.z * cstride;
+  const int nk = (kend - kbeg + TC_BK - 1) / TC_BK;
   bool ok = true;
   for (int it = 0; it < nk; ++it) {
     const int st = it & 1;
@@ -475,17 +481,17 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const bf16* __restrict__ A, con
       ok = false;
       break;
     }
-    const int k0 = it * TC_BK;
+    const int k0 = kbeg + it * TC_BK;
     for (int c = tid; c < TC_BM * 8; c += 128) {  // 128 rows x 8 chunks of 8 K elements
       const int r = c >> 3, kc = c & 7, gm = m0 + r, gk = k0 + kc * 8;
       uint4 val = make_uint4(0u, 0u, 0u, 0u);
-      if (gm < M && gk < K) val = __ldg(reinterpret_cast<const uint4*>(A + (size_t)gm * lda + gk));
+      if (gm < M && gk < kend) val = __ldg(reinterpret_cast<const uint4*>(A + (size_t)gm * lda + gk));
       *reinterpret_cast<uint4*>(As + (kc * (TC_BM / 8) + (r >> 3)) * 128 + (r & 7) * 16) = val;
     }
     for (int c = tid; c < TC_BN * 8; c += 128) {
       const int r = c >> 3, kc = c & 7, gn = n0 + r, gk = k0 + kc * 8;
       uint4 val = make_uint4(0u, 0u, 0u, 0u);
-      if (gn < N && gk < K) val = __ldg(reinterpret_cast<const uint4*>(B + (size_t)gn * ldb + gk));
+      if (gn < N && gk < kend) val = __ldg(reinterpret_cast<const uint4*>(B + (size_t)gn * ldb + gk));
       *reinterpret_cast<uint4*>(Bs + (kc * (TC_BN / 8) + (r >> 3)) * 128 + (r & 7) * 16) = val;
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // the tensor core reads through the async proxy
@@ -494,7 +500,7 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const bf16* __restrict__ A, con
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll
       for (int s = 0; s < TC_BK / 16; ++s) {
-        if (k0 + 16 * s >= K) break;
+        if (k0 + 16 * s >= kend) break;
         const uint64_t ad = umma_desc(smem_u32(As) + 2 * s * (TC_BM / 8) * 128, (TC_BM / 8) * 128, 128);
         const uint64_t bd = umma_desc(smem_u32(Bs) + 2 * s * (TC_BN / 8) * 128, (TC_BN / 8) * 128, 128);
         const uint32_t acc = (it > 0 || s > 0) ? 1u : 0u;
@@ -508,7 +514,8 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const bf16* __restrict__ A, con
                    : "memory");
     }
   }
-  // the last commit completes after every multiply of the tile
+  // the last commit completes after every multiply of the tile (the host
+  // never launches an empty K range)
   if (ok) ok = mbar_wait(smem_u32(&bar[(nk - 1) & 1]), ((nk - 1) >> 1) & 1);
   ok = __syncthreads_and(ok);
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -547,12 +554,45 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const bf16* __restrict__ A, con
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_BN));
 }
 
+// C[r][c] = sum over z of part[z][r][c] in z order (+ bias) (+ C): the
+// split-K partial products, summed deterministically.
+__global__ void k_splitk_sum(const float* __restrict__ part, int S, long long cstride, float* __restrict__ C,
+                             const float* __restrict__ bias, int M, int N, int ldc, int accum) {
+  GRID_LOOP(id, (long long)M * N) {
+    const long long r = id / N;
+    const int c = (int)(id % N);
+    float v = 0.f;
+    for (int z = 0; z < S; ++z) v += part[z * cstride + id];
+    if (bias) v += bias[c];
+    float* dst = C + r * ldc + c;
+    if (accum) v += *dst;
+    *dst = v;
+  }
+}
+
+// Grow-only device scratch of the split-K partial products.
+float* splitk_scratch(size_t n) {
+  static float* buf = nullptr;
+  static size_t cap = 0;
+  if (n > cap) {
+    if (buf) cudaFree(buf);
+    buf = nullptr;
+    cap = 0;
+    if (cudaMalloc(&buf, n * sizeof(float)) != cudaSuccess) return nullptr;
+    cap = n;
+  }
+  return buf;
+}
+
 }  // namespace
 
 extern "C" {
 
 // Returns 0, or 10 for arguments the kernel does not take.  The tcgen05
-// kernel (k_gemm_tc); BPNET_GEMM=mma selects the mma.sync one.
+// kernel (k_gemm_tc); BPNET_GEMM=mma selects the mma.sync one.  A product
+// with few output tiles and a long K (the weight gradients, K = pixels)
+// is split along K over enough CTAs to fill the GPU, its partial products
+// summed in order by k_splitk_sum.
 int bpnet_gemm_tn(const void* A, const void* B, float* C, const float* bias, int M, int N, int K, int lda,
                   int ldb, int ldc, int accum, void* stream) {
   if (M <= 0 || N <= 0 || K <= 0 || (K % 8) || (lda % 8) || (ldb % 8)) return 10;
@@ -568,9 +608,22 @@ int bpnet_gemm_tn(const void* A, const void* B, float* C, const float* bias, int
     k_gemm_tn<<<grid, 128, 0, (cudaStream_t)stream>>>((const bf16*)A, (const bf16*)B, C, bias, M, N, K, lda,
                                                        ldb, ldc, accum);
   } else {
-    dim3 grid((N + TC_BN - 1) / TC_BN, (M + TC_BM - 1) / TC_BM);
-    k_gemm_tc<<<grid, 128, 2 * TC_STAGE, (cudaStream_t)stream>>>((const bf16*)A, (const bf16*)B, C, bias, M, N,
-                                                                 K, lda, ldb, ldc, accum);
+    const int gx = (N + TC_BN - 1) / TC_BN, gy = (M + TC_BM - 1) / TC_BM, nslices = (K + TC_BK - 1) / TC_BK;
+    int S = 1;
+    if (gx * gy < 296 && nslices >= 64) S = std::min((296 + gx * gy - 1) / (gx * gy), nslices / 16);
+    if (S > 1) {
+      const int kchunk = (nslices + S - 1) / S * TC_BK;
+      S = (K + kchunk - 1) / kchunk;  // no empty chunk
+      const long long cs = (long long)M * N;
+      float* part = splitk_scratch((size_t)S * cs);
+      if (!part) return 6;
+      k_gemm_tc<<<dim3(gx, gy, S), 128, 2 * TC_STAGE, (cudaStream_t)stream>>>(
+          (const bf16*)A, (const bf16*)B, part, nullptr, M, N, K, lda, ldb, N, 0, kchunk, cs);
+      k_splitk_sum<<<grid_for(cs), 256, 0, (cudaStream_t)stream>>>(part, S, cs, C, bias, M, N, ldc, accum);
+    } else {
+      k_gemm_tc<<<dim3(gx, gy, 1), 128, 2 * TC_STAGE, (cudaStream_t)stream>>>(
+          (const bf16*)A, (const bf16*)B, C, bias, M, N, K, lda, ldb, ldc, accum, nslices * TC_BK, 0);
+    }
   }
   return cudaGetLastError() == cudaSuccess ? 0 : 6;
 }
