@@ -80,7 +80,9 @@ def _net_from_oracle(convs, channels, n_out):
     import torch
     from cism_b200 import net as netmod
 
-    dev = netmod.UNet(n_out=n_out, channels=channels)
+    w0, _, k30, _ = convs[0]
+    n_in = w0.shape[1] // 9 if k30 else w0.shape[1]  # the restatement's input channels
+    dev = netmod.UNet(n_out=n_out, channels=channels, n_in=n_in)
     for cv, (w, b, k3, act) in zip(dev.convs(), convs):
         cv.w.copy_(torch.tensor(w, dtype=torch.float32))
         cv.b.copy_(torch.tensor(b, dtype=torch.float32))
