@@ -3,7 +3,7 @@
 * The periodic slab (160 x 160 x 11) and the large marine sheet
   (400 x 400 x 11): one Picard pass from the shallow-ice velocity with
   exactly 40 PCG iterations (tolerance 0) -- setup, assembly at that
-  velocity, the column-march Krylov matvec and both PCG variants --
+  velocity (element-centric), the Krylov matvec and both PCG variants --
   against the oracle doing the same, to 1e-10 relative L2 (the same
   algorithm for a fixed iteration count: roundoff differences only).
 * The periodic slab solved to convergence against the oracle's converged
