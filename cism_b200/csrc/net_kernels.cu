@@ -402,12 +402,15 @@ inline unsigned grid_for(long long n) {
 // tcgen05.mma of a slice and commits them to the stage's mbarrier; the
 // stage is refilled once that barrier completes.  The epilogue reads the
 // accumulator with tcgen05.ld (warp w: rows 32w..32w+31) and adds the bias
-// (and C).  Every wait is bounded: past the limit the kernel raises
-// g_tc_err, stops issuing, frees its tensor memory and returns.
+// (and C) through shared memory, so that stores run along rows.  Every
+// wait is bounded: past the limit the kernel raises g_tc_err, stops
+// issuing, frees its tensor memory and returns.
 // ---------------------------------------------------------------------
-constexpr int TC_BM = 128, TC_BN = 64, TC_BK = 64;
-constexpr int TC_A_BYTES = TC_BM * TC_BK * 2, TC_B_BYTES = TC_BN * TC_BK * 2;
-constexpr int TC_STAGE = TC_A_BYTES + TC_B_BYTES;  // 24 KB; two stages in 48 KB of dynamic shared memory
+constexpr int TC_BM = 128, TC_BK = 64;
+constexpr int TC_A_BYTES = TC_BM * TC_BK * 2;
+// BN = 64, or 32 for the products with at most 32 output columns
+template <int BN>
+constexpr int tc_stage_bytes() { return TC_A_BYTES + BN * TC_BK * 2; }  // 24 or 20 KB; two stages
 
 __device__ int g_tc_err = 0;  // a wait of k_gemm_tc ran out (read and cleared by bpnet_gemm_status)
 
@@ -424,8 +427,10 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint3
 // Instruction descriptor of kind::f16: FP32 accumulator (bits 4-5 = 1), A
 // and B BF16 (bits 7-9, 10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4
 // at bit 24.
-constexpr uint32_t TC_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TC_BN >> 3) << 17) |
-                              ((uint32_t)(TC_BM >> 4) << 24);
+template <int BN>
+constexpr uint32_t tc_idesc() {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(TC_BM >> 4) << 24);
+}
 
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
   for (int i = 0; i < (1 << 24); ++i) {
@@ -445,6 +450,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
 // Split K: CTA z of the grid covers K slices [z * kchunk, min(K, (z + 1) *
 // kchunk)) (kchunk a multiple of TC_BK) and writes its partial product to
 // C + z * cstride; gridDim.z = 1 is the whole K with bias and accumulation.
+template <int BN>
 __global__ void __launch_bounds__(128) k_gemm_tc(const bf16* __restrict__ A, const bf16* __restrict__ B,
                                                  float* __restrict__ C, const float* __restrict__ bias,
                                                  int M, int N, int K, int lda, int ldb, int ldc,
@@ -453,10 +459,11 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const bf16* __restrict__ A, con
   __shared__ __align__(8) uint64_t bar[2];
   __shared__ uint32_t tmem_slot;
   const int tid = threadIdx.x, warp = tid >> 5;
-  const int m0 = blockIdx.y * TC_BM, n0 = blockIdx.x * TC_BN;
+  constexpr int STAGE = tc_stage_bytes<BN>();
+  const int m0 = blockIdx.y * TC_BM, n0 = blockIdx.x * BN;
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
-                 "r"(TC_BN));
+                 "r"(BN));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (tid == 0) {
@@ -474,7 +481,7 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const bf16* __restrict__ A, con
   bool ok = true;
   for (int it = 0; it < nk; ++it) {
     const int st = it & 1;
-    uint8_t* As = tc_smem + st * TC_STAGE;
+    uint8_t* As = tc_smem + st * STAGE;
     uint8_t* Bs = As + TC_A_BYTES;
     if (it >= 2) ok = mbar_wait(smem_u32(&bar[st]), ((it - 2) >> 1) & 1);  // the stage's last slice is done
     if (!__syncthreads_and(ok)) {
@@ -488,11 +495,11 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const bf16* __restrict__ A, con
       if (gm < M && gk < kend) val = __ldg(reinterpret_cast<const uint4*>(A + (size_t)gm * lda + gk));
       *reinterpret_cast<uint4*>(As + (kc * (TC_BM / 8) + (r >> 3)) * 128 + (r & 7) * 16) = val;
     }
-    for (int c = tid; c < TC_BN * 8; c += 128) {
+    for (int c = tid; c < BN * 8; c += 128) {
       const int r = c >> 3, kc = c & 7, gn = n0 + r, gk = k0 + kc * 8;
       uint4 val = make_uint4(0u, 0u, 0u, 0u);
       if (gn < N && gk < kend) val = __ldg(reinterpret_cast<const uint4*>(B + (size_t)gn * ldb + gk));
-      *reinterpret_cast<uint4*>(Bs + (kc * (TC_BN / 8) + (r >> 3)) * 128 + (r & 7) * 16) = val;
+      *reinterpret_cast<uint4*>(Bs + (kc * (BN / 8) + (r >> 3)) * 128 + (r & 7) * 16) = val;
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // the tensor core reads through the async proxy
     __syncthreads();
@@ -502,12 +509,12 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const bf16* __restrict__ A, con
       for (int s = 0; s < TC_BK / 16; ++s) {
         if (k0 + 16 * s >= kend) break;
         const uint64_t ad = umma_desc(smem_u32(As) + 2 * s * (TC_BM / 8) * 128, (TC_BM / 8) * 128, 128);
-        const uint64_t bd = umma_desc(smem_u32(Bs) + 2 * s * (TC_BN / 8) * 128, (TC_BN / 8) * 128, 128);
+        const uint64_t bd = umma_desc(smem_u32(Bs) + 2 * s * (BN / 8) * 128, (BN / 8) * 128, 128);
         const uint32_t acc = (it > 0 || s > 0) ? 1u : 0u;
         asm volatile(
             "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
             "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
-            ::"r"(tmem), "l"(ad), "l"(bd), "r"(TC_IDESC), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+            ::"r"(tmem), "l"(ad), "l"(bd), "r"(tc_idesc<BN>()), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
       }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                        smem_u32(&bar[st]))
@@ -520,9 +527,14 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const bf16* __restrict__ A, con
   ok = __syncthreads_and(ok);
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (ok) {
-    const int row = m0 + warp * 32 + (tid & 31);
+    // warp w holds rows 32w..32w+31 of the tile (one row per lane); each
+    // 32 x 32 block goes through shared memory (the stages are free now)
+    // so that a store instruction writes 32 consecutive columns of a row
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // after the tensor core's reads of the stages
+    float* T = reinterpret_cast<float*>(tc_smem) + warp * (32 * 33);
+    const int lane = tid & 31;
 #pragma unroll
-    for (int c0 = 0; c0 < TC_BN; c0 += 32) {
+    for (int c0 = 0; c0 < BN; c0 += 32) {
       uint32_t v[32];
       asm volatile(
           "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
@@ -534,24 +546,27 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const bf16* __restrict__ A, con
             "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
           : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0));
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      if (row < M) {
-        float* crow = C + (size_t)row * ldc;
 #pragma unroll
-        for (int j = 0; j < 32; ++j) {
-          const int col = n0 + c0 + j;
-          if (col < N) {
-            float r = __uint_as_float(v[j]);
-            if (bias) r += bias[col];
-            if (accum) r += crow[col];
-            crow[col] = r;
-          }
+      for (int j = 0; j < 32; ++j) T[lane * 33 + j] = __uint_as_float(v[j]);
+      __syncwarp();
+      const int col = n0 + c0 + lane;
+      if (col < N) {
+        const float bc = bias ? bias[col] : 0.f;
+        for (int r = 0; r < 32; ++r) {
+          const int row = m0 + warp * 32 + r;
+          if (row >= M) break;
+          float* dst = C + (size_t)row * ldc + col;
+          float x = T[r * 33 + lane] + bc;
+          if (accum) x += *dst;
+          *dst = x;
         }
       }
+      __syncwarp();
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
-  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_BN));
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN));
 }
 
 // C[r][c] = sum over z of part[z][r][c] in z order (+ bias) (+ C): the
@@ -600,15 +615,21 @@ int bpnet_gemm_tn(const void* A, const void* B, float* C, const float* bias, int
     const char* e = std::getenv("BPNET_GEMM");
     return e && std::strcmp(e, "mma") == 0;
   }();
-  static const bool smem_ok =  // 48 KB of dynamic shared memory: two stages
-      cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * TC_STAGE) == cudaSuccess;
+  static const bool smem_ok =  // two stages of dynamic shared memory (48 or 40 KB)
+      cudaFuncSetAttribute(k_gemm_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           2 * tc_stage_bytes<64>()) == cudaSuccess &&
+      cudaFuncSetAttribute(k_gemm_tc<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           2 * tc_stage_bytes<32>()) == cudaSuccess;
   if (!smem_ok) return 6;
   if (use_mma) {
     dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
     k_gemm_tn<<<grid, 128, 0, (cudaStream_t)stream>>>((const bf16*)A, (const bf16*)B, C, bias, M, N, K, lda,
                                                        ldb, ldc, accum);
   } else {
-    const int gx = (N + TC_BN - 1) / TC_BN, gy = (M + TC_BM - 1) / TC_BM, nslices = (K + TC_BK - 1) / TC_BK;
+    const bool narrow = N <= 32;  // a 128 x 32 tile: no MMA work on padding columns
+    const int bn = narrow ? 32 : 64, smem = narrow ? 2 * tc_stage_bytes<32>() : 2 * tc_stage_bytes<64>();
+    auto kern = narrow ? k_gemm_tc<32> : k_gemm_tc<64>;
+    const int gx = (N + bn - 1) / bn, gy = (M + TC_BM - 1) / TC_BM, nslices = (K + TC_BK - 1) / TC_BK;
     int S = 1;
     if (gx * gy < 296 && nslices >= 64) S = std::min((296 + gx * gy - 1) / (gx * gy), nslices / 16);
     if (S > 1) {
@@ -617,12 +638,12 @@ int bpnet_gemm_tn(const void* A, const void* B, float* C, const float* bias, int
       const long long cs = (long long)M * N;
       float* part = splitk_scratch((size_t)S * cs);
       if (!part) return 6;
-      k_gemm_tc<<<dim3(gx, gy, S), 128, 2 * TC_STAGE, (cudaStream_t)stream>>>(
-          (const bf16*)A, (const bf16*)B, part, nullptr, M, N, K, lda, ldb, N, 0, kchunk, cs);
+      kern<<<dim3(gx, gy, S), 128, smem, (cudaStream_t)stream>>>((const bf16*)A, (const bf16*)B, part, nullptr, M,
+                                                                  N, K, lda, ldb, N, 0, kchunk, cs);
       k_splitk_sum<<<grid_for(cs), 256, 0, (cudaStream_t)stream>>>(part, S, cs, C, bias, M, N, ldc, accum);
     } else {
-      k_gemm_tc<<<dim3(gx, gy, 1), 128, 2 * TC_STAGE, (cudaStream_t)stream>>>(
-          (const bf16*)A, (const bf16*)B, C, bias, M, N, K, lda, ldb, ldc, accum, nslices * TC_BK, 0);
+      kern<<<dim3(gx, gy, 1), 128, smem, (cudaStream_t)stream>>>((const bf16*)A, (const bf16*)B, C, bias, M, N, K,
+                                                                  lda, ldb, ldc, accum, nslices * TC_BK, 0);
     }
   }
   return cudaGetLastError() == cudaSuccess ? 0 : 6;
