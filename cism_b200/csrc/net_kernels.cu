@@ -19,6 +19,8 @@
 #include <cstdint>
 #include <algorithm>
 #include <cstdlib>
+#include <map>
+#include <mutex>
 #include <cstring>
 
 namespace {
@@ -585,18 +587,26 @@ __global__ void k_splitk_sum(const float* __restrict__ part, int S, long long cs
   }
 }
 
-// Grow-only device scratch of the split-K partial products.
+// Grow-only scratch of the split-K partial products, one per device (the
+// current one); a buffer is replaced only after the device has finished
+// with it.
 float* splitk_scratch(size_t n) {
-  static float* buf = nullptr;
-  static size_t cap = 0;
-  if (n > cap) {
-    if (buf) cudaFree(buf);
-    buf = nullptr;
-    cap = 0;
-    if (cudaMalloc(&buf, n * sizeof(float)) != cudaSuccess) return nullptr;
-    cap = n;
+  static std::mutex mu;
+  static std::map<int, std::pair<float*, size_t>> bufs;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  std::lock_guard<std::mutex> lock(mu);
+  auto& b = bufs[dev];
+  if (n > b.second) {
+    if (b.first) {
+      cudaDeviceSynchronize();
+      cudaFree(b.first);
+    }
+    b = {nullptr, 0};
+    if (cudaMalloc(&b.first, n * sizeof(float)) != cudaSuccess) return nullptr;
+    b.second = n;
   }
-  return buf;
+  return b.first;
 }
 
 }  // namespace
