@@ -13,6 +13,8 @@
 // gradients, the loss) run in a fixed order, so a training run is
 // deterministic.  Every entry point is extern "C" with plain device
 // pointers and the CUDA stream to launch on.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -571,6 +573,198 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const bf16* __restrict__ A, con
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN));
 }
 
+// ---------------------------------------------------------------------
+// The same product with its operands brought in by the Tensor Memory
+// Accelerator: a four-stage ring of shared-memory slices, each filled by
+// 16 cp.async.bulk.tensor boxes (one K chunk of 8 elements by 128 rows of
+// A, or by BN rows of B: exactly one column of core matrices of the
+// no-swizzle K-major layout, so the boxes land where the UMMA descriptors
+// read) that complete on the stage's "full" mbarrier.  One thread issues
+// the loads and the tcgen05.mma of every slice; a stage is refilled with
+// the slice four ahead once the tensor core's commit for it has arrived on
+// the stage's "done" mbarrier, so up to four slices of loads are in flight
+// while the tensor core works.  Out-of-range rows and K columns read as
+// zero (the tensor maps' bounds).  Epilogue as k_gemm_tc.  Every wait is
+// bounded; on a timeout the issuing thread waits (bounded) for its copies
+// and its last multiply in flight, raises g_tc_err, and the CTA frees its
+// tensor memory and returns.  Loads only: no TMA store, no multicast.
+// ---------------------------------------------------------------------
+constexpr int TM_STAGES = 4;
+
+template <int BN>
+constexpr int tm_smem_bytes() { return TM_STAGES * tc_stage_bytes<BN>() + 1024; }  // + room to align the ring
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%1], %0;" ::"r"(bytes), "r"(bar) : "memory");
+}
+
+// A box of the 2-D tensor map at (x = K element, y = row) into shared
+// memory; x is always a multiple of 8 (16 bytes).
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::
+          "r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(x), "r"(y)
+      : "memory");
+}
+
+template <int BN>
+__global__ void __launch_bounds__(128) k_gemm_tma(const __grid_constant__ CUtensorMap tmA,
+                                                  const __grid_constant__ CUtensorMap tmB, float* __restrict__ C,
+                                                  const float* __restrict__ bias, int M, int N, int K, int ldc,
+                                                  int accum, int kchunk, long long cstride) {
+  extern __shared__ __align__(1024) uint8_t tc_smem[];
+  __shared__ __align__(8) uint64_t full[TM_STAGES], done[TM_STAGES];
+  __shared__ uint32_t tmem_slot;
+  __shared__ int s_ok;
+  constexpr int STAGE = tc_stage_bytes<BN>();
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int m0 = blockIdx.y * TC_BM, n0 = blockIdx.x * BN;
+  const int kbeg = blockIdx.z * kchunk, kend = min(K, kbeg + kchunk);
+  C += (size_t)blockIdx.z * cstride;
+  const int nk = (kend - kbeg + TC_BK - 1) / TC_BK;
+  // the ring starts on a 1024-byte boundary (the boxes land on 512-byte ones)
+  const uint32_t ring = (smem_u32(tc_smem) + 1023u) & ~1023u;
+  uint8_t* ring_ptr = tc_smem + (ring - smem_u32(tc_smem));
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                 "r"(BN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    for (int st = 0; st < TM_STAGES; ++st) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&full[st])));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&done[st])));
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    s_ok = 1;
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_slot;
+  if (tid == 0) {
+    auto issue = [&](int j) {  // slice j into stage j % TM_STAGES
+      const int st = j % TM_STAGES;
+      const uint32_t a = ring + st * STAGE, b = a + TC_A_BYTES, bar = smem_u32(&full[st]);
+      mbar_expect_tx(bar, STAGE);
+      const int k0 = kbeg + j * TC_BK;
+#pragma unroll
+      for (int kc = 0; kc < 8; ++kc) {
+        tma_load_2d(a + kc * (TC_BM / 8) * 128, &tmA, k0 + kc * 8, m0, bar);
+        tma_load_2d(b + kc * (BN / 8) * 128, &tmB, k0 + kc * 8, n0, bar);
+      }
+    };
+    bool ok = true;
+    int issued = 0, it = 0, last_mma = -1;
+    for (; issued < nk && issued < TM_STAGES; ++issued) issue(issued);
+    for (; it < nk; ++it) {
+      const int st = it % TM_STAGES;
+      if (!mbar_wait(smem_u32(&full[st]), (it / TM_STAGES) & 1)) {
+        ok = false;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const int k0 = kbeg + it * TC_BK;
+      const uint32_t a = ring + st * STAGE, b = a + TC_A_BYTES;
+#pragma unroll
+      for (int s = 0; s < TC_BK / 16; ++s) {
+        if (k0 + 16 * s >= kend) break;
+        const uint64_t ad = umma_desc(a + 2 * s * (TC_BM / 8) * 128, (TC_BM / 8) * 128, 128);
+        const uint64_t bd = umma_desc(b + 2 * s * (BN / 8) * 128, (BN / 8) * 128, 128);
+        const uint32_t acc = (it > 0 || s > 0) ? 1u : 0u;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem),
+            "l"(ad), "l"(bd), "r"(tc_idesc<BN>()), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       smem_u32(&done[st]))
+                   : "memory");
+      last_mma = it;
+      if (issued < nk) {  // the stage takes the slice TM_STAGES ahead once this multiply has read it
+        if (!mbar_wait(smem_u32(&done[st]), (it / TM_STAGES) & 1)) {
+          ok = false;
+          ++it;
+          break;
+        }
+        issue(issued);
+        ++issued;
+      }
+    }
+    if (ok && last_mma >= 0)  // the last commit completes after every multiply of the tile
+      ok = mbar_wait(smem_u32(&done[last_mma % TM_STAGES]), (last_mma / TM_STAGES) & 1);
+    if (!ok) {  // no copy and no multiply may still be in flight when the CTA exits
+      for (int j = it; j < issued; ++j) mbar_wait(smem_u32(&full[j % TM_STAGES]), (j / TM_STAGES) & 1);
+      if (last_mma >= 0) mbar_wait(smem_u32(&done[last_mma % TM_STAGES]), (last_mma / TM_STAGES) & 1);
+      s_ok = 0;
+    }
+  }
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (s_ok) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // after the copies and the tensor core's reads
+    float* T = reinterpret_cast<float*>(ring_ptr) + warp * (32 * 33);
+    const int lane = tid & 31;
+#pragma unroll
+    for (int c0 = 0; c0 < BN; c0 += 32) {
+      uint32_t v[32];
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+          "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+            "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
+            "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
+            "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+          : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+      for (int j = 0; j < 32; ++j) T[lane * 33 + j] = __uint_as_float(v[j]);
+      __syncwarp();
+      const int col = n0 + c0 + lane;
+      if (col < N) {
+        const float bc = bias ? bias[col] : 0.f;
+        for (int r = 0; r < 32; ++r) {
+          const int row = m0 + warp * 32 + r;
+          if (row >= M) break;
+          float* dst = C + (size_t)row * ldc + col;
+          float x = T[r * 33 + lane] + bc;
+          if (accum) x += *dst;
+          *dst = x;
+        }
+      }
+      __syncwarp();
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN));
+}
+
+// The 2-D tensor map of a row-major BF16 operand [rows][ld] (K = the first
+// K columns) with boxes of 8 K elements by box_rows rows; false where the
+// driver has no encoder or refuses the operand (address or stride not
+// 16-byte aligned).
+bool tma_map(CUtensorMap* map, const void* ptr, int rows, int K, int ld, int box_rows) {
+  static PFN_cuTensorMapEncodeTiled_v12000 enc = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+  }();
+  if (!enc || (reinterpret_cast<uintptr_t>(ptr) & 15) || ((size_t)ld * 2) % 16) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+  const cuuint32_t box[2] = {8, (cuuint32_t)box_rows};
+  const cuuint32_t es[2] = {1, 1};
+  return enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(ptr), dims, strides, box, es,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 // C[r][c] = sum over z of part[z][r][c] in z order (+ bias) (+ C): the
 // split-K partial products, summed deterministically.
 __global__ void k_splitk_sum(const float* __restrict__ part, int S, long long cstride, float* __restrict__ C,
@@ -613,50 +807,81 @@ float* splitk_scratch(size_t n) {
 
 extern "C" {
 
-// Returns 0, or 10 for arguments the kernel does not take.  The tcgen05
-// kernel (k_gemm_tc); BPNET_GEMM=mma selects the mma.sync one.  A product
+// Returns 0, or 10 for arguments the kernels do not take.  A product
 // with few output tiles and a long K (the weight gradients, K = pixels)
 // is split along K over enough CTAs to fill the GPU, its partial products
 // summed in order by k_splitk_sum.
-int bpnet_gemm_tn(const void* A, const void* B, float* C, const float* bias, int M, int N, int K, int lda,
-                  int ldb, int ldc, int accum, void* stream) {
-  if (M <= 0 || N <= 0 || K <= 0 || (K % 8) || (lda % 8) || (ldb % 8)) return 10;
-  static const bool use_mma = [] {
-    const char* e = std::getenv("BPNET_GEMM");
-    return e && std::strcmp(e, "mma") == 0;
-  }();
-  static const bool smem_ok =  // two stages of dynamic shared memory (48 or 40 KB)
+// The product with an explicit kernel: mode 0 tcgen05 with TMA-fed operands
+// (k_gemm_tma), 1 tcgen05 with register-staged operands (k_gemm_tc), 2 the
+// mma.sync kernel.
+int bpnet_gemm_tn_mode(int mode, const void* A, const void* B, float* C, const float* bias, int M, int N, int K,
+                       int lda, int ldb, int ldc, int accum, void* stream) {
+  if (M <= 0 || N <= 0 || K <= 0 || (K % 8) || (lda % 8) || (ldb % 8) || mode < 0 || mode > 2) return 10;
+  static const bool smem_ok =
       cudaFuncSetAttribute(k_gemm_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            2 * tc_stage_bytes<64>()) == cudaSuccess &&
       cudaFuncSetAttribute(k_gemm_tc<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           2 * tc_stage_bytes<32>()) == cudaSuccess;
+                           2 * tc_stage_bytes<32>()) == cudaSuccess &&
+      cudaFuncSetAttribute(k_gemm_tma<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, tm_smem_bytes<64>()) ==
+          cudaSuccess &&
+      cudaFuncSetAttribute(k_gemm_tma<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, tm_smem_bytes<32>()) ==
+          cudaSuccess;
   if (!smem_ok) return 6;
-  if (use_mma) {
+  cudaStream_t st = (cudaStream_t)stream;
+  if (mode == 2) {
     dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
-    k_gemm_tn<<<grid, 128, 0, (cudaStream_t)stream>>>((const bf16*)A, (const bf16*)B, C, bias, M, N, K, lda,
-                                                       ldb, ldc, accum);
-  } else {
-    const bool narrow = N <= 32;  // a 128 x 32 tile: no MMA work on padding columns
-    const int bn = narrow ? 32 : 64, smem = narrow ? 2 * tc_stage_bytes<32>() : 2 * tc_stage_bytes<64>();
-    auto kern = narrow ? k_gemm_tc<32> : k_gemm_tc<64>;
-    const int gx = (N + bn - 1) / bn, gy = (M + TC_BM - 1) / TC_BM, nslices = (K + TC_BK - 1) / TC_BK;
-    int S = 1;
-    if (gx * gy < 296 && nslices >= 64) S = std::min((296 + gx * gy - 1) / (gx * gy), nslices / 16);
-    if (S > 1) {
-      const int kchunk = (nslices + S - 1) / S * TC_BK;
-      S = (K + kchunk - 1) / kchunk;  // no empty chunk
-      const long long cs = (long long)M * N;
-      float* part = splitk_scratch((size_t)S * cs);
-      if (!part) return 6;
-      kern<<<dim3(gx, gy, S), 128, smem, (cudaStream_t)stream>>>((const bf16*)A, (const bf16*)B, part, nullptr, M,
-                                                                  N, K, lda, ldb, N, 0, kchunk, cs);
-      k_splitk_sum<<<grid_for(cs), 256, 0, (cudaStream_t)stream>>>(part, S, cs, C, bias, M, N, ldc, accum);
-    } else {
-      kern<<<dim3(gx, gy, 1), 128, smem, (cudaStream_t)stream>>>((const bf16*)A, (const bf16*)B, C, bias, M, N, K,
-                                                                  lda, ldb, ldc, accum, nslices * TC_BK, 0);
-    }
+    k_gemm_tn<<<grid, 128, 0, st>>>((const bf16*)A, (const bf16*)B, C, bias, M, N, K, lda, ldb, ldc, accum);
+    return cudaGetLastError() == cudaSuccess ? 0 : 6;
   }
+  const bool narrow = N <= 32;  // a 128 x 32 tile: no MMA work on padding columns
+  const int bn = narrow ? 32 : 64;
+  const int gx = (N + bn - 1) / bn, gy = (M + TC_BM - 1) / TC_BM, nslices = (K + TC_BK - 1) / TC_BK;
+  int S = 1, kchunk = nslices * TC_BK;
+  if (gx * gy < 296 && nslices >= 64) S = std::min((296 + gx * gy - 1) / (gx * gy), nslices / 16);
+  float* out = C;
+  const float* bout = bias;
+  int ldo = ldc, acc = accum;
+  long long cs = 0;
+  if (S > 1) {  // partial products into the scratch, summed afterwards
+    kchunk = (nslices + S - 1) / S * TC_BK;
+    S = (K + kchunk - 1) / kchunk;  // no empty chunk
+    cs = (long long)M * N;
+    out = splitk_scratch((size_t)S * cs);
+    if (!out) return 6;
+    bout = nullptr;
+    ldo = N;
+    acc = 0;
+  }
+  const dim3 grid(gx, gy, S);
+  CUtensorMap ma, mb;
+  if (mode == 0 && tma_map(&ma, A, M, K, lda, TC_BM) && tma_map(&mb, B, N, K, ldb, bn)) {
+    if (narrow)
+      k_gemm_tma<32><<<grid, 128, tm_smem_bytes<32>(), st>>>(ma, mb, out, bout, M, N, K, ldo, acc, kchunk, cs);
+    else
+      k_gemm_tma<64><<<grid, 128, tm_smem_bytes<64>(), st>>>(ma, mb, out, bout, M, N, K, ldo, acc, kchunk, cs);
+  } else if (narrow) {
+    k_gemm_tc<32><<<grid, 128, 2 * tc_stage_bytes<32>(), st>>>((const bf16*)A, (const bf16*)B, out, bout, M, N, K,
+                                                               lda, ldb, ldo, acc, kchunk, cs);
+  } else {
+    k_gemm_tc<64><<<grid, 128, 2 * tc_stage_bytes<64>(), st>>>((const bf16*)A, (const bf16*)B, out, bout, M, N, K,
+                                                               lda, ldb, ldo, acc, kchunk, cs);
+  }
+  if (S > 1) k_splitk_sum<<<grid_for(cs), 256, 0, st>>>(out, S, cs, C, bias, M, N, ldc, accum);
   return cudaGetLastError() == cudaSuccess ? 0 : 6;
+}
+
+// The product on the default kernel: tcgen05 with TMA-fed operands;
+// BPNET_GEMM=tc selects the register-staged tcgen05 kernel, BPNET_GEMM=mma
+// the mma.sync one.
+int bpnet_gemm_tn(const void* A, const void* B, float* C, const float* bias, int M, int N, int K, int lda,
+                  int ldb, int ldc, int accum, void* stream) {
+  static const int mode = [] {
+    const char* e = std::getenv("BPNET_GEMM");
+    if (e && std::strcmp(e, "mma") == 0) return 2;
+    if (e && std::strcmp(e, "tc") == 0) return 1;
+    return 0;
+  }();
+  return bpnet_gemm_tn_mode(mode, A, B, C, bias, M, N, K, lda, ldb, ldc, accum, stream);
 }
 
 // The mma.sync kernel (the comparison of the tcgen05 one).

@@ -43,6 +43,7 @@ def lib():
         sig = {
             "bpnet_gemm_tn": [vp, vp, vp, vp, i, i, i, i, i, i, i, vp],
             "bpnet_gemm_tn_mma": [vp, vp, vp, vp, i, i, i, i, i, i, i, vp],
+            "bpnet_gemm_tn_mode": [i, vp, vp, vp, vp, i, i, i, i, i, i, i, vp],
             "bpnet_gemm_status": [vp],
             "bpnet_im2col": [vp, vp, i, i, i, i, i, i, vp],
             "bpnet_col2im": [vp, vp, i, i, i, i, i, i, vp],
@@ -99,11 +100,19 @@ def ceil8(x: int) -> int:
     return (x + 7) // 8 * 8
 
 
-def gemm_tn(A, B, out, bias, M, N, K, lda, ldb, ldc, accum=False, kernel="tc"):
+GEMM_KERNELS = {"tma": 0, "tc": 1, "mma": 2}
+
+
+def gemm_tn(A, B, out, bias, M, N, K, lda, ldb, ldc, accum=False, kernel=None):
     """out[M][N] (FP32) = A[M][K] . B[N][K]^T (+ bias) (+ out); BF16 operands.
-    kernel "tc": the tcgen05 kernel; "mma": the mma.sync one."""
-    fn = lib().bpnet_gemm_tn if kernel == "tc" else lib().bpnet_gemm_tn_mma
-    _ck(fn(_p(A), _p(B), _p(out), _p(bias), M, N, K, lda, ldb, ldc, int(accum), _s()), "bpnet_gemm_tn")
+    kernel None: the library's default (tcgen05, TMA-fed); "tma", "tc" (tcgen05
+    with register-staged operands) or "mma" (mma.sync) to choose."""
+    if kernel is None:
+        rc = lib().bpnet_gemm_tn(_p(A), _p(B), _p(out), _p(bias), M, N, K, lda, ldb, ldc, int(accum), _s())
+    else:
+        rc = lib().bpnet_gemm_tn_mode(GEMM_KERNELS[kernel], _p(A), _p(B), _p(out), _p(bias), M, N, K, lda, ldb,
+                                      ldc, int(accum), _s())
+    _ck(rc, "bpnet_gemm_tn")
 
 
 def gemm_status() -> int:
@@ -508,3 +517,54 @@ def predict(net: UNet, models: Sequence[configs.BPModel]):
     x = torch.tensor(feats, dtype=torch.float32, device="cuda").to(torch.bfloat16).contiguous()
     out = net.forward(x, periodic, train=False).cpu().numpy() * net.out_scale
     return [guess_from_output(m, o) for m, o in zip(models, out)]
+
+
+# ---------------------------------------------------------------------
+# timing of the GEMM kernels on the U-Net's shapes
+# ---------------------------------------------------------------------
+GEMM_SHAPES = (("forward, level 0, input", 524288, 32, 56), ("forward, level 0", 524288, 32, 288),
+               ("forward, level 1", 131072, 64, 576), ("forward, level 2", 32768, 96, 864),
+               ("forward, level 3", 8192, 128, 1152), ("head", 524288, 24, 32),
+               ("weight gradient, level 0", 32, 288, 524288), ("weight gradient, level 1", 64, 576, 131072),
+               ("weight gradient, level 3", 128, 1152, 8192), ("input gradient, level 0", 524288, 288, 32),
+               ("input gradient, level 1", 131072, 576, 64))
+
+
+def gemm_timings(reps: int = 10):
+    """CUDA-event time of every GEMM kernel on the products of one training
+    step of the marine network (batch 8 of 256 x 256 grids), and its
+    relative error against the FP32 product of the same BF16 operands."""
+    torch = _torch()
+    rows = []
+    for name, M, N, K in GEMM_SHAPES:
+        a = torch.randn(M, K, device="cuda").to(torch.bfloat16)
+        b = torch.randn(N, K, device="cuda").to(torch.bfloat16)
+        c = torch.empty(M, N, device="cuda")
+        ref = a.float() @ b.float().T
+        row = {"product": name, "M": M, "N": N, "K": K}
+        for kern in GEMM_KERNELS:
+            gemm_tn(a, b, c, None, M, N, K, K, K, N, kernel=kern)
+            torch.cuda.synchronize()
+            err = float((c - ref).norm() / ref.norm())
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(reps):
+                gemm_tn(a, b, c, None, M, N, K, K, K, N, kernel=kern)
+            e1.record()
+            torch.cuda.synchronize()
+            us = e0.elapsed_time(e1) / reps * 1e3
+            row[kern] = {"us": round(us, 1), "tflops": round(2.0 * M * N * K / (us * 1e-6) / 1e12, 1),
+                         "rel_err": float("%.2e" % err)}
+        rows.append(row)
+        del a, b, c, ref
+    return rows
+
+
+if __name__ == "__main__":
+    import json
+    import sys
+
+    if sys.argv[1:] == ["gemm"]:
+        for r in gemm_timings():
+            print(json.dumps(r), flush=True)
+        print(json.dumps({"gemm_status": gemm_status()}))
