@@ -854,7 +854,9 @@ int bpnet_gemm_tn_mode(int mode, const void* A, const void* B, float* C, const f
   }
   const dim3 grid(gx, gy, S);
   CUtensorMap ma, mb;
-  if (mode == 0 && tma_map(&ma, A, M, K, lda, TC_BM) && tma_map(&mb, B, N, K, ldb, bn)) {
+  // a product of one K slice has no pipeline to fill: the register-staged
+  // kernel starts sooner (measured faster at K <= 64, slower above)
+  if (mode == 0 && nslices > 1 && tma_map(&ma, A, M, K, lda, TC_BM) && tma_map(&mb, B, N, K, ldb, bn)) {
     if (narrow)
       k_gemm_tma<32><<<grid, 128, tm_smem_bytes<32>(), st>>>(ma, mb, out, bout, M, N, K, ldo, acc, kchunk, cs);
     else
@@ -870,9 +872,9 @@ int bpnet_gemm_tn_mode(int mode, const void* A, const void* B, float* C, const f
   return cudaGetLastError() == cudaSuccess ? 0 : 6;
 }
 
-// The product on the default kernel: tcgen05 with TMA-fed operands;
-// BPNET_GEMM=tc selects the register-staged tcgen05 kernel, BPNET_GEMM=mma
-// the mma.sync one.
+// The product on the default kernel: tcgen05 with TMA-fed operands (with
+// register-staged ones for a single K slice); BPNET_GEMM=tc selects the
+// register-staged tcgen05 kernel throughout, BPNET_GEMM=mma the mma.sync one.
 int bpnet_gemm_tn(const void* A, const void* B, float* C, const float* bias, int M, int N, int K, int lda,
                   int ldb, int ldc, int accum, void* stream) {
   static const int mode = [] {
