@@ -18,7 +18,8 @@ with the workload's solver -- for the marine workloads the reference's
 default SIA column preconditioner and Chronopoulos-Gear PCG) and the
 additions: mixed precision (FP32-inner / FP64-refined), batching (all
 domains in one resident problem) and the learned guess (the U-Net behind
-the C ABI).  The headline `value` is learned + mixed + batched; `paths`
+the C ABI); the marine workloads also time the mixed batched solve from
+the shallow-ice velocity (sia_mixed_batched), the classical start.  The headline `value` is learned + mixed + batched; `paths`
 lists every path with its iterations and its distance to P's answer.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
@@ -109,7 +110,8 @@ def make_models(args):
 
 
 class Path:
-    """One way of solving the workload: start (zero | learned), precision,
+    """One way of solving the workload: start (zero | sia: the shallow-ice
+    velocity, guess.sia_guess | learned), precision,
     preconditioner (None: the workload's; "diag" | "sia" to override), PCG
     variant (the workload's | Chronopoulos-Gear), batched (all domains in
     one resident problem) or one domain at a time."""
@@ -152,6 +154,7 @@ def paths_for(args, have_net):
     if args.workload in ("c4", "c2"):
         P = [Path("plain_fp64", "zero", False, None, False, False),
              Path("mixed" + sfx, "zero", True, None, False, multi)]
+        P.append(Path("sia_mixed" + sfx, "sia", True, None, False, multi))
         if have_net:
             P += [Path("learned_fp64" + sfx, "learned", False, None, False, multi),
                   Path("learned_mixed" + sfx, "learned", True, None, False, multi)]
@@ -389,16 +392,24 @@ def run_path(ctx, path, models, args, D, steps, warmup, weights, clocks=None):
     mode = solver.GUESS_LEARNED if path.start == "learned" else solver.GUESS_GIVEN
     ms_ = [path.model(m) for m in models]
     preps = [solver.prepare(m, precision=prec, inner_tol=args.refine_eta, guess_mode=mode)[0] for m in ms_]
-    zeros = [np.zeros(m.vshape3) for m in ms_]
-    probs = [ctx.problem(preps)] if path.batched else [ctx.problem([p]) for p in preps]
+    if path.start == "sia":  # the shallow-ice velocity (host arrays, copied in every step)
+        from cism_b200 import guess
 
-    def guesses(pb):
-        return [None if mode == solver.GUESS_LEARNED else z for z in zeros[:pb.n]]
+        starts = [guess.sia_guess(m) for m in ms_]
+    else:
+        starts = [(np.zeros(m.vshape3), np.zeros(m.vshape3)) for m in ms_]
+    probs = [ctx.problem(preps)] if path.batched else [ctx.problem([p]) for p in preps]
+    first = [0]
+    for pb in probs[:-1]:
+        first.append(first[-1] + pb.n)
 
     def step():
         sts = []
-        for pb in probs:
-            pb.set_guess(guesses(pb), guesses(pb))  # learned: the network runs on the device here
+        for pb, f0 in zip(probs, first):
+            if mode == solver.GUESS_LEARNED:  # the network runs on the device here
+                pb.set_guess([None] * pb.n, [None] * pb.n)
+            else:
+                pb.set_guess([u for u, _ in starts[f0:f0 + pb.n]], [v for _, v in starts[f0:f0 + pb.n]])
             sts += pb.run()
         return sts
 
