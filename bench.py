@@ -84,6 +84,9 @@ def parse_args(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-run", action="store_true",
                     help="one untimed run of --paths (first path) (for ncu launch lists / captures)")
+    ap.add_argument("--weights", default=None,
+                    help="U-Net weights (.bin) for the learned paths of any 3-D workload (default: the "
+                         "workload's own network, where it has one)")
     ap.add_argument("--picard-cap", type=int, default=0,
                     help="with --profile-run: stop after this many Picard iterations")
     return ap.parse_args(argv)
@@ -181,7 +184,9 @@ def headline_name(paths):
     return names[-1]
 
 
-def weights_path(workload):
+def weights_path(workload, override=None):
+    if override:
+        return override if os.path.exists(override) else None
     name = WEIGHTS.get(workload)
     if not name:
         return None
@@ -485,7 +490,7 @@ def run_ours(args, D):
 
     ctx = solver.Context(D.local)
     models = make_models(args)
-    weights = weights_path(args.workload)
+    weights = weights_path(args.workload, args.weights)
     if weights:
         ctx.load_guess(weights)
     paths = paths_for(args, weights is not None)
@@ -665,7 +670,7 @@ def profile_run(args):
     if args.picard_cap > 0:
         models = [m.copy(maxiter_nonlinear=args.picard_cap) for m in models]
     ctx = solver.Context(0)
-    w = weights_path(args.workload)
+    w = weights_path(args.workload, args.weights)
     if w:
         ctx.load_guess(w)
     p = paths_for(args, w is not None)[0]

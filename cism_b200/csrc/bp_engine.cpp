@@ -202,15 +202,15 @@ DevView make_view(Arena& a, cudaStream_t s, const HostPlan& p, bool with_cells, 
     v.qp = a.get<double>(s, "qp", (size_t)p.nelem * 80);
     v.efvs = a.get<double>(s, "efvs", p.nefvs);
     // element-centric 3-D assembly (k_asm_elem + gather): the element blocks
-    // of one assembly, 2 KiB per element, when they take at most 8 GiB and a
-    // quarter of the free device memory; otherwise (or BP_ASM_ELEM=0) each
+    // of one assembly, 2 KiB per element, when they take at most 32 GiB and
+    // a quarter of the free device memory; otherwise (or BP_ASM_ELEM=0) each
     // row integrates its incident elements itself.  Both give the same
     // matrix bitwise.
     if (!p.solve2d && p.nelem > 0) {
       const char* e = std::getenv("BP_ASM_ELEM");
       const size_t bytes = (size_t)p.nelem * 256 * sizeof(double);
       size_t free_b = 0, total_b = 0;
-      if (!(e && e[0] == '0') && bytes <= ((size_t)8 << 30) &&
+      if (!(e && e[0] == '0') && bytes <= ((size_t)32 << 30) &&
           cudaMemGetInfo(&free_b, &total_b) == cudaSuccess && bytes <= free_b / 4)
         v.Ke = a.get<double>(s, "Ke", (size_t)p.nelem * 256);
     }
