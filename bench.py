@@ -62,7 +62,9 @@ PICARD_DESC = {4: "relative nonlinear residual |A(u)u-b|/|b| < 1e-7 (which_ho_re
 # per-domain Picard / PCG iteration counts of the plain FP64 path, by
 # workload, used to extrapolate the bounded CPU samples to whole solves
 ITERATION_COUNTS = os.path.join(ROOT, "profiles", "iteration_counts.json")
-WEIGHTS = {"c4": "unet_marine", "c2": "unet_marine"}
+# the marine network also serves the c3 ensemble (domes and slabs it never
+# saw in training: its features are the solve's own fields)
+WEIGHTS = {"c4": "unet_marine", "c2": "unet_marine", "c3": "unet_marine"}
 HELDOUT_SEED = 70000  # past every training seed of the marine network
 ASM_FLOP_PER_ELEMENT = 18.1e3  # 8 quadrature points x ~2.2k + scatter (FP64)
 
