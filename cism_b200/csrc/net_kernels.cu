@@ -412,9 +412,9 @@ inline unsigned grid_for(long long n) {
 // ---------------------------------------------------------------------
 constexpr int TC_BM = 128, TC_BK = 64;
 constexpr int TC_A_BYTES = TC_BM * TC_BK * 2;
-// BN = 64, or 32 for the products with at most 32 output columns
+// BN = 64, 32 for the products with at most 32 output columns, or 128
 template <int BN>
-constexpr int tc_stage_bytes() { return TC_A_BYTES + BN * TC_BK * 2; }  // 24 or 20 KB; two stages
+constexpr int tc_stage_bytes() { return TC_A_BYTES + BN * TC_BK * 2; }  // 20, 24 or 32 KB
 
 __device__ int g_tc_err = 0;  // a wait of k_gemm_tc ran out (read and cleared by bpnet_gemm_status)
 
@@ -803,6 +803,26 @@ float* splitk_scratch(size_t n) {
   return b.first;
 }
 
+// One tcgen05 product of tile width W: TMA-fed (maps given) or register-staged.
+template <int W>
+void launch_tile(bool tma, const CUtensorMap& ma, const CUtensorMap& mb, dim3 grid, cudaStream_t st,
+                 const bf16* A, const bf16* B, float* out, const float* bout, int M, int N, int K, int lda, int ldb,
+                 int ldo, int acc, int kchunk, long long cs) {
+  if (tma)
+    k_gemm_tma<W><<<grid, 128, tm_smem_bytes<W>(), st>>>(ma, mb, out, bout, M, N, K, ldo, acc, kchunk, cs);
+  else
+    k_gemm_tc<W><<<grid, 128, 2 * tc_stage_bytes<W>(), st>>>(A, B, out, bout, M, N, K, lda, ldb, ldo, acc, kchunk,
+                                                             cs);
+}
+
+template <int W>
+bool tile_smem_ok() {
+  return cudaFuncSetAttribute(k_gemm_tc<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * tc_stage_bytes<W>()) ==
+             cudaSuccess &&
+         cudaFuncSetAttribute(k_gemm_tma<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, tm_smem_bytes<W>()) ==
+             cudaSuccess;
+}
+
 }  // namespace
 
 extern "C" {
@@ -817,15 +837,7 @@ extern "C" {
 int bpnet_gemm_tn_mode(int mode, const void* A, const void* B, float* C, const float* bias, int M, int N, int K,
                        int lda, int ldb, int ldc, int accum, void* stream) {
   if (M <= 0 || N <= 0 || K <= 0 || (K % 8) || (lda % 8) || (ldb % 8) || mode < 0 || mode > 2) return 10;
-  static const bool smem_ok =
-      cudaFuncSetAttribute(k_gemm_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           2 * tc_stage_bytes<64>()) == cudaSuccess &&
-      cudaFuncSetAttribute(k_gemm_tc<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           2 * tc_stage_bytes<32>()) == cudaSuccess &&
-      cudaFuncSetAttribute(k_gemm_tma<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, tm_smem_bytes<64>()) ==
-          cudaSuccess &&
-      cudaFuncSetAttribute(k_gemm_tma<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, tm_smem_bytes<32>()) ==
-          cudaSuccess;
+  static const bool smem_ok = tile_smem_ok<32>() && tile_smem_ok<64>() && tile_smem_ok<128>();
   if (!smem_ok) return 6;
   cudaStream_t st = (cudaStream_t)stream;
   if (mode == 2) {
@@ -833,8 +845,14 @@ int bpnet_gemm_tn_mode(int mode, const void* A, const void* B, float* C, const f
     k_gemm_tn<<<grid, 128, 0, st>>>((const bf16*)A, (const bf16*)B, C, bias, M, N, K, lda, ldb, ldc, accum);
     return cudaGetLastError() == cudaSuccess ? 0 : 6;
   }
-  const bool narrow = N <= 32;  // a 128 x 32 tile: no MMA work on padding columns
-  const int bn = narrow ? 32 : 64;
+  // tile width: 32 for at most 32 columns (no MMA work on padding); 128
+  // where it pads no more than 64 does (A is read once for both halves);
+  // else 64
+  int bn = 64;
+  if (N <= 32)
+    bn = 32;
+  else if ((N + 127) / 128 * 128 <= (N + 63) / 64 * 64)
+    bn = 128;
   const int gx = (N + bn - 1) / bn, gy = (M + TC_BM - 1) / TC_BM, nslices = (K + TC_BK - 1) / TC_BK;
   int S = 1, kchunk = nslices * TC_BK;
   if (gx * gy < 296 && nslices >= 64) S = std::min((296 + gx * gy - 1) / (gx * gy), nslices / 16);
@@ -856,18 +874,15 @@ int bpnet_gemm_tn_mode(int mode, const void* A, const void* B, float* C, const f
   CUtensorMap ma, mb;
   // a product of one K slice has no pipeline to fill: the register-staged
   // kernel starts sooner (measured faster at K <= 64, slower above)
-  if (mode == 0 && nslices > 1 && tma_map(&ma, A, M, K, lda, TC_BM) && tma_map(&mb, B, N, K, ldb, bn)) {
-    if (narrow)
-      k_gemm_tma<32><<<grid, 128, tm_smem_bytes<32>(), st>>>(ma, mb, out, bout, M, N, K, ldo, acc, kchunk, cs);
-    else
-      k_gemm_tma<64><<<grid, 128, tm_smem_bytes<64>(), st>>>(ma, mb, out, bout, M, N, K, ldo, acc, kchunk, cs);
-  } else if (narrow) {
-    k_gemm_tc<32><<<grid, 128, 2 * tc_stage_bytes<32>(), st>>>((const bf16*)A, (const bf16*)B, out, bout, M, N, K,
-                                                               lda, ldb, ldo, acc, kchunk, cs);
-  } else {
-    k_gemm_tc<64><<<grid, 128, 2 * tc_stage_bytes<64>(), st>>>((const bf16*)A, (const bf16*)B, out, bout, M, N, K,
-                                                               lda, ldb, ldo, acc, kchunk, cs);
-  }
+  const bool tma =
+      mode == 0 && nslices > 1 && tma_map(&ma, A, M, K, lda, TC_BM) && tma_map(&mb, B, N, K, ldb, bn);
+  const bf16 *a16 = (const bf16*)A, *b16 = (const bf16*)B;
+  if (bn == 32)
+    launch_tile<32>(tma, ma, mb, grid, st, a16, b16, out, bout, M, N, K, lda, ldb, ldo, acc, kchunk, cs);
+  else if (bn == 64)
+    launch_tile<64>(tma, ma, mb, grid, st, a16, b16, out, bout, M, N, K, lda, ldb, ldo, acc, kchunk, cs);
+  else
+    launch_tile<128>(tma, ma, mb, grid, st, a16, b16, out, bout, M, N, K, lda, ldb, ldo, acc, kchunk, cs);
   if (S > 1) k_splitk_sum<<<grid_for(cs), 256, 0, st>>>(out, S, cs, C, bias, M, N, ldc, accum);
   return cudaGetLastError() == cudaSuccess ? 0 : 6;
 }

@@ -106,12 +106,14 @@ def _device_setup(periodic, B=2, H=16, W=24, channels=(8, 8, 16, 16), n_out=8, s
 @pytest.mark.gpu
 @pytest.mark.parametrize("kernel", ["tma", "tc", "mma"])
 @pytest.mark.parametrize("shape", [(64, 64, 64), (100, 40, 72), (7, 130, 8), (256, 96, 1160), (300, 24, 48),
-                                   (96, 1440, 64), (130, 64, 1000), (32, 288, 8192), (64, 200, 4104)])
+                                   (96, 1440, 64), (130, 64, 1000), (200, 128, 640), (32, 288, 8192),
+                                   (64, 200, 4104)])
 def test_gemm_matches_bf16_product(shape, kernel):
     # the tcgen05 kernels -- operands by TMA boxes into a four-stage ring
     # ("tma", the default) or by register-staged loads in two stages ("tc");
-    # 128 x 64 tiles (128 x 32 for at most 32 columns); the last two shapes
-    # split K, the weight-gradient form -- and the mma.sync one against the
+    # 128 x 64, 128 x 32 (at most 32 columns) and 128 x 128 tiles (N = 96,
+    # 128, 200); the last two shapes split K, the weight-gradient form -- and
+    # the mma.sync one against the
     # FP64 product of the same BF16 operands
     torch = pytest.importorskip("torch")
     from cism_b200 import net as netmod
