@@ -846,12 +846,14 @@ int bpnet_gemm_tn_mode(int mode, const void* A, const void* B, float* C, const f
     return cudaGetLastError() == cudaSuccess ? 0 : 6;
   }
   // tile width: 32 for at most 32 columns (no MMA work on padding); 128
-  // where it pads no more than 64 does (A is read once for both halves);
-  // else 64
+  // for widths that are not a multiple of 64 where it pads no more than 64
+  // does (96: one tile instead of 64 + 32, A read once); else 64 (a
+  // multiple of 64 keeps twice the CTAs: 128 x 128 tiles measured slower at
+  // N = 128 and 1152)
   int bn = 64;
   if (N <= 32)
     bn = 32;
-  else if ((N + 127) / 128 * 128 <= (N + 63) / 64 * 64)
+  else if (N % 64 != 0 && (N + 127) / 128 * 128 <= (N + 63) / 64 * 64)
     bn = 128;
   const int gx = (N + bn - 1) / bn, gy = (M + TC_BM - 1) / TC_BM, nslices = (K + TC_BK - 1) / TC_BK;
   int S = 1, kchunk = nslices * TC_BK;
