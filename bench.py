@@ -564,7 +564,7 @@ def run_ours(args, D):
     tr = committed_traffic("mixed" if hp.mixed else "fp64")
     roof = {"bound": "hbm",
             "kernel": "%s (Krylov matvec, thread per node, %s)" % (
-                "k_cg_mv" if hp.cg else "k_std_mv",
+                "k_cg_mv" if hp.describe(models[0])["pcg"] == "chronopoulos_gear" else "k_std_mv",
                 "FP32 half storage + compensated FP64 diagonal" if hp.mixed else "FP64 half storage"),
             "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4) if peak else None,
