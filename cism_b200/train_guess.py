@@ -115,9 +115,17 @@ def make_marine_set(ctx, sizes, count: int, seed: int, batch: int, log=None, dea
     return {n: (M, np.stack(F), np.stack(T), np.stack(K)) for n, (M, F, T, K) in out.items() if M}
 
 
+def step_size(lr: float, frac: float, warm: float = 0.03) -> float:
+    """Adam's step size at the fraction `frac` of the schedule: a linear
+    ramp to `lr` over the first `warm` of it, then a cosine decay to zero."""
+    if frac < warm:
+        return lr * frac / warm
+    return lr * 0.5 * (1.0 + math.cos(math.pi * min((frac - warm) / (1.0 - warm), 1.0)))
+
+
 def train(model: net.UNet, groups, epochs: int, lr: float, batch: int, seed: int, log=None, periodic: int = 1,
           deadline=None):
-    """groups: list of (features [N,H,W,5], targets [N,H,W,C][, masks
+    """groups: list of (features [N,H,W,n_in], targets [N,H,W,C][, masks
     [N,H,W]]) of one size each, already normalised.  Adam; the step size
     ramps up linearly over the first 3% of the schedule, then decays as a
     cosine; stops at the deadline (time.time()) if given."""
@@ -157,10 +165,7 @@ def train(model: net.UNet, groups, epochs: int, lr: float, batch: int, seed: int
             frac = t / total
             if deadline is not None:  # the schedule also follows the time left
                 frac = max(frac, (time.time() - t_start) / max(deadline - t_start, 1.0))
-            warm = 0.03
-            step = (lr * frac / warm if frac < warm else
-                    lr * 0.5 * (1.0 + math.cos(math.pi * min((frac - warm) / (1.0 - warm), 1.0))))
-            model.adam(step, t)
+            model.adam(step_size(lr, frac), t)
             el += loss
         hist.append(el / len(order))
         if log and (ep % 10 == 0 or ep == epochs - 1):

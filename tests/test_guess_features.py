@@ -87,3 +87,18 @@ def test_bench_models_and_networks():
     assert bench.weights_path("c1") is None
     assert bench.weights_path("c1", os.path.join(ROOT, "cism_b200", "weights", "unet_marine.bin"))
     assert bench.weights_path("c4", "/nonexistent.bin") is None
+
+
+def test_training_step_size_schedule():
+    from cism_b200.train_guess import step_size
+
+    lr = 6e-4
+    assert step_size(lr, 0.0) == 0.0
+    assert step_size(lr, 0.015) == pytest.approx(lr / 2)  # halfway up the ramp
+    assert step_size(lr, 0.03) == pytest.approx(lr)  # the peak
+    assert step_size(lr, 0.03 + 0.97 / 2) == pytest.approx(lr / 2)  # halfway down the cosine
+    assert step_size(lr, 1.0) == pytest.approx(0.0, abs=1e-18)
+    assert step_size(lr, 1.5) == pytest.approx(0.0, abs=1e-18)  # past the deadline: stays at zero
+    xs = np.linspace(0.03, 1.0, 50)
+    ys = [step_size(lr, x) for x in xs]
+    assert all(a >= b for a, b in zip(ys, ys[1:]))  # monotone decay after the ramp
